@@ -1,0 +1,335 @@
+"""Generate the golden fixtures of this directory from the reference's own NumPy backend.
+
+Run by hand, in a container that holds the reference checkout (``SOLPROP_REFERENCE``,
+default ``/root/reference``): ``python tests/golden/generate.py``.  It backports the
+reference package into a temporary directory (``backport.py`` beside this file),
+builds small problems through the reference's own translation layer with
+caller-supplied species data (the reference's material library is not installed), runs
+the reference's ``numpy_ref`` backend on them, and writes for each case
+
+* ``<case>.problem.npz`` -- the lowered problem record (``solprop_b200.lowering``);
+* ``<case>.golden.npz``  -- the reference's outputs: one source evaluation per
+  listed lab field with its intermediate passes, a fixed-schedule run's planes, and an
+  adaptive run's planes and step history.
+
+The species data are published fits (Börzsönyi et al., Appl. Opt. 47, 4856 (2008) for
+the refractive index), the reference's own test-only ADK rate oracle
+(``tests/rate_oracles.py``) and literature hyperpolarisabilities; absolute physics
+differs from a solprop install with its material library, which does not matter for
+parity: the build and the reference are compared on identical problem arrays.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import time
+import warnings
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(HERE))
+sys.path.insert(0, str(ROOT))
+
+import backport  # noqa: E402
+
+backport.activate()
+sys.path.insert(0, str(backport.REFERENCE / "tests"))
+
+from rate_oracles import HISTORICAL_ATOMS, adk_oracle  # noqa: E402
+from solprop.backends.events import ObservationReady, Progress  # noqa: E402
+from solprop.backends.numpy_ref import NumpyRefBackend  # noqa: E402
+from solprop.backends.numpy_ref.passes.plasma import (  # noqa: E402
+    held_plasma_spectrum,
+    ionisation_rate,
+    plasma_scan,
+)
+from solprop.backends.numpy_ref.passes.responses import nonlinear_sources  # noqa: E402
+from solprop.backends.numpy_ref.passes.stepping import absorber_term, stage_output  # noqa: E402
+from solprop.backends.numpy_ref.passes.transforms import (  # noqa: E402
+    project,
+    synthesise,
+    to_frequency,
+    to_time,
+)
+from solprop.backends.session import Start  # noqa: E402
+from solprop.constants import AU_ENERGY, K_B  # noqa: E402
+from solprop.constants import C as C0  # noqa: E402
+from solprop.driver.simulation import Simulation  # noqa: E402
+from solprop.grid import EnvelopeGrid, FieldGrid  # noqa: E402
+from solprop.physdata.mixtures import Mixture  # noqa: E402
+from solprop.physdata.species import (  # noqa: E402
+    IdealGas,
+    IonisationData,
+    Species,
+    TabulatedSusceptibility,
+)
+from solprop.stepper import FixedSchedule, RungeKutta  # noqa: E402
+
+from solprop_b200.lowering import lower  # noqa: E402
+from solprop_b200.record import save_record  # noqa: E402
+
+warnings.simplefilter("ignore")
+
+# Börzsönyi two-pole fits (B1, C1 um^2, B2, C2 um^2) at 1 bar, 0 C.
+BORZSONYI = {
+    "He": (4977.77e-8, 28.54e-6, 1856.94e-8, 7.76e-3),
+    "Ne": (9154.48e-8, 656.97e-6, 4018.63e-8, 5.728e-3),
+    "Ar": (20332.29e-8, 206.12e-6, 34458.31e-8, 8.066e-3),
+}
+# Hyperpolarisabilities gamma3 in m^5/V^2 of the order the literature gives.
+GAMMA3 = {"He": 3.43e-53, "Ne": 6.8e-53, "Ar": 1.2e-51}
+
+
+def gas_species(name: str) -> Species:
+    lam = np.geomspace(120e-9, 200e-6, 4000)[::-1]
+    om = 2 * np.pi * C0 / lam
+    l2 = (lam * 1e6) ** 2
+    b1, c1, b2, c2 = BORZSONYI[name]
+    n2m1 = b1 * l2 / (l2 - c1) + b2 * l2 / (l2 - c2)
+    rho0 = 1e5 / (K_B * 273.15)
+    refr = (np.sqrt(1 + n2m1) - 1) / rho0
+    sus = TabulatedSusceptibility(
+        om, refr, np.zeros_like(om), (121e-9, 199e-6), f"Borzsonyi 2008 {name}"
+    )
+    ip = HISTORICAL_ATOMS[name][0] * AU_ENERGY
+    return Species(name, sus, IdealGas(), gamma3=GAMMA3[name], ionisation=IonisationData(ip))
+
+
+def capillary(name, *, gas, pressure, length, n_t_limits, trange, energy, fwhm, modes,
+              n_r=None, radial_rule="gauss_kronrod", absorber=None, schedule=None,
+              n_save=3, rtol=1e-6):
+    species = gas_species(gas)
+    fill = Mixture.fill({species: 1.0}, pressure, length=length if not np.isscalar(pressure) else None)
+    grid = FieldGrid.from_limits(length, 800e-9, n_t_limits, trange, fft_size="pow2")
+    kwargs = dict(
+        wavelength=800e-9, grid=grid, fwhm=fwhm, energy=energy, cladding=1.45 + 0j,
+        modes=modes, plasma=adk_oracle(gas), noise=None, rtol=rtol, n_save=n_save,
+        backend="numpy_ref",
+    )
+    if n_r is not None:
+        kwargs.update(n_r=n_r, radial_rule=radial_rule)
+    if absorber is not None:
+        kwargs["absorber"] = absorber
+    if schedule is not None:
+        kwargs["schedule"] = schedule
+    return Simulation.from_capillary(125e-6, length, fill, None, **kwargs)
+
+
+def drive(sim):
+    """Run the reference backend's session; return plane positions, states, history."""
+    problem, request = sim.translate(), sim.run_request()
+    backend = NumpyRefBackend(problem, request, grid=sim.grid, modes=sim.modes,
+                              profiles=sim.profiles)
+    session = backend.prepare(problem, request).start(Start.entrance(problem))
+    ws = backend._workspace
+    zs, states, hist = [], [], []
+    t0 = time.time()
+    while not session.finished:
+        batch = session.advance()
+        for ev in batch.events:
+            if isinstance(ev, Progress):
+                continue
+            h = getattr(ev, "history", None)
+            if h is not None and len(h.z):
+                hist.append(np.stack([h.z, h.dz, h.error_norm, h.accepted.astype(float)], 1))
+            if isinstance(ev, ObservationReady):
+                zs.append(ev.z if hasattr(ev, "z") else np.nan)
+                states.append(np.array(ws.committed()))
+            err = getattr(ev, "error", None)
+            if err is not None:
+                raise err
+        session.acknowledge(batch.receipt)
+    wall = time.time() - t0
+    status = session.status()
+    counts = np.array([getattr(status, "attempts", -1), getattr(status, "rejected", -1)])
+    history = np.concatenate(hist) if hist else np.zeros((0, 4))
+    return problem, np.array(zs), np.array(states), (history, counts), wall
+
+
+def source_passes(problem, ws, lab, z, keep_nodes):
+    """One source evaluation, pass by pass, checked against ``lab_source``."""
+    grids, transform, responses = problem.grids, problem.transform, problem.responses
+    kind = problem.grid_kind
+    bundle = ws.stage_scalars(z, z)
+    src = ws.stage_source
+    modal_t = to_time(lab, grids.crop_index, grids.n_to, kind=kind)
+    n_pol = transform._n_pol
+    field_t = synthesise(modal_t, transform.synthesis, bundle.taper_scale, n_pol)
+    raman = src._raman_spectrum(bundle.raman_rates, bundle.raman_densities)
+    sources = nonlinear_sources(
+        field_t, responses, grids.t_window_fine, kind=kind, density=bundle.density,
+        preionisation=bundle.preionisation, dt=grids.dt_fine, carrier=grids.carrier_2w0,
+        raman_spectrum=raman, scalars=bundle,
+    )
+    out = {"modal_t": modal_t, "field_nodes": field_t[keep_nodes],
+           "polarisation_nodes": sources.polarisation[keep_nodes]}
+    projected = project(sources.polarisation, transform.projection, bundle.taper_scale, n_pol)
+    spectrum = to_frequency(projected, grids.crop_index, kind=kind)
+    out["projected"] = projected
+    if sources.current is not None:
+        out["current_nodes"] = sources.current[keep_nodes]
+        rate = ionisation_rate(field_t, responses.ionisation_table[0])
+        frac, _ = plasma_scan(field_t, rate, responses.plasma_channels[0],
+                              preionisation=bundle.preionisation, dt=grids.dt_fine,
+                              integral=responses.plasma_integral)
+        out["rate_nodes"] = rate[keep_nodes]
+        out["fraction_nodes"] = frac[keep_nodes]
+        gated = project(grids.t_window_fine * sources.current, transform.projection,
+                        bundle.taper_scale, n_pol)
+        edge = project(grids.t_window_fine_derivative * sources.current, transform.projection,
+                       bundle.taper_scale, n_pol)
+        out["gated"], out["edge"] = gated, edge
+        spectrum = spectrum + held_plasma_spectrum(gated, edge, grids.omega, grids.crop_index,
+                                                   grids.active_mask)
+    if raman is not None:
+        out["raman_spectrum"] = np.asarray(raman)
+    out["spectrum"] = spectrum
+    absorb = None
+    if responses.temporal_absorber_fine is not None and responses.absorber_scheme == "nonlinear":
+        absorb = absorber_term(modal_t, responses.temporal_absorber_fine, None,
+                               grids.crop_index, grids.active_mask, kind=kind)
+        out["absorber"] = absorb
+    prefactor = ws.prefactor(bundle)
+    k = stage_output(spectrum, prefactor, grids.omega_window, np.ones(problem.shape), absorb)
+    ref = ws.lab_source(lab, z)
+    err = np.linalg.norm(k - ref) / max(np.linalg.norm(ref), 1e-300)
+    assert err < 1e-13, f"pass-by-pass source differs from lab_source: {err}"
+    out["source"] = ref
+    return out
+
+
+def source_fixture(sim, problem, zs_eval, seed):
+    request = sim.run_request()
+    backend = NumpyRefBackend(problem, request, grid=sim.grid, modes=sim.modes,
+                              profiles=sim.profiles)
+    ws = backend._workspace
+    rng = np.random.default_rng(seed)
+    field0 = np.broadcast_to(problem.initial.field0, problem.shape)
+    n_nodes = problem.transform.synthesis.shape[0] // problem.transform._n_pol
+    keep = np.unique(np.linspace(0, n_nodes - 1, min(3, n_nodes)).astype(int))
+    golden = {"src.keep_nodes": keep}
+    labs = [field0.copy()]
+    phase = np.exp(1j * rng.uniform(-0.3, 0.3, size=problem.shape))
+    scale = 1.0 + 0.2 * rng.standard_normal(problem.shape)
+    labs.append(field0 * phase * scale * problem.grids.active_mask)
+    for i, (lab, z) in enumerate(zip(labs, zs_eval)):
+        passes = source_passes(problem, ws, lab, z, keep)
+        golden[f"src{i}.lab"] = lab
+        golden[f"src{i}.z"] = np.array(z)
+        for key, value in passes.items():
+            if i == 0 or key == "source":
+                golden[f"src{i}.{key}"] = value
+    return golden
+
+
+def write(case, problem, golden):
+    record = lower(problem)
+    save_record(record, HERE / f"{case}.problem.npz")
+    np.savez_compressed(HERE / f"{case}.golden.npz", **golden)
+    size = sum((HERE / f"{case}.{k}.npz").stat().st_size for k in ("problem", "golden"))
+    print(f"{case}: wrote {size / 1024:.0f} KiB")
+
+
+def cap_case(case, *, gas, pressure, length, limits, trange, energy, fwhm, modes, n_r,
+             radial_rule, fixed_dz, n_fixed_planes, seed):
+    common = dict(gas=gas, pressure=pressure, length=length, n_t_limits=limits,
+                  trange=trange, energy=energy, fwhm=fwhm, modes=modes, n_r=n_r,
+                  radial_rule=radial_rule)
+    sim = capillary(case, **common)
+    problem = sim.translate()
+    golden = source_fixture(sim, problem, [0.0, 0.37 * length], seed)
+    # Adaptive run with the route's defaults (in-stage collar, exponential Adams).
+    _, zs, states, (hist, counts), wall = drive(capillary(case, **common, n_save=3))
+    golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.history": hist,
+                   "adaptive.counts": counts, "adaptive.wall": np.array(wall)})
+    print(f"{case}: adaptive run {counts} attempts/rejected in {wall:.2f} s")
+    # Fixed schedule without the collar, so that steps of physical size are stable.
+    planes = np.linspace(0.0, length, n_fixed_planes)
+    schedule = FixedSchedule.uniform(0.0, length, fixed_dz, save_planes=planes)
+    fixed_sim = capillary(case, **common, absorber=False, schedule=schedule,
+                          n_save=n_fixed_planes)
+    fixed_problem, zs, states, (hist, counts), wall = drive(fixed_sim)
+    golden.update({"fixed.z": zs, "fixed.states": states, "fixed.history": hist})
+    write(case, problem, golden)
+    save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
+    print(f"{case}: fixed run {len(hist)} steps in {wall:.2f} s")
+
+
+def gnlse_case(case, seed):
+    """An envelope GNLSE with Kerr, self-steepening and a Blow-Wood Raman line, DOPRI5."""
+    from solprop.nonlinear.gnlse import problem_from, raman_susceptibility
+    from solprop.nonlinear.raman import RamanResponse, normalised_damped_oscillator
+    from solprop.pulses import GaussianPulse
+    from solprop.stepper import PIController
+    from solprop.translate.assembly import assemble
+
+    length = 0.05
+    grid = EnvelopeGrid.from_limits(length, 1030e-9, (700e-9, 1600e-9), 4e-12, fft_size="pow2")
+    betas = [0.0, 0.0, 2.2e-26, 8e-41]
+    gnlse = problem_from(betas, omega_ref=grid.omega0, gamma=0.01, raman=False,
+                         raman_fraction=0.18, shock=True)
+    n2 = 0.01 * 1.0 / (grid.omega0 / C0)
+    line = normalised_damped_oscillator(raman_susceptibility(n2), 1.0 / 12.2e-15, 32e-15)
+    raman = RamanResponse(models=(line,), fraction=0.18, thg=False)
+    start = GaussianPulse(wavelength=1030e-9, fwhm=200e-15, energy=20e-9).build(grid)
+
+    def build(save_planes, schedule=None):
+        return assemble(grid, gnlse.mode, [gnlse.kerr, raman], start,
+                        controller=PIController(rtol=1e-6, atol=1e-14),
+                        save_planes=save_planes, dz_max=0.01, dz_init=1e-4,
+                        density=1.0, shock=True, prefactor_index=1.0, schedule=schedule)
+
+    def run(problem, request):
+        backend = NumpyRefBackend(problem, request, grid=grid, modes=[gnlse.mode])
+        session = backend.prepare(problem, request).start(Start.entrance(problem))
+        ws = backend._workspace
+        zs, states = [], []
+        while not session.finished:
+            batch = session.advance()
+            for ev in batch.events:
+                if isinstance(ev, ObservationReady):
+                    zs.append(ev.z)
+                    states.append(np.array(ws.committed()))
+                err = getattr(ev, "error", None)
+                if err is not None:
+                    raise err
+            session.acknowledge(batch.receipt)
+        status = session.status()
+        return np.array(zs), np.array(states), np.array([status.attempts, status.rejected])
+
+    class _Sim:
+        pass
+
+    problem, request = build([0.025, length])
+    sim = _Sim()
+    sim.run_request = lambda: request
+    sim.grid, sim.modes, sim.profiles = grid, [gnlse.mode], None
+    golden = source_fixture(sim, problem, [0.0, 0.02], seed)
+    zs, states, counts = run(problem, request)
+    golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.counts": counts})
+    print(f"{case}: adaptive RK run {counts} attempts/rejected")
+    planes = np.linspace(0.0, length, 11)[1:]
+    fixed_problem, fixed_request = build(
+        planes, FixedSchedule.uniform(0.0, length, 0.0005, save_planes=planes))
+    zs, states, counts = run(fixed_problem, fixed_request)
+    golden.update({"fixed.z": zs, "fixed.states": states})
+    write(case, problem, golden)
+    save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
+
+
+if __name__ == "__main__":
+    only = set(sys.argv[1:])
+    if not only or "cap1_ar" in only:
+        cap_case("cap1_ar", gas="Ar", pressure=1.0, length=0.02, limits=(200e-9, 4e-6),
+                 trange=100e-15, energy=30e-6, fwhm=10e-15, modes=1, n_r=None,
+                 radial_rule="gauss_kronrod", fixed_dz=0.001, n_fixed_planes=11, seed=1)
+    if not only or "cap4_he" in only:
+        cap_case("cap4_he", gas="He", pressure=(0.8, 0.0), length=0.05, limits=(150e-9, 4e-6),
+                 trange=150e-15, energy=100e-6, fwhm=7.5e-15, modes=4, n_r=16,
+                 radial_rule="gauss", fixed_dz=0.005, n_fixed_planes=11, seed=2)
+    if not only or "gnlse_raman" in only:
+        gnlse_case("gnlse_raman", seed=3)
