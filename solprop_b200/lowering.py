@@ -66,11 +66,13 @@ def lower(problem) -> ProblemRecord:
         phi_terms = np.asarray(linear.phi_constant)[np.newaxis]
         phi_weights = None
         phi_rep = "constant"
+        phi_rate = None
     else:
         expansion = linear.phi_expansion
         phi_terms = np.asarray(expansion.terms)
         phi_weights = _table(expansion.weights)
         phi_rep = "expansion"
+        phi_rate = _table(linear.rate)
     if responses.prefactor_constant is not None:
         pre_terms = np.asarray(responses.prefactor_constant)[np.newaxis]
         pre_weights = None
@@ -106,6 +108,7 @@ def lower(problem) -> ProblemRecord:
         phi_representation=phi_rep,
         phi_terms=np.ascontiguousarray(phi_terms, dtype=np.complex128),
         phi_weights=phi_weights,
+        phi_rate=phi_rate,
         hard_kinks=np.asarray(linear.hard_kinks, dtype=np.float64),
         breakpoints=np.asarray(linear.phi_breakpoints, dtype=np.float64),
         prefactor_terms=np.ascontiguousarray(pre_terms, dtype=np.complex128),

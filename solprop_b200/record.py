@@ -144,6 +144,7 @@ class ProblemRecord:
     phi_representation: str = "constant"  # "constant" | "expansion"
     phi_terms: np.ndarray | None = None  # (n_phi, n_modes, n_pol, n_omega) c128
     phi_weights: PiecewiseTable | None = None  # expansion: Phi(z) weights
+    phi_rate: PiecewiseTable | None = None  # expansion: D(z) = dPhi/dz weights
     hard_kinks: np.ndarray = field(default_factory=lambda: np.zeros(0))
     breakpoints: np.ndarray = field(default_factory=lambda: np.zeros(0))
     prefactor_terms: np.ndarray | None = None  # (n_pre, n_modes, n_pol, n_omega) c128
@@ -218,12 +219,21 @@ class ProblemRecord:
         assert self.phi_weights is not None
         return self.phi_weights(z1) - self.phi_weights(z0)
 
-    def phi_rate_weights(self, z: float) -> np.ndarray:
-        """Weights of ``D(z) = dPhi/dz`` (``translate/linop.py:2286-2335``)."""
+    def phi_rate_weights(self, z: float, before: bool = False) -> np.ndarray:
+        """Weights of ``D(z) = dPhi/dz`` (``translate/linop.py:2286-2423``).
+
+        A position on an interval edge reads the interval starting there unless
+        ``before`` asks for the one ending there (``linop.py:2402-2405``).
+        """
         if self.phi_representation == "constant":
             return np.array([1.0])
-        assert self.phi_weights is not None
-        return self.phi_weights.derivative()(z)
+        table = self.phi_rate if self.phi_rate is not None else self.phi_weights.derivative()
+        k = table.interval(z)
+        if before and k > 0 and z <= table.breakpoints[k]:
+            k -= 1
+        lo, hi = table.breakpoints[k], table.breakpoints[k + 1]
+        one = PiecewiseTable(np.array([lo, hi]), table.coefficients[k:k + 1])
+        return one(z)
 
     def prefactor_weights_at(self, z: float) -> np.ndarray:
         """Weights of the prefactor at ``z`` (``translate/stage.py:745-761``)."""

@@ -108,7 +108,7 @@ def capillary(name, *, gas, pressure, length, n_t_limits, trange, energy, fwhm, 
     kwargs = dict(
         wavelength=800e-9, grid=grid, fwhm=fwhm, energy=energy, cladding=1.45 + 0j,
         modes=modes, plasma=adk_oracle(gas), noise=None, rtol=rtol, n_save=n_save,
-        backend="numpy_ref",
+        backend="numpy_ref", boundary_check=None,
     )
     if n_r is not None:
         kwargs.update(n_r=n_r, radial_rule=radial_rule)
@@ -119,12 +119,38 @@ def capillary(name, *, gas, pressure, length, n_t_limits, trange, energy, fwhm, 
     return Simulation.from_capillary(125e-6, length, fill, None, **kwargs)
 
 
+def policy_record(session, request):
+    """The march's policy and first proposal, as JSON bytes for the golden file."""
+    import dataclasses
+    import json
+
+    march = session._method.march
+    policy = march._policy
+    values = {}
+    for f in dataclasses.fields(policy):
+        v = getattr(policy, f.name)
+        if dataclasses.is_dataclass(v):
+            v = {g.name: getattr(v, g.name) for g in dataclasses.fields(v)
+                 if not isinstance(getattr(v, g.name), np.ndarray)}
+        elif isinstance(v, np.ndarray):
+            v = v.tolist()
+        elif isinstance(v, tuple):
+            v = list(v)
+        values[f.name] = v
+    control = request.stepper.controller
+    values["rtol"], values["atol"] = float(control.rtol), float(control.atol)
+    values["march"] = type(march).__name__
+    values["proposal"] = float(march.state.proposal)
+    return np.frombuffer(json.dumps(values, default=float).encode(), dtype=np.uint8)
+
+
 def drive(sim):
     """Run the reference backend's session; return plane positions, states, history."""
     problem, request = sim.translate(), sim.run_request()
     backend = NumpyRefBackend(problem, request, grid=sim.grid, modes=sim.modes,
                               profiles=sim.profiles)
     session = backend.prepare(problem, request).start(Start.entrance(problem))
+    drive.policy = policy_record(session, request)
     ws = backend._workspace
     zs, states, hist = [], [], []
     t0 = time.time()
@@ -245,7 +271,8 @@ def cap_case(case, *, gas, pressure, length, limits, trange, energy, fwhm, modes
     # Adaptive run with the route's defaults (in-stage collar, exponential Adams).
     _, zs, states, (hist, counts), wall = drive(capillary(case, **common, n_save=3))
     golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.history": hist,
-                   "adaptive.counts": counts, "adaptive.wall": np.array(wall)})
+                   "adaptive.counts": counts, "adaptive.wall": np.array(wall),
+                   "adaptive.policy": drive.policy})
     print(f"{case}: adaptive run {counts} attempts/rejected in {wall:.2f} s")
     # Fixed schedule without the collar, so that steps of physical size are stable.
     planes = np.linspace(0.0, length, n_fixed_planes)
@@ -253,7 +280,8 @@ def cap_case(case, *, gas, pressure, length, limits, trange, energy, fwhm, modes
     fixed_sim = capillary(case, **common, absorber=False, schedule=schedule,
                           n_save=n_fixed_planes)
     fixed_problem, zs, states, (hist, counts), wall = drive(fixed_sim)
-    golden.update({"fixed.z": zs, "fixed.states": states, "fixed.history": hist})
+    golden.update({"fixed.z": zs, "fixed.states": states, "fixed.history": hist,
+                   "fixed.policy": drive.policy})
     write(case, problem, golden)
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
     print(f"{case}: fixed run {len(hist)} steps in {wall:.2f} s")
@@ -286,6 +314,7 @@ def gnlse_case(case, seed):
     def run(problem, request):
         backend = NumpyRefBackend(problem, request, grid=grid, modes=[gnlse.mode])
         session = backend.prepare(problem, request).start(Start.entrance(problem))
+        run.policy = policy_record(session, request)
         ws = backend._workspace
         zs, states = [], []
         while not session.finished:
@@ -310,13 +339,14 @@ def gnlse_case(case, seed):
     sim.grid, sim.modes, sim.profiles = grid, [gnlse.mode], None
     golden = source_fixture(sim, problem, [0.0, 0.02], seed)
     zs, states, counts = run(problem, request)
-    golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.counts": counts})
+    golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.counts": counts,
+                   "adaptive.policy": run.policy})
     print(f"{case}: adaptive RK run {counts} attempts/rejected")
     planes = np.linspace(0.0, length, 11)[1:]
     fixed_problem, fixed_request = build(
         planes, FixedSchedule.uniform(0.0, length, 0.0005, save_planes=planes))
     zs, states, counts = run(fixed_problem, fixed_request)
-    golden.update({"fixed.z": zs, "fixed.states": states})
+    golden.update({"fixed.z": zs, "fixed.states": states, "fixed.policy": run.policy})
     write(case, problem, golden)
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
 
