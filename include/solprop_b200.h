@@ -1,0 +1,166 @@
+/*
+ * solprop_b200.h -- the C ABI of the B200 propagation library.
+ *
+ * The library executes solprop's propagation hot path: the UPPE/GNLSE right-hand side
+ * (one "source evaluation") and its exponential-Adams and embedded Runge-Kutta
+ * steppers, in FP64, on one CUDA device.  Every entry point takes plain pointers and
+ * sizes; complex arrays are interleaved (re, im) doubles in C order, exactly the
+ * memory of NumPy's complex128.  Every function returns an sp_status; the message of
+ * the last failure on the calling thread is read with sp_last_error().
+ *
+ * Each entry point names the interface of the reference (LupoLab/solprop, paths inside
+ * that repository) whose role it takes:
+ *   problem   <- native/src/solprop_native/_core.pyi:51-428       (_core.Problem)
+ *   workspace <- native/src/solprop_native/_core.pyi:600-612      (_core.Workspace)
+ *   session   <- native/src/solprop_native/_core.pyi:430-470      (_core.Session)
+ *   source    <- src/solprop/backends/numpy_ref/workspace.py:819 (lab_source), the
+ *                native trial's source evaluation (native/src/general/trial.cpp:697)
+ */
+#ifndef SOLPROP_B200_H
+#define SOLPROP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int sp_status;
+enum {
+  SP_OK = 0,
+  SP_ERR_ARGUMENT = 1,   /* a pointer, size or value the call cannot take */
+  SP_ERR_REFUSED = 2,    /* a problem this backend does not execute (BackendRefusal) */
+  SP_ERR_CUDA = 3,       /* a CUDA runtime failure; the message names the call */
+  SP_ERR_STATE = 4,      /* a lifecycle error: closed object, run not started */
+  SP_ERR_CONVERGENCE = 5 /* step control fell below dz_min, or the field diverged */
+};
+
+/* A piecewise Chebyshev series in z (solprop translate/chebyshev.py:236): interval i
+ * holds n_deg coefficients of n_values values, c[(i*n_deg + j)*n_values + v].
+ * n_intervals == 0 means "absent". */
+typedef struct sp_table {
+  int32_t n_intervals, n_deg, n_values;
+  const double* breakpoints;  /* n_intervals + 1 */
+  const double* coefficients; /* n_intervals * n_deg * n_values */
+} sp_table;
+
+/* The lowered problem (solprop_b200.record.ProblemRecord; kernel-contract.md 1-6). */
+typedef struct sp_problem_desc {
+  int32_t grid_kind; /* 0 field (r2c/c2r), 1 envelope (c2c) */
+  int32_t n_modes, n_pol, n_omega, n_t, n_to, n_nodes, n_pol_transform;
+  double omega0, dt, dt_fine, z_end;
+  const double* omega;               /* n_omega */
+  const int64_t* crop_index;         /* n_omega: position in the fine spectrum */
+  const uint8_t* active_mask;        /* n_omega */
+  const uint8_t* norm_mask;          /* n_omega */
+  const double* omega_window;        /* n_omega */
+  const double* t_window;            /* n_to */
+  const double* t_window_derivative; /* n_to */
+  const double* carrier;             /* complex n_to, or NULL */
+  /* Phi = sum_j w_j(z) phi_terms[j]; constant: one term, weight z1 - z0. */
+  int32_t phi_expansion;
+  int32_t n_phi_terms;
+  const double* phi_terms; /* complex (n_phi_terms, n_modes, n_pol, n_omega) */
+  sp_table phi_weights;    /* expansion: Phi(z) weights, n_values = n_phi_terms */
+  sp_table phi_rate;       /* expansion: dPhi/dz weights */
+  int32_t n_prefactor_terms;
+  const double* prefactor_terms; /* complex (n_prefactor_terms, n_modes, n_pol, n_omega) */
+  sp_table prefactor_weights;    /* absent: the one constant term, weight 1 */
+  sp_table density, kerr_density, plasma_density, preionisation, taper_scale;
+  const double* synthesis;  /* (n_nodes*n_pol_transform, n_modes), pad scale inside */
+  const double* projection; /* (n_modes, n_nodes*n_pol_transform), weights inside */
+  /* Kerr (translate/responses.py:235-275) */
+  int32_t kerr_enabled, kerr_analytic; /* analytic: 1 for the envelope cubic form */
+  double kerr_coefficient, kerr_self, kerr_conjugate, kerr_harmonic;
+  int32_t kerr_take_real;
+  /* field plasma, one channel (translate/ionisation.py:95-323) */
+  int32_t plasma_enabled;
+  double charge_mass_ratio, ionisation_potential;
+  int32_t rate_intervals;
+  const double* rate_coefficients; /* (4, rate_intervals) */
+  double log_field_min, d_log_field, field_min, field_max, rate_max;
+  int32_t band; /* 1: band rule with taps and the exposure floor; 0: trapezoid */
+  int32_t n_taps;
+  const double* taps; /* centre first */
+  /* Raman, scalar (translate/raman.py; kernel-contract.md 5) */
+  int32_t raman_enabled, raman_terms, raman_thg;
+  const double* raman_undamped; /* (raman_terms, 2*n_to) */
+  sp_table raman_rates[4];
+  double raman_fraction;
+  sp_table raman_density;
+  /* the in-stage temporal absorber (stepping.py:286-369) */
+  int32_t absorber_in_stage;
+  const double* temporal_absorber_fine; /* n_to */
+} sp_problem_desc;
+
+typedef struct sp_problem sp_problem;
+typedef struct sp_workspace sp_workspace;
+typedef struct sp_session sp_session;
+
+/* A run: the march's policy (backends adams_core MarchPolicy / RungeKuttaPolicy). */
+typedef struct sp_run_desc {
+  int32_t method;          /* 0 exponential Adams, 1 DOPRI5 */
+  const double* field0;    /* complex (n_modes, n_pol, n_omega) */
+  double z_start, proposal, rtol, atol;
+  double dz_min, dz_max, stretch, z_end;
+  const double* save_planes; int32_t n_save_planes;
+  const double* hard_kinks; int32_t n_hard_kinks;
+  const double* breakpoints; int32_t n_breakpoints;
+  const double* schedule; int32_t n_schedule; /* fixed steps, or NULL for adaptive */
+  /* Adams */
+  int32_t order, variable_order, restart_after, equal_approach;
+  double safety, max_growth, min_factor, rejection_growth, hysteresis;
+  double collar_stability, collar_rate;
+  double real_intervals[8];
+  /* Runge-Kutta PI controller */
+  double beta1, beta2, max_factor;
+  int32_t lag, estimator_order;
+} sp_run_desc;
+
+/* What one advance() returns (the _core.SessionBatch / SessionEvent essentials). */
+typedef struct sp_batch {
+  int32_t event;       /* 0 none (work limit), 1 plane reached, 2 finished, 3 failed */
+  int32_t plane_index; /* the save plane reached, or -1 */
+  double z;            /* position after the batch */
+  int64_t attempts, rejected, evaluations; /* cumulative counts of the run */
+} sp_batch;
+
+/* ---- library ---- */
+/* Copies the message of the last failure on this thread into buf (NUL-terminated). */
+size_t sp_last_error(char* buf, size_t len);
+/* Version string of this build, e.g. "solprop-b200 0.1 sm_100a". */
+const char* sp_version(void);
+/* Number of CUDA devices visible, or a negative sp_status on failure. */
+int sp_device_count(void);
+
+/* ---- problem (replaces _core.Problem, native _core.pyi:51-428) ---- */
+sp_status sp_problem_create(const sp_problem_desc* desc, sp_problem** out);
+sp_status sp_problem_destroy(sp_problem* problem);
+
+/* ---- workspace (replaces _core.Workspace(problem), _core.pyi:600-612) ---- */
+sp_status sp_workspace_create(const sp_problem* problem, int device, sp_workspace** out);
+sp_status sp_workspace_destroy(sp_workspace* ws);
+/* One source evaluation F at a lab-frame field, untransported (numpy_ref
+ * workspace.py:819 lab_source): lab and out are host complex (n_modes,n_pol,n_omega).
+ * quiet != 0 leaves a quiet in-stage collar out (numpy_ref source.py:858-890). */
+sp_status sp_workspace_source(sp_workspace* ws, const double* lab, double z, int quiet,
+                              double* out);
+/* The same on device pointers, on the workspace's stream; for timing. */
+sp_status sp_workspace_source_device(sp_workspace* ws, const void* lab_device, double z,
+                                     int quiet, void* out_device);
+/* Kernel launches one source evaluation makes (the evidence of the device path). */
+int sp_workspace_launches_per_source(const sp_workspace* ws);
+
+/* ---- session (replaces _core.Session, _core.pyi:430-470) ---- */
+sp_status sp_session_start(sp_workspace* ws, const sp_run_desc* run, sp_session** out);
+/* Step until a save plane, the end, or work_limit attempts (the native call's bound). */
+sp_status sp_session_advance(sp_session* s, int32_t work_limit, sp_batch* out);
+/* Copies the current state to out, host complex (n_modes, n_pol, n_omega). */
+sp_status sp_session_export(sp_session* s, double* out);
+sp_status sp_session_destroy(sp_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOLPROP_B200_H */

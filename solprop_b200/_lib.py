@@ -1,0 +1,383 @@
+"""ctypes binding of the C ABI (``include/solprop_b200.h``).
+
+The structures mirror the header field for field.  Nothing here computes: every call
+forwards to ``libsolprop_b200.so``, which must have been built (``python -m
+solprop_b200.build``); a missing library is an error, never a fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIBRARY_PATH = Path(__file__).resolve().parent / "libsolprop_b200.so"
+
+SP_OK = 0
+STATUS_NAMES = {1: "argument", 2: "refused", 3: "cuda", 4: "state", 5: "convergence"}
+
+
+class SpTable(C.Structure):
+    _fields_ = [("n_intervals", C.c_int32), ("n_deg", C.c_int32), ("n_values", C.c_int32),
+                ("breakpoints", C.POINTER(C.c_double)), ("coefficients", C.POINTER(C.c_double))]
+
+
+class SpProblemDesc(C.Structure):
+    _fields_ = [
+        ("grid_kind", C.c_int32),
+        ("n_modes", C.c_int32), ("n_pol", C.c_int32), ("n_omega", C.c_int32), ("n_t", C.c_int32),
+        ("n_to", C.c_int32), ("n_nodes", C.c_int32), ("n_pol_transform", C.c_int32),
+        ("omega0", C.c_double), ("dt", C.c_double), ("dt_fine", C.c_double), ("z_end", C.c_double),
+        ("omega", C.POINTER(C.c_double)), ("crop_index", C.POINTER(C.c_int64)),
+        ("active_mask", C.POINTER(C.c_uint8)), ("norm_mask", C.POINTER(C.c_uint8)),
+        ("omega_window", C.POINTER(C.c_double)), ("t_window", C.POINTER(C.c_double)),
+        ("t_window_derivative", C.POINTER(C.c_double)), ("carrier", C.POINTER(C.c_double)),
+        ("phi_expansion", C.c_int32), ("n_phi_terms", C.c_int32),
+        ("phi_terms", C.POINTER(C.c_double)), ("phi_weights", SpTable), ("phi_rate", SpTable),
+        ("n_prefactor_terms", C.c_int32), ("prefactor_terms", C.POINTER(C.c_double)),
+        ("prefactor_weights", SpTable),
+        ("density", SpTable), ("kerr_density", SpTable), ("plasma_density", SpTable),
+        ("preionisation", SpTable), ("taper_scale", SpTable),
+        ("synthesis", C.POINTER(C.c_double)), ("projection", C.POINTER(C.c_double)),
+        ("kerr_enabled", C.c_int32), ("kerr_analytic", C.c_int32),
+        ("kerr_coefficient", C.c_double), ("kerr_self", C.c_double),
+        ("kerr_conjugate", C.c_double), ("kerr_harmonic", C.c_double),
+        ("kerr_take_real", C.c_int32),
+        ("plasma_enabled", C.c_int32), ("charge_mass_ratio", C.c_double),
+        ("ionisation_potential", C.c_double), ("rate_intervals", C.c_int32),
+        ("rate_coefficients", C.POINTER(C.c_double)),
+        ("log_field_min", C.c_double), ("d_log_field", C.c_double), ("field_min", C.c_double),
+        ("field_max", C.c_double), ("rate_max", C.c_double),
+        ("band", C.c_int32), ("n_taps", C.c_int32), ("taps", C.POINTER(C.c_double)),
+        ("raman_enabled", C.c_int32), ("raman_terms", C.c_int32), ("raman_thg", C.c_int32),
+        ("raman_undamped", C.POINTER(C.c_double)), ("raman_rates", SpTable * 4),
+        ("raman_fraction", C.c_double), ("raman_density", SpTable),
+        ("absorber_in_stage", C.c_int32), ("temporal_absorber_fine", C.POINTER(C.c_double)),
+    ]
+
+
+class SpRunDesc(C.Structure):
+    _fields_ = [
+        ("method", C.c_int32), ("field0", C.POINTER(C.c_double)),
+        ("z_start", C.c_double), ("proposal", C.c_double), ("rtol", C.c_double), ("atol", C.c_double),
+        ("dz_min", C.c_double), ("dz_max", C.c_double), ("stretch", C.c_double), ("z_end", C.c_double),
+        ("save_planes", C.POINTER(C.c_double)), ("n_save_planes", C.c_int32),
+        ("hard_kinks", C.POINTER(C.c_double)), ("n_hard_kinks", C.c_int32),
+        ("breakpoints", C.POINTER(C.c_double)), ("n_breakpoints", C.c_int32),
+        ("schedule", C.POINTER(C.c_double)), ("n_schedule", C.c_int32),
+        ("order", C.c_int32), ("variable_order", C.c_int32), ("restart_after", C.c_int32),
+        ("equal_approach", C.c_int32),
+        ("safety", C.c_double), ("max_growth", C.c_double), ("min_factor", C.c_double),
+        ("rejection_growth", C.c_double), ("hysteresis", C.c_double),
+        ("collar_stability", C.c_double), ("collar_rate", C.c_double),
+        ("real_intervals", C.c_double * 8),
+        ("beta1", C.c_double), ("beta2", C.c_double), ("max_factor", C.c_double),
+        ("lag", C.c_int32), ("estimator_order", C.c_int32),
+    ]
+
+
+class SpBatch(C.Structure):
+    _fields_ = [("event", C.c_int32), ("plane_index", C.c_int32), ("z", C.c_double),
+                ("attempts", C.c_int64), ("rejected", C.c_int64), ("evaluations", C.c_int64)]
+
+
+# the exported functions: name -> (restype, argtypes)
+SIGNATURES = {
+    "sp_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "sp_version": (C.c_char_p, []),
+    "sp_device_count": (C.c_int, []),
+    "sp_problem_create": (C.c_int, [C.POINTER(SpProblemDesc), C.POINTER(C.c_void_p)]),
+    "sp_problem_destroy": (C.c_int, [C.c_void_p]),
+    "sp_workspace_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "sp_workspace_destroy": (C.c_int, [C.c_void_p]),
+    "sp_workspace_source": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_double, C.c_int,
+                                      C.POINTER(C.c_double)]),
+    "sp_workspace_source_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p]),
+    "sp_workspace_launches_per_source": (C.c_int, [C.c_void_p]),
+    "sp_session_start": (C.c_int, [C.c_void_p, C.POINTER(SpRunDesc), C.POINTER(C.c_void_p)]),
+    "sp_session_advance": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SpBatch)]),
+    "sp_session_export": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "sp_session_destroy": (C.c_int, [C.c_void_p]),
+}
+
+_LIB: C.CDLL | None = None
+
+
+class NativeError(RuntimeError):
+    """A failure the library reported, with its status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{STATUS_NAMES.get(status, status)}] {message}")
+        self.status = status
+
+
+class BackendRefusal(NativeError):
+    """The library refuses this problem by name (``SP_ERR_REFUSED``)."""
+
+
+def library() -> C.CDLL:
+    """Load ``libsolprop_b200.so`` once; raise if it has not been built."""
+    global _LIB
+    if _LIB is None:
+        if not LIBRARY_PATH.exists():
+            raise ImportError(
+                f"{LIBRARY_PATH} is missing: build it with `python -m solprop_b200.build` "
+                "(this package has no CPU path)")
+        lib = C.CDLL(str(LIBRARY_PATH))
+        for name, (restype, argtypes) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _LIB = lib
+    return _LIB
+
+
+def check(status: int) -> None:
+    if status != SP_OK:
+        buf = C.create_string_buffer(4096)
+        library().sp_last_error(buf, 4096)
+        message = buf.value.decode(errors="replace")
+        raise (BackendRefusal if status == 2 else NativeError)(status, message)
+
+
+def _ptr(array: np.ndarray | None, ctype=C.c_double):
+    if array is None:
+        return C.POINTER(ctype)()
+    return array.ctypes.data_as(C.POINTER(ctype))
+
+
+class Marshalled:
+    """A record's arrays converted to the C layout, kept alive beside the descriptor."""
+
+    def __init__(self):
+        self.keep: list[np.ndarray] = []
+
+    def f64(self, a) -> C.POINTER(C.c_double):
+        if a is None:
+            return C.POINTER(C.c_double)()
+        arr = np.ascontiguousarray(a, dtype=np.float64)
+        self.keep.append(arr)
+        return _ptr(arr)
+
+    def c128(self, a) -> C.POINTER(C.c_double):
+        if a is None:
+            return C.POINTER(C.c_double)()
+        arr = np.ascontiguousarray(a, dtype=np.complex128)
+        self.keep.append(arr)
+        return arr.ctypes.data_as(C.POINTER(C.c_double))
+
+    def u8(self, a):
+        arr = np.ascontiguousarray(np.asarray(a).astype(np.uint8))
+        self.keep.append(arr)
+        return _ptr(arr, C.c_uint8)
+
+    def i64(self, a):
+        arr = np.ascontiguousarray(a, dtype=np.int64)
+        self.keep.append(arr)
+        return _ptr(arr, C.c_int64)
+
+    def table(self, t) -> SpTable:
+        out = SpTable()
+        if t is None:
+            return out
+        c = np.ascontiguousarray(t.coefficients, dtype=np.float64)
+        out.n_intervals, out.n_deg, out.n_values = c.shape
+        out.breakpoints = self.f64(t.breakpoints)
+        out.coefficients = self.f64(c)
+        return out
+
+
+def problem_desc(rec) -> tuple[SpProblemDesc, Marshalled]:
+    """The C descriptor of a :class:`solprop_b200.record.ProblemRecord`."""
+    m = Marshalled()
+    d = SpProblemDesc()
+    d.grid_kind = 0 if rec.grid_kind == "field" else 1
+    d.n_modes, d.n_pol, d.n_omega = rec.n_modes, rec.n_pol, rec.n_omega
+    d.n_t, d.n_to, d.n_nodes, d.n_pol_transform = rec.n_t, rec.n_to, rec.n_nodes, rec.n_pol_transform
+    d.omega0, d.dt, d.dt_fine, d.z_end = rec.omega0, rec.dt, rec.dt_fine, rec.z_end
+    d.omega = m.f64(rec.omega)
+    d.crop_index = m.i64(rec.crop_index)
+    d.active_mask = m.u8(rec.active_mask)
+    d.norm_mask = m.u8(rec.norm_mask)
+    d.omega_window = m.f64(rec.omega_window)
+    d.t_window = m.f64(rec.t_window)
+    d.t_window_derivative = m.f64(rec.t_window_derivative)
+    d.carrier = m.c128(rec.carrier)
+    d.phi_expansion = int(rec.phi_representation == "expansion")
+    d.n_phi_terms = rec.n_phi_terms
+    d.phi_terms = m.c128(rec.phi_terms)
+    d.phi_weights = m.table(rec.phi_weights)
+    d.phi_rate = m.table(rec.phi_rate)
+    d.n_prefactor_terms = rec.n_prefactor_terms
+    d.prefactor_terms = m.c128(rec.prefactor_terms)
+    d.prefactor_weights = m.table(rec.prefactor_weights)
+    d.density = m.table(rec.density)
+    d.kerr_density = m.table(rec.kerr_density)
+    d.plasma_density = m.table(rec.plasma_density)
+    d.preionisation = m.table(rec.preionisation)
+    d.taper_scale = m.table(rec.taper_scale)
+    d.synthesis = m.f64(rec.synthesis)
+    d.projection = m.f64(rec.projection)
+    d.kerr_enabled = int(rec.kerr_enabled)
+    d.kerr_analytic = int(rec.kerr_form != "real")
+    d.kerr_coefficient = rec.kerr_coefficient
+    d.kerr_self, d.kerr_conjugate, d.kerr_harmonic = rec.kerr_self, rec.kerr_conjugate, rec.kerr_harmonic
+    d.kerr_take_real = int(rec.kerr_take_real)
+    d.plasma_enabled = int(rec.plasma_enabled)
+    if rec.plasma_enabled:
+        d.charge_mass_ratio = rec.charge_mass_ratio
+        d.ionisation_potential = rec.ionisation_potential
+        d.rate_intervals = rec.rate_coefficients.shape[1]
+        d.rate_coefficients = m.f64(rec.rate_coefficients)
+        d.log_field_min, d.d_log_field = rec.log_field_min, rec.d_log_field
+        d.field_min, d.field_max, d.rate_max = rec.field_min, rec.field_max, rec.rate_max
+        d.band = int(rec.integral_policy == "band")
+        d.n_taps = rec.taps.size
+        d.taps = m.f64(rec.taps)
+    d.raman_enabled = int(rec.raman_enabled)
+    if rec.raman_enabled:
+        d.raman_terms = rec.raman_undamped.shape[0]
+        d.raman_thg = int(rec.raman_thg)
+        d.raman_undamped = m.f64(rec.raman_undamped)
+        for i, t in enumerate(rec.raman_rates[:4]):
+            d.raman_rates[i] = m.table(t)
+        d.raman_fraction = rec.raman_fraction
+        d.raman_density = m.table(rec.raman_density)
+    d.absorber_in_stage = int(rec.absorber_scheme == "nonlinear")
+    d.temporal_absorber_fine = m.f64(rec.temporal_absorber_fine)
+    return d, m
+
+
+def run_desc(rec, policy: dict, *, field0=None, schedule=None) -> tuple[SpRunDesc, Marshalled]:
+    """The C run descriptor from a march policy dict (``MarchPolicy`` / ``RungeKuttaPolicy``)."""
+    m = Marshalled()
+    r = SpRunDesc()
+    adams = policy.get("march", "HostAdamsMarch") == "HostAdamsMarch"
+    r.method = 0 if adams else 1
+    r.field0 = m.c128(rec.field0 if field0 is None else field0)
+    r.z_start = 0.0
+    r.proposal = float(policy["proposal"])
+    control = policy.get("controller", policy)
+    r.rtol, r.atol = float(control["rtol"]), float(control["atol"])
+    r.dz_min, r.dz_max = float(policy["dz_min"]), float(policy["dz_max"])
+    r.stretch, r.z_end = float(policy["stretch"]), float(policy["z_end"])
+    planes = np.asarray(policy.get("save_planes", []), dtype=np.float64)
+    kinks = np.asarray(policy.get("hard_kinks", []), dtype=np.float64)
+    edges = np.asarray(policy.get("breakpoints", [0.0, r.z_end]), dtype=np.float64)
+    r.save_planes, r.n_save_planes = m.f64(planes), planes.size
+    r.hard_kinks, r.n_hard_kinks = m.f64(kinks), kinks.size
+    r.breakpoints, r.n_breakpoints = m.f64(edges), edges.size
+    if schedule is not None:
+        steps = np.asarray(schedule, dtype=np.float64)
+        r.schedule, r.n_schedule = m.f64(steps), steps.size
+    if adams:
+        r.order = int(policy["order"])
+        r.variable_order = int(policy["variable_order"])
+        r.restart_after = int(policy["restart_after"])
+        r.equal_approach = int(policy["equal_approach"])
+        r.safety = float(policy["safety"])
+        r.max_growth = float(policy["max_growth"])
+        r.min_factor = float(policy["min_factor"])
+        r.rejection_growth = float(policy["rejection_growth"])
+        r.hysteresis = float(policy["hysteresis"])
+        r.collar_stability = float(policy["collar_stability"])
+        r.collar_rate = float(policy["collar_rate"])
+        for i, v in enumerate(policy["real_intervals"][:8]):
+            r.real_intervals[i] = float(v)
+    else:
+        r.safety = float(control["safety"])
+        r.min_factor = float(control["min_factor"])
+        r.max_factor = float(control["max_factor"])
+        r.beta1, r.beta2 = float(control["beta1"]), float(control["beta2"])
+        r.lag = int(control["lag"])
+        r.estimator_order = int(control["estimator_order"])
+    return r, m
+
+
+class Problem:
+    """A problem owned by the library (``sp_problem``)."""
+
+    def __init__(self, rec):
+        self.handle = None
+        lib = library()
+        self.record = rec
+        desc, self._keep = problem_desc(rec)
+        handle = C.c_void_p()
+        check(lib.sp_problem_create(C.byref(desc), C.byref(handle)))
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None):
+            library().sp_problem_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+
+class Workspace:
+    """Device buffers of one problem (``sp_workspace``; native ``_core.Workspace``)."""
+
+    def __init__(self, problem: Problem, device: int = 0):
+        self.handle = None
+        self.problem = problem
+        handle = C.c_void_p()
+        check(library().sp_workspace_create(problem.handle, device, C.byref(handle)))
+        self.handle = handle
+        self.shape = (problem.record.n_modes, problem.record.n_pol, problem.record.n_omega)
+
+    def source(self, lab: np.ndarray, z: float, quiet: bool = False) -> np.ndarray:
+        """One source evaluation at a lab-frame field (numpy_ref ``lab_source``)."""
+        lab = np.ascontiguousarray(np.broadcast_to(lab, self.shape), dtype=np.complex128)
+        out = np.empty(self.shape, dtype=np.complex128)
+        check(library().sp_workspace_source(
+            self.handle, lab.ctypes.data_as(C.POINTER(C.c_double)), float(z), int(quiet),
+            out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def source_device(self, lab_ptr: int, z: float, out_ptr: int, quiet: bool = False) -> None:
+        check(library().sp_workspace_source_device(self.handle, C.c_void_p(lab_ptr), float(z),
+                                                   int(quiet), C.c_void_p(out_ptr)))
+
+    @property
+    def launches_per_source(self) -> int:
+        return int(library().sp_workspace_launches_per_source(self.handle))
+
+    def start(self, policy: dict, *, field0=None, schedule=None) -> "Session":
+        return Session(self, policy, field0=field0, schedule=schedule)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            library().sp_workspace_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+
+class Session:
+    """One run on a workspace (``sp_session``; native ``_core.Session``)."""
+
+    def __init__(self, ws: Workspace, policy: dict, *, field0=None, schedule=None):
+        self.handle = None
+        self.ws = ws
+        desc, keep = run_desc(ws.problem.record, policy, field0=field0, schedule=schedule)
+        handle = C.c_void_p()
+        check(library().sp_session_start(ws.handle, C.byref(desc), C.byref(handle)))
+        self.handle = handle
+        self.batch = SpBatch()
+
+    def advance(self, work_limit: int = 256) -> SpBatch:
+        check(library().sp_session_advance(self.handle, int(work_limit), C.byref(self.batch)))
+        return self.batch
+
+    def export(self) -> np.ndarray:
+        out = np.empty(self.ws.shape, dtype=np.complex128)
+        check(library().sp_session_export(self.handle, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            library().sp_session_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close

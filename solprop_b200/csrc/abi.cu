@@ -1,0 +1,1066 @@
+// The C ABI of the library (include/solprop_b200.h): problem, workspace and session
+// objects, the host evaluation of the stage scalars (translate/stage.py:413-503, the
+// Clenshaw pass of translate/chebyshev.py:138-198), and the two marches -- exponential
+// Adams (backends/adams_core.py, numpy_ref/marches/adams.py) and DOPRI5
+// (backends/rk_core.py, numpy_ref/marches/runge_kutta.py) -- which decide on the host
+// from the norms the device reduces, one device synchronisation per attempt, as the
+// reference's native march does (native/src/march/adams_march.cpp, rk_march.cpp).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/solprop_b200.h"
+#include "kernels.cuh"
+
+using namespace sp;
+
+namespace {
+
+thread_local std::string g_error;
+
+struct Failure : std::runtime_error {
+  sp_status code;
+  Failure(sp_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CUDA_CHECK(call)                                                                    \
+  do {                                                                                      \
+    cudaError_t _e = (call);                                                                \
+    if (_e != cudaSuccess)                                                                  \
+      throw Failure(SP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));       \
+  } while (0)
+
+template <class F>
+sp_status guarded(F&& f) {
+  try {
+    f();
+    return SP_OK;
+  } catch (const Failure& e) {
+    g_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return SP_ERR_ARGUMENT;
+  }
+}
+
+// ------------------------------------------------------------------ piecewise tables
+struct Table {
+  int n_int = 0, n_deg = 0, n_val = 0;
+  std::vector<double> bp, c;
+  bool present() const { return n_int > 0; }
+  void load(const sp_table& t) {
+    n_int = t.n_intervals;
+    n_deg = t.n_deg;
+    n_val = t.n_values;
+    if (!n_int) return;
+    if (!t.breakpoints || !t.coefficients || n_deg < 1 || n_val < 1)
+      throw Failure(SP_ERR_ARGUMENT, "a table without breakpoints or coefficients");
+    bp.assign(t.breakpoints, t.breakpoints + n_int + 1);
+    c.assign(t.coefficients, t.coefficients + (size_t)n_int * n_deg * n_val);
+  }
+  int interval(double z) const {
+    // searchsorted(edges, z, side="right") - 1, clamped (chebyshev.py:171-180)
+    int lo = 0, hi = n_int + 1;
+    while (lo < hi) {
+      int mid = (lo + hi) / 2;
+      if (bp[mid] <= z) lo = mid + 1; else hi = mid;
+    }
+    return std::min(std::max(lo - 1, 0), n_int - 1);
+  }
+  // chebval by Clenshaw, operation for operation (chebyshev.py:182-198)
+  void eval_interval(int k, double z, double* out) const {
+    const double lo = bp[k], hi = bp[k + 1];
+    const double x = (2.0 * z - lo - hi) / (hi - lo);
+    const double* ck = c.data() + (size_t)k * n_deg * n_val;
+    for (int j = 0; j < n_val; ++j) {
+      if (n_deg == 1) { out[j] = ck[j] + 0.0 * x; continue; }
+      if (n_deg == 2) { out[j] = ck[j] + ck[n_val + j] * x; continue; }
+      const double x2 = 2 * x;
+      double c0 = ck[(n_deg - 2) * n_val + j], c1 = ck[(n_deg - 1) * n_val + j];
+      for (int i = 3; i <= n_deg; ++i) {
+        double tmp = c0;
+        c0 = ck[(n_deg - i) * n_val + j] - c1;
+        c1 = tmp + c1 * x2;
+      }
+      out[j] = c0 + c1 * x;
+    }
+  }
+  void eval(double z, double* out) const { eval_interval(interval(z), z, out); }
+  void eval_before(double z, double* out) const {
+    int k = interval(z);
+    if (k > 0 && z <= bp[k]) --k;
+    eval_interval(k, z, out);
+  }
+  double scalar(double z, double dflt) const {
+    if (!present()) return dflt;
+    double v;
+    eval(z, &v);
+    return v;
+  }
+};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    n = count;
+    if (count) CUDA_CHECK(cudaMalloc(&p, count * sizeof(T)));
+  }
+  void upload(const void* host, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) CUDA_CHECK(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void zero(cudaStream_t s) {
+    if (n) CUDA_CHECK(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+
+}  // namespace
+
+// ====================================================================== problem
+struct sp_problem {
+  sp_problem_desc d{};
+  int n_cols = 0, n = 0, n_fine = 0;
+  std::vector<double> omega, omega_window, t_window, t_window_d, carrier, alpha;
+  std::vector<long long> crop;
+  std::vector<unsigned char> active, norm;
+  std::vector<double> phi_terms, pre_terms, synthesis, projection, rate_coeff, taps;
+  Table phi_weights, phi_rate, pre_weights, density, kerr_density, plasma_density, preion, taper;
+};
+
+static void validate(const sp_problem_desc* d) {
+  auto need = [](bool ok, const char* what) {
+    if (!ok) throw Failure(SP_ERR_ARGUMENT, what);
+  };
+  need(d != nullptr, "problem description is NULL");
+  need(d->n_modes >= 1 && d->n_pol >= 1 && d->n_omega >= 2, "bad state shape");
+  need(d->n_to >= 64 && (d->n_to & (d->n_to - 1)) == 0,
+       "n_to must be a power of two >= 64 (mixed radices are not built)");
+  need(d->n_nodes >= 1 && d->synthesis && d->projection, "synthesis/projection required");
+  need(d->omega && d->crop_index && d->active_mask && d->norm_mask && d->omega_window &&
+           d->t_window && d->t_window_derivative,
+       "grid arrays required");
+  need(d->n_phi_terms >= 1 && d->n_phi_terms <= kMaxTerms && d->phi_terms, "phi terms");
+  need(d->n_prefactor_terms >= 1 && d->n_prefactor_terms <= kMaxTerms && d->prefactor_terms,
+       "prefactor terms");
+  if (d->grid_kind != 0)
+    throw Failure(SP_ERR_REFUSED, "the envelope grid is not built on the device yet");
+  if (d->n_pol * d->n_pol_transform != 1)
+    throw Failure(SP_ERR_REFUSED, "two field components (vector Kerr) are not built yet");
+  if (d->n_modes * d->n_pol > kMaxModes)
+    throw Failure(SP_ERR_REFUSED, "more than 8 modal columns: the tensor-core transform is not built yet");
+  if (d->raman_enabled) throw Failure(SP_ERR_REFUSED, "field-grid Raman is not built yet");
+  if (d->kerr_enabled && d->kerr_analytic)
+    throw Failure(SP_ERR_REFUSED, "the analytic Kerr cubic belongs to the envelope grid");
+  if (d->plasma_enabled) {
+    need(d->rate_intervals >= 1 && d->rate_coefficients, "rate table");
+    need(d->n_taps >= 1 && d->n_taps <= kMaxTaps && d->taps, "running-integral taps");
+  }
+  if (d->absorber_in_stage) need(d->temporal_absorber_fine != nullptr, "absorber rate");
+  for (int j = 0; j < d->n_omega; ++j) {
+    const long long k = d->crop_index[j];
+    need(k >= 0 && k <= d->n_to / 2, "crop_index outside the fine spectrum");
+  }
+}
+
+// ====================================================================== workspace
+struct sp_workspace {
+  const sp_problem* P = nullptr;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int log_m = 0, log_n_to = 0, launches = 0, n_rows = 0;
+  DevBuf<double2> phi_terms, pre_terms, twiddles, lab, out, spectra;
+  DevBuf<double> omega, omega_window, t_window, t_window_d, alpha, synthesis, projection,
+      rate_coeff, taps, modal_t, node_p, node_x, node_z, streams;
+  DevBuf<long long> crop;
+  DevBuf<int> fine_to_coarse, rows;
+  DevBuf<unsigned char> active, norm;
+  DevBuf<StageScalarsDev> stage;   // kStageSlots slots
+  StageScalarsDev* h_stage = nullptr;  // pinned
+  // stepping state
+  DevBuf<double2> state, store, states, rates, moments, flow, exponent, carried, src, adv,
+      stages, back;
+  DevBuf<AdamsDev> adams;
+  AdamsDev* h_adams = nullptr;       // pinned
+  DevBuf<double> partials, norms;
+  double* h_norms = nullptr;         // pinned
+  static constexpr int kStageSlots = 10;
+  ~sp_workspace() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (h_stage) cudaFreeHost(h_stage);
+    if (h_adams) cudaFreeHost(h_adams);
+    if (h_norms) cudaFreeHost(h_norms);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+// host evaluation of one stage's scalars into slot `slot` of the pinned buffer
+static void fill_stage(sp_workspace* ws, int slot, double z0, double z1) {
+  const sp_problem& P = *ws->P;
+  StageScalarsDev& s = ws->h_stage[slot];
+  std::memset(&s, 0, sizeof(s));
+  s.z0 = z0;
+  s.z1 = z1;
+  s.density = P.density.scalar(z1, 1.0);
+  s.taper = P.taper.scalar(z1, 1.0);
+  s.kerr_density = P.kerr_density.present() ? P.kerr_density.scalar(z1, 1.0) : s.density;
+  s.plasma_density = P.plasma_density.scalar(z1, s.density);
+  s.preionisation = P.preion.scalar(z1, 0.0);
+  s.n_phi = P.d.n_phi_terms;
+  s.n_pre = P.d.n_prefactor_terms;
+  if (!P.d.phi_expansion) {
+    s.phi_w[0] = z1 - z0;  // Phi(z) = D z: the distance (translate/stage.py:731-734)
+  } else {
+    double w1[kMaxTerms], w0[kMaxTerms];
+    P.phi_weights.eval(z1, w1);
+    P.phi_weights.eval(z0, w0);
+    for (int p = 0; p < s.n_phi; ++p) s.phi_w[p] = w1[p] - w0[p];
+  }
+  if (P.pre_weights.present()) P.pre_weights.eval(z1, s.pre_w);
+  else s.pre_w[0] = 1.0;
+}
+
+static void upload_stages(sp_workspace* ws, int count) {
+  CUDA_CHECK(cudaMemcpyAsync(ws->stage.p, ws->h_stage, count * sizeof(StageScalarsDev),
+                             cudaMemcpyHostToDevice, ws->stream));
+}
+
+// One source evaluation at lab (device), stage slot, optional inverse propagator.
+static void eval_source(sp_workspace* ws, const double2* lab, int slot, const double2* inv_prop,
+                        double2* out, bool quiet) {
+  const sp_problem& P = *ws->P;
+  const sp_problem_desc& d = P.d;
+  const bool absorber = d.absorber_in_stage && !quiet;
+  InverseArgs ia{lab, ws->fine_to_coarse.p, ws->twiddles.p, ws->modal_t.p,
+                 absorber ? ws->streams.p + (size_t)3 * P.n_cols * d.n_to : nullptr,
+                 ws->alpha.p, d.n_omega, d.n_to, ws->log_m, ws->log_n_to};
+  CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream));
+  ColumnArgs ca{};
+  ca.stage = ws->stage.p + slot;
+  ca.modal_t = ws->modal_t.p;
+  ca.synthesis = ws->synthesis.p;
+  ca.t_window = ws->t_window.p;
+  ca.t_window_derivative = ws->t_window_d.p;
+  ca.node_p = ws->node_p.p;
+  ca.node_x = ws->node_x.p;
+  ca.node_z = ws->node_z.p;
+  ca.n_modes = d.n_modes;
+  ca.n_nodes = d.n_nodes;
+  ca.n_to = d.n_to;
+  ca.kerr = d.kerr_enabled;
+  ca.plasma = d.plasma_enabled;
+  ca.band = d.band;
+  ca.half_width = d.plasma_enabled ? d.n_taps - 1 : 0;
+  ca.rate_intervals = d.rate_intervals;
+  ca.kerr_coefficient = d.kerr_coefficient;
+  ca.charge_mass_ratio = d.charge_mass_ratio;
+  ca.ionisation_potential = d.ionisation_potential;
+  ca.dt = d.dt_fine;
+  ca.log_field_min = d.log_field_min;
+  ca.d_log_field = d.d_log_field;
+  ca.field_min = d.field_min;
+  ca.field_max = d.field_max;
+  ca.rate_max = d.rate_max;
+  ca.rate_coefficients = ws->rate_coeff.p;
+  ca.taps = ws->taps.p;
+  CUDA_CHECK(launch_column(ca, ws->stream));
+  const int n_streams = d.plasma_enabled ? 3 : 1;
+  ProjectArgs pa{ws->stage.p + slot, ws->node_p.p, ws->node_x.p, ws->node_z.p, ws->projection.p,
+                 ws->streams.p, d.n_nodes, d.n_modes, P.n_cols, d.n_to, n_streams};
+  CUDA_CHECK(launch_project(pa, ws->stream));
+  // stream rows: P [0, nc), gJ [nc, 2nc), g'J [2nc, 3nc), absorber [3nc, 4nc). The row
+  // list holds [0, 4nc) for plasma runs and, at offset 4nc, [P rows, absorber rows].
+  const int nc = P.n_cols;
+  const int n_rows = (d.plasma_enabled ? 3 * nc : nc) + (absorber ? nc : 0);
+  ForwardArgs fa{ws->streams.p, d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
+                 ws->crop.p, ws->twiddles.p, ws->spectra.p, d.n_to, d.n_omega, ws->log_m,
+                 ws->log_n_to};
+  CUDA_CHECK(launch_forward(fa, n_rows, ws->stream));
+  OutputArgs oa{ws->stage.p + slot, ws->spectra.p, ws->pre_terms.p, ws->omega.p,
+                ws->omega_window.p, ws->active.p, inv_prop, out, P.n_cols, d.n_omega,
+                d.plasma_enabled, absorber};
+  CUDA_CHECK(launch_output(oa, ws->stream));
+}
+
+static void build_workspace(sp_workspace* ws) {
+  const sp_problem& P = *ws->P;
+  const sp_problem_desc& d = P.d;
+  cudaStream_t s = ws->stream;
+  const size_t n = P.n;
+  ws->log_m = ilog2(d.n_to / 2);
+  ws->log_n_to = ilog2(d.n_to);
+  ws->phi_terms.upload(P.phi_terms.data(), (size_t)d.n_phi_terms * n, s);
+  ws->pre_terms.upload(P.pre_terms.data(), (size_t)d.n_prefactor_terms * n, s);
+  // twiddles exp(-2 pi i m / n_to), m < n_to/2, in long double, rounded once
+  std::vector<double2> tw(d.n_to / 2);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < d.n_to / 2; ++m) {
+    long double ang = two_pi * (long double)m / (long double)d.n_to;
+    tw[m] = make_double2((double)cosl(ang), (double)(-sinl(ang)));
+  }
+  ws->twiddles.upload(tw.data(), tw.size(), s);
+  ws->omega.upload(P.omega.data(), d.n_omega, s);
+  ws->omega_window.upload(P.omega_window.data(), d.n_omega, s);
+  ws->t_window.upload(P.t_window.data(), d.n_to, s);
+  ws->t_window_d.upload(P.t_window_d.data(), d.n_to, s);
+  std::vector<double> alpha(d.n_to, 0.0);
+  if (d.absorber_in_stage) alpha = P.alpha;
+  ws->alpha.upload(alpha.data(), d.n_to, s);
+  ws->synthesis.upload(P.synthesis.data(), P.synthesis.size(), s);
+  ws->projection.upload(P.projection.data(), P.projection.size(), s);
+  std::vector<double> rc = P.rate_coeff.empty() ? std::vector<double>(4, 0.0) : P.rate_coeff;
+  ws->rate_coeff.upload(rc.data(), rc.size(), s);
+  std::vector<double> taps = P.taps.empty() ? std::vector<double>(1, 1.0) : P.taps;
+  ws->taps.upload(taps.data(), taps.size(), s);
+  ws->crop.upload(P.crop.data(), d.n_omega, s);
+  std::vector<int> f2c(d.n_to / 2 + 1, -1);
+  for (int j = 0; j < d.n_omega; ++j) f2c[P.crop[j]] = j;
+  ws->fine_to_coarse.upload(f2c.data(), f2c.size(), s);
+  // stream rows: [0, 3 n_cols) P X Z, then absorber [3 n_cols, 4 n_cols); a second list
+  // at 4 n_cols for the no-plasma case: P rows then absorber rows
+  std::vector<int> rows;
+  for (int r = 0; r < 4 * P.n_cols; ++r) rows.push_back(r);
+  for (int r = 0; r < P.n_cols; ++r) rows.push_back(r);
+  for (int r = 0; r < P.n_cols; ++r) rows.push_back(3 * P.n_cols + r);
+  ws->rows.upload(rows.data(), rows.size(), s);
+  ws->active.upload(P.active.data(), d.n_omega, s);
+  ws->norm.upload(P.norm.data(), d.n_omega, s);
+  ws->lab.alloc(n);
+  ws->out.alloc(n);
+  ws->modal_t.alloc((size_t)P.n_cols * d.n_to);
+  ws->node_p.alloc((size_t)d.n_nodes * d.n_to);
+  ws->node_x.alloc((size_t)d.n_nodes * d.n_to);
+  ws->node_z.alloc((size_t)d.n_nodes * d.n_to);
+  ws->streams.alloc((size_t)4 * P.n_cols * d.n_to);
+  ws->streams.zero(s);
+  ws->spectra.alloc((size_t)4 * n);
+  ws->spectra.zero(s);
+  ws->stage.alloc(sp_workspace::kStageSlots);
+  CUDA_CHECK(cudaMallocHost(&ws->h_stage, sizeof(StageScalarsDev) * sp_workspace::kStageSlots));
+  CUDA_CHECK(cudaMallocHost(&ws->h_adams, sizeof(AdamsDev)));
+  CUDA_CHECK(cudaMallocHost(&ws->h_norms, sizeof(double) * 8));
+  ws->adams.alloc(1);
+  ws->partials.alloc((kMaxOrders + 2) * kNormBlocks);
+  ws->norms.alloc(kMaxOrders + 2);
+  ws->launches = 5;
+  CUDA_CHECK(cudaStreamSynchronize(s));
+}
+
+// ====================================================================== coefficient tables
+// stepper/multistep.py _basis_rows: the Lagrange basis from its own roots, ascending
+static void basis_rows(const std::vector<double>& pts, double upper, bool integrate,
+                       std::vector<double>& rows, std::vector<double>& weights) {
+  const int n = (int)pts.size();
+  rows.assign((size_t)n * n, 0.0);
+  weights.assign(n, 0.0);
+  std::vector<double> coef(n + 1), prod(n + 1);
+  for (int index = 0; index < n; ++index) {
+    const double node = pts[index];
+    int length = 1;
+    coef[0] = 1.0;
+    double den = 1.0;
+    for (int other = 0; other < n; ++other) {
+      if (other == index) continue;
+      const double root = pts[other];
+      prod[0] = 0.0;
+      for (int p = 0; p < length; ++p) prod[p + 1] = coef[p];
+      for (int p = 0; p < length; ++p) prod[p] -= root * coef[p];
+      ++length;
+      for (int p = 0; p < length; ++p) coef[p] = prod[p];
+      den *= node - root;
+    }
+    if (integrate) {
+      double integral = 0.0;
+      for (int p = length - 1; p >= 0; --p) integral = (integral + coef[p] / (p + 1)) * upper;
+      weights[index] = integral / den;
+    } else {
+      for (int p = 0; p < length; ++p) rows[(size_t)index * n + p] = coef[p] / den;
+    }
+  }
+}
+static std::vector<double> lagrange(const std::vector<double>& pts) {
+  std::vector<double> r, w;
+  basis_rows(pts, 1.0, false, r, w);
+  return r;
+}
+static std::vector<double> integrated(const std::vector<double>& pts) {
+  std::vector<double> r, w;
+  basis_rows(pts, 1.0, true, r, w);
+  return w;
+}
+
+// ====================================================================== session
+static constexpr int kLandingUlps = 8;
+static double ulp(double x) {
+  x = std::fabs(x);
+  return std::nextafter(x, std::numeric_limits<double>::infinity()) - x;
+}
+static bool reached(double pos, double target) {
+  return pos >= target - kLandingUlps * ulp(std::max(std::fabs(pos), std::fabs(target)));
+}
+
+struct sp_session {
+  sp_workspace* ws = nullptr;
+  sp_run_desc run{};
+  std::vector<double> planes, kinks, edges, schedule, sched_edges;
+  double z = 0.0, proposal = 0.0;
+  int64_t attempts = 0, rejected = 0, evaluations = 0;
+  int plane_cursor = 0, sched_cursor = 0;
+  bool finished = false, failed = false;
+  // Adams
+  std::vector<std::pair<double, int>> history;  // (z, row), oldest first
+  int rejections = 0, order = 1;
+  bool last_rejected = false;
+  // RK
+  std::vector<double> norms_hist;
+};
+
+static void adams_start(sp_session* S) {
+  sp_workspace* ws = S->ws;
+  const sp_problem& P = *ws->P;
+  fill_stage(ws, 1, S->z, S->z);  // source at (z, z)
+  AdamsDev& ad = *ws->h_adams;
+  std::memset(&ad, 0, sizeof(ad));
+  const bool comp = P.d.phi_expansion;
+  if (comp) P.phi_rate.eval(S->z, ad.rate0_w);
+  upload_stages(ws, 2);
+  CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, &ad, sizeof(AdamsDev), cudaMemcpyHostToDevice, ws->stream));
+  eval_source(ws, ws->state.p, 1, nullptr, ws->src.p, false);
+  StepArgs a{};
+  a.stage = ws->stage.p + 1;
+  a.adams = ws->adams.p;
+  a.phi_terms = ws->phi_terms.p;
+  a.n = P.n;
+  a.n_omega = P.d.n_omega;
+  a.state = ws->state.p;
+  a.store = ws->store.p;
+  a.states = comp ? ws->states.p : nullptr;
+  a.rates = comp ? ws->rates.p : nullptr;
+  a.source = ws->src.p;
+  CUDA_CHECK(launch_adams_start(a, ws->stream));
+  S->evaluations += 1;
+  S->history.assign(1, {S->z, 0});
+  S->order = S->run.variable_order ? 1 : S->run.order;
+}
+
+static double limit_step(double dz, double factor, double dz_min, double dz_max) {
+  double proposed = std::min(dz * factor, dz_max);
+  if (proposed < dz_min) {
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "step control asked for %.3e m, below the floor dz_min = %.3e m",
+                  proposed, dz_min);
+    throw Failure(SP_ERR_CONVERGENCE, buf);
+  }
+  return proposed;
+}
+
+// One Adams attempt; returns accepted.
+static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool fixed) {
+  sp_workspace* ws = S->ws;
+  const sp_problem& P = *ws->P;
+  const sp_run_desc& R = S->run;
+  const bool comp = P.d.phi_expansion;
+  // stencil (adams_core.py:150-206)
+  std::vector<double> nodes;
+  std::vector<int> slots;
+  for (auto it = S->history.rbegin(); it != S->history.rend(); ++it) {
+    nodes.push_back((it->first - S->z) / dz);
+    slots.push_back(it->second);
+  }
+  const int held = (int)nodes.size();
+  const int order = std::min(S->order, held);
+  const bool rising = !S->last_rejected && held > order;
+  std::vector<int> orders{order};
+  if (R.variable_order) {
+    for (int o : {order - 1, order + 1})
+      if (o >= 1 && o <= R.order && o <= held && (o < order || rising)) orders.push_back(o);
+  }
+  int width = 1 + *std::max_element(orders.begin(), orders.end());
+  AdamsDev& ad = *ws->h_adams;
+  std::memset(&ad, 0, sizeof(ad));
+  ad.dz = dz;
+  ad.rtol = R.rtol;
+  ad.atol = R.atol;
+  ad.order = order;
+  ad.width = width;
+  ad.n_orders = (int)orders.size();
+  ad.compensated = comp;
+  for (int j = 0; j < width - 1 && j < held; ++j) {
+    ad.slots[j] = slots[j];
+    ad.nodes[j] = nodes[j];
+  }
+  {
+    std::vector<double> pn(nodes.begin(), nodes.begin() + order);
+    auto c = lagrange(pn);
+    for (int j = 0; j < order; ++j)
+      for (int k = 0; k < order; ++k) ad.pred[j][k] = c[(size_t)j * order + k];
+    std::vector<double> cn{1.0};
+    cn.insert(cn.end(), nodes.begin(), nodes.begin() + order);
+    auto cc = lagrange(cn);
+    for (int j = 0; j <= order; ++j)
+      for (int k = 0; k <= order; ++k) ad.corr[j][k] = cc[(size_t)j * (order + 1) + k];
+  }
+  for (int r = 0; r < (int)orders.size(); ++r) {
+    const int k = orders[r];
+    std::vector<double> st(nodes.begin(), nodes.begin() + k);
+    std::vector<double> th{1.0};
+    th.insert(th.end(), st.begin(), st.end());
+    auto a1 = lagrange(th), a2 = lagrange(st);
+    for (int j = 0; j <= k; ++j)
+      for (int q = 0; q <= k; ++q) ad.rows[r][j][q] = a1[(size_t)j * (k + 1) + q];
+    for (int j = 0; j < k; ++j)
+      for (int q = 0; q < k; ++q) ad.rows[r][j + 1][q] -= a2[(size_t)j * k + q];
+    if (comp) {
+      auto wp = integrated(st), wc = integrated(th);
+      for (int j = 0; j < k; ++j) ad.comp_pred[r][j] = wp[j];
+      for (int j = 0; j <= k; ++j) ad.comp_corr[r][j] = wc[j];
+    }
+  }
+  if (comp) {
+    std::vector<double> st(nodes.begin(), nodes.begin() + order);
+    std::vector<double> th{1.0};
+    th.insert(th.end(), st.begin(), st.end());
+    auto wp = integrated(st), wc = integrated(th);
+    for (int j = 0; j < order; ++j) ad.comp_pred_main[j] = wp[j];
+    for (int j = 0; j <= order; ++j) ad.comp_corr_main[j] = wc[j];
+    P.phi_rate.eval_before(S->z + dz, ad.rate_w);
+  }
+  fill_stage(ws, 0, S->z, S->z + dz);        // the step's exponent
+  fill_stage(ws, 1, S->z + dz, S->z + dz);   // the source at the predicted field
+  upload_stages(ws, 2);
+  CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, &ad, sizeof(AdamsDev), cudaMemcpyHostToDevice, ws->stream));
+  StepArgs a{};
+  a.stage = ws->stage.p;
+  a.adams = ws->adams.p;
+  a.phi_terms = ws->phi_terms.p;
+  a.norm_mask = ws->norm.p;
+  a.active_mask = ws->active.p;
+  a.n = P.n;
+  a.n_omega = P.d.n_omega;
+  a.state = ws->state.p;
+  a.store = ws->store.p;
+  a.states = comp ? ws->states.p : nullptr;
+  a.rates = comp ? ws->rates.p : nullptr;
+  a.moments = ws->moments.p;
+  a.flow = ws->flow.p;
+  a.exponent = ws->exponent.p;
+  a.carried = ws->carried.p;
+  a.lab = ws->lab.p;
+  a.source = ws->src.p;
+  a.advanced = ws->adv.p;
+  a.partials = ws->partials.p;
+  a.norms = ws->norms.p;
+  CUDA_CHECK(launch_adams_predict(a, ws->stream));
+  eval_source(ws, ws->lab.p, 1, nullptr, ws->src.p, false);
+  CUDA_CHECK(launch_adams_correct(a, ws->stream));
+  CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, sizeof(double) * (kMaxOrders + 1),
+                             cudaMemcpyDeviceToHost, ws->stream));
+  CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+  S->attempts += 1;
+  S->evaluations += 1;
+  const double magnitude = std::sqrt(ws->h_norms[kMaxOrders]);
+  const double scale = R.rtol * magnitude + R.atol;
+  std::vector<double> norms(orders.size());
+  for (size_t r = 0; r < orders.size(); ++r) norms[r] = std::sqrt(ws->h_norms[r]) / scale;
+  const double norm = norms[0];
+  auto factor = [&](double nm, int o, double growth) {
+    if (nm <= 0.0) return growth;
+    double raw = R.safety * std::pow(nm, -1.0 / (o + 1));
+    return std::min(growth, std::max(R.min_factor, raw));
+  };
+  if (!(norm <= 1.0) && !(fixed && std::isfinite(norm))) {
+    S->rejected += 1;
+    S->last_rejected = true;
+    int count = S->rejections + 1;
+    bool restart = count >= R.restart_after && S->history.size() > 1;
+    double sc = !std::isfinite(norm) ? R.min_factor : factor(norm, order, R.rejection_growth);
+    S->rejections = restart ? 0 : count;
+    if (restart) S->history.clear();
+    S->proposal = limit_step(dz, sc, R.dz_min, R.dz_max);
+    return false;
+  }
+  // accept: the new sample takes the oldest row past the method's need
+  std::vector<std::pair<double, int>> keep;
+  if (R.order) {
+    size_t from = S->history.size() > (size_t)R.order ? S->history.size() - R.order : 0;
+    keep.assign(S->history.begin() + from, S->history.end());
+  }
+  int free_slot = 0;
+  for (;; ++free_slot) {
+    bool used = false;
+    for (auto& e : keep) used |= e.second == free_slot;
+    if (!used) break;
+  }
+  CUDA_CHECK(launch_adams_accept(a, free_slot, nullptr, ws->stream));
+  keep.push_back({S->z + dz, free_slot});
+  S->history = keep;
+  S->rejections = 0;
+  // order choice (adams_core.py:256-301)
+  int stored = order, control = order;
+  double cnorm = norm;
+  if (!R.variable_order) {
+    stored = R.order;
+  } else {
+    auto weight = [&](double nm, int o) {
+      double rate = nm <= 0.0 ? INFINITY : std::pow(nm, -1.0 / (o + 1));
+      double allowed = R.safety * rate;
+      double stable = INFINITY;
+      if (R.collar_rate > 0.0)
+        stable = R.collar_stability * R.real_intervals[o - 1] / (R.collar_rate * dz);
+      return std::min(allowed, stable);
+    };
+    int best = orders[0];
+    double bw = weight(norms[0], orders[0]);
+    for (size_t r = 1; r < orders.size(); ++r) {
+      double w = weight(norms[r], orders[r]);
+      if (w > bw) { bw = w; best = orders[r]; }
+    }
+    if (best != order && bw > R.hysteresis * weight(norms[0], order)) {
+      stored = control = best;
+      for (size_t r = 0; r < orders.size(); ++r) if (orders[r] == best) cnorm = norms[r];
+    }
+  }
+  S->order = stored;
+  S->last_rejected = false;
+  S->z = end;
+  if (kink) S->history.clear();
+  S->proposal = limit_step(dz, factor(cnorm, control, R.max_growth), R.dz_min, R.dz_max);
+  return true;
+}
+
+// stepper/schedule.py:959-1066
+struct Stop { double dz; int kind; double target; bool landed; };
+static Stop landing(const sp_session* S, double z, double dz, double z_end) {
+  const sp_run_desc& R = S->run;
+  const double tol = kLandingUlps * ulp(std::max(std::fabs(z), std::fabs(z_end)));
+  const auto& e = S->edges;
+  int index = (int)(std::upper_bound(e.begin(), e.end(), z) - e.begin()) - 1;
+  index = std::min(std::max(index, 0), (int)e.size() - 2);
+  const double width = e[index + 1] - e[index];
+  // kinds: 0 none, 1 max_step, 2 interval_width, 3 hard_kink, 4 save_plane, 5 end
+  struct B { double dz; int kind; double pos; };
+  B caps[3] = {{dz, 0, 0}, {R.dz_max, 1, 0}, {width, 2, 0}};
+  B cap = caps[0];
+  for (auto& c : caps) if (c.dz < cap.dz || (c.dz == cap.dz && c.kind > cap.kind)) cap = c;
+  std::vector<B> lands;
+  auto add = [&](const std::vector<double>& pos, int kind) {
+    auto it = std::lower_bound(pos.begin(), pos.end(), z + tol);
+    if (it != pos.end()) lands.push_back({*it - z, kind, *it});
+  };
+  add(S->kinks, 3);
+  add(S->planes, 4);
+  add(std::vector<double>{z_end}, 5);
+  if (lands.empty())
+    throw Failure(SP_ERR_STATE, "the march is already at or past its target (no landing ahead)");
+  B best = lands[0];
+  for (auto& l : lands) if (l.dz < best.dz || (l.dz == best.dz && l.kind > best.kind)) best = l;
+  if (best.dz <= cap.dz) return {best.dz, best.kind, best.pos, true};
+  if (best.dz <= std::min(R.stretch * cap.dz, R.dz_max)) return {best.dz, best.kind, best.pos, true};
+  return {cap.dz, cap.kind, 0.0, false};
+}
+
+static void adams_adaptive_attempt(sp_session* S, double target) {
+  const sp_run_desc& R = S->run;
+  if (S->history.empty()) adams_start(S);
+  Stop stop = landing(S, S->z, S->proposal, target);
+  double dz = stop.dz, end;
+  bool kink = false;
+  if (!stop.landed && R.equal_approach) {
+    const double tol = kLandingUlps * ulp(std::max(std::fabs(S->z), std::fabs(target)));
+    double nearest = target;
+    for (const auto* pos : {&S->planes, &S->kinks}) {
+      auto it = std::upper_bound(pos->begin(), pos->end(), S->z + tol);
+      if (it != pos->end()) nearest = std::min(nearest, *it);
+    }
+    if (nearest > S->z + tol && dz < nearest - S->z && nearest - S->z < 2.0 * dz) {
+      double half = 0.5 * (nearest - S->z);
+      adams_attempt(S, half, S->z + half, false, false);
+      return;
+    }
+  }
+  end = stop.landed ? stop.target : S->z + dz;
+  const double tol = kLandingUlps * ulp(std::max(std::fabs(end), 1.0));
+  const bool interior = end < R.z_end - tol;
+  bool on_kink = false;
+  if (interior) for (double k : S->kinks) on_kink |= std::fabs(k - end) <= tol;
+  kink = stop.kind == 3 || on_kink;
+  adams_attempt(S, dz, end, kink, false);
+}
+
+// ---- DOPRI5 (backends/numpy_ref/engines.py:97-181)
+static const double kNodes[7] = {0.0, 1.0 / 5, 3.0 / 10, 4.0 / 5, 8.0 / 9, 1.0, 1.0};
+static const double kA[7][7] = {
+    {0, 0, 0, 0, 0, 0, 0},
+    {1.0 / 5, 0, 0, 0, 0, 0, 0},
+    {3.0 / 40, 9.0 / 40, 0, 0, 0, 0, 0},
+    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0, 0, 0},
+    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0, 0, 0},
+    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656, 0, 0},
+    {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84, 0}};
+static const double kB[7] = {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84, 0};
+static const double kBhat[7] = {5179.0 / 57600, 0, 7571.0 / 16695, 393.0 / 640, -92097.0 / 339200,
+                                187.0 / 2100, 1.0 / 40};
+
+static double rk_trial(sp_session* S, double dz) {
+  sp_workspace* ws = S->ws;
+  const sp_problem& P = *ws->P;
+  const sp_run_desc& R = S->run;
+  for (int i = 0; i < 7; ++i) fill_stage(ws, i, S->z, S->z + kNodes[i] * dz);
+  fill_stage(ws, 7, S->z, S->z + dz);
+  upload_stages(ws, 8);
+  RkArgs a{};
+  a.phi_terms = ws->phi_terms.p;
+  a.norm_mask = ws->norm.p;
+  a.active_mask = ws->active.p;
+  a.n = P.n;
+  a.n_omega = P.d.n_omega;
+  a.n_phi = P.d.n_phi_terms;
+  a.state = ws->state.p;
+  a.stages = ws->stages.p;
+  a.lab = ws->lab.p;
+  a.back = ws->back.p;
+  a.advanced = ws->adv.p;
+  a.partials = ws->partials.p;
+  a.norms = ws->norms.p;
+  double e[7];
+  for (int i = 0; i < 7; ++i) e[i] = kB[i] - kBhat[i];
+  for (int i = 0; i < 7; ++i) {
+    a.stage = ws->stage.p + i;
+    CUDA_CHECK(launch_rk_stage_input(a, i, kA[i], dz, ws->stream));
+    eval_source(ws, ws->lab.p, i, ws->back.p, ws->stages.p + (size_t)i * P.n, false);
+  }
+  a.stage = ws->stage.p + 7;
+  CUDA_CHECK(launch_rk_finish(a, kB, e, dz, R.rtol, R.atol, ws->stream));
+  CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                             ws->stream));
+  CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+  S->attempts += 1;
+  S->evaluations += 7;
+  const double scale = R.rtol * std::max(std::sqrt(ws->h_norms[0]), std::sqrt(ws->h_norms[1])) + R.atol;
+  return std::sqrt(ws->h_norms[2]) / scale;
+}
+
+static void rk_accept(sp_session* S) {
+  sp_workspace* ws = S->ws;
+  CUDA_CHECK(launch_mask_copy(ws->state.p, ws->adv.p, ws->active.p, ws->P->n, ws->P->d.n_omega,
+                              ws->stream));
+}
+
+static double rk_propose_factor(const sp_session* S) {
+  const sp_run_desc& R = S->run;
+  const int index = (int)S->norms_hist.size() - 1 - R.lag;
+  if (index < 0) return 1.0;
+  double current = S->norms_hist[index];
+  if (!std::isfinite(current)) return R.min_factor;
+  if (current <= 0.0) return R.max_factor;
+  double previous = index >= 1 ? S->norms_hist[index - 1] : 1.0;
+  if (!std::isfinite(previous) || previous <= 0.0) previous = 1.0;
+  double f = R.safety * std::pow(1.0 / current, R.beta1) * std::pow(1.0 / previous, R.beta2);
+  return std::min(std::max(f, R.min_factor), R.max_factor);
+}
+
+static void rk_adaptive_attempt(sp_session* S, double target) {
+  const sp_run_desc& R = S->run;
+  Stop stop = landing(S, S->z, S->proposal, target);
+  const double dz = stop.dz;
+  const double norm = rk_trial(S, dz);
+  const int q1 = R.estimator_order + 1;
+  const double equivalent = std::isfinite(norm) ? norm * std::pow(S->proposal / dz, q1) : norm;
+  const bool accepted = std::isfinite(norm) && norm <= 1.0;
+  const double end = stop.landed ? stop.target : S->z + dz;
+  if (accepted) {
+    rk_accept(S);
+    S->z = end;
+    S->norms_hist.push_back(equivalent);
+    S->proposal = limit_step(S->proposal, rk_propose_factor(S), R.dz_min, R.dz_max);
+  } else {
+    S->rejected += 1;
+    double f;
+    if (!std::isfinite(equivalent)) f = R.min_factor;
+    else if (equivalent <= 0.0) f = 1.0;
+    else f = std::min(std::max(R.safety * std::pow(1.0 / equivalent, 1.0 / q1), R.min_factor), 1.0);
+    S->proposal = limit_step(S->proposal, f, R.dz_min, R.dz_max);
+  }
+}
+
+static void alloc_step_buffers(sp_workspace* ws, int method) {
+  const sp_problem& P = *ws->P;
+  const size_t n = P.n;
+  if (!ws->state.p) ws->state.alloc(n);
+  if (!ws->src.p) ws->src.alloc(n);
+  if (!ws->adv.p) ws->adv.alloc(n);
+  if (method == 0) {
+    if (!ws->store.p) ws->store.alloc((size_t)kMaxSlots * n);
+    if (!ws->moments.p) ws->moments.alloc((size_t)kMaxWidth * n);
+    if (!ws->flow.p) ws->flow.alloc(n);
+    if (!ws->exponent.p) ws->exponent.alloc(n);
+    if (P.d.phi_expansion) {
+      if (!ws->states.p) ws->states.alloc((size_t)kMaxSlots * n);
+      if (!ws->rates.p) ws->rates.alloc((size_t)kMaxSlots * n);
+      if (!ws->carried.p) ws->carried.alloc((size_t)kMaxWidth * n);
+    }
+    ws->store.zero(ws->stream);
+    if (ws->states.p) ws->states.zero(ws->stream);
+    if (ws->rates.p) ws->rates.zero(ws->stream);
+  } else {
+    if (!ws->stages.p) ws->stages.alloc((size_t)7 * n);
+    if (!ws->back.p) ws->back.alloc(n);
+  }
+}
+
+// ====================================================================== C ABI
+extern "C" {
+
+size_t sp_last_error(char* buf, size_t len) {
+  if (buf && len) {
+    std::strncpy(buf, g_error.c_str(), len - 1);
+    buf[len - 1] = '\0';
+  }
+  return g_error.size();
+}
+
+const char* sp_version(void) { return "solprop-b200 0.1 sm_100a fp64"; }
+
+int sp_device_count(void) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    g_error = std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e);
+    return -SP_ERR_CUDA;
+  }
+  return n;
+}
+
+sp_status sp_problem_create(const sp_problem_desc* d, sp_problem** out) {
+  return guarded([&] {
+    if (!out) throw Failure(SP_ERR_ARGUMENT, "out is NULL");
+    validate(d);
+    auto P = std::make_unique<sp_problem>();
+    P->d = *d;
+    P->n_cols = d->n_modes * d->n_pol;
+    P->n = P->n_cols * d->n_omega;
+    P->omega.assign(d->omega, d->omega + d->n_omega);
+    P->omega_window.assign(d->omega_window, d->omega_window + d->n_omega);
+    P->t_window.assign(d->t_window, d->t_window + d->n_to);
+    P->t_window_d.assign(d->t_window_derivative, d->t_window_derivative + d->n_to);
+    if (d->absorber_in_stage) P->alpha.assign(d->temporal_absorber_fine, d->temporal_absorber_fine + d->n_to);
+    P->crop.assign(d->crop_index, d->crop_index + d->n_omega);
+    P->active.assign(d->active_mask, d->active_mask + d->n_omega);
+    P->norm.assign(d->norm_mask, d->norm_mask + d->n_omega);
+    P->phi_terms.assign(d->phi_terms, d->phi_terms + (size_t)2 * d->n_phi_terms * P->n);
+    P->pre_terms.assign(d->prefactor_terms, d->prefactor_terms + (size_t)2 * d->n_prefactor_terms * P->n);
+    const size_t n_rows = (size_t)d->n_nodes * d->n_pol_transform;
+    P->synthesis.assign(d->synthesis, d->synthesis + n_rows * d->n_modes);
+    P->projection.assign(d->projection, d->projection + n_rows * d->n_modes);
+    if (d->plasma_enabled) {
+      P->rate_coeff.assign(d->rate_coefficients, d->rate_coefficients + (size_t)4 * d->rate_intervals);
+      P->taps.assign(d->taps, d->taps + d->n_taps);
+    }
+    P->phi_weights.load(d->phi_weights);
+    P->phi_rate.load(d->phi_rate);
+    P->pre_weights.load(d->prefactor_weights);
+    P->density.load(d->density);
+    P->kerr_density.load(d->kerr_density);
+    P->plasma_density.load(d->plasma_density);
+    P->preion.load(d->preionisation);
+    P->taper.load(d->taper_scale);
+    if (d->phi_expansion && (!P->phi_weights.present() || !P->phi_rate.present()))
+      throw Failure(SP_ERR_ARGUMENT, "an expansion of Phi needs its weight and rate tables");
+    *out = P.release();
+  });
+}
+
+sp_status sp_problem_destroy(sp_problem* p) {
+  delete p;
+  return SP_OK;
+}
+
+sp_status sp_workspace_create(const sp_problem* problem, int device, sp_workspace** out) {
+  return guarded([&] {
+    if (!problem || !out) throw Failure(SP_ERR_ARGUMENT, "NULL problem or out");
+    CUDA_CHECK(cudaSetDevice(device));
+    static bool configured = false;
+    if (!configured) {
+      CUDA_CHECK(configure_source_kernels());
+      configured = true;
+    }
+    auto ws = std::make_unique<sp_workspace>();
+    ws->P = problem;
+    ws->device = device;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
+    build_workspace(ws.get());
+    *out = ws.release();
+  });
+}
+
+sp_status sp_workspace_destroy(sp_workspace* ws) {
+  delete ws;
+  return SP_OK;
+}
+
+int sp_workspace_launches_per_source(const sp_workspace* ws) { return ws ? ws->launches : 0; }
+
+sp_status sp_workspace_source_device(sp_workspace* ws, const void* lab, double z, int quiet,
+                                     void* out) {
+  return guarded([&] {
+    if (!ws || !lab || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    CUDA_CHECK(cudaSetDevice(ws->device));
+    fill_stage(ws, 0, z, z);
+    upload_stages(ws, 1);
+    eval_source(ws, (const double2*)lab, 0, nullptr, (double2*)out, quiet != 0);
+  });
+}
+
+sp_status sp_workspace_source(sp_workspace* ws, const double* lab, double z, int quiet, double* out) {
+  return guarded([&] {
+    if (!ws || !lab || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    CUDA_CHECK(cudaSetDevice(ws->device));
+    const size_t bytes = (size_t)ws->P->n * sizeof(double2);
+    CUDA_CHECK(cudaMemcpyAsync(ws->lab.p, lab, bytes, cudaMemcpyHostToDevice, ws->stream));
+    fill_stage(ws, 0, z, z);
+    upload_stages(ws, 1);
+    eval_source(ws, ws->lab.p, 0, nullptr, ws->out.p, quiet != 0);
+    CUDA_CHECK(cudaMemcpyAsync(out, ws->out.p, bytes, cudaMemcpyDeviceToHost, ws->stream));
+    CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+sp_status sp_session_start(sp_workspace* ws, const sp_run_desc* run, sp_session** out) {
+  return guarded([&] {
+    if (!ws || !run || !out || !run->field0) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    if (run->method != 0 && run->method != 1) throw Failure(SP_ERR_ARGUMENT, "unknown method");
+    if (run->method == 0 && (run->order < 1 || run->order > 5))
+      throw Failure(SP_ERR_ARGUMENT, "Adams order must lie in [1, 5]");
+    CUDA_CHECK(cudaSetDevice(ws->device));
+    auto S = std::make_unique<sp_session>();
+    S->ws = ws;
+    S->run = *run;
+    S->planes.assign(run->save_planes, run->save_planes + run->n_save_planes);
+    S->kinks.assign(run->hard_kinks, run->hard_kinks + run->n_hard_kinks);
+    S->edges.assign(run->breakpoints, run->breakpoints + run->n_breakpoints);
+    if (S->edges.size() < 2) S->edges = {run->z_start, run->z_end};
+    if (run->schedule && run->n_schedule > 0) {
+      S->schedule.assign(run->schedule, run->schedule + run->n_schedule);
+      S->sched_edges.assign(1, run->z_start);
+      for (double dz : S->schedule) S->sched_edges.push_back(S->sched_edges.back() + dz);
+    }
+    S->z = run->z_start;
+    S->proposal = run->proposal;
+    S->order = run->variable_order ? 1 : run->order;
+    alloc_step_buffers(ws, run->method);
+    const size_t bytes = (size_t)ws->P->n * sizeof(double2);
+    CUDA_CHECK(cudaMemcpyAsync(ws->adv.p, run->field0, bytes, cudaMemcpyHostToDevice, ws->stream));
+    CUDA_CHECK(launch_mask_copy(ws->state.p, ws->adv.p, ws->active.p, ws->P->n, ws->P->d.n_omega,
+                                ws->stream));
+    CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+    *out = S.release();
+  });
+}
+
+sp_status sp_session_advance(sp_session* S, int32_t work_limit, sp_batch* out) {
+  return guarded([&] {
+    if (!S || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    if (S->failed) throw Failure(SP_ERR_STATE, "the session failed; close it");
+    CUDA_CHECK(cudaSetDevice(S->ws->device));
+    out->event = 0;
+    out->plane_index = -1;
+    const sp_run_desc& R = S->run;
+    int done = 0;
+    try {
+      if (!S->finished && reached(S->z, R.z_end)) {
+        S->finished = true;
+        out->event = 2;
+      }
+      while (!S->finished && done < work_limit) {
+        // the next stop: a save plane or the end
+        double target = R.z_end;
+        int plane = -1;
+        while (S->plane_cursor < (int)S->planes.size() &&
+               reached(S->z, S->planes[S->plane_cursor]))
+          ++S->plane_cursor;
+        if (S->plane_cursor < (int)S->planes.size()) {
+          target = S->planes[S->plane_cursor];
+          plane = S->plane_cursor;
+        }
+        if (!S->schedule.empty()) {
+          if (S->sched_cursor >= (int)S->schedule.size()) { S->finished = true; out->event = 2; break; }
+          const double dz = S->schedule[S->sched_cursor];
+          const double end = S->sched_edges[S->sched_cursor + 1];
+          if (R.method == 0) {
+            if (S->history.empty()) adams_start(S);
+            adams_attempt(S, dz, end, false, true);
+          } else {
+            double nm = rk_trial(S, dz);
+            if (!std::isfinite(nm)) throw Failure(SP_ERR_CONVERGENCE, "a replayed step diverged");
+            rk_accept(S);
+            S->z = end;
+          }
+          ++S->sched_cursor;
+        } else if (R.method == 0) {
+          adams_adaptive_attempt(S, target);
+        } else {
+          rk_adaptive_attempt(S, target);
+        }
+        ++done;
+        const bool on_plane =
+            plane >= 0 && std::fabs(S->z - S->planes[plane]) <=
+                              std::max(1e-9 * std::fabs(R.z_end), kLandingUlps * ulp(S->planes[plane]));
+        if (on_plane) {
+          ++S->plane_cursor;
+          out->plane_index = plane;
+        }
+        if (reached(S->z, R.z_end)) {
+          S->finished = true;
+          out->event = 2;
+          break;
+        }
+        if (on_plane) {
+          out->event = 1;
+          break;
+        }
+      }
+    } catch (const Failure&) {
+      S->failed = true;
+      out->event = 3;
+      throw;
+    }
+    out->z = S->z;
+    out->attempts = S->attempts;
+    out->rejected = S->rejected;
+    out->evaluations = S->evaluations;
+  });
+}
+
+sp_status sp_session_export(sp_session* S, double* out) {
+  return guarded([&] {
+    if (!S || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    CUDA_CHECK(cudaSetDevice(S->ws->device));
+    const size_t bytes = (size_t)S->ws->P->n * sizeof(double2);
+    CUDA_CHECK(cudaMemcpyAsync(out, S->ws->state.p, bytes, cudaMemcpyDeviceToHost, S->ws->stream));
+    CUDA_CHECK(cudaStreamSynchronize(S->ws->stream));
+  });
+}
+
+sp_status sp_session_destroy(sp_session* S) {
+  delete S;
+  return SP_OK;
+}
+
+}  // extern "C"

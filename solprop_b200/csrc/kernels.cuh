@@ -1,0 +1,157 @@
+// Argument records and launchers of the device kernels.  Every per-stage scalar a
+// kernel reads lives in device memory (StageScalarsDev, AttemptDev), written by one
+// host-to-device copy before the launches, so that a captured CUDA graph replays with
+// the values of the current attempt.
+#pragma once
+#include "sp_common.cuh"
+
+namespace sp {
+
+constexpr int kMaxTerms = 64;      // stage terms of Phi or of the prefactor
+constexpr int kMaxWidth = 8;       // Adams interpolation nodes (order 5 + 1, padded)
+constexpr int kMaxOrders = 3;      // scored orders per trial
+constexpr int kMaxSlots = 8;       // history rows (order + 2)
+constexpr int kNormBlocks = 148;   // partial-sum blocks of the norm reductions
+
+struct StageScalarsDev {
+  double z0, z1, taper, density, kerr_density, plasma_density, preionisation, raman_density;
+  int n_pre, n_phi;
+  double pre_w[kMaxTerms];
+  double phi_w[kMaxTerms];   // weights of Phi(z1) - Phi(z0)
+  double raman_rates[4];
+};
+
+// One Adams trial's tables (backends/numpy_ref/adams_tables.py, multistep.py _trial).
+struct AdamsDev {
+  double dz, rtol, atol;
+  int order, width, n_orders, compensated;
+  int slots[kMaxWidth];                 // history rows read, newest first
+  double nodes[kMaxWidth];              // theta_j, newest first
+  double pred[kMaxWidth][kMaxWidth];    // Lagrange coefficients c_jk of the predictor
+  double corr[kMaxWidth][kMaxWidth];    // corrector over (source, newest, ...)
+  double rows[kMaxOrders][kMaxWidth][kMaxWidth];  // defect rows
+  // compensation (integrated Adams weights) for the predictor, corrector, per order
+  double comp_pred[kMaxOrders][kMaxWidth];        // weights over carried rows
+  double comp_corr[kMaxOrders][kMaxWidth + 1];    // [0] endpoint, then carried rows
+  double comp_pred_main[kMaxWidth];
+  double comp_corr_main[kMaxWidth + 1];
+  double rate_w[kMaxTerms];   // D(z + dz) weights (the endpoint rate, "before")
+  double rate0_w[kMaxTerms];  // D(z) weights (startup)
+};
+
+struct InverseArgs {
+  const double2* lab;            // (n_cols, n_omega)
+  const int* fine_to_coarse;     // (n_to/2 + 1)
+  const double2* twiddles;       // exp(-2 pi i m / n_to), m < n_to / 2
+  double* modal_t;               // (n_cols, n_to)
+  double* absorber_stream;       // (n_cols, n_to) or null
+  const double* alpha;           // (n_to)
+  int n_omega, n_to, log_m, log_n_to;
+};
+
+struct ColumnArgs {
+  const StageScalarsDev* stage;
+  const double* modal_t;   // (n_modes, n_to)
+  const double* synthesis; // (n_nodes, n_modes)
+  const double* t_window;
+  const double* t_window_derivative;
+  double* node_p;          // (n_nodes, n_to)
+  double* node_x;
+  double* node_z;
+  int n_modes, n_nodes, n_to;
+  int kerr, plasma, band, half_width, rate_intervals;
+  double kerr_coefficient, charge_mass_ratio, ionisation_potential, dt;
+  double log_field_min, d_log_field, field_min, field_max, rate_max;
+  const double* rate_coefficients;
+  const double* taps;
+};
+
+struct ProjectArgs {
+  const StageScalarsDev* stage;
+  const double* node_p;
+  const double* node_x;
+  const double* node_z;
+  const double* projection;  // (n_modes, n_nodes)
+  double* streams;           // (n_stream_rows, n_cols, n_to)
+  int n_nodes, n_modes, n_cols, n_to, n_streams;
+};
+
+struct ForwardArgs {
+  const double* streams;       // rows of n_to
+  const int* rows;             // which rows to transform
+  const long long* crop_index; // (n_omega)
+  const double2* twiddles;
+  double2* spectra;            // rows of n_omega
+  int n_to, n_omega, log_m, log_n_to;
+};
+
+struct OutputArgs {
+  const StageScalarsDev* stage;
+  const double2* spectra;          // (4, n_cols, n_omega): P, gJ, g'J, absorber
+  const double2* prefactor_terms;  // (n_pre, n_cols, n_omega)
+  const double* omega;
+  const double* omega_window;
+  const unsigned char* active_mask;
+  const double2* inverse_propagator;  // (n_cols, n_omega) or null
+  double2* out;
+  int n_cols, n_omega, plasma, absorber;
+};
+
+cudaError_t configure_source_kernels();
+cudaError_t launch_inverse(const InverseArgs& a, int n_cols, cudaStream_t stream);
+cudaError_t launch_column(const ColumnArgs& a, cudaStream_t stream);
+cudaError_t launch_project(const ProjectArgs& a, cudaStream_t stream);
+cudaError_t launch_forward(const ForwardArgs& a, int n_rows, cudaStream_t stream);
+cudaError_t launch_output(const OutputArgs& a, cudaStream_t stream);
+
+// ---- stepping kernels (step_kernels.cu)
+struct StepArgs {
+  const StageScalarsDev* stage;
+  const AdamsDev* adams;
+  const double2* phi_terms;   // (n_phi, n)
+  const unsigned char* norm_mask;
+  const unsigned char* active_mask;
+  int n, n_omega;             // state elements, bins per column
+  double2* state;             // (n)
+  double2* store;             // (n_slots, n)
+  double2* states;            // compensated: (n_slots, n)
+  double2* rates;             // compensated: (n_slots, n)
+  double2* moments;           // (width, n)
+  double2* flow;              // (n)
+  double2* exponent;          // (n)
+  double2* carried;           // compensated: (width - 1, n)
+  double2* lab;               // (n)
+  double2* source;            // (n)
+  double2* advanced;          // (n)
+  double* partials;           // (kMaxOrders + 2, kNormBlocks)
+  double* norms;              // (kMaxOrders + 2)
+};
+
+cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t stream);
+cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t stream);
+cudaError_t launch_adams_accept(const StepArgs& a, int free_slot, double2* rate_out, cudaStream_t s);
+cudaError_t launch_adams_start(const StepArgs& a, cudaStream_t stream);
+
+struct RkArgs {
+  const StageScalarsDev* stage;
+  const double2* phi_terms;
+  const unsigned char* norm_mask;
+  const unsigned char* active_mask;
+  int n, n_omega, n_phi;
+  double2* state;
+  double2* stages;        // (7, n)
+  double2* lab;
+  double2* back;          // inverse propagator of the stage
+  double2* advanced;
+  double* partials;
+  double* norms;
+};
+// stage_input: lab = exp(x)(y + dz sum_j a_ij k_j), back = exp(-x); coefficients by value
+cudaError_t launch_rk_stage_input(const RkArgs& a, int stage, const double* coeffs, double dz,
+                                  cudaStream_t stream);
+cudaError_t launch_rk_finish(const RkArgs& a, const double* b, const double* e, double dz,
+                             double rtol, double atol, cudaStream_t stream);
+cudaError_t launch_mask_copy(double2* dst, const double2* src, const unsigned char* active,
+                             int n, int n_omega, cudaStream_t stream);
+
+}  // namespace sp

@@ -1,0 +1,48 @@
+// Shared definitions of the B200 propagation library: complex FP64 helpers, error
+// plumbing and launch constants.  Complex numbers are double2 (x = re, y = im), the
+// memory layout of NumPy's complex128.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sp {
+
+__host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+__host__ __device__ __forceinline__ double2 cscale(double s, double2 a) {
+  return make_double2(s * a.x, s * a.y);
+}
+__host__ __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+// multiply by -i (forward) or +i (inverse): exact
+__host__ __device__ __forceinline__ double2 mul_mi(double2 a) { return make_double2(a.y, -a.x); }
+__host__ __device__ __forceinline__ double2 mul_pi(double2 a) { return make_double2(-a.y, a.x); }
+// complex division a / b, Smith's algorithm (one scaling, robust to overflow)
+__host__ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+  if (fabs(b.x) >= fabs(b.y)) {
+    double r = b.y / b.x, d = b.x + b.y * r;
+    return make_double2((a.x + a.y * r) / d, (a.y - a.x * r) / d);
+  }
+  double r = b.x / b.y, d = b.x * r + b.y;
+  return make_double2((a.x * r + a.y) / d, (a.y * r - a.x) / d);
+}
+// exp of a complex number
+__device__ __forceinline__ double2 cexp(double2 z) {
+  double e = exp(z.x), s, c;
+  sincos(z.y, &s, &c);
+  return make_double2(e * c, e * s);
+}
+
+// Largest fine-grid length one response-column CTA holds; longer rows use a cluster.
+constexpr int kColumnSpan = 4096;
+constexpr int kColumnThreads = 512;
+constexpr int kMaxModes = 8;   // modal route columns handled by the projection kernel
+constexpr int kMaxTaps = 16;   // band-rule half-width K + 1
+
+}  // namespace sp

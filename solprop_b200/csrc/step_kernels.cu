@@ -1,0 +1,360 @@
+// The stepping kernels: the exponential Adams trial's predict and correct passes with
+// their fused norms and the accept pass (backends/numpy_ref/adams_kernels.py:404-741,
+// multistep.py:901-1070), and the DOPRI5 trial's stage input and finish
+// (backends/numpy_ref/engines.py:97-181, passes/stepping.py:38-283).  Each kernel is a
+// single pass over the state; the norms are two-level deterministic reductions: a fixed
+// grid of kNormBlocks blocks writes one partial per block, one block adds them.
+#include "kernels.cuh"
+
+namespace sp {
+
+__constant__ double c_recip_fact[16] = {
+    1.0, 1.0, 1.0 / 2, 1.0 / 6, 1.0 / 24, 1.0 / 120, 1.0 / 720, 1.0 / 5040, 1.0 / 40320,
+    1.0 / 362880, 1.0 / 3628800, 1.0 / 39916800, 1.0 / 479001600, 1.0 / 6227020800.0,
+    1.0 / 87178291200.0, 1.0 / 1307674368000.0};
+
+// phi_0(x) .. phi_order(x) (backends/exponential.py:131-224): the upward recurrence
+// from exp(x) beyond |x| = 3, the scaled Taylor series of the highest function, the
+// downward recurrence and repeated doubling below.
+__device__ void phi_functions(double2 x, int order, double2* out) {
+  const double mag = hypot(x.x, x.y);
+  if (mag > 3.0) {
+    out[0] = cexp(x);
+    for (int k = 1; k <= order; ++k)
+      out[k] = cdiv(make_double2(out[k - 1].x - c_recip_fact[k - 1], out[k - 1].y), x);
+    return;
+  }
+  int sq = 0;
+  if (mag > 0.5) sq = (int)ceil(log2(fmax(mag, 0.5) / 0.5));
+  const double scale = exp2(-(double)sq);
+  const double2 y = make_double2(x.x * scale, x.y * scale);
+  double2 term = make_double2(c_recip_fact[order], 0.0);
+  double2 total = term;
+  for (int m = 1; m < 24; ++m) {
+    term = cmul(term, y);
+    term = make_double2(term.x / (double)(m + order), term.y / (double)(m + order));
+    total = cadd(total, term);
+  }
+  out[order] = total;
+  for (int k = order - 1; k >= 1; --k) {
+    double2 t = cmul(y, out[k + 1]);
+    out[k] = make_double2(c_recip_fact[k] + t.x, t.y);
+  }
+  out[0] = cexp(y);
+  for (int level = 0; level < sq; ++level) {
+    double2 old[kMaxWidth + 1];
+    for (int k = 0; k <= order; ++k) old[k] = out[k];
+    out[0] = cmul(old[0], old[0]);
+    double p2 = 1.0;
+    for (int k = 1; k <= order; ++k) {
+      p2 *= 2.0;
+      double2 t = cmul(old[0], old[k]);
+      for (int j = 1; j <= k; ++j) t = cadd(t, cscale(c_recip_fact[k - j], old[j]));
+      out[k] = make_double2(t.x / p2, t.y / p2);
+    }
+  }
+}
+
+__device__ __forceinline__ double2 combine_terms(const double* w, int n_terms,
+                                                 const double2* terms, int n, int i) {
+  // translate/stage.py:292-342: one term multiplied (or itself for a unit weight),
+  // several contracted in order
+  if (n_terms == 1) {
+    double2 t = terms[i];
+    return w[0] == 1.0 ? t : cscale(w[0], t);
+  }
+  double2 acc = make_double2(0.0, 0.0);
+  for (int p = 0; p < n_terms; ++p) acc = cadd(acc, cscale(w[p], terms[(size_t)p * n + i]));
+  return acc;
+}
+
+// sum of n_q values per thread into partials[q][blockIdx.x]; deterministic order
+template <int NQ>
+__device__ void block_partials(double (&v)[NQ], double* partials) {
+  __shared__ double red[NQ][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double x = v[q];
+    for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+    if (lane == 0) red[q][warp] = x;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double x = lane < nw ? red[q][lane] : 0.0;
+      for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+      if (lane == 0) partials[q * kNormBlocks + blockIdx.x] = x;
+    }
+  }
+}
+
+__global__ void k_reduce(const double* partials, double* out, int nq) {
+  // one block of 32 threads per quantity; fixed order
+  const int q = blockIdx.x;
+  if (q >= nq) return;
+  double x = 0.0;
+  for (int b = threadIdx.x; b < kNormBlocks; b += 32) x += partials[q * kNormBlocks + b];
+  for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+  if (threadIdx.x == 0) out[q] = x;
+}
+
+// ------------------------------------------------------------------ Adams predict
+__global__ void __launch_bounds__(256) k_adams_predict(StepArgs a) {
+  const AdamsDev& ad = *a.adams;
+  const StageScalarsDev& st = *a.stage;
+  const int width = ad.width, order = ad.order;
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const double2 x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
+    double2 phi[kMaxWidth + 1];
+    phi_functions(x, width, phi);
+    const double2 fl = cexp(x);
+    double fact = 1.0;
+    double2 mom[kMaxWidth];
+    for (int k = 0; k < width; ++k) {
+      if (k > 0) fact *= (double)k;
+      mom[k] = cscale(fact, phi[k + 1]);
+      a.moments[(size_t)k * a.n + i] = mom[k];
+    }
+    a.flow[i] = fl;
+    a.exponent[i] = x;
+    const double2 y = a.state[i];
+    double2 total = make_double2(0.0, 0.0);
+    for (int k = 0; k < order; ++k) {
+      double2 comb = make_double2(0.0, 0.0);
+      for (int j = 0; j < order; ++j) {
+        const double c = ad.pred[j][k];
+        if (c != 0.0) comb = cadd(comb, cscale(c, a.store[(size_t)ad.slots[j] * a.n + i]));
+      }
+      total = cadd(total, cmul(mom[k], comb));
+    }
+    double2 lab = cadd(cmul(fl, y), cscale(ad.dz, total));
+    if (ad.compensated) {
+      // carried rows exp((1 - theta_j) x) ((D(z_j) - x/dz) u_j)   (adams_kernels.py carry)
+      const double2 ref = make_double2(x.x / ad.dz, x.y / ad.dz);
+      double2 comp = make_double2(0.0, 0.0);
+      for (int j = 0; j < width - 1; ++j) {
+        const int s = ad.slots[j];
+        const double span = 1.0 - ad.nodes[j];
+        const double2 diff = csub(a.rates[(size_t)s * a.n + i], ref);
+        const double2 c = cmul(cexp(cscale(span, x)), cmul(diff, a.states[(size_t)s * a.n + i]));
+        a.carried[(size_t)j * a.n + i] = c;
+        if (j < order) comp = cadd(comp, cscale(ad.comp_pred_main[j], c));
+      }
+      lab = cadd(lab, cscale(ad.dz, comp));
+    }
+    a.lab[i] = lab;
+    const int bin = i % a.n_omega;
+    if (a.norm_mask[bin]) v[0] += y.x * y.x + y.y * y.y;
+  }
+  block_partials<1>(v, a.partials + (size_t)kMaxOrders * kNormBlocks);
+}
+
+// ------------------------------------------------------------------ Adams correct
+__global__ void __launch_bounds__(256) k_adams_correct(StepArgs a) {
+  const AdamsDev& ad = *a.adams;
+  const int width = ad.width, n_orders = ad.n_orders;
+  double v[kMaxOrders] = {0.0, 0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    double2 xs[kMaxWidth];
+    xs[0] = a.source[i];
+    for (int j = 1; j < width; ++j) xs[j] = a.store[(size_t)ad.slots[j - 1] * a.n + i];
+    double2 mom[kMaxWidth];
+    for (int k = 0; k < width; ++k) mom[k] = a.moments[(size_t)k * a.n + i];
+    // advanced = flow u + dz sum_k M_k sum_j corr_jk X_j
+    double2 total = make_double2(0.0, 0.0);
+    for (int k = 0; k < width; ++k) {
+      double2 comb = make_double2(0.0, 0.0);
+      for (int j = 0; j < width; ++j) {
+        const double c = ad.corr[j][k];
+        if (c != 0.0) comb = cadd(comb, cscale(c, xs[j]));
+      }
+      total = cadd(total, cmul(mom[k], comb));
+    }
+    double2 adv = cadd(cmul(a.flow[i], a.state[i]), cscale(ad.dz, total));
+    double2 endpoint = make_double2(0.0, 0.0);
+    double2 carried[kMaxWidth];
+    if (ad.compensated) {
+      const double2 x = a.exponent[i];
+      const double2 ref = make_double2(x.x / ad.dz, x.y / ad.dz);
+      // D(z + dz) = sum_p r_p terms_p, contracted always (translate/linop.py:2332-2334)
+      double2 rate_end = make_double2(0.0, 0.0);
+      for (int p = 0; p < a.stage->n_phi; ++p)
+        rate_end = cadd(rate_end, cscale(ad.rate_w[p], a.phi_terms[(size_t)p * a.n + i]));
+      endpoint = cmul(csub(rate_end, ref), a.lab[i]);
+      for (int j = 0; j < width - 1; ++j) carried[j] = a.carried[(size_t)j * a.n + i];
+      double2 c = cscale(ad.comp_corr_main[0], endpoint);
+      double2 t = make_double2(0.0, 0.0);
+      for (int j = 0; j < ad.order; ++j) t = cadd(t, cscale(ad.comp_corr_main[j + 1], carried[j]));
+      adv = cadd(adv, cscale(ad.dz, cadd(t, c)));
+    }
+    a.advanced[i] = adv;
+    const int bin = i % a.n_omega;
+    const bool scored = a.norm_mask[bin];
+    for (int r = 0; r < n_orders; ++r) {
+      double2 d = make_double2(0.0, 0.0);
+      for (int k = 0; k < width; ++k) {
+        double2 comb = make_double2(0.0, 0.0);
+        for (int j = 0; j < width; ++j) {
+          const double c = ad.rows[r][j][k];
+          if (c != 0.0) comb = cadd(comb, cscale(c, xs[j]));
+        }
+        d = cadd(d, cmul(mom[k], comb));
+      }
+      d = cscale(ad.dz, d);
+      if (ad.compensated) {
+        // corrector(k) - predictor(k) of the compensation
+        double2 tc = make_double2(0.0, 0.0), tp = make_double2(0.0, 0.0);
+        for (int j = 0; j < width - 1; ++j) {
+          tc = cadd(tc, cscale(ad.comp_corr[r][j + 1], carried[j]));
+          tp = cadd(tp, cscale(ad.comp_pred[r][j], carried[j]));
+        }
+        tc = cadd(tc, cscale(ad.comp_corr[r][0], endpoint));
+        d = cadd(d, csub(cscale(ad.dz, tc), cscale(ad.dz, tp)));
+      }
+      if (scored) v[r] += d.x * d.x + d.y * d.y;
+    }
+  }
+  block_partials<kMaxOrders>(v, a.partials);
+}
+
+__global__ void k_adams_accept(StepArgs a, int free_slot, int write_rate) {
+  const AdamsDev& ad = *a.adams;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const int bin = i % a.n_omega;
+    const double2 adv = a.advanced[i];
+    a.state[i] = a.active_mask[bin] ? adv : make_double2(adv.x * 0.0, adv.y * 0.0);
+    a.store[(size_t)free_slot * a.n + i] = a.source[i];
+    if (write_rate) {
+      a.states[(size_t)free_slot * a.n + i] = a.lab[i];
+      double2 r = make_double2(0.0, 0.0);
+      for (int p = 0; p < a.stage->n_phi; ++p)
+        r = cadd(r, cscale(ad.rate_w[p], a.phi_terms[(size_t)p * a.n + i]));
+      a.rates[(size_t)free_slot * a.n + i] = r;
+    }
+  }
+}
+
+__global__ void k_adams_start(StepArgs a, int write_rate) {
+  const AdamsDev& ad = *a.adams;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    a.store[i] = a.source[i];
+    if (write_rate) {
+      a.states[i] = a.state[i];
+      double2 r = make_double2(0.0, 0.0);
+      for (int p = 0; p < a.stage->n_phi; ++p)
+        r = cadd(r, cscale(ad.rate0_w[p], a.phi_terms[(size_t)p * a.n + i]));
+      a.rates[i] = r;
+    }
+  }
+}
+
+cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t s) {
+  k_adams_predict<<<kNormBlocks, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t s) {
+  k_adams_correct<<<kNormBlocks, 256, 0, s>>>(a);
+  k_reduce<<<kMaxOrders + 1, 32, 0, s>>>(a.partials, a.norms, kMaxOrders + 1);
+  return cudaGetLastError();
+}
+cudaError_t launch_adams_accept(const StepArgs& a, int free_slot, double2*, cudaStream_t s) {
+  k_adams_accept<<<kNormBlocks, 256, 0, s>>>(a, free_slot, a.states != nullptr);
+  return cudaGetLastError();
+}
+cudaError_t launch_adams_start(const StepArgs& a, cudaStream_t s) {
+  k_adams_start<<<kNormBlocks, 256, 0, s>>>(a, a.states != nullptr);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ DOPRI5
+struct RkCoeffs {
+  double a[8];
+  int stage;
+  double dz;
+};
+
+__global__ void __launch_bounds__(256) k_rk_stage_input(RkArgs a, RkCoeffs c) {
+  const StageScalarsDev& st = *a.stage;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const double2 x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
+    double2 comb = make_double2(0.0, 0.0);
+    for (int j = 0; j < c.stage; ++j) comb = cadd(comb, cscale(c.a[j], a.stages[(size_t)j * a.n + i]));
+    const double2 y = a.state[i];
+    const double2 inner = cadd(y, cscale(c.dz, comb));
+    a.lab[i] = cmul(cexp(x), inner);
+    a.back[i] = cexp(make_double2(-x.x, -x.y));
+  }
+}
+
+struct RkFinish {
+  double b[8], e[8];
+  double dz;
+};
+
+__global__ void __launch_bounds__(256) k_rk_finish(RkArgs a, RkFinish f) {
+  const StageScalarsDev& st = *a.stage;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    double2 sol = make_double2(0.0, 0.0), err = make_double2(0.0, 0.0);
+    for (int j = 0; j < 7; ++j) {
+      const double2 k = a.stages[(size_t)j * a.n + i];
+      sol = cadd(sol, cscale(f.b[j], k));
+      err = cadd(err, cscale(f.e[j], k));
+    }
+    const double2 x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
+    const double2 prop = cexp(x);
+    const double2 y = a.state[i];
+    const double2 adv = cmul(prop, cadd(y, cscale(f.dz, sol)));
+    const double2 e = cmul(prop, cscale(f.dz, err));
+    a.advanced[i] = adv;
+    if (a.norm_mask[i % a.n_omega]) {
+      v[0] += y.x * y.x + y.y * y.y;
+      v[1] += adv.x * adv.x + adv.y * adv.y;
+      v[2] += e.x * e.x + e.y * e.y;
+    }
+  }
+  block_partials<3>(v, a.partials);
+}
+
+__global__ void k_mask_copy(double2* dst, const double2* src, const unsigned char* active, int n,
+                            int n_omega) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double2 v = src[i];
+    dst[i] = active[i % n_omega] ? v : make_double2(v.x * 0.0, v.y * 0.0);
+  }
+}
+
+cudaError_t launch_rk_stage_input(const RkArgs& a, int stage, const double* coeffs, double dz,
+                                  cudaStream_t s) {
+  RkCoeffs c = {};
+  for (int j = 0; j < stage && j < 8; ++j) c.a[j] = coeffs[j];
+  c.stage = stage;
+  c.dz = dz;
+  k_rk_stage_input<<<kNormBlocks, 256, 0, s>>>(a, c);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rk_finish(const RkArgs& a, const double* b, const double* e, double dz,
+                             double, double, cudaStream_t s) {
+  RkFinish f = {};
+  for (int j = 0; j < 7; ++j) {
+    f.b[j] = b[j];
+    f.e[j] = e[j];
+  }
+  f.dz = dz;
+  k_rk_finish<<<kNormBlocks, 256, 0, s>>>(a, f);
+  k_reduce<<<3, 32, 0, s>>>(a.partials, a.norms, 3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mask_copy(double2* dst, const double2* src, const unsigned char* active, int n,
+                             int n_omega, cudaStream_t s) {
+  k_mask_copy<<<kNormBlocks, 256, 0, s>>>(dst, src, active, n, n_omega);
+  return cudaGetLastError();
+}
+
+}  // namespace sp

@@ -1,0 +1,52 @@
+"""The C ABI without a GPU: the library loads and exports every declared symbol."""
+
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from solprop_b200 import _lib
+from solprop_b200.record import load_record
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols() -> set[str]:
+    text = "\n".join(p.read_text() for p in (ROOT / "include").glob("*.h"))
+    return set(re.findall(r"\b(sp_[a-z_]+)\s*\(", text))
+
+
+def test_header_declares_the_bound_functions():
+    assert declared_symbols() == set(_lib.SIGNATURES)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.library()
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_version_and_error_buffer():
+    lib = _lib.library()
+    assert b"sm_100a" in lib.sp_version()
+
+
+def test_problem_descriptor_round_trip_and_refusals():
+    rec = load_record(ROOT / "tests" / "golden" / "cap1_ar.problem.npz")
+    desc, keep = _lib.problem_desc(rec)
+    assert desc.n_to == rec.n_to and desc.n_phi_terms == 1 and desc.band == 1
+    assert desc.n_taps == rec.taps.size
+    # the problem object validates and copies on the host; no device needed
+    problem = _lib.Problem(rec)
+    problem.close()
+    env = load_record(ROOT / "tests" / "golden" / "gnlse_raman.problem.npz")
+    with pytest.raises(_lib.BackendRefusal, match="envelope"):
+        _lib.Problem(env)
+
+
+def test_invalid_descriptor_is_an_argument_error():
+    rec = load_record(ROOT / "tests" / "golden" / "cap1_ar.problem.npz")
+    rec.n_to = 1000  # not a power of two
+    with pytest.raises(_lib.NativeError, match="power of two"):
+        _lib.Problem(rec)

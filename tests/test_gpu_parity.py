@@ -1,0 +1,95 @@
+"""Parity of the CUDA path with the reference, through the C ABI, on a B200.
+
+One source evaluation against the golden vectors at 1e-10 relative L2 (the contract's
+per-step bar; measured values are ~1e-15); fixed schedules plane by plane at 1e-10;
+adaptive runs within the stepper's rtol at every plane, with the attempt counts of
+the reference.
+"""
+
+import numpy as np
+import pytest
+
+from tests._cases import fixed_schedule, golden, policy, record, rel
+
+pytestmark = pytest.mark.gpu
+
+SOURCE_TOL = 1e-10
+STEP_TOL = 1e-10
+
+
+def _workspace(case, fixed=False):
+    from solprop_b200 import _lib
+
+    rec = record(case, fixed)
+    problem = _lib.Problem(rec)
+    return rec, problem, _lib.Workspace(problem)
+
+
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he"])
+@pytest.mark.parametrize("index", [0, 1])
+def test_source_matches_reference(case, index):
+    rec, problem, ws = _workspace(case)
+    g = golden(case)
+    got = ws.source(g[f"src{index}.lab"], float(g[f"src{index}.z"]))
+    assert rel(got, g[f"src{index}.source"]) < SOURCE_TOL
+
+
+def test_source_matches_oracle_on_random_fields():
+    from oracle import source as S
+
+    rec, problem, ws = _workspace("cap1_ar")
+    rng = np.random.default_rng(7)
+    for z in (0.0, 0.011):
+        lab = rec.field0 * np.exp(1j * rng.uniform(-1, 1, rec.field0.shape)) * 1.5
+        lab = lab * rec.active_mask
+        assert rel(ws.source(lab, z), S.lab_source(rec, lab, z)) < SOURCE_TOL
+
+
+def test_quiet_collar_drops_the_absorber():
+    from oracle import source as S
+
+    rec, problem, ws = _workspace("cap1_ar")
+    g = golden("cap1_ar")
+    got = ws.source(g["src0.lab"], 0.0, quiet=True)
+    assert rel(got, S.lab_source(rec, g["src0.lab"], 0.0, quiet=True)) < SOURCE_TOL
+
+
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he"])
+def test_fixed_schedule_matches_reference(case):
+    rec, problem, ws = _workspace(case, fixed=True)
+    g = golden(case)
+    pol = policy(g, "fixed")
+    steps, edges = fixed_schedule(g)
+    session = ws.start(pol, schedule=steps)
+    zs, states = g["fixed.z"], g["fixed.states"]
+    plane = 1
+    while True:
+        batch = session.advance(1)
+        if plane < len(zs) and abs(batch.z - zs[plane]) < 1e-12:
+            assert rel(session.export(), states[plane]) < STEP_TOL, (case, plane)
+            plane += 1
+        if batch.event in (2, 3):
+            break
+    assert plane == len(zs)
+
+
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he"])
+def test_adaptive_run_matches_reference(case):
+    rec, problem, ws = _workspace(case)
+    g = golden(case)
+    pol = policy(g, "adaptive")
+    session = ws.start(pol)
+    zs, states = g["adaptive.z"], g["adaptive.states"]
+    seen = 1
+    while True:
+        batch = session.advance(256)
+        assert batch.event != 3
+        if batch.event in (1, 2):
+            assert abs(batch.z - zs[seen]) < 1e-12
+            assert rel(session.export(), states[seen]) < pol["rtol"]
+            seen += 1
+        if batch.event == 2:
+            break
+    assert seen == len(zs)
+    # decisions follow the reference's (rounding may move a borderline one)
+    assert abs(batch.attempts - int(g["adaptive.counts"][0])) <= 3
