@@ -1,0 +1,287 @@
+"""Benchmark of the B200 propagation hot path (one JSON line on stdout, rank 0).
+
+Workload: BASELINE config 2, the four-mode (HE11-HE14) helium capillary with a 0.8 -> 0
+bar gradient, 1.5 m, 800 nm, 7.5 fs, 275 uJ, 90 nm - 4 um, n_to = 16384 fine samples,
+64 Gauss nodes, Kerr + field plasma (band rule) + the in-stage collar, exponential
+Adams at rtol 1e-6 -- lowered from the reference's own translation
+(``tests/golden/config2.problem.npz``, made by ``tests/golden/generate.py``).
+
+A step is one exponential-Adams attempt of that run: predictor, one source evaluation
+(inverse FFT, synthesis + plasma/Kerr column, projection, forward FFT, stage output),
+corrector with its defect norms, and the accept -- FP64 throughout.  ``value`` is
+attempts per second with the state resident in HBM, timed with CUDA events on the
+library's stream, L2 flushed (a 256 MiB write) between steps.  ``e2e`` is the same
+through the public C ABI from host memory: session start (host field upload), the
+attempts, and the export of the final field.  Multi-GPU: the run does not shard
+(z is sequential), so N ranks run N independent replicas (weak scaling).
+
+``--impl reference`` times the reference's CPU implementation of the path -- the
+oracle port of ``numpy_ref`` (``oracle/``), pinned bit for bit to it by the tests --
+on the host cores, on the same workload and unit.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "config2"
+METRIC = "steps/s (exponential-Adams attempts, plain FP64, config 2 four-mode He capillary)"
+UNIT = "steps/s"
+
+
+def load_workload():
+    from tests._cases import golden, policy, record
+
+    rec = record(WORKLOAD)
+    pol = policy(golden(WORKLOAD), "adaptive")
+    return rec, pol
+
+
+def algorithmic_bytes(rec) -> dict:
+    """Bytes each kernel family must move per launch (reads + writes of its operands)."""
+    n = rec.n_cols * rec.n_omega
+    c128, f64 = 16, 8
+    nt, nn, nc = rec.n_to, rec.n_nodes, rec.n_cols
+    streams = 3 if rec.plasma_enabled else 1
+    absorber = 1 if rec.absorber_scheme == "nonlinear" else 0
+    return {
+        "adams_predict": (2 + 5) * n * c128 + 7 * n * c128,  # state, history read; lab, moments, flow, exp
+        "inverse_fft": n * c128 + (1 + absorber) * nc * nt * f64 + nt * f64,
+        "response_column": nc * nt * f64 + 2 * nt * f64 + streams * nn * nt * f64,
+        "project": streams * nn * nt * f64 + streams * nc * nt * f64,
+        "forward_fft": (streams + absorber) * nc * (nt * f64 + rec.n_omega * c128),
+        "stage_output": (streams + absorber) * n * c128 + rec.n_prefactor_terms * n * c128 + n * c128,
+        "adams_correct": (1 + 6 + 6 + 2) * n * c128,
+        "adams_accept": 4 * n * c128,
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+
+    def summary(self) -> dict:
+        rows = []
+        for line in self.path.read_text().splitlines() if self.path.exists() else []:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_arm(rec, pol, steps: int, warmup: int, budget_s: float, threads: int | None):
+    """The oracle march on the host: one attempt per step, wall-clock timed."""
+    from threadpoolctl import threadpool_limits
+
+    from oracle import march as M
+
+    with threadpool_limits(limits=threads):
+        ws = M.Workspace(rec)
+        march = M.AdamsMarch(M.AdamsEngine(ws, pol), pol, pol["proposal"])
+        target = float(pol["save_planes"][0]) if pol["save_planes"] else rec.z_end
+        for _ in range(warmup):
+            march.attempt_towards(target)
+        done, t0 = 0, time.perf_counter()
+        while done < steps and (time.perf_counter() - t0) < budget_s:
+            march.attempt_towards(target)
+            done += 1
+        elapsed = time.perf_counter() - t0
+    return done, elapsed
+
+
+def main() -> int:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=200)
+    parser.add_argument("--warmup", type=int, default=10)
+    parser.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    parser.add_argument("--cpu-budget", type=float, default=20.0)
+    args = parser.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rec, pol = load_workload()
+    config = {"workload": "config2: 4-mode He capillary 1.5 m 0.8->0 bar, n_to 16384, 64 nodes",
+              "state": [rec.n_modes, rec.n_pol, rec.n_omega], "n_to": rec.n_to,
+              "n_nodes": rec.n_nodes, "phi_terms": rec.n_phi_terms, "rtol": pol["rtol"],
+              "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{args.gpus}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = os.cpu_count()
+        done, elapsed = cpu_arm(rec, pol, args.steps, args.warmup, budget_s=150.0, threads=None)
+        value = done / elapsed
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+                "n_gpus": args.gpus, "steps": done, "warmup": args.warmup,
+                "ms_per_step": 1e3 * elapsed / done, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config,
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                                 "sample": f"{done} attempts of the config-2 run from z=0 "
+                                           "(oracle port of numpy_ref, all host threads)"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+
+    from solprop_b200 import _lib
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    problem = _lib.Problem(rec)
+    ws = _lib.Workspace(problem, local)
+    stream = torch.cuda.ExternalStream(ws.stream, device=torch.device("cuda", local))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    # ---- device-resident throughput
+    session = ws.start(pol)
+    for _ in range(max(args.warmup, 3)):
+        session.advance(1)
+    times = []
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+            batch = session.advance(1)
+            end.record(stream)
+            times.append((start, end))
+            if batch.event == 2:
+                session = ws.start(pol)  # the run ended: start it again
+        torch.cuda.synchronize()
+    total_ms = sum(s.elapsed_time(e) for s, e in times)
+    if world > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms / 1e3)
+
+    # ---- per-kernel device times over a second timed pass (same steps, events per launch)
+    session.set_timing(True)
+    session.timing(reset=True)
+    kernel_steps = min(args.steps, 100)
+    for _ in range(kernel_steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        if session.advance(1).event == 2:
+            session = ws.start(pol)
+            session.set_timing(True)
+    kernels = session.timing(reset=True)
+    session.set_timing(False)
+    launches_per_step = sum(c for c in (v[1] for v in kernels.values())) / kernel_steps
+    launches_per_step += kernels["adams_correct"][1] / kernel_steps  # correct + its reduction
+    top = max(kernels, key=lambda k: kernels[k][0])
+    top_ms = kernels[top][0] / max(kernels[top][1], 1)
+    algo = algorithmic_bytes(rec)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = algo.get(top, 0) / (top_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "algorithmic_bytes": algo.get(top, 0), "avg_launch_ms": top_ms,
+                "kernels_ms_per_step": {k: v[0] / kernel_steps for k, v in kernels.items() if v[1]}}
+
+    # ---- end to end through the C ABI from host memory
+    field_host = torch.from_numpy(np.ascontiguousarray(rec.field0).view(np.float64)).pin_memory()
+    out_host = torch.empty_like(field_host).pin_memory()
+    e2e_steps = args.steps
+    torch.cuda.synchronize()
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s_ev.record(stream)
+    s2 = ws.start(pol, field0=field_host.numpy().view(np.complex128).reshape(rec.field0.shape))
+    for _ in range(e2e_steps):
+        if s2.advance(1).event == 2:
+            break
+    result = s2.export()
+    e_ev.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = s_ev.elapsed_time(e_ev)
+    state_bytes = rec.n_cols * rec.n_omega * 16
+    per_attempt_h2d = 2 * 1200 + 4000  # two stage-scalar slots and the Adams tables
+    e2e = {"value": world * e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(state_bytes / e2e_steps + per_attempt_h2d),
+           "d2h_bytes_per_step": int(state_bytes / e2e_steps + 32)}
+    assert np.all(np.isfinite(result))
+
+    cpu = None
+    if rank == 0:
+        done, elapsed = cpu_arm(rec, pol, steps=1000, warmup=1, budget_s=args.cpu_budget, threads=1)
+        cpu = {"value": done / elapsed, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{done} attempts of the config-2 run from z=0 on one host thread "
+                         f"({os.cpu_count()} cores on the box)"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(round(launches_per_step * args.steps)),
+            "clocks": clocks.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del session, s2
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

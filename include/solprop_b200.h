@@ -152,6 +152,10 @@ sp_status sp_workspace_source_device(sp_workspace* ws, const void* lab_device, d
 /* Kernel launches one source evaluation makes (the evidence of the device path). */
 int sp_workspace_launches_per_source(const sp_workspace* ws);
 
+/* The CUDA stream (cudaStream_t) every launch of this workspace goes to; callers that
+ * time the device record their events on it. */
+void* sp_workspace_stream(sp_workspace* ws);
+
 /* ---- session (replaces _core.Session, _core.pyi:430-470) ---- */
 sp_status sp_session_start(sp_workspace* ws, const sp_run_desc* run, sp_session** out);
 /* Step until a save plane, the end, or work_limit attempts (the native call's bound). */
@@ -159,6 +163,19 @@ sp_status sp_session_advance(sp_session* s, int32_t work_limit, sp_batch* out);
 /* Copies the current state to out, host complex (n_modes, n_pol, n_omega). */
 sp_status sp_session_export(sp_session* s, double* out);
 sp_status sp_session_destroy(sp_session* s);
+
+/* Per-kernel device timing of a session (replaces the native timing probe and counters,
+ * _core.Workspace.probe/counters, _core.pyi:600-612, bindings/module.cpp:832).  While
+ * enabled, CUDA events are recorded on the workspace stream around every launch and the
+ * elapsed times accumulate per kernel family, in this order: */
+enum {
+  SP_K_PREDICT = 0, SP_K_INVERSE, SP_K_COLUMN, SP_K_PROJECT, SP_K_FORWARD, SP_K_OUTPUT,
+  SP_K_CORRECT, SP_K_ACCEPT, SP_K_START, SP_K_RK_STAGE, SP_K_RK_FINISH, SP_K_COUNT
+};
+sp_status sp_session_set_timing(sp_session* s, int enable);
+/* ms[SP_K_COUNT] accumulated milliseconds, launches[SP_K_COUNT] launch counts; reset=1
+ * clears them after reading. */
+sp_status sp_session_timing(sp_session* s, double* ms, int64_t* launches, int reset);
 
 #ifdef __cplusplus
 }

@@ -435,18 +435,22 @@ class AdamsMarch:
         on_kink = interior and any(abs(k - end) <= tol for k in kinks)
         return dz, end, kind == "hard_kink" or on_kink
 
-    def march_to(self, target):
+    def attempt_towards(self, target):
+        """One attempt of :meth:`march_to` (a startup first when the history is empty)."""
         p = self.p
         planes = tuple(float(v) for v in p["save_planes"]) if not p["interpolate"] else ()
         kinks = tuple(float(v) for v in p["hard_kinks"])
         edges = tuple(float(v) for v in p["breakpoints"])
         z_end = p["z_end"] if p["interpolate"] else target
+        if not self.history:
+            self._start()
+        stop = _landing(self.z, self.proposal, planes, kinks, edges, p["dz_max"], z_end, p["stretch"])
+        dz, end, kink = self._approach(stop, planes, kinks, target)
+        return self._attempt(dz, end, kink)
+
+    def march_to(self, target):
         while not reached(self.z, target):
-            if not self.history:
-                self._start()
-            stop = _landing(self.z, self.proposal, planes, kinks, edges, p["dz_max"], z_end, p["stretch"])
-            dz, end, kink = self._approach(stop, planes, kinks, target)
-            self._attempt(dz, end, kink)
+            self.attempt_towards(target)
 
     def replay(self, steps, edges):
         for i, dz in enumerate(steps):

@@ -99,7 +99,14 @@ SIGNATURES = {
     "sp_session_advance": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SpBatch)]),
     "sp_session_export": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "sp_session_destroy": (C.c_int, [C.c_void_p]),
+    "sp_workspace_stream": (C.c_void_p, [C.c_void_p]),
+    "sp_session_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "sp_session_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]),
 }
+
+KERNEL_NAMES = ("adams_predict", "inverse_fft", "response_column", "project", "forward_fft",
+                "stage_output", "adams_correct", "adams_accept", "adams_start", "rk_stage_input",
+                "rk_finish")
 
 _LIB: C.CDLL | None = None
 
@@ -340,6 +347,11 @@ class Workspace:
                                                    int(quiet), C.c_void_p(out_ptr)))
 
     @property
+    def stream(self) -> int:
+        """The ``cudaStream_t`` of every launch of this workspace, as an integer."""
+        return int(library().sp_workspace_stream(self.handle) or 0)
+
+    @property
     def launches_per_source(self) -> int:
         return int(library().sp_workspace_launches_per_source(self.handle))
 
@@ -369,6 +381,17 @@ class Session:
     def advance(self, work_limit: int = 256) -> SpBatch:
         check(library().sp_session_advance(self.handle, int(work_limit), C.byref(self.batch)))
         return self.batch
+
+    def set_timing(self, enable: bool) -> None:
+        check(library().sp_session_set_timing(self.handle, int(enable)))
+
+    def timing(self, reset: bool = False) -> dict:
+        """Accumulated device milliseconds and launch counts per kernel family."""
+        n = len(KERNEL_NAMES)
+        ms = (C.c_double * n)()
+        counts = (C.c_int64 * n)()
+        check(library().sp_session_timing(self.handle, ms, counts, int(reset)))
+        return {name: (ms[i], counts[i]) for i, name in enumerate(KERNEL_NAMES)}
 
     def export(self) -> np.ndarray:
         out = np.empty(self.ws.shape, dtype=np.complex128)

@@ -202,12 +202,57 @@ struct sp_workspace {
   DevBuf<double> partials, norms;
   double* h_norms = nullptr;         // pinned
   static constexpr int kStageSlots = 10;
+  // per-kernel timing (sp_session_set_timing)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  size_t ev_next = 0;
+  double t_ms[SP_K_COUNT] = {};
+  int64_t t_count[SP_K_COUNT] = {};
+  cudaEvent_t next_event() {
+    if (ev_next == ev_pool.size()) {
+      cudaEvent_t e;
+      CUDA_CHECK(cudaEventCreate(&e));
+      ev_pool.push_back(e);
+    }
+    return ev_pool[ev_next++];
+  }
+  void flush_timing() {
+    if (pending.empty()) return;
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    for (auto& p : pending) {
+      float ms = 0.f;
+      CUDA_CHECK(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+      t_ms[p.first] += ms;
+      t_count[p.first] += 1;
+    }
+    pending.clear();
+    ev_next = 0;
+  }
   ~sp_workspace() {
+    for (auto e : ev_pool) cudaEventDestroy(e);
     if (stream) cudaStreamSynchronize(stream);
     if (h_stage) cudaFreeHost(h_stage);
     if (h_adams) cudaFreeHost(h_adams);
     if (h_norms) cudaFreeHost(h_norms);
     if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+// Records events around one launch family while timing is on.
+struct KernelTimer {
+  sp_workspace* ws;
+  int kind;
+  cudaEvent_t end{};
+  KernelTimer(sp_workspace* w, int k) : ws(w), kind(k) {
+    if (!ws->timing) return;
+    cudaEvent_t start = ws->next_event();
+    end = ws->next_event();
+    CUDA_CHECK(cudaEventRecord(start, ws->stream));
+    ws->pending.push_back({kind, {start, end}});
+  }
+  ~KernelTimer() {
+    if (ws->timing) cudaEventRecord(end, ws->stream);
   }
 };
 
@@ -251,7 +296,7 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
   InverseArgs ia{lab, ws->fine_to_coarse.p, ws->twiddles.p, ws->modal_t.p,
                  absorber ? ws->streams.p + (size_t)3 * P.n_cols * d.n_to : nullptr,
                  ws->alpha.p, d.n_omega, d.n_to, ws->log_m, ws->log_n_to};
-  CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream));
+  { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
   ColumnArgs ca{};
   ca.stage = ws->stage.p + slot;
   ca.modal_t = ws->modal_t.p;
@@ -280,11 +325,11 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
   ca.rate_max = d.rate_max;
   ca.rate_coefficients = ws->rate_coeff.p;
   ca.taps = ws->taps.p;
-  CUDA_CHECK(launch_column(ca, ws->stream));
+  { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column(ca, ws->stream)); }
   const int n_streams = d.plasma_enabled ? 3 : 1;
   ProjectArgs pa{ws->stage.p + slot, ws->node_p.p, ws->node_x.p, ws->node_z.p, ws->projection.p,
                  ws->streams.p, d.n_nodes, d.n_modes, P.n_cols, d.n_to, n_streams};
-  CUDA_CHECK(launch_project(pa, ws->stream));
+  { KernelTimer t(ws, SP_K_PROJECT); CUDA_CHECK(launch_project(pa, ws->stream)); }
   // stream rows: P [0, nc), gJ [nc, 2nc), g'J [2nc, 3nc), absorber [3nc, 4nc). The row
   // list holds [0, 4nc) for plasma runs and, at offset 4nc, [P rows, absorber rows].
   const int nc = P.n_cols;
@@ -292,11 +337,11 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
   ForwardArgs fa{ws->streams.p, d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
                  ws->crop.p, ws->twiddles.p, ws->spectra.p, d.n_to, d.n_omega, ws->log_m,
                  ws->log_n_to};
-  CUDA_CHECK(launch_forward(fa, n_rows, ws->stream));
+  { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, n_rows, ws->stream)); }
   OutputArgs oa{ws->stage.p + slot, ws->spectra.p, ws->pre_terms.p, ws->omega.p,
                 ws->omega_window.p, ws->active.p, inv_prop, out, P.n_cols, d.n_omega,
                 d.plasma_enabled, absorber};
-  CUDA_CHECK(launch_output(oa, ws->stream));
+  { KernelTimer t(ws, SP_K_OUTPUT); CUDA_CHECK(launch_output(oa, ws->stream)); }
 }
 
 static void build_workspace(sp_workspace* ws) {
@@ -454,7 +499,7 @@ static void adams_start(sp_session* S) {
   a.states = comp ? ws->states.p : nullptr;
   a.rates = comp ? ws->rates.p : nullptr;
   a.source = ws->src.p;
-  CUDA_CHECK(launch_adams_start(a, ws->stream));
+  { KernelTimer t(ws, SP_K_START); CUDA_CHECK(launch_adams_start(a, ws->stream)); }
   S->evaluations += 1;
   S->history.assign(1, {S->z, 0});
   S->order = S->run.variable_order ? 1 : S->run.order;
@@ -567,12 +612,13 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
   a.advanced = ws->adv.p;
   a.partials = ws->partials.p;
   a.norms = ws->norms.p;
-  CUDA_CHECK(launch_adams_predict(a, ws->stream));
+  { KernelTimer t(ws, SP_K_PREDICT); CUDA_CHECK(launch_adams_predict(a, ws->stream)); }
   eval_source(ws, ws->lab.p, 1, nullptr, ws->src.p, false);
-  CUDA_CHECK(launch_adams_correct(a, ws->stream));
+  { KernelTimer t(ws, SP_K_CORRECT); CUDA_CHECK(launch_adams_correct(a, ws->stream)); }
   CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, sizeof(double) * (kMaxOrders + 1),
                              cudaMemcpyDeviceToHost, ws->stream));
   CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+  ws->flush_timing();
   S->attempts += 1;
   S->evaluations += 1;
   const double magnitude = std::sqrt(ws->h_norms[kMaxOrders]);
@@ -608,7 +654,7 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
     for (auto& e : keep) used |= e.second == free_slot;
     if (!used) break;
   }
-  CUDA_CHECK(launch_adams_accept(a, free_slot, nullptr, ws->stream));
+  { KernelTimer t(ws, SP_K_ACCEPT); CUDA_CHECK(launch_adams_accept(a, free_slot, nullptr, ws->stream)); }
   keep.push_back({S->z + dz, free_slot});
   S->history = keep;
   S->rejections = 0;
@@ -743,11 +789,11 @@ static double rk_trial(sp_session* S, double dz) {
   for (int i = 0; i < 7; ++i) e[i] = kB[i] - kBhat[i];
   for (int i = 0; i < 7; ++i) {
     a.stage = ws->stage.p + i;
-    CUDA_CHECK(launch_rk_stage_input(a, i, kA[i], dz, ws->stream));
+    { KernelTimer t(ws, SP_K_RK_STAGE); CUDA_CHECK(launch_rk_stage_input(a, i, kA[i], dz, ws->stream)); }
     eval_source(ws, ws->lab.p, i, ws->back.p, ws->stages.p + (size_t)i * P.n, false);
   }
   a.stage = ws->stage.p + 7;
-  CUDA_CHECK(launch_rk_finish(a, kB, e, dz, R.rtol, R.atol, ws->stream));
+  { KernelTimer t(ws, SP_K_RK_FINISH); CUDA_CHECK(launch_rk_finish(a, kB, e, dz, R.rtol, R.atol, ws->stream)); }
   CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, 3 * sizeof(double), cudaMemcpyDeviceToHost,
                              ws->stream));
   CUDA_CHECK(cudaStreamSynchronize(ws->stream));
@@ -1061,6 +1107,32 @@ sp_status sp_session_export(sp_session* S, double* out) {
 sp_status sp_session_destroy(sp_session* S) {
   delete S;
   return SP_OK;
+}
+
+void* sp_workspace_stream(sp_workspace* ws) { return ws ? (void*)ws->stream : nullptr; }
+
+sp_status sp_session_set_timing(sp_session* S, int enable) {
+  return guarded([&] {
+    if (!S) throw Failure(SP_ERR_ARGUMENT, "NULL session");
+    S->ws->flush_timing();
+    S->ws->timing = enable != 0;
+  });
+}
+
+sp_status sp_session_timing(sp_session* S, double* ms, int64_t* launches, int reset) {
+  return guarded([&] {
+    if (!S || !ms || !launches) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    sp_workspace* ws = S->ws;
+    ws->flush_timing();
+    for (int k = 0; k < SP_K_COUNT; ++k) {
+      ms[k] = ws->t_ms[k];
+      launches[k] = ws->t_count[k];
+      if (reset) {
+        ws->t_ms[k] = 0.0;
+        ws->t_count[k] = 0;
+      }
+    }
+  });
 }
 
 }  // extern "C"

@@ -84,16 +84,19 @@ BORZSONYI = {
 GAMMA3 = {"He": 3.43e-53, "Ne": 6.8e-53, "Ar": 1.2e-51}
 
 
-def gas_species(name: str) -> Species:
-    lam = np.geomspace(120e-9, 200e-6, 4000)[::-1]
+def gas_species(name: str, deep_uv: bool = False) -> Species:
+    """A species of supplied data; ``deep_uv`` keeps only the fit's far pole, so that the
+    table reaches 40 nm (a grid limited at 90 nm samples below the fit's second pole)."""
+    shortest = 40e-9 if deep_uv else 120e-9
+    lam = np.geomspace(shortest, 200e-6, 4000)[::-1]
     om = 2 * np.pi * C0 / lam
     l2 = (lam * 1e6) ** 2
     b1, c1, b2, c2 = BORZSONYI[name]
-    n2m1 = b1 * l2 / (l2 - c1) + b2 * l2 / (l2 - c2)
+    n2m1 = b1 * l2 / (l2 - c1) + (0.0 if deep_uv else b2 * l2 / (l2 - c2))
     rho0 = 1e5 / (K_B * 273.15)
     refr = (np.sqrt(1 + n2m1) - 1) / rho0
     sus = TabulatedSusceptibility(
-        om, refr, np.zeros_like(om), (121e-9, 199e-6), f"Borzsonyi 2008 {name}"
+        om, refr, np.zeros_like(om), (shortest * 1.01, 199e-6), f"Borzsonyi 2008 {name}"
     )
     ip = HISTORICAL_ATOMS[name][0] * AU_ENERGY
     return Species(name, sus, IdealGas(), gamma3=GAMMA3[name], ionisation=IonisationData(ip))
@@ -101,8 +104,8 @@ def gas_species(name: str) -> Species:
 
 def capillary(name, *, gas, pressure, length, n_t_limits, trange, energy, fwhm, modes,
               n_r=None, radial_rule="gauss_kronrod", absorber=None, schedule=None,
-              n_save=3, rtol=1e-6):
-    species = gas_species(gas)
+              n_save=3, rtol=1e-6, deep_uv=False):
+    species = gas_species(gas, deep_uv)
     fill = Mixture.fill({species: 1.0}, pressure, length=length if not np.isscalar(pressure) else None)
     grid = FieldGrid.from_limits(length, 800e-9, n_t_limits, trange, fft_size="pow2")
     kwargs = dict(
@@ -351,6 +354,27 @@ def gnlse_case(case, seed):
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
 
 
+def workload_case(case, *, seed, **common):
+    """A full-size configuration: the problem, the march policy and two reference
+    source evaluations (no run: at this size the reference takes seconds per step)."""
+    sim = capillary(case, **common)
+    problem, request = sim.translate(), sim.run_request()
+    backend = NumpyRefBackend(problem, request, grid=sim.grid, modes=sim.modes,
+                              profiles=sim.profiles)
+    session = backend.prepare(problem, request).start(Start.entrance(problem))
+    policy = policy_record(session, request)
+    ws = backend._workspace
+    field0 = np.broadcast_to(problem.initial.field0, problem.shape).copy()
+    rng = np.random.default_rng(seed)
+    lab1 = field0 * np.exp(1j * rng.uniform(-0.3, 0.3, problem.shape)) * problem.grids.active_mask
+    golden = {"adaptive.policy": policy, "fixed.policy": policy}
+    for i, (lab, z) in enumerate([(field0, 0.0), (lab1, 0.4 * problem.linear.phi_breakpoints[-1])]):
+        golden[f"src{i}.lab"] = lab
+        golden[f"src{i}.z"] = np.array(z)
+        golden[f"src{i}.source"] = ws.lab_source(lab, z)
+    write(case, problem, golden)
+
+
 if __name__ == "__main__":
     only = set(sys.argv[1:])
     if not only or "cap1_ar" in only:
@@ -363,3 +387,15 @@ if __name__ == "__main__":
                  radial_rule="gauss", fixed_dz=0.005, n_fixed_planes=11, seed=2)
     if not only or "gnlse_raman" in only:
         gnlse_case("gnlse_raman", seed=3)
+    if not only or "config2" in only:
+        # He 125 um, 1.5 m, 0.8 -> 0 bar, 800 nm, 7.5 fs, 275 uJ,
+        # HE11-HE14, 90 nm - 4 um, 400 fs, pow2 grid (n_to 16384), 64 Gauss nodes
+        workload_case("config2", seed=4, gas="He", pressure=(0.8, 0.0), length=1.5,
+                      n_t_limits=(90e-9, 4e-6), trange=400e-15, energy=275e-6, fwhm=7.5e-15,
+                      modes=4, n_r=64, radial_rule="gauss", deep_uv=True)
+    if not only or "config1" in only:
+        # Ar 125 um, 1 m, 1 bar, 800 nm, 10 fs, 100 uJ, HE11,
+        # 150 nm - 4 um, 400 fs, pow2 grid (n_to 8192)
+        workload_case("config1", seed=5, gas="Ar", pressure=1.0, length=1.0,
+                      n_t_limits=(150e-9, 4e-6), trange=400e-15, energy=100e-6, fwhm=10e-15,
+                      modes=1)

@@ -25,7 +25,7 @@ def _workspace(case, fixed=False):
     return rec, problem, _lib.Workspace(problem)
 
 
-@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he"])
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he", "config1", "config2"])
 @pytest.mark.parametrize("index", [0, 1])
 def test_source_matches_reference(case, index):
     rec, problem, ws = _workspace(case)
@@ -93,3 +93,19 @@ def test_adaptive_run_matches_reference(case):
     assert seen == len(zs)
     # decisions follow the reference's (rounding may move a borderline one)
     assert abs(batch.attempts - int(g["adaptive.counts"][0])) <= 3
+
+
+def test_full_size_steps_match_oracle():
+    """Config 2 at full size (n_to 16384, 64 nodes): three fixed Adams steps."""
+    from oracle import march as M
+
+    rec, problem, ws = _workspace("config2")
+    pol = policy(golden("config2"), "adaptive")
+    steps = np.full(3, 2e-5)
+    session = ws.start(pol, schedule=steps)
+    for _ in range(3):
+        session.advance(1)
+    ows = M.Workspace(rec)
+    march = M.AdamsMarch(M.AdamsEngine(ows, pol), pol, pol["proposal"])
+    march.replay(steps, np.concatenate([[0.0], np.cumsum(steps)]))
+    assert rel(session.export(), ows.state) < STEP_TOL
