@@ -177,6 +177,25 @@ sp_status sp_session_set_timing(sp_session* s, int enable);
  * clears them after reading. */
 sp_status sp_session_timing(sp_session* s, double* ms, int64_t* launches, int reset);
 
+/* One source evaluation that allocates no device memory, for callers that cannot call
+ * cudaMalloc: code whose device memory belongs to a pool or a framework that owns every
+ * allocation, or that runs where an allocation would synchronise the device or fail.
+ * It has no counterpart in the reference.  It computes what sp_workspace_source_device
+ * computes, from the host-side problem (sp_problem_create allocates host memory only),
+ * with lab and out device pointers (complex (n_modes, n_pol, n_omega)) on the caller's
+ * stream (NULL: the legacy default stream), and returns once the result is written.
+ *
+ * Every device buffer it uses -- the problem's tables, uploaded again on every call,
+ * and the evaluation's intermediates -- lies in one fixed array of 40 MiB inside the
+ * library, which every GPU that loads the library holds until the process exits; a
+ * problem needing more is refused with SP_ERR_ARGUMENT.  The first call on a device
+ * resolves that array's device address (cudaGetSymbolAddress) with the device current,
+ * so make the first call on each device before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU -- from several threads or streams at once -- race,
+ * so serialise them. */
+sp_status sp_source_noalloc(const sp_problem* problem, const void* lab, double z, int quiet,
+                            void* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

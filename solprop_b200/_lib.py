@@ -102,6 +102,8 @@ SIGNATURES = {
     "sp_workspace_stream": (C.c_void_p, [C.c_void_p]),
     "sp_session_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
     "sp_session_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]),
+    "sp_source_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p,
+                                    C.c_void_p]),
 }
 
 KERNEL_NAMES = ("adams_predict", "inverse_fft", "response_column", "project", "forward_fft",

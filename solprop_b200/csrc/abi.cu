@@ -110,6 +110,7 @@ template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  bool owned = true;
   void alloc(size_t count) {
     n = count;
     if (count) CUDA_CHECK(cudaMalloc(&p, count * sizeof(T)));
@@ -122,7 +123,7 @@ struct DevBuf {
     if (n) CUDA_CHECK(cudaMemsetAsync(p, 0, n * sizeof(T), s));
   }
   ~DevBuf() {
-    if (p) cudaFree(p);
+    if (p && owned) cudaFree(p);
   }
 };
 
@@ -1136,3 +1137,164 @@ sp_status sp_session_timing(sp_session* S, double* ms, int64_t* launches, int re
 }
 
 }  // extern "C"
+
+// ====================================================================== no-allocation entry
+// sp_source_noalloc: one source evaluation for callers that cannot allocate device
+// memory.  Every device buffer it needs -- the problem's tables and the evaluation's
+// intermediates -- is carved out of one file-scope array of kNoAllocBytes, which each
+// device that loads this library holds until the process exits.
+#include <mutex>
+
+namespace {
+
+constexpr size_t kNoAllocBytes = size_t(40) << 20;  // 40 MiB
+constexpr int kNoAllocDevices = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_base[kNoAllocDevices];       // device address, per device
+StageScalarsDev g_noalloc_stage[kNoAllocDevices][sp_workspace::kStageSlots];
+
+// Bump allocation over the array, 256-byte aligned; throws when the problem does not fit.
+struct Carver {
+  unsigned char* base;
+  size_t used = 0;
+  template <class T>
+  void take(DevBuf<T>& buf, size_t count) {
+    const size_t bytes = ((count * sizeof(T)) + 255) & ~size_t(255);
+    if (used + bytes > kNoAllocBytes) {
+      char msg[200];
+      std::snprintf(msg, sizeof msg,
+                    "the problem needs more than the %zu MiB the no-allocation entry point holds",
+                    kNoAllocBytes >> 20);
+      throw Failure(SP_ERR_ARGUMENT, msg);
+    }
+    buf.p = reinterpret_cast<T*>(base + used);
+    buf.n = count;
+    buf.owned = false;
+    used += bytes;
+  }
+};
+
+unsigned char* noalloc_base(int device) {
+  if (device < 0 || device >= kNoAllocDevices) throw Failure(SP_ERR_ARGUMENT, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_base[device]) {
+    // With the device current, resolve the array's device address once; host code
+    // cannot use the symbol's name as a device pointer.
+    void* ptr = nullptr;
+    CUDA_CHECK(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    g_noalloc_base[device] = static_cast<unsigned char*>(ptr);
+  }
+  return g_noalloc_base[device];
+}
+
+template <class T>
+void put(DevBuf<T>& buf, const void* host, size_t count, cudaStream_t s) {
+  if (count) CUDA_CHECK(cudaMemcpyAsync(buf.p, host, count * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+}  // namespace
+
+extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* lab, double z,
+                                       int quiet, void* out, void* stream_handle) {
+  return guarded([&] {
+    if (!problem || !lab || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    int device = 0;
+    CUDA_CHECK(cudaGetDevice(&device));
+    unsigned char* base = noalloc_base(device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream_handle);
+    const sp_problem& P = *problem;
+    const sp_problem_desc& d = P.d;
+    static std::mutex call_mutex;
+    std::lock_guard<std::mutex> lock(call_mutex);
+    // A view of the workspace whose buffers are regions of the array; it owns nothing.
+    static sp_workspace views[kNoAllocDevices];
+    sp_workspace& ws = views[device];
+    ws.P = problem;
+    ws.device = device;
+    ws.stream = s;
+    ws.h_stage = g_noalloc_stage[device];
+    ws.log_m = ilog2(d.n_to / 2);
+    ws.log_n_to = ilog2(d.n_to);
+    ws.launches = 5;
+    Carver carve{base};
+    const size_t n = P.n;
+    carve.take(ws.phi_terms, (size_t)d.n_phi_terms * n);
+    carve.take(ws.pre_terms, (size_t)d.n_prefactor_terms * n);
+    carve.take(ws.twiddles, (size_t)d.n_to / 2);
+    carve.take(ws.omega, d.n_omega);
+    carve.take(ws.omega_window, d.n_omega);
+    carve.take(ws.t_window, d.n_to);
+    carve.take(ws.t_window_d, d.n_to);
+    carve.take(ws.alpha, d.n_to);
+    carve.take(ws.synthesis, P.synthesis.size());
+    carve.take(ws.projection, P.projection.size());
+    carve.take(ws.rate_coeff, std::max<size_t>(P.rate_coeff.size(), 4));
+    carve.take(ws.taps, std::max<size_t>(P.taps.size(), 1));
+    carve.take(ws.crop, d.n_omega);
+    carve.take(ws.fine_to_coarse, (size_t)d.n_to / 2 + 1);
+    carve.take(ws.rows, (size_t)6 * P.n_cols);
+    carve.take(ws.active, d.n_omega);
+    carve.take(ws.norm, d.n_omega);
+    carve.take(ws.modal_t, (size_t)P.n_cols * d.n_to);
+    carve.take(ws.node_p, (size_t)d.n_nodes * d.n_to);
+    carve.take(ws.node_x, (size_t)d.n_nodes * d.n_to);
+    carve.take(ws.node_z, (size_t)d.n_nodes * d.n_to);
+    carve.take(ws.streams, (size_t)4 * P.n_cols * d.n_to);
+    carve.take(ws.spectra, (size_t)4 * n);
+    carve.take(ws.stage, sp_workspace::kStageSlots);
+    // the problem's tables, every call: the array keeps the last call's contents, which
+    // may be another problem's
+    put(ws.phi_terms, P.phi_terms.data(), (size_t)d.n_phi_terms * n, s);
+    put(ws.pre_terms, P.pre_terms.data(), (size_t)d.n_prefactor_terms * n, s);
+    std::vector<double2> tw(d.n_to / 2);
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int m = 0; m < d.n_to / 2; ++m) {
+      long double ang = two_pi * (long double)m / (long double)d.n_to;
+      tw[m] = make_double2((double)cosl(ang), (double)(-sinl(ang)));
+    }
+    put(ws.twiddles, tw.data(), tw.size(), s);
+    put(ws.omega, P.omega.data(), d.n_omega, s);
+    put(ws.omega_window, P.omega_window.data(), d.n_omega, s);
+    put(ws.t_window, P.t_window.data(), d.n_to, s);
+    put(ws.t_window_d, P.t_window_d.data(), d.n_to, s);
+    std::vector<double> alpha(d.n_to, 0.0);
+    if (d.absorber_in_stage) alpha = P.alpha;
+    put(ws.alpha, alpha.data(), d.n_to, s);
+    put(ws.synthesis, P.synthesis.data(), P.synthesis.size(), s);
+    put(ws.projection, P.projection.data(), P.projection.size(), s);
+    std::vector<double> rc = P.rate_coeff.empty() ? std::vector<double>(4, 0.0) : P.rate_coeff;
+    put(ws.rate_coeff, rc.data(), rc.size(), s);
+    std::vector<double> taps = P.taps.empty() ? std::vector<double>(1, 1.0) : P.taps;
+    put(ws.taps, taps.data(), taps.size(), s);
+    put(ws.crop, P.crop.data(), d.n_omega, s);
+    std::vector<int> f2c(d.n_to / 2 + 1, -1);
+    for (int j = 0; j < d.n_omega; ++j) f2c[P.crop[j]] = j;
+    put(ws.fine_to_coarse, f2c.data(), f2c.size(), s);
+    std::vector<int> rows;
+    for (int r = 0; r < 4 * P.n_cols; ++r) rows.push_back(r);
+    for (int r = 0; r < P.n_cols; ++r) rows.push_back(r);
+    for (int r = 0; r < P.n_cols; ++r) rows.push_back(3 * P.n_cols + r);
+    put(ws.rows, rows.data(), rows.size(), s);
+    put(ws.active, P.active.data(), d.n_omega, s);
+    put(ws.norm, P.norm.data(), d.n_omega, s);
+    // the buffers the allocating workspace starts at zero
+    ws.streams.zero(s);
+    ws.spectra.zero(s);
+    static bool configured[kNoAllocDevices];
+    if (!configured[device]) {
+      CUDA_CHECK(configure_source_kernels());
+      configured[device] = true;
+    }
+    fill_stage(&ws, 0, z, z);
+    upload_stages(&ws, 1);
+    eval_source(&ws, static_cast<const double2*>(lab), 0, nullptr, static_cast<double2*>(out),
+                quiet != 0);
+    // the host copies above read pageable buffers of this call; finish before they go
+    CUDA_CHECK(cudaStreamSynchronize(s));
+    ws.stream = nullptr;   // the view never owns the caller's stream
+    ws.h_stage = nullptr;  // nor the host scalars
+  });
+}
