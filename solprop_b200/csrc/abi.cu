@@ -139,6 +139,7 @@ int ilog2(int n) {
 struct sp_problem {
   sp_problem_desc d{};
   int n_cols = 0, n = 0, n_fine = 0;
+  int crop_identity = 0;  // crop_index[j] == j for every coarse bin
   std::vector<double> omega, omega_window, t_window, t_window_d, carrier, alpha;
   std::vector<long long> crop;
   std::vector<unsigned char> active, norm;
@@ -172,7 +173,8 @@ static void validate(const sp_problem_desc* d) {
     throw Failure(SP_ERR_REFUSED, "the analytic Kerr cubic belongs to the envelope grid");
   if (d->plasma_enabled) {
     need(d->rate_intervals >= 1 && d->rate_coefficients, "rate table");
-    need(d->n_taps >= 1 && d->n_taps <= kMaxTaps && d->taps, "running-integral taps");
+    need(d->n_taps >= 1 && d->n_taps - 1 <= kHalo && d->taps,
+         "running-integral taps: a band-rule half-width above 8 is not built");
   }
   if (d->absorber_in_stage) need(d->temporal_absorber_fine != nullptr, "absorber rate");
   for (int j = 0; j < d->n_omega; ++j) {
@@ -189,7 +191,7 @@ struct sp_workspace {
   int log_m = 0, log_n_to = 0, launches = 0, n_rows = 0;
   DevBuf<double2> phi_terms, pre_terms, twiddles, lab, out, spectra;
   DevBuf<double> omega, omega_window, t_window, t_window_d, alpha, synthesis, projection,
-      rate_coeff, taps, modal_t, node_p, node_x, node_z, streams;
+      rate_coeff, taps, modal_t, streams, sums0, offsets0, sums1, offsets1, proj;
   DevBuf<long long> crop;
   DevBuf<int> fine_to_coarse, rows;
   DevBuf<unsigned char> active, norm;
@@ -296,20 +298,26 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
   const bool absorber = d.absorber_in_stage && !quiet;
   InverseArgs ia{lab, ws->fine_to_coarse.p, ws->twiddles.p, ws->modal_t.p,
                  absorber ? ws->streams.p + (size_t)3 * P.n_cols * d.n_to : nullptr,
-                 ws->alpha.p, d.n_omega, d.n_to, ws->log_m, ws->log_n_to};
+                 ws->alpha.p, d.n_omega, d.n_to, ws->log_m, ws->log_n_to, P.crop_identity};
   { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
-  ColumnArgs ca{};
+  ColumnTileArgs ca{};
   ca.stage = ws->stage.p + slot;
   ca.modal_t = ws->modal_t.p;
   ca.synthesis = ws->synthesis.p;
+  ca.projection = ws->projection.p;
   ca.t_window = ws->t_window.p;
   ca.t_window_derivative = ws->t_window_d.p;
-  ca.node_p = ws->node_p.p;
-  ca.node_x = ws->node_x.p;
-  ca.node_z = ws->node_z.p;
+  ca.sums0 = ws->sums0.p;
+  ca.offsets0 = ws->offsets0.p;
+  ca.sums1 = ws->sums1.p;
+  ca.offsets1 = ws->offsets1.p;
+  ca.partials = ws->proj.p;
   ca.n_modes = d.n_modes;
   ca.n_nodes = d.n_nodes;
+  ca.n_cols = P.n_cols;
   ca.n_to = d.n_to;
+  ca.n_tiles = (d.n_to + kSeg - 1) / kSeg;
+  ca.n_groups = (d.n_nodes + kGroup - 1) / kGroup;
   ca.kerr = d.kerr_enabled;
   ca.plasma = d.plasma_enabled;
   ca.band = d.band;
@@ -326,18 +334,16 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
   ca.rate_max = d.rate_max;
   ca.rate_coefficients = ws->rate_coeff.p;
   ca.taps = ws->taps.p;
-  { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column(ca, ws->stream)); }
+  { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column_tiled(ca, ws->stream)); }
   const int n_streams = d.plasma_enabled ? 3 : 1;
-  ProjectArgs pa{ws->stage.p + slot, ws->node_p.p, ws->node_x.p, ws->node_z.p, ws->projection.p,
-                 ws->streams.p, d.n_nodes, d.n_modes, P.n_cols, d.n_to, n_streams};
-  { KernelTimer t(ws, SP_K_PROJECT); CUDA_CHECK(launch_project(pa, ws->stream)); }
   // stream rows: P [0, nc), gJ [nc, 2nc), g'J [2nc, 3nc), absorber [3nc, 4nc). The row
   // list holds [0, 4nc) for plasma runs and, at offset 4nc, [P rows, absorber rows].
   const int nc = P.n_cols;
   const int n_rows = (d.plasma_enabled ? 3 * nc : nc) + (absorber ? nc : 0);
-  ForwardArgs fa{ws->streams.p, d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
+  ForwardArgs fa{ws->streams.p, ws->proj.p, ca.n_groups, 3 * nc,
+                 d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
                  ws->crop.p, ws->twiddles.p, ws->spectra.p, d.n_to, d.n_omega, ws->log_m,
-                 ws->log_n_to};
+                 ws->log_n_to, P.crop_identity};
   { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, n_rows, ws->stream)); }
   OutputArgs oa{ws->stage.p + slot, ws->spectra.p, ws->pre_terms.p, ws->omega.p,
                 ws->omega_window.p, ws->active.p, inv_prop, out, P.n_cols, d.n_omega,
@@ -391,9 +397,14 @@ static void build_workspace(sp_workspace* ws) {
   ws->lab.alloc(n);
   ws->out.alloc(n);
   ws->modal_t.alloc((size_t)P.n_cols * d.n_to);
-  ws->node_p.alloc((size_t)d.n_nodes * d.n_to);
-  ws->node_x.alloc((size_t)d.n_nodes * d.n_to);
-  ws->node_z.alloc((size_t)d.n_nodes * d.n_to);
+  const size_t n_tiles = (d.n_to + kSeg - 1) / kSeg;
+  const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
+  ws->sums0.alloc((size_t)d.n_nodes * n_tiles);
+  ws->offsets0.alloc((size_t)d.n_nodes * n_tiles);
+  ws->sums1.alloc((size_t)d.n_nodes * n_tiles);
+  ws->offsets1.alloc((size_t)d.n_nodes * n_tiles);
+  ws->proj.alloc(n_groups * 3 * P.n_cols * d.n_to);
+  ws->proj.zero(s);
   ws->streams.alloc((size_t)4 * P.n_cols * d.n_to);
   ws->streams.zero(s);
   ws->spectra.alloc((size_t)4 * n);
@@ -909,6 +920,8 @@ sp_status sp_problem_create(const sp_problem_desc* d, sp_problem** out) {
     P->t_window_d.assign(d->t_window_derivative, d->t_window_derivative + d->n_to);
     if (d->absorber_in_stage) P->alpha.assign(d->temporal_absorber_fine, d->temporal_absorber_fine + d->n_to);
     P->crop.assign(d->crop_index, d->crop_index + d->n_omega);
+    P->crop_identity = 1;
+    for (int j = 0; j < d->n_omega; ++j) P->crop_identity &= (P->crop[j] == j);
     P->active.assign(d->active_mask, d->active_mask + d->n_omega);
     P->norm.assign(d->norm_mask, d->norm_mask + d->n_omega);
     P->phi_terms.assign(d->phi_terms, d->phi_terms + (size_t)2 * d->n_phi_terms * P->n);
@@ -1239,9 +1252,13 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     carve.take(ws.active, d.n_omega);
     carve.take(ws.norm, d.n_omega);
     carve.take(ws.modal_t, (size_t)P.n_cols * d.n_to);
-    carve.take(ws.node_p, (size_t)d.n_nodes * d.n_to);
-    carve.take(ws.node_x, (size_t)d.n_nodes * d.n_to);
-    carve.take(ws.node_z, (size_t)d.n_nodes * d.n_to);
+    const size_t n_tiles = (d.n_to + kSeg - 1) / kSeg;
+    const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
+    carve.take(ws.sums0, (size_t)d.n_nodes * n_tiles);
+    carve.take(ws.offsets0, (size_t)d.n_nodes * n_tiles);
+    carve.take(ws.sums1, (size_t)d.n_nodes * n_tiles);
+    carve.take(ws.offsets1, (size_t)d.n_nodes * n_tiles);
+    carve.take(ws.proj, n_groups * 3 * P.n_cols * d.n_to);
     carve.take(ws.streams, (size_t)4 * P.n_cols * d.n_to);
     carve.take(ws.spectra, (size_t)4 * n);
     carve.take(ws.stage, sp_workspace::kStageSlots);
@@ -1283,6 +1300,7 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     // the buffers the allocating workspace starts at zero
     ws.streams.zero(s);
     ws.spectra.zero(s);
+    ws.proj.zero(s);
     static bool configured[kNoAllocDevices];
     if (!configured[device]) {
       CUDA_CHECK(configure_source_kernels());

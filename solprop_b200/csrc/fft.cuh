@@ -23,7 +23,7 @@ __device__ __forceinline__ double2 twiddle(const double2* __restrict__ table, in
 }
 
 // In-place DIF FFT of s[0..n) by the whole block; n = 2^log_n <= n_table.
-__device__ void fft_dif_inplace(double2* s, int log_n, const double2* __restrict__ table,
+__device__ __noinline__ static void fft_dif_inplace(double2* s, int log_n, const double2* __restrict__ table,
                                 int log_table, bool inverse) {
   const int n = 1 << log_n;
   int log_len = log_n;

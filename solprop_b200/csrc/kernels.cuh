@@ -47,6 +47,7 @@ struct InverseArgs {
   double* absorber_stream;       // (n_cols, n_to) or null
   const double* alpha;           // (n_to)
   int n_omega, n_to, log_m, log_n_to;
+  int crop_identity;             // crop_index[j] == j for every coarse bin
 };
 
 struct ColumnArgs {
@@ -66,6 +67,34 @@ struct ColumnArgs {
   const double* taps;
 };
 
+// The tiled response column (column_kernels.cu): tiles of kSeg samples of kGroup nodes.
+constexpr int kSeg = 64;
+constexpr int kGroup = 16;
+constexpr int kHalo = 8;   // the largest band-rule half-width K the tiles carry
+
+struct ColumnTileArgs {
+  const StageScalarsDev* stage;
+  const double* modal_t;   // (n_modes, n_to)
+  const double* synthesis; // (n_nodes, n_modes)
+  const double* projection;// (n_modes, n_nodes)
+  const double* t_window;
+  const double* t_window_derivative;
+  double* sums0;           // (n_nodes, n_tiles) exposure tile sums
+  double* offsets0;
+  double* sums1;           // current tile sums
+  double* offsets1;
+  double* partials;        // (n_groups, 3, n_cols, n_to) projected streams per node group
+  int n_modes, n_nodes, n_cols, n_to, n_tiles, n_groups;
+  int kerr, plasma, band, half_width, rate_intervals;
+  double kerr_coefficient, charge_mass_ratio, ionisation_potential, dt;
+  double log_field_min, d_log_field, field_min, field_max, rate_max;
+  const double* rate_coefficients;
+  const double* taps;
+};
+
+cudaError_t launch_column_tiled(const ColumnTileArgs& a, cudaStream_t stream);
+cudaError_t configure_column_kernels();
+
 struct ProjectArgs {
   const StageScalarsDev* stage;
   const double* node_p;
@@ -78,11 +107,14 @@ struct ProjectArgs {
 
 struct ForwardArgs {
   const double* streams;       // rows of n_to
+  const double* partials;      // (n_groups, n_partial_rows, n_to): summed for rows below
+  int n_groups, n_partial_rows;
   const int* rows;             // which rows to transform
   const long long* crop_index; // (n_omega)
   const double2* twiddles;
   double2* spectra;            // rows of n_omega
   int n_to, n_omega, log_m, log_n_to;
+  int crop_identity;
 };
 
 struct OutputArgs {
@@ -98,6 +130,9 @@ struct OutputArgs {
 };
 
 cudaError_t configure_source_kernels();
+int fft_cluster_size(int n_to);
+cudaError_t launch_inverse_cluster(const InverseArgs& a, int n_cols, cudaStream_t stream);
+cudaError_t launch_forward_cluster(const ForwardArgs& a, int n_rows, cudaStream_t stream);
 cudaError_t launch_inverse(const InverseArgs& a, int n_cols, cudaStream_t stream);
 cudaError_t launch_column(const ColumnArgs& a, cudaStream_t stream);
 cudaError_t launch_project(const ProjectArgs& a, cudaStream_t stream);

@@ -26,7 +26,7 @@ namespace cg = cooperative_groups;
 namespace sp {
 
 // ----------------------------------------------------------------------------- K1
-__global__ void __launch_bounds__(512) k_inverse_field(InverseArgs a) {
+__global__ void __launch_bounds__(1024) k_inverse_field(InverseArgs a) {
   extern __shared__ double2 smem_c[];
   const int col = blockIdx.x;
   const int M = a.n_to >> 1;  // complex length
@@ -34,12 +34,20 @@ __global__ void __launch_bounds__(512) k_inverse_field(InverseArgs a) {
   const double2* tw = a.twiddles;
   // X[k] for k in [0, M]; pocketfft's irfft reads only the real part of the DC and
   // Nyquist bins, so those are taken real here too.
+  // the field grid's crop is the leading bins (crop_index[j] = j) unless told otherwise,
+  // so the fine spectrum is the coarse one padded: no index load on that path
   auto fine = [&](int k) -> double2 {
-    int j = a.fine_to_coarse[k];
-    double2 v = j >= 0 ? lab[j] : make_double2(0.0, 0.0);
+    double2 v;
+    if (a.crop_identity) {
+      v = k < a.n_omega ? lab[k] : make_double2(0.0, 0.0);
+    } else {
+      const int j = a.fine_to_coarse[k];
+      v = j >= 0 ? lab[j] : make_double2(0.0, 0.0);
+    }
     if (k == 0 || k == M) v.y = 0.0;
     return v;
   };
+#pragma unroll 4
   for (int k = threadIdx.x; k < M; k += blockDim.x) {
     double2 xk = fine(k), xm = cconj(fine(M - k));
     double2 e = cscale(0.5, cadd(xk, xm));
@@ -53,6 +61,7 @@ __global__ void __launch_bounds__(512) k_inverse_field(InverseArgs a) {
   const double inv_m = 1.0 / (double)M;
   double* row = a.modal_t + (size_t)col * a.n_to;
   double* absorb = a.absorber_stream ? a.absorber_stream + (size_t)col * a.n_to : nullptr;
+#pragma unroll 4
   for (int m = threadIdx.x; m < M; m += blockDim.x) {
     double2 z = smem_c[bitrev(m, a.log_m)];
     double x0 = z.x * inv_m, x1 = z.y * inv_m;
@@ -284,17 +293,33 @@ __global__ void __launch_bounds__(256) k_project(ProjectArgs a) {
 }
 
 // ----------------------------------------------------------------------------- K4
-__global__ void __launch_bounds__(512) k_forward_field(ForwardArgs a) {
+__global__ void __launch_bounds__(1024) k_forward_field(ForwardArgs a) {
   extern __shared__ double2 smem_c[];
   const int row = a.rows[blockIdx.x];
   const int M = a.n_to >> 1;
-  const double2* x = reinterpret_cast<const double2*>(a.streams + (size_t)row * a.n_to);
-  for (int m = threadIdx.x; m < M; m += blockDim.x) smem_c[m] = x[m];  // z = x_even + i x_odd
+  if (row < a.n_partial_rows) {
+    // a projected stream: the node groups' partial projections, summed in group order
+#pragma unroll 4
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int g = 0; g < a.n_groups; ++g) {
+        const double2 v = reinterpret_cast<const double2*>(
+            a.partials + ((size_t)g * a.n_partial_rows + row) * a.n_to)[m];
+        acc = cadd(acc, v);
+      }
+      smem_c[m] = acc;  // z = x_even + i x_odd
+    }
+  } else {
+    const double2* x = reinterpret_cast<const double2*>(a.streams + (size_t)row * a.n_to);
+#pragma unroll 4
+    for (int m = threadIdx.x; m < M; m += blockDim.x) smem_c[m] = x[m];
+  }
   __syncthreads();
   fft_dif_inplace(smem_c, a.log_m, a.twiddles, a.log_n_to, /*inverse=*/false);
   double2* out = a.spectra + (size_t)row * a.n_omega;
+#pragma unroll 4
   for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) {
-    const int k = (int)a.crop_index[j];
+    const int k = a.crop_identity ? j : (int)a.crop_index[j];
     const int km = (k == 0) ? 0 : M - k;
     double2 zk = smem_c[bitrev(k == M ? 0 : k, a.log_m)];
     double2 zm = cconj(smem_c[bitrev(km == M ? 0 : km, a.log_m)]);
@@ -374,9 +399,10 @@ cudaError_t launch_column(const ColumnArgs& a, cudaStream_t stream) {
   }
 }
 
-static int threads_for(int m) { return m >= 512 ? 512 : (m >= 32 ? m : 32); }
+static int threads_for(int m) { return m >= 1024 ? 1024 : (m >= 32 ? m : 32); }
 
 cudaError_t launch_inverse(const InverseArgs& a, int n_cols, cudaStream_t stream) {
+  if (fft_cluster_size(a.n_to) > 1) return launch_inverse_cluster(a, n_cols, stream);
   const int M = a.n_to >> 1;
   const size_t shm = (size_t)M * sizeof(double2);
   k_inverse_field<<<n_cols, threads_for(M), shm, stream>>>(a);
@@ -389,6 +415,7 @@ cudaError_t launch_project(const ProjectArgs& a, cudaStream_t stream) {
 }
 
 cudaError_t launch_forward(const ForwardArgs& a, int n_rows, cudaStream_t stream) {
+  if (fft_cluster_size(a.n_to) > 1) return launch_forward_cluster(a, n_rows, stream);
   const int M = a.n_to >> 1;
   const size_t shm = (size_t)M * sizeof(double2);
   k_forward_field<<<n_rows, threads_for(M), shm, stream>>>(a);
@@ -407,6 +434,8 @@ cudaError_t configure_source_kernels() {
   e = cudaFuncSetAttribute(k_inverse_field, cudaFuncAttributeMaxDynamicSharedMemorySize, max_shm);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_forward_field, cudaFuncAttributeMaxDynamicSharedMemorySize, max_shm);
+  if (e != cudaSuccess) return e;
+  e = configure_column_kernels();
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_column_field<1>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
