@@ -52,20 +52,26 @@ def load_workload():
 
 
 def algorithmic_bytes(rec) -> dict:
-    """Bytes each kernel family must move per launch (reads + writes of its operands)."""
+    """Bytes each kernel family must move per launch (reads + writes of its operands).
+
+    The column's three passes read the modal field each and write the projected partial
+    streams; nothing node-sized is stored.  The forward transform reads those partials.
+    """
     n = rec.n_cols * rec.n_omega
     c128, f64 = 16, 8
     nt, nn, nc = rec.n_to, rec.n_nodes, rec.n_cols
+    groups = -(-nn // 16)
+    tiles = nt // 64
     streams = 3 if rec.plasma_enabled else 1
     absorber = 1 if rec.absorber_scheme == "nonlinear" else 0
+    partials = groups * streams * nc * nt * f64
     return {
-        "adams_predict": (2 + 5) * n * c128 + 7 * n * c128,  # state, history read; lab, moments, flow, exp
-        "inverse_fft": n * c128 + (1 + absorber) * nc * nt * f64 + nt * f64,
-        "response_column": nc * nt * f64 + 2 * nt * f64 + streams * nn * nt * f64,
-        "project": streams * nn * nt * f64 + streams * nc * nt * f64,
-        "forward_fft": (streams + absorber) * nc * (nt * f64 + rec.n_omega * c128),
+        "adams_predict": 14 * n * c128,
+        "inverse_fft": n * c128 + (1 + absorber) * nc * nt * f64 + absorber * nt * f64,
+        "response_column": 3 * nc * nt * f64 + 2 * nt * f64 + 4 * nn * tiles * f64 + partials,
+        "forward_fft": partials + absorber * nc * nt * f64 + (streams + absorber) * n * c128,
         "stage_output": (streams + absorber) * n * c128 + rec.n_prefactor_terms * n * c128 + n * c128,
-        "adams_correct": (1 + 6 + 6 + 2) * n * c128,
+        "adams_correct": 15 * n * c128,
         "adams_accept": 4 * n * c128,
     }
 
