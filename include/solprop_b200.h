@@ -177,6 +177,27 @@ sp_status sp_session_set_timing(sp_session* s, int enable);
  * clears them after reading. */
 sp_status sp_session_timing(sp_session* s, double* ms, int64_t* launches, int reset);
 
+/* ---- scans: many independent runs stepped together ---- */
+/* The parameter-scan workload (solprop's run_scan, src/solprop/driver/scan.py:30, runs
+ * each point as its own process through an executor, driver/executors/*.py; the native
+ * backend has no batch, native SEP 36 follow-up).  Each batch step gives every
+ * unfinished run one exponential-Adams attempt with batched launches and one host
+ * decision pass; runs keep their own grids, mode counts, step sizes and orders. */
+typedef struct sp_scan sp_scan;
+typedef struct sp_scan_status {
+  int32_t active;                          /* runs not yet finished */
+  int64_t attempts, rejected, evaluations; /* summed over the runs */
+  int64_t batch_steps;
+} sp_scan_status;
+sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems,
+                         const sp_run_desc* runs, int device, sp_scan** out);
+/* Up to `steps` batch steps (fewer when every run has finished). */
+sp_status sp_scan_advance(sp_scan* scan, int32_t steps, sp_scan_status* out);
+/* One run's state (host complex, may be NULL) and counts (event 2: finished, 3: failed). */
+sp_status sp_scan_run(sp_scan* scan, int32_t run, double* state, sp_batch* info);
+void* sp_scan_stream(sp_scan* scan);
+sp_status sp_scan_destroy(sp_scan* scan);
+
 /* One source evaluation that allocates no device memory, for callers that cannot call
  * cudaMalloc: code whose device memory belongs to a pool or a framework that owns every
  * allocation, or that runs where an allocation would synchronise the device or fail.

@@ -176,7 +176,7 @@ class Workspace:
 
     def __init__(self, rec, state=None):
         self.rec = rec
-        self.state = np.array(rec.field0 if state is None else state, dtype=np.complex128)
+        self.state = np.array(rec.launch_field() if state is None else state, dtype=np.complex128)
         self.state = self.mask(self.state)
         self.evaluations = 0
 

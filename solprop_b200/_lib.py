@@ -82,6 +82,11 @@ class SpBatch(C.Structure):
                 ("attempts", C.c_int64), ("rejected", C.c_int64), ("evaluations", C.c_int64)]
 
 
+class SpScanStatus(C.Structure):
+    _fields_ = [("active", C.c_int32), ("attempts", C.c_int64), ("rejected", C.c_int64),
+                ("evaluations", C.c_int64), ("batch_steps", C.c_int64)]
+
+
 # the exported functions: name -> (restype, argtypes)
 SIGNATURES = {
     "sp_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
@@ -104,6 +109,12 @@ SIGNATURES = {
     "sp_session_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]),
     "sp_source_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p,
                                     C.c_void_p]),
+    "sp_scan_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(SpRunDesc), C.c_int,
+                                 C.POINTER(C.c_void_p)]),
+    "sp_scan_advance": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SpScanStatus)]),
+    "sp_scan_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(SpBatch)]),
+    "sp_scan_stream": (C.c_void_p, [C.c_void_p]),
+    "sp_scan_destroy": (C.c_int, [C.c_void_p]),
 }
 
 KERNEL_NAMES = ("adams_predict", "inverse_fft", "response_column", "project", "forward_fft",
@@ -264,7 +275,7 @@ def run_desc(rec, policy: dict, *, field0=None, schedule=None) -> tuple[SpRunDes
     r = SpRunDesc()
     adams = policy.get("march", "HostAdamsMarch") == "HostAdamsMarch"
     r.method = 0 if adams else 1
-    r.field0 = m.c128(rec.field0 if field0 is None else field0)
+    r.field0 = m.c128(rec.launch_field() if field0 is None else field0)
     r.z_start = 0.0
     r.proposal = float(policy["proposal"])
     control = policy.get("controller", policy)
@@ -403,6 +414,50 @@ class Session:
     def close(self):
         if getattr(self, "handle", None):
             library().sp_session_destroy(self.handle)
+            self.handle = None
+
+    __del__ = close
+
+
+class Scan:
+    """Many independent runs stepped together on one device (``sp_scan``)."""
+
+    def __init__(self, records, policies, device: int = 0):
+        self.handle = None
+        self.records = list(records)
+        self.problems = [Problem(r) for r in self.records]
+        descs, self._keep = [], []
+        for rec, pol in zip(self.records, policies):
+            d, k = run_desc(rec, pol)
+            descs.append(d)
+            self._keep.append(k)
+        n = len(descs)
+        handles = (C.c_void_p * n)(*[p.handle.value for p in self.problems])
+        runs = (SpRunDesc * n)(*descs)
+        handle = C.c_void_p()
+        check(library().sp_scan_create(n, handles, runs, device, C.byref(handle)))
+        self.handle = handle
+        self.status = SpScanStatus()
+
+    def advance(self, steps: int = 1) -> SpScanStatus:
+        check(library().sp_scan_advance(self.handle, int(steps), C.byref(self.status)))
+        return self.status
+
+    def run(self, index: int, state: bool = True):
+        rec = self.records[index]
+        info = SpBatch()
+        out = np.empty((rec.n_modes, rec.n_pol, rec.n_omega), dtype=np.complex128) if state else None
+        ptr = out.ctypes.data_as(C.POINTER(C.c_double)) if state else C.POINTER(C.c_double)()
+        check(library().sp_scan_run(self.handle, int(index), ptr, C.byref(info)))
+        return out, info
+
+    @property
+    def stream(self) -> int:
+        return int(library().sp_scan_stream(self.handle) or 0)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            library().sp_scan_destroy(self.handle)
             self.handle = None
 
     __del__ = close

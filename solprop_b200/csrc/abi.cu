@@ -290,18 +290,20 @@ static void upload_stages(sp_workspace* ws, int count) {
                              cudaMemcpyHostToDevice, ws->stream));
 }
 
-// One source evaluation at lab (device), stage slot, optional inverse propagator.
-static void eval_source(sp_workspace* ws, const double2* lab, int slot, const double2* inv_prop,
-                        double2* out, bool quiet) {
+// The argument records of one source evaluation on a workspace.
+static InverseArgs inverse_args(const sp_workspace* ws, const double2* lab, bool absorber) {
   const sp_problem& P = *ws->P;
   const sp_problem_desc& d = P.d;
-  const bool absorber = d.absorber_in_stage && !quiet;
-  InverseArgs ia{lab, ws->fine_to_coarse.p, ws->twiddles.p, ws->modal_t.p,
-                 absorber ? ws->streams.p + (size_t)3 * P.n_cols * d.n_to : nullptr,
-                 ws->alpha.p, d.n_omega, d.n_to, ws->log_m, ws->log_n_to, P.crop_identity};
-  { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
+  return InverseArgs{lab, ws->fine_to_coarse.p, ws->twiddles.p, ws->modal_t.p,
+                     absorber ? ws->streams.p + (size_t)3 * P.n_cols * d.n_to : nullptr,
+                     ws->alpha.p, d.n_omega, d.n_to, ws->log_m, ws->log_n_to, P.crop_identity};
+}
+
+static ColumnTileArgs column_args(const sp_workspace* ws, const StageScalarsDev* stage) {
+  const sp_problem& P = *ws->P;
+  const sp_problem_desc& d = P.d;
   ColumnTileArgs ca{};
-  ca.stage = ws->stage.p + slot;
+  ca.stage = stage;
   ca.modal_t = ws->modal_t.p;
   ca.synthesis = ws->synthesis.p;
   ca.projection = ws->projection.p;
@@ -334,20 +336,46 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
   ca.rate_max = d.rate_max;
   ca.rate_coefficients = ws->rate_coeff.p;
   ca.taps = ws->taps.p;
-  { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column_tiled(ca, ws->stream)); }
-  const int n_streams = d.plasma_enabled ? 3 : 1;
-  // stream rows: P [0, nc), gJ [nc, 2nc), g'J [2nc, 3nc), absorber [3nc, 4nc). The row
-  // list holds [0, 4nc) for plasma runs and, at offset 4nc, [P rows, absorber rows].
+  return ca;
+}
+
+// stream rows: P [0, nc), gJ [nc, 2nc), g'J [2nc, 3nc), absorber [3nc, 4nc). The row
+// list holds [0, 4nc) for plasma runs and, at offset 4nc, [P rows, absorber rows].
+static int forward_rows(const sp_workspace* ws, bool absorber) {
+  const sp_problem& P = *ws->P;
+  return (P.d.plasma_enabled ? 3 * P.n_cols : P.n_cols) + (absorber ? P.n_cols : 0);
+}
+
+static ForwardArgs forward_args(const sp_workspace* ws) {
+  const sp_problem& P = *ws->P;
+  const sp_problem_desc& d = P.d;
   const int nc = P.n_cols;
-  const int n_rows = (d.plasma_enabled ? 3 * nc : nc) + (absorber ? nc : 0);
-  ForwardArgs fa{ws->streams.p, ws->proj.p, ca.n_groups, 3 * nc,
-                 d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
-                 ws->crop.p, ws->twiddles.p, ws->spectra.p, d.n_to, d.n_omega, ws->log_m,
-                 ws->log_n_to, P.crop_identity};
-  { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, n_rows, ws->stream)); }
-  OutputArgs oa{ws->stage.p + slot, ws->spectra.p, ws->pre_terms.p, ws->omega.p,
-                ws->omega_window.p, ws->active.p, inv_prop, out, P.n_cols, d.n_omega,
-                d.plasma_enabled, absorber};
+  return ForwardArgs{ws->streams.p, ws->proj.p, (d.n_nodes + kGroup - 1) / kGroup, 3 * nc,
+                     d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
+                     ws->crop.p, ws->twiddles.p, ws->spectra.p, d.n_to, d.n_omega, ws->log_m,
+                     ws->log_n_to, P.crop_identity};
+}
+
+static OutputArgs output_args(const sp_workspace* ws, const StageScalarsDev* stage,
+                              const double2* inv_prop, double2* out, bool absorber) {
+  const sp_problem& P = *ws->P;
+  return OutputArgs{stage, ws->spectra.p, ws->pre_terms.p, ws->omega.p, ws->omega_window.p,
+                    ws->active.p, inv_prop, out, P.n_cols, P.d.n_omega, P.d.plasma_enabled,
+                    absorber};
+}
+
+// One source evaluation at lab (device), stage slot, optional inverse propagator.
+static void eval_source(sp_workspace* ws, const double2* lab, int slot, const double2* inv_prop,
+                        double2* out, bool quiet) {
+  const sp_problem& P = *ws->P;
+  const bool absorber = P.d.absorber_in_stage && !quiet;
+  const InverseArgs ia = inverse_args(ws, lab, absorber);
+  { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
+  const ColumnTileArgs ca = column_args(ws, ws->stage.p + slot);
+  { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column_tiled(ca, ws->stream)); }
+  const ForwardArgs fa = forward_args(ws);
+  { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
+  const OutputArgs oa = output_args(ws, ws->stage.p + slot, inv_prop, out, absorber);
   { KernelTimer t(ws, SP_K_OUTPUT); CUDA_CHECK(launch_output(oa, ws->stream)); }
 }
 
@@ -511,6 +539,7 @@ static void adams_start(sp_session* S) {
   a.states = comp ? ws->states.p : nullptr;
   a.rates = comp ? ws->rates.p : nullptr;
   a.source = ws->src.p;
+  a.n_blocks = kNormBlocks;
   { KernelTimer t(ws, SP_K_START); CUDA_CHECK(launch_adams_start(a, ws->stream)); }
   S->evaluations += 1;
   S->history.assign(1, {S->z, 0});
@@ -528,12 +557,26 @@ static double limit_step(double dz, double factor, double dz_min, double dz_max)
   return proposed;
 }
 
-// One Adams attempt; returns accepted.
-static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool fixed) {
+// One Adams attempt, split in three so that a batch of runs can share the launches:
+// prepare (stencil, tables and stage scalars into the workspace's pinned records),
+// the launches, and decide (the host's acceptance, order and step choice).
+struct Pending {
+  double dz = 0, end = 0;
+  bool kink = false, fixed = false;
+  int order = 1, free_slot = 0;
+  std::vector<int> orders;
+};
+
+static Pending prepare_attempt(sp_session* S, double dz, double end, bool kink, bool fixed) {
   sp_workspace* ws = S->ws;
   const sp_problem& P = *ws->P;
   const sp_run_desc& R = S->run;
   const bool comp = P.d.phi_expansion;
+  Pending pd;
+  pd.dz = dz;
+  pd.end = end;
+  pd.kink = kink;
+  pd.fixed = fixed;
   // stencil (adams_core.py:150-206)
   std::vector<double> nodes;
   std::vector<int> slots;
@@ -549,6 +592,23 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
     for (int o : {order - 1, order + 1})
       if (o >= 1 && o <= R.order && o <= held && (o < order || rising)) orders.push_back(o);
   }
+  pd.order = order;
+  pd.orders = orders;
+  // the row an accepted step writes: the first not kept (marches/adams.py:593-596)
+  {
+    std::vector<std::pair<double, int>> keep;
+    if (R.order) {
+      size_t from = S->history.size() > (size_t)R.order ? S->history.size() - R.order : 0;
+      keep.assign(S->history.begin() + from, S->history.end());
+    }
+    int free_slot = 0;
+    for (;; ++free_slot) {
+      bool used = false;
+      for (auto& e : keep) used |= e.second == free_slot;
+      if (!used) break;
+    }
+    pd.free_slot = free_slot;
+  }
   int width = 1 + *std::max_element(orders.begin(), orders.end());
   AdamsDev& ad = *ws->h_adams;
   std::memset(&ad, 0, sizeof(ad));
@@ -559,6 +619,7 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
   ad.width = width;
   ad.n_orders = (int)orders.size();
   ad.compensated = comp;
+  ad.free_slot = pd.free_slot;
   for (int j = 0; j < width - 1 && j < held; ++j) {
     ad.slots[j] = slots[j];
     ad.nodes[j] = nodes[j];
@@ -601,11 +662,85 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
   }
   fill_stage(ws, 0, S->z, S->z + dz);        // the step's exponent
   fill_stage(ws, 1, S->z + dz, S->z + dz);   // the source at the predicted field
-  upload_stages(ws, 2);
-  CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, &ad, sizeof(AdamsDev), cudaMemcpyHostToDevice, ws->stream));
+  return pd;
+}
+
+// The host's decision on a trial from its four reduced sums (defect norms squared in
+// the orders' order, then the state's squared norm); returns whether it was accepted.
+static bool decide_attempt(sp_session* S, const Pending& pd, const double* sums) {
+  const sp_run_desc& R = S->run;
+  S->attempts += 1;
+  S->evaluations += 1;
+  const double magnitude = std::sqrt(sums[kMaxOrders]);
+  const double scale = R.rtol * magnitude + R.atol;
+  std::vector<double> norms(pd.orders.size());
+  for (size_t r = 0; r < pd.orders.size(); ++r) norms[r] = std::sqrt(sums[r]) / scale;
+  const double norm = norms[0];
+  const int order = pd.order;
+  const double dz = pd.dz;
+  auto factor = [&](double nm, int o, double growth) {
+    if (nm <= 0.0) return growth;
+    double raw = R.safety * std::pow(nm, -1.0 / (o + 1));
+    return std::min(growth, std::max(R.min_factor, raw));
+  };
+  if (!(norm <= 1.0) && !(pd.fixed && std::isfinite(norm))) {
+    S->rejected += 1;
+    S->last_rejected = true;
+    int count = S->rejections + 1;
+    bool restart = count >= R.restart_after && S->history.size() > 1;
+    double sc = !std::isfinite(norm) ? R.min_factor : factor(norm, order, R.rejection_growth);
+    S->rejections = restart ? 0 : count;
+    if (restart) S->history.clear();
+    S->proposal = limit_step(dz, sc, R.dz_min, R.dz_max);
+    return false;
+  }
+  std::vector<std::pair<double, int>> keep;
+  if (R.order) {
+    size_t from = S->history.size() > (size_t)R.order ? S->history.size() - R.order : 0;
+    keep.assign(S->history.begin() + from, S->history.end());
+  }
+  keep.push_back({S->z + dz, pd.free_slot});
+  S->history = keep;
+  S->rejections = 0;
+  // order choice (adams_core.py:256-301)
+  int stored = order, control = order;
+  double cnorm = norm;
+  if (!R.variable_order) {
+    stored = R.order;
+  } else {
+    auto weight = [&](double nm, int o) {
+      double rate = nm <= 0.0 ? INFINITY : std::pow(nm, -1.0 / (o + 1));
+      double allowed = R.safety * rate;
+      double stable = INFINITY;
+      if (R.collar_rate > 0.0)
+        stable = R.collar_stability * R.real_intervals[o - 1] / (R.collar_rate * dz);
+      return std::min(allowed, stable);
+    };
+    int best = pd.orders[0];
+    double bw = weight(norms[0], pd.orders[0]);
+    for (size_t r = 1; r < pd.orders.size(); ++r) {
+      double w = weight(norms[r], pd.orders[r]);
+      if (w > bw) { bw = w; best = pd.orders[r]; }
+    }
+    if (best != order && bw > R.hysteresis * weight(norms[0], order)) {
+      stored = control = best;
+      for (size_t r = 0; r < pd.orders.size(); ++r) if (pd.orders[r] == best) cnorm = norms[r];
+    }
+  }
+  S->order = stored;
+  S->last_rejected = false;
+  S->z = pd.end;
+  if (pd.kink) S->history.clear();
+  S->proposal = limit_step(dz, factor(cnorm, control, R.max_growth), R.dz_min, R.dz_max);
+  return true;
+}
+
+static StepArgs step_args_of(sp_workspace* ws, const AdamsDev* adams_dev, const StageScalarsDev* stage0) {
+  const sp_problem& P = *ws->P;
+  const bool comp = P.d.phi_expansion;
   StepArgs a{};
-  a.stage = ws->stage.p;
-  a.adams = ws->adams.p;
+  a.stage = stage0;
+  a.adams = adams_dev;
   a.phi_terms = ws->phi_terms.p;
   a.norm_mask = ws->norm.p;
   a.active_mask = ws->active.p;
@@ -624,6 +759,17 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
   a.advanced = ws->adv.p;
   a.partials = ws->partials.p;
   a.norms = ws->norms.p;
+  a.n_blocks = kNormBlocks;
+  return a;
+}
+
+// One Adams attempt of a single run; returns accepted.
+static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool fixed) {
+  sp_workspace* ws = S->ws;
+  Pending pd = prepare_attempt(S, dz, end, kink, fixed);
+  upload_stages(ws, 2);
+  CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, ws->h_adams, sizeof(AdamsDev), cudaMemcpyHostToDevice, ws->stream));
+  StepArgs a = step_args_of(ws, ws->adams.p, ws->stage.p);
   { KernelTimer t(ws, SP_K_PREDICT); CUDA_CHECK(launch_adams_predict(a, ws->stream)); }
   eval_source(ws, ws->lab.p, 1, nullptr, ws->src.p, false);
   { KernelTimer t(ws, SP_K_CORRECT); CUDA_CHECK(launch_adams_correct(a, ws->stream)); }
@@ -631,77 +777,18 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
                              cudaMemcpyDeviceToHost, ws->stream));
   CUDA_CHECK(cudaStreamSynchronize(ws->stream));
   ws->flush_timing();
-  S->attempts += 1;
-  S->evaluations += 1;
-  const double magnitude = std::sqrt(ws->h_norms[kMaxOrders]);
-  const double scale = R.rtol * magnitude + R.atol;
-  std::vector<double> norms(orders.size());
-  for (size_t r = 0; r < orders.size(); ++r) norms[r] = std::sqrt(ws->h_norms[r]) / scale;
-  const double norm = norms[0];
-  auto factor = [&](double nm, int o, double growth) {
-    if (nm <= 0.0) return growth;
-    double raw = R.safety * std::pow(nm, -1.0 / (o + 1));
-    return std::min(growth, std::max(R.min_factor, raw));
-  };
-  if (!(norm <= 1.0) && !(fixed && std::isfinite(norm))) {
-    S->rejected += 1;
-    S->last_rejected = true;
-    int count = S->rejections + 1;
-    bool restart = count >= R.restart_after && S->history.size() > 1;
-    double sc = !std::isfinite(norm) ? R.min_factor : factor(norm, order, R.rejection_growth);
-    S->rejections = restart ? 0 : count;
-    if (restart) S->history.clear();
-    S->proposal = limit_step(dz, sc, R.dz_min, R.dz_max);
-    return false;
+  const bool accepted = decide_attempt(S, pd, ws->h_norms);
+  if (accepted) {
+    KernelTimer t(ws, SP_K_ACCEPT);
+    CUDA_CHECK(launch_adams_accept(a, pd.free_slot, nullptr, ws->stream));
   }
-  // accept: the new sample takes the oldest row past the method's need
-  std::vector<std::pair<double, int>> keep;
-  if (R.order) {
-    size_t from = S->history.size() > (size_t)R.order ? S->history.size() - R.order : 0;
-    keep.assign(S->history.begin() + from, S->history.end());
-  }
-  int free_slot = 0;
-  for (;; ++free_slot) {
-    bool used = false;
-    for (auto& e : keep) used |= e.second == free_slot;
-    if (!used) break;
-  }
-  { KernelTimer t(ws, SP_K_ACCEPT); CUDA_CHECK(launch_adams_accept(a, free_slot, nullptr, ws->stream)); }
-  keep.push_back({S->z + dz, free_slot});
-  S->history = keep;
-  S->rejections = 0;
-  // order choice (adams_core.py:256-301)
-  int stored = order, control = order;
-  double cnorm = norm;
-  if (!R.variable_order) {
-    stored = R.order;
-  } else {
-    auto weight = [&](double nm, int o) {
-      double rate = nm <= 0.0 ? INFINITY : std::pow(nm, -1.0 / (o + 1));
-      double allowed = R.safety * rate;
-      double stable = INFINITY;
-      if (R.collar_rate > 0.0)
-        stable = R.collar_stability * R.real_intervals[o - 1] / (R.collar_rate * dz);
-      return std::min(allowed, stable);
-    };
-    int best = orders[0];
-    double bw = weight(norms[0], orders[0]);
-    for (size_t r = 1; r < orders.size(); ++r) {
-      double w = weight(norms[r], orders[r]);
-      if (w > bw) { bw = w; best = orders[r]; }
-    }
-    if (best != order && bw > R.hysteresis * weight(norms[0], order)) {
-      stored = control = best;
-      for (size_t r = 0; r < orders.size(); ++r) if (orders[r] == best) cnorm = norms[r];
-    }
-  }
-  S->order = stored;
-  S->last_rejected = false;
-  S->z = end;
-  if (kink) S->history.clear();
-  S->proposal = limit_step(dz, factor(cnorm, control, R.max_growth), R.dz_min, R.dz_max);
-  return true;
+  return accepted;
 }
+
+// The attempt an adaptive march takes next: the landing rule and the equal approach
+// (adams_core.py:401-470); returns (dz, end, kink).
+struct Next { double dz, end; bool kink; };
+static Next adams_next(const sp_session* S, double target);
 
 // stepper/schedule.py:959-1066
 struct Stop { double dz; int kind; double target; bool landed; };
@@ -734,12 +821,10 @@ static Stop landing(const sp_session* S, double z, double dz, double z_end) {
   return {cap.dz, cap.kind, 0.0, false};
 }
 
-static void adams_adaptive_attempt(sp_session* S, double target) {
+static Next adams_next(const sp_session* S, double target) {
   const sp_run_desc& R = S->run;
-  if (S->history.empty()) adams_start(S);
   Stop stop = landing(S, S->z, S->proposal, target);
-  double dz = stop.dz, end;
-  bool kink = false;
+  double dz = stop.dz;
   if (!stop.landed && R.equal_approach) {
     const double tol = kLandingUlps * ulp(std::max(std::fabs(S->z), std::fabs(target)));
     double nearest = target;
@@ -749,17 +834,21 @@ static void adams_adaptive_attempt(sp_session* S, double target) {
     }
     if (nearest > S->z + tol && dz < nearest - S->z && nearest - S->z < 2.0 * dz) {
       double half = 0.5 * (nearest - S->z);
-      adams_attempt(S, half, S->z + half, false, false);
-      return;
+      return {half, S->z + half, false};
     }
   }
-  end = stop.landed ? stop.target : S->z + dz;
+  const double end = stop.landed ? stop.target : S->z + dz;
   const double tol = kLandingUlps * ulp(std::max(std::fabs(end), 1.0));
   const bool interior = end < R.z_end - tol;
   bool on_kink = false;
   if (interior) for (double k : S->kinks) on_kink |= std::fabs(k - end) <= tol;
-  kink = stop.kind == 3 || on_kink;
-  adams_attempt(S, dz, end, kink, false);
+  return {dz, end, stop.kind == 3 || on_kink};
+}
+
+static void adams_adaptive_attempt(sp_session* S, double target) {
+  if (S->history.empty()) adams_start(S);
+  const Next nx = adams_next(S, target);
+  adams_attempt(S, nx.dz, nx.end, nx.kink, false);
 }
 
 // ---- DOPRI5 (backends/numpy_ref/engines.py:97-181)
@@ -1147,6 +1236,354 @@ sp_status sp_session_timing(sp_session* S, double* ms, int64_t* launches, int re
       }
     }
   });
+}
+
+}  // extern "C"
+
+// ====================================================================== scans
+// sp_scan: many independent runs stepped together.  Every batch step gives each
+// unfinished run one exponential-Adams attempt: one staging upload of all runs' tables
+// and flags, the batched launches (predict, inverse FFT per grid size, the three column
+// passes, forward FFT per grid size, stage output, correct and its reductions), one
+// read-back of all runs' norms, the host's decisions, and a batched accept.
+namespace {
+
+struct FftClass {
+  int n_to = 0;
+  bool cluster = false;
+  DevBuf<int2> inv_items, fwd_items;
+  int n_inv = 0, n_fwd = 0;
+};
+
+template <class T>
+T* pinned(size_t n) {
+  T* p = nullptr;
+  CUDA_CHECK(cudaMallocHost(&p, sizeof(T) * std::max<size_t>(n, 1)));
+  std::memset(p, 0, sizeof(T) * std::max<size_t>(n, 1));
+  return p;
+}
+
+}  // namespace
+
+struct sp_scan {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int R = 0;
+  std::vector<std::unique_ptr<sp_workspace>> ws;
+  std::vector<std::unique_ptr<sp_session>> ss;
+  std::vector<int> done;
+  std::vector<Pending> pending;
+  DevBuf<InverseArgs> inv_start, inv_att;
+  DevBuf<ColumnTileArgs> col_start, col_att;
+  DevBuf<ForwardArgs> fwd;
+  DevBuf<OutputArgs> out_start, out_att;
+  DevBuf<StepArgs> step_start, step_att;
+  DevBuf<AdamsDev> adams_start, adams_att;
+  DevBuf<StageScalarsDev> stages_start, stages_att;
+  DevBuf<double> norms;
+  DevBuf<int> flag_start, flag_att, flag_accept;
+  DevBuf<int2> step_items, out_items;
+  DevBuf<int4> col_items;
+  int n_step_items = 0, n_out_items = 0, n_col_items = 0;
+  std::vector<std::unique_ptr<FftClass>> classes;
+  AdamsDev *h_adams_start = nullptr, *h_adams_att = nullptr;
+  StageScalarsDev *h_stages_start = nullptr, *h_stages_att = nullptr;
+  double* h_norms = nullptr;
+  int *h_flag_start = nullptr, *h_flag_att = nullptr, *h_flag_accept = nullptr;
+  int64_t batch_steps = 0;
+  ~sp_scan() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (void* p : {(void*)h_adams_start, (void*)h_adams_att, (void*)h_stages_start,
+                    (void*)h_stages_att, (void*)h_norms, (void*)h_flag_start, (void*)h_flag_att,
+                    (void*)h_flag_accept})
+      if (p) cudaFreeHost(p);
+    ss.clear();
+    ws.clear();
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+template <class T>
+void upload_all(DevBuf<T>& dev, const T* host, size_t n, cudaStream_t s) {
+  CUDA_CHECK(cudaMemcpyAsync(dev.p, host, n * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+void scan_source(sp_scan* S, bool start) {
+  const DevBuf<int>& flags = start ? S->flag_start : S->flag_att;
+  const DevBuf<InverseArgs>& inv = start ? S->inv_start : S->inv_att;
+  const DevBuf<ColumnTileArgs>& col = start ? S->col_start : S->col_att;
+  const DevBuf<OutputArgs>& out = start ? S->out_start : S->out_att;
+  for (auto& c : S->classes) {
+    if (c->cluster)
+      CUDA_CHECK(launch_inverse_cluster_b(inv.p, c->inv_items.p, flags.p, c->n_inv, c->n_to, S->stream));
+    else
+      CUDA_CHECK(launch_inverse_b(inv.p, c->inv_items.p, flags.p, c->n_inv, c->n_to, S->stream));
+  }
+  for (int pass = 0; pass < 3; ++pass)
+    CUDA_CHECK(launch_column_tiled_b(col.p, S->col_items.p, flags.p, S->n_col_items, pass, S->stream));
+  for (auto& c : S->classes) {
+    if (c->cluster)
+      CUDA_CHECK(launch_forward_cluster_b(S->fwd.p, c->fwd_items.p, flags.p, c->n_fwd, c->n_to, S->stream));
+    else
+      CUDA_CHECK(launch_forward_b(S->fwd.p, c->fwd_items.p, flags.p, c->n_fwd, c->n_to, S->stream));
+  }
+  CUDA_CHECK(launch_output_b(out.p, S->out_items.p, flags.p, S->n_out_items, S->stream));
+}
+
+void scan_step(sp_scan* S) {
+  const int R = S->R;
+  // phase A: runs with an empty history take their startup sample
+  int n_start = 0;
+  for (int r = 0; r < R; ++r) {
+    S->h_flag_start[r] = 0;
+    if (S->done[r]) continue;
+    sp_session* ss = S->ss[r].get();
+    if (!ss->history.empty()) continue;
+    sp_workspace* w = S->ws[r].get();
+    fill_stage(w, 2, ss->z, ss->z);
+    S->h_stages_start[r] = w->h_stage[2];
+    std::memset(&S->h_adams_start[r], 0, sizeof(AdamsDev));
+    if (w->P->d.phi_expansion) w->P->phi_rate.eval(ss->z, S->h_adams_start[r].rate0_w);
+    S->h_flag_start[r] = 1;
+    ++n_start;
+  }
+  if (n_start) {
+    upload_all(S->flag_start, S->h_flag_start, R, S->stream);
+    upload_all(S->stages_start, S->h_stages_start, R, S->stream);
+    upload_all(S->adams_start, S->h_adams_start, R, S->stream);
+    scan_source(S, true);
+    CUDA_CHECK(launch_step_b(3, S->step_start.p, S->step_items.p, S->flag_start.p, S->n_step_items, R, S->stream));
+    for (int r = 0; r < R; ++r) {
+      if (!S->h_flag_start[r]) continue;
+      sp_session* ss = S->ss[r].get();
+      ss->evaluations += 1;
+      ss->history.assign(1, {ss->z, 0});
+      ss->order = ss->run.variable_order ? 1 : ss->run.order;
+    }
+  }
+  // phase B: one attempt for every unfinished run
+  int n_att = 0;
+  for (int r = 0; r < R; ++r) {
+    S->h_flag_att[r] = 0;
+    if (S->done[r]) continue;
+    sp_session* ss = S->ss[r].get();
+    sp_workspace* w = S->ws[r].get();
+    const Next nx = adams_next(ss, ss->run.z_end);
+    S->pending[r] = prepare_attempt(ss, nx.dz, nx.end, nx.kink, false);
+    S->h_adams_att[r] = *w->h_adams;
+    S->h_stages_att[2 * r] = w->h_stage[0];
+    S->h_stages_att[2 * r + 1] = w->h_stage[1];
+    S->h_flag_att[r] = 1;
+    ++n_att;
+  }
+  if (!n_att) return;
+  upload_all(S->flag_att, S->h_flag_att, R, S->stream);
+  upload_all(S->stages_att, S->h_stages_att, 2 * (size_t)R, S->stream);
+  upload_all(S->adams_att, S->h_adams_att, R, S->stream);
+  CUDA_CHECK(launch_step_b(0, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
+  scan_source(S, false);
+  CUDA_CHECK(launch_step_b(1, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
+  CUDA_CHECK(cudaMemcpyAsync(S->h_norms, S->norms.p, sizeof(double) * 8 * R, cudaMemcpyDeviceToHost,
+                             S->stream));
+  CUDA_CHECK(cudaStreamSynchronize(S->stream));
+  for (int r = 0; r < R; ++r) {
+    S->h_flag_accept[r] = 0;
+    if (!S->h_flag_att[r]) continue;
+    sp_session* ss = S->ss[r].get();
+    try {
+      S->h_flag_accept[r] = decide_attempt(ss, S->pending[r], S->h_norms + 8 * r) ? 1 : 0;
+    } catch (const Failure&) {
+      ss->failed = true;  // below dz_min: this run stops; the others go on
+      S->done[r] = 1;
+      continue;
+    }
+  }
+  upload_all(S->flag_accept, S->h_flag_accept, R, S->stream);
+  CUDA_CHECK(launch_step_b(2, S->step_att.p, S->step_items.p, S->flag_accept.p, S->n_step_items, R, S->stream));
+  for (int r = 0; r < R; ++r) {
+    sp_session* ss = S->ss[r].get();
+    if (!S->done[r] && reached(ss->z, ss->run.z_end)) {
+      ss->finished = true;
+      S->done[r] = 1;
+    }
+  }
+  S->batch_steps += 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, const sp_run_desc* runs,
+                         int device, sp_scan** out) {
+  return guarded([&] {
+    if (n_runs < 1 || !problems || !runs || !out) throw Failure(SP_ERR_ARGUMENT, "bad scan arguments");
+    CUDA_CHECK(cudaSetDevice(device));
+    static bool configured = false;
+    if (!configured) {
+      CUDA_CHECK(configure_source_kernels());
+      configured = true;
+    }
+    auto S = std::make_unique<sp_scan>();
+    S->device = device;
+    S->R = n_runs;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    const int R = n_runs;
+    for (int r = 0; r < R; ++r) {
+      if (runs[r].method != 0 || runs[r].schedule)
+        throw Failure(SP_ERR_REFUSED, "a scan steps adaptive exponential-Adams runs only");
+      if (problems[r]->d.phi_expansion)
+        throw Failure(SP_ERR_REFUSED, "a scan run with a varying operator (Phi expansion)");
+      auto w = std::make_unique<sp_workspace>();
+      w->P = problems[r];
+      w->device = device;
+      CUDA_CHECK(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+      build_workspace(w.get());
+      sp_session* raw = nullptr;
+      sp_status st = sp_session_start(w.get(), &runs[r], &raw);
+      if (st != SP_OK) throw Failure(st, g_error);
+      S->ss.emplace_back(raw);
+      S->ws.push_back(std::move(w));
+    }
+    S->done.assign(R, 0);
+    S->pending.resize(R);
+    S->h_adams_start = pinned<AdamsDev>(R);
+    S->h_adams_att = pinned<AdamsDev>(R);
+    S->h_stages_start = pinned<StageScalarsDev>(R);
+    S->h_stages_att = pinned<StageScalarsDev>(2 * (size_t)R);
+    S->h_norms = pinned<double>(8 * (size_t)R);
+    S->h_flag_start = pinned<int>(R);
+    S->h_flag_att = pinned<int>(R);
+    S->h_flag_accept = pinned<int>(R);
+    S->adams_start.alloc(R);
+    S->adams_att.alloc(R);
+    S->stages_start.alloc(R);
+    S->stages_att.alloc(2 * (size_t)R);
+    S->norms.alloc(8 * (size_t)R);
+    S->flag_start.alloc(R);
+    S->flag_att.alloc(R);
+    S->flag_accept.alloc(R);
+    // per-run argument records and the static work tables
+    std::vector<InverseArgs> is(R), ia(R);
+    std::vector<ColumnTileArgs> cs(R), ca(R);
+    std::vector<ForwardArgs> fa(R);
+    std::vector<OutputArgs> os(R), oa(R);
+    std::vector<StepArgs> ts(R), ta(R);
+    std::vector<int2> step_items, out_items;
+    std::vector<int4> col_items;
+    std::vector<int> sizes;
+    for (int r = 0; r < R; ++r) {
+      sp_workspace* w = S->ws[r].get();
+      const sp_problem& P = *w->P;
+      const bool absorber = P.d.absorber_in_stage != 0;
+      is[r] = inverse_args(w, w->state.p, absorber);
+      ia[r] = inverse_args(w, w->lab.p, absorber);
+      cs[r] = column_args(w, S->stages_start.p + r);
+      ca[r] = column_args(w, S->stages_att.p + 2 * r + 1);
+      fa[r] = forward_args(w);
+      os[r] = output_args(w, S->stages_start.p + r, nullptr, w->src.p, absorber);
+      oa[r] = output_args(w, S->stages_att.p + 2 * r + 1, nullptr, w->src.p, absorber);
+      const int nb = std::min(kNormBlocks, (P.n + 255) / 256);
+      ts[r] = step_args_of(w, S->adams_start.p + r, S->stages_start.p + r);
+      ta[r] = step_args_of(w, S->adams_att.p + r, S->stages_att.p + 2 * r);
+      ts[r].n_blocks = ta[r].n_blocks = nb;
+      ts[r].norms = ta[r].norms = S->norms.p + 8 * r;
+      for (int b = 0; b < nb; ++b) step_items.push_back(make_int2(r, b));
+      const int no = (P.n + 255) / 256;
+      for (int b = 0; b < no; ++b) out_items.push_back(make_int2(r, b));
+      for (int t = 0; t < cs[r].n_tiles; ++t)
+        for (int g = 0; g < cs[r].n_groups; ++g) col_items.push_back(make_int4(r, t, g, 0));
+      if (std::find(sizes.begin(), sizes.end(), P.d.n_to) == sizes.end()) sizes.push_back(P.d.n_to);
+    }
+    std::sort(sizes.begin(), sizes.end());
+    for (int n_to : sizes) {
+      auto c = std::make_unique<FftClass>();
+      c->n_to = n_to;
+      c->cluster = fft_cluster_size(n_to) > 1;
+      std::vector<int2> inv, fwd;
+      for (int r = 0; r < R; ++r) {
+        sp_workspace* w = S->ws[r].get();
+        if (w->P->d.n_to != n_to) continue;
+        for (int col = 0; col < w->P->n_cols; ++col) inv.push_back(make_int2(r, col));
+        const int rows = forward_rows(w, w->P->d.absorber_in_stage != 0);
+        for (int row = 0; row < rows; ++row) fwd.push_back(make_int2(r, row));
+      }
+      c->n_inv = (int)inv.size();
+      c->n_fwd = (int)fwd.size();
+      c->inv_items.upload(inv.data(), inv.size(), S->stream);
+      c->fwd_items.upload(fwd.data(), fwd.size(), S->stream);
+      S->classes.push_back(std::move(c));
+    }
+    S->inv_start.upload(is.data(), R, S->stream);
+    S->inv_att.upload(ia.data(), R, S->stream);
+    S->col_start.upload(cs.data(), R, S->stream);
+    S->col_att.upload(ca.data(), R, S->stream);
+    S->fwd.upload(fa.data(), R, S->stream);
+    S->out_start.upload(os.data(), R, S->stream);
+    S->out_att.upload(oa.data(), R, S->stream);
+    S->step_start.upload(ts.data(), R, S->stream);
+    S->step_att.upload(ta.data(), R, S->stream);
+    S->step_items.upload(step_items.data(), step_items.size(), S->stream);
+    S->out_items.upload(out_items.data(), out_items.size(), S->stream);
+    S->col_items.upload(col_items.data(), col_items.size(), S->stream);
+    S->n_step_items = (int)step_items.size();
+    S->n_out_items = (int)out_items.size();
+    S->n_col_items = (int)col_items.size();
+    CUDA_CHECK(cudaStreamSynchronize(S->stream));
+    *out = S.release();
+  });
+}
+
+sp_status sp_scan_advance(sp_scan* S, int32_t steps, sp_scan_status* out) {
+  return guarded([&] {
+    if (!S || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    CUDA_CHECK(cudaSetDevice(S->device));
+    for (int i = 0; i < steps; ++i) {
+      bool any = false;
+      for (int d : S->done) any |= !d;
+      if (!any) break;
+      scan_step(S);
+    }
+    out->active = 0;
+    out->attempts = out->rejected = out->evaluations = 0;
+    for (int r = 0; r < S->R; ++r) {
+      out->active += !S->done[r];
+      out->attempts += S->ss[r]->attempts;
+      out->rejected += S->ss[r]->rejected;
+      out->evaluations += S->ss[r]->evaluations;
+    }
+    out->batch_steps = S->batch_steps;
+  });
+}
+
+sp_status sp_scan_run(sp_scan* S, int32_t run, double* state, sp_batch* info) {
+  return guarded([&] {
+    if (!S || run < 0 || run >= S->R) throw Failure(SP_ERR_ARGUMENT, "run index out of range");
+    CUDA_CHECK(cudaSetDevice(S->device));
+    CUDA_CHECK(cudaStreamSynchronize(S->stream));
+    sp_session* ss = S->ss[run].get();
+    if (state) {
+      const size_t bytes = (size_t)S->ws[run]->P->n * sizeof(double2);
+      CUDA_CHECK(cudaMemcpy(state, S->ws[run]->state.p, bytes, cudaMemcpyDeviceToHost));
+    }
+    if (info) {
+      info->event = ss->failed ? 3 : (ss->finished ? 2 : 0);
+      info->plane_index = -1;
+      info->z = ss->z;
+      info->attempts = ss->attempts;
+      info->rejected = ss->rejected;
+      info->evaluations = ss->evaluations;
+    }
+  });
+}
+
+void* sp_scan_stream(sp_scan* S) { return S ? (void*)S->stream : nullptr; }
+
+sp_status sp_scan_destroy(sp_scan* S) {
+  delete S;
+  return SP_OK;
 }
 
 }  // extern "C"

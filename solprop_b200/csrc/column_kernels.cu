@@ -38,11 +38,11 @@ struct Tile {
   int node, lane;  // this thread's node within the group (thread / kLanes) and lane
 };
 
-__device__ __forceinline__ Tile tile_of(const ColumnTileArgs& a) {
+__device__ __forceinline__ Tile tile_of(const ColumnTileArgs& a, int tile, int group) {
   Tile c;
-  c.tile = blockIdx.x;
-  c.t0 = blockIdx.x * kSeg;
-  c.n0 = blockIdx.y * kGroup;
+  c.tile = tile;
+  c.t0 = tile * kSeg;
+  c.n0 = group * kGroup;
   c.nodes = min(kGroup, a.n_nodes - c.n0);
   c.node = threadIdx.x / kLanes;
   c.lane = threadIdx.x % kLanes;
@@ -239,13 +239,13 @@ __device__ void rescan(const Tile& c, const double* inc, double* out, double off
 }  // namespace
 
 // pass 0: the exposure's tile sums
-__global__ void __launch_bounds__(kThreads) k_column_pass0(ColumnTileArgs a) {
+__device__ __forceinline__ void pass0_body(const ColumnTileArgs& a, int tile, int group) {
   extern __shared__ double dyn0[];
   double* E = dyn0;
   double* W = E + kGroup * kLen;
   double* T = W + kGroup * kLen;
   double* modal = T + kGroup * kLen;
-  const Tile c = tile_of(a);
+  const Tile c = tile_of(a, tile, group);
   // W~ on [t0, t1] needs W on [t0 - H, t1 + H]
   field_and_rate(a, c, modal, E, W, kI0 - kHalo, kI0 + kSeg + kHalo + 1, true);
   increments(a, c, W, T, E, c.t0, c.t0 + kSeg);
@@ -253,14 +253,14 @@ __global__ void __launch_bounds__(kThreads) k_column_pass0(ColumnTileArgs a) {
 }
 
 // pass 1: the exposure rescanned, the fraction, the current's tile sums
-__global__ void __launch_bounds__(kThreads) k_column_pass1(ColumnTileArgs a) {
+__device__ __forceinline__ void pass1_body(const ColumnTileArgs& a, int tile, int group) {
   extern __shared__ double dyn1[];
   double* E = dyn1;
   double* W = E + kGroup * kLen;
   double* T = W + kGroup * kLen;
   double* S = T + kGroup * kLen;
   double* modal = S + kGroup * kLen;
-  const Tile c = tile_of(a);
+  const Tile c = tile_of(a, tile, group);
   const double off0 = predecessors(c, a.sums0, a.n_tiles);
   if (c.lane == 0 && c.node < c.nodes) a.offsets0[(size_t)(c.n0 + c.node) * a.n_tiles + c.tile] = off0;
   field_and_rate(a, c, modal, E, W, 0, kLen, true);
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kThreads) k_column_pass1(ColumnTileArgs a) {
 }
 
 // pass 2: both rescans, the total current, Kerr, the collar and the projection
-__global__ void __launch_bounds__(kThreads) k_column_pass2(ColumnTileArgs a) {
+__device__ __forceinline__ void pass2_body(const ColumnTileArgs& a, int tile, int group) {
   extern __shared__ double dyn2[];
   double* E = dyn2;
   double* W = E + kGroup * kLen;
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(kThreads) k_column_pass2(ColumnTileArgs a) {
   double* Y1 = F + kGroup * kLen;  // integrand -> increments
   double* Y2 = Y1 + kGroup * kLen; // filtered scratch -> running integral
   double* modal = Y2 + kGroup * kLen;
-  const Tile c = tile_of(a);
+  const Tile c = tile_of(a, tile, group);
   const bool plasma = a.plasma;
   double off1 = 0.0, off0 = 0.0;
   if (plasma) {
@@ -384,8 +384,45 @@ __global__ void __launch_bounds__(kThreads) k_column_pass2(ColumnTileArgs a) {
     const double* row = rows[s];
     double acc = 0.0;
     for (int n = 0; n < c.nodes; ++n) acc += wt[m * kGroup + n] * row[n * kSeg + q];
-    a.partials[(((size_t)blockIdx.y * 3 + s) * a.n_cols + m) * a.n_to + t] = acc;
+    a.partials[(((size_t)group * 3 + s) * a.n_cols + m) * a.n_to + t] = acc;
   }
+}
+
+__global__ void __launch_bounds__(kThreads) k_column_pass0(ColumnTileArgs a) {
+  pass0_body(a, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(kThreads) k_column_pass1(ColumnTileArgs a) {
+  pass1_body(a, blockIdx.x, blockIdx.y);
+}
+__global__ void __launch_bounds__(kThreads) k_column_pass2(ColumnTileArgs a) {
+  pass2_body(a, blockIdx.x, blockIdx.y);
+}
+// batched: items[blockIdx.x] = (run, tile, group, -)
+__global__ void __launch_bounds__(kThreads) k_column_pass0_b(const ColumnTileArgs* args, const int4* items,
+                                                                const int* flags) {
+  const int4 it = items[blockIdx.x];
+  if (!flags[it.x]) return;
+  pass0_body(args[it.x], it.y, it.z);
+}
+__global__ void __launch_bounds__(kThreads) k_column_pass1_b(const ColumnTileArgs* args, const int4* items,
+                                                                const int* flags) {
+  const int4 it = items[blockIdx.x];
+  if (!flags[it.x]) return;
+  pass1_body(args[it.x], it.y, it.z);
+}
+__global__ void __launch_bounds__(kThreads) k_column_pass2_b(const ColumnTileArgs* args, const int4* items,
+                                                                const int* flags) {
+  const int4 it = items[blockIdx.x];
+  if (!flags[it.x]) return;
+  pass2_body(args[it.x], it.y, it.z);
+}
+
+cudaError_t launch_column_tiled_b(const ColumnTileArgs* args, const int4* items, const int* flags,
+                                  int n_items, int pass, cudaStream_t stream) {
+  if (pass == 0) k_column_pass0_b<<<n_items, kThreads, kPass0Smem, stream>>>(args, items, flags);
+  else if (pass == 1) k_column_pass1_b<<<n_items, kThreads, kPass1Smem, stream>>>(args, items, flags);
+  else k_column_pass2_b<<<n_items, kThreads, kPass2Smem, stream>>>(args, items, flags);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_column_tiled(const ColumnTileArgs& a, cudaStream_t stream) {
@@ -399,13 +436,16 @@ cudaError_t launch_column_tiled(const ColumnTileArgs& a, cudaStream_t stream) {
 }
 
 cudaError_t configure_column_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(k_column_pass0, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kPass0Smem);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_column_pass1, cudaFuncAttributeMaxDynamicSharedMemorySize, kPass1Smem);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_column_pass2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              kPass2Smem);
+  const void* kernels[6] = {(const void*)k_column_pass0, (const void*)k_column_pass1,
+                            (const void*)k_column_pass2, (const void*)k_column_pass0_b,
+                            (const void*)k_column_pass1_b, (const void*)k_column_pass2_b};
+  const size_t shm[6] = {kPass0Smem, kPass1Smem, kPass2Smem, kPass0Smem, kPass1Smem, kPass2Smem};
+  for (int i = 0; i < 6; ++i) {
+    cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)shm[i]);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace sp

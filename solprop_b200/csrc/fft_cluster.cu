@@ -66,11 +66,10 @@ __device__ __forceinline__ void cross_dft(cg::cluster_group& cluster, double2* s
 }  // namespace
 
 // inverse (c2r): coarse spectrum -> modal field (and the absorber's stream)
-__global__ void __launch_bounds__(512) k_inverse_cluster(InverseArgs a) {
+__device__ __forceinline__ void inverse_cluster_body(const InverseArgs& a, int col) {
   cg::cluster_group cluster = cg::this_cluster();
   const int C = (int)cluster.num_blocks();
   const int r = (int)cluster.block_rank();
-  const int col = blockIdx.y;
   extern __shared__ double2 sc[];
   const int M = a.n_to >> 1;
   const int Mp = M / C;
@@ -124,12 +123,24 @@ __global__ void __launch_bounds__(512) k_inverse_cluster(InverseArgs a) {
   cluster.sync();  // no CTA leaves while another reads its shared memory
 }
 
+__global__ void __launch_bounds__(512) k_inverse_cluster(InverseArgs a) {
+  inverse_cluster_body(a, blockIdx.y);
+}
+
+// batched: items[blockIdx.y] = (run, column)
+__global__ void __launch_bounds__(512) k_inverse_cluster_b(const InverseArgs* args, const int2* items,
+                                                          const int* flags) {
+  const int2 it = items[blockIdx.y];
+  if (!flags[it.x]) return;  // uniform over the cluster: every CTA of it has this item
+  inverse_cluster_body(args[it.x], it.y);
+}
+
 // forward (r2c): stream rows -> cropped coarse spectra
-__global__ void __launch_bounds__(512) k_forward_cluster(ForwardArgs a) {
+__device__ __forceinline__ void forward_cluster_body(const ForwardArgs& a, int row_index) {
   cg::cluster_group cluster = cg::this_cluster();
   const int C = (int)cluster.num_blocks();
   const int r = (int)cluster.block_rank();
-  const int row = a.rows[blockIdx.y];
+  const int row = a.rows[row_index];
   extern __shared__ double2 sc[];
   const int M = a.n_to >> 1;
   const int Mp = M / C;
@@ -184,6 +195,18 @@ __global__ void __launch_bounds__(512) k_forward_cluster(ForwardArgs a) {
   cluster.sync();
 }
 
+__global__ void __launch_bounds__(512) k_forward_cluster(ForwardArgs a) {
+  forward_cluster_body(a, blockIdx.y);
+}
+
+// batched: items[blockIdx.y] = (run, row index)
+__global__ void __launch_bounds__(512) k_forward_cluster_b(const ForwardArgs* args, const int2* items,
+                                                          const int* flags) {
+  const int2 it = items[blockIdx.y];
+  if (!flags[it.x]) return;
+  forward_cluster_body(args[it.x], it.y);
+}
+
 static cudaError_t launch_cluster(const void* kernel, dim3 grid, int threads, size_t shm, int C,
                                   cudaStream_t stream, void** args) {
   cudaLaunchConfig_t cfg = {};
@@ -223,6 +246,37 @@ cudaError_t launch_forward_cluster(const ForwardArgs& a, int n_rows, cudaStream_
   void* args[] = {&copy};
   return launch_cluster((const void*)k_forward_cluster, dim3(C, n_rows), Mp >= 512 ? 512 : Mp,
                         (size_t)2 * Mp * sizeof(double2), C, stream, args);
+}
+
+cudaError_t launch_inverse_cluster_b(const InverseArgs* args, const int2* items, const int* flags,
+                                     int n_items, int n_to, cudaStream_t stream) {
+  const int C = fft_cluster_size(n_to);
+  const int Mp = (n_to / 2) / C;
+  void* params[] = {(void*)&args, (void*)&items, (void*)&flags};
+  return launch_cluster((const void*)k_inverse_cluster_b, dim3(C, n_items), Mp >= 512 ? 512 : Mp,
+                        (size_t)Mp * sizeof(double2), C, stream, params);
+}
+
+cudaError_t launch_forward_cluster_b(const ForwardArgs* args, const int2* items, const int* flags,
+                                     int n_items, int n_to, cudaStream_t stream) {
+  const int C = fft_cluster_size(n_to);
+  const int Mp = (n_to / 2) / C;
+  void* params[] = {(void*)&args, (void*)&items, (void*)&flags};
+  return launch_cluster((const void*)k_forward_cluster_b, dim3(C, n_items), Mp >= 512 ? 512 : Mp,
+                        (size_t)2 * Mp * sizeof(double2), C, stream, params);
+}
+
+cudaError_t configure_cluster_fft() {
+  // rows of up to 2^15 real samples: 2048 complex points per CTA, two buffers forward
+  const int shm = 2 * 2048 * (int)sizeof(double2);
+  cudaError_t e;
+  e = cudaFuncSetAttribute(k_inverse_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_forward_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_inverse_cluster_b, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_forward_cluster_b, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
 }
 
 }  // namespace sp

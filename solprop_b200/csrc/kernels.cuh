@@ -35,6 +35,7 @@ struct AdamsDev {
   double comp_corr[kMaxOrders][kMaxWidth + 1];    // [0] endpoint, then carried rows
   double comp_pred_main[kMaxWidth];
   double comp_corr_main[kMaxWidth + 1];
+  int free_slot;               // the history row an accepted step writes
   double rate_w[kMaxTerms];   // D(z + dz) weights (the endpoint rate, "before")
   double rate0_w[kMaxTerms];  // D(z) weights (startup)
 };
@@ -48,23 +49,6 @@ struct InverseArgs {
   const double* alpha;           // (n_to)
   int n_omega, n_to, log_m, log_n_to;
   int crop_identity;             // crop_index[j] == j for every coarse bin
-};
-
-struct ColumnArgs {
-  const StageScalarsDev* stage;
-  const double* modal_t;   // (n_modes, n_to)
-  const double* synthesis; // (n_nodes, n_modes)
-  const double* t_window;
-  const double* t_window_derivative;
-  double* node_p;          // (n_nodes, n_to)
-  double* node_x;
-  double* node_z;
-  int n_modes, n_nodes, n_to;
-  int kerr, plasma, band, half_width, rate_intervals;
-  double kerr_coefficient, charge_mass_ratio, ionisation_potential, dt;
-  double log_field_min, d_log_field, field_min, field_max, rate_max;
-  const double* rate_coefficients;
-  const double* taps;
 };
 
 // The tiled response column (column_kernels.cu): tiles of kSeg samples of kGroup nodes.
@@ -95,16 +79,6 @@ struct ColumnTileArgs {
 cudaError_t launch_column_tiled(const ColumnTileArgs& a, cudaStream_t stream);
 cudaError_t configure_column_kernels();
 
-struct ProjectArgs {
-  const StageScalarsDev* stage;
-  const double* node_p;
-  const double* node_x;
-  const double* node_z;
-  const double* projection;  // (n_modes, n_nodes)
-  double* streams;           // (n_stream_rows, n_cols, n_to)
-  int n_nodes, n_modes, n_cols, n_to, n_streams;
-};
-
 struct ForwardArgs {
   const double* streams;       // rows of n_to
   const double* partials;      // (n_groups, n_partial_rows, n_to): summed for rows below
@@ -134,10 +108,24 @@ int fft_cluster_size(int n_to);
 cudaError_t launch_inverse_cluster(const InverseArgs& a, int n_cols, cudaStream_t stream);
 cudaError_t launch_forward_cluster(const ForwardArgs& a, int n_rows, cudaStream_t stream);
 cudaError_t launch_inverse(const InverseArgs& a, int n_cols, cudaStream_t stream);
-cudaError_t launch_column(const ColumnArgs& a, cudaStream_t stream);
-cudaError_t launch_project(const ProjectArgs& a, cudaStream_t stream);
 cudaError_t launch_forward(const ForwardArgs& a, int n_rows, cudaStream_t stream);
 cudaError_t launch_output(const OutputArgs& a, cudaStream_t stream);
+
+// ---- batched launches over several runs: items map each block to (run, index)
+cudaError_t configure_cluster_fft();
+// flags[run] != 0 selects the runs a launch serves; other items return at once
+cudaError_t launch_inverse_b(const InverseArgs* args, const int2* items, const int* flags,
+                             int n_items, int n_to, cudaStream_t stream);
+cudaError_t launch_forward_b(const ForwardArgs* args, const int2* items, const int* flags,
+                             int n_items, int n_to, cudaStream_t stream);
+cudaError_t launch_inverse_cluster_b(const InverseArgs* args, const int2* items, const int* flags,
+                                     int n_items, int n_to, cudaStream_t stream);
+cudaError_t launch_forward_cluster_b(const ForwardArgs* args, const int2* items, const int* flags,
+                                     int n_items, int n_to, cudaStream_t stream);
+cudaError_t launch_output_b(const OutputArgs* args, const int2* items, const int* flags,
+                            int n_items, cudaStream_t stream);
+cudaError_t launch_column_tiled_b(const ColumnTileArgs* args, const int4* items, const int* flags,
+                                  int n_items, int pass, cudaStream_t stream);
 
 // ---- stepping kernels (step_kernels.cu)
 struct StepArgs {
@@ -160,12 +148,16 @@ struct StepArgs {
   double2* advanced;          // (n)
   double* partials;           // (kMaxOrders + 2, kNormBlocks)
   double* norms;              // (kMaxOrders + 2)
+  int n_blocks;               // blocks of the grid-stride loops (<= kNormBlocks)
 };
 
 cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t stream);
 cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t stream);
 cudaError_t launch_adams_accept(const StepArgs& a, int free_slot, double2* rate_out, cudaStream_t s);
 cudaError_t launch_adams_start(const StepArgs& a, cudaStream_t stream);
+// batched step kernels: which = 0 predict, 1 correct (+ reduction), 2 accept, 3 start
+cudaError_t launch_step_b(int which, const StepArgs* args, const int2* items, const int* flags,
+                          int n_items, int n_runs, cudaStream_t stream);
 
 struct RkArgs {
   const StageScalarsDev* stage;

@@ -70,7 +70,7 @@ __device__ __forceinline__ double2 combine_terms(const double* w, int n_terms,
 
 // sum of n_q values per thread into partials[q][blockIdx.x]; deterministic order
 template <int NQ>
-__device__ void block_partials(double (&v)[NQ], double* partials) {
+__device__ void block_partials(double (&v)[NQ], double* partials, int block) {
   __shared__ double red[NQ][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -86,28 +86,39 @@ __device__ void block_partials(double (&v)[NQ], double* partials) {
     for (int q = 0; q < NQ; ++q) {
       double x = lane < nw ? red[q][lane] : 0.0;
       for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
-      if (lane == 0) partials[q * kNormBlocks + blockIdx.x] = x;
+      if (lane == 0) partials[q * kNormBlocks + block] = x;
     }
   }
 }
 
-__global__ void k_reduce(const double* partials, double* out, int nq) {
-  // one block of 32 threads per quantity; fixed order
-  const int q = blockIdx.x;
-  if (q >= nq) return;
+__device__ __forceinline__ void reduce_body(const double* partials, double* out, int q, int nb) {
+  // one warp per quantity; fixed order
   double x = 0.0;
-  for (int b = threadIdx.x; b < kNormBlocks; b += 32) x += partials[q * kNormBlocks + b];
+  for (int b = threadIdx.x; b < nb; b += 32) x += partials[q * kNormBlocks + b];
   for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
   if (threadIdx.x == 0) out[q] = x;
 }
 
+__global__ void k_reduce(const double* partials, double* out, int nq, int nb) {
+  if ((int)blockIdx.x >= nq) return;
+  reduce_body(partials, out, blockIdx.x, nb);
+}
+
+// batched: one block per (quantity, run); runs[blockIdx.y]
+__global__ void k_reduce_b(const StepArgs* args, const int* flags, int nq) {
+  if (!flags[blockIdx.y]) return;
+  const StepArgs& a = args[blockIdx.y];
+  if ((int)blockIdx.x >= nq) return;
+  reduce_body(a.partials, a.norms, blockIdx.x, a.n_blocks);
+}
+
 // ------------------------------------------------------------------ Adams predict
-__global__ void __launch_bounds__(256) k_adams_predict(StepArgs a) {
+__device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block) {
   const AdamsDev& ad = *a.adams;
   const StageScalarsDev& st = *a.stage;
   const int width = ad.width, order = ad.order;
   double v[1] = {0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+  for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
     const double2 x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
     double2 phi[kMaxWidth + 1];
     phi_functions(x, width, phi);
@@ -150,15 +161,15 @@ __global__ void __launch_bounds__(256) k_adams_predict(StepArgs a) {
     const int bin = i % a.n_omega;
     if (a.norm_mask[bin]) v[0] += y.x * y.x + y.y * y.y;
   }
-  block_partials<1>(v, a.partials + (size_t)kMaxOrders * kNormBlocks);
+  block_partials<1>(v, a.partials + (size_t)kMaxOrders * kNormBlocks, block);
 }
 
 // ------------------------------------------------------------------ Adams correct
-__global__ void __launch_bounds__(256) k_adams_correct(StepArgs a) {
+__device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block) {
   const AdamsDev& ad = *a.adams;
   const int width = ad.width, n_orders = ad.n_orders;
   double v[kMaxOrders] = {0.0, 0.0, 0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+  for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
     double2 xs[kMaxWidth];
     xs[0] = a.source[i];
     for (int j = 1; j < width; ++j) xs[j] = a.store[(size_t)ad.slots[j - 1] * a.n + i];
@@ -218,12 +229,13 @@ __global__ void __launch_bounds__(256) k_adams_correct(StepArgs a) {
       if (scored) v[r] += d.x * d.x + d.y * d.y;
     }
   }
-  block_partials<kMaxOrders>(v, a.partials);
+  block_partials<kMaxOrders>(v, a.partials, block);
 }
 
-__global__ void k_adams_accept(StepArgs a, int free_slot, int write_rate) {
+__device__ __forceinline__ void adams_accept_body(const StepArgs& a, int free_slot, int write_rate,
+                                                  int block) {
   const AdamsDev& ad = *a.adams;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+  for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
     const int bin = i % a.n_omega;
     const double2 adv = a.advanced[i];
     a.state[i] = a.active_mask[bin] ? adv : make_double2(adv.x * 0.0, adv.y * 0.0);
@@ -238,9 +250,9 @@ __global__ void k_adams_accept(StepArgs a, int free_slot, int write_rate) {
   }
 }
 
-__global__ void k_adams_start(StepArgs a, int write_rate) {
+__device__ __forceinline__ void adams_start_body(const StepArgs& a, int write_rate, int block) {
   const AdamsDev& ad = *a.adams;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+  for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
     a.store[i] = a.source[i];
     if (write_rate) {
       a.states[i] = a.state[i];
@@ -252,21 +264,69 @@ __global__ void k_adams_start(StepArgs a, int write_rate) {
   }
 }
 
+__global__ void __launch_bounds__(256) k_adams_predict(StepArgs a) { adams_predict_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(256) k_adams_correct(StepArgs a) { adams_correct_body(a, blockIdx.x); }
+__global__ void k_adams_accept(StepArgs a, int free_slot, int write_rate) {
+  adams_accept_body(a, free_slot, write_rate, blockIdx.x);
+}
+__global__ void k_adams_start(StepArgs a, int write_rate) { adams_start_body(a, write_rate, blockIdx.x); }
+
+// batched: items[blockIdx.x] = (run, block of that run)
+__global__ void __launch_bounds__(256) k_adams_predict_b(const StepArgs* args, const int2* items,
+                                                        const int* flags) {
+  const int2 it = items[blockIdx.x];
+  if (!flags[it.x]) return;
+  adams_predict_body(args[it.x], it.y);
+}
+__global__ void __launch_bounds__(256) k_adams_correct_b(const StepArgs* args, const int2* items,
+                                                        const int* flags) {
+  const int2 it = items[blockIdx.x];
+  if (!flags[it.x]) return;
+  adams_correct_body(args[it.x], it.y);
+}
+__global__ void k_adams_accept_b(const StepArgs* args, const int2* items, const int* flags) {
+  const int2 it = items[blockIdx.x];
+  if (!flags[it.x]) return;
+  const StepArgs& a = args[it.x];
+  adams_accept_body(a, a.adams->free_slot, a.states != nullptr, it.y);
+}
+__global__ void k_adams_start_b(const StepArgs* args, const int2* items, const int* flags) {
+  const int2 it = items[blockIdx.x];
+  if (!flags[it.x]) return;
+  const StepArgs& a = args[it.x];
+  adams_start_body(a, a.states != nullptr, it.y);
+}
+
 cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t s) {
-  k_adams_predict<<<kNormBlocks, 256, 0, s>>>(a);
+  k_adams_predict<<<a.n_blocks, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t s) {
-  k_adams_correct<<<kNormBlocks, 256, 0, s>>>(a);
-  k_reduce<<<kMaxOrders + 1, 32, 0, s>>>(a.partials, a.norms, kMaxOrders + 1);
+  k_adams_correct<<<a.n_blocks, 256, 0, s>>>(a);
+  k_reduce<<<kMaxOrders + 1, 32, 0, s>>>(a.partials, a.norms, kMaxOrders + 1, a.n_blocks);
   return cudaGetLastError();
 }
 cudaError_t launch_adams_accept(const StepArgs& a, int free_slot, double2*, cudaStream_t s) {
-  k_adams_accept<<<kNormBlocks, 256, 0, s>>>(a, free_slot, a.states != nullptr);
+  k_adams_accept<<<a.n_blocks, 256, 0, s>>>(a, free_slot, a.states != nullptr);
   return cudaGetLastError();
 }
 cudaError_t launch_adams_start(const StepArgs& a, cudaStream_t s) {
-  k_adams_start<<<kNormBlocks, 256, 0, s>>>(a, a.states != nullptr);
+  k_adams_start<<<a.n_blocks, 256, 0, s>>>(a, a.states != nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step_b(int which, const StepArgs* args, const int2* items, const int* flags,
+                          int n_items, int n_runs, cudaStream_t s) {
+  switch (which) {
+    case 0: k_adams_predict_b<<<n_items, 256, 0, s>>>(args, items, flags); break;
+    case 1:
+      k_adams_correct_b<<<n_items, 256, 0, s>>>(args, items, flags);
+      k_reduce_b<<<dim3(kMaxOrders + 1, n_runs), 32, 0, s>>>(args, flags, kMaxOrders + 1);
+      break;
+    case 2: k_adams_accept_b<<<n_items, 256, 0, s>>>(args, items, flags); break;
+    case 3: k_adams_start_b<<<n_items, 256, 0, s>>>(args, items, flags); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
@@ -317,7 +377,7 @@ __global__ void __launch_bounds__(256) k_rk_finish(RkArgs a, RkFinish f) {
       v[2] += e.x * e.x + e.y * e.y;
     }
   }
-  block_partials<3>(v, a.partials);
+  block_partials<3>(v, a.partials, blockIdx.x);
 }
 
 __global__ void k_mask_copy(double2* dst, const double2* src, const unsigned char* active, int n,
@@ -347,7 +407,7 @@ cudaError_t launch_rk_finish(const RkArgs& a, const double* b, const double* e, 
   }
   f.dz = dz;
   k_rk_finish<<<kNormBlocks, 256, 0, s>>>(a, f);
-  k_reduce<<<3, 32, 0, s>>>(a.partials, a.norms, 3);
+  k_reduce<<<3, 32, 0, s>>>(a.partials, a.norms, 3, kNormBlocks);
   return cudaGetLastError();
 }
 

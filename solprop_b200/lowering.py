@@ -129,7 +129,10 @@ def lower(problem) -> ProblemRecord:
         else np.asarray(responses.temporal_absorber, dtype=np.float64),
         field0=np.ascontiguousarray(np.broadcast_to(initial.field0, problem.shape), dtype=np.complex128),
         noise0=None if initial.noise0 is None else np.asarray(initial.noise0, dtype=np.complex128),
+        noise_model=str(getattr(initial, "noise_model", "none") or "none"),
     )
+    if record.noise0 is not None and record.noise_model == "modified":
+        raise BackendRefusal("the modified noise model (a draw added at every stage)")
     if np.iscomplexobj(transform.synthesis):
         raise BackendRefusal("a complex synthesis matrix")
     if kerr is not None:

@@ -194,6 +194,15 @@ class ProblemRecord:
     # ---- initial state (kernel-contract.md section 6)
     field0: np.ndarray | None = None
     noise0: np.ndarray | None = None
+    noise_model: str = "none"  # "input": added to the launch field; "modified": every stage
+
+    def launch_field(self) -> np.ndarray:
+        """The state a run starts from: ``field0``, plus the ``input`` noise draw
+        (``backends/numpy_ref/workspace.py:260-306``); the device masks it to the band."""
+        field = np.broadcast_to(self.field0, (self.n_modes, self.n_pol, self.n_omega))
+        if self.noise0 is not None and self.noise_model == "input":
+            return field + self.noise0
+        return np.array(field)
 
     @property
     def n_cols(self) -> int:

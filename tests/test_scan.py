@@ -1,0 +1,80 @@
+"""The scan workload: the seeded problem builder (CPU) and the batched solver (GPU)."""
+
+import numpy as np
+import pytest
+
+from oracle import march as M
+from oracle import source as S
+from solprop_b200 import scan
+from tests._cases import rel
+
+
+def test_draw_points_follows_the_stated_distribution():
+    pts = scan.draw_points(400, 11)
+    r = np.array([p.radius for p in pts])
+    e = np.array([p.energy for p in pts])
+    assert r.min() >= 50e-6 and r.max() <= 150e-6
+    assert e.min() >= 20e-6 and e.max() <= 500e-6
+    assert {p.gas for p in pts} == {"He", "Ne", "Ar"}
+    assert {p.n_to for p in pts} == {4096, 8192, 16384, 32768}
+    assert {p.modes for p in pts} == set(range(1, 9))
+    assert scan.draw_points(5, 11) == pts[:5]  # seeded
+
+
+def test_capillary_record_is_a_consistent_problem():
+    p = scan.ScanPoint(100e-6, 1.0, "Ar", 1.0, 50e-6, 20e-15, 3, 4096, 7)
+    rec, pol = scan.capillary_record(p)
+    # projection @ synthesis = pad_scale I on the orthonormal set (kernel-contract.md 4)
+    ps = rec.projection @ rec.synthesis
+    assert np.allclose(ps, rec.pad_scale * np.eye(3), atol=1e-12)
+    # operator and prefactor vanish off the active band
+    assert np.all(rec.phi_terms[..., ~rec.active_mask] == 0)
+    assert np.all(rec.prefactor_terms[..., ~rec.active_mask] == 0)
+    # the pulse carries its energy (Parseval on the coarse grid, half spectrum)
+    x = np.fft.irfft(rec.field0[0, 0], n=rec.n_t)
+    assert abs(np.sum(x * x) * rec.dt / 50e-6 - 1) < 1e-3
+    out = {}
+    k = S.lab_source(rec, rec.launch_field() * rec.active_mask, 0.0, out=out)
+    assert np.all(np.isfinite(k)) and np.abs(k).max() > 0
+    assert out["rate"].max() > 0  # the pulse ionises
+
+
+@pytest.mark.gpu
+def test_batched_runs_match_single_runs():
+    from solprop_b200 import _lib
+
+    points = [
+        scan.ScanPoint(120e-6, 1.0, "He", 1.0, 60e-6, 20e-15, 2, 4096, 1),
+        scan.ScanPoint(90e-6, 0.8, "Ar", 0.5, 30e-6, 25e-15, 1, 8192, 2),
+        scan.ScanPoint(140e-6, 1.5, "Ne", 2.0, 100e-6, 12e-15, 3, 4096, 3),
+    ]
+    built = [scan.capillary_record(p) for p in points]
+    sc = _lib.Scan([r for r, _ in built], [q for _, q in built])
+    steps = 12
+    sc.advance(steps)
+    for i, (rec, pol) in enumerate(built):
+        state, info = sc.run(i)
+        problem = _lib.Problem(rec)
+        ws = _lib.Workspace(problem)
+        session = ws.start(pol)
+        for _ in range(int(info.attempts)):
+            session.advance(1)
+        assert rel(state, session.export()) < 1e-12, i
+        assert info.attempts == steps
+
+
+@pytest.mark.gpu
+def test_batched_run_matches_the_oracle():
+    from solprop_b200 import _lib
+
+    p = scan.ScanPoint(110e-6, 1.0, "Ar", 1.0, 40e-6, 20e-15, 2, 4096, 5)
+    rec, pol = scan.capillary_record(p)
+    sc = _lib.Scan([rec], [pol])
+    sc.advance(6)
+    state, info = sc.run(0)
+    ws = M.Workspace(rec)
+    march = M.AdamsMarch(M.AdamsEngine(ws, pol), pol, pol["proposal"])
+    for _ in range(int(info.attempts)):
+        march.attempt_towards(rec.z_end)
+    assert march.attempts == info.attempts
+    assert rel(state, ws.state) < 1e-10
