@@ -141,6 +141,66 @@ def cpu_arm(rec, pol, steps: int, warmup: int, budget_s: float, threads: int | N
     return done, elapsed
 
 
+def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024) -> dict:
+    """BASELINE config 4's workload: n_runs seeded uneven capillary runs, stepped together.
+
+    Reports attempts per second of the batched solver (every batch step gives every run
+    one exponential-Adams attempt, FP64) and of the plain path on the same runs one at a
+    time (one session per run, its attempts back to back), on the device's clock.
+    """
+    import torch
+
+    from solprop_b200 import _lib, scan
+
+    points = scan.draw_points(n_runs, seed)
+    built = [scan.capillary_record(p) for p in points]
+    records, policies = [b[0] for b in built], [b[1] for b in built]
+    sc = _lib.Scan(records, policies, device)
+    stream = torch.cuda.ExternalStream(sc.stream, device=torch.device("cuda", device))
+    sc.advance(warmup)
+    before = sc.advance(0).attempts
+    torch.cuda.synchronize()
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s_ev.record(stream)
+    status = sc.advance(steps)
+    e_ev.record(stream)
+    torch.cuda.synchronize()
+    batched_ms = s_ev.elapsed_time(e_ev)
+    batched_attempts = status.attempts - before
+    active = status.active
+    del sc
+    # the plain path: each run alone, three attempts after one warm-up
+    plain_ms, plain_attempts = 0.0, 0
+    sample = list(range(0, n_runs, max(1, n_runs // 64)))
+    for i in sample:
+        problem = _lib.Problem(records[i])
+        ws = _lib.Workspace(problem, device)
+        st = torch.cuda.ExternalStream(ws.stream, device=torch.device("cuda", device))
+        session = ws.start(policies[i])
+        session.advance(1)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        for _ in range(3):
+            session.advance(1)
+        b.record(st)
+        torch.cuda.synchronize()
+        plain_ms += a.elapsed_time(b)
+        plain_attempts += 3
+        session.close()
+        ws.close()
+        problem.close()
+    batched = batched_attempts / (batched_ms / 1e3)
+    plain = plain_attempts / (plain_ms / 1e3)
+    return {"workload": f"config 4: {n_runs} seeded capillary runs (radius 50-150 um, length "
+                        "0.5-2 m, He/Ne/Ar, 0.2-3 bar, 20-500 uJ, 5-30 fs, 1-8 modes, "
+                        "n_to 2^12-2^15), Kerr + plasma + input shot noise, exp. Adams rtol 1e-6",
+            "dtype": "f64", "batched_attempts_per_s": batched, "batch_steps": steps,
+            "ms_per_batch_step": batched_ms / steps, "active_runs_at_end": active,
+            "plain_attempts_per_s": plain, "plain_sample_runs": len(sample),
+            "speedup_batched_vs_plain": batched / plain}
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -148,6 +208,8 @@ def main() -> int:
     parser.add_argument("--warmup", type=int, default=10)
     parser.add_argument("--impl", default="ours", choices=["ours", "reference"])
     parser.add_argument("--cpu-budget", type=float, default=20.0)
+    parser.add_argument("--scan-runs", type=int, default=256)
+    parser.add_argument("--scan-steps", type=int, default=30)
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -275,12 +337,16 @@ def main() -> int:
                "sample": f"{done} attempts of the config-2 run from z=0 on one host thread "
                          f"({os.cpu_count()} cores on the box)"}
 
+    scan_result = None
+    if args.scan_runs > 0:
+        scan_result = scan_leg(local, args.scan_runs, args.scan_steps, warmup=3)
+
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * args.steps)),
-            "clocks": clocks.summary()}
+            "clocks": clocks.summary(), "scan": scan_result}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del session, s2
