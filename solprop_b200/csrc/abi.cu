@@ -191,9 +191,10 @@ struct sp_workspace {
   int log_m = 0, log_n_to = 0, launches = 0, n_rows = 0;
   DevBuf<double2> phi_terms, pre_terms, twiddles, lab, out, spectra;
   DevBuf<double> omega, omega_window, t_window, t_window_d, alpha, synthesis, projection,
-      rate_coeff, taps, modal_t, streams, sums0, offsets0, sums1, offsets1, proj;
+      rate_coeff, taps, modal_t, streams, sums0, sums1, proj;
   DevBuf<long long> crop;
-  DevBuf<int> fine_to_coarse, rows;
+  DevBuf<int> fine_to_coarse, rows, chain_flags;
+  DevBuf<unsigned long long> ticket;  // the response column's tile counter
   DevBuf<unsigned char> active, norm;
   DevBuf<StageScalarsDev> stage;   // kStageSlots slots
   StageScalarsDev* h_stage = nullptr;  // pinned
@@ -310,9 +311,10 @@ static ColumnTileArgs column_args(const sp_workspace* ws, const StageScalarsDev*
   ca.t_window = ws->t_window.p;
   ca.t_window_derivative = ws->t_window_d.p;
   ca.sums0 = ws->sums0.p;
-  ca.offsets0 = ws->offsets0.p;
   ca.sums1 = ws->sums1.p;
-  ca.offsets1 = ws->offsets1.p;
+  ca.ticket = ws->ticket.p;
+  ca.flags = ws->chain_flags.p;
+  ca.status = ws->norms.p + kColumnStatus;
   ca.partials = ws->proj.p;
   ca.n_modes = d.n_modes;
   ca.n_nodes = d.n_nodes;
@@ -320,6 +322,7 @@ static ColumnTileArgs column_args(const sp_workspace* ws, const StageScalarsDev*
   ca.n_to = d.n_to;
   ca.n_tiles = (d.n_to + kSeg - 1) / kSeg;
   ca.n_groups = (d.n_nodes + kGroup - 1) / kGroup;
+  ca.n_blocks = ca.n_tiles * ca.n_groups;
   ca.kerr = d.kerr_enabled;
   ca.plasma = d.plasma_enabled;
   ca.band = d.band;
@@ -372,7 +375,7 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
   const InverseArgs ia = inverse_args(ws, lab, absorber);
   { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
   const ColumnTileArgs ca = column_args(ws, ws->stage.p + slot);
-  { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column_tiled(ca, ws->stream)); }
+  { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column(ca, ws->stream)); }
   const ForwardArgs fa = forward_args(ws);
   { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
   const OutputArgs oa = output_args(ws, ws->stage.p + slot, inv_prop, out, absorber);
@@ -428,9 +431,11 @@ static void build_workspace(sp_workspace* ws) {
   const size_t n_tiles = (d.n_to + kSeg - 1) / kSeg;
   const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
   ws->sums0.alloc((size_t)d.n_nodes * n_tiles);
-  ws->offsets0.alloc((size_t)d.n_nodes * n_tiles);
   ws->sums1.alloc((size_t)d.n_nodes * n_tiles);
-  ws->offsets1.alloc((size_t)d.n_nodes * n_tiles);
+  ws->chain_flags.alloc(n_groups * n_tiles);
+  ws->chain_flags.zero(s);
+  ws->ticket.alloc(1);
+  ws->ticket.zero(s);
   ws->proj.alloc(n_groups * 3 * P.n_cols * d.n_to);
   ws->proj.zero(s);
   ws->streams.alloc((size_t)4 * P.n_cols * d.n_to);
@@ -444,6 +449,7 @@ static void build_workspace(sp_workspace* ws) {
   ws->adams.alloc(1);
   ws->partials.alloc((kMaxOrders + 2) * kNormBlocks);
   ws->norms.alloc(kMaxOrders + 2);
+  ws->norms.zero(s);
   ws->launches = 5;
   CUDA_CHECK(cudaStreamSynchronize(s));
 }
@@ -763,6 +769,14 @@ static StepArgs step_args_of(sp_workspace* ws, const AdamsDev* adams_dev, const 
   return a;
 }
 
+// A response column whose tiles gave up waiting on one another marks the norms' status
+// slot; the host turns that into an error (and clears the mark).
+static void check_column(const double* h_norms, double* d_norms, cudaStream_t s) {
+  if (h_norms[kColumnStatus] == 0.0) return;
+  CUDA_CHECK(cudaMemsetAsync(d_norms + kColumnStatus, 0, sizeof(double), s));
+  throw Failure(SP_ERR_CUDA, "response column: a tile gave up waiting for its predecessors");
+}
+
 // One Adams attempt of a single run; returns accepted.
 static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool fixed) {
   sp_workspace* ws = S->ws;
@@ -773,10 +787,11 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
   { KernelTimer t(ws, SP_K_PREDICT); CUDA_CHECK(launch_adams_predict(a, ws->stream)); }
   eval_source(ws, ws->lab.p, 1, nullptr, ws->src.p, false);
   { KernelTimer t(ws, SP_K_CORRECT); CUDA_CHECK(launch_adams_correct(a, ws->stream)); }
-  CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, sizeof(double) * (kMaxOrders + 1),
+  CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, sizeof(double) * (kColumnStatus + 1),
                              cudaMemcpyDeviceToHost, ws->stream));
   CUDA_CHECK(cudaStreamSynchronize(ws->stream));
   ws->flush_timing();
+  check_column(ws->h_norms, ws->norms.p, ws->stream);
   const bool accepted = decide_attempt(S, pd, ws->h_norms);
   if (accepted) {
     KernelTimer t(ws, SP_K_ACCEPT);
@@ -895,9 +910,10 @@ static double rk_trial(sp_session* S, double dz) {
   }
   a.stage = ws->stage.p + 7;
   { KernelTimer t(ws, SP_K_RK_FINISH); CUDA_CHECK(launch_rk_finish(a, kB, e, dz, R.rtol, R.atol, ws->stream)); }
-  CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, 3 * sizeof(double), cudaMemcpyDeviceToHost,
-                             ws->stream));
+  CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, (kColumnStatus + 1) * sizeof(double),
+                             cudaMemcpyDeviceToHost, ws->stream));
   CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+  check_column(ws->h_norms, ws->norms.p, ws->stream);
   S->attempts += 1;
   S->evaluations += 7;
   const double scale = R.rtol * std::max(std::sqrt(ws->h_norms[0]), std::sqrt(ws->h_norms[1])) + R.atol;
@@ -1087,7 +1103,10 @@ sp_status sp_workspace_source(sp_workspace* ws, const double* lab, double z, int
     upload_stages(ws, 1);
     eval_source(ws, ws->lab.p, 0, nullptr, ws->out.p, quiet != 0);
     CUDA_CHECK(cudaMemcpyAsync(out, ws->out.p, bytes, cudaMemcpyDeviceToHost, ws->stream));
+    CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, (kColumnStatus + 1) * sizeof(double),
+                               cudaMemcpyDeviceToHost, ws->stream));
     CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+    check_column(ws->h_norms, ws->norms.p, ws->stream);
   });
 }
 
@@ -1321,8 +1340,7 @@ void scan_source(sp_scan* S, bool start) {
     else
       CUDA_CHECK(launch_inverse_b(inv.p, c->inv_items.p, flags.p, c->n_inv, c->n_to, S->stream));
   }
-  for (int pass = 0; pass < 3; ++pass)
-    CUDA_CHECK(launch_column_tiled_b(col.p, S->col_items.p, flags.p, S->n_col_items, pass, S->stream));
+  CUDA_CHECK(launch_column_b(col.p, S->col_items.p, flags.p, S->n_col_items, S->stream));
   for (auto& c : S->classes) {
     if (c->cluster)
       CUDA_CHECK(launch_forward_cluster_b(S->fwd.p, c->fwd_items.p, flags.p, c->n_fwd, c->n_to, S->stream));
@@ -1388,6 +1406,8 @@ void scan_step(sp_scan* S) {
   CUDA_CHECK(cudaMemcpyAsync(S->h_norms, S->norms.p, sizeof(double) * 8 * R, cudaMemcpyDeviceToHost,
                              S->stream));
   CUDA_CHECK(cudaStreamSynchronize(S->stream));
+  for (int r = 0; r < R; ++r)
+    if (S->h_flag_att[r]) check_column(S->h_norms + 8 * r, S->norms.p + 8 * r, S->stream);
   for (int r = 0; r < R; ++r) {
     S->h_flag_accept[r] = 0;
     if (!S->h_flag_att[r]) continue;
@@ -1462,6 +1482,7 @@ sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, cons
     S->stages_start.alloc(R);
     S->stages_att.alloc(2 * (size_t)R);
     S->norms.alloc(8 * (size_t)R);
+    S->norms.zero(S->stream);
     S->flag_start.alloc(R);
     S->flag_att.alloc(R);
     S->flag_accept.alloc(R);
@@ -1482,6 +1503,7 @@ sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, cons
       ia[r] = inverse_args(w, w->lab.p, absorber);
       cs[r] = column_args(w, S->stages_start.p + r);
       ca[r] = column_args(w, S->stages_att.p + 2 * r + 1);
+      cs[r].status = ca[r].status = S->norms.p + 8 * r + kColumnStatus;
       fa[r] = forward_args(w);
       os[r] = output_args(w, S->stages_start.p + r, nullptr, w->src.p, absorber);
       oa[r] = output_args(w, S->stages_att.p + 2 * r + 1, nullptr, w->src.p, absorber);
@@ -1493,8 +1515,7 @@ sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, cons
       for (int b = 0; b < nb; ++b) step_items.push_back(make_int2(r, b));
       const int no = (P.n + 255) / 256;
       for (int b = 0; b < no; ++b) out_items.push_back(make_int2(r, b));
-      for (int t = 0; t < cs[r].n_tiles; ++t)
-        for (int g = 0; g < cs[r].n_groups; ++g) col_items.push_back(make_int4(r, t, g, 0));
+      for (int b = 0; b < cs[r].n_blocks; ++b) col_items.push_back(make_int4(r, b, 0, 0));
       if (std::find(sizes.begin(), sizes.end(), P.d.n_to) == sizes.end()) sizes.push_back(P.d.n_to);
     }
     std::sort(sizes.begin(), sizes.end());
@@ -1692,9 +1713,10 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     const size_t n_tiles = (d.n_to + kSeg - 1) / kSeg;
     const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
     carve.take(ws.sums0, (size_t)d.n_nodes * n_tiles);
-    carve.take(ws.offsets0, (size_t)d.n_nodes * n_tiles);
     carve.take(ws.sums1, (size_t)d.n_nodes * n_tiles);
-    carve.take(ws.offsets1, (size_t)d.n_nodes * n_tiles);
+    carve.take(ws.chain_flags, n_groups * n_tiles);
+    carve.take(ws.ticket, 1);
+    carve.take(ws.norms, kMaxOrders + 2);
     carve.take(ws.proj, n_groups * 3 * P.n_cols * d.n_to);
     carve.take(ws.streams, (size_t)4 * P.n_cols * d.n_to);
     carve.take(ws.spectra, (size_t)4 * n);
@@ -1738,6 +1760,9 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     ws.streams.zero(s);
     ws.spectra.zero(s);
     ws.proj.zero(s);
+    ws.chain_flags.zero(s);
+    ws.ticket.zero(s);
+    ws.norms.zero(s);
     static bool configured[kNoAllocDevices];
     if (!configured[device]) {
       CUDA_CHECK(configure_source_kernels());

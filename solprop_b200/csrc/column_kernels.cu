@@ -1,4 +1,4 @@
-// The response column of the field-plasma route as three tiled passes, fused with the
+// The response column of the field-plasma route in one launch, fused with the
 // projection (passes 3-5 of docs/dev/architecture.md section 8: synthesis, the fused
 // response, projection; backends/numpy_ref/passes/plasma.py:59-323, responses.py:678-819,
 // transforms.py:87-187; nonlinear/ionisation.py:410-675 for the band rule).
@@ -6,16 +6,14 @@
 // A tile is kSeg fine samples of a group of kGroup quadrature nodes, one CTA of 256
 // threads: 16 threads per node, each owning kSeg/16 consecutive samples.  The two
 // running integrals (the exposure int W dt and the free current int f E dt) are split
-// the way the reference's native device scan splits them -- tile totals, then a rescan
-// of every tile from its offset (native trial_response.inc:597-700):
-//   pass 0  exposure increments of each tile, summed;
-//   pass 1  offset = the predecessors' sums in tile order, exposure rescanned, fraction,
-//           current increments summed;
-//   pass 2  both rescans, the total current, the Kerr cubic, the temporal collar, and the
-//           tile projected onto the modes (partial sums per node group).
-// Each pass recomputes the synthesis and the rate on its tile and a halo of 2K + 1
-// samples, staging the modal field in shared memory first.  Every sum has a fixed order,
-// so the results are reproducible bit for bit.
+// the way the reference's native device scan splits them -- tile totals, then every tile
+// rescanned from its offset (native trial_response.inc:597-700) -- but in a single pass:
+// a tile publishes its exposure sum, adds its predecessors' sums (in a fixed order) once
+// they are published, rescans, publishes its current sum the same way, and goes on to the
+// total current, the Kerr cubic, the temporal collar and the projection onto the modes
+// (partial sums per node group).  The synthesis and the rate are computed once per tile
+// and its halo of 2K + 1 samples, from the modal field staged in shared memory.  Every
+// sum has a fixed order, so the results are reproducible bit for bit.
 #include "kernels.cuh"
 
 namespace sp {
@@ -29,9 +27,7 @@ constexpr int kPer = kSeg / kLanes;          // samples of the tile per thread (
 constexpr int kI0 = 2 * kHalo + 1;           // local index of t0
 constexpr size_t kRowBytes = sizeof(double) * kGroup * kLen;
 constexpr size_t kModalBytes = sizeof(double) * kMaxModes * kLen;
-constexpr size_t kPass0Smem = 3 * kRowBytes + kModalBytes;
-constexpr size_t kPass1Smem = 4 * kRowBytes + kModalBytes;
-constexpr size_t kPass2Smem = 5 * kRowBytes + kModalBytes;
+constexpr size_t kChainSmem = 5 * kRowBytes + kModalBytes;
 
 struct Tile {
   int t0, n0, nodes, tile;
@@ -176,27 +172,6 @@ __device__ void tile_sum(const Tile& c, const double* inc, double* out, int n_ti
   if (c.lane == 0 && c.node < c.nodes) out[(size_t)(c.n0 + c.node) * n_tiles + c.tile] = s;
 }
 
-// The sum of the predecessors' tile sums of this thread's node, in a fixed order: lane l
-// adds tiles l, l + kLanes, ... below the tile, then the lanes are added as a tree.
-__device__ double predecessors(const Tile& c, const double* sums, int n_tiles) {
-  double s = 0.0;
-  if (c.node < c.nodes) {
-    const double* row = sums + (size_t)(c.n0 + c.node) * n_tiles;
-    int k = c.lane;
-    // four loads in flight, added in tile order
-    for (; k + 3 * kLanes < c.tile; k += 4 * kLanes) {
-      const double v0 = row[k], v1 = row[k + kLanes], v2 = row[k + 2 * kLanes],
-                   v3 = row[k + 3 * kLanes];
-      s += v0;
-      s += v1;
-      s += v2;
-      s += v3;
-    }
-    for (; k < c.tile; k += kLanes) s += row[k];
-  }
-  return lanes_total(s);
-}
-
 // The running integral on [t0 - H, t1 + H] of this thread's node, into out: the
 // increments on [t0 - H, t1 + H) scanned across the node's lanes, anchored so that
 // out[t0] = offset.  Each lane scans 5 consecutive samples (kSeg + 2H = 80 = 16 x 5).
@@ -236,75 +211,103 @@ __device__ void rescan(const Tile& c, const double* inc, double* out, double off
   __syncthreads();
 }
 
-}  // namespace
+// ---- tile order and the hand-over between tiles
+// Every CTA takes a ticket from the workspace's counter; tickets are handed out in tile
+// order (tile-major, node group minor), so a CTA only ever waits on tiles whose CTAs took
+// their tickets earlier and are therefore resident: the waits always end.  A launch takes
+// exactly n_blocks tickets, so ticket / n_blocks numbers the evaluation (its epoch) and the
+// ready flags need no reset: a tile's flag reads 2 e + 1 once its exposure sums of
+// evaluation e are published and 2 e + 2 once its current sums are.
+constexpr long kSpinLimit = 1L << 20;  // polls of one flag before the wait gives up
 
-// pass 0: the exposure's tile sums
-__device__ __forceinline__ void pass0_body(const ColumnTileArgs& a, int tile, int group) {
-  extern __shared__ double dyn0[];
-  double* E = dyn0;
-  double* W = E + kGroup * kLen;
-  double* T = W + kGroup * kLen;
-  double* modal = T + kGroup * kLen;
-  const Tile c = tile_of(a, tile, group);
-  // W~ on [t0, t1] needs W on [t0 - H, t1 + H]
-  field_and_rate(a, c, modal, E, W, kI0 - kHalo, kI0 + kSeg + kHalo + 1, true);
-  increments(a, c, W, T, E, c.t0, c.t0 + kSeg);
-  tile_sum(c, E, a.sums0, a.n_tiles);
+__device__ __forceinline__ int load_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
-// pass 1: the exposure rescanned, the fraction, the current's tile sums
-__device__ __forceinline__ void pass1_body(const ColumnTileArgs& a, int tile, int group) {
-  extern __shared__ double dyn1[];
-  double* E = dyn1;
-  double* W = E + kGroup * kLen;
-  double* T = W + kGroup * kLen;
-  double* S = T + kGroup * kLen;
-  double* modal = S + kGroup * kLen;
-  const Tile c = tile_of(a, tile, group);
-  const double off0 = predecessors(c, a.sums0, a.n_tiles);
-  if (c.lane == 0 && c.node < c.nodes) a.offsets0[(size_t)(c.n0 + c.node) * a.n_tiles + c.tile] = off0;
-  field_and_rate(a, c, modal, E, W, 0, kLen, true);
-  increments(a, c, W, T, S, c.t0 - kHalo, c.t0 + kSeg + kHalo);
-  rescan(c, S, T, off0);  // T = exposure on [t0 - H, t1 + H]
-  const double f0 = a.stage->preionisation;
-  if (c.node < c.nodes) {
-    for (int i = c.lane; i < kLen; i += kLanes) {
-      const int idx = c.node * kLen + i;
-      const int t = c.t0 - kI0 + i;
-      double g = 0.0;
-      if (t >= c.t0 - kHalo && t <= c.t0 + kSeg + kHalo && t >= 0 && t < a.n_to) {
-        const double x = a.band ? fmax(T[idx], 0.0) : T[idx];
-        const double f = 1.0 - (1.0 - f0) * (x == 0.0 ? 1.0 : exp(-x));
-        g = f * a.charge_mass_ratio * E[idx];
+__device__ __forceinline__ void store_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// publish this tile's sums (already written by the nodes' lane 0) as stage `target`
+__device__ __forceinline__ void publish(const ColumnTileArgs& a, const Tile& c, int group, int target) {
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) store_release(a.flags + (size_t)group * a.n_tiles + c.tile, target);
+}
+
+// wait until every earlier tile of the group has published stage `target`; a wait that
+// gives up marks the evaluation failed in *status (read by the host) and goes on
+__device__ __forceinline__ void await_predecessors(const ColumnTileArgs& a, const Tile& c, int group,
+                                                   int target) {
+  const int* f = a.flags + (size_t)group * a.n_tiles;
+  for (int j = threadIdx.x; j < c.tile; j += blockDim.x) {
+    long polls = 0;
+    while (load_acquire(f + j) < target) {
+      if (++polls > kSpinLimit) {
+        *a.status = 1.0;
+        break;
       }
-      W[idx] = g;  // the current's integrand
+      __nanosleep(64);
     }
   }
+  __threadfence();
   __syncthreads();
-  increments(a, c, W, T, S, c.t0, c.t0 + kSeg);
-  tile_sum(c, S, a.sums1, a.n_tiles);
 }
 
-// pass 2: both rescans, the total current, Kerr, the collar and the projection
-__device__ __forceinline__ void pass2_body(const ColumnTileArgs& a, int tile, int group) {
-  extern __shared__ double dyn2[];
-  double* E = dyn2;
+// the predecessors' sums, read past L1 (other CTAs wrote them during this launch)
+__device__ double predecessors_cg(const Tile& c, const double* sums, int n_tiles) {
+  double s = 0.0;
+  if (c.node < c.nodes) {
+    const double* row = sums + (size_t)(c.n0 + c.node) * n_tiles;
+    int k = c.lane;
+    for (; k + 3 * kLanes < c.tile; k += 4 * kLanes) {
+      const double v0 = __ldcg(row + k), v1 = __ldcg(row + k + kLanes),
+                   v2 = __ldcg(row + k + 2 * kLanes), v3 = __ldcg(row + k + 3 * kLanes);
+      s += v0;
+      s += v1;
+      s += v2;
+      s += v3;
+    }
+    for (; k < c.tile; k += kLanes) s += __ldcg(row + k);
+  }
+  return lanes_total(s);
+}
+
+}  // namespace
+
+// One tile of the column, start to finish: synthesis and rate on the tile and its halo,
+// the exposure's increments and tile sum (published), the exposure from the
+// predecessors' sums, the fraction and the current's increments and tile sum (published),
+// the current from the predecessors' sums, then the total current, Kerr, the collar and
+// the tile projected onto the modes (partial sums per node group).
+__device__ __forceinline__ void chain_body(const ColumnTileArgs& a) {
+  extern __shared__ double dyn[];
+  double* E = dyn;
   double* W = E + kGroup * kLen;
   double* F = W + kGroup * kLen;   // exposure, then the fraction in place
-  double* Y1 = F + kGroup * kLen;  // integrand -> increments
+  double* Y1 = F + kGroup * kLen;  // increments
   double* Y2 = Y1 + kGroup * kLen; // filtered scratch -> running integral
   double* modal = Y2 + kGroup * kLen;
+  __shared__ unsigned long long ticket;
+  if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1ull);
+  __syncthreads();
+  const unsigned long long epoch = ticket / (unsigned long long)a.n_blocks;
+  const int index = (int)(ticket % (unsigned long long)a.n_blocks);
+  const int tile = index / a.n_groups, group = index % a.n_groups;
   const Tile c = tile_of(a, tile, group);
   const bool plasma = a.plasma;
-  double off1 = 0.0, off0 = 0.0;
-  if (plasma) {
-    off1 = predecessors(c, a.sums1, a.n_tiles);
-    if (c.node < c.nodes) off0 = a.offsets0[(size_t)(c.n0 + c.node) * a.n_tiles + c.tile];
-  }
   field_and_rate(a, c, modal, E, W, plasma ? 0 : kI0, plasma ? kLen : kI0 + kSeg, plasma);
   if (plasma) {
+    const int first = (int)(2 * epoch + 1);
+    // exposure increments on [t0 - H, t1 + H) into Y1; the tile's own sum is published
     increments(a, c, W, Y2, Y1, c.t0 - kHalo, c.t0 + kSeg + kHalo);
-    rescan(c, Y1, F, off0);  // F = exposure
+    tile_sum(c, Y1, a.sums0, a.n_tiles);
+    publish(a, c, group, first);
+    await_predecessors(a, c, group, first);
+    const double off0 = predecessors_cg(c, a.sums0, a.n_tiles);
+    rescan(c, Y1, F, off0);  // F = exposure on [t0 - H, t1 + H]
     const double f0 = a.stage->preionisation;
     if (c.node < c.nodes) {
       for (int i = c.lane; i < kLen; i += kLanes) {
@@ -322,7 +325,11 @@ __device__ __forceinline__ void pass2_body(const ColumnTileArgs& a, int tile, in
     }
     __syncthreads();
     increments(a, c, Y1, Y2, Y1, c.t0, c.t0 + kSeg);  // Y1: the current's increments
-    rescan(c, Y1, Y2, off1);                          // Y2: free current per unit density
+    tile_sum(c, Y1, a.sums1, a.n_tiles);
+    publish(a, c, group, first + 1);
+    await_predecessors(a, c, group, first + 1);
+    const double off1 = predecessors_cg(c, a.sums1, a.n_tiles);
+    rescan(c, Y1, Y2, off1);  // Y2: free current per unit density
   }
   // outputs on [t0, t1): P = (c rho E^2 E) g, X = g rho J, Z = g' rho J
   const StageScalarsDev& st = *a.stage;
@@ -388,61 +395,32 @@ __device__ __forceinline__ void pass2_body(const ColumnTileArgs& a, int tile, in
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_column_pass0(ColumnTileArgs a) {
-  pass0_body(a, blockIdx.x, blockIdx.y);
-}
-__global__ void __launch_bounds__(kThreads) k_column_pass1(ColumnTileArgs a) {
-  pass1_body(a, blockIdx.x, blockIdx.y);
-}
-__global__ void __launch_bounds__(kThreads) k_column_pass2(ColumnTileArgs a) {
-  pass2_body(a, blockIdx.x, blockIdx.y);
-}
-// batched: items[blockIdx.x] = (run, tile, group, -)
-__global__ void __launch_bounds__(kThreads) k_column_pass0_b(const ColumnTileArgs* args, const int4* items,
-                                                                const int* flags) {
-  const int4 it = items[blockIdx.x];
-  if (!flags[it.x]) return;
-  pass0_body(args[it.x], it.y, it.z);
-}
-__global__ void __launch_bounds__(kThreads) k_column_pass1_b(const ColumnTileArgs* args, const int4* items,
-                                                                const int* flags) {
-  const int4 it = items[blockIdx.x];
-  if (!flags[it.x]) return;
-  pass1_body(args[it.x], it.y, it.z);
-}
-__global__ void __launch_bounds__(kThreads) k_column_pass2_b(const ColumnTileArgs* args, const int4* items,
-                                                                const int* flags) {
-  const int4 it = items[blockIdx.x];
-  if (!flags[it.x]) return;
-  pass2_body(args[it.x], it.y, it.z);
+__global__ void __launch_bounds__(kThreads, 3) k_column(ColumnTileArgs a) { chain_body(a); }
+
+// batched: items[blockIdx.x].x = the run; a run's CTAs take their tiles from its counter
+__global__ void __launch_bounds__(kThreads, 3) k_column_b(const ColumnTileArgs* args, const int4* items,
+                                                       const int* flags) {
+  const int run = items[blockIdx.x].x;
+  if (!flags[run]) return;  // every CTA of an idle run leaves before its ticket
+  chain_body(args[run]);
 }
 
-cudaError_t launch_column_tiled_b(const ColumnTileArgs* args, const int4* items, const int* flags,
-                                  int n_items, int pass, cudaStream_t stream) {
-  if (pass == 0) k_column_pass0_b<<<n_items, kThreads, kPass0Smem, stream>>>(args, items, flags);
-  else if (pass == 1) k_column_pass1_b<<<n_items, kThreads, kPass1Smem, stream>>>(args, items, flags);
-  else k_column_pass2_b<<<n_items, kThreads, kPass2Smem, stream>>>(args, items, flags);
+cudaError_t launch_column_b(const ColumnTileArgs* args, const int4* items, const int* flags,
+                            int n_items, cudaStream_t stream) {
+  k_column_b<<<n_items, kThreads, kChainSmem, stream>>>(args, items, flags);
   return cudaGetLastError();
 }
 
-cudaError_t launch_column_tiled(const ColumnTileArgs& a, cudaStream_t stream) {
-  const dim3 grid(a.n_tiles, a.n_groups);
-  if (a.plasma) {
-    k_column_pass0<<<grid, kThreads, kPass0Smem, stream>>>(a);
-    k_column_pass1<<<grid, kThreads, kPass1Smem, stream>>>(a);
-  }
-  k_column_pass2<<<grid, kThreads, kPass2Smem, stream>>>(a);
+cudaError_t launch_column(const ColumnTileArgs& a, cudaStream_t stream) {
+  k_column<<<a.n_blocks, kThreads, kChainSmem, stream>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t configure_column_kernels() {
-  const void* kernels[6] = {(const void*)k_column_pass0, (const void*)k_column_pass1,
-                            (const void*)k_column_pass2, (const void*)k_column_pass0_b,
-                            (const void*)k_column_pass1_b, (const void*)k_column_pass2_b};
-  const size_t shm[6] = {kPass0Smem, kPass1Smem, kPass2Smem, kPass0Smem, kPass1Smem, kPass2Smem};
-  for (int i = 0; i < 6; ++i) {
+  const void* kernels[2] = {(const void*)k_column, (const void*)k_column_b};
+  for (int i = 0; i < 2; ++i) {
     cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)shm[i]);
+                                         (int)kChainSmem);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -10,6 +10,7 @@ namespace sp {
 constexpr int kMaxTerms = 64;      // stage terms of Phi or of the prefactor
 constexpr int kMaxWidth = 8;       // Adams interpolation nodes (order 5 + 1, padded)
 constexpr int kMaxOrders = 3;      // scored orders per trial
+constexpr int kColumnStatus = kMaxOrders + 1;  // norms slot the response column marks on failure
 constexpr int kMaxSlots = 8;       // history rows (order + 2)
 constexpr int kNormBlocks = 148;   // partial-sum blocks of the norm reductions
 
@@ -64,11 +65,12 @@ struct ColumnTileArgs {
   const double* t_window;
   const double* t_window_derivative;
   double* sums0;           // (n_nodes, n_tiles) exposure tile sums
-  double* offsets0;
   double* sums1;           // current tile sums
-  double* offsets1;
+  unsigned long long* ticket;  // tiles handed out so far (n_blocks per evaluation)
+  int* flags;              // (n_groups, n_tiles) publication stage of each tile
+  double* status;          // set to 1 when a tile gave up waiting
   double* partials;        // (n_groups, 3, n_cols, n_to) projected streams per node group
-  int n_modes, n_nodes, n_cols, n_to, n_tiles, n_groups;
+  int n_modes, n_nodes, n_cols, n_to, n_tiles, n_groups, n_blocks;
   int kerr, plasma, band, half_width, rate_intervals;
   double kerr_coefficient, charge_mass_ratio, ionisation_potential, dt;
   double log_field_min, d_log_field, field_min, field_max, rate_max;
@@ -76,7 +78,7 @@ struct ColumnTileArgs {
   const double* taps;
 };
 
-cudaError_t launch_column_tiled(const ColumnTileArgs& a, cudaStream_t stream);
+cudaError_t launch_column(const ColumnTileArgs& a, cudaStream_t stream);
 cudaError_t configure_column_kernels();
 
 struct ForwardArgs {
@@ -124,8 +126,8 @@ cudaError_t launch_forward_cluster_b(const ForwardArgs* args, const int2* items,
                                      int n_items, int n_to, cudaStream_t stream);
 cudaError_t launch_output_b(const OutputArgs* args, const int2* items, const int* flags,
                             int n_items, cudaStream_t stream);
-cudaError_t launch_column_tiled_b(const ColumnTileArgs* args, const int4* items, const int* flags,
-                                  int n_items, int pass, cudaStream_t stream);
+cudaError_t launch_column_b(const ColumnTileArgs* args, const int4* items, const int* flags,
+                            int n_items, cudaStream_t stream);
 
 // ---- stepping kernels (step_kernels.cu)
 struct StepArgs {
