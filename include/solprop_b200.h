@@ -36,6 +36,14 @@ enum {
   SP_ERR_CONVERGENCE = 5 /* step control fell below dz_min, or the field diverged */
 };
 
+/* Precision of a workspace's source evaluations.  FP64 is the plain form, the reference's
+ * arithmetic.  MIXED evaluates the transforms and the response column (synthesis, rate,
+ * fraction, currents, Kerr, projection) in FP32; the state, the propagator phase and its
+ * exponentials, the Adams history and accumulation, the stage output, the error norms and
+ * the plasma running integrals (compensated: FP32 increments summed in FP64) stay FP64.
+ * It has no counterpart in the reference. */
+enum { SP_PRECISION_FP64 = 0, SP_PRECISION_MIXED = 1 };
+
 /* A piecewise Chebyshev series in z (solprop translate/chebyshev.py:236): interval i
  * holds n_deg coefficients of n_values values, c[(i*n_deg + j)*n_values + v].
  * n_intervals == 0 means "absent". */
@@ -140,6 +148,9 @@ sp_status sp_problem_destroy(sp_problem* problem);
 
 /* ---- workspace (replaces _core.Workspace(problem), _core.pyi:600-612) ---- */
 sp_status sp_workspace_create(const sp_problem* problem, int device, sp_workspace** out);
+/* The same with a precision (SP_PRECISION_*). */
+sp_status sp_workspace_create_ex(const sp_problem* problem, int device, int precision,
+                                 sp_workspace** out);
 sp_status sp_workspace_destroy(sp_workspace* ws);
 /* One source evaluation F at a lab-frame field, untransported (numpy_ref
  * workspace.py:819 lab_source): lab and out are host complex (n_modes,n_pol,n_omega).
@@ -191,6 +202,9 @@ typedef struct sp_scan_status {
 } sp_scan_status;
 sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems,
                          const sp_run_desc* runs, int device, sp_scan** out);
+/* The same with a precision (SP_PRECISION_*) for every run. */
+sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems,
+                            const sp_run_desc* runs, int device, int precision, sp_scan** out);
 /* Up to `steps` batch steps (fewer when every run has finished). */
 sp_status sp_scan_advance(sp_scan* scan, int32_t steps, sp_scan_status* out);
 /* One run's state (host complex, may be NULL) and counts (event 2: finished, 3: failed). */

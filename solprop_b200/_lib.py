@@ -95,6 +95,7 @@ SIGNATURES = {
     "sp_problem_create": (C.c_int, [C.POINTER(SpProblemDesc), C.POINTER(C.c_void_p)]),
     "sp_problem_destroy": (C.c_int, [C.c_void_p]),
     "sp_workspace_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "sp_workspace_create_ex": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "sp_workspace_destroy": (C.c_int, [C.c_void_p]),
     "sp_workspace_source": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_double, C.c_int,
                                       C.POINTER(C.c_double)]),
@@ -110,6 +111,8 @@ SIGNATURES = {
     "sp_source_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p,
                                     C.c_void_p]),
     "sp_scan_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(SpRunDesc), C.c_int,
+                                 C.POINTER(C.c_void_p)]),
+    "sp_scan_create_ex": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(SpRunDesc), C.c_int, C.c_int,
                                  C.POINTER(C.c_void_p)]),
     "sp_scan_advance": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SpScanStatus)]),
     "sp_scan_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(SpBatch)]),
@@ -320,6 +323,7 @@ class Problem:
 
     def __init__(self, rec):
         self.handle = None
+        self._lib = library()
         lib = library()
         self.record = rec
         desc, self._keep = problem_desc(rec)
@@ -329,20 +333,34 @@ class Problem:
 
     def close(self):
         if getattr(self, "handle", None):
-            library().sp_problem_destroy(self.handle)
+            self._lib.sp_problem_destroy(self.handle)
             self.handle = None
 
     __del__ = close
 
 
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
+def precision_code(precision: str) -> int:
+    """``SP_PRECISION_*`` of a precision name: "fp64" (the plain form) or "mixed"."""
+    try:
+        return PRECISIONS[precision]
+    except KeyError:
+        raise ValueError(f"unknown precision {precision!r}; expected one of {sorted(PRECISIONS)}") from None
+
+
 class Workspace:
     """Device buffers of one problem (``sp_workspace``; native ``_core.Workspace``)."""
 
-    def __init__(self, problem: Problem, device: int = 0):
+    def __init__(self, problem: Problem, device: int = 0, precision: str = "fp64"):
         self.handle = None
+        self._lib = library()
         self.problem = problem
+        self.precision = precision
         handle = C.c_void_p()
-        check(library().sp_workspace_create(problem.handle, device, C.byref(handle)))
+        check(library().sp_workspace_create_ex(problem.handle, device, precision_code(precision),
+                                               C.byref(handle)))
         self.handle = handle
         self.shape = (problem.record.n_modes, problem.record.n_pol, problem.record.n_omega)
 
@@ -373,7 +391,7 @@ class Workspace:
 
     def close(self):
         if getattr(self, "handle", None):
-            library().sp_workspace_destroy(self.handle)
+            self._lib.sp_workspace_destroy(self.handle)
             self.handle = None
 
     __del__ = close
@@ -384,6 +402,7 @@ class Session:
 
     def __init__(self, ws: Workspace, policy: dict, *, field0=None, schedule=None):
         self.handle = None
+        self._lib = library()
         self.ws = ws
         desc, keep = run_desc(ws.problem.record, policy, field0=field0, schedule=schedule)
         handle = C.c_void_p()
@@ -413,7 +432,7 @@ class Session:
 
     def close(self):
         if getattr(self, "handle", None):
-            library().sp_session_destroy(self.handle)
+            self._lib.sp_session_destroy(self.handle)
             self.handle = None
 
     __del__ = close
@@ -422,8 +441,10 @@ class Session:
 class Scan:
     """Many independent runs stepped together on one device (``sp_scan``)."""
 
-    def __init__(self, records, policies, device: int = 0):
+    def __init__(self, records, policies, device: int = 0, precision: str = "fp64"):
         self.handle = None
+        self._lib = library()
+        self.precision = precision
         self.records = list(records)
         self.problems = [Problem(r) for r in self.records]
         descs, self._keep = [], []
@@ -435,7 +456,8 @@ class Scan:
         handles = (C.c_void_p * n)(*[p.handle.value for p in self.problems])
         runs = (SpRunDesc * n)(*descs)
         handle = C.c_void_p()
-        check(library().sp_scan_create(n, handles, runs, device, C.byref(handle)))
+        check(library().sp_scan_create_ex(n, handles, runs, device, precision_code(precision),
+                                          C.byref(handle)))
         self.handle = handle
         self.status = SpScanStatus()
 
@@ -457,7 +479,7 @@ class Scan:
 
     def close(self):
         if getattr(self, "handle", None):
-            library().sp_scan_destroy(self.handle)
+            self._lib.sp_scan_destroy(self.handle)
             self.handle = None
 
     __del__ = close

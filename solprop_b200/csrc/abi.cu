@@ -195,6 +195,12 @@ struct sp_workspace {
   DevBuf<long long> crop;
   DevBuf<int> fine_to_coarse, rows, chain_flags;
   DevBuf<unsigned long long> ticket;  // the response column's tile counter
+  // the mixed-precision form's FP32 copies of the source evaluation's buffers
+  int precision = SP_PRECISION_FP64;
+  struct {
+    DevBuf<float2> twiddles, spectra;
+    DevBuf<float> t_window, t_window_d, synthesis, projection, rate_coeff, taps, proj;
+  } f32;
   DevBuf<unsigned char> active, norm;
   DevBuf<StageScalarsDev> stage;   // kStageSlots slots
   StageScalarsDev* h_stage = nullptr;  // pinned
@@ -291,7 +297,32 @@ static void upload_stages(sp_workspace* ws, int count) {
                              cudaMemcpyHostToDevice, ws->stream));
 }
 
-// The argument records of one source evaluation on a workspace.
+// The buffers one source evaluation reads and writes, in the evaluation's real type.
+template <class R>
+struct SourceView {
+  const cplx<R>* twiddles;
+  cplx<R>* spectra;
+  const R *t_window, *t_window_d, *synthesis, *projection, *rate_coeff, *taps;
+  R* proj;
+};
+
+template <class R>
+static SourceView<R> source_view(const sp_workspace* ws);
+template <>
+SourceView<double> source_view<double>(const sp_workspace* ws) {
+  return {ws->twiddles.p, ws->spectra.p, ws->t_window.p, ws->t_window_d.p, ws->synthesis.p,
+          ws->projection.p, ws->rate_coeff.p, ws->taps.p, ws->proj.p};
+}
+template <>
+SourceView<float> source_view<float>(const sp_workspace* ws) {
+  const auto& f = ws->f32;
+  return {f.twiddles.p, f.spectra.p, f.t_window.p, f.t_window_d.p, f.synthesis.p,
+          f.projection.p, f.rate_coeff.p, f.taps.p, f.proj.p};
+}
+
+// The argument records of one source evaluation on a workspace.  The inverse transform
+// is FP64 in both forms (the FP32 noise floor of the modal field would swamp the
+// absorber's stream, which lives where the field is weak).
 static InverseArgs inverse_args(const sp_workspace* ws, const double2* lab, bool absorber) {
   const sp_problem& P = *ws->P;
   const sp_problem_desc& d = P.d;
@@ -300,22 +331,24 @@ static InverseArgs inverse_args(const sp_workspace* ws, const double2* lab, bool
                      ws->alpha.p, d.n_omega, d.n_to, ws->log_m, ws->log_n_to, P.crop_identity};
 }
 
-static ColumnTileArgs column_args(const sp_workspace* ws, const StageScalarsDev* stage) {
+template <class R = double>
+static ColumnArgsT<R> column_args(const sp_workspace* ws, const StageScalarsDev* stage) {
   const sp_problem& P = *ws->P;
   const sp_problem_desc& d = P.d;
-  ColumnTileArgs ca{};
+  const SourceView<R> v = source_view<R>(ws);
+  ColumnArgsT<R> ca{};
   ca.stage = stage;
   ca.modal_t = ws->modal_t.p;
-  ca.synthesis = ws->synthesis.p;
-  ca.projection = ws->projection.p;
-  ca.t_window = ws->t_window.p;
-  ca.t_window_derivative = ws->t_window_d.p;
+  ca.synthesis = v.synthesis;
+  ca.projection = v.projection;
+  ca.t_window = v.t_window;
+  ca.t_window_derivative = v.t_window_d;
   ca.sums0 = ws->sums0.p;
   ca.sums1 = ws->sums1.p;
   ca.ticket = ws->ticket.p;
   ca.flags = ws->chain_flags.p;
   ca.status = ws->norms.p + kColumnStatus;
-  ca.partials = ws->proj.p;
+  ca.partials = v.proj;
   ca.n_modes = d.n_modes;
   ca.n_nodes = d.n_nodes;
   ca.n_cols = P.n_cols;
@@ -337,8 +370,8 @@ static ColumnTileArgs column_args(const sp_workspace* ws, const StageScalarsDev*
   ca.field_min = d.field_min;
   ca.field_max = d.field_max;
   ca.rate_max = d.rate_max;
-  ca.rate_coefficients = ws->rate_coeff.p;
-  ca.taps = ws->taps.p;
+  ca.rate_coefficients = v.rate_coeff;
+  ca.taps = v.taps;
   return ca;
 }
 
@@ -349,20 +382,24 @@ static int forward_rows(const sp_workspace* ws, bool absorber) {
   return (P.d.plasma_enabled ? 3 * P.n_cols : P.n_cols) + (absorber ? P.n_cols : 0);
 }
 
-static ForwardArgs forward_args(const sp_workspace* ws) {
+template <class R = double>
+static ForwardArgsT<R> forward_args(const sp_workspace* ws) {
   const sp_problem& P = *ws->P;
   const sp_problem_desc& d = P.d;
   const int nc = P.n_cols;
-  return ForwardArgs{ws->streams.p, ws->proj.p, (d.n_nodes + kGroup - 1) / kGroup, 3 * nc,
-                     d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
-                     ws->crop.p, ws->twiddles.p, ws->spectra.p, d.n_to, d.n_omega, ws->log_m,
-                     ws->log_n_to, P.crop_identity};
+  const SourceView<R> v = source_view<R>(ws);
+  return ForwardArgsT<R>{ws->streams.p, v.proj, (d.n_nodes + kGroup - 1) / kGroup, 3 * nc,
+                         d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
+                         ws->crop.p, v.twiddles, v.spectra, d.n_to, d.n_omega, ws->log_m,
+                         ws->log_n_to, P.crop_identity};
 }
 
 static OutputArgs output_args(const sp_workspace* ws, const StageScalarsDev* stage,
                               const double2* inv_prop, double2* out, bool absorber) {
   const sp_problem& P = *ws->P;
-  return OutputArgs{stage, ws->spectra.p, ws->pre_terms.p, ws->omega.p, ws->omega_window.p,
+  return OutputArgs{stage, ws->spectra.p,
+                    ws->precision == SP_PRECISION_MIXED ? ws->f32.spectra.p : nullptr,
+                    ws->pre_terms.p, ws->omega.p, ws->omega_window.p,
                     ws->active.p, inv_prop, out, P.n_cols, P.d.n_omega, P.d.plasma_enabled,
                     absorber};
 }
@@ -372,14 +409,74 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
                         double2* out, bool quiet) {
   const sp_problem& P = *ws->P;
   const bool absorber = P.d.absorber_in_stage && !quiet;
-  const InverseArgs ia = inverse_args(ws, lab, absorber);
-  { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
-  const ColumnTileArgs ca = column_args(ws, ws->stage.p + slot);
-  { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column(ca, ws->stream)); }
-  const ForwardArgs fa = forward_args(ws);
-  { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
+  if (ws->precision == SP_PRECISION_MIXED) {
+    const auto ia = inverse_args(ws, lab, absorber);
+    { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
+    const auto ca = column_args<float>(ws, ws->stage.p + slot);
+    { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column(ca, ws->stream)); }
+    const auto fa = forward_args<float>(ws);
+    { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
+  } else {
+    const auto ia = inverse_args(ws, lab, absorber);
+    { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
+    const auto ca = column_args<double>(ws, ws->stage.p + slot);
+    { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column(ca, ws->stream)); }
+    const auto fa = forward_args<double>(ws);
+    { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
+  }
   const OutputArgs oa = output_args(ws, ws->stage.p + slot, inv_prop, out, absorber);
   { KernelTimer t(ws, SP_K_OUTPUT); CUDA_CHECK(launch_output(oa, ws->stream)); }
+}
+
+template <class T>
+static std::vector<float> to_float(const std::vector<T>& v) {
+  return std::vector<float>(v.begin(), v.end());
+}
+
+// The mixed-precision form's FP32 tables and buffers.  The rate table becomes (c0, c1,
+// c2, exp c3, 1 / knot) per interval, the form the FP32 lookup evaluates.
+static void build_mixed(sp_workspace* ws, const std::vector<double2>& tw, const std::vector<double>& rc,
+                        const std::vector<double>& taps) {
+  const sp_problem& P = *ws->P;
+  const sp_problem_desc& d = P.d;
+  cudaStream_t s = ws->stream;
+  auto& f = ws->f32;
+  std::vector<float2> tw32(tw.size());
+  for (size_t m = 0; m < tw.size(); ++m) tw32[m] = make_float2((float)tw[m].x, (float)tw[m].y);
+  f.twiddles.upload(tw32.data(), tw32.size(), s);
+  auto up = [&](DevBuf<float>& dst, const std::vector<float>& v) { dst.upload(v.data(), v.size(), s); };
+  // the uploads are asynchronous: keep the host copies alive until the stream is synchronised
+  std::vector<std::vector<float>> keep;
+  keep.reserve(8);
+  keep.push_back(to_float(P.t_window));
+  up(f.t_window, keep.back());
+  keep.push_back(to_float(P.t_window_d));
+  up(f.t_window_d, keep.back());
+  keep.push_back(to_float(P.synthesis));
+  up(f.synthesis, keep.back());
+  keep.push_back(to_float(P.projection));
+  up(f.projection, keep.back());
+  keep.push_back(to_float(taps));
+  up(f.taps, keep.back());
+  const int n = std::max(d.rate_intervals, 1);
+  std::vector<float> r32((size_t)5 * n, 0.0f);
+  if (rc.size() >= (size_t)4 * n) {
+    for (int i = 0; i < n; ++i) {
+      r32[i] = (float)rc[i];
+      r32[n + i] = (float)rc[n + i];
+      r32[2 * n + i] = (float)rc[2 * n + i];
+      r32[3 * n + i] = (float)std::exp(rc[3 * n + i]);
+      r32[4 * n + i] = (float)std::exp(-(d.log_field_min + (double)i * d.d_log_field));
+    }
+  }
+  keep.push_back(std::move(r32));
+  up(f.rate_coeff, keep.back());
+  const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
+  f.proj.alloc(n_groups * 3 * P.n_cols * d.n_to);
+  f.proj.zero(s);
+  f.spectra.alloc((size_t)4 * P.n);
+  f.spectra.zero(s);
+  CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
 static void build_workspace(sp_workspace* ws) {
@@ -451,6 +548,7 @@ static void build_workspace(sp_workspace* ws) {
   ws->norms.alloc(kMaxOrders + 2);
   ws->norms.zero(s);
   ws->launches = 5;
+  if (ws->precision == SP_PRECISION_MIXED) build_mixed(ws, tw, rc, taps);
   CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
@@ -1058,8 +1156,15 @@ sp_status sp_problem_destroy(sp_problem* p) {
 }
 
 sp_status sp_workspace_create(const sp_problem* problem, int device, sp_workspace** out) {
+  return sp_workspace_create_ex(problem, device, SP_PRECISION_FP64, out);
+}
+
+sp_status sp_workspace_create_ex(const sp_problem* problem, int device, int precision,
+                                 sp_workspace** out) {
   return guarded([&] {
     if (!problem || !out) throw Failure(SP_ERR_ARGUMENT, "NULL problem or out");
+    if (precision != SP_PRECISION_FP64 && precision != SP_PRECISION_MIXED)
+      throw Failure(SP_ERR_ARGUMENT, "unknown precision");
     CUDA_CHECK(cudaSetDevice(device));
     static bool configured = false;
     if (!configured) {
@@ -1069,6 +1174,7 @@ sp_status sp_workspace_create(const sp_problem* problem, int device, sp_workspac
     auto ws = std::make_unique<sp_workspace>();
     ws->P = problem;
     ws->device = device;
+    ws->precision = precision;
     CUDA_CHECK(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
     build_workspace(ws.get());
     *out = ws.release();
@@ -1292,9 +1398,12 @@ struct sp_scan {
   std::vector<std::unique_ptr<sp_session>> ss;
   std::vector<int> done;
   std::vector<Pending> pending;
+  int precision = SP_PRECISION_FP64;
   DevBuf<InverseArgs> inv_start, inv_att;
   DevBuf<ColumnTileArgs> col_start, col_att;
   DevBuf<ForwardArgs> fwd;
+  DevBuf<ColumnArgsT<float>> col32_start, col32_att;
+  DevBuf<ForwardArgsT<float>> fwd32;
   DevBuf<OutputArgs> out_start, out_att;
   DevBuf<StepArgs> step_start, step_att;
   DevBuf<AdamsDev> adams_start, adams_att;
@@ -1329,25 +1438,34 @@ void upload_all(DevBuf<T>& dev, const T* host, size_t n, cudaStream_t s) {
   CUDA_CHECK(cudaMemcpyAsync(dev.p, host, n * sizeof(T), cudaMemcpyHostToDevice, s));
 }
 
+template <class R>
+void scan_transforms(sp_scan* S, const int* flags, const InverseArgs* inv, const ColumnArgsT<R>* col,
+                     const ForwardArgsT<R>* fwd) {
+  for (auto& c : S->classes) {
+    if (c->cluster)
+      CUDA_CHECK(launch_inverse_cluster_b(inv, c->inv_items.p, flags, c->n_inv, c->n_to, S->stream));
+    else
+      CUDA_CHECK(launch_inverse_b(inv, c->inv_items.p, flags, c->n_inv, c->n_to, S->stream));
+  }
+  CUDA_CHECK(launch_column_b(col, S->col_items.p, flags, S->n_col_items, S->stream));
+  for (auto& c : S->classes) {
+    if (c->cluster)
+      CUDA_CHECK(launch_forward_cluster_b(fwd, c->fwd_items.p, flags, c->n_fwd, c->n_to, S->stream));
+    else
+      CUDA_CHECK(launch_forward_b(fwd, c->fwd_items.p, flags, c->n_fwd, c->n_to, S->stream));
+  }
+}
+
 void scan_source(sp_scan* S, bool start) {
-  const DevBuf<int>& flags = start ? S->flag_start : S->flag_att;
-  const DevBuf<InverseArgs>& inv = start ? S->inv_start : S->inv_att;
-  const DevBuf<ColumnTileArgs>& col = start ? S->col_start : S->col_att;
+  const int* flags = start ? S->flag_start.p : S->flag_att.p;
+  if (S->precision == SP_PRECISION_MIXED)
+    scan_transforms(S, flags, start ? S->inv_start.p : S->inv_att.p,
+                    start ? S->col32_start.p : S->col32_att.p, S->fwd32.p);
+  else
+    scan_transforms(S, flags, start ? S->inv_start.p : S->inv_att.p,
+                    start ? S->col_start.p : S->col_att.p, S->fwd.p);
   const DevBuf<OutputArgs>& out = start ? S->out_start : S->out_att;
-  for (auto& c : S->classes) {
-    if (c->cluster)
-      CUDA_CHECK(launch_inverse_cluster_b(inv.p, c->inv_items.p, flags.p, c->n_inv, c->n_to, S->stream));
-    else
-      CUDA_CHECK(launch_inverse_b(inv.p, c->inv_items.p, flags.p, c->n_inv, c->n_to, S->stream));
-  }
-  CUDA_CHECK(launch_column_b(col.p, S->col_items.p, flags.p, S->n_col_items, S->stream));
-  for (auto& c : S->classes) {
-    if (c->cluster)
-      CUDA_CHECK(launch_forward_cluster_b(S->fwd.p, c->fwd_items.p, flags.p, c->n_fwd, c->n_to, S->stream));
-    else
-      CUDA_CHECK(launch_forward_b(S->fwd.p, c->fwd_items.p, flags.p, c->n_fwd, c->n_to, S->stream));
-  }
-  CUDA_CHECK(launch_output_b(out.p, S->out_items.p, flags.p, S->n_out_items, S->stream));
+  CUDA_CHECK(launch_output_b(out.p, S->out_items.p, flags, S->n_out_items, S->stream));
 }
 
 void scan_step(sp_scan* S) {
@@ -1438,8 +1556,15 @@ extern "C" {
 
 sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, const sp_run_desc* runs,
                          int device, sp_scan** out) {
+  return sp_scan_create_ex(n_runs, problems, runs, device, SP_PRECISION_FP64, out);
+}
+
+sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, const sp_run_desc* runs,
+                            int device, int precision, sp_scan** out) {
   return guarded([&] {
     if (n_runs < 1 || !problems || !runs || !out) throw Failure(SP_ERR_ARGUMENT, "bad scan arguments");
+    if (precision != SP_PRECISION_FP64 && precision != SP_PRECISION_MIXED)
+      throw Failure(SP_ERR_ARGUMENT, "unknown precision");
     CUDA_CHECK(cudaSetDevice(device));
     static bool configured = false;
     if (!configured) {
@@ -1448,6 +1573,7 @@ sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, cons
     }
     auto S = std::make_unique<sp_scan>();
     S->device = device;
+    S->precision = precision;
     S->R = n_runs;
     CUDA_CHECK(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
     const int R = n_runs;
@@ -1459,6 +1585,7 @@ sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, cons
       auto w = std::make_unique<sp_workspace>();
       w->P = problems[r];
       w->device = device;
+      w->precision = precision;
       CUDA_CHECK(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
       build_workspace(w.get());
       sp_session* raw = nullptr;
@@ -1490,6 +1617,8 @@ sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, cons
     std::vector<InverseArgs> is(R), ia(R);
     std::vector<ColumnTileArgs> cs(R), ca(R);
     std::vector<ForwardArgs> fa(R);
+      std::vector<ColumnArgsT<float>> cs32(R), ca32(R);
+    std::vector<ForwardArgsT<float>> fa32(R);
     std::vector<OutputArgs> os(R), oa(R);
     std::vector<StepArgs> ts(R), ta(R);
     std::vector<int2> step_items, out_items;
@@ -1505,6 +1634,12 @@ sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, cons
       ca[r] = column_args(w, S->stages_att.p + 2 * r + 1);
       cs[r].status = ca[r].status = S->norms.p + 8 * r + kColumnStatus;
       fa[r] = forward_args(w);
+      if (precision == SP_PRECISION_MIXED) {
+        cs32[r] = column_args<float>(w, S->stages_start.p + r);
+        ca32[r] = column_args<float>(w, S->stages_att.p + 2 * r + 1);
+        cs32[r].status = ca32[r].status = S->norms.p + 8 * r + kColumnStatus;
+        fa32[r] = forward_args<float>(w);
+      }
       os[r] = output_args(w, S->stages_start.p + r, nullptr, w->src.p, absorber);
       oa[r] = output_args(w, S->stages_att.p + 2 * r + 1, nullptr, w->src.p, absorber);
       const int nb = std::min(kNormBlocks, (P.n + 255) / 256);
@@ -1542,6 +1677,11 @@ sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems, cons
     S->col_start.upload(cs.data(), R, S->stream);
     S->col_att.upload(ca.data(), R, S->stream);
     S->fwd.upload(fa.data(), R, S->stream);
+    if (precision == SP_PRECISION_MIXED) {
+      S->col32_start.upload(cs32.data(), R, S->stream);
+      S->col32_att.upload(ca32.data(), R, S->stream);
+      S->fwd32.upload(fa32.data(), R, S->stream);
+    }
     S->out_start.upload(os.data(), R, S->stream);
     S->out_att.upload(oa.data(), R, S->stream);
     S->step_start.upload(ts.data(), R, S->stream);

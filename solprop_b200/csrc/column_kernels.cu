@@ -25,16 +25,19 @@ constexpr int kThreads = 256;
 constexpr int kLanes = kThreads / kGroup;    // threads per node (16)
 constexpr int kPer = kSeg / kLanes;          // samples of the tile per thread (4)
 constexpr int kI0 = 2 * kHalo + 1;           // local index of t0
-constexpr size_t kRowBytes = sizeof(double) * kGroup * kLen;
-constexpr size_t kModalBytes = sizeof(double) * kMaxModes * kLen;
-constexpr size_t kChainSmem = 5 * kRowBytes + kModalBytes;
+// dynamic shared memory of one tile: five node rows and the staged modal field
+template <class R>
+constexpr size_t chain_smem() {
+  return sizeof(R) * (5 * kGroup * kLen + kMaxModes * kLen);
+}
 
 struct Tile {
   int t0, n0, nodes, tile;
   int node, lane;  // this thread's node within the group (thread / kLanes) and lane
 };
 
-__device__ __forceinline__ Tile tile_of(const ColumnTileArgs& a, int tile, int group) {
+template <class R>
+__device__ __forceinline__ Tile tile_of(const ColumnArgsT<R>& a, int tile, int group) {
   Tile c;
   c.tile = tile;
   c.t0 = tile * kSeg;
@@ -47,7 +50,7 @@ __device__ __forceinline__ Tile tile_of(const ColumnTileArgs& a, int tile, int g
 
 __device__ __forceinline__ int local_of(int t, int t0) { return t - t0 + kI0; }
 
-__device__ __forceinline__ double rate_of(const ColumnTileArgs& a, double magnitude) {
+__device__ __forceinline__ double rate_of(const ColumnArgsT<double>& a, double magnitude) {
   if (magnitude > a.field_max) return a.rate_max;
   if (!(magnitude >= a.field_min)) return 0.0;
   const double lf = log(magnitude);
@@ -60,35 +63,53 @@ __device__ __forceinline__ double rate_of(const ColumnTileArgs& a, double magnit
   return exp(((c[idx] * local + c[n + idx]) * local + c[2 * n + idx]) * local + c[3 * n + idx]);
 }
 
+// The same lookup in FP32.  Its table is (c0, c1, c2, exp c3, 1 / knot) per interval, the
+// knot being the field at the interval's start, so that W = exp(c3) exp(((c0 l + c1) l +
+// c2) l) with l = log1p(|E| / knot - 1): no large logarithm or exponent is rounded to
+// FP32, and the error of W is that of |E| times the rate's slope d log W / d log |E|.
+__device__ __forceinline__ float rate_of(const ColumnArgsT<float>& a, float magnitude) {
+  if (magnitude > (float)a.field_max) return (float)a.rate_max;
+  if (!(magnitude >= (float)a.field_min)) return 0.0f;
+  const int n = a.rate_intervals;
+  const float pos = (__logf(magnitude) - (float)a.log_field_min) * (float)(1.0 / a.d_log_field);
+  int idx = (int)pos;
+  if (idx < 0) idx = 0;
+  if (idx > n - 1) idx = n - 1;
+  const float* c = a.rate_coefficients;
+  const float local = log1pf(fmaf(magnitude, c[4 * n + idx], -1.0f));
+  return c[3 * n + idx] * expf(((c[idx] * local + c[n + idx]) * local + c[2 * n + idx]) * local);
+}
+
 // Stage the modal field a[m][t] for the tile's local range, then synthesise E and the
 // rate W on local indices [lo, hi) of every node (each thread: its node, every 16th).
-__device__ void field_and_rate(const ColumnTileArgs& a, const Tile& c, double* modal, double* E,
-                               double* W, int lo, int hi, bool need_rate) {
+template <class R>
+__device__ void field_and_rate(const ColumnArgsT<R>& a, const Tile& c, R* modal, R* E, R* W, int lo,
+                               int hi, bool need_rate) {
   const int base = c.t0 - kI0;
   for (int m = 0; m < a.n_modes; ++m) {
     for (int i = threadIdx.x; i < kLen; i += blockDim.x) {
       const int t = base + i;
-      modal[m * kLen + i] = (t >= 0 && t < a.n_to) ? a.modal_t[(size_t)m * a.n_to + t] : 0.0;
+      modal[m * kLen + i] = (t >= 0 && t < a.n_to) ? R(a.modal_t[(size_t)m * a.n_to + t]) : R(0);
     }
   }
   __syncthreads();
   if (c.node < c.nodes) {
-    const double tau = a.stage->taper;
-    double srow[kMaxModes];
-    const double* sp = a.synthesis + (c.n0 + c.node) * a.n_modes;
+    const R tau = R(a.stage->taper);
+    R srow[kMaxModes];
+    const R* sp = a.synthesis + (c.n0 + c.node) * a.n_modes;
 #pragma unroll
-    for (int m = 0; m < kMaxModes; ++m) srow[m] = m < a.n_modes ? sp[m] * tau : 0.0;
-    double* e_row = E + c.node * kLen;
-    double* w_row = W + c.node * kLen;
+    for (int m = 0; m < kMaxModes; ++m) srow[m] = m < a.n_modes ? sp[m] * tau : R(0);
+    R* e_row = E + c.node * kLen;
+    R* w_row = W + c.node * kLen;
     for (int i = lo + c.lane; i < hi; i += kLanes) {
-      double e = 0.0;
+      R e = R(0);
 #pragma unroll
       for (int m = 0; m < kMaxModes; ++m)
         if (m < a.n_modes) e += srow[m] * modal[m * kLen + i];
       e_row[i] = e;
       if (need_rate) {
         const int t = base + i;
-        w_row[i] = (t >= 0 && t < a.n_to) ? rate_of(a, fabs(e)) : 0.0;
+        w_row[i] = (t >= 0 && t < a.n_to) ? rate_of(a, fabs(e)) : R(0);
       }
     }
   }
@@ -96,26 +117,28 @@ __device__ void field_and_rate(const ColumnTileArgs& a, const Tile& c, double* m
 }
 
 // point reflection at the row's ends: y[-m] = 2 y[0] - y[m], y[N-1+m] = 2 y[N-1] - y[N-1-m]
-__device__ __forceinline__ double reflected(const double* y, int t, int t0, int n_to) {
-  if (t < 0) return 2.0 * y[local_of(0, t0)] - y[local_of(-t, t0)];
+template <class R>
+__device__ __forceinline__ R reflected(const R* y, int t, int t0, int n_to) {
+  if (t < 0) return R(2) * y[local_of(0, t0)] - y[local_of(-t, t0)];
   if (t > n_to - 1) {
     const int m = t - (n_to - 1);
-    return 2.0 * y[local_of(n_to - 1, t0)] - y[local_of(n_to - 1 - m, t0)];
+    return R(2) * y[local_of(n_to - 1, t0)] - y[local_of(n_to - 1 - m, t0)];
   }
   return y[local_of(t, t0)];
 }
 
 // filtered value c0 y[t] + sum_k c_k (y[t-k] + y[t+k]), centre first, pairs in k order
-__device__ __forceinline__ double filtered(const ColumnTileArgs& a, const double* y, int t, int t0) {
-  const double* c = a.taps;
+template <class R>
+__device__ __forceinline__ R filtered(const ColumnArgsT<R>& a, const R* y, int t, int t0) {
+  const R* c = a.taps;
   const bool inside = t - a.half_width >= 0 && t + a.half_width <= a.n_to - 1;
   if (inside) {
-    const double* p = y + local_of(t, t0);
-    double f = c[0] * p[0];
+    const R* p = y + local_of(t, t0);
+    R f = c[0] * p[0];
     for (int k = 1; k <= a.half_width; ++k) f = f + c[k] * (p[-k] + p[k]);
     return f;
   }
-  double f = c[0] * reflected(y, t, t0, a.n_to);
+  R f = c[0] * reflected(y, t, t0, a.n_to);
   for (int k = 1; k <= a.half_width; ++k)
     f = f + c[k] * (reflected(y, t - k, t0, a.n_to) + reflected(y, t + k, t0, a.n_to));
   return f;
@@ -123,23 +146,25 @@ __device__ __forceinline__ double filtered(const ColumnTileArgs& a, const double
 
 // inc[t] = dt (y~[t] + y~[t+1]) / 2 for t in [lo, hi) (zero at the last sample and outside);
 // ytil is scratch for y~ on [lo, hi].  Positions are global samples.
-__device__ void increments(const ColumnTileArgs& a, const Tile& c, const double* y, double* ytil,
-                           double* inc, int lo, int hi) {
+template <class R>
+__device__ void increments(const ColumnArgsT<R>& a, const Tile& c, const R* y, R* ytil, R* inc, int lo,
+                           int hi) {
   if (c.node < c.nodes) {
-    const double* y_row = y + c.node * kLen;
-    double* yt = ytil + c.node * kLen;
+    const R* y_row = y + c.node * kLen;
+    R* yt = ytil + c.node * kLen;
     for (int t = lo + c.lane; t <= hi; t += kLanes)
       if (t >= 0 && t < a.n_to) yt[local_of(t, c.t0)] = filtered(a, y_row, t, c.t0);
   }
   __syncthreads();
   if (c.node < c.nodes) {
-    const double* yt = ytil + c.node * kLen;
-    double* o = inc + c.node * kLen;
+    const R* yt = ytil + c.node * kLen;
+    R* o = inc + c.node * kLen;
     const int last = a.n_to - 1;
+    const R dt = R(a.dt);
     for (int i = c.lane; i < kLen; i += kLanes) {
       const int t = c.t0 - kI0 + i;
-      double v = 0.0;
-      if (t >= lo && t < hi && t >= 0 && t < last) v = a.dt * (yt[i + 1] + yt[i]) / 2.0;
+      R v = R(0);
+      if (t >= lo && t < hi && t >= 0 && t < last) v = dt * (yt[i + 1] + yt[i]) / R(2);
       o[i] = v;
     }
   }
@@ -162,10 +187,11 @@ __device__ __forceinline__ double lanes_total(double v) {
   return v;
 }
 
-// The tile's sum of increments over [t0, t1), per node; lane 0 writes it.
-__device__ void tile_sum(const Tile& c, const double* inc, double* out, int n_tiles) {
+// The tile's sum of increments over [t0, t1), per node, in FP64; lane 0 writes it.
+template <class R>
+__device__ void tile_sum(const Tile& c, const R* inc, double* out, int n_tiles) {
   double s = 0.0;
-  const double* in = inc + c.node * kLen + kI0 + c.lane * kPer;
+  const R* in = inc + c.node * kLen + kI0 + c.lane * kPer;
 #pragma unroll
   for (int q = 0; q < kPer; ++q) s += in[q];
   s = lanes_total(s);
@@ -175,7 +201,9 @@ __device__ void tile_sum(const Tile& c, const double* inc, double* out, int n_ti
 // The running integral on [t0 - H, t1 + H] of this thread's node, into out: the
 // increments on [t0 - H, t1 + H) scanned across the node's lanes, anchored so that
 // out[t0] = offset.  Each lane scans 5 consecutive samples (kSeg + 2H = 80 = 16 x 5).
-__device__ void rescan(const Tile& c, const double* inc, double* out, double offset) {
+// The sums are FP64 whatever the rows' type (the mixed form's compensated integral).
+template <class R>
+__device__ void rescan(const Tile& c, const R* inc, R* out, double offset) {
   constexpr int kSpan = kSeg + 2 * kHalo;
   constexpr int kEach = kSpan / kLanes;
   static_assert(kSpan % kLanes == 0, "rescan span");
@@ -205,8 +233,8 @@ __device__ void rescan(const Tile& c, const double* inc, double* out, double off
   const double at_t0 = __shfl_sync(0xffffffffu, pref[kQ0], kL0, kLanes);
   if (n < c.nodes) {
 #pragma unroll
-    for (int q = 0; q < kEach; ++q) out[n * kLen + first + q] = offset + (pref[q] - at_t0);
-    if (c.lane == kLanes - 1) out[n * kLen + first + kEach] = offset + (pref[kEach] - at_t0);
+    for (int q = 0; q < kEach; ++q) out[n * kLen + first + q] = R(offset + (pref[q] - at_t0));
+    if (c.lane == kLanes - 1) out[n * kLen + first + kEach] = R(offset + (pref[kEach] - at_t0));
   }
   __syncthreads();
 }
@@ -231,7 +259,8 @@ __device__ __forceinline__ void store_release(int* p, int v) {
 }
 
 // publish this tile's sums (already written by the nodes' lane 0) as stage `target`
-__device__ __forceinline__ void publish(const ColumnTileArgs& a, const Tile& c, int group, int target) {
+template <class R>
+__device__ __forceinline__ void publish(const ColumnArgsT<R>& a, const Tile& c, int group, int target) {
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) store_release(a.flags + (size_t)group * a.n_tiles + c.tile, target);
@@ -239,7 +268,8 @@ __device__ __forceinline__ void publish(const ColumnTileArgs& a, const Tile& c, 
 
 // wait until every earlier tile of the group has published stage `target`; a wait that
 // gives up marks the evaluation failed in *status (read by the host) and goes on
-__device__ __forceinline__ void await_predecessors(const ColumnTileArgs& a, const Tile& c, int group,
+template <class R>
+__device__ __forceinline__ void await_predecessors(const ColumnArgsT<R>& a, const Tile& c, int group,
                                                    int target) {
   const int* f = a.flags + (size_t)group * a.n_tiles;
   for (int j = threadIdx.x; j < c.tile; j += blockDim.x) {
@@ -275,6 +305,15 @@ __device__ double predecessors_cg(const Tile& c, const double* sums, int n_tiles
   return lanes_total(s);
 }
 
+// the ionised fraction f = 1 - (1 - f0) e^-x (plasma.py:104-191); in FP32 as
+// f0 + (1 - f0)(1 - e^-x) through expm1, which keeps its relative accuracy for small x
+__device__ __forceinline__ double fraction(double f0, double x) {
+  return 1.0 - (1.0 - f0) * (x == 0.0 ? 1.0 : exp(-x));
+}
+__device__ __forceinline__ float fraction(float f0, float x) {
+  return fmaf(1.0f - f0, -expm1f(-x), f0);
+}
+
 }  // namespace
 
 // One tile of the column, start to finish: synthesis and rate on the tile and its halo,
@@ -282,14 +321,15 @@ __device__ double predecessors_cg(const Tile& c, const double* sums, int n_tiles
 // predecessors' sums, the fraction and the current's increments and tile sum (published),
 // the current from the predecessors' sums, then the total current, Kerr, the collar and
 // the tile projected onto the modes (partial sums per node group).
-__device__ __forceinline__ void chain_body(const ColumnTileArgs& a) {
-  extern __shared__ double dyn[];
-  double* E = dyn;
-  double* W = E + kGroup * kLen;
-  double* F = W + kGroup * kLen;   // exposure, then the fraction in place
-  double* Y1 = F + kGroup * kLen;  // increments
-  double* Y2 = Y1 + kGroup * kLen; // filtered scratch -> running integral
-  double* modal = Y2 + kGroup * kLen;
+template <class R>
+__device__ __forceinline__ void chain_body(const ColumnArgsT<R>& a) {
+  extern __shared__ __align__(16) unsigned char dyn_raw[];
+  R* E = reinterpret_cast<R*>(dyn_raw);
+  R* W = E + kGroup * kLen;
+  R* F = W + kGroup * kLen;   // exposure, then the fraction in place
+  R* Y1 = F + kGroup * kLen;  // increments
+  R* Y2 = Y1 + kGroup * kLen; // filtered scratch -> running integral
+  R* modal = Y2 + kGroup * kLen;
   __shared__ unsigned long long ticket;
   if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1ull);
   __syncthreads();
@@ -308,16 +348,17 @@ __device__ __forceinline__ void chain_body(const ColumnTileArgs& a) {
     await_predecessors(a, c, group, first);
     const double off0 = predecessors_cg(c, a.sums0, a.n_tiles);
     rescan(c, Y1, F, off0);  // F = exposure on [t0 - H, t1 + H]
-    const double f0 = a.stage->preionisation;
+    const R f0 = R(a.stage->preionisation);
+    const R qm = R(a.charge_mass_ratio);
     if (c.node < c.nodes) {
       for (int i = c.lane; i < kLen; i += kLanes) {
         const int idx = c.node * kLen + i;
         const int t = c.t0 - kI0 + i;
-        double f = 0.0, g = 0.0;
+        R f = R(0), g = R(0);
         if (t >= c.t0 - kHalo && t <= c.t0 + kSeg + kHalo && t >= 0 && t < a.n_to) {
-          const double x = a.band ? fmax(F[idx], 0.0) : F[idx];
-          f = 1.0 - (1.0 - f0) * (x == 0.0 ? 1.0 : exp(-x));
-          g = f * a.charge_mass_ratio * E[idx];
+          const R x = a.band ? fmax(F[idx], R(0)) : F[idx];
+          f = fraction(f0, x);
+          g = f * qm * E[idx];
         }
         F[idx] = f;
         Y1[idx] = g;
@@ -333,25 +374,26 @@ __device__ __forceinline__ void chain_body(const ColumnTileArgs& a) {
   }
   // outputs on [t0, t1): P = (c rho E^2 E) g, X = g rho J, Z = g' rho J
   const StageScalarsDev& st = *a.stage;
-  const double factor = a.kerr ? a.kerr_coefficient * st.kerr_density : 0.0;
-  const double rho = st.plasma_density;
-  double outp[kPer], outx[kPer], outz[kPer];
+  const R factor = R(a.kerr ? a.kerr_coefficient * st.kerr_density : 0.0);
+  const R rho = R(st.plasma_density);
+  const R ip = R(a.ionisation_potential);
+  R outp[kPer], outx[kPer], outz[kPer];
 #pragma unroll
   for (int k = 0; k < kPer; ++k) {
     const int q = c.lane * kPer + k;
     const int li = c.node * kLen + kI0 + q;
     const int t = c.t0 + q;
-    double p = 0.0, x = 0.0, z = 0.0;
+    R p = R(0), x = R(0), z = R(0);
     if (c.node < c.nodes && t < a.n_to) {
-      const double e = E[li];
-      const double win = a.t_window[t];
-      p = (a.kerr ? factor * (e * e) * e : 0.0) * win;
+      const R e = E[li];
+      const R win = a.t_window[t];
+      p = (a.kerr ? factor * (e * e) * e : R(0)) * win;
       if (plasma) {
-        const double w = W[li], f = F[li];
-        const double squared = fabs(e) * fabs(e);
-        double scale = 0.0;
-        if (w > 0.0 && squared > 0.0) scale = a.ionisation_potential * w * (1.0 - f) / squared;
-        const double current = rho * (Y2[li] + scale * e);
+        const R w = W[li], f = F[li];
+        const R squared = fabs(e) * fabs(e);
+        R scale = R(0);
+        if (w > R(0) && squared > R(0)) scale = ip * w * (R(1) - f) / squared;
+        const R current = rho * (Y2[li] + scale * e);
         x = win * current;
         z = a.t_window_derivative[t] * current;
       }
@@ -361,9 +403,9 @@ __device__ __forceinline__ void chain_body(const ColumnTileArgs& a) {
     outz[k] = z;
   }
   __syncthreads();
-  double* P = E;  // [node][kSeg] output tiles over the spent rows
-  double* X = W;
-  double* Z = F;
+  R* P = E;  // [node][kSeg] output tiles over the spent rows
+  R* X = W;
+  R* Z = F;
 #pragma unroll
   for (int k = 0; k < kPer; ++k) {
     const int o = c.node * kSeg + c.lane * kPer + k;
@@ -373,14 +415,14 @@ __device__ __forceinline__ void chain_body(const ColumnTileArgs& a) {
   }
   __syncthreads();
   // projection of the tile onto the modes: sum over the group's nodes in node order
-  const double tau = st.taper;
+  const R tau = R(st.taper);
   const int n_streams = plasma ? 3 : 1;
-  const double* rows[3] = {P, X, Z};
+  const R* rows[3] = {P, X, Z};
   // weights W[m, node] / tau of the group, once
-  __shared__ double wt[kMaxModes * kGroup];
+  __shared__ R wt[kMaxModes * kGroup];
   for (int k = threadIdx.x; k < a.n_modes * kGroup; k += blockDim.x) {
     const int m = k / kGroup, n = k % kGroup;
-    wt[k] = n < c.nodes ? a.projection[m * a.n_nodes + c.n0 + n] / tau : 0.0;
+    wt[k] = n < c.nodes ? a.projection[m * a.n_nodes + c.n0 + n] / tau : R(0);
   }
   __syncthreads();
   const int q = threadIdx.x % kSeg;  // sample of the tile
@@ -388,39 +430,53 @@ __device__ __forceinline__ void chain_body(const ColumnTileArgs& a) {
   for (int sm = threadIdx.x / kSeg; sm < n_streams * a.n_modes; sm += kThreads / kSeg) {
     const int s = sm / a.n_modes, m = sm - s * a.n_modes;
     if (t >= a.n_to) continue;
-    const double* row = rows[s];
-    double acc = 0.0;
+    const R* row = rows[s];
+    R acc = R(0);
     for (int n = 0; n < c.nodes; ++n) acc += wt[m * kGroup + n] * row[n * kSeg + q];
     a.partials[(((size_t)group * 3 + s) * a.n_cols + m) * a.n_to + t] = acc;
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 3) k_column(ColumnTileArgs a) { chain_body(a); }
+template <class R>
+__global__ void __launch_bounds__(kThreads, 3) k_column(ColumnArgsT<R> a) { chain_body(a); }
 
 // batched: items[blockIdx.x].x = the run; a run's CTAs take their tiles from its counter
-__global__ void __launch_bounds__(kThreads, 3) k_column_b(const ColumnTileArgs* args, const int4* items,
-                                                       const int* flags) {
+template <class R>
+__global__ void __launch_bounds__(kThreads, 3) k_column_b(const ColumnArgsT<R>* args, const int4* items,
+                                                          const int* flags) {
   const int run = items[blockIdx.x].x;
   if (!flags[run]) return;  // every CTA of an idle run leaves before its ticket
   chain_body(args[run]);
 }
 
-cudaError_t launch_column_b(const ColumnTileArgs* args, const int4* items, const int* flags,
+template <class R>
+cudaError_t launch_column_b(const ColumnArgsT<R>* args, const int4* items, const int* flags,
                             int n_items, cudaStream_t stream) {
-  k_column_b<<<n_items, kThreads, kChainSmem, stream>>>(args, items, flags);
+  k_column_b<R><<<n_items, kThreads, chain_smem<R>(), stream>>>(args, items, flags);
   return cudaGetLastError();
 }
 
-cudaError_t launch_column(const ColumnTileArgs& a, cudaStream_t stream) {
-  k_column<<<a.n_blocks, kThreads, kChainSmem, stream>>>(a);
+template <class R>
+cudaError_t launch_column(const ColumnArgsT<R>& a, cudaStream_t stream) {
+  k_column<R><<<a.n_blocks, kThreads, chain_smem<R>(), stream>>>(a);
   return cudaGetLastError();
 }
+
+template cudaError_t launch_column<double>(const ColumnArgsT<double>&, cudaStream_t);
+template cudaError_t launch_column<float>(const ColumnArgsT<float>&, cudaStream_t);
+template cudaError_t launch_column_b<double>(const ColumnArgsT<double>*, const int4*, const int*, int,
+                                             cudaStream_t);
+template cudaError_t launch_column_b<float>(const ColumnArgsT<float>*, const int4*, const int*, int,
+                                            cudaStream_t);
 
 cudaError_t configure_column_kernels() {
-  const void* kernels[2] = {(const void*)k_column, (const void*)k_column_b};
-  for (int i = 0; i < 2; ++i) {
+  const void* kernels[4] = {(const void*)k_column<double>, (const void*)k_column_b<double>,
+                            (const void*)k_column<float>, (const void*)k_column_b<float>};
+  const size_t shm[4] = {chain_smem<double>(), chain_smem<double>(), chain_smem<float>(),
+                         chain_smem<float>()};
+  for (int i = 0; i < 4; ++i) {
     cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kChainSmem);
+                                         (int)shm[i]);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

@@ -1,4 +1,5 @@
-// A complex FP64 FFT of one row held in shared memory, for power-of-two lengths.
+// A complex FFT (FP64, or FP32 in the mixed-precision form) of one row held in shared
+// memory, for power-of-two lengths.
 //
 // In-place decimation in frequency: natural-order input, bit-reversed output; two
 // radix-2 stages are fused per pass (a radix-4 butterfly in registers), so a 2^13-point
@@ -16,15 +17,17 @@ __device__ __forceinline__ unsigned bitrev(unsigned k, int log_n) {
 }
 
 // w_L^j for the table of n_table entries (stride = n_table / L); conj for inverse.
-__device__ __forceinline__ double2 twiddle(const double2* __restrict__ table, int index,
-                                           bool inverse) {
-  double2 w = __ldg(table + index);
-  return inverse ? make_double2(w.x, -w.y) : w;
+template <class C>
+__device__ __forceinline__ C twiddle(const C* __restrict__ table, int index, bool inverse) {
+  C w = __ldg(table + index);
+  if (inverse) w.y = -w.y;
+  return w;
 }
 
 // In-place DIF FFT of s[0..n) by the whole block; n = 2^log_n <= n_table.
-__device__ __noinline__ static void fft_dif_inplace(double2* s, int log_n, const double2* __restrict__ table,
-                                int log_table, bool inverse) {
+template <class C>
+__device__ __noinline__ static void fft_dif_inplace(C* s, int log_n, const C* __restrict__ table,
+                                                    int log_table, bool inverse) {
   const int n = 1 << log_n;
   int log_len = log_n;
   // radix-4 passes: stages of span L and L/2
@@ -37,15 +40,15 @@ __device__ __noinline__ static void fft_dif_inplace(double2* s, int log_n, const
       const int b = p >> log_q;
       const int j = p & (q - 1);
       const int base = (b << log_len) + j;
-      double2 a0 = s[base], a1 = s[base + q], a2 = s[base + 2 * q], a3 = s[base + 3 * q];
-      const double2 w1 = twiddle(table, j << shift_L, inverse);        // w_L^j
-      const double2 w2 = twiddle(table, (2 * j) << shift_L, inverse);  // w_{L/2}^j
-      double2 t0 = cadd(a0, a2);
-      double2 t2 = cmul(csub(a0, a2), w1);
-      double2 t1 = cadd(a1, a3);
-      double2 d13 = csub(a1, a3);
+      C a0 = s[base], a1 = s[base + q], a2 = s[base + 2 * q], a3 = s[base + 3 * q];
+      const C w1 = twiddle(table, j << shift_L, inverse);        // w_L^j
+      const C w2 = twiddle(table, (2 * j) << shift_L, inverse);  // w_{L/2}^j
+      C t0 = cadd(a0, a2);
+      C t2 = cmul(csub(a0, a2), w1);
+      C t1 = cadd(a1, a3);
+      C d13 = csub(a1, a3);
       // w_L^{j+q} = w_L^j * (-i) forward, (+i) inverse
-      double2 t3 = cmul(inverse ? mul_pi(d13) : mul_mi(d13), w1);
+      C t3 = cmul(inverse ? mul_pi(d13) : mul_mi(d13), w1);
       s[base] = cadd(t0, t1);
       s[base + q] = cmul(csub(t0, t1), w2);
       s[base + 2 * q] = cadd(t2, t3);
@@ -55,7 +58,7 @@ __device__ __noinline__ static void fft_dif_inplace(double2* s, int log_n, const
   }
   if (log_len == 1) {  // one radix-2 stage of span 2, twiddle 1
     for (int p = threadIdx.x; p < (n >> 1); p += blockDim.x) {
-      double2 a = s[2 * p], b = s[2 * p + 1];
+      C a = s[2 * p], b = s[2 * p + 1];
       s[2 * p] = cadd(a, b);
       s[2 * p + 1] = csub(a, b);
     }

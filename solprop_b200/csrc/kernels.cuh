@@ -41,61 +41,73 @@ struct AdamsDev {
   double rate0_w[kMaxTerms];  // D(z) weights (startup)
 };
 
-struct InverseArgs {
-  const double2* lab;            // (n_cols, n_omega)
+// The source evaluation's argument records are templates over the real type R of the
+// forward transforms and the response column: double in the plain form, float in the
+// mixed form, whose inverse transform (the modal field and the absorber's stream), state,
+// propagator phase, accumulation and norms stay FP64.
+template <class R>
+struct InverseArgsT {
+  const double2* lab;            // (n_cols, n_omega), FP64 in both forms
   const int* fine_to_coarse;     // (n_to/2 + 1)
-  const double2* twiddles;       // exp(-2 pi i m / n_to), m < n_to / 2
-  double* modal_t;               // (n_cols, n_to)
-  double* absorber_stream;       // (n_cols, n_to) or null
-  const double* alpha;           // (n_to)
+  const cplx<R>* twiddles;       // exp(-2 pi i m / n_to), m < n_to / 2
+  R* modal_t;                    // (n_cols, n_to)
+  R* absorber_stream;            // (n_cols, n_to) or null
+  const R* alpha;                // (n_to)
   int n_omega, n_to, log_m, log_n_to;
   int crop_identity;             // crop_index[j] == j for every coarse bin
 };
+using InverseArgs = InverseArgsT<double>;
 
 // The tiled response column (column_kernels.cu): tiles of kSeg samples of kGroup nodes.
 constexpr int kSeg = 64;
 constexpr int kGroup = 16;
 constexpr int kHalo = 8;   // the largest band-rule half-width K the tiles carry
 
-struct ColumnTileArgs {
+template <class R>
+struct ColumnArgsT {
   const StageScalarsDev* stage;
-  const double* modal_t;   // (n_modes, n_to)
-  const double* synthesis; // (n_nodes, n_modes)
-  const double* projection;// (n_modes, n_nodes)
-  const double* t_window;
-  const double* t_window_derivative;
+  const double* modal_t;   // (n_modes, n_to), FP64 in both forms
+  const R* synthesis;      // (n_nodes, n_modes)
+  const R* projection;     // (n_modes, n_nodes)
+  const R* t_window;
+  const R* t_window_derivative;
   double* sums0;           // (n_nodes, n_tiles) exposure tile sums
   double* sums1;           // current tile sums
   unsigned long long* ticket;  // tiles handed out so far (n_blocks per evaluation)
   int* flags;              // (n_groups, n_tiles) publication stage of each tile
   double* status;          // set to 1 when a tile gave up waiting
-  double* partials;        // (n_groups, 3, n_cols, n_to) projected streams per node group
+  R* partials;             // (n_groups, 3, n_cols, n_to) projected streams per node group
   int n_modes, n_nodes, n_cols, n_to, n_tiles, n_groups, n_blocks;
   int kerr, plasma, band, half_width, rate_intervals;
   double kerr_coefficient, charge_mass_ratio, ionisation_potential, dt;
   double log_field_min, d_log_field, field_min, field_max, rate_max;
-  const double* rate_coefficients;
-  const double* taps;
+  const R* rate_coefficients;
+  const R* taps;
 };
+using ColumnTileArgs = ColumnArgsT<double>;
 
-cudaError_t launch_column(const ColumnTileArgs& a, cudaStream_t stream);
+template <class R>
+cudaError_t launch_column(const ColumnArgsT<R>& a, cudaStream_t stream);
 cudaError_t configure_column_kernels();
 
-struct ForwardArgs {
-  const double* streams;       // rows of n_to
-  const double* partials;      // (n_groups, n_partial_rows, n_to): summed for rows below
+template <class R>
+struct ForwardArgsT {
+  const double* streams;       // rows of n_to (the absorber's), FP64 in both forms
+  const R* partials;           // (n_groups, n_partial_rows, n_to): summed for rows below
   int n_groups, n_partial_rows;
   const int* rows;             // which rows to transform
   const long long* crop_index; // (n_omega)
-  const double2* twiddles;
-  double2* spectra;            // rows of n_omega
+  const cplx<R>* twiddles;
+  cplx<R>* spectra;            // rows of n_omega
   int n_to, n_omega, log_m, log_n_to;
   int crop_identity;
 };
+using ForwardArgs = ForwardArgsT<double>;
 
 struct OutputArgs {
   const StageScalarsDev* stage;
   const double2* spectra;          // (4, n_cols, n_omega): P, gJ, g'J, absorber
+  const float2* spectra32;         // the same in complex64 (mixed form), else null
   const double2* prefactor_terms;  // (n_pre, n_cols, n_omega)
   const double* omega;
   const double* omega_window;
@@ -107,26 +119,35 @@ struct OutputArgs {
 
 cudaError_t configure_source_kernels();
 int fft_cluster_size(int n_to);
-cudaError_t launch_inverse_cluster(const InverseArgs& a, int n_cols, cudaStream_t stream);
-cudaError_t launch_forward_cluster(const ForwardArgs& a, int n_rows, cudaStream_t stream);
-cudaError_t launch_inverse(const InverseArgs& a, int n_cols, cudaStream_t stream);
-cudaError_t launch_forward(const ForwardArgs& a, int n_rows, cudaStream_t stream);
+template <class R>
+cudaError_t launch_inverse_cluster(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream);
+template <class R>
+cudaError_t launch_forward_cluster(const ForwardArgsT<R>& a, int n_rows, cudaStream_t stream);
+template <class R>
+cudaError_t launch_inverse(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream);
+template <class R>
+cudaError_t launch_forward(const ForwardArgsT<R>& a, int n_rows, cudaStream_t stream);
 cudaError_t launch_output(const OutputArgs& a, cudaStream_t stream);
 
 // ---- batched launches over several runs: items map each block to (run, index)
 cudaError_t configure_cluster_fft();
 // flags[run] != 0 selects the runs a launch serves; other items return at once
-cudaError_t launch_inverse_b(const InverseArgs* args, const int2* items, const int* flags,
+template <class R>
+cudaError_t launch_inverse_b(const InverseArgsT<R>* args, const int2* items, const int* flags,
                              int n_items, int n_to, cudaStream_t stream);
-cudaError_t launch_forward_b(const ForwardArgs* args, const int2* items, const int* flags,
+template <class R>
+cudaError_t launch_forward_b(const ForwardArgsT<R>* args, const int2* items, const int* flags,
                              int n_items, int n_to, cudaStream_t stream);
-cudaError_t launch_inverse_cluster_b(const InverseArgs* args, const int2* items, const int* flags,
+template <class R>
+cudaError_t launch_inverse_cluster_b(const InverseArgsT<R>* args, const int2* items, const int* flags,
                                      int n_items, int n_to, cudaStream_t stream);
-cudaError_t launch_forward_cluster_b(const ForwardArgs* args, const int2* items, const int* flags,
+template <class R>
+cudaError_t launch_forward_cluster_b(const ForwardArgsT<R>* args, const int2* items, const int* flags,
                                      int n_items, int n_to, cudaStream_t stream);
 cudaError_t launch_output_b(const OutputArgs* args, const int2* items, const int* flags,
                             int n_items, cudaStream_t stream);
-cudaError_t launch_column_b(const ColumnTileArgs* args, const int4* items, const int* flags,
+template <class R>
+cudaError_t launch_column_b(const ColumnArgsT<R>* args, const int4* items, const int* flags,
                             int n_items, cudaStream_t stream);
 
 // ---- stepping kernels (step_kernels.cu)

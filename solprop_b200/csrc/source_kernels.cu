@@ -1,5 +1,7 @@
 // The kernels of one source evaluation on the modal route (field grid): solprop's
-// passes 2-7 (docs/dev/architecture.md section 8), restated for sm_100a.
+// passes 2-7 (docs/dev/architecture.md section 8), restated for sm_100a.  The transforms
+// are templates over the real type: FP64, or FP32 in the mixed-precision form, whose
+// stage output still combines in FP64.
 //
 //   k_inverse_field   pad + c2r inverse transform of every modal column, in shared
 //                     memory; epilogue writes the modal field and the in-stage
@@ -16,16 +18,19 @@
 namespace sp {
 
 // ----------------------------------------------------------------------------- K1
-__device__ __forceinline__ void inverse_field_body(const InverseArgs& a, int col) {
-  extern __shared__ double2 smem_c[];
+template <class R>
+__device__ __forceinline__ void inverse_field_body(const InverseArgsT<R>& a, int col) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* smem_c = reinterpret_cast<C*>(smem_raw);
   const int M = a.n_to >> 1;  // complex length
   const double2* lab = a.lab + (size_t)col * a.n_omega;
-  const double2* tw = a.twiddles;
+  const C* tw = a.twiddles;
   // X[k] for k in [0, M]; pocketfft's irfft reads only the real part of the DC and
   // Nyquist bins, so those are taken real here too.
   // the field grid's crop is the leading bins (crop_index[j] = j) unless told otherwise,
   // so the fine spectrum is the coarse one padded: no index load on that path
-  auto fine = [&](int k) -> double2 {
+  auto fine = [&](int k) -> C {
     double2 v;
     if (a.crop_identity) {
       v = k < a.n_omega ? lab[k] : make_double2(0.0, 0.0);
@@ -34,41 +39,49 @@ __device__ __forceinline__ void inverse_field_body(const InverseArgs& a, int col
       v = j >= 0 ? lab[j] : make_double2(0.0, 0.0);
     }
     if (k == 0 || k == M) v.y = 0.0;
-    return v;
+    return to_c<C>(v);
   };
+  const R half = R(0.5);
 #pragma unroll 4
   for (int k = threadIdx.x; k < M; k += blockDim.x) {
-    double2 xk = fine(k), xm = cconj(fine(M - k));
-    double2 e = cscale(0.5, cadd(xk, xm));
+    C xk = fine(k), xm = cconj(fine(M - k));
+    C e = cscale(half, cadd(xk, xm));
     // O[k] = (X[k] - conj X[M-k]) W^-k / 2, W^-k = conj(exp(-i pi k / M))
-    double2 w = __ldg(tw + k);  // exp(-2 pi i k / n_to)
-    double2 o = cscale(0.5, cmul(csub(xk, xm), cconj(w)));
+    C w = __ldg(tw + k);  // exp(-2 pi i k / n_to)
+    C o = cscale(half, cmul(csub(xk, xm), cconj(w)));
     smem_c[k] = cadd(e, mul_pi(o));  // Z = E + i O
   }
   __syncthreads();
   fft_dif_inplace(smem_c, a.log_m, tw, a.log_n_to, /*inverse=*/true);
-  const double inv_m = 1.0 / (double)M;
-  double* row = a.modal_t + (size_t)col * a.n_to;
-  double* absorb = a.absorber_stream ? a.absorber_stream + (size_t)col * a.n_to : nullptr;
+  const R inv_m = R(1.0 / (double)M);
+  R* row = a.modal_t + (size_t)col * a.n_to;
+  R* absorb = a.absorber_stream ? a.absorber_stream + (size_t)col * a.n_to : nullptr;
 #pragma unroll 4
   for (int m = threadIdx.x; m < M; m += blockDim.x) {
-    double2 z = smem_c[bitrev(m, a.log_m)];
-    double x0 = z.x * inv_m, x1 = z.y * inv_m;
-    reinterpret_cast<double2*>(row)[m] = make_double2(x0, x1);
+    C z = smem_c[bitrev(m, a.log_m)];
+    R x0 = z.x * inv_m, x1 = z.y * inv_m;
+    C v;
+    v.x = x0;
+    v.y = x1;
+    reinterpret_cast<C*>(row)[m] = v;
     if (absorb) {
-      const double2 al = reinterpret_cast<const double2*>(a.alpha)[m];
-      reinterpret_cast<double2*>(absorb)[m] =
-          make_double2(-0.5 * al.x * x0, -0.5 * al.y * x1);
+      const C al = reinterpret_cast<const C*>(a.alpha)[m];
+      C ab;
+      ab.x = -half * al.x * x0;
+      ab.y = -half * al.y * x1;
+      reinterpret_cast<C*>(absorb)[m] = ab;
     }
   }
 }
 
-__global__ void __launch_bounds__(1024) k_inverse_field(InverseArgs a) {
+template <class R>
+__global__ void __launch_bounds__(1024) k_inverse_field(InverseArgsT<R> a) {
   inverse_field_body(a, blockIdx.x);
 }
 
 // batched: items[blockIdx.x] = (run, column)
-__global__ void __launch_bounds__(1024) k_inverse_field_b(const InverseArgs* args, const int2* items,
+template <class R>
+__global__ void __launch_bounds__(1024) k_inverse_field_b(const InverseArgsT<R>* args, const int2* items,
                                                          const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
@@ -76,17 +89,22 @@ __global__ void __launch_bounds__(1024) k_inverse_field_b(const InverseArgs* arg
 }
 
 // ----------------------------------------------------------------------------- K4
-__device__ __forceinline__ void forward_field_body(const ForwardArgs& a, int row_index) {
-  extern __shared__ double2 smem_c[];
+template <class R>
+__device__ __forceinline__ void forward_field_body(const ForwardArgsT<R>& a, int row_index) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* smem_c = reinterpret_cast<C*>(smem_raw);
   const int row = a.rows[row_index];
   const int M = a.n_to >> 1;
   if (row < a.n_partial_rows) {
     // a projected stream: the node groups' partial projections, summed in group order
 #pragma unroll 4
     for (int m = threadIdx.x; m < M; m += blockDim.x) {
-      double2 acc = make_double2(0.0, 0.0);
+      C acc;
+      acc.x = R(0);
+      acc.y = R(0);
       for (int g = 0; g < a.n_groups; ++g) {
-        const double2 v = reinterpret_cast<const double2*>(
+        const C v = reinterpret_cast<const C*>(
             a.partials + ((size_t)g * a.n_partial_rows + row) * a.n_to)[m];
         acc = cadd(acc, v);
       }
@@ -95,30 +113,39 @@ __device__ __forceinline__ void forward_field_body(const ForwardArgs& a, int row
   } else {
     const double2* x = reinterpret_cast<const double2*>(a.streams + (size_t)row * a.n_to);
 #pragma unroll 4
-    for (int m = threadIdx.x; m < M; m += blockDim.x) smem_c[m] = x[m];
+    for (int m = threadIdx.x; m < M; m += blockDim.x) smem_c[m] = to_c<C>(x[m]);
   }
   __syncthreads();
   fft_dif_inplace(smem_c, a.log_m, a.twiddles, a.log_n_to, /*inverse=*/false);
-  double2* out = a.spectra + (size_t)row * a.n_omega;
+  C* out = a.spectra + (size_t)row * a.n_omega;
+  const R half = R(0.5);
 #pragma unroll 4
   for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) {
     const int k = a.crop_identity ? j : (int)a.crop_index[j];
     const int km = (k == 0) ? 0 : M - k;
-    double2 zk = smem_c[bitrev(k == M ? 0 : k, a.log_m)];
-    double2 zm = cconj(smem_c[bitrev(km == M ? 0 : km, a.log_m)]);
-    double2 e = cscale(0.5, cadd(zk, zm));
-    double2 o = cscale(0.5, mul_mi(csub(zk, zm)));  // (Z[k] - conj Z[M-k]) / (2 i)
-    double2 w = k < M ? __ldg(a.twiddles + k) : make_double2(-1.0, 0.0);
+    C zk = smem_c[bitrev(k == M ? 0 : k, a.log_m)];
+    C zm = cconj(smem_c[bitrev(km == M ? 0 : km, a.log_m)]);
+    C e = cscale(half, cadd(zk, zm));
+    C o = cscale(half, mul_mi(csub(zk, zm)));  // (Z[k] - conj Z[M-k]) / (2 i)
+    C w;
+    if (k < M) {
+      w = __ldg(a.twiddles + k);
+    } else {
+      w.x = R(-1);
+      w.y = R(0);
+    }
     out[j] = cadd(e, cmul(w, o));
   }
 }
 
-__global__ void __launch_bounds__(1024) k_forward_field(ForwardArgs a) {
+template <class R>
+__global__ void __launch_bounds__(1024) k_forward_field(ForwardArgsT<R> a) {
   forward_field_body(a, blockIdx.x);
 }
 
 // batched: items[blockIdx.x] = (run, row index)
-__global__ void __launch_bounds__(1024) k_forward_field_b(const ForwardArgs* args, const int2* items,
+template <class R>
+__global__ void __launch_bounds__(1024) k_forward_field_b(const ForwardArgsT<R>* args, const int2* items,
                                                          const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
@@ -126,7 +153,8 @@ __global__ void __launch_bounds__(1024) k_forward_field_b(const ForwardArgs* arg
 }
 
 // ----------------------------------------------------------------------------- K5
-__device__ __forceinline__ void stage_output_body(const OutputArgs& a, int block) {
+template <class CS>
+__device__ __forceinline__ void stage_output_body(const OutputArgs& a, const CS* spectra, int block) {
   const int idx = block * blockDim.x + threadIdx.x;
   const int total = a.n_cols * a.n_omega;
   if (idx >= total) return;
@@ -142,51 +170,63 @@ __device__ __forceinline__ void stage_output_body(const OutputArgs& a, int block
     for (int p = 0; p < st.n_pre; ++p)
       pre = cadd(pre, cscale(st.pre_w[p], a.prefactor_terms[(size_t)p * total + idx]));
   }
-  double2 spec = a.spectra[idx];  // stream 0: P
+  double2 spec = to_d2(spectra[idx]);  // stream 0: P
   const bool active = a.active_mask[j];
   if (a.plasma && active) {
-    const double2 xs = a.spectra[(size_t)1 * total + idx];
-    const double2 zs = a.spectra[(size_t)2 * total + idx];
+    const double2 xs = to_d2(spectra[(size_t)1 * total + idx]);
+    const double2 zs = to_d2(spectra[(size_t)2 * total + idx]);
     const double2 qv = make_double2(0.0, a.omega[j]);
     const double2 q2 = cmul(qv, qv);
     spec = cadd(spec, csub(cdiv(xs, qv), cdiv(zs, q2)));
   }
   double2 normalised = cmul(cscale(a.omega_window[j], pre), spec);
   if (a.absorber) {
-    double2 ab = active ? a.spectra[(size_t)3 * total + idx] : make_double2(0.0, 0.0);
+    double2 ab = active ? to_d2(spectra[(size_t)3 * total + idx]) : make_double2(0.0, 0.0);
     normalised = cadd(normalised, ab);
   }
   if (a.inverse_propagator) normalised = cmul(a.inverse_propagator[idx], normalised);
   a.out[idx] = normalised;
 }
 
-__global__ void k_stage_output(OutputArgs a) { stage_output_body(a, blockIdx.x); }
+__device__ __forceinline__ void stage_output_any(const OutputArgs& a, int block) {
+  if (a.spectra32) stage_output_body(a, a.spectra32, block);
+  else stage_output_body(a, a.spectra, block);
+}
+
+__global__ void k_stage_output(OutputArgs a) { stage_output_any(a, blockIdx.x); }
 
 // batched: items[blockIdx.x] = (run, block of 256 elements)
 __global__ void k_stage_output_b(const OutputArgs* args, const int2* items, const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  stage_output_body(args[it.x], it.y);
+  stage_output_any(args[it.x], it.y);
 }
 
 // ----------------------------------------------------------------------------- launch
 static int threads_for(int m) { return m >= 1024 ? 1024 : (m >= 32 ? m : 32); }
 
-cudaError_t launch_inverse(const InverseArgs& a, int n_cols, cudaStream_t stream) {
+template <class R>
+cudaError_t launch_inverse(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream) {
   if (fft_cluster_size(a.n_to) > 1) return launch_inverse_cluster(a, n_cols, stream);
   const int M = a.n_to >> 1;
-  const size_t shm = (size_t)M * sizeof(double2);
-  k_inverse_field<<<n_cols, threads_for(M), shm, stream>>>(a);
+  const size_t shm = (size_t)M * sizeof(cplx<R>);
+  k_inverse_field<R><<<n_cols, threads_for(M), shm, stream>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_forward(const ForwardArgs& a, int n_rows, cudaStream_t stream) {
+template <class R>
+cudaError_t launch_forward(const ForwardArgsT<R>& a, int n_rows, cudaStream_t stream) {
   if (fft_cluster_size(a.n_to) > 1) return launch_forward_cluster(a, n_rows, stream);
   const int M = a.n_to >> 1;
-  const size_t shm = (size_t)M * sizeof(double2);
-  k_forward_field<<<n_rows, threads_for(M), shm, stream>>>(a);
+  const size_t shm = (size_t)M * sizeof(cplx<R>);
+  k_forward_field<R><<<n_rows, threads_for(M), shm, stream>>>(a);
   return cudaGetLastError();
 }
+
+template cudaError_t launch_inverse<double>(const InverseArgsT<double>&, int, cudaStream_t);
+template cudaError_t launch_inverse<float>(const InverseArgsT<float>&, int, cudaStream_t);
+template cudaError_t launch_forward<double>(const ForwardArgsT<double>&, int, cudaStream_t);
+template cudaError_t launch_forward<float>(const ForwardArgsT<float>&, int, cudaStream_t);
 
 cudaError_t launch_output(const OutputArgs& a, cudaStream_t stream) {
   const int total = a.n_cols * a.n_omega;
@@ -197,15 +237,15 @@ cudaError_t launch_output(const OutputArgs& a, cudaStream_t stream) {
 cudaError_t configure_source_kernels() {
   const int max_shm = 227 * 1024;
   cudaError_t e;
-  e = cudaFuncSetAttribute(k_inverse_field, cudaFuncAttributeMaxDynamicSharedMemorySize, max_shm);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_forward_field, cudaFuncAttributeMaxDynamicSharedMemorySize, max_shm);
-  if (e != cudaSuccess) return e;
+  const void* kernels[8] = {(const void*)k_inverse_field<double>, (const void*)k_forward_field<double>,
+                            (const void*)k_inverse_field_b<double>, (const void*)k_forward_field_b<double>,
+                            (const void*)k_inverse_field<float>, (const void*)k_forward_field<float>,
+                            (const void*)k_inverse_field_b<float>, (const void*)k_forward_field_b<float>};
+  for (const void* k : kernels) {
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_shm);
+    if (e != cudaSuccess) return e;
+  }
   e = configure_column_kernels();
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_inverse_field_b, cudaFuncAttributeMaxDynamicSharedMemorySize, max_shm);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_forward_field_b, cudaFuncAttributeMaxDynamicSharedMemorySize, max_shm);
   if (e != cudaSuccess) return e;
   return configure_cluster_fft();
 }
@@ -214,19 +254,26 @@ cudaError_t configure_source_kernels() {
 
 namespace sp {
 
-cudaError_t launch_inverse_b(const InverseArgs* args, const int2* items, const int* flags,
+template <class R>
+cudaError_t launch_inverse_b(const InverseArgsT<R>* args, const int2* items, const int* flags,
                              int n_items, int n_to, cudaStream_t stream) {
   const int M = n_to >> 1;
-  k_inverse_field_b<<<n_items, threads_for(M), (size_t)M * sizeof(double2), stream>>>(args, items, flags);
+  k_inverse_field_b<R><<<n_items, threads_for(M), (size_t)M * sizeof(cplx<R>), stream>>>(args, items, flags);
   return cudaGetLastError();
 }
 
-cudaError_t launch_forward_b(const ForwardArgs* args, const int2* items, const int* flags,
+template <class R>
+cudaError_t launch_forward_b(const ForwardArgsT<R>* args, const int2* items, const int* flags,
                              int n_items, int n_to, cudaStream_t stream) {
   const int M = n_to >> 1;
-  k_forward_field_b<<<n_items, threads_for(M), (size_t)M * sizeof(double2), stream>>>(args, items, flags);
+  k_forward_field_b<R><<<n_items, threads_for(M), (size_t)M * sizeof(cplx<R>), stream>>>(args, items, flags);
   return cudaGetLastError();
 }
+
+template cudaError_t launch_inverse_b<double>(const InverseArgsT<double>*, const int2*, const int*, int, int, cudaStream_t);
+template cudaError_t launch_inverse_b<float>(const InverseArgsT<float>*, const int2*, const int*, int, int, cudaStream_t);
+template cudaError_t launch_forward_b<double>(const ForwardArgsT<double>*, const int2*, const int*, int, int, cudaStream_t);
+template cudaError_t launch_forward_b<float>(const ForwardArgsT<float>*, const int2*, const int*, int, int, cudaStream_t);
 
 cudaError_t launch_output_b(const OutputArgs* args, const int2* items, const int* flags,
                             int n_items, cudaStream_t stream) {

@@ -1,0 +1,124 @@
+"""The mixed-precision form (SP_PRECISION_MIXED) against the FP64 reference, on a B200.
+
+The mixed form runs the forward transforms and the response column in FP32 and keeps the
+inverse transform, the propagator, the Adams accumulation, the norms and the plasma
+running integrals in FP64.  Its error against the FP64 reference is stated per result:
+
+* one source evaluation: relative L2 at most ``SOURCE_TOL`` (measured 1e-7 to 4e-7);
+* a fixed schedule: every plane within ``STEP_TOL`` of the reference's (measured ~1e-7);
+* an adaptive run: every plane within the run's rtol (its own step sequence differs
+  from the FP64 run's, so the difference includes the stepping error), and the full
+  config-1 and config-2 runs within ``RUN_TOL`` of the FP64 ones;
+* a batched mixed scan against the same runs alone: FP32 rounding only (the two
+  launches are separate compilations, free to contract products differently).
+"""
+
+import numpy as np
+import pytest
+
+from tests._cases import fixed_schedule, golden, policy, record, rel
+
+pytestmark = pytest.mark.gpu
+
+SOURCE_TOL = 2e-6
+STEP_TOL = 1e-6
+RUN_TOL = 5e-6
+
+
+def _mixed(case, fixed=False):
+    from solprop_b200 import _lib
+
+    rec = record(case, fixed)
+    problem = _lib.Problem(rec)
+    return rec, problem, _lib.Workspace(problem, 0, "mixed")
+
+
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he", "config1", "config2"])
+@pytest.mark.parametrize("index", [0, 1])
+def test_mixed_source_error(case, index):
+    rec, problem, ws = _mixed(case)
+    g = golden(case)
+    out = ws.source(g[f"src{index}.lab"], float(g[f"src{index}.z"]))
+    assert rel(out, g[f"src{index}.source"]) < SOURCE_TOL
+
+
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he"])
+def test_mixed_fixed_schedule_error(case):
+    rec, problem, ws = _mixed(case, fixed=True)
+    g = golden(case)
+    steps, _ = fixed_schedule(g)
+    session = ws.start(policy(g, "fixed"), schedule=steps)
+    zs, states = g["fixed.z"], g["fixed.states"]
+    plane = 1
+    while True:
+        batch = session.advance(1)
+        if plane < len(zs) and abs(batch.z - zs[plane]) < 1e-12:
+            assert rel(session.export(), states[plane]) < STEP_TOL, (case, plane)
+            plane += 1
+        if batch.event in (2, 3):
+            break
+    assert plane == len(zs)
+
+
+@pytest.mark.parametrize("case", ["config1", "config2"])
+def test_mixed_full_adaptive_run(case):
+    """BASELINE configs 1 and 2 in full, mixed against FP64 on the device (which is the
+    reference's arithmetic to 1e-10): the final spectra within ``RUN_TOL`` and the
+    attempt counts within 20 %.  Each run chooses its own steps, so the difference
+    includes the stepping error at rtol 1e-6 (measured 2.5e-6 and 3.6e-7)."""
+    from solprop_b200 import _lib
+
+    rec = record(case)
+    pol = policy(golden(case), "adaptive")
+    problem = _lib.Problem(rec)
+    finals = {}
+    for precision in ("fp64", "mixed"):
+        ws = _lib.Workspace(problem, 0, precision)
+        session = ws.start(pol)
+        while True:
+            batch = session.advance(512)
+            if batch.event in (2, 3):
+                break
+        assert batch.event == 2
+        finals[precision] = (session.export(), batch.attempts)
+    assert rel(finals["mixed"][0], finals["fp64"][0]) < RUN_TOL
+    assert abs(finals["mixed"][1] - finals["fp64"][1]) <= 0.2 * finals["fp64"][1]
+
+
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he"])
+def test_mixed_adaptive_run_within_rtol(case):
+    rec, problem, ws = _mixed(case)
+    g = golden(case)
+    pol = policy(g, "adaptive")
+    session = ws.start(pol)
+    zs, states = g["adaptive.z"], g["adaptive.states"]
+    seen = 1
+    while True:
+        batch = session.advance(256)
+        assert batch.event != 3
+        if batch.event in (1, 2):
+            assert rel(session.export(), states[seen]) < pol["rtol"]
+            seen += 1
+        if batch.event == 2:
+            break
+    assert seen == len(zs)
+
+
+def test_mixed_scan_matches_mixed_single_runs():
+    from solprop_b200 import _lib, scan
+
+    points = [
+        scan.ScanPoint(120e-6, 1.0, "He", 1.0, 60e-6, 20e-15, 2, 4096, 1),
+        scan.ScanPoint(90e-6, 0.8, "Ar", 0.5, 30e-6, 25e-15, 1, 16384, 2),
+    ]
+    built = [scan.capillary_record(p) for p in points]
+    sc = _lib.Scan([r for r, _ in built], [q for _, q in built], 0, "mixed")
+    sc.advance(10)
+    for i, (rec, pol) in enumerate(built):
+        state, info = sc.run(i)
+        problem = _lib.Problem(rec)
+        ws = _lib.Workspace(problem, 0, "mixed")
+        session = ws.start(pol)
+        for _ in range(int(info.attempts)):
+            session.advance(1)
+        assert rel(state, session.export()) < 1e-6, i
