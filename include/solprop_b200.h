@@ -212,6 +212,32 @@ sp_status sp_scan_run(sp_scan* scan, int32_t run, double* state, sp_batch* info)
 void* sp_scan_stream(sp_scan* scan);
 sp_status sp_scan_destroy(sp_scan* scan);
 
+/* ---- the scan surrogate's multilayer perceptron (no counterpart in the reference) ----
+ * Device pointers to row-major FP32 tensors; products run in BF16 on the tensor cores
+ * with FP32 accumulation.  stream may be NULL (the legacy default stream).
+ * sp_mlp_gemm: C[M,N] = op(A) op(B) with op(A)(m,k) = transA ? A[k*lda+m] : A[m*lda+k],
+ * op(B)(k,n) = transB ? B[n*ldb+k] : B[k*ldb+n]; epilogue 0: none, 1: + bias[n],
+ * 2: GELU(. + bias[n]) with the pre-activation written to pre (ld = ldc) when not NULL. */
+sp_status sp_mlp_gemm(const float* A, int lda, int transA, const float* B, int ldb, int transB,
+                      float* C, int ldc, int M, int N, int K, const float* bias, int epilogue,
+                      float* pre, void* stream);
+/* dZ = dA * GELU'(pre), elementwise over n values. */
+sp_status sp_mlp_gelu_backward(const float* dA, const float* pre, float* dZ, size_t n, void* stream);
+/* db[n] = sum over the M rows of dZ[m, n] (rows in order). */
+sp_status sp_mlp_bias_grad(const float* dZ, int M, int N, float* db, void* stream);
+/* Mean squared error of Y against T (M x N): dY = 2 (Y - T) / (M N), *loss (device) the mean;
+ * row_loss is M floats of scratch. */
+sp_status sp_mlp_mse(const float* Y, const float* T, int M, int N, float* dY, float* row_loss,
+                     float* loss, void* stream);
+/* One Adam step (bias-corrected, step >= 1) on n FP32 weights. */
+sp_status sp_mlp_adam(float* w, const float* grad, float* m1, float* m2, size_t n, float lr,
+                      float beta1, float beta2, float eps, int step, void* stream);
+/* Ensemble statistics of Y (members, M, N) of log10 spectral densities: mean (M, N) and,
+ * per row, the disagreement: the standard deviation over members of each output weighted
+ * by 10^mean (the mean spectrum's energy there), over the summed weights. */
+sp_status sp_mlp_ensemble_stats(const float* Y, int members, int M, int N, float* mean,
+                                float* spread, void* stream);
+
 /* One source evaluation that allocates no device memory, for callers that cannot call
  * cudaMalloc: code whose device memory belongs to a pool or a framework that owns every
  * allocation, or that runs where an allocation would synchronise the device or fail.

@@ -96,6 +96,18 @@ SIGNATURES = {
     "sp_problem_destroy": (C.c_int, [C.c_void_p]),
     "sp_workspace_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "sp_workspace_create_ex": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    # the scan surrogate's perceptron kernels (device pointers, stream may be NULL)
+    "sp_mlp_gemm": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                              C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                              C.c_void_p]),
+    "sp_mlp_gelu_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "sp_mlp_bias_grad": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
+    "sp_mlp_mse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.c_void_p]),
+    "sp_mlp_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_float,
+                              C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]),
+    "sp_mlp_ensemble_stats": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
     "sp_workspace_destroy": (C.c_int, [C.c_void_p]),
     "sp_workspace_source": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_double, C.c_int,
                                       C.POINTER(C.c_double)]),

@@ -153,8 +153,8 @@ static void validate(const sp_problem_desc* d) {
   };
   need(d != nullptr, "problem description is NULL");
   need(d->n_modes >= 1 && d->n_pol >= 1 && d->n_omega >= 2, "bad state shape");
-  need(d->n_to >= 64 && (d->n_to & (d->n_to - 1)) == 0,
-       "n_to must be a power of two >= 64 (mixed radices are not built)");
+  need(d->n_to >= 2 * kWindow && (d->n_to & (d->n_to - 1)) == 0,
+       "n_to must be a power of two >= 512 (mixed radices and shorter rows are not built)");
   need(d->n_nodes >= 1 && d->synthesis && d->projection, "synthesis/projection required");
   need(d->omega && d->crop_index && d->active_mask && d->norm_mask && d->omega_window &&
            d->t_window && d->t_window_derivative,
@@ -297,6 +297,13 @@ static void upload_stages(sp_workspace* ws, int count) {
                              cudaMemcpyHostToDevice, ws->stream));
 }
 
+// The response column's tiles: windows of kWindow samples owning column_owned(K) each.
+static int column_halfwidth(const sp_problem_desc& d) { return d.plasma_enabled ? d.n_taps - 1 : 0; }
+static int column_tiles(const sp_problem_desc& d) {
+  const int owned = column_owned(column_halfwidth(d));
+  return (d.n_to + owned - 1) / owned;
+}
+
 // The buffers one source evaluation reads and writes, in the evaluation's real type.
 template <class R>
 struct SourceView {
@@ -353,13 +360,15 @@ static ColumnArgsT<R> column_args(const sp_workspace* ws, const StageScalarsDev*
   ca.n_nodes = d.n_nodes;
   ca.n_cols = P.n_cols;
   ca.n_to = d.n_to;
-  ca.n_tiles = (d.n_to + kSeg - 1) / kSeg;
+  ca.half_width = column_halfwidth(d);
+  ca.lead = column_lead(ca.half_width);
+  ca.owned = column_owned(ca.half_width);
+  ca.n_tiles = column_tiles(d);
   ca.n_groups = (d.n_nodes + kGroup - 1) / kGroup;
   ca.n_blocks = ca.n_tiles * ca.n_groups;
   ca.kerr = d.kerr_enabled;
   ca.plasma = d.plasma_enabled;
   ca.band = d.band;
-  ca.half_width = d.plasma_enabled ? d.n_taps - 1 : 0;
   ca.rate_intervals = d.rate_intervals;
   ca.kerr_coefficient = d.kerr_coefficient;
   ca.charge_mass_ratio = d.charge_mass_ratio;
@@ -525,7 +534,7 @@ static void build_workspace(sp_workspace* ws) {
   ws->lab.alloc(n);
   ws->out.alloc(n);
   ws->modal_t.alloc((size_t)P.n_cols * d.n_to);
-  const size_t n_tiles = (d.n_to + kSeg - 1) / kSeg;
+  const size_t n_tiles = column_tiles(d);
   const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
   ws->sums0.alloc((size_t)d.n_nodes * n_tiles);
   ws->sums1.alloc((size_t)d.n_nodes * n_tiles);
@@ -1850,7 +1859,7 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     carve.take(ws.active, d.n_omega);
     carve.take(ws.norm, d.n_omega);
     carve.take(ws.modal_t, (size_t)P.n_cols * d.n_to);
-    const size_t n_tiles = (d.n_to + kSeg - 1) / kSeg;
+    const size_t n_tiles = column_tiles(d);
     const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
     carve.take(ws.sums0, (size_t)d.n_nodes * n_tiles);
     carve.take(ws.sums1, (size_t)d.n_nodes * n_tiles);

@@ -58,10 +58,16 @@ struct InverseArgsT {
 };
 using InverseArgs = InverseArgsT<double>;
 
-// The tiled response column (column_kernels.cu): tiles of kSeg samples of kGroup nodes.
-constexpr int kSeg = 64;
-constexpr int kGroup = 16;
-constexpr int kHalo = 8;   // the largest band-rule half-width K the tiles carry
+// The response column (column_kernels.cu): a warp holds one node's window of kWindow
+// samples, a CTA kGroup nodes; a window owns column_owned(K) samples between halos of
+// 2K + 1 (K the band filter's half-width, at most kHalo).
+constexpr int kWindow = 256;
+constexpr int kGroup = 8;
+constexpr int kHalo = 8;
+__host__ __device__ constexpr int column_lead(int half_width) { return 2 * half_width + 1; }
+__host__ __device__ constexpr int column_owned(int half_width) {
+  return kWindow - 2 * column_lead(half_width);
+}
 
 template <class R>
 struct ColumnArgsT {
@@ -78,6 +84,7 @@ struct ColumnArgsT {
   double* status;          // set to 1 when a tile gave up waiting
   R* partials;             // (n_groups, 3, n_cols, n_to) projected streams per node group
   int n_modes, n_nodes, n_cols, n_to, n_tiles, n_groups, n_blocks;
+  int lead, owned;         // a window's halo and owned samples (column_lead, column_owned)
   int kerr, plasma, band, half_width, rate_intervals;
   double kerr_coefficient, charge_mass_ratio, ionisation_potential, dt;
   double log_field_min, d_log_field, field_min, field_max, rate_max;

@@ -259,9 +259,9 @@ def capillary_record(p: ScanPoint) -> tuple[ProblemRecord, dict]:
 def exit_log_spectrum(rec: ProblemRecord, state: np.ndarray, bins: int = 2048) -> np.ndarray:
     """The surrogate's target: log10 of the exit energy spectral density, summed over modes,
     on ``bins`` wavelengths from 100 nm to 4 um (interpolated), floored at 1e-30."""
-    power = np.sum(np.abs(state) ** 2, axis=(0, 1))
-    lam = 2 * np.pi * C0 / np.maximum(rec.omega, 1e-300)
+    power = np.sum(np.abs(state) ** 2, axis=(0, 1))[1:]
+    lam = 2 * np.pi * C0 / rec.omega[1:]  # the DC bin has no wavelength
     grid = np.linspace(100e-9, 4e-6, bins)
-    order = np.argsort(lam[1:]) + 1
+    order = np.argsort(lam)
     values = np.interp(grid, lam[order], power[order], left=0.0, right=0.0)
     return np.log10(np.maximum(values, 1e-30))
