@@ -194,6 +194,7 @@ struct sp_workspace {
       rate_coeff, taps, modal_t, streams, sums0, sums1, proj;
   DevBuf<long long> crop;
   DevBuf<int> fine_to_coarse, rows, chain_flags;
+  DevBuf<unsigned> arrivals;
   DevBuf<unsigned long long> ticket;  // the response column's tile counter
   // the mixed-precision form's FP32 copies of the source evaluation's buffers
   int precision = SP_PRECISION_FP64;
@@ -354,6 +355,7 @@ static ColumnArgsT<R> column_args(const sp_workspace* ws, const StageScalarsDev*
   ca.sums1 = ws->sums1.p;
   ca.ticket = ws->ticket.p;
   ca.flags = ws->chain_flags.p;
+  ca.arrivals = ws->arrivals.p;
   ca.status = ws->norms.p + kColumnStatus;
   ca.partials = v.proj;
   ca.n_modes = d.n_modes;
@@ -397,7 +399,8 @@ static ForwardArgsT<R> forward_args(const sp_workspace* ws) {
   const sp_problem_desc& d = P.d;
   const int nc = P.n_cols;
   const SourceView<R> v = source_view<R>(ws);
-  return ForwardArgsT<R>{ws->streams.p, v.proj, (d.n_nodes + kGroup - 1) / kGroup, 3 * nc,
+  // the response column leaves the node groups' sum in group 0's rows
+  return ForwardArgsT<R>{ws->streams.p, v.proj, 1, 3 * nc,
                          d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
                          ws->crop.p, v.twiddles, v.spectra, d.n_to, d.n_omega, ws->log_m,
                          ws->log_n_to, P.crop_identity};
@@ -540,6 +543,8 @@ static void build_workspace(sp_workspace* ws) {
   ws->sums1.alloc((size_t)d.n_nodes * n_tiles);
   ws->chain_flags.alloc(n_groups * n_tiles);
   ws->chain_flags.zero(s);
+  ws->arrivals.alloc(n_tiles);
+  ws->arrivals.zero(s);
   ws->ticket.alloc(1);
   ws->ticket.zero(s);
   ws->proj.alloc(n_groups * 3 * P.n_cols * d.n_to);
@@ -1864,6 +1869,7 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     carve.take(ws.sums0, (size_t)d.n_nodes * n_tiles);
     carve.take(ws.sums1, (size_t)d.n_nodes * n_tiles);
     carve.take(ws.chain_flags, n_groups * n_tiles);
+    carve.take(ws.arrivals, n_tiles);
     carve.take(ws.ticket, 1);
     carve.take(ws.norms, kMaxOrders + 2);
     carve.take(ws.proj, n_groups * 3 * P.n_cols * d.n_to);
@@ -1910,6 +1916,7 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     ws.spectra.zero(s);
     ws.proj.zero(s);
     ws.chain_flags.zero(s);
+    ws.arrivals.zero(s);
     ws.ticket.zero(s);
     ws.norms.zero(s);
     static bool configured[kNoAllocDevices];

@@ -16,8 +16,8 @@
 // order once they are published, and rescans its window from that offset.  The sums are
 // FP64 in both precisions (the mixed form's compensated integral).  The tile then forms
 // the total current, the Kerr cubic and the temporal collar, and projects the owned
-// samples onto the modes (partial sums per node group, summed by the forward transform's
-// load).  Every sum has a fixed order, so the results are reproducible bit for bit.
+// samples onto the modes (partial sums per node group, added in group order by the tile's
+// last CTA).  Every sum has a fixed order, so the results are reproducible bit for bit.
 #include "kernels.cuh"
 
 namespace sp {
@@ -30,12 +30,17 @@ static_assert(kPer == 8, "the filter's halo exchange assumes eight samples per l
 static_assert(kHalo <= kPer, "a tap may reach one neighbouring lane at most");
 static_assert(3 * kGroup >= kMaxModes, "the stream buffer must cover the modal window");
 
-// shared memory: the modal window (n_modes x kWindow), later the three projected
-// streams of the group (3 x kGroup x kWindow) over the same space, and one scratch row
-// per warp for the point reflection at the row's ends
+// Shared rows are padded by one element after every eight (pad(u) = u + u / 8), so that
+// the 32 lanes of a warp, each at its own eight-sample run, hit distinct banks.
+constexpr int kPitch = kWindow + kWindow / kPer;
+__device__ __forceinline__ int pad(int u) { return u + (u >> 3); }
+
+// shared memory: the modal window (n_modes rows), later the three projected streams of
+// the group (3 x kGroup rows) over the same space, and one scratch row per warp for the
+// point reflection at the row's ends
 template <class R>
 constexpr size_t column_smem() {
-  return sizeof(R) * ((size_t)3 * kGroup * kWindow + (size_t)kGroup * kWindow);
+  return sizeof(R) * ((size_t)3 * kGroup * kPitch + (size_t)kGroup * kPitch);
 }
 
 __device__ __forceinline__ double rate_of(const ColumnArgsT<double>& a, double magnitude) {
@@ -86,17 +91,17 @@ __device__ __forceinline__ R shfl_down1(R v) { return __shfl_down_sync(0xfffffff
 // Point reflection at the row's ends, y[-m] = 2 y[0] - y[m] and y[N-1+m] = 2 y[N-1] -
 // y[N-1-m] for m <= K, through the warp's scratch row (tiles that touch an end only).
 template <class R>
-__device__ void reflect_ends(R (&v)[kPer], R* row, int tw, int n_to, int K, int lane) {
+__device__ __forceinline__ void reflect_ends(R (&v)[kPer], R* row, int tw, int n_to, int K, int lane) {
 #pragma unroll
-  for (int j = 0; j < kPer; ++j) row[kPer * lane + j] = v[j];
+  for (int j = 0; j < kPer; ++j) row[pad(kPer * lane + j)] = v[j];
   __syncwarp();
 #pragma unroll
   for (int j = 0; j < kPer; ++j) {
     const int t = tw + kPer * lane + j;
-    if (t < 0 && t >= -K) v[j] = R(2) * row[0 - tw] - row[-t - tw];
+    if (t < 0 && t >= -K) v[j] = R(2) * row[pad(0 - tw)] - row[pad(-t - tw)];
     if (t > n_to - 1 && t <= n_to - 1 + K) {
       const int m = t - (n_to - 1);
-      v[j] = R(2) * row[n_to - 1 - tw] - row[n_to - 1 - m - tw];
+      v[j] = R(2) * row[pad(n_to - 1 - tw)] - row[pad(n_to - 1 - m - tw)];
     }
   }
   __syncwarp();
@@ -107,26 +112,22 @@ __device__ void reflect_ends(R (&v)[kPer], R* row, int tw, int n_to, int K, int 
 // window are garbage and lie in the halo, which the caller does not use)
 template <class R>
 __device__ __forceinline__ void band_filter(const R (&y)[kPer], R (&out)[kPer], const R* taps, int K) {
-  R left[kPer], right[kPer];
+  R ext[3 * kPer];  // the left neighbour's samples, this lane's, the right neighbour's
 #pragma unroll
   for (int j = 0; j < kPer; ++j) {
-    left[j] = shfl_up1(y[j]);
-    right[j] = shfl_down1(y[j]);
+    ext[j] = shfl_up1(y[j]);
+    ext[kPer + j] = y[j];
+    ext[2 * kPer + j] = shfl_down1(y[j]);
   }
   R c[kHalo + 1];
 #pragma unroll
   for (int k = 0; k <= kHalo; ++k) c[k] = k <= K ? taps[k] : R(0);
 #pragma unroll
   for (int j = 0; j < kPer; ++j) {
-    R f = c[0] * y[j];
+    R f = c[0] * ext[kPer + j];
 #pragma unroll
-    for (int k = 1; k <= kHalo; ++k) {
-      if (k <= K) {
-        const R lo = (j - k >= 0) ? y[j - k] : left[kPer + j - k];
-        const R hi = (j + k < kPer) ? y[j + k] : right[j + k - kPer];
-        f = f + c[k] * (lo + hi);
-      }
-    }
+    for (int k = 1; k <= kHalo; ++k)
+      if (k <= K) f = f + c[k] * (ext[kPer + j - k] + ext[kPer + j + k]);
     out[j] = f;
   }
 }
@@ -257,9 +258,9 @@ __device__ __forceinline__ double predecessors(const double* sums, int node, int
 template <class R>
 __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   extern __shared__ __align__(16) unsigned char column_raw[];
-  R* modal = reinterpret_cast<R*>(column_raw);    // [m][kWindow], then the streams
-  R* streams = modal;                              // [s][warp][kWindow]
-  R* scratch = modal + (size_t)3 * kGroup * kWindow;
+  R* modal = reinterpret_cast<R*>(column_raw);    // [m][kPitch], then the streams
+  R* streams = modal;                              // [s][warp][kPitch]
+  R* scratch = modal + (size_t)3 * kGroup * kPitch;
   __shared__ unsigned long long ticket;
   __shared__ R wt[kMaxModes * kGroup];
   if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1ull);
@@ -279,7 +280,7 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   // the modal window and the group's projection weights W[m, node] / tau
   for (int i = threadIdx.x; i < a.n_modes * kWindow; i += blockDim.x) {
     const int m = i / kWindow, u = i % kWindow, t = tw + u;
-    modal[i] = (t >= 0 && t < a.n_to) ? R(a.modal_t[(size_t)m * a.n_to + t]) : R(0);
+    modal[m * kPitch + pad(u)] = (t >= 0 && t < a.n_to) ? R(a.modal_t[(size_t)m * a.n_to + t]) : R(0);
   }
   for (int k = threadIdx.x; k < a.n_modes * kGroup; k += blockDim.x) {
     const int m = k / kGroup, w = k % kGroup, nd = group * kGroup + w;
@@ -299,7 +300,7 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
       R e = R(0);
 #pragma unroll
       for (int m = 0; m < kMaxModes; ++m)
-        if (m < a.n_modes) e += srow[m] * modal[m * kWindow + u];
+        if (m < a.n_modes) e += srow[m] * modal[m * kPitch + pad(u)];
       E[j] = e;
       W[j] = (plasma && t >= 0 && t < a.n_to) ? rate_of(a, fabs(e)) : R(0);
     }
@@ -312,7 +313,7 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   if (plasma) {
     const int first = (int)(2 * epoch + 1);
     const R dt = R(a.dt);
-    R* row = scratch + (size_t)warp * kWindow;
+    R* row = scratch + (size_t)warp * kPitch;
     // exposure: W~ on [A - K, A + owned + K], increments on [A - K, A + owned + K)
     R Wf[kPer], inc[kPer];
     if (at_end) {
@@ -382,23 +383,55 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
           z = a.t_window_derivative[t] * current;
         }
       }
-      streams[(0 * kGroup + warp) * kWindow + u] = p;
-      streams[(1 * kGroup + warp) * kWindow + u] = x;
-      streams[(2 * kGroup + warp) * kWindow + u] = z;
+      streams[(0 * kGroup + warp) * kPitch + pad(u)] = p;
+      streams[(1 * kGroup + warp) * kPitch + pad(u)] = x;
+      streams[(2 * kGroup + warp) * kPitch + pad(u)] = z;
     }
   }
   __syncthreads();
-  // projection of the owned samples onto the modes: the group's nodes summed in order
+  // projection of the owned samples onto the modes: thread u takes window sample u of
+  // every stream and mode, the group's nodes summed in order
+  static_assert(kThreads == kWindow, "one thread per window sample");
   const int n_streams = plasma ? 3 : 1;
-  const int span = own_hi - A;
-  for (int item = threadIdx.x; item < n_streams * a.n_modes * span; item += blockDim.x) {
-    const int q = item % span, sm = item / span;
-    const int s = sm / a.n_modes, m = sm - s * a.n_modes;
-    const int u = A + q;
-    R acc = R(0);
+  const int u = threadIdx.x;
+  const bool mine = u >= A && u < own_hi;
+  const size_t row_of_group = (size_t)3 * a.n_cols * a.n_to;
+  R* base = a.partials + (mine ? tw + u : 0);  // sample t = tw + u of row (group 3 + s) n_cols + m
+  if (mine) {
+    for (int s = 0; s < n_streams; ++s) {
+      R v[kGroup];
 #pragma unroll
-    for (int w = 0; w < kGroup; ++w) acc += wt[m * kGroup + w] * streams[(s * kGroup + w) * kWindow + u];
-    a.partials[(((size_t)group * 3 + s) * a.n_cols + m) * a.n_to + t0 + q] = acc;
+      for (int w = 0; w < kGroup; ++w) v[w] = streams[(s * kGroup + w) * kPitch + pad(u)];
+      for (int m = 0; m < a.n_modes; ++m) {
+        R acc = R(0);
+#pragma unroll
+        for (int w = 0; w < kGroup; ++w) acc += wt[m * kGroup + w] * v[w];
+        base[group * row_of_group + ((size_t)s * a.n_cols + m) * a.n_to] = acc;
+      }
+    }
+  }
+  // The tile's node groups: the last of its n_groups CTAs to arrive adds the groups'
+  // partial rows in group order into group 0's (the forward transform reads those).
+  // Arrivals count up by n_groups per evaluation, so the counter needs no reset.
+  if (a.n_groups > 1) {
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned arrived = atomicAdd(a.arrivals + tile, 1u);
+      last = (arrived % (unsigned)a.n_groups) == (unsigned)(a.n_groups - 1);
+    }
+    __syncthreads();
+    if (last && mine) {
+      __threadfence();
+      for (int s = 0; s < n_streams; ++s)
+        for (int m = 0; m < a.n_modes; ++m) {
+          R* out = base + ((size_t)s * a.n_cols + m) * a.n_to;
+          R acc = R(0);
+          for (int g = 0; g < a.n_groups; ++g) acc = acc + __ldcg(out + g * row_of_group);
+          *out = acc;
+        }
+    }
   }
 }
 
