@@ -1,6 +1,6 @@
 """Benchmark of the B200 propagation hot path (one JSON line on stdout, rank 0).
 
-Workload: BASELINE config 2, the four-mode (HE11-HE14) helium capillary with a 0.8 -> 0
+Workload: config 2, the four-mode (HE11-HE14) helium capillary with a 0.8 -> 0
 bar gradient, 1.5 m, 800 nm, 7.5 fs, 275 uJ, 90 nm - 4 um, n_to = 16384 fine samples,
 64 Gauss nodes, Kerr + field plasma (band rule) + the in-stage collar, exponential
 Adams at rtol 1e-6 -- lowered from the reference's own translation
@@ -54,22 +54,25 @@ def load_workload():
 def algorithmic_bytes(rec) -> dict:
     """Bytes each kernel family must move per launch (reads + writes of its operands).
 
-    The column's three passes read the modal field each and write the projected partial
-    streams; nothing node-sized is stored.  The forward transform reads those partials.
+    The response column reads the modal field and the two temporal windows once and writes
+    the projected streams (and its tiles' running-integral sums); nothing node-sized is
+    stored, and the node groups' partial rows (summed by the tile's last CTA) are not counted.
+    The forward transform reads the projected streams and writes the spectra.
     """
     n = rec.n_cols * rec.n_omega
     c128, f64 = 16, 8
     nt, nn, nc = rec.n_to, rec.n_nodes, rec.n_cols
-    groups = -(-nn // 16)
-    tiles = nt // 64
+    k = (len(rec.taps) - 1) if rec.plasma_enabled else 0
+    owned = 256 - 2 * (2 * k + 1)
+    tiles = -(-nt // owned)
     streams = 3 if rec.plasma_enabled else 1
     absorber = 1 if rec.absorber_scheme == "nonlinear" else 0
-    partials = groups * streams * nc * nt * f64
+    projected = streams * nc * nt * f64
     return {
         "adams_predict": 14 * n * c128,
         "inverse_fft": n * c128 + (1 + absorber) * nc * nt * f64 + absorber * nt * f64,
-        "response_column": 3 * nc * nt * f64 + 2 * nt * f64 + 4 * nn * tiles * f64 + partials,
-        "forward_fft": partials + absorber * nc * nt * f64 + (streams + absorber) * n * c128,
+        "response_column": nc * nt * f64 + 2 * nt * f64 + 2 * nn * tiles * f64 + projected,
+        "forward_fft": projected + absorber * nc * nt * f64 + (streams + absorber) * n * c128,
         "stage_output": (streams + absorber) * n * c128 + rec.n_prefactor_terms * n * c128 + n * c128,
         "adams_correct": 15 * n * c128,
         "adams_accept": 4 * n * c128,
@@ -142,7 +145,7 @@ def cpu_arm(rec, pol, steps: int, warmup: int, budget_s: float, threads: int | N
 
 
 def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024) -> dict:
-    """BASELINE config 4's workload: n_runs seeded uneven capillary runs, stepped together.
+    """The parameter-scan workload (config 4): n_runs seeded uneven capillary runs, stepped together.
 
     Reports attempts per second of the batched solver (every batch step gives every run
     one exponential-Adams attempt, FP64) and of the plain path on the same runs one at a

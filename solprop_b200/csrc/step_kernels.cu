@@ -64,6 +64,7 @@ __device__ __forceinline__ double2 combine_terms(const double* w, int n_terms,
     return w[0] == 1.0 ? t : cscale(w[0], t);
   }
   double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 8
   for (int p = 0; p < n_terms; ++p) acc = cadd(acc, cscale(w[p], terms[(size_t)p * n + i]));
   return acc;
 }
@@ -119,6 +120,19 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
   const int width = ad.width, order = ad.order;
   double v[1] = {0.0};
   for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
+    // every operand row of this element is loaded up front, so that the loads overlap
+    // one another and the phi functions instead of waiting in the loops below
+    const double2 y = a.state[i];
+    constexpr int kRows = 5;  // the Adams order is at most 5: order and width - 1 rows
+    double2 rows[kRows], rate_rows[kRows], state_rows[kRows];
+#pragma unroll
+    for (int j = 0; j < kRows; ++j) {
+      if (j < order) rows[j] = a.store[(size_t)ad.slots[j] * a.n + i];
+      if (ad.compensated && j < width - 1) {
+        rate_rows[j] = a.rates[(size_t)ad.slots[j] * a.n + i];
+        state_rows[j] = a.states[(size_t)ad.slots[j] * a.n + i];
+      }
+    }
     const double2 x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
     double2 phi[kMaxWidth + 1];
     phi_functions(x, width, phi);
@@ -132,13 +146,16 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
     }
     a.flow[i] = fl;
     a.exponent[i] = x;
-    const double2 y = a.state[i];
     double2 total = make_double2(0.0, 0.0);
-    for (int k = 0; k < order; ++k) {
+#pragma unroll
+    for (int k = 0; k < kRows; ++k) {
+      if (k >= order) break;
       double2 comb = make_double2(0.0, 0.0);
-      for (int j = 0; j < order; ++j) {
+#pragma unroll
+      for (int j = 0; j < kRows; ++j) {
+        if (j >= order) break;
         const double c = ad.pred[j][k];
-        if (c != 0.0) comb = cadd(comb, cscale(c, a.store[(size_t)ad.slots[j] * a.n + i]));
+        if (c != 0.0) comb = cadd(comb, cscale(c, rows[j]));
       }
       total = cadd(total, cmul(mom[k], comb));
     }
@@ -147,11 +164,12 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
       // carried rows exp((1 - theta_j) x) ((D(z_j) - x/dz) u_j)   (adams_kernels.py carry)
       const double2 ref = make_double2(x.x / ad.dz, x.y / ad.dz);
       double2 comp = make_double2(0.0, 0.0);
-      for (int j = 0; j < width - 1; ++j) {
-        const int s = ad.slots[j];
+#pragma unroll
+      for (int j = 0; j < kRows; ++j) {
+        if (j >= width - 1) break;
         const double span = 1.0 - ad.nodes[j];
-        const double2 diff = csub(a.rates[(size_t)s * a.n + i], ref);
-        const double2 c = cmul(cexp(cscale(span, x)), cmul(diff, a.states[(size_t)s * a.n + i]));
+        const double2 diff = csub(rate_rows[j], ref);
+        const double2 c = cmul(cexp(cscale(span, x)), cmul(diff, state_rows[j]));
         a.carried[(size_t)j * a.n + i] = c;
         if (j < order) comp = cadd(comp, cscale(ad.comp_pred_main[j], c));
       }

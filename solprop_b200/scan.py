@@ -1,4 +1,4 @@
-"""Seeded capillary problems for parameter scans (BASELINE configs 4 and 5).
+"""Seeded capillary problems for parameter scans (configs 4 and 5: the batched scan and its surrogate).
 
 A scan point is a gas-filled capillary run: core radius, length, gas, constant pressure,
 pulse energy and duration at 800 nm, mode count and fine time-grid size.  This module
@@ -24,7 +24,7 @@ machine without solprop:
 * an in-stage temporal collar, a Gaussian input pulse in HE11 and one photon per mode
   per frequency bin of input shot noise, seeded (``noise.py``).
 
-The scan's parameter distribution is BASELINE config 4's (:func:`draw_points`).
+The scan's parameter distribution is config 4's (:func:`draw_points`).
 """
 
 from __future__ import annotations
@@ -87,7 +87,7 @@ class ScanPoint:
 
 
 def draw_points(n: int, seed: int, *, modes=(1, 8), grids=(12, 13, 14, 15)) -> list[ScanPoint]:
-    """BASELINE config 4's distribution: radius U[50, 150] um, length U[0.5, 2] m, gas from
+    """Config 4's distribution: radius U[50, 150] um, length U[0.5, 2] m, gas from
     {He, Ne, Ar}, pressure U[0.2, 3] bar, energy log-U[20, 500] uJ, FWHM U[5, 30] fs,
     mode count U{modes}, n_to uniform over 2**grids."""
     rng = np.random.default_rng(seed)

@@ -388,13 +388,13 @@ if __name__ == "__main__":
     if not only or "gnlse_raman" in only:
         gnlse_case("gnlse_raman", seed=3)
     if not only or "config2" in only:
-        # He 125 um, 1.5 m, 0.8 -> 0 bar, 800 nm, 7.5 fs, 275 uJ,
+        # config 2: He 125 um, 1.5 m, 0.8 -> 0 bar, 800 nm, 7.5 fs, 275 uJ,
         # HE11-HE14, 90 nm - 4 um, 400 fs, pow2 grid (n_to 16384), 64 Gauss nodes
         workload_case("config2", seed=4, gas="He", pressure=(0.8, 0.0), length=1.5,
                       n_t_limits=(90e-9, 4e-6), trange=400e-15, energy=275e-6, fwhm=7.5e-15,
                       modes=4, n_r=64, radial_rule="gauss", deep_uv=True)
     if not only or "config1" in only:
-        # Ar 125 um, 1 m, 1 bar, 800 nm, 10 fs, 100 uJ, HE11,
+        # config 1: Ar 125 um, 1 m, 1 bar, 800 nm, 10 fs, 100 uJ, HE11,
         # 150 nm - 4 um, 400 fs, pow2 grid (n_to 8192)
         workload_case("config1", seed=5, gas="Ar", pressure=1.0, length=1.0,
                       n_t_limits=(150e-9, 4e-6), trange=400e-15, energy=100e-6, fwhm=10e-15,

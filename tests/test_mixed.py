@@ -62,7 +62,7 @@ def test_mixed_fixed_schedule_error(case):
 
 @pytest.mark.parametrize("case", ["config1", "config2"])
 def test_mixed_full_adaptive_run(case):
-    """BASELINE configs 1 and 2 in full, mixed against FP64 on the device (which is the
+    """Configs 1 and 2 in full, mixed against FP64 on the device (which is the
     reference's arithmetic to 1e-10): the final spectra within ``RUN_TOL`` and the
     attempt counts within 20 %.  Each run chooses its own steps, so the difference
     includes the stepping error at rtol 1e-6 (measured 2.5e-6 and 3.6e-7)."""
