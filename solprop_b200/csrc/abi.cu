@@ -145,6 +145,8 @@ struct sp_problem {
   std::vector<unsigned char> active, norm;
   std::vector<double> phi_terms, pre_terms, synthesis, projection, rate_coeff, taps;
   Table phi_weights, phi_rate, pre_weights, density, kerr_density, plasma_density, preion, taper;
+  Table raman_rates[4], raman_density;
+  std::vector<double> raman_undamped;  // (raman_terms, 2 n_to)
 };
 
 static void validate(const sp_problem_desc* d) {
@@ -162,24 +164,43 @@ static void validate(const sp_problem_desc* d) {
   need(d->n_phi_terms >= 1 && d->n_phi_terms <= kMaxTerms && d->phi_terms, "phi terms");
   need(d->n_prefactor_terms >= 1 && d->n_prefactor_terms <= kMaxTerms && d->prefactor_terms,
        "prefactor terms");
-  if (d->grid_kind != 0)
-    throw Failure(SP_ERR_REFUSED, "the envelope grid is not built on the device yet");
+  if (d->grid_kind != 0 && d->grid_kind != 1) throw Failure(SP_ERR_ARGUMENT, "unknown grid kind");
+  const bool envelope = d->grid_kind == 1;
   if (d->n_pol * d->n_pol_transform != 1)
     throw Failure(SP_ERR_REFUSED, "two field components (vector Kerr) are not built yet");
   if (d->n_modes * d->n_pol > kMaxModes)
     throw Failure(SP_ERR_REFUSED, "more than 8 modal columns: the tensor-core transform is not built yet");
-  if (d->raman_enabled) throw Failure(SP_ERR_REFUSED, "field-grid Raman is not built yet");
-  if (d->kerr_enabled && d->kerr_analytic)
-    throw Failure(SP_ERR_REFUSED, "the analytic Kerr cubic belongs to the envelope grid");
+  if (envelope) {
+    // the envelope route: one modal column on one node (the single-mode GNLSE)
+    if (d->n_modes * d->n_pol != 1 || d->n_nodes != 1)
+      throw Failure(SP_ERR_REFUSED, "the envelope grid with more than one mode or node is not built yet");
+    if (d->n_to > kMaxEnvelopeSamples)
+      throw Failure(SP_ERR_REFUSED, "the envelope grid above 4096 samples is not built yet");
+    if (d->plasma_enabled) throw Failure(SP_ERR_REFUSED, "envelope plasma is not built yet");
+    if (d->absorber_in_stage)
+      throw Failure(SP_ERR_REFUSED, "the in-stage absorber on the envelope grid is not built yet");
+    if (d->kerr_enabled && (!d->kerr_analytic || d->kerr_take_real ||
+                            (d->carrier && d->kerr_harmonic != 0.0)))
+      throw Failure(SP_ERR_REFUSED, "the envelope route takes the analytic Kerr cubic without a harmonic");
+    if (d->raman_enabled) {
+      need(d->raman_terms >= 1 && d->raman_terms <= 4 && d->raman_undamped, "Raman terms");
+      if (d->raman_thg) throw Failure(SP_ERR_REFUSED, "a third-harmonic Raman drive on the envelope grid");
+    }
+  } else {
+    if (d->raman_enabled) throw Failure(SP_ERR_REFUSED, "field-grid Raman is not built yet");
+    if (d->kerr_enabled && d->kerr_analytic)
+      throw Failure(SP_ERR_REFUSED, "the analytic Kerr cubic belongs to the envelope grid");
+  }
   if (d->plasma_enabled) {
     need(d->rate_intervals >= 1 && d->rate_coefficients, "rate table");
     need(d->n_taps >= 1 && d->n_taps - 1 <= kHalo && d->taps,
          "running-integral taps: a band-rule half-width above 8 is not built");
   }
   if (d->absorber_in_stage) need(d->temporal_absorber_fine != nullptr, "absorber rate");
+  const long long n_fine = envelope ? d->n_to : d->n_to / 2 + 1;
   for (int j = 0; j < d->n_omega; ++j) {
     const long long k = d->crop_index[j];
-    need(k >= 0 && k <= d->n_to / 2, "crop_index outside the fine spectrum");
+    need(k >= 0 && k < n_fine, "crop_index outside the fine spectrum");
   }
 }
 
@@ -196,6 +217,8 @@ struct sp_workspace {
   DevBuf<int> fine_to_coarse, rows, chain_flags;
   DevBuf<unsigned> arrivals;
   DevBuf<unsigned long long> ticket;  // the response column's tile counter
+  DevBuf<double2> env_twiddles;       // envelope route: exp(-2 pi i m / (2 n_to)), m < n_to
+  DevBuf<double> raman_undamped;
   // the mixed-precision form's FP32 copies of the source evaluation's buffers
   int precision = SP_PRECISION_FP64;
   struct {
@@ -279,6 +302,10 @@ static void fill_stage(sp_workspace* ws, int slot, double z0, double z1) {
   s.kerr_density = P.kerr_density.present() ? P.kerr_density.scalar(z1, 1.0) : s.density;
   s.plasma_density = P.plasma_density.scalar(z1, s.density);
   s.preionisation = P.preion.scalar(z1, 0.0);
+  if (P.d.raman_enabled) {  // translate/stage.py scalars: the damping rates and the density
+    for (int r = 0; r < P.d.raman_terms; ++r) s.raman_rates[r] = P.raman_rates[r].scalar(z1, 0.0);
+    s.raman_density = P.raman_density.scalar(z1, s.density);
+  }
   s.n_phi = P.d.n_phi_terms;
   s.n_pre = P.d.n_prefactor_terms;
   if (!P.d.phi_expansion) {
@@ -421,7 +448,30 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
                         double2* out, bool quiet) {
   const sp_problem& P = *ws->P;
   const bool absorber = P.d.absorber_in_stage && !quiet;
-  if (ws->precision == SP_PRECISION_MIXED) {
+  if (P.d.grid_kind == 1) {
+    const sp_problem_desc& d = P.d;
+    EnvelopeArgs ea{};
+    ea.stage = ws->stage.p + slot;
+    ea.lab = lab;
+    ea.crop = ws->crop.p;
+    ea.twiddles = ws->env_twiddles.p;
+    ea.t_window = ws->t_window.p;
+    ea.raman_undamped = d.raman_enabled ? ws->raman_undamped.p : nullptr;
+    ea.spectra = ws->spectra.p;
+    ea.synthesis = P.synthesis[0];
+    ea.projection = P.projection[0];
+    ea.dt = d.dt_fine;
+    ea.kerr = d.kerr_enabled;
+    ea.kerr_coefficient = d.kerr_coefficient;
+    ea.kerr_self = d.kerr_self;
+    ea.kerr_conjugate = d.kerr_conjugate;
+    ea.raman_fraction = d.raman_fraction;
+    ea.raman_terms = d.raman_enabled ? d.raman_terms : 0;
+    ea.n_omega = d.n_omega;
+    ea.n_to = d.n_to;
+    ea.log_n_to = ws->log_n_to;
+    { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_envelope(ea, ws->stream)); }
+  } else if (ws->precision == SP_PRECISION_MIXED) {
     const auto ia = inverse_args(ws, lab, absorber);
     { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
     const auto ca = column_args<float>(ws, ws->stage.p + slot);
@@ -522,8 +572,9 @@ static void build_workspace(sp_workspace* ws) {
   std::vector<double> taps = P.taps.empty() ? std::vector<double>(1, 1.0) : P.taps;
   ws->taps.upload(taps.data(), taps.size(), s);
   ws->crop.upload(P.crop.data(), d.n_omega, s);
-  std::vector<int> f2c(d.n_to / 2 + 1, -1);
-  for (int j = 0; j < d.n_omega; ++j) f2c[P.crop[j]] = j;
+  // the fine spectrum's bins: n_to / 2 + 1 on the field grid, n_to on the envelope grid
+  std::vector<int> f2c(d.grid_kind == 1 ? d.n_to : d.n_to / 2 + 1, -1);
+  for (int j = 0; j < d.n_omega; ++j) f2c.at(P.crop[j]) = j;
   ws->fine_to_coarse.upload(f2c.data(), f2c.size(), s);
   // stream rows: [0, 3 n_cols) P X Z, then absorber [3 n_cols, 4 n_cols); a second list
   // at 4 n_cols for the no-plasma case: P rows then absorber rows
@@ -563,6 +614,16 @@ static void build_workspace(sp_workspace* ws) {
   ws->norms.zero(s);
   ws->launches = 5;
   if (ws->precision == SP_PRECISION_MIXED) build_mixed(ws, tw, rc, taps);
+  if (d.grid_kind == 1) {
+    std::vector<double2> tw2(d.n_to);
+    for (int m = 0; m < d.n_to; ++m) {
+      long double ang = two_pi * (long double)m / (long double)(2 * d.n_to);
+      tw2[m] = make_double2((double)cosl(ang), (double)(-sinl(ang)));
+    }
+    ws->env_twiddles.upload(tw2.data(), tw2.size(), s);
+    if (d.raman_enabled) ws->raman_undamped.upload(P.raman_undamped.data(), P.raman_undamped.size(), s);
+    CUDA_CHECK(cudaStreamSynchronize(s));
+  }
   CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
@@ -1158,6 +1219,11 @@ sp_status sp_problem_create(const sp_problem_desc* d, sp_problem** out) {
     P->plasma_density.load(d->plasma_density);
     P->preion.load(d->preionisation);
     P->taper.load(d->taper_scale);
+    if (d->raman_enabled) {
+      for (int r = 0; r < d->raman_terms; ++r) P->raman_rates[r].load(d->raman_rates[r]);
+      P->raman_density.load(d->raman_density);
+      P->raman_undamped.assign(d->raman_undamped, d->raman_undamped + (size_t)d->raman_terms * 2 * d->n_to);
+    }
     if (d->phi_expansion && (!P->phi_weights.present() || !P->phi_rate.present()))
       throw Failure(SP_ERR_ARGUMENT, "an expansion of Phi needs its weight and rate tables");
     *out = P.release();
@@ -1179,6 +1245,8 @@ sp_status sp_workspace_create_ex(const sp_problem* problem, int device, int prec
     if (!problem || !out) throw Failure(SP_ERR_ARGUMENT, "NULL problem or out");
     if (precision != SP_PRECISION_FP64 && precision != SP_PRECISION_MIXED)
       throw Failure(SP_ERR_ARGUMENT, "unknown precision");
+    if (precision == SP_PRECISION_MIXED && problem->d.grid_kind == 1)
+      throw Failure(SP_ERR_REFUSED, "the mixed precision of the envelope route is not built yet");
     CUDA_CHECK(cudaSetDevice(device));
     static bool configured = false;
     if (!configured) {
@@ -1596,6 +1664,8 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
         throw Failure(SP_ERR_REFUSED, "a scan steps adaptive exponential-Adams runs only");
       if (problems[r]->d.phi_expansion)
         throw Failure(SP_ERR_REFUSED, "a scan run with a varying operator (Phi expansion)");
+      if (problems[r]->d.grid_kind != 0)
+        throw Failure(SP_ERR_REFUSED, "a scan run on the envelope grid");
       auto w = std::make_unique<sp_workspace>();
       w->P = problems[r];
       w->device = device;
@@ -1826,6 +1896,8 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
                                        int quiet, void* out, void* stream_handle) {
   return guarded([&] {
     if (!problem || !lab || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    if (problem->d.grid_kind != 0)
+      throw Failure(SP_ERR_REFUSED, "the no-allocation entry point takes field-grid problems");
     int device = 0;
     CUDA_CHECK(cudaGetDevice(&device));
     unsigned char* base = noalloc_base(device);
@@ -1901,8 +1973,8 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     std::vector<double> taps = P.taps.empty() ? std::vector<double>(1, 1.0) : P.taps;
     put(ws.taps, taps.data(), taps.size(), s);
     put(ws.crop, P.crop.data(), d.n_omega, s);
-    std::vector<int> f2c(d.n_to / 2 + 1, -1);
-    for (int j = 0; j < d.n_omega; ++j) f2c[P.crop[j]] = j;
+    std::vector<int> f2c(d.n_to / 2 + 1, -1);  // field grid only (checked above)
+    for (int j = 0; j < d.n_omega; ++j) f2c.at(P.crop[j]) = j;
     put(ws.fine_to_coarse, f2c.data(), f2c.size(), s);
     std::vector<int> rows;
     for (int r = 0; r < 4 * P.n_cols; ++r) rows.push_back(r);

@@ -125,6 +125,23 @@ struct OutputArgs {
   int n_cols, n_omega, plasma, absorber;
 };
 
+// The envelope route (envelope_kernels.cu): one modal column on one node, one CTA.
+constexpr int kMaxEnvelopeSamples = 4096;
+struct EnvelopeArgs {
+  const StageScalarsDev* stage;
+  const double2* lab;            // (n_omega)
+  const long long* crop;         // (n_omega): coarse bin -> fine bin
+  const double2* twiddles;       // exp(-2 pi i m / (2 n_to)), m < n_to
+  const double* t_window;        // (n_to)
+  const double* raman_undamped;  // (raman_terms, 2 n_to), or null
+  double2* spectra;              // (n_omega): the projected polarisation's spectrum
+  double synthesis, projection, dt;
+  double kerr_coefficient, kerr_self, kerr_conjugate, raman_fraction;
+  int kerr, raman_terms, n_omega, n_to, log_n_to;
+};
+cudaError_t launch_envelope(const EnvelopeArgs& a, cudaStream_t stream);
+cudaError_t configure_envelope_kernels();
+
 cudaError_t configure_source_kernels();
 int fft_cluster_size(int n_to);
 template <class R>

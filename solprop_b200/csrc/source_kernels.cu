@@ -247,6 +247,8 @@ cudaError_t configure_source_kernels() {
   }
   e = configure_column_kernels();
   if (e != cudaSuccess) return e;
+  e = configure_envelope_kernels();
+  if (e != cudaSuccess) return e;
   return configure_cluster_fft();
 }
 

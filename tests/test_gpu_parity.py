@@ -3,7 +3,8 @@
 One source evaluation against the golden vectors at 1e-10 relative L2 (the contract's
 per-step bar; measured values are ~1e-15); fixed schedules plane by plane at 1e-10;
 adaptive runs within the stepper's rtol at every plane, with the attempt counts of
-the reference.
+the reference.  The cases: two capillaries on the field grid with plasma and the
+exponential-Adams stepper, and the envelope GNLSE with Kerr and Raman on DOPRI5.
 """
 
 import numpy as np
@@ -25,7 +26,7 @@ def _workspace(case, fixed=False):
     return rec, problem, _lib.Workspace(problem)
 
 
-@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he", "config1", "config2"])
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he", "gnlse_raman", "config1", "config2"])
 @pytest.mark.parametrize("index", [0, 1])
 def test_source_matches_reference(case, index):
     rec, problem, ws = _workspace(case)
@@ -54,7 +55,7 @@ def test_quiet_collar_drops_the_absorber():
     assert rel(got, S.lab_source(rec, g["src0.lab"], 0.0, quiet=True)) < SOURCE_TOL
 
 
-@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he"])
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he", "gnlse_raman"])
 def test_fixed_schedule_matches_reference(case):
     rec, problem, ws = _workspace(case, fixed=True)
     g = golden(case)
@@ -73,7 +74,7 @@ def test_fixed_schedule_matches_reference(case):
     assert plane == len(zs)
 
 
-@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he"])
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he", "gnlse_raman"])
 def test_adaptive_run_matches_reference(case):
     rec, problem, ws = _workspace(case)
     g = golden(case)
