@@ -1457,10 +1457,14 @@ namespace {
 
 struct FftClass {
   int n_to = 0;
-  bool cluster = false;
+  bool cluster_inv = false, cluster_fwd = false;
   DevBuf<int2> inv_items, fwd_items;
   int n_inv = 0, n_fwd = 0;
 };
+
+// the largest transform row (complex samples x element size) a batched launch keeps in
+// one CTA's shared memory
+constexpr size_t kBatchedRowBytes = 128 * 1024;
 
 template <class T>
 T* pinned(size_t n) {
@@ -1524,14 +1528,14 @@ template <class R>
 void scan_transforms(sp_scan* S, const int* flags, const InverseArgs* inv, const ColumnArgsT<R>* col,
                      const ForwardArgsT<R>* fwd) {
   for (auto& c : S->classes) {
-    if (c->cluster)
+    if (c->cluster_inv)
       CUDA_CHECK(launch_inverse_cluster_b(inv, c->inv_items.p, flags, c->n_inv, c->n_to, S->stream));
     else
       CUDA_CHECK(launch_inverse_b(inv, c->inv_items.p, flags, c->n_inv, c->n_to, S->stream));
   }
   CUDA_CHECK(launch_column_b(col, S->col_items.p, flags, S->n_col_items, S->stream));
   for (auto& c : S->classes) {
-    if (c->cluster)
+    if (c->cluster_fwd)
       CUDA_CHECK(launch_forward_cluster_b(fwd, c->fwd_items.p, flags, c->n_fwd, c->n_to, S->stream));
     else
       CUDA_CHECK(launch_forward_b(fwd, c->fwd_items.p, flags, c->n_fwd, c->n_to, S->stream));
@@ -1741,7 +1745,13 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     for (int n_to : sizes) {
       auto c = std::make_unique<FftClass>();
       c->n_to = n_to;
-      c->cluster = fft_cluster_size(n_to) > 1;
+      // Batched rows are many: a row is one CTA whenever it fits in shared memory (no
+      // cluster exchange); only the longest rows are split over a cluster.
+      // (the inverse transform is FP64 in both precisions)
+      const size_t fwd_bytes = (size_t)(n_to / 2) * (precision == SP_PRECISION_MIXED ? 8 : 16);
+      const size_t inv_bytes = (size_t)(n_to / 2) * 16;
+      c->cluster_inv = fft_cluster_size(n_to) > 1 && inv_bytes > kBatchedRowBytes;
+      c->cluster_fwd = fft_cluster_size(n_to) > 1 && fwd_bytes > kBatchedRowBytes;
       std::vector<int2> inv, fwd;
       for (int r = 0; r < R; ++r) {
         sp_workspace* w = S->ws[r].get();

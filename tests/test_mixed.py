@@ -9,8 +9,9 @@ running integrals in FP64.  Its error against the FP64 reference is stated per r
 * an adaptive run: every plane within the run's rtol (its own step sequence differs
   from the FP64 run's, so the difference includes the stepping error), and the full
   config-1 and config-2 runs within ``RUN_TOL`` of the FP64 ones;
-* a batched mixed scan against the same runs alone: FP32 rounding only (the two
-  launches are separate compilations, free to contract products differently).
+* a batched mixed scan against the same runs alone: FP32 rounding only (a batched row
+  that fits in one CTA's shared memory is transformed there, a lone run's row of more
+  than 4096 samples over a cluster; the two factorisations round differently).
 """
 
 import numpy as np
@@ -121,4 +122,4 @@ def test_mixed_scan_matches_mixed_single_runs():
         session = ws.start(pol)
         for _ in range(int(info.attempts)):
             session.advance(1)
-        assert rel(state, session.export()) < 1e-6, i
+        assert rel(state, session.export()) < 1e-5, i
