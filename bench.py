@@ -39,6 +39,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "config2"
+# DRAM bytes read + written per k_column launch on this workload, from one ncu capture
+# (profiles/k_column_config2.md: 0.95 MB read, 9 kB written; the rest stays in L2)
+COLUMN_TRAFFIC = 964_096
 METRIC = "steps/s (exponential-Adams attempts, plain FP64, config 2 four-mode He capillary)"
 UNIT = "steps/s"
 
@@ -144,19 +147,34 @@ def cpu_arm(rec, pol, steps: int, warmup: int, budget_s: float, threads: int | N
     return done, elapsed
 
 
-def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024) -> dict:
+def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024,
+             rank: int = 0, world: int = 1) -> dict:
     """The parameter-scan workload (config 4): n_runs seeded uneven capillary runs, stepped together.
 
     Reports attempts per second of the batched solver (every batch step gives every run
     one exponential-Adams attempt, FP64) and of the plain path on the same runs one at a
-    time (one session per run, its attempts back to back), on the device's clock.
+    time (one session per run, its attempts back to back), on the device's clock.  With
+    several ranks each solves its cost-balanced share of the runs (``scan.shard``, no
+    exchange); attempts add over ranks and the time is the slowest rank's.
     """
     import torch
 
     from solprop_b200 import _lib, scan
 
     points = scan.draw_points(n_runs, seed)
+    points = [points[i] for i in scan.shard(points, rank, world)]
     built = [scan.capillary_record(p) for p in points]
+
+    def across_ranks(attempts: float, ms: float) -> tuple[float, float]:
+        if world == 1:
+            return attempts, ms
+        import torch.distributed as dist
+
+        a = torch.tensor([attempts], dtype=torch.float64, device=f"cuda:{device}")
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(a, op=dist.ReduceOp.SUM)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(a.item()), float(t.item())
     records, policies = [b[0] for b in built], [b[1] for b in built]
     batched = {}
     for precision in ("fp64", "mixed"):
@@ -170,13 +188,13 @@ def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024
         status = sc.advance(steps)
         e_ev.record(stream)
         torch.cuda.synchronize()
-        ms = s_ev.elapsed_time(e_ev)
-        batched[precision] = {"attempts_per_s": (status.attempts - before) / (ms / 1e3),
+        attempts, ms = across_ranks(status.attempts - before, s_ev.elapsed_time(e_ev))
+        batched[precision] = {"attempts_per_s": attempts / (ms / 1e3),
                               "ms_per_batch_step": ms / steps, "active_runs_at_end": status.active}
         sc.close()
     # the plain path: each run alone, three attempts after one warm-up
     plain_ms, plain_attempts = 0.0, 0
-    sample = list(range(0, n_runs, max(1, n_runs // 64)))
+    sample = list(range(0, len(points), max(1, n_runs // 64)))
     for i in sample:
         problem = _lib.Problem(records[i])
         ws = _lib.Workspace(problem, device)
@@ -195,11 +213,12 @@ def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024
         session.close()
         ws.close()
         problem.close()
+    plain_attempts, plain_ms = across_ranks(plain_attempts, plain_ms)
     plain = plain_attempts / (plain_ms / 1e3)
     return {"workload": f"config 4: {n_runs} seeded capillary runs (radius 50-150 um, length "
                         "0.5-2 m, He/Ne/Ar, 0.2-3 bar, 20-500 uJ, 5-30 fs, 1-8 modes, "
                         "n_to 2^12-2^15), Kerr + plasma + input shot noise, exp. Adams rtol 1e-6",
-            "batch_steps": steps, "batched": batched,
+            "ranks": world, "batch_steps": steps, "batched": batched,
             "plain_fp64_attempts_per_s": plain, "plain_sample_runs": len(sample),
             "speedup_vs_plain": {k: v["attempts_per_s"] / plain for k, v in batched.items()}}
 
@@ -307,7 +326,7 @@ def main() -> int:
     achieved = algo.get(top, 0) / (top_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peak,
                 "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": COLUMN_TRAFFIC if top == "response_column" else None,
                 "algorithmic_bytes": algo.get(top, 0), "avg_launch_ms": top_ms,
                 "kernels_ms_per_step": {k: v[0] / kernel_steps for k, v in kernels.items() if v[1]}}
 
@@ -342,7 +361,7 @@ def main() -> int:
 
     scan_result = None
     if args.scan_runs > 0:
-        scan_result = scan_leg(local, args.scan_runs, args.scan_steps, warmup=3)
+        scan_result = scan_leg(local, args.scan_runs, args.scan_steps, warmup=3, rank=rank, world=world)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,

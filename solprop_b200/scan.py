@@ -256,6 +256,39 @@ def capillary_record(p: ScanPoint) -> tuple[ProblemRecord, dict]:
     return rec, policy
 
 
+def shard(points, rank: int, world: int) -> list[int]:
+    """The indices of the points rank ``rank`` of ``world`` solves: the runs sorted by their
+    cost (fine samples x modes, the response column's work) and dealt round-robin, so every
+    rank gets a like share of each size.  Runs are independent: no exchange while they run."""
+    if not 0 <= rank < world:
+        raise ValueError(f"rank {rank} outside a world of {world}")
+    order = sorted(range(len(points)), key=lambda i: (-points[i].n_to * points[i].modes, i))
+    return sorted(i for k, i in enumerate(order) if k % world == rank)
+
+
+def gather_by_index(indices, values, n_total: int, group=None):
+    """Every rank's per-point rows, assembled in point order on rank 0 (None elsewhere):
+    the scan's one collective, after all runs have finished."""
+    import torch.distributed as dist
+
+    payload = (list(indices), np.asarray(values))
+    gathered = [None] * dist.get_world_size(group) if dist.get_rank(group) == 0 else None
+    dist.gather_object(payload, gathered, dst=0, group=group)
+    if gathered is None:
+        return None
+    first = next(v for _, v in gathered if len(v))
+    out = np.zeros((n_total,) + first.shape[1:], dtype=first.dtype)
+    seen = np.zeros(n_total, bool)
+    for idx, vals in gathered:
+        for i, v in zip(idx, vals):
+            if seen[i]:
+                raise ValueError(f"point {i} solved twice")
+            out[i], seen[i] = v, True
+    if not seen.all():
+        raise ValueError(f"{int((~seen).sum())} points solved by no rank")
+    return out
+
+
 def exit_log_spectrum(rec: ProblemRecord, state: np.ndarray, bins: int = 2048) -> np.ndarray:
     """The surrogate's target: log10 of the exit energy spectral density, summed over modes,
     on ``bins`` wavelengths from 100 nm to 4 um (interpolated), floored at 1e-30."""
