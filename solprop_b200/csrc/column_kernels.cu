@@ -435,13 +435,18 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   }
 }
 
+// resident CTAs per SM: two in FP64 (128 registers), three in FP32 (85)
+template <class R> constexpr int column_residency() { return sizeof(R) == 8 ? 2 : 3; }
+
 template <class R>
-__global__ void __launch_bounds__(kThreads, 2) k_column(ColumnArgsT<R> a) { column_body(a); }
+__global__ void __launch_bounds__(kThreads, column_residency<R>()) k_column(ColumnArgsT<R> a) {
+  column_body(a);
+}
 
 // batched: items[blockIdx.x].x = the run; a run's CTAs take their tiles from its counter
 template <class R>
-__global__ void __launch_bounds__(kThreads, 2) k_column_b(const ColumnArgsT<R>* args, const int4* items,
-                                                          const int* flags) {
+__global__ void __launch_bounds__(kThreads, column_residency<R>())
+    k_column_b(const ColumnArgsT<R>* args, const int4* items, const int* flags) {
   const int run = items[blockIdx.x].x;
   if (!flags[run]) return;  // every CTA of an idle run leaves before its ticket
   column_body(args[run]);
