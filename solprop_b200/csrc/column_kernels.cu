@@ -263,6 +263,7 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   R* scratch = modal + (size_t)3 * kGroup * kPitch;
   __shared__ unsigned long long ticket;
   __shared__ R wt[kMaxModes * kGroup];
+  __shared__ R gate[kWindow], gate_d[kWindow];  // the temporal window g and g' on the window
   if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1ull);
   __syncthreads();
   const unsigned long long epoch = ticket / (unsigned long long)a.n_blocks;
@@ -285,6 +286,12 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   for (int k = threadIdx.x; k < a.n_modes * kGroup; k += blockDim.x) {
     const int m = k / kGroup, w = k % kGroup, nd = group * kGroup + w;
     wt[k] = nd < a.n_nodes ? a.projection[m * a.n_nodes + nd] / tau : R(0);
+  }
+  for (int u = threadIdx.x; u < kWindow; u += blockDim.x) {
+    const int t = tw + u;
+    const bool in = t >= 0 && t < a.n_to;
+    gate[u] = in ? a.t_window[t] : R(0);
+    gate_d[u] = in ? a.t_window_derivative[t] : R(0);
   }
   __syncthreads();
   // synthesis and rate on the window
@@ -367,11 +374,11 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
     const R rho = R(st.plasma_density), ip = R(a.ionisation_potential);
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
-      const int u = kPer * lane + j, t = tw + u;
+      const int u = kPer * lane + j;
       R p = R(0), x = R(0), z = R(0);
       if (live && u >= A && u < own_hi) {
         const R e = E[j];
-        const R win = a.t_window[t];
+        const R win = gate[u];
         p = (a.kerr ? factor * (e * e) * e : R(0)) * win;
         if (plasma) {
           const R w = W[j], f = F[j];
@@ -380,7 +387,7 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
           if (w > R(0) && squared > R(0)) scale = ip * w * (R(1) - f) / squared;
           const R current = rho * (J[j] + scale * e);
           x = win * current;
-          z = a.t_window_derivative[t] * current;
+          z = gate_d[u] * current;
         }
       }
       streams[(0 * kGroup + warp) * kPitch + pad(u)] = p;
@@ -449,7 +456,7 @@ __global__ void __launch_bounds__(kThreads, column_residency<R>())
     k_column_b(const ColumnArgsT<R>* args, const int4* items, const int* flags) {
   const int run = items[blockIdx.x].x;
   if (!flags[run]) return;  // every CTA of an idle run leaves before its ticket
-  column_body(args[run]);
+  column_body(own_args(args, run));
 }
 
 template <class R>

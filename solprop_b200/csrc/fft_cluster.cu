@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(512) k_inverse_cluster_b(const InverseArgsT<R>
                                                           const int* flags) {
   const int2 it = items[blockIdx.y];
   if (!flags[it.x]) return;  // uniform over the cluster: every CTA of it has this item
-  inverse_cluster_body(args[it.x], it.y);
+  inverse_cluster_body(own_args(args, it.x), it.y);
 }
 
 // forward (r2c): stream rows -> cropped coarse spectra
@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(512) k_forward_cluster_b(const ForwardArgsT<R>
                                                           const int* flags) {
   const int2 it = items[blockIdx.y];
   if (!flags[it.x]) return;
-  forward_cluster_body(args[it.x], it.y);
+  forward_cluster_body(own_args(args, it.x), it.y);
 }
 
 static cudaError_t launch_cluster(const void* kernel, dim3 grid, int threads, size_t shm, int C,

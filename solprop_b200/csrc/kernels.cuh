@@ -14,6 +14,17 @@ constexpr int kColumnStatus = kMaxOrders + 1;  // norms slot the response column
 constexpr int kMaxSlots = 8;       // history rows (order + 2)
 constexpr int kNormBlocks = 148;   // partial-sum blocks of the norm reductions
 
+// A batched kernel's argument record, copied once per CTA into shared memory: the
+// kernel body reads its fields throughout, and from the global array of records each read
+// would be a load of its own.  Every thread of the CTA must call it.
+template <class T>
+__device__ __forceinline__ const T& own_args(const T* args, int run) {
+  __shared__ T own;
+  if (threadIdx.x == 0) own = args[run];
+  __syncthreads();
+  return own;
+}
+
 struct StageScalarsDev {
   double z0, z1, taper, density, kerr_density, plasma_density, preionisation, raman_density;
   int n_pre, n_phi;

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(1024) k_inverse_field_b(const InverseArgsT<R>*
                                                          const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  inverse_field_body(args[it.x], it.y);
+  inverse_field_body(own_args(args, it.x), it.y);
 }
 
 // ----------------------------------------------------------------------------- K4
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(1024) k_forward_field_b(const ForwardArgsT<R>*
                                                          const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  forward_field_body(args[it.x], it.y);
+  forward_field_body(own_args(args, it.x), it.y);
 }
 
 // ----------------------------------------------------------------------------- K5
@@ -199,7 +199,7 @@ __global__ void k_stage_output(OutputArgs a) { stage_output_any(a, blockIdx.x); 
 __global__ void k_stage_output_b(const OutputArgs* args, const int2* items, const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  stage_output_any(args[it.x], it.y);
+  stage_output_any(own_args(args, it.x), it.y);
 }
 
 // ----------------------------------------------------------------------------- launch
@@ -235,7 +235,7 @@ cudaError_t launch_output(const OutputArgs& a, cudaStream_t stream) {
 }
 
 cudaError_t configure_source_kernels() {
-  const int max_shm = 227 * 1024;
+  const int max_shm = 200 * 1024;  // rows of up to 128 KB, and room for static shared memory
   cudaError_t e;
   const void* kernels[8] = {(const void*)k_inverse_field<double>, (const void*)k_forward_field<double>,
                             (const void*)k_inverse_field_b<double>, (const void*)k_forward_field_b<double>,

@@ -294,24 +294,24 @@ __global__ void __launch_bounds__(256) k_adams_predict_b(const StepArgs* args, c
                                                         const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  adams_predict_body(args[it.x], it.y);
+  adams_predict_body(own_args(args, it.x), it.y);
 }
 __global__ void __launch_bounds__(256) k_adams_correct_b(const StepArgs* args, const int2* items,
                                                         const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  adams_correct_body(args[it.x], it.y);
+  adams_correct_body(own_args(args, it.x), it.y);
 }
 __global__ void k_adams_accept_b(const StepArgs* args, const int2* items, const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  const StepArgs& a = args[it.x];
+  const StepArgs& a = own_args(args, it.x);
   adams_accept_body(a, a.adams->free_slot, a.states != nullptr, it.y);
 }
 __global__ void k_adams_start_b(const StepArgs* args, const int2* items, const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  const StepArgs& a = args[it.x];
+  const StepArgs& a = own_args(args, it.x);
   adams_start_body(a, a.states != nullptr, it.y);
 }
 
