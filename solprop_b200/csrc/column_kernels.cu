@@ -69,9 +69,24 @@ __device__ __forceinline__ float rate_of(const ColumnArgsT<float>& a, float magn
   if (idx < 0) idx = 0;
   if (idx > n - 1) idx = n - 1;
   const float* c = a.rate_coefficients;
-  const float local = log1pf(fmaf(magnitude, c[4 * n + idx], -1.0f));
-  return c[3 * n + idx] * expf(((c[idx] * local + c[n + idx]) * local + c[2 * n + idx]) * local);
+  // l = log1p(v), v = |E| / knot - 1: within an interval |v| is a few 1e-2 at most, where
+  // the series to v^5 is as good as FP32 (its first omitted term, v^6 / 6, stays below
+  // 6e-8 |v|)
+  const float v = fmaf(magnitude, c[4 * n + idx], -1.0f);
+  float local;
+  if (fabsf(v) < 0.05f)
+    local = v * (1.0f + v * (-0.5f + v * (1.0f / 3.0f + v * (-0.25f + v * 0.2f))));
+  else
+    local = log1pf(v);
+  // the exponent stays small (|l| <= the interval's width), where the fast exponential
+  // keeps its relative error to a few units in the last place
+  return c[3 * n + idx] * __expf(((c[idx] * local + c[n + idx]) * local + c[2 * n + idx]) * local);
 }
+
+// a / b: exact in FP64; in FP32 the fast reciprocal-based division (2 ulp), for b far
+// below 2^126 (here |E|^2)
+__device__ __forceinline__ double divide(double a, double b) { return a / b; }
+__device__ __forceinline__ float divide(float a, float b) { return __fdividef(a, b); }
 
 // the ionised fraction f = 1 - (1 - f0) e^-x (plasma.py:104-191); in FP32 as
 // f0 + (1 - f0)(1 - e^-x) through expm1, which keeps its relative accuracy for small x
@@ -112,6 +127,12 @@ __device__ __forceinline__ void reflect_ends(R (&v)[kPer], R* row, int tw, int n
 // window are garbage and lie in the halo, which the caller does not use)
 template <class R>
 __device__ __forceinline__ void band_filter(const R (&y)[kPer], R (&out)[kPer], const R* taps, int K) {
+  if (K == 0) {  // the trapezoid rule: the single tap (warp-uniform)
+    const R c0 = taps[0];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) out[j] = c0 * y[j];
+    return;
+  }
   R ext[3 * kPer];  // the left neighbour's samples, this lane's, the right neighbour's
 #pragma unroll
   for (int j = 0; j < kPer; ++j) {
@@ -384,7 +405,7 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
           const R w = W[j], f = F[j];
           const R squared = fabs(e) * fabs(e);
           R scale = R(0);
-          if (w > R(0) && squared > R(0)) scale = ip * w * (R(1) - f) / squared;
+          if (w > R(0) && squared > R(0)) scale = divide(ip * w * (R(1) - f), squared);
           const R current = rho * (J[j] + scale * e);
           x = win * current;
           z = gate_d[u] * current;
