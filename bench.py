@@ -190,7 +190,8 @@ def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024
         torch.cuda.synchronize()
         attempts, ms = across_ranks(status.attempts - before, s_ev.elapsed_time(e_ev))
         batched[precision] = {"attempts_per_s": attempts / (ms / 1e3),
-                              "ms_per_batch_step": ms / steps, "active_runs_at_end": status.active}
+                              "ms_per_batch_step": ms / steps, "active_runs_at_end": status.active,
+                              "transform_plan": sc.describe().strip().splitlines()}
         sc.close()
     # the plain path: each run alone, three attempts after one warm-up
     plain_ms, plain_attempts = 0.0, 0

@@ -127,6 +127,7 @@ SIGNATURES = {
     "sp_scan_create_ex": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p), C.POINTER(SpRunDesc), C.c_int, C.c_int,
                                  C.POINTER(C.c_void_p)]),
     "sp_scan_advance": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SpScanStatus)]),
+    "sp_scan_describe": (C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "sp_scan_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(SpBatch)]),
     "sp_scan_stream": (C.c_void_p, [C.c_void_p]),
     "sp_scan_destroy": (C.c_int, [C.c_void_p]),
@@ -472,6 +473,12 @@ class Scan:
                                           C.byref(handle)))
         self.handle = handle
         self.status = SpScanStatus()
+
+    def describe(self) -> str:
+        """The transform plan the autotuner chose, one line per grid size."""
+        buf = C.create_string_buffer(8192)
+        self._lib.sp_scan_describe(self.handle, buf, 8192)
+        return buf.value.decode()
 
     def advance(self, steps: int = 1) -> SpScanStatus:
         check(library().sp_scan_advance(self.handle, int(steps), C.byref(self.status)))

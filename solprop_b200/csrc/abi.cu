@@ -1458,12 +1458,14 @@ namespace {
 struct FftClass {
   int n_to = 0;
   bool cluster_inv = false, cluster_fwd = false;
+  // the autotuner's measurements (ms per launch over this class's rows; < 0: not a candidate)
+  float inv_single_ms = -1, inv_cluster_ms = -1, fwd_single_ms = -1, fwd_cluster_ms = -1;
   DevBuf<int2> inv_items, fwd_items;
   int n_inv = 0, n_fwd = 0;
 };
 
-// the largest transform row (complex samples x element size) a batched launch keeps in
-// one CTA's shared memory
+// the largest transform row (complex samples x element size) one CTA's shared memory
+// takes (the single-CTA transforms are configured for 200 KB)
 constexpr size_t kBatchedRowBytes = 128 * 1024;
 
 template <class T>
@@ -1540,6 +1542,48 @@ void scan_transforms(sp_scan* S, const int* flags, const InverseArgs* inv, const
     else
       CUDA_CHECK(launch_forward_b(fwd, c->fwd_items.p, flags, c->n_fwd, c->n_to, S->stream));
   }
+}
+
+// The scan's autotuner: for every grid size whose rows fit in one CTA and may also be split
+// over a cluster, time both forms of the inverse and the forward transform on this scan's
+// own rows (one warm-up and three timed launches each, every run selected) and keep the
+// faster.  The launches write the workspaces' scratch rows only.
+template <class R>
+void tune_transforms(sp_scan* S, const ForwardArgsT<R>* fwd) {
+  std::vector<int> ones(S->R, 1);
+  DevBuf<int> all;
+  all.upload(ones.data(), ones.size(), S->stream);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  auto time = [&](auto&& launch) -> float {
+    CUDA_CHECK(launch());
+    CUDA_CHECK(cudaEventRecord(e0, S->stream));
+    for (int i = 0; i < 3; ++i) CUDA_CHECK(launch());
+    CUDA_CHECK(cudaEventRecord(e1, S->stream));
+    CUDA_CHECK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    return ms / 3;
+  };
+  const size_t elem = sizeof(cplx<R>);
+  for (auto& c : S->classes) {
+    if (fft_cluster_size(c->n_to) <= 1) continue;  // a single CTA is the only form
+    const InverseArgs* inv = S->inv_att.p;
+    if ((size_t)(c->n_to / 2) * 16 <= kBatchedRowBytes) {
+      c->inv_single_ms = time([&] { return launch_inverse_b(inv, c->inv_items.p, all.p, c->n_inv, c->n_to, S->stream); });
+      c->inv_cluster_ms = time([&] { return launch_inverse_cluster_b(inv, c->inv_items.p, all.p, c->n_inv, c->n_to, S->stream); });
+      c->cluster_inv = c->inv_cluster_ms < c->inv_single_ms;
+    }
+    if ((size_t)(c->n_to / 2) * elem <= kBatchedRowBytes) {
+      c->fwd_single_ms = time([&] { return launch_forward_b(fwd, c->fwd_items.p, all.p, c->n_fwd, c->n_to, S->stream); });
+      c->fwd_cluster_ms = time([&] { return launch_forward_cluster_b(fwd, c->fwd_items.p, all.p, c->n_fwd, c->n_to, S->stream); });
+      c->cluster_fwd = c->fwd_cluster_ms < c->fwd_single_ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CUDA_CHECK(cudaStreamSynchronize(S->stream));
 }
 
 void scan_source(sp_scan* S, bool start) {
@@ -1745,9 +1789,10 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     for (int n_to : sizes) {
       auto c = std::make_unique<FftClass>();
       c->n_to = n_to;
-      // Batched rows are many: a row is one CTA whenever it fits in shared memory (no
-      // cluster exchange); only the longest rows are split over a cluster.
-      // (the inverse transform is FP64 in both precisions)
+      // A row that fits in one CTA's shared memory may be transformed there or over a
+      // cluster; the autotuner (tune_transforms) times both and keeps the faster.  Rows
+      // that do not fit take the cluster.  (The inverse transform is FP64 in both
+      // precisions.)
       const size_t fwd_bytes = (size_t)(n_to / 2) * (precision == SP_PRECISION_MIXED ? 8 : 16);
       const size_t inv_bytes = (size_t)(n_to / 2) * 16;
       c->cluster_inv = fft_cluster_size(n_to) > 1 && inv_bytes > kBatchedRowBytes;
@@ -1787,6 +1832,8 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     S->n_out_items = (int)out_items.size();
     S->n_col_items = (int)col_items.size();
     CUDA_CHECK(cudaStreamSynchronize(S->stream));
+    if (precision == SP_PRECISION_MIXED) tune_transforms(S.get(), S->fwd32.p);
+    else tune_transforms(S.get(), S->fwd.p);
     *out = S.release();
   });
 }
@@ -1835,6 +1882,28 @@ sp_status sp_scan_run(sp_scan* S, int32_t run, double* state, sp_batch* info) {
 }
 
 void* sp_scan_stream(sp_scan* S) { return S ? (void*)S->stream : nullptr; }
+
+size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
+  std::string text;
+  if (S) {
+    char line[256];
+    for (const auto& c : S->classes) {
+      std::snprintf(line, sizeof line,
+                    "n_to %d: inverse %s (single %.4f ms, cluster %.4f ms), forward %s "
+                    "(single %.4f ms, cluster %.4f ms)\n",
+                    c->n_to, c->cluster_inv ? "cluster" : "single", c->inv_single_ms,
+                    c->inv_cluster_ms, c->cluster_fwd ? "cluster" : "single", c->fwd_single_ms,
+                    c->fwd_cluster_ms);
+      text += line;
+    }
+  }
+  if (buf && len) {
+    const size_t n = std::min(len - 1, text.size());
+    std::memcpy(buf, text.data(), n);
+    buf[n] = 0;
+  }
+  return text.size();
+}
 
 sp_status sp_scan_destroy(sp_scan* S) {
   delete S;
