@@ -147,6 +147,87 @@ def cpu_arm(rec, pol, steps: int, warmup: int, budget_s: float, threads: int | N
     return done, elapsed
 
 
+def runs_leg(device: int) -> dict:
+    """Configs 1 and 2 run start to end, plain FP64 and mixed precision: runs per second,
+    attempts per second, and the mixed run's relative L2 error against the FP64 run in
+    the final spectrum and in time (each run takes its own adaptive steps)."""
+    import torch
+
+    from solprop_b200 import _lib
+    from tests._cases import golden, policy, record
+
+    out = {}
+    for case in ("config1", "config2"):
+        rec = record(case)
+        pol = policy(golden(case), "adaptive")
+        problem = _lib.Problem(rec)
+        finals = {}
+        for precision in ("fp64", "mixed"):
+            ws = _lib.Workspace(problem, device, precision)
+            stream = torch.cuda.ExternalStream(ws.stream, device=torch.device("cuda", device))
+            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            s_ev.record(stream)
+            session = ws.start(pol)
+            while True:
+                batch = session.advance(4096)
+                if batch.event in (2, 3):
+                    break
+            e_ev.record(stream)
+            torch.cuda.synchronize()
+            sec = s_ev.elapsed_time(e_ev) / 1e3
+            finals[precision] = session.export()
+            out.setdefault(case, {})[precision] = {
+                "finished": batch.event == 2, "attempts": int(batch.attempts), "seconds": sec,
+                "runs_per_s": 1.0 / sec, "attempts_per_s": batch.attempts / sec}
+        a64, a32 = finals["fp64"], finals["mixed"]
+        t64 = np.fft.irfft(a64.reshape(-1, a64.shape[-1]), axis=-1)
+        t32 = np.fft.irfft(a32.reshape(-1, a32.shape[-1]), axis=-1)
+        out[case]["mixed_vs_fp64_spectral_rel_l2"] = float(np.linalg.norm(a32 - a64) / np.linalg.norm(a64))
+        out[case]["mixed_vs_fp64_temporal_rel_l2"] = float(np.linalg.norm(t32 - t64) / np.linalg.norm(t64))
+    return out
+
+
+def surrogate_leg(device: int, points: int = 16384, members: int = 5, repeats: int = 5) -> dict:
+    """The surrogate's inference: ``members`` perceptrons (6 -> 4 x 512 -> 2048) over
+    ``points`` inputs, device time per pass (CUDA events) and the FLOP rate against the
+    measured BF16 peak -- on the tcgen05 path (TMA tiles, tensor-memory accumulators, BF16
+    activations) and, for comparison, on the mma.sync path the training uses."""
+    import torch
+
+    from solprop_b200 import surrogate
+
+    ens = surrogate.Ensemble(members=members, seed=1, device=device)
+    x = torch.rand((points, 6), device=f"cuda:{device}") * 2 - 1
+    sizes = (6,) + surrogate.HIDDEN + (surrogate.N_OUT,)
+    flops = 2.0 * points * members * sum(a * b for a, b in zip(sizes[:-1], sizes[1:]))
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("bf16_tflops", 1590.0)
+    status = torch.zeros(1, dtype=torch.int32, device=f"cuda:{device}")
+
+    def timed(run) -> float:
+        run()
+        torch.cuda.synchronize()
+        s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_ev.record()
+        for _ in range(repeats):
+            run()
+        e_ev.record()
+        torch.cuda.synchronize()
+        return s_ev.elapsed_time(e_ev) / repeats
+
+    ms_tc = timed(lambda: [m.infer(x, status) for m in ens.members])
+    ms_mma = timed(lambda: [m.forward(x) for m in ens.members])
+    if int(status.item()):
+        raise RuntimeError("a tensor-core product's wait gave up")
+    achieved = flops / (ms_tc * 1e-3) / 1e12
+    return {"points": points, "members": members, "ms_per_pass": ms_tc, "points_per_s": points / (ms_tc * 1e-3),
+            "mma_sync_ms_per_pass": ms_mma,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak,
+                         "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"}}
+
+
 def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024,
              rank: int = 0, world: int = 1) -> dict:
     """The parameter-scan workload (config 4): n_runs seeded uneven capillary runs, stepped together.
@@ -360,6 +441,8 @@ def main() -> int:
                "sample": f"{done} attempts of the config-2 run from z=0 on one host thread "
                          f"({os.cpu_count()} cores on the box)"}
 
+    runs_result = runs_leg(local)
+    surrogate_result = surrogate_leg(local)
     scan_result = None
     if args.scan_runs > 0:
         scan_result = scan_leg(local, args.scan_runs, args.scan_steps, warmup=3, rank=rank, world=world)
@@ -369,7 +452,8 @@ def main() -> int:
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * args.steps)),
-            "clocks": clocks.summary(), "scan": scan_result}
+            "clocks": clocks.summary(), "runs": runs_result, "scan": scan_result,
+            "surrogate": surrogate_result}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del session, s2

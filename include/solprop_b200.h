@@ -225,6 +225,17 @@ sp_status sp_scan_destroy(sp_scan* scan);
 sp_status sp_mlp_gemm(const float* A, int lda, int transA, const float* B, int ldb, int transB,
                       float* C, int ldc, int M, int N, int K, const float* bias, int epilogue,
                       float* pre, void* stream);
+/* The forward product on the fifth-generation tensor cores (tcgen05, operands brought by
+ * TMA): C[M,N] = A[M,K] W[N,K]^T (+ bias) (GELU), A and W BF16 with K contiguous (row
+ * pitches lda, ldw elements, multiples of 8; 16-byte aligned), K a multiple of 64, N a
+ * multiple of 256; writes FP32 C (pitch ldc) and/or BF16 C16 (pitch ldc16) when not NULL.
+ * *status (device int) is set to 1 if a wait inside the kernel gave up. */
+sp_status sp_mlp_gemm_tc(const void* A, int lda, const void* W, int ldw, float* C, int ldc,
+                         void* C16, int ldc16, int M, int N, int K, const float* bias,
+                         int epilogue, int* status, void* stream);
+/* FP32 rows to BF16 rows, zero-padded from cols to cols_out columns. */
+sp_status sp_mlp_to_bf16(const float* src, int ld_src, int rows, int cols, void* dst,
+                         int ld_dst, int cols_out, void* stream);
 /* dZ = dA * GELU'(pre), elementwise over n values. */
 sp_status sp_mlp_gelu_backward(const float* dA, const float* pre, float* dZ, size_t n, void* stream);
 /* db[n] = sum over the M rows of dZ[m, n] (rows in order). */

@@ -1,0 +1,304 @@
+// Forward products of the surrogate's perceptron on the fifth-generation tensor cores:
+//
+//   C[M, N] = A[M, K] W[N, K]^T (+ bias[n]) (GELU)     A, W: BF16, K contiguous, in HBM
+//
+// One CTA of four warps computes a 128 x 256 tile.  The tensor memory accelerator brings
+// 64-wide K slices of A (128 rows) and W (256 rows) into shared memory, swizzled by 128
+// bytes, through a four-stage ring guarded by mbarriers; one thread issues tcgen05.mma
+// (kind::f16: BF16 operands, FP32 accumulation) for each 16-wide K step into a 128 x 256
+// FP32 accumulator held in tensor memory, and commits each stage back to its producer.
+// When the ring drains, each warp reads its 32 rows of the accumulator with tcgen05.ld and
+// applies the epilogue (bias, GELU, FP32 and/or BF16 stores).  Every mbarrier wait is
+// bounded: a wait that gives up sets *status, and the CTA still releases its tensor memory
+// before it returns.  No load is multicast.
+//
+// The shared-memory and instruction descriptors follow the sm_100 UMMA formats (K-major,
+// 128-byte swizzle: stride between 8-row groups 1024 bytes; a 16-element K step advances
+// the start address by 32 bytes inside the swizzle atom).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+
+#include "solprop_b200.h"
+
+namespace sp {
+namespace {
+
+constexpr int kTM = 128, kTN = 256, kTK = 64, kStages = 4, kThreads = 128;
+constexpr uint32_t kABytes = kTM * kTK * 2;  // 16 KB
+constexpr uint32_t kBBytes = kTN * kTK * 2;  // 32 KB
+constexpr uint32_t kStageBytes = kABytes + kBBytes;
+constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 + 256;
+constexpr uint32_t kTmemColumns = 256;     // the FP32 accumulator: 256 columns x 128 lanes
+constexpr long kWaitLimit = 1L << 26;      // polls of an mbarrier before the wait gives up
+
+// instruction descriptor: FP32 accumulator (bit 4), BF16 A (bits 7-9) and B (10-12), both
+// K-major, N / 8 at bits 17-22, M / 16 at bits 24-28
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTN >> 3) << 17) |
+                            ((uint32_t)(kTM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// wait for the phase of parity `parity` to complete; false when the wait gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (long i = 0; i < kWaitLimit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// K-major, 128-byte-swizzled operand tile starting at `tile` (1024-byte aligned)
+__device__ __forceinline__ uint64_t sw128_desc(const void* tile) {
+  const uint64_t addr = smem_u32(tile);
+  uint64_t d = (addr >> 4) & 0x3FFFull;  // start address, 16-byte units, bits 0-13
+  d |= 1ull << 16;                       // leading byte offset (16 bytes; unused when swizzled)
+  d |= (uint64_t)(1024 >> 4) << 32;      // stride byte offset: 8 rows x 128 bytes
+  d |= 1ull << 46;                       // descriptor version 1 (sm_100)
+  d |= 2ull << 61;                       // layout: 128-byte swizzle
+  return d;
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a_desc, uint64_t b_desc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(a_desc), "l"(b_desc), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_load_32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_mlp_gemm_tc(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_w,
+                  float* C, __nv_bfloat16* C16, const float* bias, int M, int N, int K, int ldc, int ldc16,
+                  int epilogue, int* status) {
+  extern __shared__ __align__(1024) unsigned char tc_raw[];
+  unsigned char* ring = reinterpret_cast<unsigned char*>(((uintptr_t)tc_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)kStages * kStageBytes);
+  uint64_t* empty = full + kStages;
+  uint64_t* done = empty + kStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  __shared__ int failed;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int m0 = blockIdx.y * kTM, n0 = blockIdx.x * kTN;
+  const int n_k = K / kTK;
+  if (threadIdx.x == 0) {
+    failed = 0;
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (warp == 0) {  // the whole warp allocates the accumulator's columns
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemColumns)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (threadIdx.x == 0) {
+    // producer: the K slices of A and W, stage by stage
+    for (int k = 0; k < n_k; ++k) {
+      const int s = k % kStages;
+      const uint32_t round = k / kStages;
+      if (k >= kStages && !mbar_wait(&empty[s], (round - 1) & 1)) {
+        failed = 1;
+        break;
+      }
+      unsigned char* stage = ring + (size_t)s * kStageBytes;
+      mbar_expect_tx(&full[s], kStageBytes);
+      tma_load_2d(stage, &map_a, &full[s], k * kTK, m0);
+      tma_load_2d(stage + kABytes, &map_w, &full[s], k * kTK, n0);
+    }
+  } else if (threadIdx.x == 32) {
+    // the MMA issuer: four 16-wide K steps per stage, the stage handed back on completion
+    for (int k = 0; k < n_k; ++k) {
+      const int s = k % kStages;
+      const uint32_t round = k / kStages;
+      if (!mbar_wait(&full[s], round & 1)) {
+        failed = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const unsigned char* stage = ring + (size_t)s * kStageBytes;
+      const uint64_t da = sw128_desc(stage), db = sw128_desc(stage + kABytes);
+#pragma unroll
+      for (int kk = 0; kk < kTK / 16; ++kk)
+        umma_bf16(tmem, da + 2ull * kk, db + 2ull * kk, (k | kk) != 0 ? 1u : 0u);
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);  // every MMA issued above has completed when this arrives
+  }
+  __syncwarp();
+  // epilogue: warp w holds accumulator lanes (rows) 32 w .. 32 w + 31; the tile goes
+  // through shared memory (the drained ring, rows padded by one word against bank
+  // conflicts) so that it leaves in coalesced rows
+  const bool ok = mbar_wait(done, 0);
+  __syncwarp();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  constexpr int kPitch = kTN + 1;
+  static_assert((size_t)kTM * kPitch * 4 <= (size_t)kStages * kStageBytes, "the tile fits in the ring");
+  float* tile = reinterpret_cast<float*>(ring);
+  const int row = warp * 32 + lane;
+  for (int c = 0; c < kTN; c += 32) {
+    uint32_t r[32];
+    __syncwarp();  // the load is warp-wide (.sync.aligned)
+    tmem_load_32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) tile[row * kPitch + c + j] = __uint_as_float(r[j]);
+  }
+  __syncthreads();
+  if (ok && !failed) {
+    for (int rr = warp; rr < kTM && m0 + rr < M; rr += kThreads / 32) {
+      const size_t m = (size_t)(m0 + rr);
+      for (int cc = lane; cc < kTN; cc += 32) {
+        const int n = n0 + cc;
+        float v = tile[rr * kPitch + cc];
+        if (epilogue >= 1 && bias) v += bias[n];
+        if (epilogue == 2) v = gelu(v);
+        if (C) C[m * ldc + n] = v;
+        if (C16) C16[m * ldc16 + n] = __float2bfloat16_rn(v);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns) : "memory");
+  if (threadIdx.x == 0 && (!ok || failed)) atomicExch(status, 1);
+}
+
+// FP32 rows -> BF16 rows (zero-padded to `cols_out` columns)
+__global__ void k_to_bf16(const float* src, int ld_src, int rows, int cols, __nv_bfloat16* dst, int ld_dst,
+                          int cols_out) {
+  const size_t total = (size_t)rows * cols_out;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i / cols_out), c = (int)(i % cols_out);
+    dst[(size_t)r * ld_dst + c] = __float2bfloat16_rn(c < cols ? src[(size_t)r * ld_src + c] : 0.0f);
+  }
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled() {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  });
+  return fn;
+}
+
+// a rows x cols BF16 matrix (row pitch ld elements) as 2-D tiles of box_rows x 64
+bool make_map(CUtensorMap* map, const void* base, int rows, int cols, int ld, int box_rows) {
+  EncodeTiled fn = encode_tiled();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)kTK, (cuuint32_t)box_rows};
+  const cuuint32_t elem[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, elem,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+}  // namespace sp
+
+extern "C" {
+
+sp_status sp_mlp_gemm_tc(const void* A, int lda, const void* W, int ldw, float* C, int ldc, void* C16,
+                         int ldc16, int M, int N, int K, const float* bias, int epilogue, int* status,
+                         void* stream) {
+  using namespace sp;
+  if (!A || !W || (!C && !C16) || !status || M < 1 || N < 1 || K < 1 || epilogue < 0 || epilogue > 2)
+    return SP_ERR_ARGUMENT;
+  // the tiling's and the tensor maps' rules: whole 256-column tiles and 64-wide K slices,
+  // 16-byte aligned rows
+  if (N % kTN || K % kTK || lda % 8 || ldw % 8 || lda < K || ldw < K) return SP_ERR_ARGUMENT;
+  if (((uintptr_t)A | (uintptr_t)W) & 15) return SP_ERR_ARGUMENT;
+  CUtensorMap map_a, map_w;
+  if (!make_map(&map_a, A, M, K, lda, kTM) || !make_map(&map_w, W, N, K, ldw, kTN)) return SP_ERR_CUDA;
+  static std::once_flag configured;
+  std::call_once(configured, [] {
+    cudaFuncSetAttribute(k_mlp_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
+  });
+  const dim3 grid(N / kTN, (M + kTM - 1) / kTM);
+  k_mlp_gemm_tc<<<grid, kThreads, kSmemBytes, (cudaStream_t)stream>>>(
+      map_a, map_w, C, static_cast<__nv_bfloat16*>(C16), bias, M, N, K, ldc, ldc16, epilogue, status);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ERR_CUDA;
+}
+
+sp_status sp_mlp_to_bf16(const float* src, int ld_src, int rows, int cols, void* dst, int ld_dst, int cols_out,
+                         void* stream) {
+  if (!src || !dst || rows < 0 || cols < 0 || cols_out < cols) return SP_ERR_ARGUMENT;
+  if (!rows || !cols_out) return SP_OK;
+  const size_t total = (size_t)rows * cols_out;
+  const unsigned blocks = (unsigned)((total + 255) / 256 < 148 * 16 ? (total + 255) / 256 : 148 * 16);
+  sp::k_to_bf16<<<blocks, 256, 0, (cudaStream_t)stream>>>(src, ld_src, rows, cols,
+                                                          static_cast<__nv_bfloat16*>(dst), ld_dst, cols_out);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ERR_CUDA;
+}
+
+}  // extern "C"

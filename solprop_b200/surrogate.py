@@ -64,6 +64,36 @@ def gemm(a, b, c, *, trans_a=False, trans_b=False, bias=None, epilogue=0, pre=No
                            _ptr(pre) if pre is not None else None, stream))
 
 
+def gemm_tc(a16, w16, *, out=None, out16=None, bias=None, epilogue=0, status=None, stream=None):
+    """out / out16 = a16 w16^T (+ bias) (GELU) on the tcgen05 tensor cores; a16 (M, K) and
+    w16 (N, K) are BF16 tensors with K a multiple of 64 and N a multiple of 256."""
+    import torch
+
+    lib = _bind()
+    m, k = a16.shape
+    n, kw = w16.shape
+    if kw != k:
+        raise ValueError(f"gemm_tc shapes: a {tuple(a16.shape)}, w {tuple(w16.shape)}")
+    if status is None:
+        status = torch.zeros(1, dtype=torch.int32, device=a16.device)
+    _check(lib.sp_mlp_gemm_tc(_ptr(a16), a16.stride(0), _ptr(w16), w16.stride(0),
+                              _ptr(out) if out is not None else None, out.stride(0) if out is not None else 0,
+                              _ptr(out16) if out16 is not None else None,
+                              out16.stride(0) if out16 is not None else 0, m, n, k,
+                              _ptr(bias) if bias is not None else None, epilogue, _ptr(status), stream))
+    return status
+
+
+def to_bf16(x, cols_out: int):
+    """BF16 copy of an FP32 (rows, cols) tensor, zero-padded to cols_out columns."""
+    import torch
+
+    out = torch.empty((x.shape[0], cols_out), dtype=torch.bfloat16, device=x.device)
+    _check(_bind().sp_mlp_to_bf16(_ptr(x), x.stride(0), x.shape[0], x.shape[1], _ptr(out), out.stride(0),
+                                  cols_out, None))
+    return out
+
+
 # ------------------------------------------------------------------ features and targets
 def features(points) -> np.ndarray:
     """The six inputs of each point, each mapped onto [-1, 1] over the scan's ranges."""
@@ -129,6 +159,29 @@ class Perceptron:
         self.m1 = [torch.zeros_like(t) for t in self.params]
         self.m2 = [torch.zeros_like(t) for t in self.params]
         self.step = 0
+        self.w16 = None  # BF16 copies for the tensor-core inference (K padded to 64)
+
+    def refresh_bf16(self):
+        """BF16 copies of the weights for ``infer`` (after initialisation or training)."""
+        self.w16 = [to_bf16(w, -(-w.shape[1] // 64) * 64) for w in self.weights]
+
+    def infer(self, x, status=None):
+        """Outputs for x (rows) through the tcgen05 products: BF16 activations between the
+        layers, FP32 accumulation, the output layer in FP32."""
+        import torch
+
+        if self.w16 is None:
+            self.refresh_bf16()
+        a = to_bf16(x, self.w16[0].shape[1])
+        last = len(self.weights) - 1
+        for i, (w16, b) in enumerate(zip(self.w16, self.biases)):
+            if i == last:
+                out = torch.empty((a.shape[0], w16.shape[0]), dtype=torch.float32, device=self.device)
+                status = gemm_tc(a, w16, out=out, bias=b, epilogue=1, status=status)
+                return out, status
+            nxt = torch.empty((a.shape[0], w16.shape[0]), dtype=torch.bfloat16, device=self.device)
+            status = gemm_tc(a, w16, out16=nxt, bias=b, epilogue=2, status=status)
+            a = nxt
 
     def forward(self, x, keep: bool = False):
         """Outputs for x (rows); with ``keep`` the layers' inputs and pre-activations."""
@@ -235,6 +288,7 @@ class Ensemble:
                 if log and (epoch % 50 == 0 or epoch == epochs - 1):
                     log(f"member {k} epoch {epoch} loss {float(total) / max(count, 1):.4e}")
             last = float(total) / max(count, 1)
+            member.refresh_bf16()
         return last
 
     def predict(self, x: np.ndarray, chunk: int = 16384):
@@ -252,9 +306,15 @@ class Ensemble:
             xb = torch.tensor(x[s:s + chunk], device=dev)
             m = xb.shape[0]
             ys = torch.empty((e, m, N_OUT), dtype=torch.float32, device=dev)
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
             for k, member in enumerate(self.members):
-                out, _ = member.forward(xb)
+                if m >= 128:
+                    out, status = member.infer(xb, status)
+                else:
+                    out, _ = member.forward(xb)
                 ys[k] = out * scale + offset
+            if int(status.item()):
+                raise RuntimeError("a tensor-core product's wait gave up")
             mu = torch.empty((m, N_OUT), dtype=torch.float32, device=dev)
             sd = torch.empty(m, dtype=torch.float32, device=dev)
             _check(lib.sp_mlp_ensemble_stats(_ptr(ys), e, m, N_OUT, _ptr(mu), _ptr(sd), None))

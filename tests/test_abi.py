@@ -14,7 +14,7 @@ ROOT = Path(__file__).resolve().parent.parent
 
 def declared_symbols() -> set[str]:
     text = "\n".join(p.read_text() for p in (ROOT / "include").glob("*.h"))
-    return set(re.findall(r"\b(sp_[a-z_]+)\s*\(", text))
+    return set(re.findall(r"\b(sp_[a-z0-9_]+)\s*\(", text))
 
 
 def test_header_declares_the_bound_functions():

@@ -69,6 +69,45 @@ def test_gemm_matches_bf16_oracle(ta, tb, shape):
 
 
 @gpu
+@pytest.mark.parametrize("shape", [(300, 512, 512), (1000, 2048, 512), (128, 512, 64), (4096, 256, 128)])
+def test_tcgen05_gemm_matches_bf16_oracle(shape):
+    """The tcgen05 product (TMA tiles, tensor-memory accumulator) against the same BF16
+    operands multiplied in float64: FP32 accumulation error only."""
+    from solprop_b200 import surrogate as S
+
+    torch = _torch()
+    m, n, k = shape
+    rng = np.random.default_rng(m + n + k)
+    a = rng.normal(size=(m, k)).astype(np.float32)
+    w = rng.normal(size=(n, k)).astype(np.float32)
+    bias = rng.normal(size=n).astype(np.float32)
+    a16 = torch.tensor(a, device="cuda").to(torch.bfloat16)
+    w16 = torch.tensor(w, device="cuda").to(torch.bfloat16)
+    out = torch.empty((m, n), device="cuda")
+    out16 = torch.empty((m, n), dtype=torch.bfloat16, device="cuda")
+    status = S.gemm_tc(a16, w16, out=out, out16=out16, bias=torch.tensor(bias, device="cuda"), epilogue=2)
+    assert int(status.item()) == 0
+    ref = O.gelu(O.bf16(a) @ O.bf16(w).T + bias)
+    got = out.cpu().numpy()
+    assert np.max(np.abs(got - ref)) <= 2e-5 * np.max(np.abs(ref)) + 1e-5
+    assert np.allclose(out16.float().cpu().numpy(), got, rtol=1e-2, atol=1e-2)
+
+
+@gpu
+def test_inference_on_tcgen05_matches_the_training_path():
+    from solprop_b200 import surrogate as S
+
+    torch = _torch()
+    net = S.Perceptron(seed=11)
+    x = torch.tensor(np.random.default_rng(1).uniform(-1, 1, (700, 6)).astype(np.float32), device="cuda")
+    y_train, _ = net.forward(x)
+    y_infer, status = net.infer(x)
+    assert int(status.item()) == 0
+    a, b = y_infer.cpu().numpy(), y_train.cpu().numpy()
+    assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b)
+
+
+@gpu
 def test_gelu_epilogue_and_preactivation():
     from solprop_b200 import surrogate as S
 
