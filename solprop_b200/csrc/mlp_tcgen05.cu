@@ -2,7 +2,7 @@
 //
 //   C[M, N] = A[M, K] W[N, K]^T (+ bias[n]) (GELU)     A, W: BF16, K contiguous, in HBM
 //
-// One CTA of four warps computes a 128 x 256 tile.  The tensor memory accelerator brings
+// One CTA of sixteen warps computes a 128 x 256 tile.  The tensor memory accelerator brings
 // 64-wide K slices of A (128 rows) and W (256 rows) into shared memory, swizzled by 128
 // bytes, through a four-stage ring guarded by mbarriers; one thread issues tcgen05.mma
 // (kind::f16: BF16 operands, FP32 accumulation) for each 16-wide K step into a 128 x 256
@@ -27,7 +27,12 @@
 namespace sp {
 namespace {
 
-constexpr int kTM = 128, kTN = 256, kTK = 64, kStages = 4, kThreads = 128;
+constexpr int kTM = 128, kTN = 256, kTK = 64, kStages = 4;
+// sixteen warps: one thread of warp 0 feeds the ring, one of warp 1 issues the products, and
+// all sixteen drain the accumulator (warp w reads lanes 32 (w % 4) .. + 31, columns
+// 64 (w / 4) .. + 63), so that the epilogue's arithmetic has warps to hide its latency
+constexpr int kThreads = 512;
+constexpr int kEpilogueColumns = kTN / (kThreads / 128);
 constexpr uint32_t kABytes = kTM * kTK * 2;  // 16 KB
 constexpr uint32_t kBBytes = kTN * kTK * 2;  // 32 KB
 constexpr uint32_t kStageBytes = kABytes + kBBytes;
@@ -194,11 +199,13 @@ __global__ void __launch_bounds__(kThreads, 1)
   constexpr int kPitch = kTN + 1;
   static_assert((size_t)kTM * kPitch * 4 <= (size_t)kStages * kStageBytes, "the tile fits in the ring");
   float* tile = reinterpret_cast<float*>(ring);
-  const int row = warp * 32 + lane;
-  for (int c = 0; c < kTN; c += 32) {
+  const int quarter = warp % 4;  // the accumulator lanes this warp may read
+  const int row = quarter * 32 + lane;
+  const int c_lo = (warp / 4) * kEpilogueColumns;
+  for (int c = c_lo; c < c_lo + kEpilogueColumns; c += 32) {
     uint32_t r[32];
     __syncwarp();  // the load is warp-wide (.sync.aligned)
-    tmem_load_32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, r);
+    tmem_load_32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c, r);
 #pragma unroll
     for (int j = 0; j < 32; ++j) tile[row * kPitch + c + j] = __uint_as_float(r[j]);
   }
