@@ -1507,8 +1507,13 @@ struct sp_scan {
   double* h_norms = nullptr;
   int *h_flag_start = nullptr, *h_flag_att = nullptr, *h_flag_accept = nullptr;
   int64_t batch_steps = 0;
+  // the attempt phase (uploads, predictor, source, corrector, norms read-back) as one
+  // CUDA graph, captured at the first attempt and replayed at every later one
+  cudaGraphExec_t attempt_graph = nullptr;
+  bool graph_failed = false;
   ~sp_scan() {
     if (stream) cudaStreamSynchronize(stream);
+    if (attempt_graph) cudaGraphExecDestroy(attempt_graph);
     for (void* p : {(void*)h_adams_start, (void*)h_adams_att, (void*)h_stages_start,
                     (void*)h_stages_att, (void*)h_norms, (void*)h_flag_start, (void*)h_flag_att,
                     (void*)h_flag_accept})
@@ -1598,6 +1603,18 @@ void scan_source(sp_scan* S, bool start) {
   CUDA_CHECK(launch_output_b(out.p, S->out_items.p, flags, S->n_out_items, S->stream));
 }
 
+void scan_attempt_launches(sp_scan* S) {
+  const int R = S->R;
+  upload_all(S->flag_att, S->h_flag_att, R, S->stream);
+  upload_all(S->stages_att, S->h_stages_att, 2 * (size_t)R, S->stream);
+  upload_all(S->adams_att, S->h_adams_att, R, S->stream);
+  CUDA_CHECK(launch_step_b(0, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
+  scan_source(S, false);
+  CUDA_CHECK(launch_step_b(1, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
+  CUDA_CHECK(cudaMemcpyAsync(S->h_norms, S->norms.p, sizeof(double) * 8 * R, cudaMemcpyDeviceToHost,
+                             S->stream));
+}
+
 void scan_step(sp_scan* S) {
   const int R = S->R;
   // phase A: runs with an empty history take their startup sample
@@ -1645,14 +1662,29 @@ void scan_step(sp_scan* S) {
     ++n_att;
   }
   if (!n_att) return;
-  upload_all(S->flag_att, S->h_flag_att, R, S->stream);
-  upload_all(S->stages_att, S->h_stages_att, 2 * (size_t)R, S->stream);
-  upload_all(S->adams_att, S->h_adams_att, R, S->stream);
-  CUDA_CHECK(launch_step_b(0, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
-  scan_source(S, false);
-  CUDA_CHECK(launch_step_b(1, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
-  CUDA_CHECK(cudaMemcpyAsync(S->h_norms, S->norms.p, sizeof(double) * 8 * R, cudaMemcpyDeviceToHost,
-                             S->stream));
+  // every operand of the attempt phase lives at a fixed address (pinned host tables, device
+  // argument arrays), so its launches are captured once and replayed
+  if (!S->attempt_graph && !S->graph_failed) {
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      try {
+        scan_attempt_launches(S);
+      } catch (const Failure&) {
+        ok = false;
+      }
+      ok = (cudaStreamEndCapture(S->stream, &graph) == cudaSuccess) && ok;
+    }
+    if (ok) ok = cudaGraphInstantiate(&S->attempt_graph, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+      S->attempt_graph = nullptr;
+      S->graph_failed = true;  // plain launches from here on
+      cudaGetLastError();
+    }
+  }
+  if (S->attempt_graph) CUDA_CHECK(cudaGraphLaunch(S->attempt_graph, S->stream));
+  else scan_attempt_launches(S);
   CUDA_CHECK(cudaStreamSynchronize(S->stream));
   for (int r = 0; r < R; ++r)
     if (S->h_flag_att[r]) check_column(S->h_norms + 8 * r, S->norms.p + 8 * r, S->stream);
@@ -1886,6 +1918,9 @@ void* sp_scan_stream(sp_scan* S) { return S ? (void*)S->stream : nullptr; }
 size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
   std::string text;
   if (S) {
+    text += S->attempt_graph ? "attempt phase: one CUDA graph\n"
+                             : (S->graph_failed ? "attempt phase: plain launches (capture failed)\n"
+                                                : "attempt phase: not yet captured\n");
     char line[256];
     for (const auto& c : S->classes) {
       std::snprintf(line, sizeof line,

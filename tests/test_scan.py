@@ -52,6 +52,7 @@ def test_batched_runs_match_single_runs():
     sc = _lib.Scan([r for r, _ in built], [q for _, q in built])
     steps = 12
     sc.advance(steps)
+    assert "attempt phase: one CUDA graph" in sc.describe()
     for i, (rec, pol) in enumerate(built):
         state, info = sc.run(i)
         problem = _lib.Problem(rec)
