@@ -215,6 +215,15 @@ void* sp_scan_stream(sp_scan* scan);
  * over a cluster, with the autotuner's timings (ms per launch; -1 where a form was not a
  * candidate).  Returns the text's length. */
 size_t sp_scan_describe(const sp_scan* scan, char* buf, size_t len);
+/* The response column's form in a scan.  The scan's autotuner times both at creation
+ * and keeps the faster; this call fixes one (a later attempt recaptures its graph).
+ * SP_SCAN_COLUMN_TILES: one CTA per (tile, node group), the running integrals handed
+ * from tile to tile between CTAs; SP_SCAN_COLUMN_SWEEP: one CTA per (run, node group)
+ * walking the tiles in order.  Both give the same bits.  No counterpart in the
+ * reference, which has no batch. */
+#define SP_SCAN_COLUMN_TILES 1
+#define SP_SCAN_COLUMN_SWEEP 2
+sp_status sp_scan_set_column(sp_scan* scan, int32_t form);
 sp_status sp_scan_destroy(sp_scan* scan);
 
 /* ---- the scan surrogate's multilayer perceptron (no counterpart in the reference) ----

@@ -133,6 +133,7 @@ SIGNATURES = {
                                  C.POINTER(C.c_void_p)]),
     "sp_scan_advance": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SpScanStatus)]),
     "sp_scan_describe": (C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "sp_scan_set_column": (C.c_int, [C.c_void_p, C.c_int32]),
     "sp_scan_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(SpBatch)]),
     "sp_scan_stream": (C.c_void_p, [C.c_void_p]),
     "sp_scan_destroy": (C.c_int, [C.c_void_p]),
@@ -484,6 +485,16 @@ class Scan:
         buf = C.create_string_buffer(8192)
         self._lib.sp_scan_describe(self.handle, buf, 8192)
         return buf.value.decode()
+
+    COLUMN_FORMS = {"tiles": 1, "sweep": 2}
+
+    def set_column(self, form: str) -> None:
+        """Fix the response column's form: ``"tiles"`` (one CTA per tile and node group,
+        the running integrals handed over between CTAs) or ``"sweep"`` (one CTA per run and
+        node group walking the tiles).  The autotuner's choice stands otherwise."""
+        if form not in self.COLUMN_FORMS:
+            raise ValueError(f"column form {form!r}: expected one of {sorted(self.COLUMN_FORMS)}")
+        check(library().sp_scan_set_column(self.handle, self.COLUMN_FORMS[form]))
 
     def advance(self, steps: int = 1) -> SpScanStatus:
         check(library().sp_scan_advance(self.handle, int(steps), C.byref(self.status)))

@@ -1499,8 +1499,17 @@ struct sp_scan {
   DevBuf<double> norms;
   DevBuf<int> flag_start, flag_att, flag_accept;
   DevBuf<int2> step_items, out_items;
-  DevBuf<int4> col_items;
-  int n_step_items = 0, n_out_items = 0, n_col_items = 0;
+  DevBuf<int4> col_items, sweep_items;
+  int n_step_items = 0, n_out_items = 0, n_col_items = 0, n_sweep_items = 0;
+  // the column's form, chosen by tune_column: one CTA per (tile, node group) with the
+  // running integrals handed over between CTAs, or one CTA per (run, node group) walking
+  // the tiles (ms per launch over all runs; < 0: not timed)
+  bool column_sweep = false;
+  float column_tile_ms = -1, column_sweep_ms = -1;
+  // host copies of the forward records (their n_groups follows the column's form)
+  std::vector<ForwardArgs> h_fwd;
+  std::vector<ForwardArgsT<float>> h_fwd32;
+  std::vector<int> groups;  // node groups per run
   std::vector<std::unique_ptr<FftClass>> classes;
   AdamsDev *h_adams_start = nullptr, *h_adams_att = nullptr;
   StageScalarsDev *h_stages_start = nullptr, *h_stages_att = nullptr;
@@ -1540,7 +1549,10 @@ void scan_transforms(sp_scan* S, const int* flags, const InverseArgs* inv, const
     else
       CUDA_CHECK(launch_inverse_b(inv, c->inv_items.p, flags, c->n_inv, c->n_to, S->stream));
   }
-  CUDA_CHECK(launch_column_b(col, S->col_items.p, flags, S->n_col_items, S->stream));
+  if (S->column_sweep)
+    CUDA_CHECK(launch_column_sweep_b(col, S->sweep_items.p, flags, S->n_sweep_items, S->stream));
+  else
+    CUDA_CHECK(launch_column_b(col, S->col_items.p, flags, S->n_col_items, S->stream));
   for (auto& c : S->classes) {
     if (c->cluster_fwd)
       CUDA_CHECK(launch_forward_cluster_b(fwd, c->fwd_items.p, flags, c->n_fwd, c->n_to, S->stream));
@@ -1589,6 +1601,68 @@ void tune_transforms(sp_scan* S, const ForwardArgsT<R>* fwd) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CUDA_CHECK(cudaStreamSynchronize(S->stream));
+}
+
+// The column's autotuner: time both forms of the response column on this scan's own runs
+// at their initial fields (one warm-up and three timed launches each, every run selected)
+// and keep the faster.  The sweep has no hand-over between CTAs but one CTA walks a whole
+// row, so it wins when the batch holds enough (run, node group) rows to fill the device;
+// the tile-parallel form wins for a few long rows.  The stage records are a unit taper
+// with zero densities while timing, then put back.
+template <class R>
+void tune_column(sp_scan* S, const ColumnArgsT<R>* col) {
+  std::vector<int> ones(S->R, 1);
+  DevBuf<int> all;
+  all.upload(ones.data(), ones.size(), S->stream);
+  std::vector<StageScalarsDev> unit(S->R);
+  std::memset(unit.data(), 0, sizeof(StageScalarsDev) * unit.size());
+  for (auto& u : unit) u.taper = 1.0;
+  upload_all(S->stages_start, unit.data(), S->R, S->stream);
+  for (auto& c : S->classes) {
+    if (c->cluster_inv)
+      CUDA_CHECK(launch_inverse_cluster_b(S->inv_start.p, c->inv_items.p, all.p, c->n_inv, c->n_to, S->stream));
+    else
+      CUDA_CHECK(launch_inverse_b(S->inv_start.p, c->inv_items.p, all.p, c->n_inv, c->n_to, S->stream));
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CUDA_CHECK(cudaEventCreate(&e0));
+  CUDA_CHECK(cudaEventCreate(&e1));
+  auto time = [&](auto&& launch) -> float {
+    CUDA_CHECK(launch());
+    CUDA_CHECK(cudaEventRecord(e0, S->stream));
+    for (int i = 0; i < 3; ++i) CUDA_CHECK(launch());
+    CUDA_CHECK(cudaEventRecord(e1, S->stream));
+    CUDA_CHECK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    return ms / 3;
+  };
+  S->column_tile_ms = time([&] { return launch_column_b(col, S->col_items.p, all.p, S->n_col_items, S->stream); });
+  S->column_sweep_ms = time([&] { return launch_column_sweep_b(col, S->sweep_items.p, all.p, S->n_sweep_items, S->stream); });
+  S->column_sweep = S->column_sweep_ms < S->column_tile_ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  upload_all(S->stages_start, S->h_stages_start, S->R, S->stream);
+  S->norms.zero(S->stream);
+  CUDA_CHECK(cudaStreamSynchronize(S->stream));
+}
+
+// The forward records for the column's form: the sweep leaves every node group's partial
+// rows for the forward transform to add, the tile-parallel column leaves their sum in
+// group 0's rows.  A captured attempt graph holds the old launches and is dropped.
+void set_column_form(sp_scan* S, bool sweep) {
+  S->column_sweep = sweep;
+  for (int r = 0; r < S->R; ++r) {
+    S->h_fwd[r].n_groups = sweep ? S->groups[r] : 1;
+    S->h_fwd32[r].n_groups = sweep ? S->groups[r] : 1;
+  }
+  upload_all(S->fwd, S->h_fwd.data(), S->R, S->stream);
+  if (S->precision == SP_PRECISION_MIXED) upload_all(S->fwd32, S->h_fwd32.data(), S->R, S->stream);
+  CUDA_CHECK(cudaStreamSynchronize(S->stream));
+  if (S->attempt_graph) {
+    CUDA_CHECK(cudaGraphExecDestroy(S->attempt_graph));
+    S->attempt_graph = nullptr;
+  }
 }
 
 void scan_source(sp_scan* S, bool start) {
@@ -1863,7 +1937,22 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     S->n_step_items = (int)step_items.size();
     S->n_out_items = (int)out_items.size();
     S->n_col_items = (int)col_items.size();
-    CUDA_CHECK(cudaStreamSynchronize(S->stream));
+    // the sweep's items: every (run, node group), longest row first
+    std::vector<int4> sweep_items;
+    for (int r = 0; r < R; ++r)
+      for (int g = 0; g < cs[r].n_groups; ++g) sweep_items.push_back(make_int4(r, g, 0, 0));
+    std::stable_sort(sweep_items.begin(), sweep_items.end(), [&](const int4& x, const int4& y) {
+      return cs[x.x].n_tiles > cs[y.x].n_tiles;
+    });
+    S->sweep_items.upload(sweep_items.data(), sweep_items.size(), S->stream);
+    S->n_sweep_items = (int)sweep_items.size();
+    CUDA_CHECK(cudaDeviceSynchronize());  // the sessions' initial fields are in place
+    if (precision == SP_PRECISION_MIXED) tune_column(S.get(), S->col32_start.p);
+    else tune_column(S.get(), S->col_start.p);
+    S->h_fwd = fa;
+    S->h_fwd32 = fa32;
+    for (int r = 0; r < R; ++r) S->groups.push_back(cs[r].n_groups);
+    set_column_form(S.get(), S->column_sweep);
     if (precision == SP_PRECISION_MIXED) tune_transforms(S.get(), S->fwd32.p);
     else tune_transforms(S.get(), S->fwd.p);
     *out = S.release();
@@ -1922,6 +2011,9 @@ size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
                              : (S->graph_failed ? "attempt phase: plain launches (capture failed)\n"
                                                 : "attempt phase: not yet captured\n");
     char line[256];
+    std::snprintf(line, sizeof line, "column: %s (tile-parallel %.4f ms, sweep %.4f ms)\n",
+                  S->column_sweep ? "sweep" : "tile-parallel", S->column_tile_ms, S->column_sweep_ms);
+    text += line;
     for (const auto& c : S->classes) {
       std::snprintf(line, sizeof line,
                     "n_to %d: inverse %s (single %.4f ms, cluster %.4f ms), forward %s "
@@ -1938,6 +2030,17 @@ size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
     buf[n] = 0;
   }
   return text.size();
+}
+
+sp_status sp_scan_set_column(sp_scan* S, int32_t form) {
+  return guarded([&] {
+    if (!S) throw Failure(SP_ERR_ARGUMENT, "NULL scan");
+    if (form != SP_SCAN_COLUMN_TILES && form != SP_SCAN_COLUMN_SWEEP)
+      throw Failure(SP_ERR_ARGUMENT, "unknown column form");
+    CUDA_CHECK(cudaSetDevice(S->device));
+    CUDA_CHECK(cudaStreamSynchronize(S->stream));
+    set_column_form(S, form == SP_SCAN_COLUMN_SWEEP);
+  });
 }
 
 sp_status sp_scan_destroy(sp_scan* S) {

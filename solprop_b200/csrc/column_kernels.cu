@@ -276,20 +276,23 @@ __device__ __forceinline__ double predecessors(const double* sums, int node, int
 
 }  // namespace
 
-template <class R>
-__device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
+// One tile of one node group: the window's synthesis, rate, running integrals, outputs and
+// projection.  kSweep = false: the tile is one CTA's whole work and learns its running
+// integrals' offsets from its predecessors' published sums (the hand-over above); the
+// node groups' projections are added by the tile's last CTA.  kSweep = true: one CTA walks
+// a node group through all tiles in order, so the offsets are its own running sums,
+// carried per lane -- lane l holds the sum of tiles l, l + 32, ... added in tile order,
+// the association predecessors() uses, so both forms give the same bits -- and every
+// group keeps its own partial rows, which the forward transform adds in group order.
+template <class R, bool kSweep>
+__device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, int group,
+                                            unsigned long long epoch, double& carry0, double& carry1) {
   extern __shared__ __align__(16) unsigned char column_raw[];
   R* modal = reinterpret_cast<R*>(column_raw);    // [m][kPitch], then the streams
   R* streams = modal;                              // [s][warp][kPitch]
   R* scratch = modal + (size_t)3 * kGroup * kPitch;
-  __shared__ unsigned long long ticket;
   __shared__ R wt[kMaxModes * kGroup];
   __shared__ R gate[kWindow], gate_d[kWindow];  // the temporal window g and g' on the window
-  if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1ull);
-  __syncthreads();
-  const unsigned long long epoch = ticket / (unsigned long long)a.n_blocks;
-  const int index = (int)(ticket % (unsigned long long)a.n_blocks);
-  const int tile = index / a.n_groups, group = index % a.n_groups;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int node = group * kGroup + warp;
   const bool live = node < a.n_nodes;
@@ -355,10 +358,16 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
     }
     trapezoid(Wf, inc, dt, tw, A - K, A + owned + K, a.n_to, lane);
     const double s0 = owned_sum(inc, A, own_hi, lane);
-    if (lane == 0 && live) a.sums0[(size_t)node * a.n_tiles + tile] = s0;
-    publish(a, group, tile, first);
-    await_predecessors(a, group, tile, first);
-    const double off0 = live ? predecessors(a.sums0, node, a.n_tiles, tile, lane) : 0.0;
+    double off0;
+    if constexpr (kSweep) {
+      off0 = live ? warp_total(carry0) : 0.0;
+      if (lane == (tile & 31)) carry0 += s0;
+    } else {
+      if (lane == 0 && live) a.sums0[(size_t)node * a.n_tiles + tile] = s0;
+      publish(a, group, tile, first);
+      await_predecessors(a, group, tile, first);
+      off0 = live ? predecessors(a.sums0, node, a.n_tiles, tile, lane) : 0.0;
+    }
     double P[kPer];
     const double at_t0 = window_prefix(inc, P, A, lane);
     // fraction and the current's integrand on [A - K, A + owned + K]
@@ -381,10 +390,16 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
     band_filter(g, gf, a.taps, K);
     trapezoid(gf, inc, dt, tw, A, A + owned, a.n_to, lane);
     const double s1 = owned_sum(inc, A, own_hi, lane);
-    if (lane == 0 && live) a.sums1[(size_t)node * a.n_tiles + tile] = s1;
-    publish(a, group, tile, first + 1);
-    await_predecessors(a, group, tile, first + 1);
-    const double off1 = live ? predecessors(a.sums1, node, a.n_tiles, tile, lane) : 0.0;
+    double off1;
+    if constexpr (kSweep) {
+      off1 = live ? warp_total(carry1) : 0.0;
+      if (lane == (tile & 31)) carry1 += s1;
+    } else {
+      if (lane == 0 && live) a.sums1[(size_t)node * a.n_tiles + tile] = s1;
+      publish(a, group, tile, first + 1);
+      await_predecessors(a, group, tile, first + 1);
+      off1 = live ? predecessors(a.sums1, node, a.n_tiles, tile, lane) : 0.0;
+    }
     const double at_t0_1 = window_prefix(inc, P, A, lane);
 #pragma unroll
     for (int j = 0; j < kPer; ++j) J[j] = R(off1 + (P[j] - at_t0_1));
@@ -441,7 +456,7 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   // The tile's node groups: the last of its n_groups CTAs to arrive adds the groups'
   // partial rows in group order into group 0's (the forward transform reads those).
   // Arrivals count up by n_groups per evaluation, so the counter needs no reset.
-  if (a.n_groups > 1) {
+  if (!kSweep && a.n_groups > 1) {
     __shared__ int last;
     __threadfence();
     __syncthreads();
@@ -463,6 +478,27 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   }
 }
 
+template <class R>
+__device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
+  __shared__ unsigned long long ticket;
+  if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1ull);
+  __syncthreads();
+  const unsigned long long epoch = ticket / (unsigned long long)a.n_blocks;
+  const int index = (int)(ticket % (unsigned long long)a.n_blocks);
+  double unused0 = 0.0, unused1 = 0.0;
+  column_tile<R, false>(a, index / a.n_groups, index % a.n_groups, epoch, unused0, unused1);
+}
+
+// one node group through every tile of the row, in tile order
+template <class R>
+__device__ __forceinline__ void column_sweep(const ColumnArgsT<R>& a, int group) {
+  double carry0 = 0.0, carry1 = 0.0;
+  for (int tile = 0; tile < a.n_tiles; ++tile) {
+    if (tile > 0) __syncthreads();  // the last tile's projection is done with the shared rows
+    column_tile<R, true>(a, tile, group, 0ull, carry0, carry1);
+  }
+}
+
 // resident CTAs per SM: two in FP64 (128 registers), three in FP32 (85)
 template <class R> constexpr int column_residency() { return sizeof(R) == 8 ? 2 : 3; }
 
@@ -478,6 +514,23 @@ __global__ void __launch_bounds__(kThreads, column_residency<R>())
   const int run = items[blockIdx.x].x;
   if (!flags[run]) return;  // every CTA of an idle run leaves before its ticket
   column_body(own_args(args, run));
+}
+
+// batched, one CTA per (run, node group) walking the run's tiles: items[blockIdx.x] =
+// (run, group), listed longest row first so that the long walks start in the first wave
+template <class R>
+__global__ void __launch_bounds__(kThreads, column_residency<R>())
+    k_column_sweep_b(const ColumnArgsT<R>* args, const int4* items, const int* flags) {
+  const int4 it = items[blockIdx.x];
+  if (!flags[it.x]) return;  // block-uniform
+  column_sweep(own_args(args, it.x), it.y);
+}
+
+template <class R>
+cudaError_t launch_column_sweep_b(const ColumnArgsT<R>* args, const int4* items, const int* flags,
+                                  int n_items, cudaStream_t stream) {
+  k_column_sweep_b<R><<<n_items, kThreads, column_smem<R>(), stream>>>(args, items, flags);
+  return cudaGetLastError();
 }
 
 template <class R>
@@ -499,13 +552,18 @@ template cudaError_t launch_column_b<double>(const ColumnArgsT<double>*, const i
                                              cudaStream_t);
 template cudaError_t launch_column_b<float>(const ColumnArgsT<float>*, const int4*, const int*, int,
                                             cudaStream_t);
+template cudaError_t launch_column_sweep_b<double>(const ColumnArgsT<double>*, const int4*, const int*,
+                                                   int, cudaStream_t);
+template cudaError_t launch_column_sweep_b<float>(const ColumnArgsT<float>*, const int4*, const int*,
+                                                  int, cudaStream_t);
 
 cudaError_t configure_column_kernels() {
-  const void* kernels[4] = {(const void*)k_column<double>, (const void*)k_column_b<double>,
-                            (const void*)k_column<float>, (const void*)k_column_b<float>};
-  const size_t shm[4] = {column_smem<double>(), column_smem<double>(), column_smem<float>(),
-                         column_smem<float>()};
-  for (int i = 0; i < 4; ++i) {
+  const void* kernels[6] = {(const void*)k_column<double>, (const void*)k_column_b<double>,
+                            (const void*)k_column_sweep_b<double>, (const void*)k_column<float>,
+                            (const void*)k_column_b<float>, (const void*)k_column_sweep_b<float>};
+  const size_t shm[6] = {column_smem<double>(), column_smem<double>(), column_smem<double>(),
+                         column_smem<float>(), column_smem<float>(), column_smem<float>()};
+  for (int i = 0; i < 6; ++i) {
     cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shm[i]);
     if (e != cudaSuccess) return e;

@@ -185,6 +185,11 @@ cudaError_t launch_output_b(const OutputArgs* args, const int2* items, const int
 template <class R>
 cudaError_t launch_column_b(const ColumnArgsT<R>* args, const int4* items, const int* flags,
                             int n_items, cudaStream_t stream);
+// the same column, one CTA per (run, node group) walking the run's tiles in order; each
+// group leaves its own partial rows (ForwardArgsT::n_groups = the column's n_groups)
+template <class R>
+cudaError_t launch_column_sweep_b(const ColumnArgsT<R>* args, const int4* items, const int* flags,
+                                  int n_items, cudaStream_t stream);
 
 // ---- stepping kernels (step_kernels.cu)
 struct StepArgs {

@@ -39,20 +39,25 @@ def test_capillary_record_is_a_consistent_problem():
     assert out["rate"].max() > 0  # the pulse ionises
 
 
+SMALL_SCAN = [
+    scan.ScanPoint(120e-6, 1.0, "He", 1.0, 60e-6, 20e-15, 2, 4096, 1),
+    scan.ScanPoint(90e-6, 0.8, "Ar", 0.5, 30e-6, 25e-15, 1, 8192, 2),
+    scan.ScanPoint(140e-6, 1.5, "Ne", 2.0, 100e-6, 12e-15, 3, 4096, 3),
+]
+
+
 @pytest.mark.gpu
-def test_batched_runs_match_single_runs():
+@pytest.mark.parametrize("form", ["tiles", "sweep"])
+def test_batched_runs_match_single_runs(form):
     from solprop_b200 import _lib
 
-    points = [
-        scan.ScanPoint(120e-6, 1.0, "He", 1.0, 60e-6, 20e-15, 2, 4096, 1),
-        scan.ScanPoint(90e-6, 0.8, "Ar", 0.5, 30e-6, 25e-15, 1, 8192, 2),
-        scan.ScanPoint(140e-6, 1.5, "Ne", 2.0, 100e-6, 12e-15, 3, 4096, 3),
-    ]
-    built = [scan.capillary_record(p) for p in points]
+    built = [scan.capillary_record(p) for p in SMALL_SCAN]
     sc = _lib.Scan([r for r, _ in built], [q for _, q in built])
+    sc.set_column(form)
     steps = 12
     sc.advance(steps)
     assert "attempt phase: one CUDA graph" in sc.describe()
+    assert f"column: {'sweep' if form == 'sweep' else 'tile-parallel'}" in sc.describe()
     for i, (rec, pol) in enumerate(built):
         state, info = sc.run(i)
         problem = _lib.Problem(rec)
@@ -79,3 +84,30 @@ def test_batched_run_matches_the_oracle():
         march.attempt_towards(rec.z_end)
     assert march.attempts == info.attempts
     assert rel(state, ws.state) < 1e-10
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_column_forms_give_the_same_bits(precision):
+    """The sweep carries each node's running sums in the order the tile-parallel column
+    adds its predecessors' sums, and the forward transform adds the node groups' partial
+    rows in the order the tile's last CTA does: the runs come out bit for bit equal."""
+    from solprop_b200 import _lib
+
+    built = [scan.capillary_record(p) for p in SMALL_SCAN]
+    states = {}
+    for form in ("tiles", "sweep"):
+        sc = _lib.Scan([r for r, _ in built], [q for _, q in built], 0, precision)
+        sc.set_column(form)
+        sc.advance(8)
+        states[form] = [sc.run(i)[0] for i in range(len(built))]
+        sc.close()
+    for a, b in zip(states["tiles"], states["sweep"]):
+        assert np.array_equal(a, b)
+
+
+def test_unknown_column_form_is_refused():
+    from solprop_b200 import _lib
+
+    with pytest.raises(ValueError):
+        object.__new__(_lib.Scan).set_column("rows")
