@@ -291,8 +291,8 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   R* modal = reinterpret_cast<R*>(column_raw);    // [m][kPitch], then the streams
   R* streams = modal;                              // [s][warp][kPitch]
   R* scratch = modal + (size_t)3 * kGroup * kPitch;
-  __shared__ R wt[kMaxModes * kGroup];
-  __shared__ R gate[kWindow], gate_d[kWindow];  // the temporal window g and g' on the window
+  __shared__ __align__(16) R wt[kMaxModes * kGroup];
+  __shared__ R gate[kPitch], gate_d[kPitch];  // the temporal window g and g' on the window (padded)
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int node = group * kGroup + warp;
   const bool live = node < a.n_nodes;
@@ -314,8 +314,8 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   for (int u = threadIdx.x; u < kWindow; u += blockDim.x) {
     const int t = tw + u;
     const bool in = t >= 0 && t < a.n_to;
-    gate[u] = in ? a.t_window[t] : R(0);
-    gate_d[u] = in ? a.t_window_derivative[t] : R(0);
+    gate[pad(u)] = in ? a.t_window[t] : R(0);
+    gate_d[pad(u)] = in ? a.t_window_derivative[t] : R(0);
   }
   __syncthreads();
   // synthesis and rate on the window
@@ -345,19 +345,34 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
     const int first = (int)(2 * epoch + 1);
     const R dt = R(a.dt);
     R* row = scratch + (size_t)warp * kPitch;
-    // exposure: W~ on [A - K, A + owned + K], increments on [A - K, A + owned + K)
-    R Wf[kPer], inc[kPer];
-    if (at_end) {
-      R Wg[kPer];  // with the reflected ghosts, for the filter only
+    // A node whose rate is zero on the whole window (every tile but the few the pulse
+    // ionises) has zero exposure increments: the filter, the trapezoid and the prefix
+    // would return exact zeros, so they are skipped, the exposure is the offset alone and
+    // the fraction one value.  Where that fraction is zero too (ahead of the pulse) the
+    // current's integrand vanishes and its pass is skipped the same way.  The shortcuts
+    // give the bits of the full path: its zeros may carry a sign, but every sum starts
+    // from +0, which absorbs them.
+    bool dark = true;
 #pragma unroll
-      for (int j = 0; j < kPer; ++j) Wg[j] = W[j];
-      reflect_ends(Wg, row, tw, a.n_to, K, lane);
-      band_filter(Wg, Wf, a.taps, K);
-    } else {
-      band_filter(W, Wf, a.taps, K);
+    for (int j = 0; j < kPer; ++j) dark = dark && W[j] == R(0);
+    dark = __all_sync(0xffffffffu, dark);
+    // exposure: W~ on [A - K, A + owned + K], increments on [A - K, A + owned + K)
+    R inc[kPer];
+    double s0 = 0.0;
+    if (!dark) {
+      R Wf[kPer];
+      if (at_end) {
+        R Wg[kPer];  // with the reflected ghosts, for the filter only
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) Wg[j] = W[j];
+        reflect_ends(Wg, row, tw, a.n_to, K, lane);
+        band_filter(Wg, Wf, a.taps, K);
+      } else {
+        band_filter(W, Wf, a.taps, K);
+      }
+      trapezoid(Wf, inc, dt, tw, A - K, A + owned + K, a.n_to, lane);
+      s0 = owned_sum(inc, A, own_hi, lane);
     }
-    trapezoid(Wf, inc, dt, tw, A - K, A + owned + K, a.n_to, lane);
-    const double s0 = owned_sum(inc, A, own_hi, lane);
     double off0;
     if constexpr (kSweep) {
       off0 = live ? warp_total(carry0) : 0.0;
@@ -368,28 +383,47 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       await_predecessors(a, group, tile, first);
       off0 = live ? predecessors(a.sums0, node, a.n_tiles, tile, lane) : 0.0;
     }
-    double P[kPer];
-    const double at_t0 = window_prefix(inc, P, A, lane);
     // fraction and the current's integrand on [A - K, A + owned + K]
     const R f0 = R(st.preionisation), qm = R(a.charge_mass_ratio);
     R g[kPer];
+    if (dark) {
+      const R x = R(off0);
+      const R f_dark = fraction(f0, a.band ? fmax(x, R(0)) : x);
 #pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-      const int u = kPer * lane + j, t = tw + u;
-      R f = R(0), gv = R(0);
-      if (u >= A - K && u <= A + owned + K && t >= 0 && t < a.n_to) {
-        const R x = R(off0 + (P[j] - at_t0));
-        f = fraction(f0, a.band ? fmax(x, R(0)) : x);
-        gv = f * qm * E[j];
+      for (int j = 0; j < kPer; ++j) {
+        const int u = kPer * lane + j, t = tw + u;
+        const bool in = u >= A - K && u <= A + owned + K && t >= 0 && t < a.n_to;
+        F[j] = in ? f_dark : R(0);
+        g[j] = in ? f_dark * qm * E[j] : R(0);
       }
-      F[j] = f;
-      g[j] = gv;
+    } else {
+      double P[kPer];
+      const double at_t0 = window_prefix(inc, P, A, lane);
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) {
+        const int u = kPer * lane + j, t = tw + u;
+        R f = R(0), gv = R(0);
+        if (u >= A - K && u <= A + owned + K && t >= 0 && t < a.n_to) {
+          const R x = R(off0 + (P[j] - at_t0));
+          f = fraction(f0, a.band ? fmax(x, R(0)) : x);
+          gv = f * qm * E[j];
+        }
+        F[j] = f;
+        g[j] = gv;
+      }
     }
-    if (at_end) reflect_ends(g, row, tw, a.n_to, K, lane);
-    R gf[kPer];
-    band_filter(g, gf, a.taps, K);
-    trapezoid(gf, inc, dt, tw, A, A + owned, a.n_to, lane);
-    const double s1 = owned_sum(inc, A, own_hi, lane);
+    bool still = true;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) still = still && g[j] == R(0);
+    still = __all_sync(0xffffffffu, still);
+    double s1 = 0.0;
+    if (!still) {
+      if (at_end) reflect_ends(g, row, tw, a.n_to, K, lane);
+      R gf[kPer];
+      band_filter(g, gf, a.taps, K);
+      trapezoid(gf, inc, dt, tw, A, A + owned, a.n_to, lane);
+      s1 = owned_sum(inc, A, own_hi, lane);
+    }
     double off1;
     if constexpr (kSweep) {
       off1 = live ? warp_total(carry1) : 0.0;
@@ -400,9 +434,15 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       await_predecessors(a, group, tile, first + 1);
       off1 = live ? predecessors(a.sums1, node, a.n_tiles, tile, lane) : 0.0;
     }
-    const double at_t0_1 = window_prefix(inc, P, A, lane);
+    if (still) {
 #pragma unroll
-    for (int j = 0; j < kPer; ++j) J[j] = R(off1 + (P[j] - at_t0_1));
+      for (int j = 0; j < kPer; ++j) J[j] = R(off1);
+    } else {
+      double P[kPer];
+      const double at_t0_1 = window_prefix(inc, P, A, lane);
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) J[j] = R(off1 + (P[j] - at_t0_1));
+    }
   }
   // outputs on the owned samples: P = (c rho E^2 E) g, X = g rho J, Z = g' rho J
   {
@@ -414,7 +454,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       R p = R(0), x = R(0), z = R(0);
       if (live && u >= A && u < own_hi) {
         const R e = E[j];
-        const R win = gate[u];
+        const R win = gate[pad(u)];
         p = (a.kerr ? factor * (e * e) * e : R(0)) * win;
         if (plasma) {
           const R w = W[j], f = F[j];
@@ -423,7 +463,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
           if (w > R(0) && squared > R(0)) scale = divide(ip * w * (R(1) - f), squared);
           const R current = rho * (J[j] + scale * e);
           x = win * current;
-          z = gate_d[u] * current;
+          z = gate_d[pad(u)] * current;
         }
       }
       streams[(0 * kGroup + warp) * kPitch + pad(u)] = p;
@@ -441,15 +481,28 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   const size_t row_of_group = (size_t)3 * a.n_cols * a.n_to;
   R* base = a.partials + (mine ? tw + u : 0);  // sample t = tw + u of row (group 3 + s) n_cols + m
   if (mine) {
-    for (int s = 0; s < n_streams; ++s) {
-      R v[kGroup];
+    // the three streams' samples of the group's nodes, then mode by mode: the weights
+    // are read once per mode for all streams
+    R v[3][kGroup];
 #pragma unroll
-      for (int w = 0; w < kGroup; ++w) v[w] = streams[(s * kGroup + w) * kPitch + pad(u)];
-      for (int m = 0; m < a.n_modes; ++m) {
-        R acc = R(0);
+    for (int s = 0; s < 3; ++s)
 #pragma unroll
-        for (int w = 0; w < kGroup; ++w) acc += wt[m * kGroup + w] * v[w];
-        base[group * row_of_group + ((size_t)s * a.n_cols + m) * a.n_to] = acc;
+      for (int w = 0; w < kGroup; ++w)
+        v[s][w] = s < n_streams ? streams[(s * kGroup + w) * kPitch + pad(u)] : R(0);
+    R* out = base + group * row_of_group;
+    const size_t stream_stride = (size_t)a.n_cols * a.n_to;
+    for (int m = 0; m < a.n_modes; ++m) {
+      R c[kGroup];
+#pragma unroll
+      for (int w = 0; w < kGroup; ++w) c[w] = wt[m * kGroup + w];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        if (s < n_streams) {
+          R acc = R(0);
+#pragma unroll
+          for (int w = 0; w < kGroup; ++w) acc += c[w] * v[s][w];
+          out[s * stream_stride + (size_t)m * a.n_to] = acc;
+        }
       }
     }
   }
