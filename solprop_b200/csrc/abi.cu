@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/solprop_b200.h"
+#include "host_pool.hpp"
 #include "kernels.cuh"
 
 using namespace sp;
@@ -1510,6 +1511,8 @@ struct sp_scan {
   std::vector<ForwardArgs> h_fwd;
   std::vector<ForwardArgsT<float>> h_fwd32;
   std::vector<int> groups;  // node groups per run
+  // host threads for the per-run work between the batched launches
+  std::unique_ptr<HostPool> pool;
   std::vector<std::unique_ptr<FftClass>> classes;
   AdamsDev *h_adams_start = nullptr, *h_adams_att = nullptr;
   StageScalarsDev *h_stages_start = nullptr, *h_stages_att = nullptr;
@@ -1720,11 +1723,10 @@ void scan_step(sp_scan* S) {
       ss->order = ss->run.variable_order ? 1 : ss->run.order;
     }
   }
-  // phase B: one attempt for every unfinished run
-  int n_att = 0;
-  for (int r = 0; r < R; ++r) {
+  // phase B: one attempt for every unfinished run (the runs' host work on the pool)
+  S->pool->run(R, [&](int r) {
     S->h_flag_att[r] = 0;
-    if (S->done[r]) continue;
+    if (S->done[r]) return;
     sp_session* ss = S->ss[r].get();
     sp_workspace* w = S->ws[r].get();
     const Next nx = adams_next(ss, ss->run.z_end);
@@ -1733,8 +1735,9 @@ void scan_step(sp_scan* S) {
     S->h_stages_att[2 * r] = w->h_stage[0];
     S->h_stages_att[2 * r + 1] = w->h_stage[1];
     S->h_flag_att[r] = 1;
-    ++n_att;
-  }
+  });
+  int n_att = 0;
+  for (int r = 0; r < R; ++r) n_att += S->h_flag_att[r];
   if (!n_att) return;
   // every operand of the attempt phase lives at a fixed address (pinned host tables, device
   // argument arrays), so its launches are captured once and replayed
@@ -1762,18 +1765,17 @@ void scan_step(sp_scan* S) {
   CUDA_CHECK(cudaStreamSynchronize(S->stream));
   for (int r = 0; r < R; ++r)
     if (S->h_flag_att[r]) check_column(S->h_norms + 8 * r, S->norms.p + 8 * r, S->stream);
-  for (int r = 0; r < R; ++r) {
+  S->pool->run(R, [&](int r) {
     S->h_flag_accept[r] = 0;
-    if (!S->h_flag_att[r]) continue;
+    if (!S->h_flag_att[r]) return;
     sp_session* ss = S->ss[r].get();
     try {
       S->h_flag_accept[r] = decide_attempt(ss, S->pending[r], S->h_norms + 8 * r) ? 1 : 0;
     } catch (const Failure&) {
       ss->failed = true;  // below dz_min: this run stops; the others go on
       S->done[r] = 1;
-      continue;
     }
-  }
+  });
   upload_all(S->flag_accept, S->h_flag_accept, R, S->stream);
   CUDA_CHECK(launch_step_b(2, S->step_att.p, S->step_items.p, S->flag_accept.p, S->n_step_items, R, S->stream));
   for (int r = 0; r < R; ++r) {
@@ -1834,6 +1836,12 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     }
     S->done.assign(R, 0);
     S->pending.resize(R);
+    {
+      // up to eight host threads when the batch is large enough to pay for the hand-off
+      const int cores = (int)std::thread::hardware_concurrency();
+      const int workers = R >= 16 ? std::max(0, std::min(cores, 8) - 1) : 0;
+      S->pool = std::make_unique<HostPool>(workers);
+    }
     S->h_adams_start = pinned<AdamsDev>(R);
     S->h_adams_att = pinned<AdamsDev>(R);
     S->h_stages_start = pinned<StageScalarsDev>(R);

@@ -8,49 +8,79 @@
 
 namespace sp {
 
-__constant__ double c_recip_fact[16] = {
-    1.0, 1.0, 1.0 / 2, 1.0 / 6, 1.0 / 24, 1.0 / 120, 1.0 / 720, 1.0 / 5040, 1.0 / 40320,
-    1.0 / 362880, 1.0 / 3628800, 1.0 / 39916800, 1.0 / 479001600, 1.0 / 6227020800.0,
-    1.0 / 87178291200.0, 1.0 / 1307674368000.0};
+// 1 / n! for n < 32, each the double nearest the exact value
+__constant__ double c_inv_fact[32] = {
+    1.0, 1.0, 0.5, 0.16666666666666666,
+    0.041666666666666664, 0.008333333333333333, 0.001388888888888889, 0.0001984126984126984,
+    2.48015873015873e-05, 2.7557319223985893e-06, 2.755731922398589e-07, 2.505210838544172e-08,
+    2.08767569878681e-09, 1.6059043836821613e-10, 1.1470745597729725e-11, 7.647163731819816e-13,
+    4.779477332387385e-14, 2.8114572543455206e-15, 1.5619206968586225e-16, 8.22063524662433e-18,
+    4.110317623312165e-19, 1.9572941063391263e-20, 8.896791392450574e-22, 3.868170170630684e-23,
+    1.6117375710961184e-24, 6.446950284384474e-26, 2.4795962632247976e-27, 9.183689863795546e-29,
+    3.279889237069838e-30, 1.1309962886447716e-31, 3.7699876288159054e-33, 1.216125041553518e-34};
+
+// acc y + c for complex acc, y and real c
+__device__ __forceinline__ double2 horner_step(double2 acc, double2 y, double c) {
+  return make_double2(fma(acc.x, y.x, fma(-acc.y, y.y, c)), fma(acc.x, y.y, acc.y * y.x));
+}
 
 // phi_0(x) .. phi_order(x) (backends/exponential.py:131-224): the upward recurrence
-// from exp(x) beyond |x| = 3, the scaled Taylor series of the highest function, the
-// downward recurrence and repeated doubling below.
-__device__ void phi_functions(double2 x, int order, double2* out) {
-  const double mag = hypot(x.x, x.y);
-  if (mag > 3.0) {
+// phi_k = (phi_{k-1} - 1/(k-1)!) / x from exp(x) beyond |x| = 3; below, x is halved sq
+// times to |y| <= 1/2, phi_order(y) = sum_{m<24} y^m / (m + order)! is summed by Horner's
+// rule, the lower functions follow by the downward recurrence phi_k = 1/k! + y phi_{k+1},
+// and sq doublings phi_k(2y) = 2^-k (phi_0 phi_k + sum_{j=1..k} phi_j / (k - j)!) undo the
+// halving.  Every index is a compile-time one (order <= kMaxWidth), so the functions stay
+// in registers; the divisions are products with 1/x, 1/n! and 2^-k.
+__device__ __forceinline__ void phi_functions(double2 x, int order, double2 (&out)[kMaxWidth + 1]) {
+  const double mag2 = x.x * x.x + x.y * x.y;
+  if (mag2 > 9.0) {
+    const double s = 1.0 / mag2;
+    const double2 rx = make_double2(x.x * s, -x.y * s);
     out[0] = cexp(x);
-    for (int k = 1; k <= order; ++k)
-      out[k] = cdiv(make_double2(out[k - 1].x - c_recip_fact[k - 1], out[k - 1].y), x);
+#pragma unroll
+    for (int k = 1; k <= kMaxWidth; ++k) {
+      if (k > order) break;
+      out[k] = cmul(make_double2(out[k - 1].x - c_inv_fact[k - 1], out[k - 1].y), rx);
+    }
     return;
   }
   int sq = 0;
-  if (mag > 0.5) sq = (int)ceil(log2(fmax(mag, 0.5) / 0.5));
-  const double scale = exp2(-(double)sq);
-  const double2 y = make_double2(x.x * scale, x.y * scale);
-  double2 term = make_double2(c_recip_fact[order], 0.0);
-  double2 total = term;
-  for (int m = 1; m < 24; ++m) {
-    term = cmul(term, y);
-    term = make_double2(term.x / (double)(m + order), term.y / (double)(m + order));
-    total = cadd(total, term);
+  if (mag2 > 0.25) {  // the least sq with 2 |x| <= 2^sq
+    int e;
+    const double f = frexp(2.0 * sqrt(mag2), &e);
+    sq = f == 0.5 ? e - 1 : e;
   }
-  out[order] = total;
-  for (int k = order - 1; k >= 1; --k) {
-    double2 t = cmul(y, out[k + 1]);
-    out[k] = make_double2(c_recip_fact[k] + t.x, t.y);
+  const double scale = ldexp(1.0, -sq);
+  const double2 y = make_double2(x.x * scale, x.y * scale);
+  double2 acc = make_double2(c_inv_fact[23 + order], 0.0);
+#pragma unroll 4
+  for (int m = 22; m >= 0; --m) acc = horner_step(acc, y, c_inv_fact[m + order]);
+  // the downward recurrence from phi_order = acc
+#pragma unroll
+  for (int k = kMaxWidth; k >= 1; --k) {
+    if (k > order) continue;
+    if (k == order) {
+      out[k] = acc;
+    } else {
+      const double2 t = cmul(y, out[k + 1]);
+      out[k] = make_double2(c_inv_fact[k] + t.x, t.y);
+    }
   }
   out[0] = cexp(y);
   for (int level = 0; level < sq; ++level) {
     double2 old[kMaxWidth + 1];
-    for (int k = 0; k <= order; ++k) old[k] = out[k];
+#pragma unroll
+    for (int k = 0; k <= kMaxWidth; ++k) old[k] = out[k];
     out[0] = cmul(old[0], old[0]);
     double p2 = 1.0;
-    for (int k = 1; k <= order; ++k) {
-      p2 *= 2.0;
+#pragma unroll
+    for (int k = 1; k <= kMaxWidth; ++k) {
+      if (k > order) break;
+      p2 *= 0.5;
       double2 t = cmul(old[0], old[k]);
-      for (int j = 1; j <= k; ++j) t = cadd(t, cscale(c_recip_fact[k - j], old[j]));
-      out[k] = make_double2(t.x / p2, t.y / p2);
+#pragma unroll
+      for (int j = 1; j <= k; ++j) t = cadd(t, cscale(c_inv_fact[k - j], old[j]));
+      out[k] = make_double2(t.x * p2, t.y * p2);
     }
   }
 }
@@ -136,10 +166,13 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
     const double2 x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
     double2 phi[kMaxWidth + 1];
     phi_functions(x, width, phi);
-    const double2 fl = cexp(x);
+    // beyond |x| = 3 the recurrence started from exp(x) itself
+    const double2 fl = x.x * x.x + x.y * x.y > 9.0 ? phi[0] : cexp(x);
     double fact = 1.0;
     double2 mom[kMaxWidth];
-    for (int k = 0; k < width; ++k) {
+#pragma unroll
+    for (int k = 0; k < kMaxWidth; ++k) {
+      if (k >= width) break;
       if (k > 0) fact *= (double)k;
       mom[k] = cscale(fact, phi[k + 1]);
       a.moments[(size_t)k * a.n + i] = mom[k];
@@ -183,21 +216,34 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
 }
 
 // ------------------------------------------------------------------ Adams correct
+// Every loop runs to the compile-time bound (kMaxWidth, kMaxOrders) and stops at the
+// trial's width and order count, so the operand rows stay in registers.
 __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block) {
   const AdamsDev& ad = *a.adams;
   const int width = ad.width, n_orders = ad.n_orders;
   double v[kMaxOrders] = {0.0, 0.0, 0.0};
   for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
-    double2 xs[kMaxWidth];
+    double2 xs[kMaxWidth], mom[kMaxWidth];
     xs[0] = a.source[i];
-    for (int j = 1; j < width; ++j) xs[j] = a.store[(size_t)ad.slots[j - 1] * a.n + i];
-    double2 mom[kMaxWidth];
-    for (int k = 0; k < width; ++k) mom[k] = a.moments[(size_t)k * a.n + i];
+#pragma unroll
+    for (int j = 1; j < kMaxWidth; ++j) {
+      if (j >= width) break;
+      xs[j] = a.store[(size_t)ad.slots[j - 1] * a.n + i];
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxWidth; ++k) {
+      if (k >= width) break;
+      mom[k] = a.moments[(size_t)k * a.n + i];
+    }
     // advanced = flow u + dz sum_k M_k sum_j corr_jk X_j
     double2 total = make_double2(0.0, 0.0);
-    for (int k = 0; k < width; ++k) {
+#pragma unroll
+    for (int k = 0; k < kMaxWidth; ++k) {
+      if (k >= width) break;
       double2 comb = make_double2(0.0, 0.0);
-      for (int j = 0; j < width; ++j) {
+#pragma unroll
+      for (int j = 0; j < kMaxWidth; ++j) {
+        if (j >= width) break;
         const double c = ad.corr[j][k];
         if (c != 0.0) comb = cadd(comb, cscale(c, xs[j]));
       }
@@ -214,20 +260,34 @@ __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block)
       for (int p = 0; p < a.stage->n_phi; ++p)
         rate_end = cadd(rate_end, cscale(ad.rate_w[p], a.phi_terms[(size_t)p * a.n + i]));
       endpoint = cmul(csub(rate_end, ref), a.lab[i]);
-      for (int j = 0; j < width - 1; ++j) carried[j] = a.carried[(size_t)j * a.n + i];
+#pragma unroll
+      for (int j = 0; j < kMaxWidth - 1; ++j) {
+        if (j >= width - 1) break;
+        carried[j] = a.carried[(size_t)j * a.n + i];
+      }
       double2 c = cscale(ad.comp_corr_main[0], endpoint);
       double2 t = make_double2(0.0, 0.0);
-      for (int j = 0; j < ad.order; ++j) t = cadd(t, cscale(ad.comp_corr_main[j + 1], carried[j]));
+#pragma unroll
+      for (int j = 0; j < kMaxWidth - 1; ++j) {
+        if (j >= ad.order) break;
+        t = cadd(t, cscale(ad.comp_corr_main[j + 1], carried[j]));
+      }
       adv = cadd(adv, cscale(ad.dz, cadd(t, c)));
     }
     a.advanced[i] = adv;
     const int bin = i % a.n_omega;
     const bool scored = a.norm_mask[bin];
-    for (int r = 0; r < n_orders; ++r) {
+#pragma unroll
+    for (int r = 0; r < kMaxOrders; ++r) {
+      if (r >= n_orders) break;
       double2 d = make_double2(0.0, 0.0);
-      for (int k = 0; k < width; ++k) {
+#pragma unroll
+      for (int k = 0; k < kMaxWidth; ++k) {
+        if (k >= width) break;
         double2 comb = make_double2(0.0, 0.0);
-        for (int j = 0; j < width; ++j) {
+#pragma unroll
+        for (int j = 0; j < kMaxWidth; ++j) {
+          if (j >= width) break;
           const double c = ad.rows[r][j][k];
           if (c != 0.0) comb = cadd(comb, cscale(c, xs[j]));
         }
@@ -237,7 +297,9 @@ __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block)
       if (ad.compensated) {
         // corrector(k) - predictor(k) of the compensation
         double2 tc = make_double2(0.0, 0.0), tp = make_double2(0.0, 0.0);
-        for (int j = 0; j < width - 1; ++j) {
+#pragma unroll
+        for (int j = 0; j < kMaxWidth - 1; ++j) {
+          if (j >= width - 1) break;
           tc = cadd(tc, cscale(ad.comp_corr[r][j + 1], carried[j]));
           tp = cadd(tp, cscale(ad.comp_pred[r][j], carried[j]));
         }
@@ -282,22 +344,27 @@ __device__ __forceinline__ void adams_start_body(const StepArgs& a, int write_ra
   }
 }
 
-__global__ void __launch_bounds__(256) k_adams_predict(StepArgs a) { adams_predict_body(a, blockIdx.x); }
-__global__ void __launch_bounds__(256) k_adams_correct(StepArgs a) { adams_correct_body(a, blockIdx.x); }
+// One run alone: the state is small and the passes are latency-bound, so the blocks are
+// narrow (128 threads) to spread the elements over every SM, and each thread keeps all its
+// operand rows in registers.  Batched, the passes stream far more than L2 holds and are
+// bound by HBM: the register budget is capped so that more warps keep loads in flight.
+constexpr int kStepThreads = 128;
+__global__ void __launch_bounds__(kStepThreads) k_adams_predict(StepArgs a) { adams_predict_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(kStepThreads) k_adams_correct(StepArgs a) { adams_correct_body(a, blockIdx.x); }
 __global__ void k_adams_accept(StepArgs a, int free_slot, int write_rate) {
   adams_accept_body(a, free_slot, write_rate, blockIdx.x);
 }
 __global__ void k_adams_start(StepArgs a, int write_rate) { adams_start_body(a, write_rate, blockIdx.x); }
 
 // batched: items[blockIdx.x] = (run, block of that run)
-__global__ void __launch_bounds__(256) k_adams_predict_b(const StepArgs* args, const int2* items,
-                                                        const int* flags) {
+__global__ void __launch_bounds__(256, 2) k_adams_predict_b(const StepArgs* args, const int2* items,
+                                                           const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
   adams_predict_body(own_args(args, it.x), it.y);
 }
-__global__ void __launch_bounds__(256) k_adams_correct_b(const StepArgs* args, const int2* items,
-                                                        const int* flags) {
+__global__ void __launch_bounds__(256, 4) k_adams_correct_b(const StepArgs* args, const int2* items,
+                                                           const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
   adams_correct_body(own_args(args, it.x), it.y);
@@ -316,11 +383,11 @@ __global__ void k_adams_start_b(const StepArgs* args, const int2* items, const i
 }
 
 cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t s) {
-  k_adams_predict<<<a.n_blocks, 256, 0, s>>>(a);
+  k_adams_predict<<<a.n_blocks, kStepThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t s) {
-  k_adams_correct<<<a.n_blocks, 256, 0, s>>>(a);
+  k_adams_correct<<<a.n_blocks, kStepThreads, 0, s>>>(a);
   k_reduce<<<kMaxOrders + 1, 32, 0, s>>>(a.partials, a.norms, kMaxOrders + 1, a.n_blocks);
   return cudaGetLastError();
 }
