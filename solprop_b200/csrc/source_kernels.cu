@@ -12,10 +12,16 @@
 //                                                                (transforms.py:190)
 //   k_stage_output    held plasma assembly, prefactor, window, absorber, inverse
 //                     propagator                       (plasma.py:579, stepping.py:88)
+#include <algorithm>
+
 #include "fft.cuh"
 #include "kernels.cuh"
 
 namespace sp {
+
+// a row's block: up to 512 threads, so that each keeps its 16 (FP32) or 8 (FP64) points
+// and their twiddles in registers
+constexpr int kRowThreads = 512;
 
 // ----------------------------------------------------------------------------- K1
 template <class R>
@@ -49,16 +55,16 @@ __device__ __forceinline__ void inverse_field_body(const InverseArgsT<R>& a, int
     // O[k] = (X[k] - conj X[M-k]) W^-k / 2, W^-k = conj(exp(-i pi k / M))
     C w = __ldg(tw + k);  // exp(-2 pi i k / n_to)
     C o = cscale(half, cmul(csub(xk, xm), cconj(w)));
-    smem_c[k] = cadd(e, mul_pi(o));  // Z = E + i O
+    smem_c[padded_index<C>(k)] = cadd(e, mul_pi(o));  // Z = E + i O
   }
   __syncthreads();
-  fft_dif_inplace(smem_c, a.log_m, tw, a.log_n_to, /*inverse=*/true);
+  fft_dif_padded</*kInv=*/true>(smem_c, a.log_m, tw, a.log_n_to);
   const R inv_m = R(1.0 / (double)M);
   R* row = a.modal_t + (size_t)col * a.n_to;
   R* absorb = a.absorber_stream ? a.absorber_stream + (size_t)col * a.n_to : nullptr;
 #pragma unroll 4
   for (int m = threadIdx.x; m < M; m += blockDim.x) {
-    C z = smem_c[bitrev(m, a.log_m)];
+    C z = smem_c[padded_index<C>(bitrev(m, a.log_m))];
     R x0 = z.x * inv_m, x1 = z.y * inv_m;
     C v;
     v.x = x0;
@@ -75,13 +81,13 @@ __device__ __forceinline__ void inverse_field_body(const InverseArgsT<R>& a, int
 }
 
 template <class R>
-__global__ void __launch_bounds__(1024) k_inverse_field(InverseArgsT<R> a) {
+__global__ void __launch_bounds__(kRowThreads) k_inverse_field(InverseArgsT<R> a) {
   inverse_field_body(a, blockIdx.x);
 }
 
 // batched: items[blockIdx.x] = (run, column)
 template <class R>
-__global__ void __launch_bounds__(1024) k_inverse_field_b(const InverseArgsT<R>* args, const int2* items,
+__global__ void __launch_bounds__(kRowThreads) k_inverse_field_b(const InverseArgsT<R>* args, const int2* items,
                                                          const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
@@ -89,6 +95,17 @@ __global__ void __launch_bounds__(1024) k_inverse_field_b(const InverseArgsT<R>*
 }
 
 // ----------------------------------------------------------------------------- K4
+// 16-byte loads of a row of complex samples: two in FP32, one in FP64
+template <class R> struct Load16Of;
+template <> struct Load16Of<float> { using type = float4; };
+template <> struct Load16Of<double> { using type = double2; };
+template <class R> using Load16 = typename Load16Of<R>::type;
+__device__ __forceinline__ void split16(const float4& v, float2 (&c)[2]) {
+  c[0] = make_float2(v.x, v.y);
+  c[1] = make_float2(v.z, v.w);
+}
+__device__ __forceinline__ void split16(const double2& v, double2 (&c)[1]) { c[0] = v; }
+
 template <class R>
 __device__ __forceinline__ void forward_field_body(const ForwardArgsT<R>& a, int row_index) {
   using C = cplx<R>;
@@ -97,34 +114,50 @@ __device__ __forceinline__ void forward_field_body(const ForwardArgsT<R>& a, int
   const int row = a.rows[row_index];
   const int M = a.n_to >> 1;
   if (row < a.n_partial_rows) {
-    // a projected stream: the node groups' partial projections, summed in group order
-#pragma unroll 4
-    for (int m = threadIdx.x; m < M; m += blockDim.x) {
-      C acc;
-      acc.x = R(0);
-      acc.y = R(0);
-      for (int g = 0; g < a.n_groups; ++g) {
-        const C v = reinterpret_cast<const C*>(
-            a.partials + ((size_t)g * a.n_partial_rows + row) * a.n_to)[m];
-        acc = cadd(acc, v);
+    // a projected stream: the node groups' partial projections, summed in group order.
+    // 16-byte loads (two complex samples in FP32, one in FP64), eight groups' loads issued
+    // before their sums, so that enough bytes are in flight to stream the rows
+    constexpr int kPair = 16 / (int)sizeof(C);
+    constexpr int kBatch = 8;
+    const size_t group_stride = (size_t)a.n_partial_rows * a.n_to / (2 * kPair);  // in 16-byte units
+    using V = Load16<R>;
+    const V* rows16 = reinterpret_cast<const V*>(a.partials + (size_t)row * a.n_to);
+    for (int v = threadIdx.x; v < M / kPair; v += blockDim.x) {
+      C acc[kPair];
+#pragma unroll
+      for (int h = 0; h < kPair; ++h) acc[h].x = acc[h].y = R(0);
+      for (int g0 = 0; g0 < a.n_groups; g0 += kBatch) {
+        V x[kBatch];
+#pragma unroll
+        for (int g = 0; g < kBatch; ++g)
+          if (g0 + g < a.n_groups) x[g] = __ldg(rows16 + (size_t)(g0 + g) * group_stride + v);
+#pragma unroll
+        for (int g = 0; g < kBatch; ++g) {
+          if (g0 + g >= a.n_groups) break;
+          C c[kPair];
+          split16(x[g], c);
+#pragma unroll
+          for (int h = 0; h < kPair; ++h) acc[h] = cadd(acc[h], c[h]);
+        }
       }
-      smem_c[m] = acc;  // z = x_even + i x_odd
+#pragma unroll
+      for (int h = 0; h < kPair; ++h) smem_c[padded_index<C>(kPair * v + h)] = acc[h];  // z = x_even + i x_odd
     }
   } else {
     const double2* x = reinterpret_cast<const double2*>(a.streams + (size_t)row * a.n_to);
 #pragma unroll 4
-    for (int m = threadIdx.x; m < M; m += blockDim.x) smem_c[m] = to_c<C>(x[m]);
+    for (int m = threadIdx.x; m < M; m += blockDim.x) smem_c[padded_index<C>(m)] = to_c<C>(x[m]);
   }
   __syncthreads();
-  fft_dif_inplace(smem_c, a.log_m, a.twiddles, a.log_n_to, /*inverse=*/false);
+  fft_dif_padded</*kInv=*/false>(smem_c, a.log_m, a.twiddles, a.log_n_to);
   C* out = a.spectra + (size_t)row * a.n_omega;
   const R half = R(0.5);
 #pragma unroll 4
   for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) {
     const int k = a.crop_identity ? j : (int)a.crop_index[j];
     const int km = (k == 0) ? 0 : M - k;
-    C zk = smem_c[bitrev(k == M ? 0 : k, a.log_m)];
-    C zm = cconj(smem_c[bitrev(km == M ? 0 : km, a.log_m)]);
+    C zk = smem_c[padded_index<C>(bitrev(k == M ? 0 : k, a.log_m))];
+    C zm = cconj(smem_c[padded_index<C>(bitrev(km == M ? 0 : km, a.log_m))]);
     C e = cscale(half, cadd(zk, zm));
     C o = cscale(half, mul_mi(csub(zk, zm)));  // (Z[k] - conj Z[M-k]) / (2 i)
     C w;
@@ -139,13 +172,13 @@ __device__ __forceinline__ void forward_field_body(const ForwardArgsT<R>& a, int
 }
 
 template <class R>
-__global__ void __launch_bounds__(1024) k_forward_field(ForwardArgsT<R> a) {
+__global__ void __launch_bounds__(kRowThreads) k_forward_field(ForwardArgsT<R> a) {
   forward_field_body(a, blockIdx.x);
 }
 
 // batched: items[blockIdx.x] = (run, row index)
 template <class R>
-__global__ void __launch_bounds__(1024) k_forward_field_b(const ForwardArgsT<R>* args, const int2* items,
+__global__ void __launch_bounds__(kRowThreads) k_forward_field_b(const ForwardArgsT<R>* args, const int2* items,
                                                          const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
@@ -203,14 +236,20 @@ __global__ void k_stage_output_b(const OutputArgs* args, const int2* items, cons
 }
 
 // ----------------------------------------------------------------------------- launch
-static int threads_for(int m) { return m >= 1024 ? 1024 : (m >= 32 ? m : 32); }
+// a block per row: one thread per register group of the transform's passes (M / 16 in FP32,
+// M / 8 in FP64), at least 64 and at most kRowThreads
+template <class R>
+static int threads_for(int m) {
+  return std::min(kRowThreads, std::max(64, m >> kRadixBits<cplx<R>>));
+}
+template <class R>
+static size_t row_smem(int m) { return padded_length<cplx<R>>(m) * sizeof(cplx<R>); }
 
 template <class R>
 cudaError_t launch_inverse(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream) {
   if (fft_cluster_size(a.n_to) > 1) return launch_inverse_cluster(a, n_cols, stream);
   const int M = a.n_to >> 1;
-  const size_t shm = (size_t)M * sizeof(cplx<R>);
-  k_inverse_field<R><<<n_cols, threads_for(M), shm, stream>>>(a);
+  k_inverse_field<R><<<n_cols, threads_for<R>(M), row_smem<R>(M), stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -218,8 +257,7 @@ template <class R>
 cudaError_t launch_forward(const ForwardArgsT<R>& a, int n_rows, cudaStream_t stream) {
   if (fft_cluster_size(a.n_to) > 1) return launch_forward_cluster(a, n_rows, stream);
   const int M = a.n_to >> 1;
-  const size_t shm = (size_t)M * sizeof(cplx<R>);
-  k_forward_field<R><<<n_rows, threads_for(M), shm, stream>>>(a);
+  k_forward_field<R><<<n_rows, threads_for<R>(M), row_smem<R>(M), stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -260,7 +298,7 @@ template <class R>
 cudaError_t launch_inverse_b(const InverseArgsT<R>* args, const int2* items, const int* flags,
                              int n_items, int n_to, cudaStream_t stream) {
   const int M = n_to >> 1;
-  k_inverse_field_b<R><<<n_items, threads_for(M), (size_t)M * sizeof(cplx<R>), stream>>>(args, items, flags);
+  k_inverse_field_b<R><<<n_items, threads_for<R>(M), row_smem<R>(M), stream>>>(args, items, flags);
   return cudaGetLastError();
 }
 
@@ -268,7 +306,7 @@ template <class R>
 cudaError_t launch_forward_b(const ForwardArgsT<R>* args, const int2* items, const int* flags,
                              int n_items, int n_to, cudaStream_t stream) {
   const int M = n_to >> 1;
-  k_forward_field_b<R><<<n_items, threads_for(M), (size_t)M * sizeof(cplx<R>), stream>>>(args, items, flags);
+  k_forward_field_b<R><<<n_items, threads_for<R>(M), row_smem<R>(M), stream>>>(args, items, flags);
   return cudaGetLastError();
 }
 
