@@ -72,18 +72,25 @@ __device__ __noinline__ static void fft_dif_inplace(C* s, int log_n, const C* __
 // 2^K-point DFT in registers, multiplies output f by w_L^(f j) and stores it back where it
 // came from -- so the row ends in the same bit-reversed order as fft_dif_inplace, in
 // ceil(log_n / K) passes instead of log_n / 2.  Radix 16 in FP32 and 8 in FP64 (the
-// points fill 32 registers either way).  The row is padded by one element per 128 bytes
-// (padded_index), which keeps every pass's loads and stores at the minimum number of
-// shared-memory wavefronts, the short spans of the last passes included.
+// points fill 32 registers either way).  The row is stored swizzled (row_slot): the low
+// bits of an index, which pick the element's place in a 128-byte line of banks, are XORed
+// with every higher group of as many bits.  That is a bijection, and it keeps each pass's
+// strided loads and stores and the epilogues' bit-reversed reads (stride M / 32 across a
+// warp) at the minimum number of shared-memory wavefronts.
 
 template <class C>
-constexpr int kPadShift = sizeof(C) == 8 ? 4 : 3;  // elements per 128 bytes: 16 or 8
+constexpr int kBankBits = sizeof(C) == 8 ? 4 : 3;  // log2 of the elements per 128 bytes
 template <class C>
-__host__ __device__ __forceinline__ int padded_index(int i) { return i + (i >> kPadShift<C>); }
-template <class C>
-__host__ __device__ constexpr size_t padded_length(int n) {
-  return (size_t)n + ((size_t)n >> kPadShift<C>);
+__host__ __device__ __forceinline__ int row_slot(int i) {
+  constexpr int b = kBankBits<C>;
+  constexpr int mask = (1 << b) - 1;
+  int fold = 0;
+#pragma unroll
+  for (int shift = b; shift < 16; shift += b) fold ^= i >> shift;
+  return i ^ (fold & mask);
 }
+template <class C>
+__host__ __device__ constexpr size_t row_length(int n) { return (size_t)n; }
 template <class C>
 constexpr int kRadixBits = sizeof(C) == 8 ? 4 : 3;
 
@@ -150,7 +157,7 @@ __device__ __forceinline__ C span_twiddle(const C* __restrict__ table, int e, in
   return w;
 }
 
-// one pass of K fused stages at span 2^log_len over the padded row
+// one pass of K fused stages at span 2^log_len over the swizzled row
 template <int K, bool kInv, class C>
 __device__ __forceinline__ void dif_pass(C* s, int log_n, int log_len, const C* __restrict__ table,
                                          int log_table) {
@@ -164,7 +171,7 @@ __device__ __forceinline__ void dif_pass(C* s, int log_n, int log_len, const C* 
     const int base = ((p >> log_q) << log_len) + j;
     C x[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) x[r] = s[padded_index<C>(base + r * q)];
+    for (int r = 0; r < R; ++r) x[r] = s[row_slot<C>(base + r * q)];
     dft_registers<K, kInv>(x);
     if (j != 0) {
 #pragma unroll
@@ -172,16 +179,16 @@ __device__ __forceinline__ void dif_pass(C* s, int log_n, int log_len, const C* 
         x[r] = cmul(x[r], span_twiddle<kInv>(table, bitrev_const<K>(r) * j, shift, half_table));
     }
 #pragma unroll
-    for (int r = 0; r < R; ++r) s[padded_index<C>(base + r * q)] = x[r];
+    for (int r = 0; r < R; ++r) s[row_slot<C>(base + r * q)] = x[r];
   }
   __syncthreads();
 }
 
-// The padded row s (padded_length(n) elements, natural order, made visible by the caller's
-// barrier) is transformed in place into bit-reversed order: s[padded_index(bitrev(k))] =
-// X[k].  Twiddles as for fft_dif_inplace.
+// The swizzled row s (s[row_slot(i)] = x[i], made visible by the caller's barrier) is
+// transformed in place into bit-reversed order: s[row_slot(bitrev(k))] = X[k].  Twiddles as
+// for fft_dif_inplace.
 template <bool kInv, class C>
-__device__ __forceinline__ void fft_dif_padded(C* s, int log_n, const C* __restrict__ table, int log_table) {
+__device__ __forceinline__ void fft_dif_swizzled(C* s, int log_n, const C* __restrict__ table, int log_table) {
   constexpr int K = kRadixBits<C>;
   int log_len = log_n;
   for (; log_len >= K; log_len -= K) dif_pass<K, kInv>(s, log_n, log_len, table, log_table);

@@ -48,7 +48,7 @@ __device__ __forceinline__ void cross_dft(cg::cluster_group& cluster, Cx* sc, in
                                           bool inverse, Cx (&out)[C]) {
   Cx y[C], w[C];
 #pragma unroll
-  for (int n1 = 0; n1 < C; ++n1) y[n1] = cluster.map_shared_rank(sc, n1)[bitrev(k1, log_mp)];
+  for (int n1 = 0; n1 < C; ++n1) y[n1] = cluster.map_shared_rank(sc, n1)[row_slot<Cx>(bitrev(k1, log_mp))];
 #pragma unroll
   for (int n1 = 0; n1 < C; ++n1) w[n1] = w_m(tw, (long)n1 * k1, log_m, inverse);
   const int Mp = 1 << log_mp;
@@ -102,10 +102,10 @@ __device__ __forceinline__ void inverse_cluster_body(const InverseArgsT<R>& a, i
     const Cx e = cscale(half, cadd(xk, xm));
     const Cx w = __ldg(tw + k);
     const Cx o = cscale(half, cmul(csub(xk, xm), cconj(w)));
-    sc[n2] = cadd(e, mul_pi(o));
+    sc[row_slot<Cx>(n2)] = cadd(e, mul_pi(o));
   }
   __syncthreads();
-  fft_dif_inplace(sc, log_mp, tw, a.log_n_to, /*inverse=*/true);  // sc[bitrev(k1)] = Y_r[k1]
+  fft_dif_swizzled</*kInv=*/true>(sc, log_mp, tw, a.log_n_to);  // sc[slot(bitrev(k1))] = Y_r[k1]
   cluster.sync();
   // this CTA's slice of k1; z[k1 + Mp k2] for every k2
   const int slice = Mp / C;
@@ -175,15 +175,15 @@ __device__ __forceinline__ void forward_cluster_body(const ForwardArgsT<R>& a, i
       for (int g = 0; g < a.n_groups; ++g)
         acc = cadd(acc, reinterpret_cast<const Cx*>(
                             a.partials + ((size_t)g * a.n_partial_rows + row) * a.n_to)[m]);
-      sc[n2] = acc;
+      sc[row_slot<Cx>(n2)] = acc;
     }
   } else {
     const double2* x = reinterpret_cast<const double2*>(a.streams + (size_t)row * a.n_to);
 #pragma unroll 4
-    for (int n2 = threadIdx.x; n2 < Mp; n2 += blockDim.x) sc[n2] = to_c<Cx>(x[C * n2 + r]);
+    for (int n2 = threadIdx.x; n2 < Mp; n2 += blockDim.x) sc[row_slot<Cx>(n2)] = to_c<Cx>(x[C * n2 + r]);
   }
   __syncthreads();
-  fft_dif_inplace(sc, log_mp, a.twiddles, a.log_n_to, /*inverse=*/false);
+  fft_dif_swizzled</*kInv=*/false>(sc, log_mp, a.twiddles, a.log_n_to);
   cluster.sync();
   for (int kk = threadIdx.x; kk < slice; kk += blockDim.x) {
     const int k1 = r * slice + kk;

@@ -55,16 +55,16 @@ __device__ __forceinline__ void inverse_field_body(const InverseArgsT<R>& a, int
     // O[k] = (X[k] - conj X[M-k]) W^-k / 2, W^-k = conj(exp(-i pi k / M))
     C w = __ldg(tw + k);  // exp(-2 pi i k / n_to)
     C o = cscale(half, cmul(csub(xk, xm), cconj(w)));
-    smem_c[padded_index<C>(k)] = cadd(e, mul_pi(o));  // Z = E + i O
+    smem_c[row_slot<C>(k)] = cadd(e, mul_pi(o));  // Z = E + i O
   }
   __syncthreads();
-  fft_dif_padded</*kInv=*/true>(smem_c, a.log_m, tw, a.log_n_to);
+  fft_dif_swizzled</*kInv=*/true>(smem_c, a.log_m, tw, a.log_n_to);
   const R inv_m = R(1.0 / (double)M);
   R* row = a.modal_t + (size_t)col * a.n_to;
   R* absorb = a.absorber_stream ? a.absorber_stream + (size_t)col * a.n_to : nullptr;
 #pragma unroll 4
   for (int m = threadIdx.x; m < M; m += blockDim.x) {
-    C z = smem_c[padded_index<C>(bitrev(m, a.log_m))];
+    C z = smem_c[row_slot<C>(bitrev(m, a.log_m))];
     R x0 = z.x * inv_m, x1 = z.y * inv_m;
     C v;
     v.x = x0;
@@ -141,23 +141,23 @@ __device__ __forceinline__ void forward_field_body(const ForwardArgsT<R>& a, int
         }
       }
 #pragma unroll
-      for (int h = 0; h < kPair; ++h) smem_c[padded_index<C>(kPair * v + h)] = acc[h];  // z = x_even + i x_odd
+      for (int h = 0; h < kPair; ++h) smem_c[row_slot<C>(kPair * v + h)] = acc[h];  // z = x_even + i x_odd
     }
   } else {
     const double2* x = reinterpret_cast<const double2*>(a.streams + (size_t)row * a.n_to);
 #pragma unroll 4
-    for (int m = threadIdx.x; m < M; m += blockDim.x) smem_c[padded_index<C>(m)] = to_c<C>(x[m]);
+    for (int m = threadIdx.x; m < M; m += blockDim.x) smem_c[row_slot<C>(m)] = to_c<C>(x[m]);
   }
   __syncthreads();
-  fft_dif_padded</*kInv=*/false>(smem_c, a.log_m, a.twiddles, a.log_n_to);
+  fft_dif_swizzled</*kInv=*/false>(smem_c, a.log_m, a.twiddles, a.log_n_to);
   C* out = a.spectra + (size_t)row * a.n_omega;
   const R half = R(0.5);
 #pragma unroll 4
   for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) {
     const int k = a.crop_identity ? j : (int)a.crop_index[j];
     const int km = (k == 0) ? 0 : M - k;
-    C zk = smem_c[padded_index<C>(bitrev(k == M ? 0 : k, a.log_m))];
-    C zm = cconj(smem_c[padded_index<C>(bitrev(km == M ? 0 : km, a.log_m))]);
+    C zk = smem_c[row_slot<C>(bitrev(k == M ? 0 : k, a.log_m))];
+    C zm = cconj(smem_c[row_slot<C>(bitrev(km == M ? 0 : km, a.log_m))]);
     C e = cscale(half, cadd(zk, zm));
     C o = cscale(half, mul_mi(csub(zk, zm)));  // (Z[k] - conj Z[M-k]) / (2 i)
     C w;
@@ -243,7 +243,7 @@ static int threads_for(int m) {
   return std::min(kRowThreads, std::max(64, m >> kRadixBits<cplx<R>>));
 }
 template <class R>
-static size_t row_smem(int m) { return padded_length<cplx<R>>(m) * sizeof(cplx<R>); }
+static size_t row_smem(int m) { return row_length<cplx<R>>(m) * sizeof(cplx<R>); }
 
 template <class R>
 cudaError_t launch_inverse(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream) {
