@@ -211,9 +211,10 @@ sp_status sp_scan_advance(sp_scan* scan, int32_t steps, sp_scan_status* out);
 sp_status sp_scan_run(sp_scan* scan, int32_t run, double* state, sp_batch* info);
 void* sp_scan_stream(sp_scan* scan);
 /* The scan's plan, as text: whether the attempt phase runs as one captured CUDA graph,
- * and per grid size whether the inverse and forward transforms run in one CTA per row or
- * over a cluster, with the autotuner's timings (ms per launch; -1 where a form was not a
- * candidate).  Returns the text's length. */
+ * the response column's form, the host's time per batch step so far, and per grid size
+ * whether the inverse and forward transforms run in one CTA per row or over a cluster,
+ * with the autotuner's timings (ms per launch; -1 where a form was not a candidate).
+ * Returns the text's length. */
 size_t sp_scan_describe(const sp_scan* scan, char* buf, size_t len);
 /* The response column's form in a scan.  The scan's autotuner times both at creation
  * and keeps the faster; this call fixes one (a later attempt recaptures its graph).

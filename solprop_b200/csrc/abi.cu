@@ -6,6 +6,7 @@
 // from the norms the device reduces, one device synchronisation per attempt, as the
 // reference's native march does (native/src/march/adams_march.cpp, rk_march.cpp).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -629,46 +630,55 @@ static void build_workspace(sp_workspace* ws) {
 }
 
 // ====================================================================== coefficient tables
-// stepper/multistep.py _basis_rows: the Lagrange basis from its own roots, ascending
-static void basis_rows(const std::vector<double>& pts, double upper, bool integrate,
-                       std::vector<double>& rows, std::vector<double>& weights) {
-  const int n = (int)pts.size();
-  rows.assign((size_t)n * n, 0.0);
-  weights.assign(n, 0.0);
-  std::vector<double> coef(n + 1), prod(n + 1);
-  for (int index = 0; index < n; ++index) {
-    const double node = pts[index];
-    int length = 1;
-    coef[0] = 1.0;
-    double den = 1.0;
-    for (int other = 0; other < n; ++other) {
-      if (other == index) continue;
-      const double root = pts[other];
-      prod[0] = 0.0;
-      for (int p = 0; p < length; ++p) prod[p + 1] = coef[p];
-      for (int p = 0; p < length; ++p) prod[p] -= root * coef[p];
-      ++length;
-      for (int p = 0; p < length; ++p) coef[p] = prod[p];
-      den *= node - root;
-    }
-    if (integrate) {
-      double integral = 0.0;
-      for (int p = length - 1; p >= 0; --p) integral = (integral + coef[p] / (p + 1)) * upper;
-      weights[index] = integral / den;
-    } else {
-      for (int p = 0; p < length; ++p) rows[(size_t)index * n + p] = coef[p] / den;
-    }
+// stepper/multistep.py _basis_rows: the Lagrange basis from its own roots, ascending.
+// The stencils hold a few points (at most kBasis), so every list and table here is a
+// fixed-size array: the per-run host work of a batch step allocates nothing.
+constexpr int kBasis = kMaxWidth + 1;
+struct Points {
+  double v[kBasis];
+  int n = 0;
+  void push(double x) {
+    if (n >= kBasis) throw Failure(SP_ERR_ARGUMENT, "an Adams stencil longer than the tables hold");
+    v[n++] = x;
+  }
+};
+// coef (ascending powers) and denominator of basis polynomial `index`
+static int basis_poly(const Points& pts, int index, double (&coef)[kBasis + 1], double& den) {
+  double prod[kBasis + 1];
+  const double node = pts.v[index];
+  int length = 1;
+  coef[0] = 1.0;
+  den = 1.0;
+  for (int other = 0; other < pts.n; ++other) {
+    if (other == index) continue;
+    const double root = pts.v[other];
+    prod[0] = 0.0;
+    for (int p = 0; p < length; ++p) prod[p + 1] = coef[p];
+    for (int p = 0; p < length; ++p) prod[p] -= root * coef[p];
+    ++length;
+    for (int p = 0; p < length; ++p) coef[p] = prod[p];
+    den *= node - root;
+  }
+  return length;
+}
+// rows[i][p]: coefficient p of basis polynomial i
+static void lagrange(const Points& pts, double (&rows)[kBasis][kBasis]) {
+  for (int index = 0; index < pts.n; ++index) {
+    double coef[kBasis + 1], den;
+    const int length = basis_poly(pts, index, coef, den);
+    for (int p = 0; p < length; ++p) rows[index][p] = coef[p] / den;
   }
 }
-static std::vector<double> lagrange(const std::vector<double>& pts) {
-  std::vector<double> r, w;
-  basis_rows(pts, 1.0, false, r, w);
-  return r;
-}
-static std::vector<double> integrated(const std::vector<double>& pts) {
-  std::vector<double> r, w;
-  basis_rows(pts, 1.0, true, r, w);
-  return w;
+// weights[i]: the integral of basis polynomial i over [0, 1]
+static void integrated(const Points& pts, double (&weights)[kBasis]) {
+  const double upper = 1.0;
+  for (int index = 0; index < pts.n; ++index) {
+    double coef[kBasis + 1], den;
+    const int length = basis_poly(pts, index, coef, den);
+    double integral = 0.0;
+    for (int p = length - 1; p >= 0; --p) integral = (integral + coef[p] / (p + 1)) * upper;
+    weights[index] = integral / den;
+  }
 }
 
 // ====================================================================== session
@@ -744,7 +754,8 @@ struct Pending {
   double dz = 0, end = 0;
   bool kink = false, fixed = false;
   int order = 1, free_slot = 0;
-  std::vector<int> orders;
+  int orders[kMaxOrders] = {0, 0, 0};  // the scored orders, the trial's own first
+  int n_orders = 0;
 };
 
 static Pending prepare_attempt(sp_session* S, double dz, double end, bool kink, bool fixed) {
@@ -758,38 +769,34 @@ static Pending prepare_attempt(sp_session* S, double dz, double end, bool kink, 
   pd.kink = kink;
   pd.fixed = fixed;
   // stencil (adams_core.py:150-206)
-  std::vector<double> nodes;
-  std::vector<int> slots;
+  Points nodes;
+  int slots[kBasis];
   for (auto it = S->history.rbegin(); it != S->history.rend(); ++it) {
-    nodes.push_back((it->first - S->z) / dz);
-    slots.push_back(it->second);
+    nodes.push((it->first - S->z) / dz);
+    slots[nodes.n - 1] = it->second;
   }
-  const int held = (int)nodes.size();
+  const int held = nodes.n;
   const int order = std::min(S->order, held);
   const bool rising = !S->last_rejected && held > order;
-  std::vector<int> orders{order};
+  pd.orders[pd.n_orders++] = order;
   if (R.variable_order) {
     for (int o : {order - 1, order + 1})
-      if (o >= 1 && o <= R.order && o <= held && (o < order || rising)) orders.push_back(o);
+      if (o >= 1 && o <= R.order && o <= held && (o < order || rising)) pd.orders[pd.n_orders++] = o;
   }
   pd.order = order;
-  pd.orders = orders;
   // the row an accepted step writes: the first not kept (marches/adams.py:593-596)
   {
-    std::vector<std::pair<double, int>> keep;
-    if (R.order) {
-      size_t from = S->history.size() > (size_t)R.order ? S->history.size() - R.order : 0;
-      keep.assign(S->history.begin() + from, S->history.end());
-    }
+    const size_t from = !R.order ? S->history.size()
+                        : S->history.size() > (size_t)R.order ? S->history.size() - R.order : 0;
     int free_slot = 0;
     for (;; ++free_slot) {
       bool used = false;
-      for (auto& e : keep) used |= e.second == free_slot;
+      for (size_t e = from; e < S->history.size(); ++e) used |= S->history[e].second == free_slot;
       if (!used) break;
     }
     pd.free_slot = free_slot;
   }
-  int width = 1 + *std::max_element(orders.begin(), orders.end());
+  int width = 1 + *std::max_element(pd.orders, pd.orders + pd.n_orders);
   AdamsDev& ad = *ws->h_adams;
   std::memset(&ad, 0, sizeof(ad));
   ad.dz = dz;
@@ -797,45 +804,49 @@ static Pending prepare_attempt(sp_session* S, double dz, double end, bool kink, 
   ad.atol = R.atol;
   ad.order = order;
   ad.width = width;
-  ad.n_orders = (int)orders.size();
+  ad.n_orders = pd.n_orders;
   ad.compensated = comp;
   ad.free_slot = pd.free_slot;
   for (int j = 0; j < width - 1 && j < held; ++j) {
     ad.slots[j] = slots[j];
-    ad.nodes[j] = nodes[j];
+    ad.nodes[j] = nodes.v[j];
   }
-  {
-    std::vector<double> pn(nodes.begin(), nodes.begin() + order);
-    auto c = lagrange(pn);
-    for (int j = 0; j < order; ++j)
-      for (int k = 0; k < order; ++k) ad.pred[j][k] = c[(size_t)j * order + k];
-    std::vector<double> cn{1.0};
-    cn.insert(cn.end(), nodes.begin(), nodes.begin() + order);
-    auto cc = lagrange(cn);
-    for (int j = 0; j <= order; ++j)
-      for (int k = 0; k <= order; ++k) ad.corr[j][k] = cc[(size_t)j * (order + 1) + k];
-  }
-  for (int r = 0; r < (int)orders.size(); ++r) {
-    const int k = orders[r];
-    std::vector<double> st(nodes.begin(), nodes.begin() + k);
-    std::vector<double> th{1.0};
-    th.insert(th.end(), st.begin(), st.end());
-    auto a1 = lagrange(th), a2 = lagrange(st);
+  // the first k nodes, and the same behind the new point theta = 1
+  auto stencil = [&](int k, bool with_one) {
+    Points p;
+    if (with_one) p.push(1.0);
+    for (int j = 0; j < k; ++j) p.push(nodes.v[j]);
+    return p;
+  };
+  double c[kBasis][kBasis];
+  lagrange(stencil(order, false), c);
+  for (int j = 0; j < order; ++j)
+    for (int k = 0; k < order; ++k) ad.pred[j][k] = c[j][k];
+  lagrange(stencil(order, true), c);
+  for (int j = 0; j <= order; ++j)
+    for (int k = 0; k <= order; ++k) ad.corr[j][k] = c[j][k];
+  for (int r = 0; r < pd.n_orders; ++r) {
+    const int k = pd.orders[r];
+    const Points st = stencil(k, false), th = stencil(k, true);
+    double a2[kBasis][kBasis];
+    lagrange(th, c);
+    lagrange(st, a2);
     for (int j = 0; j <= k; ++j)
-      for (int q = 0; q <= k; ++q) ad.rows[r][j][q] = a1[(size_t)j * (k + 1) + q];
+      for (int q = 0; q <= k; ++q) ad.rows[r][j][q] = c[j][q];
     for (int j = 0; j < k; ++j)
-      for (int q = 0; q < k; ++q) ad.rows[r][j + 1][q] -= a2[(size_t)j * k + q];
+      for (int q = 0; q < k; ++q) ad.rows[r][j + 1][q] -= a2[j][q];
     if (comp) {
-      auto wp = integrated(st), wc = integrated(th);
+      double wp[kBasis], wc[kBasis];
+      integrated(st, wp);
+      integrated(th, wc);
       for (int j = 0; j < k; ++j) ad.comp_pred[r][j] = wp[j];
       for (int j = 0; j <= k; ++j) ad.comp_corr[r][j] = wc[j];
     }
   }
   if (comp) {
-    std::vector<double> st(nodes.begin(), nodes.begin() + order);
-    std::vector<double> th{1.0};
-    th.insert(th.end(), st.begin(), st.end());
-    auto wp = integrated(st), wc = integrated(th);
+    double wp[kBasis], wc[kBasis];
+    integrated(stencil(order, false), wp);
+    integrated(stencil(order, true), wc);
     for (int j = 0; j < order; ++j) ad.comp_pred_main[j] = wp[j];
     for (int j = 0; j <= order; ++j) ad.comp_corr_main[j] = wc[j];
     P.phi_rate.eval_before(S->z + dz, ad.rate_w);
@@ -853,8 +864,8 @@ static bool decide_attempt(sp_session* S, const Pending& pd, const double* sums)
   S->evaluations += 1;
   const double magnitude = std::sqrt(sums[kMaxOrders]);
   const double scale = R.rtol * magnitude + R.atol;
-  std::vector<double> norms(pd.orders.size());
-  for (size_t r = 0; r < pd.orders.size(); ++r) norms[r] = std::sqrt(sums[r]) / scale;
+  double norms[kMaxOrders];
+  for (int r = 0; r < pd.n_orders; ++r) norms[r] = std::sqrt(sums[r]) / scale;
   const double norm = norms[0];
   const int order = pd.order;
   const double dz = pd.dz;
@@ -874,13 +885,13 @@ static bool decide_attempt(sp_session* S, const Pending& pd, const double* sums)
     S->proposal = limit_step(dz, sc, R.dz_min, R.dz_max);
     return false;
   }
-  std::vector<std::pair<double, int>> keep;
-  if (R.order) {
-    size_t from = S->history.size() > (size_t)R.order ? S->history.size() - R.order : 0;
-    keep.assign(S->history.begin() + from, S->history.end());
+  // keep the newest R.order rows (none for order 0), then the new one -- in place
+  {
+    const size_t from = !R.order ? S->history.size()
+                        : S->history.size() > (size_t)R.order ? S->history.size() - R.order : 0;
+    S->history.erase(S->history.begin(), S->history.begin() + from);
+    S->history.push_back({S->z + dz, pd.free_slot});
   }
-  keep.push_back({S->z + dz, pd.free_slot});
-  S->history = keep;
   S->rejections = 0;
   // order choice (adams_core.py:256-301)
   int stored = order, control = order;
@@ -898,13 +909,13 @@ static bool decide_attempt(sp_session* S, const Pending& pd, const double* sums)
     };
     int best = pd.orders[0];
     double bw = weight(norms[0], pd.orders[0]);
-    for (size_t r = 1; r < pd.orders.size(); ++r) {
+    for (int r = 1; r < pd.n_orders; ++r) {
       double w = weight(norms[r], pd.orders[r]);
       if (w > bw) { bw = w; best = pd.orders[r]; }
     }
     if (best != order && bw > R.hysteresis * weight(norms[0], order)) {
       stored = control = best;
-      for (size_t r = 0; r < pd.orders.size(); ++r) if (pd.orders[r] == best) cnorm = norms[r];
+      for (int r = 0; r < pd.n_orders; ++r) if (pd.orders[r] == best) cnorm = norms[r];
     }
   }
   S->order = stored;
@@ -1519,6 +1530,9 @@ struct sp_scan {
   double* h_norms = nullptr;
   int *h_flag_start = nullptr, *h_flag_att = nullptr, *h_flag_accept = nullptr;
   int64_t batch_steps = 0;
+  // host time per batch step, summed over the steps: the runs' preparation before the
+  // attempt phase, the wait for it, and the decisions after it (ms)
+  double host_prepare_ms = 0, host_wait_ms = 0, host_decide_ms = 0;
   // the attempt phase (uploads, predictor, source, corrector, norms read-back) as one
   // CUDA graph, captured at the first attempt and replayed at every later one
   cudaGraphExec_t attempt_graph = nullptr;
@@ -1724,6 +1738,8 @@ void scan_step(sp_scan* S) {
     }
   }
   // phase B: one attempt for every unfinished run (the runs' host work on the pool)
+  using clock = std::chrono::steady_clock;
+  const auto t_prepare = clock::now();
   S->pool->run(R, [&](int r) {
     S->h_flag_att[r] = 0;
     if (S->done[r]) return;
@@ -1760,9 +1776,11 @@ void scan_step(sp_scan* S) {
       cudaGetLastError();
     }
   }
+  const auto t_launch = clock::now();
   if (S->attempt_graph) CUDA_CHECK(cudaGraphLaunch(S->attempt_graph, S->stream));
   else scan_attempt_launches(S);
   CUDA_CHECK(cudaStreamSynchronize(S->stream));
+  const auto t_decide = clock::now();
   for (int r = 0; r < R; ++r)
     if (S->h_flag_att[r]) check_column(S->h_norms + 8 * r, S->norms.p + 8 * r, S->stream);
   S->pool->run(R, [&](int r) {
@@ -1778,6 +1796,13 @@ void scan_step(sp_scan* S) {
   });
   upload_all(S->flag_accept, S->h_flag_accept, R, S->stream);
   CUDA_CHECK(launch_step_b(2, S->step_att.p, S->step_items.p, S->flag_accept.p, S->n_step_items, R, S->stream));
+  const auto t_end = clock::now();
+  auto ms = [](clock::time_point a, clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+  };
+  S->host_prepare_ms += ms(t_prepare, t_launch);
+  S->host_wait_ms += ms(t_launch, t_decide);
+  S->host_decide_ms += ms(t_decide, t_end);
   for (int r = 0; r < R; ++r) {
     sp_session* ss = S->ss[r].get();
     if (!S->done[r] && reached(ss->z, ss->run.z_end)) {
@@ -2021,6 +2046,13 @@ size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
     char line[256];
     std::snprintf(line, sizeof line, "column: %s (tile-parallel %.4f ms, sweep %.4f ms)\n",
                   S->column_sweep ? "sweep" : "tile-parallel", S->column_tile_ms, S->column_sweep_ms);
+    text += line;
+    const double steps = (double)std::max<int64_t>(S->batch_steps, 1);
+    std::snprintf(line, sizeof line,
+                  "host per batch step: prepare %.4f ms, attempt phase (launch to its end) %.4f ms, "
+                  "decide %.4f ms, on %d threads\n",
+                  S->host_prepare_ms / steps, S->host_wait_ms / steps, S->host_decide_ms / steps,
+                  S->pool ? S->pool->threads() : 1);
     text += line;
     for (const auto& c : S->classes) {
       std::snprintf(line, sizeof line,

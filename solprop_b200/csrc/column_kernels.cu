@@ -341,6 +341,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   R F[kPer], J[kPer];
 #pragma unroll
   for (int j = 0; j < kPer; ++j) F[j] = J[j] = R(0);
+  bool quiet = true;  // this node carries no current on the window (warp-uniform)
   if (plasma) {
     const int first = (int)(2 * epoch + 1);
     const R dt = R(a.dt);
@@ -434,6 +435,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       await_predecessors(a, group, tile, first + 1);
       off1 = live ? predecessors(a.sums1, node, a.n_tiles, tile, lane) : 0.0;
     }
+    quiet = dark && still && off1 == 0.0;
     if (still) {
 #pragma unroll
       for (int j = 0; j < kPer; ++j) J[j] = R(off1);
@@ -471,7 +473,9 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       streams[(2 * kGroup + warp) * kPitch + pad(u)] = z;
     }
   }
-  __syncthreads();
+  // Ahead of the pulse no node of the group carries a current: the two current streams
+  // are zeros of either sign, whose projections are +0, written without the products.
+  const bool currents = __syncthreads_or(!quiet) != 0;
   // projection of the owned samples onto the modes: thread u takes window sample u of
   // every stream and mode, the group's nodes summed in order
   static_assert(kThreads == kWindow, "one thread per window sample");
@@ -488,7 +492,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
     for (int s = 0; s < 3; ++s)
 #pragma unroll
       for (int w = 0; w < kGroup; ++w)
-        v[s][w] = s < n_streams ? streams[(s * kGroup + w) * kPitch + pad(u)] : R(0);
+        v[s][w] = s < n_streams && (s == 0 || currents) ? streams[(s * kGroup + w) * kPitch + pad(u)] : R(0);
     R* out = base + group * row_of_group;
     const size_t stream_stride = (size_t)a.n_cols * a.n_to;
     for (int m = 0; m < a.n_modes; ++m) {
@@ -499,8 +503,10 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       for (int s = 0; s < 3; ++s) {
         if (s < n_streams) {
           R acc = R(0);
+          if (s == 0 || currents) {
 #pragma unroll
-          for (int w = 0; w < kGroup; ++w) acc += c[w] * v[s][w];
+            for (int w = 0; w < kGroup; ++w) acc += c[w] * v[s][w];
+          }
           out[s * stream_stride + (size_t)m * a.n_to] = acc;
         }
       }

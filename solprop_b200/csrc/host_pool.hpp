@@ -1,10 +1,13 @@
 // A small persistent pool of host threads for the scan's per-run host work (the Adams
 // stencil and tables before an attempt, the acceptance and step choice after it).  The
 // runs are independent, so the pool hands them out one at a time from an atomic counter;
-// the calling thread works too.  An exception thrown by a task is caught and the first one
-// is rethrown on the caller once every task has finished.
+// the calling thread works too.  Waiting threads spin for a short while before they sleep,
+// since the pool is asked for work every few milliseconds and a sleeping thread takes tens
+// of microseconds to wake.  An exception thrown by a task is caught and the first one is
+// rethrown on the caller once every task has finished.
 #pragma once
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <exception>
 #include <functional>
@@ -25,7 +28,7 @@ class HostPool {
   ~HostPool() {
     {
       std::lock_guard<std::mutex> lock(mutex_);
-      stop_ = true;
+      stop_.store(true);
     }
     wake_.notify_all();
     for (auto& t : workers_) t.join();
@@ -45,19 +48,42 @@ class HostPool {
       body_ = &body;
       count_ = count;
       next_.store(0);
-      busy_ = (int)workers_.size();
+      busy_.store((int)workers_.size());
       error_ = nullptr;
-      ++generation_;
+      generation_.fetch_add(1);
     }
     wake_.notify_all();
     drain();
-    std::unique_lock<std::mutex> lock(mutex_);
-    done_.wait(lock, [this] { return busy_ == 0; });
+    if (!spin([&] { return busy_.load(std::memory_order_acquire) == 0; })) {
+      std::unique_lock<std::mutex> lock(mutex_);
+      done_.wait(lock, [&] { return busy_.load() == 0; });
+    }
     body_ = nullptr;
     if (error_) std::rethrow_exception(error_);
   }
 
  private:
+  static constexpr std::chrono::microseconds kSpin{200};
+
+  static void relax() {
+#if defined(__x86_64__) || defined(__i386__)
+    __builtin_ia32_pause();
+#else
+    std::this_thread::yield();
+#endif
+  }
+
+  // true once ready() holds, false if it still does not after kSpin
+  template <class F>
+  static bool spin(F&& ready) {
+    const auto until = std::chrono::steady_clock::now() + kSpin;
+    for (int i = 0;; ++i) {
+      if (ready()) return true;
+      relax();
+      if ((i & 63) == 63 && std::chrono::steady_clock::now() > until) return ready();
+    }
+  }
+
   void drain() {
     for (int i = next_.fetch_add(1); i < count_; i = next_.fetch_add(1)) {
       try {
@@ -72,16 +98,17 @@ class HostPool {
   void work() {
     unsigned long long seen = 0;
     for (;;) {
-      {
+      auto posted = [&] { return stop_.load() || generation_.load(std::memory_order_acquire) != seen; };
+      if (!spin(posted)) {
         std::unique_lock<std::mutex> lock(mutex_);
-        wake_.wait(lock, [&] { return stop_ || generation_ != seen; });
-        if (stop_) return;
-        seen = generation_;
+        wake_.wait(lock, posted);
       }
+      if (stop_.load()) return;
+      seen = generation_.load(std::memory_order_acquire);
       drain();
-      {
+      if (busy_.fetch_sub(1, std::memory_order_acq_rel) == 1) {
         std::lock_guard<std::mutex> lock(mutex_);
-        if (--busy_ == 0) done_.notify_one();
+        done_.notify_one();
       }
     }
   }
@@ -90,10 +117,10 @@ class HostPool {
   std::mutex mutex_;
   std::condition_variable wake_, done_;
   const std::function<void(int)>* body_ = nullptr;
-  int count_ = 0, busy_ = 0;
-  std::atomic<int> next_{0};
-  unsigned long long generation_ = 0;
-  bool stop_ = false;
+  int count_ = 0;
+  std::atomic<int> next_{0}, busy_{0};
+  std::atomic<unsigned long long> generation_{0};
+  std::atomic<bool> stop_{false};
   std::exception_ptr error_;
 };
 
