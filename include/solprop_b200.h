@@ -212,8 +212,9 @@ sp_status sp_scan_run(sp_scan* scan, int32_t run, double* state, sp_batch* info)
 void* sp_scan_stream(sp_scan* scan);
 /* The scan's plan, as text: whether the attempt phase runs as one captured CUDA graph,
  * the response column's form, the host's time per batch step so far, and per grid size
- * whether the inverse and forward transforms run in one CTA per row or over a cluster,
- * with the autotuner's timings (ms per launch; -1 where a form was not a candidate).
+ * whether the inverse and forward transforms run in one CTA per row or over a cluster of
+ * 2, 4 or 8 CTAs, with the autotuner's timings (ms per launch; -1 where a form was not a
+ * candidate).
  * Returns the text's length. */
 size_t sp_scan_describe(const sp_scan* scan, char* buf, size_t len);
 /* The response column's form in a scan.  The scan's autotuner times both at creation
@@ -225,6 +226,12 @@ size_t sp_scan_describe(const sp_scan* scan, char* buf, size_t len);
 #define SP_SCAN_COLUMN_TILES 1
 #define SP_SCAN_COLUMN_SWEEP 2
 sp_status sp_scan_set_column(sp_scan* scan, int32_t form);
+/* The transforms' forms for the runs of one grid size: 0 for one CTA per row, or a
+ * cluster of 2, 4 or 8 CTAs per row.  The autotuner's choice stands otherwise; fixing the
+ * forms makes two scans of the same runs give the same bits.  SP_ERR_ARGUMENT when no run
+ * has that grid size or a row does not fit the form.  No counterpart in the reference. */
+sp_status sp_scan_set_transforms(sp_scan* scan, int32_t n_to, int32_t inverse_cluster,
+                                 int32_t forward_cluster);
 sp_status sp_scan_destroy(sp_scan* scan);
 
 /* ---- the scan surrogate's multilayer perceptron (no counterpart in the reference) ----

@@ -134,6 +134,7 @@ SIGNATURES = {
     "sp_scan_advance": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SpScanStatus)]),
     "sp_scan_describe": (C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "sp_scan_set_column": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sp_scan_set_transforms": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "sp_scan_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(SpBatch)]),
     "sp_scan_stream": (C.c_void_p, [C.c_void_p]),
     "sp_scan_destroy": (C.c_int, [C.c_void_p]),
@@ -495,6 +496,11 @@ class Scan:
         if form not in self.COLUMN_FORMS:
             raise ValueError(f"column form {form!r}: expected one of {sorted(self.COLUMN_FORMS)}")
         check(library().sp_scan_set_column(self.handle, self.COLUMN_FORMS[form]))
+
+    def set_transforms(self, n_to: int, inverse: int, forward: int) -> None:
+        """Fix the transforms' forms for the runs with ``n_to`` fine samples: 0 for one CTA
+        per row, or a cluster of 2, 4 or 8 CTAs."""
+        check(library().sp_scan_set_transforms(self.handle, int(n_to), int(inverse), int(forward)))
 
     def advance(self, steps: int = 1) -> SpScanStatus:
         check(library().sp_scan_advance(self.handle, int(steps), C.byref(self.status)))

@@ -1467,11 +1467,16 @@ sp_status sp_session_timing(sp_session* S, double* ms, int64_t* launches, int re
 // read-back of all runs' norms, the host's decisions, and a batched accept.
 namespace {
 
+// a transform's forms: one CTA per row (width 0), or a cluster of 2, 4 or 8 CTAs per row
+constexpr int kForms = 4;
+constexpr int kFormWidth[kForms] = {0, 2, 4, 8};
+
 struct FftClass {
   int n_to = 0;
-  bool cluster_inv = false, cluster_fwd = false;
-  // the autotuner's measurements (ms per launch over this class's rows; < 0: not a candidate)
-  float inv_single_ms = -1, inv_cluster_ms = -1, fwd_single_ms = -1, fwd_cluster_ms = -1;
+  int inv_form = 0, fwd_form = 0;  // indices into kFormWidth
+  // the autotuner's measurements by form (ms per launch over this class's rows; < 0: not
+  // a candidate)
+  float inv_ms[kForms] = {-1, -1, -1, -1}, fwd_ms[kForms] = {-1, -1, -1, -1};
   DevBuf<int2> inv_items, fwd_items;
   int n_inv = 0, n_fwd = 0;
 };
@@ -1557,31 +1562,48 @@ void upload_all(DevBuf<T>& dev, const T* host, size_t n, cudaStream_t s) {
   CUDA_CHECK(cudaMemcpyAsync(dev.p, host, n * sizeof(T), cudaMemcpyHostToDevice, s));
 }
 
+// Which forms a class's rows may take: one CTA when the row fits its shared memory, a
+// cluster of C CTAs when the row is longer than 4096 real samples and a CTA's share fits.
+bool inverse_form_ok(int n_to, int form) {
+  const int C = kFormWidth[form];
+  if (!C) return (size_t)(n_to / 2) * 16 <= kBatchedRowBytes;
+  return fft_cluster_size(n_to) > 1 && cluster_transform_smem(n_to, C, 16, false) <= kClusterSmem;
+}
+bool forward_form_ok(int n_to, int form, size_t elem) {
+  const int C = kFormWidth[form];
+  if (!C) return (size_t)(n_to / 2) * elem <= kBatchedRowBytes;
+  return fft_cluster_size(n_to) > 1 && cluster_transform_smem(n_to, C, elem, true) <= kClusterSmem;
+}
+
+cudaError_t launch_inverse_form(const InverseArgs* inv, const FftClass& c, int form, const int* flags,
+                                cudaStream_t s) {
+  const int C = kFormWidth[form];
+  return C ? launch_inverse_cluster_b(inv, c.inv_items.p, flags, c.n_inv, c.n_to, C, s)
+           : launch_inverse_b(inv, c.inv_items.p, flags, c.n_inv, c.n_to, s);
+}
+template <class R>
+cudaError_t launch_forward_form(const ForwardArgsT<R>* fwd, const FftClass& c, int form, const int* flags,
+                                cudaStream_t s) {
+  const int C = kFormWidth[form];
+  return C ? launch_forward_cluster_b(fwd, c.fwd_items.p, flags, c.n_fwd, c.n_to, C, s)
+           : launch_forward_b(fwd, c.fwd_items.p, flags, c.n_fwd, c.n_to, s);
+}
+
 template <class R>
 void scan_transforms(sp_scan* S, const int* flags, const InverseArgs* inv, const ColumnArgsT<R>* col,
                      const ForwardArgsT<R>* fwd) {
-  for (auto& c : S->classes) {
-    if (c->cluster_inv)
-      CUDA_CHECK(launch_inverse_cluster_b(inv, c->inv_items.p, flags, c->n_inv, c->n_to, S->stream));
-    else
-      CUDA_CHECK(launch_inverse_b(inv, c->inv_items.p, flags, c->n_inv, c->n_to, S->stream));
-  }
+  for (auto& c : S->classes) CUDA_CHECK(launch_inverse_form(inv, *c, c->inv_form, flags, S->stream));
   if (S->column_sweep)
     CUDA_CHECK(launch_column_sweep_b(col, S->sweep_items.p, flags, S->n_sweep_items, S->stream));
   else
     CUDA_CHECK(launch_column_b(col, S->col_items.p, flags, S->n_col_items, S->stream));
-  for (auto& c : S->classes) {
-    if (c->cluster_fwd)
-      CUDA_CHECK(launch_forward_cluster_b(fwd, c->fwd_items.p, flags, c->n_fwd, c->n_to, S->stream));
-    else
-      CUDA_CHECK(launch_forward_b(fwd, c->fwd_items.p, flags, c->n_fwd, c->n_to, S->stream));
-  }
+  for (auto& c : S->classes) CUDA_CHECK(launch_forward_form(fwd, *c, c->fwd_form, flags, S->stream));
 }
 
-// The scan's autotuner: for every grid size whose rows fit in one CTA and may also be split
-// over a cluster, time both forms of the inverse and the forward transform on this scan's
-// own rows (one warm-up and three timed launches each, every run selected) and keep the
-// faster.  The launches write the workspaces' scratch rows only.
+// The scan's transform autotuner: for every grid size, time every form each transform may
+// take (one CTA per row; clusters of 2, 4 and 8 CTAs) on this scan's own rows (one warm-up
+// and three timed launches each, every run selected) and keep the fastest.  The launches
+// write the workspaces' scratch rows only.
 template <class R>
 void tune_transforms(sp_scan* S, const ForwardArgsT<R>* fwd) {
   std::vector<int> ones(S->R, 1);
@@ -1602,17 +1624,20 @@ void tune_transforms(sp_scan* S, const ForwardArgsT<R>* fwd) {
   };
   const size_t elem = sizeof(cplx<R>);
   for (auto& c : S->classes) {
-    if (fft_cluster_size(c->n_to) <= 1) continue;  // a single CTA is the only form
-    const InverseArgs* inv = S->inv_att.p;
-    if ((size_t)(c->n_to / 2) * 16 <= kBatchedRowBytes) {
-      c->inv_single_ms = time([&] { return launch_inverse_b(inv, c->inv_items.p, all.p, c->n_inv, c->n_to, S->stream); });
-      c->inv_cluster_ms = time([&] { return launch_inverse_cluster_b(inv, c->inv_items.p, all.p, c->n_inv, c->n_to, S->stream); });
-      c->cluster_inv = c->inv_cluster_ms < c->inv_single_ms;
+    int n_inv = 0, n_fwd = 0;
+    for (int f = 0; f < kForms; ++f) {
+      n_inv += inverse_form_ok(c->n_to, f);
+      n_fwd += forward_form_ok(c->n_to, f, elem);
     }
-    if ((size_t)(c->n_to / 2) * elem <= kBatchedRowBytes) {
-      c->fwd_single_ms = time([&] { return launch_forward_b(fwd, c->fwd_items.p, all.p, c->n_fwd, c->n_to, S->stream); });
-      c->fwd_cluster_ms = time([&] { return launch_forward_cluster_b(fwd, c->fwd_items.p, all.p, c->n_fwd, c->n_to, S->stream); });
-      c->cluster_fwd = c->fwd_cluster_ms < c->fwd_single_ms;
+    for (int f = 0; f < kForms && n_inv > 1; ++f) {
+      if (!inverse_form_ok(c->n_to, f)) continue;
+      c->inv_ms[f] = time([&] { return launch_inverse_form(S->inv_att.p, *c, f, all.p, S->stream); });
+      if (c->inv_ms[f] < c->inv_ms[c->inv_form]) c->inv_form = f;
+    }
+    for (int f = 0; f < kForms && n_fwd > 1; ++f) {
+      if (!forward_form_ok(c->n_to, f, elem)) continue;
+      c->fwd_ms[f] = time([&] { return launch_forward_form(fwd, *c, f, all.p, S->stream); });
+      if (c->fwd_ms[f] < c->fwd_ms[c->fwd_form]) c->fwd_form = f;
     }
   }
   cudaEventDestroy(e0);
@@ -1635,12 +1660,7 @@ void tune_column(sp_scan* S, const ColumnArgsT<R>* col) {
   std::memset(unit.data(), 0, sizeof(StageScalarsDev) * unit.size());
   for (auto& u : unit) u.taper = 1.0;
   upload_all(S->stages_start, unit.data(), S->R, S->stream);
-  for (auto& c : S->classes) {
-    if (c->cluster_inv)
-      CUDA_CHECK(launch_inverse_cluster_b(S->inv_start.p, c->inv_items.p, all.p, c->n_inv, c->n_to, S->stream));
-    else
-      CUDA_CHECK(launch_inverse_b(S->inv_start.p, c->inv_items.p, all.p, c->n_inv, c->n_to, S->stream));
-  }
+  for (auto& c : S->classes) CUDA_CHECK(launch_inverse_form(S->inv_start.p, *c, c->inv_form, all.p, S->stream));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
@@ -1928,14 +1948,12 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     for (int n_to : sizes) {
       auto c = std::make_unique<FftClass>();
       c->n_to = n_to;
-      // A row that fits in one CTA's shared memory may be transformed there or over a
-      // cluster; the autotuner (tune_transforms) times both and keeps the faster.  Rows
-      // that do not fit take the cluster.  (The inverse transform is FP64 in both
-      // precisions.)
-      const size_t fwd_bytes = (size_t)(n_to / 2) * (precision == SP_PRECISION_MIXED ? 8 : 16);
-      const size_t inv_bytes = (size_t)(n_to / 2) * 16;
-      c->cluster_inv = fft_cluster_size(n_to) > 1 && inv_bytes > kBatchedRowBytes;
-      c->cluster_fwd = fft_cluster_size(n_to) > 1 && fwd_bytes > kBatchedRowBytes;
+      // Until the autotuner (tune_transforms) has timed the forms, a row takes the first
+      // that holds it: one CTA, else the narrowest cluster.  (The inverse transform is FP64
+      // in both precisions.)
+      const size_t elem = precision == SP_PRECISION_MIXED ? 8 : 16;
+      while (c->inv_form + 1 < kForms && !inverse_form_ok(n_to, c->inv_form)) ++c->inv_form;
+      while (c->fwd_form + 1 < kForms && !forward_form_ok(n_to, c->fwd_form, elem)) ++c->fwd_form;
       std::vector<int2> inv, fwd;
       for (int r = 0; r < R; ++r) {
         sp_workspace* w = S->ws[r].get();
@@ -2043,7 +2061,7 @@ size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
     text += S->attempt_graph ? "attempt phase: one CUDA graph\n"
                              : (S->graph_failed ? "attempt phase: plain launches (capture failed)\n"
                                                 : "attempt phase: not yet captured\n");
-    char line[256];
+    char line[512];
     std::snprintf(line, sizeof line, "column: %s (tile-parallel %.4f ms, sweep %.4f ms)\n",
                   S->column_sweep ? "sweep" : "tile-parallel", S->column_tile_ms, S->column_sweep_ms);
     text += line;
@@ -2054,13 +2072,16 @@ size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
                   S->host_prepare_ms / steps, S->host_wait_ms / steps, S->host_decide_ms / steps,
                   S->pool ? S->pool->threads() : 1);
     text += line;
+    auto form = [](int f) -> std::string {
+      return kFormWidth[f] ? "cluster" + std::to_string(kFormWidth[f]) : std::string("single");
+    };
     for (const auto& c : S->classes) {
       std::snprintf(line, sizeof line,
-                    "n_to %d: inverse %s (single %.4f ms, cluster %.4f ms), forward %s "
-                    "(single %.4f ms, cluster %.4f ms)\n",
-                    c->n_to, c->cluster_inv ? "cluster" : "single", c->inv_single_ms,
-                    c->inv_cluster_ms, c->cluster_fwd ? "cluster" : "single", c->fwd_single_ms,
-                    c->fwd_cluster_ms);
+                    "n_to %d: inverse %s (single %.4f, cluster2 %.4f, cluster4 %.4f, cluster8 %.4f ms), "
+                    "forward %s (single %.4f, cluster2 %.4f, cluster4 %.4f, cluster8 %.4f ms)\n",
+                    c->n_to, form(c->inv_form).c_str(), c->inv_ms[0], c->inv_ms[1], c->inv_ms[2],
+                    c->inv_ms[3], form(c->fwd_form).c_str(), c->fwd_ms[0], c->fwd_ms[1], c->fwd_ms[2],
+                    c->fwd_ms[3]);
       text += line;
     }
   }
@@ -2080,6 +2101,35 @@ sp_status sp_scan_set_column(sp_scan* S, int32_t form) {
     CUDA_CHECK(cudaSetDevice(S->device));
     CUDA_CHECK(cudaStreamSynchronize(S->stream));
     set_column_form(S, form == SP_SCAN_COLUMN_SWEEP);
+  });
+}
+
+sp_status sp_scan_set_transforms(sp_scan* S, int32_t n_to, int32_t inverse_cluster,
+                                 int32_t forward_cluster) {
+  return guarded([&] {
+    if (!S) throw Failure(SP_ERR_ARGUMENT, "NULL scan");
+    auto form_of = [](int32_t width) {
+      for (int f = 0; f < kForms; ++f)
+        if (kFormWidth[f] == width) return f;
+      throw Failure(SP_ERR_ARGUMENT, "a transform's cluster width is 0 (one CTA), 2, 4 or 8");
+    };
+    const int fi = form_of(inverse_cluster), ff = form_of(forward_cluster);
+    const size_t elem = S->precision == SP_PRECISION_MIXED ? 8 : 16;
+    for (auto& c : S->classes) {
+      if (c->n_to != n_to) continue;
+      if (!inverse_form_ok(n_to, fi) || !forward_form_ok(n_to, ff, elem))
+        throw Failure(SP_ERR_ARGUMENT, "that transform form does not hold this grid's rows");
+      CUDA_CHECK(cudaSetDevice(S->device));
+      CUDA_CHECK(cudaStreamSynchronize(S->stream));
+      c->inv_form = fi;
+      c->fwd_form = ff;
+      if (S->attempt_graph) {
+        CUDA_CHECK(cudaGraphExecDestroy(S->attempt_graph));
+        S->attempt_graph = nullptr;
+      }
+      return;
+    }
+    throw Failure(SP_ERR_ARGUMENT, "no run of the scan has that grid size");
   });
 }
 

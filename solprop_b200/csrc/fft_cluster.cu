@@ -68,12 +68,12 @@ __device__ __forceinline__ void cross_dft(cg::cluster_group& cluster, Cx* sc, in
 
 }  // namespace
 
-// inverse (c2r): coarse spectrum -> modal field (and the absorber's stream)
-template <class R>
+// inverse (c2r): coarse spectrum -> modal field (and the absorber's stream), over a
+// cluster of C CTAs
+template <int C, class R>
 __device__ __forceinline__ void inverse_cluster_body(const InverseArgsT<R>& a, int col) {
   using Cx = cplx<R>;
   cg::cluster_group cluster = cg::this_cluster();
-  const int C = (int)cluster.num_blocks();
   const int r = (int)cluster.block_rank();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx* sc = reinterpret_cast<Cx*>(smem_raw);
@@ -114,10 +114,10 @@ __device__ __forceinline__ void inverse_cluster_body(const InverseArgsT<R>& a, i
   R* absorb = a.absorber_stream ? a.absorber_stream + (size_t)col * a.n_to : nullptr;
   for (int kk = threadIdx.x; kk < slice; kk += blockDim.x) {
     const int k1 = r * slice + kk;
-    Cx z[kFftCluster];
-    cross_dft<kFftCluster>(cluster, sc, k1, log_mp, tw, a.log_m, true, z);
+    Cx z[C];
+    cross_dft<C>(cluster, sc, k1, log_mp, tw, a.log_m, true, z);
 #pragma unroll
-    for (int k2 = 0; k2 < kFftCluster; ++k2) {
+    for (int k2 = 0; k2 < C; ++k2) {
       const int m = k1 + Mp * k2;
       Cx v;
       v.x = z[k2].x * inv_m;
@@ -137,24 +137,23 @@ __device__ __forceinline__ void inverse_cluster_body(const InverseArgsT<R>& a, i
 
 template <class R>
 __global__ void __launch_bounds__(512) k_inverse_cluster(InverseArgsT<R> a) {
-  inverse_cluster_body(a, blockIdx.y);
+  inverse_cluster_body<kFftCluster>(a, blockIdx.y);
 }
 
 // batched: items[blockIdx.y] = (run, column)
-template <class R>
+template <class R, int C>
 __global__ void __launch_bounds__(512) k_inverse_cluster_b(const InverseArgsT<R>* args, const int2* items,
                                                           const int* flags) {
   const int2 it = items[blockIdx.y];
   if (!flags[it.x]) return;  // uniform over the cluster: every CTA of it has this item
-  inverse_cluster_body(own_args(args, it.x), it.y);
+  inverse_cluster_body<C>(own_args(args, it.x), it.y);
 }
 
-// forward (r2c): stream rows -> cropped coarse spectra
-template <class R>
+// forward (r2c): stream rows -> cropped coarse spectra, over a cluster of C CTAs
+template <int C, class R>
 __device__ __forceinline__ void forward_cluster_body(const ForwardArgsT<R>& a, int row_index) {
   using Cx = cplx<R>;
   cg::cluster_group cluster = cg::this_cluster();
-  const int C = (int)cluster.num_blocks();
   const int r = (int)cluster.block_rank();
   const int row = a.rows[row_index];
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -187,10 +186,10 @@ __device__ __forceinline__ void forward_cluster_body(const ForwardArgsT<R>& a, i
   cluster.sync();
   for (int kk = threadIdx.x; kk < slice; kk += blockDim.x) {
     const int k1 = r * slice + kk;
-    Cx z[kFftCluster];
-    cross_dft<kFftCluster>(cluster, sc, k1, log_mp, a.twiddles, a.log_m, false, z);
+    Cx z[C];
+    cross_dft<C>(cluster, sc, k1, log_mp, a.twiddles, a.log_m, false, z);
 #pragma unroll
-    for (int k2 = 0; k2 < kFftCluster; ++k2) zb[k2 * slice + kk] = z[k2];
+    for (int k2 = 0; k2 < C; ++k2) zb[k2 * slice + kk] = z[k2];
   }
   cluster.sync();
   // X[k] = E[k] + w^k O[k] from Z[k] and Z[M - k] (Z[M] = Z[0]); bins strided by rank
@@ -223,16 +222,16 @@ __device__ __forceinline__ void forward_cluster_body(const ForwardArgsT<R>& a, i
 
 template <class R>
 __global__ void __launch_bounds__(512) k_forward_cluster(ForwardArgsT<R> a) {
-  forward_cluster_body(a, blockIdx.y);
+  forward_cluster_body<kFftCluster>(a, blockIdx.y);
 }
 
 // batched: items[blockIdx.y] = (run, row index)
-template <class R>
+template <class R, int C>
 __global__ void __launch_bounds__(512) k_forward_cluster_b(const ForwardArgsT<R>* args, const int2* items,
                                                           const int* flags) {
   const int2 it = items[blockIdx.y];
   if (!flags[it.x]) return;
-  forward_cluster_body(own_args(args, it.x), it.y);
+  forward_cluster_body<C>(own_args(args, it.x), it.y);
 }
 
 static cudaError_t launch_cluster(const void* kernel, dim3 grid, int threads, size_t shm, int C,
@@ -279,46 +278,77 @@ cudaError_t launch_forward_cluster(const ForwardArgsT<R>& a, int n_rows, cudaStr
 }
 
 template <class R>
+static const void* inverse_cluster_kernel(int C) {
+  switch (C) {
+    case 2: return (const void*)k_inverse_cluster_b<R, 2>;
+    case 4: return (const void*)k_inverse_cluster_b<R, 4>;
+    case 8: return (const void*)k_inverse_cluster_b<R, 8>;
+    default: return nullptr;
+  }
+}
+template <class R>
+static const void* forward_cluster_kernel(int C) {
+  switch (C) {
+    case 2: return (const void*)k_forward_cluster_b<R, 2>;
+    case 4: return (const void*)k_forward_cluster_b<R, 4>;
+    case 8: return (const void*)k_forward_cluster_b<R, 8>;
+    default: return nullptr;
+  }
+}
+
+size_t cluster_transform_smem(int n_to, int C, size_t complex_bytes, bool forward) {
+  return (size_t)(forward ? 2 : 1) * (size_t)(n_to / 2 / C) * complex_bytes;
+}
+
+template <class R>
 cudaError_t launch_inverse_cluster_b(const InverseArgsT<R>* args, const int2* items, const int* flags,
-                                     int n_items, int n_to, cudaStream_t stream) {
-  const int C = fft_cluster_size(n_to);
+                                     int n_items, int n_to, int C, cudaStream_t stream) {
+  const void* kernel = inverse_cluster_kernel<R>(C);
+  if (!kernel) return cudaErrorInvalidValue;
   const int Mp = (n_to / 2) / C;
   void* params[] = {(void*)&args, (void*)&items, (void*)&flags};
-  return launch_cluster((const void*)k_inverse_cluster_b<R>, dim3(C, n_items), Mp >= 512 ? 512 : Mp,
-                        (size_t)Mp * sizeof(cplx<R>), C, stream, params);
+  return launch_cluster(kernel, dim3(C, n_items), Mp >= 512 ? 512 : Mp,
+                        cluster_transform_smem(n_to, C, sizeof(cplx<R>), false), C, stream, params);
 }
 
 template <class R>
 cudaError_t launch_forward_cluster_b(const ForwardArgsT<R>* args, const int2* items, const int* flags,
-                                     int n_items, int n_to, cudaStream_t stream) {
-  const int C = fft_cluster_size(n_to);
+                                     int n_items, int n_to, int C, cudaStream_t stream) {
+  const void* kernel = forward_cluster_kernel<R>(C);
+  if (!kernel) return cudaErrorInvalidValue;
   const int Mp = (n_to / 2) / C;
   void* params[] = {(void*)&args, (void*)&items, (void*)&flags};
-  return launch_cluster((const void*)k_forward_cluster_b<R>, dim3(C, n_items), Mp >= 512 ? 512 : Mp,
-                        (size_t)2 * Mp * sizeof(cplx<R>), C, stream, params);
+  return launch_cluster(kernel, dim3(C, n_items), Mp >= 512 ? 512 : Mp,
+                        cluster_transform_smem(n_to, C, sizeof(cplx<R>), true), C, stream, params);
 }
 
 #define SP_CLUSTER_INSTANCES(R)                                                                      \
   template cudaError_t launch_inverse_cluster<R>(const InverseArgsT<R>&, int, cudaStream_t);         \
   template cudaError_t launch_forward_cluster<R>(const ForwardArgsT<R>&, int, cudaStream_t);         \
   template cudaError_t launch_inverse_cluster_b<R>(const InverseArgsT<R>*, const int2*, const int*, \
-                                                   int, int, cudaStream_t);                          \
+                                                   int, int, int, cudaStream_t);                     \
   template cudaError_t launch_forward_cluster_b<R>(const ForwardArgsT<R>*, const int2*, const int*, \
-                                                   int, int, cudaStream_t);
+                                                   int, int, int, cudaStream_t);
 SP_CLUSTER_INSTANCES(double)
 SP_CLUSTER_INSTANCES(float)
 #undef SP_CLUSTER_INSTANCES
 
 cudaError_t configure_cluster_fft() {
-  // rows of up to 2^15 real samples: 2048 complex points per CTA, two buffers forward
-  const int shm = 2 * 2048 * (int)sizeof(double2);
-  const void* kernels[8] = {(const void*)k_inverse_cluster<double>, (const void*)k_forward_cluster<double>,
-                            (const void*)k_inverse_cluster_b<double>, (const void*)k_forward_cluster_b<double>,
-                            (const void*)k_inverse_cluster<float>, (const void*)k_forward_cluster<float>,
-                            (const void*)k_inverse_cluster_b<float>, (const void*)k_forward_cluster_b<float>};
-  for (const void* k : kernels) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
+  // the single-run kernels (eight CTAs): rows of up to 2^15 real samples, 2048 complex points
+  // per CTA, two buffers forward; the batched ones of every width: up to kClusterSmem
+  const int single = 2 * 2048 * (int)sizeof(double2);
+  const void* singles[4] = {(const void*)k_inverse_cluster<double>, (const void*)k_forward_cluster<double>,
+                            (const void*)k_inverse_cluster<float>, (const void*)k_forward_cluster<float>};
+  for (const void* k : singles) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, single);
     if (e != cudaSuccess) return e;
+  }
+  for (int C : {2, 4, 8}) {
+    for (const void* k : {inverse_cluster_kernel<double>(C), forward_cluster_kernel<double>(C),
+                          inverse_cluster_kernel<float>(C), forward_cluster_kernel<float>(C)}) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmem);
+      if (e != cudaSuccess) return e;
+    }
   }
   return cudaSuccess;
 }

@@ -174,12 +174,16 @@ cudaError_t launch_inverse_b(const InverseArgsT<R>* args, const int2* items, con
 template <class R>
 cudaError_t launch_forward_b(const ForwardArgsT<R>* args, const int2* items, const int* flags,
                              int n_items, int n_to, cudaStream_t stream);
+// batched transforms over clusters of C = 2, 4 or 8 CTAs (the scan's autotuner picks);
+// their dynamic shared memory (cluster_transform_smem) may be up to kClusterSmem
+constexpr size_t kClusterSmem = 200 * 1024;
+size_t cluster_transform_smem(int n_to, int C, size_t complex_bytes, bool forward);
 template <class R>
 cudaError_t launch_inverse_cluster_b(const InverseArgsT<R>* args, const int2* items, const int* flags,
-                                     int n_items, int n_to, cudaStream_t stream);
+                                     int n_items, int n_to, int C, cudaStream_t stream);
 template <class R>
 cudaError_t launch_forward_cluster_b(const ForwardArgsT<R>* args, const int2* items, const int* flags,
-                                     int n_items, int n_to, cudaStream_t stream);
+                                     int n_items, int n_to, int C, cudaStream_t stream);
 cudaError_t launch_output_b(const OutputArgs* args, const int2* items, const int* flags,
                             int n_items, cudaStream_t stream);
 template <class R>

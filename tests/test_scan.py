@@ -98,6 +98,8 @@ def test_column_forms_give_the_same_bits(precision):
     states = {}
     for form in ("tiles", "sweep"):
         sc = _lib.Scan([r for r, _ in built], [q for _, q in built], 0, precision)
+        for n_to in sorted({p.n_to for p in SMALL_SCAN}):  # the same transforms in both scans
+            sc.set_transforms(n_to, 0, 0)
         sc.set_column(form)
         sc.advance(8)
         states[form] = [sc.run(i)[0] for i in range(len(built))]
@@ -111,3 +113,27 @@ def test_unknown_column_form_is_refused():
 
     with pytest.raises(ValueError):
         object.__new__(_lib.Scan).set_column("rows")
+
+
+@pytest.mark.gpu
+def test_transform_forms_are_checked_and_all_agree():
+    """Every transform form a grid admits gives the same run to rounding; a form that does
+    not hold the rows, or a grid the scan does not have, is refused."""
+    from solprop_b200 import _lib
+
+    p = scan.ScanPoint(100e-6, 1.0, "Ar", 1.0, 40e-6, 20e-15, 2, 16384, 7)
+    rec, pol = scan.capillary_record(p)
+    states = []
+    for width in (0, 2, 4, 8):
+        sc = _lib.Scan([rec], [pol])
+        sc.set_transforms(16384, width, width)
+        sc.advance(6)
+        states.append(sc.run(0)[0])
+        sc.close()
+    for s in states[1:]:
+        assert rel(s, states[0]) < 1e-12
+    sc = _lib.Scan([rec], [pol])
+    with pytest.raises(_lib.NativeError):
+        sc.set_transforms(8192, 0, 0)
+    with pytest.raises(_lib.NativeError):
+        sc.set_transforms(16384, 3, 0)
