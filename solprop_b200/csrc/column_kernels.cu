@@ -43,16 +43,33 @@ constexpr size_t column_smem() {
   return sizeof(R) * ((size_t)3 * kGroup * kPitch + (size_t)kGroup * kPitch);
 }
 
-__device__ __forceinline__ double rate_of(const ColumnArgsT<double>& a, double magnitude) {
+// The rate table's scalars, read from the argument record once per tile into registers
+// (the record lives in shared memory, where every read after a shared store is a load).
+template <class R>
+struct RateLookup {
+  R field_min, field_max, rate_max, log_field_min, step;  // step: d log|E| (FP64), 1 / d (FP32)
+  const R* c;
+  int n;
+};
+__device__ __forceinline__ RateLookup<double> rate_lookup(const ColumnArgsT<double>& a) {
+  return {a.field_min, a.field_max, a.rate_max, a.log_field_min, a.d_log_field, a.rate_coefficients,
+          a.rate_intervals};
+}
+__device__ __forceinline__ RateLookup<float> rate_lookup(const ColumnArgsT<float>& a) {
+  return {(float)a.field_min, (float)a.field_max, (float)a.rate_max, (float)a.log_field_min,
+          (float)(1.0 / a.d_log_field), a.rate_coefficients, a.rate_intervals};
+}
+
+__device__ __forceinline__ double rate_of(const RateLookup<double>& a, double magnitude) {
   if (magnitude > a.field_max) return a.rate_max;
   if (!(magnitude >= a.field_min)) return 0.0;
   const double lf = log(magnitude);
-  long idx = (long)((lf - a.log_field_min) / a.d_log_field);
+  long idx = (long)((lf - a.log_field_min) / a.step);
   if (idx < 0) idx = 0;
-  if (idx > a.rate_intervals - 1) idx = a.rate_intervals - 1;
-  const double local = lf - (a.log_field_min + (double)idx * a.d_log_field);
-  const double* c = a.rate_coefficients;
-  const int n = a.rate_intervals;
+  if (idx > a.n - 1) idx = a.n - 1;
+  const double local = lf - (a.log_field_min + (double)idx * a.step);
+  const double* c = a.c;
+  const int n = a.n;
   return exp(((c[idx] * local + c[n + idx]) * local + c[2 * n + idx]) * local + c[3 * n + idx]);
 }
 
@@ -60,15 +77,15 @@ __device__ __forceinline__ double rate_of(const ColumnArgsT<double>& a, double m
 // knot being the field at the interval's start, so that W = exp(c3) exp(((c0 l + c1) l +
 // c2) l) with l = log1p(|E| / knot - 1): no large logarithm or exponent is rounded to
 // FP32, and the error of W is that of |E| times the rate's slope d log W / d log |E|.
-__device__ __forceinline__ float rate_of(const ColumnArgsT<float>& a, float magnitude) {
-  if (magnitude > (float)a.field_max) return (float)a.rate_max;
-  if (!(magnitude >= (float)a.field_min)) return 0.0f;
-  const int n = a.rate_intervals;
-  const float pos = (__logf(magnitude) - (float)a.log_field_min) * (float)(1.0 / a.d_log_field);
+__device__ __forceinline__ float rate_of(const RateLookup<float>& a, float magnitude) {
+  if (magnitude > a.field_max) return a.rate_max;
+  if (!(magnitude >= a.field_min)) return 0.0f;
+  const int n = a.n;
+  const float pos = (__logf(magnitude) - a.log_field_min) * a.step;
   int idx = (int)pos;
   if (idx < 0) idx = 0;
   if (idx > n - 1) idx = n - 1;
-  const float* c = a.rate_coefficients;
+  const float* c = a.c;
   // l = log1p(v), v = |E| / knot - 1: within an interval |v| is a few 1e-2 at most, where
   // the series to v^5 is as good as FP32 (its first omitted term, v^6 / 6, stays below
   // 6e-8 |v|)
@@ -294,26 +311,34 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   __shared__ __align__(16) R wt[kMaxModes * kGroup];
   __shared__ R gate[kPitch], gate_d[kPitch];  // the temporal window g and g' on the window (padded)
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  // the record's scalars this tile reads, into registers once
+  const int n_to = a.n_to, n_modes = a.n_modes, n_nodes = a.n_nodes, n_cols = a.n_cols;
   const int node = group * kGroup + warp;
-  const bool live = node < a.n_nodes;
+  const bool live = node < n_nodes;
   const int K = a.half_width, A = a.lead, owned = a.owned;
   const int t0 = tile * owned, tw = t0 - A;  // owned samples [t0, t0 + owned): window [A, A + owned)
-  const int own_hi = A + min(owned, a.n_to - t0);
+  const int own_hi = A + min(owned, n_to - t0);
   const StageScalarsDev& st = *a.stage;
   const R tau = R(st.taper);
   const bool plasma = a.plasma;
   // the modal window and the group's projection weights W[m, node] / tau
-  for (int i = threadIdx.x; i < a.n_modes * kWindow; i += blockDim.x) {
-    const int m = i / kWindow, u = i % kWindow, t = tw + u;
-    modal[m * kPitch + pad(u)] = (t >= 0 && t < a.n_to) ? R(a.modal_t[(size_t)m * a.n_to + t]) : R(0);
+  {
+    const double* modal_t = a.modal_t;
+    for (int i = threadIdx.x; i < n_modes * kWindow; i += blockDim.x) {
+      const int m = i / kWindow, u = i % kWindow, t = tw + u;
+      modal[m * kPitch + pad(u)] = (t >= 0 && t < n_to) ? R(modal_t[(size_t)m * n_to + t]) : R(0);
+    }
   }
-  for (int k = threadIdx.x; k < a.n_modes * kGroup; k += blockDim.x) {
-    const int m = k / kGroup, w = k % kGroup, nd = group * kGroup + w;
-    wt[k] = nd < a.n_nodes ? a.projection[m * a.n_nodes + nd] / tau : R(0);
+  if (!kSweep || tile == 0) {  // the weights do not change along a sweep
+    const R* projection = a.projection;
+    for (int k = threadIdx.x; k < n_modes * kGroup; k += blockDim.x) {
+      const int m = k / kGroup, w = k % kGroup, nd = group * kGroup + w;
+      wt[k] = nd < n_nodes ? projection[m * n_nodes + nd] / tau : R(0);
+    }
   }
   for (int u = threadIdx.x; u < kWindow; u += blockDim.x) {
     const int t = tw + u;
-    const bool in = t >= 0 && t < a.n_to;
+    const bool in = t >= 0 && t < n_to;
     gate[pad(u)] = in ? a.t_window[t] : R(0);
     gate_d[pad(u)] = in ? a.t_window_derivative[t] : R(0);
   }
@@ -322,22 +347,24 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   R E[kPer], W[kPer];
   {
     R srow[kMaxModes];
+    const R* synthesis = a.synthesis;
 #pragma unroll
     for (int m = 0; m < kMaxModes; ++m)
-      srow[m] = (live && m < a.n_modes) ? a.synthesis[node * a.n_modes + m] * tau : R(0);
+      srow[m] = (live && m < n_modes) ? synthesis[node * n_modes + m] * tau : R(0);
+    const RateLookup<R> rates = rate_lookup(a);
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
       const int u = kPer * lane + j, t = tw + u;
       R e = R(0);
 #pragma unroll
       for (int m = 0; m < kMaxModes; ++m)
-        if (m < a.n_modes) e += srow[m] * modal[m * kPitch + pad(u)];
+        if (m < n_modes) e += srow[m] * modal[m * kPitch + pad(u)];
       E[j] = e;
-      W[j] = (plasma && t >= 0 && t < a.n_to) ? rate_of(a, fabs(e)) : R(0);
+      W[j] = (plasma && t >= 0 && t < n_to) ? rate_of(rates, fabs(e)) : R(0);
     }
   }
   __syncthreads();  // the modal window's space becomes the streams'
-  const bool at_end = tw < 0 || tw + kWindow > a.n_to;  // block-uniform
+  const bool at_end = tw < 0 || tw + kWindow > n_to;  // block-uniform
   R F[kPer], J[kPer];
 #pragma unroll
   for (int j = 0; j < kPer; ++j) F[j] = J[j] = R(0);
@@ -366,12 +393,12 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
         R Wg[kPer];  // with the reflected ghosts, for the filter only
 #pragma unroll
         for (int j = 0; j < kPer; ++j) Wg[j] = W[j];
-        reflect_ends(Wg, row, tw, a.n_to, K, lane);
+        reflect_ends(Wg, row, tw, n_to, K, lane);
         band_filter(Wg, Wf, a.taps, K);
       } else {
         band_filter(W, Wf, a.taps, K);
       }
-      trapezoid(Wf, inc, dt, tw, A - K, A + owned + K, a.n_to, lane);
+      trapezoid(Wf, inc, dt, tw, A - K, A + owned + K, n_to, lane);
       s0 = owned_sum(inc, A, own_hi, lane);
     }
     double off0;
@@ -393,7 +420,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
 #pragma unroll
       for (int j = 0; j < kPer; ++j) {
         const int u = kPer * lane + j, t = tw + u;
-        const bool in = u >= A - K && u <= A + owned + K && t >= 0 && t < a.n_to;
+        const bool in = u >= A - K && u <= A + owned + K && t >= 0 && t < n_to;
         F[j] = in ? f_dark : R(0);
         g[j] = in ? f_dark * qm * E[j] : R(0);
       }
@@ -404,7 +431,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       for (int j = 0; j < kPer; ++j) {
         const int u = kPer * lane + j, t = tw + u;
         R f = R(0), gv = R(0);
-        if (u >= A - K && u <= A + owned + K && t >= 0 && t < a.n_to) {
+        if (u >= A - K && u <= A + owned + K && t >= 0 && t < n_to) {
           const R x = R(off0 + (P[j] - at_t0));
           f = fraction(f0, a.band ? fmax(x, R(0)) : x);
           gv = f * qm * E[j];
@@ -419,10 +446,10 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
     still = __all_sync(0xffffffffu, still);
     double s1 = 0.0;
     if (!still) {
-      if (at_end) reflect_ends(g, row, tw, a.n_to, K, lane);
+      if (at_end) reflect_ends(g, row, tw, n_to, K, lane);
       R gf[kPer];
       band_filter(g, gf, a.taps, K);
-      trapezoid(gf, inc, dt, tw, A, A + owned, a.n_to, lane);
+      trapezoid(gf, inc, dt, tw, A, A + owned, n_to, lane);
       s1 = owned_sum(inc, A, own_hi, lane);
     }
     double off1;
@@ -482,7 +509,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   const int n_streams = plasma ? 3 : 1;
   const int u = threadIdx.x;
   const bool mine = u >= A && u < own_hi;
-  const size_t row_of_group = (size_t)3 * a.n_cols * a.n_to;
+  const size_t row_of_group = (size_t)3 * n_cols * n_to;
   R* base = a.partials + (mine ? tw + u : 0);  // sample t = tw + u of row (group 3 + s) n_cols + m
   if (mine) {
     // the three streams' samples of the group's nodes, then mode by mode: the weights
@@ -494,8 +521,8 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       for (int w = 0; w < kGroup; ++w)
         v[s][w] = s < n_streams && (s == 0 || currents) ? streams[(s * kGroup + w) * kPitch + pad(u)] : R(0);
     R* out = base + group * row_of_group;
-    const size_t stream_stride = (size_t)a.n_cols * a.n_to;
-    for (int m = 0; m < a.n_modes; ++m) {
+    const size_t stream_stride = (size_t)n_cols * n_to;
+    for (int m = 0; m < n_modes; ++m) {
       R c[kGroup];
 #pragma unroll
       for (int w = 0; w < kGroup; ++w) c[w] = wt[m * kGroup + w];
@@ -507,7 +534,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
 #pragma unroll
             for (int w = 0; w < kGroup; ++w) acc += c[w] * v[s][w];
           }
-          out[s * stream_stride + (size_t)m * a.n_to] = acc;
+          out[s * stream_stride + (size_t)m * n_to] = acc;
         }
       }
     }
@@ -527,8 +554,8 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
     if (last && mine) {
       __threadfence();
       for (int s = 0; s < n_streams; ++s)
-        for (int m = 0; m < a.n_modes; ++m) {
-          R* out = base + ((size_t)s * a.n_cols + m) * a.n_to;
+        for (int m = 0; m < n_modes; ++m) {
+          R* out = base + ((size_t)s * n_cols + m) * n_to;
           R acc = R(0);
           for (int g = 0; g < a.n_groups; ++g) acc = acc + __ldcg(out + g * row_of_group);
           *out = acc;
