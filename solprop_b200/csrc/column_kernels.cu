@@ -42,6 +42,24 @@ template <class R>
 constexpr size_t column_smem() {
   return sizeof(R) * ((size_t)3 * kGroup * kPitch + (size_t)kGroup * kPitch);
 }
+// the sweep adds the next tile's modal window (FP64, as in global memory) and temporal
+// windows, copied in while the current tile is computed
+template <class R>
+constexpr size_t column_sweep_smem() {
+  return column_smem<R>() + sizeof(double) * (size_t)kMaxModes * kWindow + sizeof(R) * 2 * kWindow;
+}
+
+// asynchronous global -> shared copies of 4 or 8 bytes (zero-filled when !valid, which
+// reads nothing), their commit and the wait for all of this thread's copies
+template <int kBytes>
+__device__ __forceinline__ void copy_async(void* smem, const void* gmem, bool valid) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(gmem), "n"(kBytes),
+               "r"(valid ? kBytes : 0)
+               : "memory");
+}
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // The rate table's scalars, read from the argument record once per tile into registers
 // (the record lives in shared memory, where every read after a shared store is a load).
@@ -322,7 +340,15 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   const R tau = R(st.taper);
   const bool plasma = a.plasma;
   // the modal window and the group's projection weights W[m, node] / tau
-  {
+  // the sweep's copies of this tile's windows arrived during the last tile (the caller
+  // waited for them before its barrier)
+  double* next_modal = reinterpret_cast<double*>(column_raw + column_smem<R>());
+  R* next_gate = reinterpret_cast<R*>(next_modal + (size_t)kMaxModes * kWindow);
+  const bool copied = kSweep && tile > 0;
+  if (copied) {
+    for (int i = threadIdx.x; i < n_modes * kWindow; i += blockDim.x)
+      modal[(i / kWindow) * kPitch + pad(i % kWindow)] = R(next_modal[i]);
+  } else {
     const double* modal_t = a.modal_t;
     for (int i = threadIdx.x; i < n_modes * kWindow; i += blockDim.x) {
       const int m = i / kWindow, u = i % kWindow, t = tw + u;
@@ -337,12 +363,34 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
     }
   }
   for (int u = threadIdx.x; u < kWindow; u += blockDim.x) {
-    const int t = tw + u;
-    const bool in = t >= 0 && t < n_to;
-    gate[pad(u)] = in ? a.t_window[t] : R(0);
-    gate_d[pad(u)] = in ? a.t_window_derivative[t] : R(0);
+    if (copied) {
+      gate[pad(u)] = next_gate[u];
+      gate_d[pad(u)] = next_gate[kWindow + u];
+    } else {
+      const int t = tw + u;
+      const bool in = t >= 0 && t < n_to;
+      gate[pad(u)] = in ? a.t_window[t] : R(0);
+      gate_d[pad(u)] = in ? a.t_window_derivative[t] : R(0);
+    }
   }
   __syncthreads();
+  if (kSweep && tile + 1 < a.n_tiles) {
+    // the next tile's windows, copied while this one is computed
+    const int tn = tw + owned;  // the next window's first sample
+    const double* modal_t = a.modal_t;
+    for (int i = threadIdx.x; i < n_modes * kWindow; i += blockDim.x) {
+      const int m = i / kWindow, t = tn + i % kWindow;
+      const bool in = t >= 0 && t < n_to;
+      copy_async<8>(next_modal + i, modal_t + (size_t)m * n_to + (in ? t : 0), in);
+    }
+    for (int u = threadIdx.x; u < kWindow; u += blockDim.x) {
+      const int t = tn + u;
+      const bool in = t >= 0 && t < n_to;
+      copy_async<sizeof(R)>(next_gate + u, a.t_window + (in ? t : 0), in);
+      copy_async<sizeof(R)>(next_gate + kWindow + u, a.t_window_derivative + (in ? t : 0), in);
+    }
+    copy_async_commit();
+  }
   // synthesis and rate on the window
   R E[kPer], W[kPer];
   {
@@ -580,7 +628,10 @@ template <class R>
 __device__ __forceinline__ void column_sweep(const ColumnArgsT<R>& a, int group) {
   double carry0 = 0.0, carry1 = 0.0;
   for (int tile = 0; tile < a.n_tiles; ++tile) {
-    if (tile > 0) __syncthreads();  // the last tile's projection is done with the shared rows
+    if (tile > 0) {
+      copy_async_wait();  // this thread's copies of the tile's windows
+      __syncthreads();    // everyone's, and the last tile's projection is done with the rows
+    }
     column_tile<R, true>(a, tile, group, 0ull, carry0, carry1);
   }
 }
@@ -615,7 +666,7 @@ __global__ void __launch_bounds__(kThreads, column_residency<R>())
 template <class R>
 cudaError_t launch_column_sweep_b(const ColumnArgsT<R>* args, const int4* items, const int* flags,
                                   int n_items, cudaStream_t stream) {
-  k_column_sweep_b<R><<<n_items, kThreads, column_smem<R>(), stream>>>(args, items, flags);
+  k_column_sweep_b<R><<<n_items, kThreads, column_sweep_smem<R>(), stream>>>(args, items, flags);
   return cudaGetLastError();
 }
 
@@ -647,8 +698,8 @@ cudaError_t configure_column_kernels() {
   const void* kernels[6] = {(const void*)k_column<double>, (const void*)k_column_b<double>,
                             (const void*)k_column_sweep_b<double>, (const void*)k_column<float>,
                             (const void*)k_column_b<float>, (const void*)k_column_sweep_b<float>};
-  const size_t shm[6] = {column_smem<double>(), column_smem<double>(), column_smem<double>(),
-                         column_smem<float>(), column_smem<float>(), column_smem<float>()};
+  const size_t shm[6] = {column_smem<double>(), column_smem<double>(), column_sweep_smem<double>(),
+                         column_smem<float>(), column_smem<float>(), column_sweep_smem<float>()};
   for (int i = 0; i < 6; ++i) {
     cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shm[i]);
