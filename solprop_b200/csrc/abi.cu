@@ -1529,6 +1529,18 @@ struct sp_scan {
   std::vector<int> groups;  // node groups per run
   // host threads for the per-run work between the batched launches
   std::unique_ptr<HostPool> pool;
+  // the runs' work-list sizes, and the re-planning as runs finish: every batched launch
+  // covers the runs still going; when their number has halved since the last plan, the
+  // lists are rebuilt and the column's and transforms' forms tuned again
+  struct RunWork {
+    int n_to, step_blocks, out_blocks, col_blocks, groups, tiles, cols, fwd_rows;
+  };
+  std::vector<RunWork> work;
+  int planned_active = 0, replans = 0;
+  // the tail: once no more than kTailRuns runs are going, each goes on as a single run (its
+  // own stream, on a host thread of its own), one attempt per batch step
+  bool tail = false;
+  int64_t tail_from = -1;  // the batch step the tail began at
   std::vector<std::unique_ptr<FftClass>> classes;
   AdamsDev *h_adams_start = nullptr, *h_adams_att = nullptr;
   StageScalarsDev *h_stages_start = nullptr, *h_stages_att = nullptr;
@@ -1589,15 +1601,71 @@ cudaError_t launch_forward_form(const ForwardArgsT<R>* fwd, const FftClass& c, i
            : launch_forward_b(fwd, c.fwd_items.p, flags, c.n_fwd, c.n_to, s);
 }
 
+// a work list rewritten in place (the lists only shrink after the first plan)
+template <class T>
+void refill(DevBuf<T>& dev, const std::vector<T>& host, cudaStream_t s, bool first) {
+  if (first) {
+    dev.upload(host.data(), host.size(), s);
+    return;
+  }
+  if (host.size() > dev.n) throw Failure(SP_ERR_ARGUMENT, "a scan's work list grew after its first plan");
+  if (!host.empty())
+    CUDA_CHECK(cudaMemcpyAsync(dev.p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+// The batched launches' work lists for the runs with live[r] set: the stepping and output
+// blocks, both forms of the column (the sweep's longest rows first), and every grid
+// size's transform rows.
+void plan_items(sp_scan* S, const std::vector<int>& live, bool first) {
+  std::vector<int2> step, out;
+  std::vector<int4> col, sweep;
+  for (int r = 0; r < S->R; ++r) {
+    if (!live[r]) continue;
+    const auto& w = S->work[r];
+    for (int b = 0; b < w.step_blocks; ++b) step.push_back(make_int2(r, b));
+    for (int b = 0; b < w.out_blocks; ++b) out.push_back(make_int2(r, b));
+    for (int b = 0; b < w.col_blocks; ++b) col.push_back(make_int4(r, b, 0, 0));
+    for (int g = 0; g < w.groups; ++g) sweep.push_back(make_int4(r, g, 0, 0));
+  }
+  std::stable_sort(sweep.begin(), sweep.end(), [&](const int4& x, const int4& y) {
+    return S->work[x.x].tiles > S->work[y.x].tiles;
+  });
+  refill(S->step_items, step, S->stream, first);
+  refill(S->out_items, out, S->stream, first);
+  refill(S->col_items, col, S->stream, first);
+  refill(S->sweep_items, sweep, S->stream, first);
+  S->n_step_items = (int)step.size();
+  S->n_out_items = (int)out.size();
+  S->n_col_items = (int)col.size();
+  S->n_sweep_items = (int)sweep.size();
+  for (auto& c : S->classes) {
+    std::vector<int2> inv, fwd;
+    for (int r = 0; r < S->R; ++r) {
+      if (!live[r] || S->work[r].n_to != c->n_to) continue;
+      for (int k = 0; k < S->work[r].cols; ++k) inv.push_back(make_int2(r, k));
+      for (int k = 0; k < S->work[r].fwd_rows; ++k) fwd.push_back(make_int2(r, k));
+    }
+    refill(c->inv_items, inv, S->stream, first);
+    refill(c->fwd_items, fwd, S->stream, first);
+    c->n_inv = (int)inv.size();
+    c->n_fwd = (int)fwd.size();
+  }
+  int active = 0;
+  for (int r = 0; r < S->R; ++r) active += live[r] != 0;
+  S->planned_active = active;
+}
+
 template <class R>
 void scan_transforms(sp_scan* S, const int* flags, const InverseArgs* inv, const ColumnArgsT<R>* col,
                      const ForwardArgsT<R>* fwd) {
-  for (auto& c : S->classes) CUDA_CHECK(launch_inverse_form(inv, *c, c->inv_form, flags, S->stream));
+  for (auto& c : S->classes)
+    if (c->n_inv) CUDA_CHECK(launch_inverse_form(inv, *c, c->inv_form, flags, S->stream));
   if (S->column_sweep)
     CUDA_CHECK(launch_column_sweep_b(col, S->sweep_items.p, flags, S->n_sweep_items, S->stream));
   else
     CUDA_CHECK(launch_column_b(col, S->col_items.p, flags, S->n_col_items, S->stream));
-  for (auto& c : S->classes) CUDA_CHECK(launch_forward_form(fwd, *c, c->fwd_form, flags, S->stream));
+  for (auto& c : S->classes)
+    if (c->n_fwd) CUDA_CHECK(launch_forward_form(fwd, *c, c->fwd_form, flags, S->stream));
 }
 
 // The scan's transform autotuner: for every grid size, time every form each transform may
@@ -1605,10 +1673,9 @@ void scan_transforms(sp_scan* S, const int* flags, const InverseArgs* inv, const
 // and three timed launches each, every run selected) and keep the fastest.  The launches
 // write the workspaces' scratch rows only.
 template <class R>
-void tune_transforms(sp_scan* S, const ForwardArgsT<R>* fwd) {
-  std::vector<int> ones(S->R, 1);
+void tune_transforms(sp_scan* S, const ForwardArgsT<R>* fwd, const std::vector<int>& live) {
   DevBuf<int> all;
-  all.upload(ones.data(), ones.size(), S->stream);
+  all.upload(live.data(), live.size(), S->stream);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
@@ -1624,6 +1691,7 @@ void tune_transforms(sp_scan* S, const ForwardArgsT<R>* fwd) {
   };
   const size_t elem = sizeof(cplx<R>);
   for (auto& c : S->classes) {
+    if (!c->n_inv) continue;  // no run of this grid size is going
     int n_inv = 0, n_fwd = 0;
     for (int f = 0; f < kForms; ++f) {
       n_inv += inverse_form_ok(c->n_to, f);
@@ -1652,15 +1720,15 @@ void tune_transforms(sp_scan* S, const ForwardArgsT<R>* fwd) {
 // the tile-parallel form wins for a few long rows.  The stage records are a unit taper
 // with zero densities while timing, then put back.
 template <class R>
-void tune_column(sp_scan* S, const ColumnArgsT<R>* col) {
-  std::vector<int> ones(S->R, 1);
+void tune_column(sp_scan* S, const ColumnArgsT<R>* col, const std::vector<int>& live) {
   DevBuf<int> all;
-  all.upload(ones.data(), ones.size(), S->stream);
+  all.upload(live.data(), live.size(), S->stream);
   std::vector<StageScalarsDev> unit(S->R);
   std::memset(unit.data(), 0, sizeof(StageScalarsDev) * unit.size());
   for (auto& u : unit) u.taper = 1.0;
   upload_all(S->stages_start, unit.data(), S->R, S->stream);
-  for (auto& c : S->classes) CUDA_CHECK(launch_inverse_form(S->inv_start.p, *c, c->inv_form, all.p, S->stream));
+  for (auto& c : S->classes)
+    if (c->n_inv) CUDA_CHECK(launch_inverse_form(S->inv_start.p, *c, c->inv_form, all.p, S->stream));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CUDA_CHECK(cudaEventCreate(&e0));
   CUDA_CHECK(cudaEventCreate(&e1));
@@ -1726,7 +1794,72 @@ void scan_attempt_launches(sp_scan* S) {
                              S->stream));
 }
 
+constexpr int kTailRuns = 4;
+
+// the runs' host work: on the pool while many runs are going, on this thread for a few
+void for_runs(sp_scan* S, const std::function<void(int)>& body) {
+  if (S->planned_active >= 16) {
+    S->pool->run(S->R, body);
+  } else {
+    for (int r = 0; r < S->R; ++r) body(r);
+  }
+}
+
+// The runs still going have halved since the last plan: their work lists only, and the
+// column's and transforms' forms tuned again on them (few long rows favour the
+// tile-parallel column and wider transform clusters); the next attempt recaptures its graph.
+void replan(sp_scan* S) {
+  std::vector<int> live(S->R);
+  for (int r = 0; r < S->R; ++r) live[r] = !S->done[r];
+  CUDA_CHECK(cudaStreamSynchronize(S->stream));
+  plan_items(S, live, /*first=*/false);
+  if (S->precision == SP_PRECISION_MIXED) tune_column(S, S->col32_start.p, live);
+  else tune_column(S, S->col_start.p, live);
+  set_column_form(S, S->column_sweep);
+  if (S->precision == SP_PRECISION_MIXED) tune_transforms(S, S->fwd32.p, live);
+  else tune_transforms(S, S->fwd.p, live);
+  if (S->attempt_graph) {
+    CUDA_CHECK(cudaGraphExecDestroy(S->attempt_graph));
+    S->attempt_graph = nullptr;
+  }
+  S->replans += 1;
+}
+
+// One batch step of the tail: every run still going takes one attempt on the single-run
+// path, the runs side by side on the host pool (each on its workspace's stream).  A run
+// whose step control falls below its floor stops, as in a batched step; any other failure
+// propagates.
+void tail_step(sp_scan* S) {
+  std::vector<int> live;
+  for (int r = 0; r < S->R; ++r)
+    if (!S->done[r]) live.push_back(r);
+  auto body = [&](int k) {
+    const int r = live[k];
+    CUDA_CHECK(cudaSetDevice(S->device));
+    sp_session* ss = S->ss[r].get();
+    try {
+      adams_adaptive_attempt(ss, ss->run.z_end);
+    } catch (const Failure& f) {
+      if (f.code != SP_ERR_CONVERGENCE) throw;
+      ss->failed = true;
+      S->done[r] = 1;
+      return;
+    }
+    if (reached(ss->z, ss->run.z_end)) {
+      ss->finished = true;
+      S->done[r] = 1;
+    }
+  };
+  if (live.size() > 1) S->pool->run((int)live.size(), body);
+  else if (!live.empty()) body(0);
+}
+
 void scan_step(sp_scan* S) {
+  if (S->tail) {
+    tail_step(S);
+    S->batch_steps += 1;
+    return;
+  }
   const int R = S->R;
   // phase A: runs with an empty history take their startup sample
   int n_start = 0;
@@ -1760,7 +1893,7 @@ void scan_step(sp_scan* S) {
   // phase B: one attempt for every unfinished run (the runs' host work on the pool)
   using clock = std::chrono::steady_clock;
   const auto t_prepare = clock::now();
-  S->pool->run(R, [&](int r) {
+  for_runs(S, [&](int r) {
     S->h_flag_att[r] = 0;
     if (S->done[r]) return;
     sp_session* ss = S->ss[r].get();
@@ -1803,7 +1936,7 @@ void scan_step(sp_scan* S) {
   const auto t_decide = clock::now();
   for (int r = 0; r < R; ++r)
     if (S->h_flag_att[r]) check_column(S->h_norms + 8 * r, S->norms.p + 8 * r, S->stream);
-  S->pool->run(R, [&](int r) {
+  for_runs(S, [&](int r) {
     S->h_flag_accept[r] = 0;
     if (!S->h_flag_att[r]) return;
     sp_session* ss = S->ss[r].get();
@@ -1831,6 +1964,16 @@ void scan_step(sp_scan* S) {
     }
   }
   S->batch_steps += 1;
+  int active = 0;
+  for (int r = 0; r < R; ++r) active += !S->done[r];
+  if (S->R > kTailRuns && active > 0 && active <= kTailRuns) {
+    // the batched launches' fixed costs outweigh their work: the last runs go on alone
+    CUDA_CHECK(cudaStreamSynchronize(S->stream));
+    S->tail = true;
+    S->tail_from = S->batch_steps;
+  } else if (active > 0 && 2 * active <= S->planned_active) {
+    replan(S);
+  }
 }
 
 }  // namespace
@@ -1912,9 +2055,8 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     std::vector<ForwardArgsT<float>> fa32(R);
     std::vector<OutputArgs> os(R), oa(R);
     std::vector<StepArgs> ts(R), ta(R);
-    std::vector<int2> step_items, out_items;
-    std::vector<int4> col_items;
     std::vector<int> sizes;
+    S->work.resize(R);
     for (int r = 0; r < R; ++r) {
       sp_workspace* w = S->ws[r].get();
       const sp_problem& P = *w->P;
@@ -1938,10 +2080,8 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
       ta[r] = step_args_of(w, S->adams_att.p + r, S->stages_att.p + 2 * r);
       ts[r].n_blocks = ta[r].n_blocks = nb;
       ts[r].norms = ta[r].norms = S->norms.p + 8 * r;
-      for (int b = 0; b < nb; ++b) step_items.push_back(make_int2(r, b));
-      const int no = (P.n + 255) / 256;
-      for (int b = 0; b < no; ++b) out_items.push_back(make_int2(r, b));
-      for (int b = 0; b < cs[r].n_blocks; ++b) col_items.push_back(make_int4(r, b, 0, 0));
+      S->work[r] = {P.d.n_to, nb, (P.n + 255) / 256, cs[r].n_blocks, cs[r].n_groups, cs[r].n_tiles,
+                    P.n_cols, forward_rows(w, absorber)};
       if (std::find(sizes.begin(), sizes.end(), P.d.n_to) == sizes.end()) sizes.push_back(P.d.n_to);
     }
     std::sort(sizes.begin(), sizes.end());
@@ -1954,18 +2094,6 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
       const size_t elem = precision == SP_PRECISION_MIXED ? 8 : 16;
       while (c->inv_form + 1 < kForms && !inverse_form_ok(n_to, c->inv_form)) ++c->inv_form;
       while (c->fwd_form + 1 < kForms && !forward_form_ok(n_to, c->fwd_form, elem)) ++c->fwd_form;
-      std::vector<int2> inv, fwd;
-      for (int r = 0; r < R; ++r) {
-        sp_workspace* w = S->ws[r].get();
-        if (w->P->d.n_to != n_to) continue;
-        for (int col = 0; col < w->P->n_cols; ++col) inv.push_back(make_int2(r, col));
-        const int rows = forward_rows(w, w->P->d.absorber_in_stage != 0);
-        for (int row = 0; row < rows; ++row) fwd.push_back(make_int2(r, row));
-      }
-      c->n_inv = (int)inv.size();
-      c->n_fwd = (int)fwd.size();
-      c->inv_items.upload(inv.data(), inv.size(), S->stream);
-      c->fwd_items.upload(fwd.data(), fwd.size(), S->stream);
       S->classes.push_back(std::move(c));
     }
     S->inv_start.upload(is.data(), R, S->stream);
@@ -1982,30 +2110,17 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     S->out_att.upload(oa.data(), R, S->stream);
     S->step_start.upload(ts.data(), R, S->stream);
     S->step_att.upload(ta.data(), R, S->stream);
-    S->step_items.upload(step_items.data(), step_items.size(), S->stream);
-    S->out_items.upload(out_items.data(), out_items.size(), S->stream);
-    S->col_items.upload(col_items.data(), col_items.size(), S->stream);
-    S->n_step_items = (int)step_items.size();
-    S->n_out_items = (int)out_items.size();
-    S->n_col_items = (int)col_items.size();
-    // the sweep's items: every (run, node group), longest row first
-    std::vector<int4> sweep_items;
-    for (int r = 0; r < R; ++r)
-      for (int g = 0; g < cs[r].n_groups; ++g) sweep_items.push_back(make_int4(r, g, 0, 0));
-    std::stable_sort(sweep_items.begin(), sweep_items.end(), [&](const int4& x, const int4& y) {
-      return cs[x.x].n_tiles > cs[y.x].n_tiles;
-    });
-    S->sweep_items.upload(sweep_items.data(), sweep_items.size(), S->stream);
-    S->n_sweep_items = (int)sweep_items.size();
+    const std::vector<int> all(R, 1);
+    plan_items(S.get(), all, /*first=*/true);
     CUDA_CHECK(cudaDeviceSynchronize());  // the sessions' initial fields are in place
-    if (precision == SP_PRECISION_MIXED) tune_column(S.get(), S->col32_start.p);
-    else tune_column(S.get(), S->col_start.p);
+    if (precision == SP_PRECISION_MIXED) tune_column(S.get(), S->col32_start.p, all);
+    else tune_column(S.get(), S->col_start.p, all);
     S->h_fwd = fa;
     S->h_fwd32 = fa32;
     for (int r = 0; r < R; ++r) S->groups.push_back(cs[r].n_groups);
     set_column_form(S.get(), S->column_sweep);
-    if (precision == SP_PRECISION_MIXED) tune_transforms(S.get(), S->fwd32.p);
-    else tune_transforms(S.get(), S->fwd.p);
+    if (precision == SP_PRECISION_MIXED) tune_transforms(S.get(), S->fwd32.p, all);
+    else tune_transforms(S.get(), S->fwd.p, all);
     *out = S.release();
   });
 }
@@ -2064,6 +2179,11 @@ size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
     char line[512];
     std::snprintf(line, sizeof line, "column: %s (tile-parallel %.4f ms, sweep %.4f ms)\n",
                   S->column_sweep ? "sweep" : "tile-parallel", S->column_tile_ms, S->column_sweep_ms);
+    text += line;
+    std::snprintf(line, sizeof line,
+                  "work lists: planned for %d running runs, re-planned %d times; the last %d runs "
+                  "alone from batch step %lld\n",
+                  S->planned_active, S->replans, kTailRuns, (long long)S->tail_from);
     text += line;
     const double steps = (double)std::max<int64_t>(S->batch_steps, 1);
     std::snprintf(line, sizeof line,

@@ -137,3 +137,34 @@ def test_transform_forms_are_checked_and_all_agree():
         sc.set_transforms(8192, 0, 0)
     with pytest.raises(_lib.NativeError):
         sc.set_transforms(16384, 3, 0)
+
+
+@pytest.mark.gpu
+def test_scan_to_completion_replans_and_matches_single_runs():
+    """Runs of different lengths finish at different batch steps; the scan re-plans its
+    work lists as they do (only the running runs are launched, the forms tuned again), the
+    last few go on as single runs side by side, and every run still ends where it ends
+    alone."""
+    from solprop_b200 import _lib
+
+    lengths = (0.02, 0.025, 0.03, 0.035, 0.04, 0.05, 0.06, 0.08, 0.1, 0.12, 0.14, 0.16)
+    points = [scan.ScanPoint(120e-6, length, "He", 1.0, 60e-6, 20e-15, 1, 4096, 11 + k)
+              for k, length in enumerate(lengths)]
+    built = [scan.capillary_record(p) for p in points]
+    sc = _lib.Scan([r for r, _ in built], [q for _, q in built])
+    for _ in range(200):
+        if sc.advance(500).active == 0:
+            break
+    assert sc.advance(0).active == 0
+    text = sc.describe()
+    assert "re-planned 0 times" not in text, text
+    assert "alone from batch step -1" not in text, text  # the last runs went on alone
+    for i, (rec, pol) in enumerate(built):
+        state, info = sc.run(i)
+        assert info.event == 2  # finished
+        ws = _lib.Workspace(_lib.Problem(rec))
+        session = ws.start(pol)
+        while session.advance(4096).event != 2:
+            pass
+        assert session.batch.attempts == info.attempts, i
+        assert rel(state, session.export()) < 1e-12, i
