@@ -205,7 +205,9 @@ sp_status sp_scan_create(int32_t n_runs, const sp_problem* const* problems,
 /* The same with a precision (SP_PRECISION_*) for every run. */
 sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems,
                             const sp_run_desc* runs, int device, int precision, sp_scan** out);
-/* Up to `steps` batch steps (fewer when every run has finished). */
+/* Up to `steps` batch steps (fewer when every run has finished).  A batch step gives every
+ * run in the batch one attempt; runs gone on alone (sp_scan_set_alone) step meanwhile, and
+ * once no batch is left the call lets them take up to `steps` attempts each. */
 sp_status sp_scan_advance(sp_scan* scan, int32_t steps, sp_scan_status* out);
 /* One run's state (host complex, may be NULL) and counts (event 2: finished, 3: failed). */
 sp_status sp_scan_run(sp_scan* scan, int32_t run, double* state, sp_batch* info);
@@ -226,6 +228,13 @@ size_t sp_scan_describe(const sp_scan* scan, char* buf, size_t len);
 #define SP_SCAN_COLUMN_TILES 1
 #define SP_SCAN_COLUMN_SWEEP 2
 sp_status sp_scan_set_column(sp_scan* scan, int32_t form);
+/* Runs that go on alone.  A run whose remaining attempts (the distance left over its next
+ * step) exceed `factor` times the median of the batch's runs and `min_remaining` leaves
+ * the batch -- which would otherwise give it one attempt per batch step for many steps --
+ * and goes on as a single run on a host thread of its own, beside the batched steps, at
+ * most `max_runs` at a time (0: none; defaults 6, 2000, 4).  Such a run takes as many
+ * attempts per batch step as it manages.  No counterpart in the reference. */
+sp_status sp_scan_set_alone(sp_scan* scan, int32_t max_runs, double min_remaining, double factor);
 /* The transforms' forms for the runs of one grid size: 0 for one CTA per row, or a
  * cluster of 2, 4 or 8 CTAs per row.  The autotuner's choice stands otherwise; fixing the
  * forms makes two scans of the same runs give the same bits.  SP_ERR_ARGUMENT when no run

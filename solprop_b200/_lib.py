@@ -134,6 +134,7 @@ SIGNATURES = {
     "sp_scan_advance": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SpScanStatus)]),
     "sp_scan_describe": (C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "sp_scan_set_column": (C.c_int, [C.c_void_p, C.c_int32]),
+    "sp_scan_set_alone": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.c_double]),
     "sp_scan_set_transforms": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "sp_scan_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(SpBatch)]),
     "sp_scan_stream": (C.c_void_p, [C.c_void_p]),
@@ -496,6 +497,12 @@ class Scan:
         if form not in self.COLUMN_FORMS:
             raise ValueError(f"column form {form!r}: expected one of {sorted(self.COLUMN_FORMS)}")
         check(library().sp_scan_set_column(self.handle, self.COLUMN_FORMS[form]))
+
+    def set_alone(self, max_runs: int = 6, min_remaining: float = 2000.0, factor: float = 4.0) -> None:
+        """Let runs whose remaining attempts exceed ``factor`` x the batch's median and
+        ``min_remaining`` go on as single runs beside the batch (``max_runs`` at a time; 0
+        keeps every run in the batch)."""
+        check(library().sp_scan_set_alone(self.handle, int(max_runs), float(min_remaining), float(factor)))
 
     def set_transforms(self, n_to: int, inverse: int, forward: int) -> None:
         """Fix the transforms' forms for the runs with ``n_to`` fine samples: 0 for one CTA

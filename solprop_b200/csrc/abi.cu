@@ -1541,6 +1541,13 @@ struct sp_scan {
   // own stream, on a host thread of its own), one attempt per batch step
   bool tail = false;
   int64_t tail_from = -1;  // the batch step the tail began at
+  // runs gone on alone: a run whose remaining attempts (distance left over its next step)
+  // exceed alone_factor x the median of the batch's and alone_min leaves the batch, which
+  // it would hold back for many steps, and goes on as a single run on a host thread of its
+  // own, side by side with the batched steps (at most alone_max at a time)
+  std::vector<int> alone;
+  int alone_max = 6, alone_count = 0;
+  double alone_min = 2000.0, alone_factor = 4.0;
   std::vector<std::unique_ptr<FftClass>> classes;
   AdamsDev *h_adams_start = nullptr, *h_adams_att = nullptr;
   StageScalarsDev *h_stages_start = nullptr, *h_stages_att = nullptr;
@@ -1810,7 +1817,7 @@ void for_runs(sp_scan* S, const std::function<void(int)>& body) {
 // tile-parallel column and wider transform clusters); the next attempt recaptures its graph.
 void replan(sp_scan* S) {
   std::vector<int> live(S->R);
-  for (int r = 0; r < S->R; ++r) live[r] = !S->done[r];
+  for (int r = 0; r < S->R; ++r) live[r] = !S->done[r] && !S->alone[r];
   CUDA_CHECK(cudaStreamSynchronize(S->stream));
   plan_items(S, live, /*first=*/false);
   if (S->precision == SP_PRECISION_MIXED) tune_column(S, S->col32_start.p, live);
@@ -1832,7 +1839,7 @@ void replan(sp_scan* S) {
 void tail_step(sp_scan* S) {
   std::vector<int> live;
   for (int r = 0; r < S->R; ++r)
-    if (!S->done[r]) live.push_back(r);
+    if (!S->done[r] && !S->alone[r]) live.push_back(r);
   auto body = [&](int k) {
     const int r = live[k];
     CUDA_CHECK(cudaSetDevice(S->device));
@@ -1865,7 +1872,7 @@ void scan_step(sp_scan* S) {
   int n_start = 0;
   for (int r = 0; r < R; ++r) {
     S->h_flag_start[r] = 0;
-    if (S->done[r]) continue;
+    if (S->done[r] || S->alone[r]) continue;
     sp_session* ss = S->ss[r].get();
     if (!ss->history.empty()) continue;
     sp_workspace* w = S->ws[r].get();
@@ -1895,7 +1902,7 @@ void scan_step(sp_scan* S) {
   const auto t_prepare = clock::now();
   for_runs(S, [&](int r) {
     S->h_flag_att[r] = 0;
-    if (S->done[r]) return;
+    if (S->done[r] || S->alone[r]) return;
     sp_session* ss = S->ss[r].get();
     sp_workspace* w = S->ws[r].get();
     const Next nx = adams_next(ss, ss->run.z_end);
@@ -1958,14 +1965,14 @@ void scan_step(sp_scan* S) {
   S->host_decide_ms += ms(t_decide, t_end);
   for (int r = 0; r < R; ++r) {
     sp_session* ss = S->ss[r].get();
-    if (!S->done[r] && reached(ss->z, ss->run.z_end)) {
+    if (!S->done[r] && !S->alone[r] && reached(ss->z, ss->run.z_end)) {
       ss->finished = true;
       S->done[r] = 1;
     }
   }
   S->batch_steps += 1;
-  int active = 0;
-  for (int r = 0; r < R; ++r) active += !S->done[r];
+  int active = 0;  // runs still in the batch
+  for (int r = 0; r < R; ++r) active += !S->done[r] && !S->alone[r];
   if (S->R > kTailRuns && active > 0 && active <= kTailRuns) {
     // the batched launches' fixed costs outweigh their work: the last runs go on alone
     CUDA_CHECK(cudaStreamSynchronize(S->stream));
@@ -1975,6 +1982,133 @@ void scan_step(sp_scan* S) {
     replan(S);
   }
 }
+
+// The runs gone on alone during one sp_scan_advance call: a host thread each, stepping its
+// run on the single-run path (its workspace's stream) until the run ends or the call's
+// batched steps are done.  The threads are joined before the call returns -- also when it
+// throws -- and runs still going resume on fresh threads at the next call.
+class LoneRuns {
+ public:
+  explicit LoneRuns(sp_scan* S) : S_(S) {}
+  LoneRuns(const LoneRuns&) = delete;
+  LoneRuns& operator=(const LoneRuns&) = delete;
+  ~LoneRuns() { join(); }
+
+  // resume the runs already alone, then let the batch's longest runs go
+  void start() {
+    for (int r = 0; r < S_->R; ++r)
+      if (S_->alone[r] && !S_->done[r]) spawn(r);
+    release_long_runs();
+  }
+
+  // the runs whose remaining attempts stand far above the batch's median leave it
+  void release_long_runs() {
+    if ((int)lone_.size() >= S_->alone_max) return;
+    std::vector<std::pair<double, int>> rem;
+    for (int r = 0; r < S_->R; ++r) {
+      if (S_->done[r] || S_->alone[r]) continue;
+      const sp_session* ss = S_->ss[r].get();
+      if (ss->history.empty() || !(ss->proposal > 0.0)) continue;
+      rem.push_back({(ss->run.z_end - ss->z) / ss->proposal, r});
+    }
+    if (rem.size() < 2) return;
+    std::vector<double> v;
+    for (auto& e : rem) v.push_back(e.first);
+    std::nth_element(v.begin(), v.begin() + v.size() / 2, v.end());
+    const double median = v[v.size() / 2];
+    std::sort(rem.begin(), rem.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    bool synced = false;
+    for (auto& e : rem) {
+      if ((int)lone_.size() >= S_->alone_max) break;
+      if (!(e.first > S_->alone_min && e.first > S_->alone_factor * median)) break;
+      if (!synced) {  // the batch's last launches may still touch the run's buffers
+        CUDA_CHECK(cudaStreamSynchronize(S_->stream));
+        synced = true;
+      }
+      S_->alone[e.second] = 1;
+      S_->alone_count += 1;
+      spawn(e.second);
+    }
+  }
+
+  bool any_running() const {
+    for (auto& l : lone_)
+      if (l->state.load() == 0) return true;
+    return false;
+  }
+
+  // with no batch left: until every run alone has ended or taken `steps` more attempts
+  void wait(int steps) {
+    std::vector<long long> from;
+    for (auto& l : lone_) from.push_back(l->attempts.load());
+    for (;;) {
+      bool waiting = false;
+      for (size_t k = 0; k < lone_.size(); ++k)
+        waiting |= lone_[k]->state.load() == 0 && lone_[k]->attempts.load() - from[k] < steps;
+      if (!waiting) return;
+      std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+  }
+
+  // stop and join the threads; ended runs leave the scan, and a thread's unexpected
+  // failure is rethrown here
+  void join() {
+    stop_.store(true);
+    std::exception_ptr error;
+    for (auto& l : lone_) {
+      if (l->thread.joinable()) l->thread.join();
+      if (l->state.load() == 1 || l->state.load() == 2) S_->done[l->run] = 1;
+      if (l->state.load() == 3 && !error) error = l->error;
+    }
+    lone_.clear();
+    if (error && !std::uncaught_exceptions()) std::rethrow_exception(error);
+  }
+
+ private:
+  struct Lone {
+    int run = 0;
+    std::thread thread;
+    std::atomic<int> state{0};  // 0 going, 1 finished, 2 failed (step floor), 3 error
+    std::atomic<long long> attempts{0};
+    std::exception_ptr error;
+  };
+
+  void spawn(int r) {
+    auto l = std::make_unique<Lone>();
+    l->run = r;
+    Lone* me = l.get();
+    me->thread = std::thread([this, me] {
+      sp_session* ss = S_->ss[me->run].get();
+      try {
+        CUDA_CHECK(cudaSetDevice(S_->device));
+        while (!stop_.load()) {
+          try {
+            adams_adaptive_attempt(ss, ss->run.z_end);
+          } catch (const Failure& f) {
+            if (f.code != SP_ERR_CONVERGENCE) throw;
+            ss->failed = true;
+            me->state.store(2);
+            return;
+          }
+          me->attempts.fetch_add(1);
+          if (reached(ss->z, ss->run.z_end)) {
+            ss->finished = true;
+            me->state.store(1);
+            return;
+          }
+        }
+      } catch (...) {
+        me->error = std::current_exception();
+        me->state.store(3);
+      }
+    });
+    lone_.push_back(std::move(l));
+  }
+
+  sp_scan* S_;
+  std::atomic<bool> stop_{false};
+  std::vector<std::unique_ptr<Lone>> lone_;
+};
 
 }  // namespace
 
@@ -2023,6 +2157,7 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
       S->ws.push_back(std::move(w));
     }
     S->done.assign(R, 0);
+    S->alone.assign(R, 0);
     S->pending.resize(R);
     {
       // up to eight host threads when the batch is large enough to pay for the hand-off
@@ -2129,11 +2264,21 @@ sp_status sp_scan_advance(sp_scan* S, int32_t steps, sp_scan_status* out) {
   return guarded([&] {
     if (!S || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
     CUDA_CHECK(cudaSetDevice(S->device));
-    for (int i = 0; i < steps; ++i) {
-      bool any = false;
-      for (int d : S->done) any |= !d;
-      if (!any) break;
-      scan_step(S);
+    auto batched = [&] {
+      for (int r = 0; r < S->R; ++r)
+        if (!S->done[r] && !S->alone[r]) return true;
+      return false;
+    };
+    {
+      LoneRuns lone(S);
+      if (S->alone_max > 0) lone.start();
+      int i = 0;
+      for (; i < steps && batched(); ++i) {
+        scan_step(S);
+        if (S->alone_max > 0 && (i + 1) % 128 == 0) lone.release_long_runs();
+      }
+      if (i < steps && lone.any_running()) lone.wait(steps - i);
+      lone.join();
     }
     out->active = 0;
     out->attempts = out->rejected = out->evaluations = 0;
@@ -2152,6 +2297,7 @@ sp_status sp_scan_run(sp_scan* S, int32_t run, double* state, sp_batch* info) {
     if (!S || run < 0 || run >= S->R) throw Failure(SP_ERR_ARGUMENT, "run index out of range");
     CUDA_CHECK(cudaSetDevice(S->device));
     CUDA_CHECK(cudaStreamSynchronize(S->stream));
+    CUDA_CHECK(cudaStreamSynchronize(S->ws[run]->stream));  // a run that went on alone
     sp_session* ss = S->ss[run].get();
     if (state) {
       const size_t bytes = (size_t)S->ws[run]->P->n * sizeof(double2);
@@ -2182,8 +2328,8 @@ size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
     text += line;
     std::snprintf(line, sizeof line,
                   "work lists: planned for %d running runs, re-planned %d times; the last %d runs "
-                  "alone from batch step %lld\n",
-                  S->planned_active, S->replans, kTailRuns, (long long)S->tail_from);
+                  "alone from batch step %lld; %d long runs went on alone\n",
+                  S->planned_active, S->replans, kTailRuns, (long long)S->tail_from, S->alone_count);
     text += line;
     const double steps = (double)std::max<int64_t>(S->batch_steps, 1);
     std::snprintf(line, sizeof line,
@@ -2221,6 +2367,17 @@ sp_status sp_scan_set_column(sp_scan* S, int32_t form) {
     CUDA_CHECK(cudaSetDevice(S->device));
     CUDA_CHECK(cudaStreamSynchronize(S->stream));
     set_column_form(S, form == SP_SCAN_COLUMN_SWEEP);
+  });
+}
+
+sp_status sp_scan_set_alone(sp_scan* S, int32_t max_runs, double min_remaining, double factor) {
+  return guarded([&] {
+    if (!S) throw Failure(SP_ERR_ARGUMENT, "NULL scan");
+    if (max_runs < 0 || !(min_remaining >= 0.0) || !(factor >= 1.0))
+      throw Failure(SP_ERR_ARGUMENT, "alone: max_runs >= 0, min_remaining >= 0, factor >= 1");
+    S->alone_max = max_runs;
+    S->alone_min = min_remaining;
+    S->alone_factor = factor;
   });
 }
 

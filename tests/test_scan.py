@@ -152,6 +152,7 @@ def test_scan_to_completion_replans_and_matches_single_runs():
               for k, length in enumerate(lengths)]
     built = [scan.capillary_record(p) for p in points]
     sc = _lib.Scan([r for r, _ in built], [q for _, q in built])
+    sc.set_alone(0)
     for _ in range(200):
         if sc.advance(500).active == 0:
             break
@@ -168,3 +169,35 @@ def test_scan_to_completion_replans_and_matches_single_runs():
             pass
         assert session.batch.attempts == info.attempts, i
         assert rel(state, session.export()) < 1e-12, i
+
+
+
+@pytest.mark.gpu
+def test_long_runs_go_on_alone_and_match_single_runs():
+    """With a low threshold the longest runs leave the batch and step on host threads of
+    their own beside it; every run still ends where it ends alone."""
+    from solprop_b200 import _lib
+
+    lengths = (0.02, 0.02, 0.025, 0.03, 0.03, 0.035, 0.2, 0.3)
+    points = [scan.ScanPoint(120e-6, length, "He", 1.0, 60e-6, 20e-15, 1, 4096, 31 + k)
+              for k, length in enumerate(lengths)]
+    built = [scan.capillary_record(p) for p in points]
+    sc = _lib.Scan([r for r, _ in built], [q for _, q in built])
+    sc.set_alone(2, 20.0, 2.0)
+    for _ in range(400):
+        if sc.advance(16).active == 0:
+            break
+    assert sc.advance(0).active == 0
+    text = sc.describe()
+    assert "0 long runs went on alone" not in text, text
+    for i, (rec, pol) in enumerate(built):
+        state, info = sc.run(i)
+        assert info.event == 2
+        ws = _lib.Workspace(_lib.Problem(rec))
+        session = ws.start(pol)
+        while session.advance(4096).event != 2:
+            pass
+        assert session.batch.attempts == info.attempts, i
+        assert rel(state, session.export()) < 1e-12, i
+    with pytest.raises(_lib.NativeError):
+        sc.set_alone(-1)
