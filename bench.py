@@ -232,9 +232,10 @@ def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024
              rank: int = 0, world: int = 1) -> dict:
     """The parameter-scan workload (config 4): n_runs seeded uneven capillary runs, stepped together.
 
-    Reports attempts per second of the batched solver (every batch step gives every run
-    one exponential-Adams attempt, FP64) and of the plain path on the same runs one at a
-    time (one session per run, its attempts back to back), on the device's clock.  With
+    Reports attempts per second of the batched solver at full batch (every batch step gives
+    every run one exponential-Adams attempt; no run leaves the batch to go on alone) and of
+    the plain path on the same runs one at a time (one session per run, its attempts back
+    to back), on the device's clock.  With
     several ranks each solves its cost-balanced share of the runs (``scan.shard``, no
     exchange); attempts add over ranks and the time is the slowest rank's.
     """
@@ -260,6 +261,7 @@ def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024
     batched = {}
     for precision in ("fp64", "mixed"):
         sc = _lib.Scan(records, policies, device, precision)
+        sc.set_alone(0)
         stream = torch.cuda.ExternalStream(sc.stream, device=torch.device("cuda", device))
         sc.advance(warmup)
         before = sc.advance(0).attempts
@@ -305,6 +307,62 @@ def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024
             "speedup_vs_plain": {k: v["attempts_per_s"] / plain for k, v in batched.items()}}
 
 
+def complete_scan_leg(device: int, n_runs: int, seed: int = 2024, rank: int = 0, world: int = 1) -> dict:
+    """The scan's first n_runs points solved to the end, in runs per second: the batched
+    mixed solver (re-planning as runs finish, long runs going on alone) against the plain
+    FP64 path solving the same runs one after another.  Host wall time around the stepping
+    (creation excluded on both sides), slowest rank's for the batched side."""
+    import time
+
+    import torch
+
+    from solprop_b200 import _lib, scan
+
+    points = scan.draw_points(n_runs, seed)
+    points = [points[i] for i in scan.shard(points, rank, world)]
+    built = [scan.capillary_record(p) for p in points]
+    records, policies = [b[0] for b in built], [b[1] for b in built]
+    sc = _lib.Scan(records, policies, device, "mixed")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    while sc.advance(1000).active:
+        pass
+    torch.cuda.synchronize()
+    batched_s = time.perf_counter() - t0
+    infos = [sc.run(i, state=False)[1] for i in range(len(records))]
+    batched_attempts = sum(int(i.attempts) for i in infos)
+    finished = sum(int(i.event) == 2 for i in infos)
+    plan = [line for line in sc.describe().splitlines() if line.startswith("work lists")]
+    sc.close()
+    plain_s, plain_attempts = 0.0, 0
+    for rec, pol in zip(records, policies):
+        problem = _lib.Problem(rec)
+        ws = _lib.Workspace(problem, device)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        session = ws.start(pol)
+        while session.advance(4096).event not in (2, 3):
+            pass
+        torch.cuda.synchronize()
+        plain_s += time.perf_counter() - t0
+        plain_attempts += int(session.batch.attempts)
+        session.close()
+        ws.close()
+        problem.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([batched_s, plain_s], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        batched_s, plain_s = float(t[0].item()), float(t[1].item())
+    return {"runs": n_runs, "finished": finished * world if world > 1 else finished,
+            "batched_mixed": {"seconds": batched_s, "runs_per_s": n_runs / batched_s,
+                              "attempts": batched_attempts, "plan": plan},
+            "plain_fp64": {"seconds": plain_s, "runs_per_s": n_runs / plain_s, "attempts": plain_attempts},
+            "runs_per_s_ratio": plain_s / batched_s}
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -314,6 +372,8 @@ def main() -> int:
     parser.add_argument("--cpu-budget", type=float, default=20.0)
     parser.add_argument("--scan-runs", type=int, default=256)
     parser.add_argument("--scan-steps", type=int, default=30)
+    parser.add_argument("--complete-runs", type=int, default=32,
+                        help="scan runs solved to the end for the runs/s comparison (0: skip)")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -446,6 +506,8 @@ def main() -> int:
     scan_result = None
     if args.scan_runs > 0:
         scan_result = scan_leg(local, args.scan_runs, args.scan_steps, warmup=3, rank=rank, world=world)
+    if args.complete_runs > 0 and scan_result is not None:
+        scan_result["complete"] = complete_scan_leg(local, args.complete_runs, rank=rank, world=world)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
