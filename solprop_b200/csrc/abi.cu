@@ -2271,7 +2271,7 @@ sp_status sp_scan_advance(sp_scan* S, int32_t steps, sp_scan_status* out) {
     };
     {
       LoneRuns lone(S);
-      if (S->alone_max > 0) lone.start();
+      if (S->alone_max > 0 && steps > 0) lone.start();
       int i = 0;
       for (; i < steps && batched(); ++i) {
         scan_step(S);
