@@ -374,6 +374,8 @@ def main() -> int:
     parser.add_argument("--scan-steps", type=int, default=30)
     parser.add_argument("--complete-runs", type=int, default=32,
                         help="scan runs solved to the end for the runs/s comparison (0: skip)")
+    parser.add_argument("--config2-only", action="store_true",
+                        help="measure config 2 alone (no runs, surrogate or scan legs), e.g. under ncu")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -501,10 +503,10 @@ def main() -> int:
                "sample": f"{done} attempts of the config-2 run from z=0 on one host thread "
                          f"({os.cpu_count()} cores on the box)"}
 
-    runs_result = runs_leg(local)
-    surrogate_result = surrogate_leg(local)
+    runs_result = None if args.config2_only else runs_leg(local)
+    surrogate_result = None if args.config2_only else surrogate_leg(local)
     scan_result = None
-    if args.scan_runs > 0:
+    if args.scan_runs > 0 and not args.config2_only:
         scan_result = scan_leg(local, args.scan_runs, args.scan_steps, warmup=3, rank=rank, world=world)
     if args.complete_runs > 0 and scan_result is not None:
         scan_result["complete"] = complete_scan_leg(local, args.complete_runs, rank=rank, world=world)
