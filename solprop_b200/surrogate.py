@@ -5,8 +5,8 @@ layers of 512 GELU units -> the log10 exit spectral density on 2048 wavelengths 
 100 nm to 4 um (``scan.exit_log_spectrum``).  Five members trained from different seeds
 and shuffles form an ensemble; a point whose members disagree by more than a threshold
 (the standard deviation over members of each output in log10 units, weighted by the mean
-spectrum's energy there) is routed to the solver, which stays the judge of the surrogate's
-error.  Targets are the exit log10 spectra floored at ``DECADES`` below each spectrum's
+spectrum's energy there) is routed to the solver, whose solutions remain the measure of the
+surrogate's error.  Targets are the exit log10 spectra floored at ``DECADES`` below each spectrum's
 peak: the error measure weights bins by energy, and the floor keeps the empty bins' noise
 out of the fit.
 
@@ -365,7 +365,7 @@ def plain_seconds_per_point(points, device: int = 0, max_attempts: int = 8192):
 def study(*, n_train: int = 4096, n_screen: int = 100_000, threshold: float = 5e-3, epochs: int = 600,
           max_batch_steps: int = 4096, resolve_cap: int = 256, device: int = 0, seed: int = 2025,
           log=print) -> dict:
-    """Train the ensemble on solver runs, screen ``n_screen`` seeded points, judge a held-out
+    """Train the ensemble on solver runs, screen ``n_screen`` seeded points, score a held-out
     1 % against plain FP64 solves.  Returns the figures as a dict."""
     import time
 
