@@ -157,7 +157,10 @@ sp_status sp_workspace_destroy(sp_workspace* ws);
  * quiet != 0 leaves a quiet in-stage collar out (numpy_ref source.py:858-890). */
 sp_status sp_workspace_source(sp_workspace* ws, const double* lab, double z, int quiet,
                               double* out);
-/* The same on device pointers, on the workspace's stream; for timing. */
+/* The same on device pointers, on the workspace's stream; for timing.  It returns before
+ * the evaluation ends, so a response column that gave up waiting is reported by the next
+ * call on the workspace that reads the result back (sp_workspace_source, advance): the
+ * column's status mark stays set until a call reports it. */
 sp_status sp_workspace_source_device(sp_workspace* ws, const void* lab_device, double z,
                                      int quiet, void* out_device);
 /* Kernel launches one source evaluation makes (the evidence of the device path). */

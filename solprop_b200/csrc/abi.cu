@@ -12,6 +12,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -51,6 +52,29 @@ sp_status guarded(F&& f) {
     return SP_ERR_ARGUMENT;
   }
 }
+
+// The source kernels' shared-memory limits are attributes of one device: every entry point
+// that launches them sets them once per device, with that device current.
+constexpr int kMaxDevices = 64;
+std::mutex g_configure_mutex;
+bool g_configured[kMaxDevices];
+
+void ensure_configured(int device) {
+  if (device < 0 || device >= kMaxDevices) throw Failure(SP_ERR_ARGUMENT, "device index out of range");
+  std::lock_guard<std::mutex> lock(g_configure_mutex);
+  if (g_configured[device]) return;
+  CUDA_CHECK(configure_source_kernels());
+  g_configured[device] = true;
+}
+
+// Runs a callable when the scope ends, however it ends.
+template <class F>
+struct ScopeExit {
+  F f;
+  ~ScopeExit() { f(); }
+};
+template <class F>
+ScopeExit<F> on_scope_exit(F f) { return ScopeExit<F>{f}; }
 
 // ------------------------------------------------------------------ piecewise tables
 struct Table {
@@ -265,7 +289,11 @@ struct sp_workspace {
     pending.clear();
     ev_next = 0;
   }
+  // A borrowed workspace is a view over memory it does not own (the no-allocation entry
+  // point's): its stream and host scalars belong to others, and it frees nothing.
+  bool borrowed = false;
   ~sp_workspace() {
+    if (borrowed) return;
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (stream) cudaStreamSynchronize(stream);
     if (h_stage) cudaFreeHost(h_stage);
@@ -1260,11 +1288,7 @@ sp_status sp_workspace_create_ex(const sp_problem* problem, int device, int prec
     if (precision == SP_PRECISION_MIXED && problem->d.grid_kind == 1)
       throw Failure(SP_ERR_REFUSED, "the mixed precision of the envelope route is not built yet");
     CUDA_CHECK(cudaSetDevice(device));
-    static bool configured = false;
-    if (!configured) {
-      CUDA_CHECK(configure_source_kernels());
-      configured = true;
-    }
+    ensure_configured(device);
     auto ws = std::make_unique<sp_workspace>();
     ws->P = problem;
     ws->device = device;
@@ -2126,11 +2150,7 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     if (precision != SP_PRECISION_FP64 && precision != SP_PRECISION_MIXED)
       throw Failure(SP_ERR_ARGUMENT, "unknown precision");
     CUDA_CHECK(cudaSetDevice(device));
-    static bool configured = false;
-    if (!configured) {
-      CUDA_CHECK(configure_source_kernels());
-      configured = true;
-    }
+    ensure_configured(device);
     auto S = std::make_unique<sp_scan>();
     S->device = device;
     S->precision = precision;
@@ -2493,6 +2513,14 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     // A view of the workspace whose buffers are regions of the array; it owns nothing.
     static sp_workspace views[kNoAllocDevices];
     sp_workspace& ws = views[device];
+    ws.borrowed = true;
+    // the caller's stream and the static host scalars are lent for this call only, on
+    // every way out of it (a refusal or a failed upload included)
+    auto release = on_scope_exit([&ws] {
+      ws.stream = nullptr;
+      ws.h_stage = nullptr;
+      ws.P = nullptr;
+    });
     ws.P = problem;
     ws.device = device;
     ws.stream = s;
@@ -2575,18 +2603,17 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     ws.arrivals.zero(s);
     ws.ticket.zero(s);
     ws.norms.zero(s);
-    static bool configured[kNoAllocDevices];
-    if (!configured[device]) {
-      CUDA_CHECK(configure_source_kernels());
-      configured[device] = true;
-    }
+    ensure_configured(device);
     fill_stage(&ws, 0, z, z);
     upload_stages(&ws, 1);
     eval_source(&ws, static_cast<const double2*>(lab), 0, nullptr, static_cast<double2*>(out),
                 quiet != 0);
-    // the host copies above read pageable buffers of this call; finish before they go
+    // the response column marks its status slot when a tile gave up waiting: read it with
+    // the result (the host copies above also read pageable buffers of this call)
+    double status[kColumnStatus + 1] = {};
+    CUDA_CHECK(cudaMemcpyAsync(&status[kColumnStatus], ws.norms.p + kColumnStatus, sizeof(double),
+                               cudaMemcpyDeviceToHost, s));
     CUDA_CHECK(cudaStreamSynchronize(s));
-    ws.stream = nullptr;   // the view never owns the caller's stream
-    ws.h_stage = nullptr;  // nor the host scalars
+    check_column(status, ws.norms.p, s);
   });
 }

@@ -76,3 +76,54 @@ def test_no_alloc_refuses_a_problem_larger_than_its_array():
         _lib.check(_lib.library().sp_source_noalloc(
             problem.handle, C.c_void_p(lab.ctypes.data), 0.0, 0, C.c_void_p(lab.ctypes.data),
             None))
+
+
+def test_no_alloc_after_a_refusal_leaves_the_callers_stream_usable():
+    """A refused call on the caller's own stream, then a good call on it, then more work.
+
+    The entry point lends the caller's stream to its internal view only for the call; a
+    refusal part-way through (the problem does not fit the array) must leave nothing of
+    it behind.  Free device memory is also unchanged across warm calls: the evaluation
+    allocates nothing.
+    """
+    torch = pytest.importorskip("torch")
+    from solprop_b200 import _lib
+
+    lib = _lib.library()
+    side = torch.cuda.Stream(device="cuda:0")
+    big = record("config2")
+    big.n_nodes = 512
+    big.synthesis = np.tile(big.synthesis, (8, 1))
+    big.projection = np.tile(big.projection, (1, 8))
+    too_big = _lib.Problem(big)
+    rec = record("cap1_ar")
+    g = golden("cap1_ar")
+    problem = _lib.Problem(rec)
+    shape = (rec.n_modes, rec.n_pol, rec.n_omega)
+    with torch.cuda.stream(side):
+        lab_dev = _device_copy(torch, g["src1.lab"])
+        out = torch.empty_like(lab_dev)
+        junk = torch.zeros(big.n_cols * big.n_omega * 2, dtype=torch.float64, device="cuda:0")
+    side.synchronize()
+    handle = C.c_void_p(side.cuda_stream)
+    with pytest.raises(_lib.NativeError, match="MiB"):
+        _lib.check(lib.sp_source_noalloc(too_big.handle, C.c_void_p(junk.data_ptr()), 0.0, 0,
+                                         C.c_void_p(junk.data_ptr()), handle))
+    z = float(g["src1.z"])
+    for _ in range(2):  # the first call on a device may resolve the array's address
+        _lib.check(lib.sp_source_noalloc(problem.handle, C.c_void_p(lab_dev.data_ptr()), z, 0,
+                                         C.c_void_p(out.data_ptr()), handle))
+    free_before, _ = torch.cuda.mem_get_info(0)
+    _lib.check(lib.sp_source_noalloc(problem.handle, C.c_void_p(lab_dev.data_ptr()), z, 0,
+                                     C.c_void_p(out.data_ptr()), handle))
+    free_after, _ = torch.cuda.mem_get_info(0)
+    assert free_after == free_before
+    # the stream still takes work after the calls
+    with torch.cuda.stream(side):
+        doubled = out * 2.0
+    side.synchronize()
+    got = _host(out, shape)
+    assert rel(got, g["src1.source"]) < SOURCE_TOL
+    assert rel(_host(doubled, shape), 2.0 * got) == 0.0
+    problem.close()
+    too_big.close()
