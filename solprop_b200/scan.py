@@ -22,7 +22,9 @@ machine without solprop:
   cubic in log |E| on uniform knots (``translate/ionisation.py``), the trapezoid running
   integral;
 * an in-stage temporal collar, a Gaussian input pulse in HE11 and one photon per mode
-  per frequency bin of input shot noise, seeded (``noise.py``).
+  per frequency bin of input shot noise, seeded: the reference's draw
+  (``noise.py:195-294``), which the tests hold bit for bit to the reference's own
+  realisation on the same grid and seed.
 
 The scan's parameter distribution is config 4's (:func:`draw_points`).
 """
@@ -41,7 +43,7 @@ from solprop_b200.record import PiecewiseTable, ProblemRecord
 
 C0 = 299792458.0
 EPS0 = 8.8541878188e-12
-HBAR = 1.054571817e-34
+HBAR = 6.62607015e-34 / (2 * math.pi)  # h / 2 pi, as scipy.constants defines it
 E_CHARGE = 1.602176634e-19
 M_E = 9.1093837139e-31
 K_B = 1.380649e-23
@@ -150,6 +152,23 @@ def rate_table(gas: str, intervals: int = 512):
                 field_max=field_max, rate_max=float(adk_rate(gas, np.array([field_max]))[0]))
 
 
+def input_noise(omega: np.ndarray, active: np.ndarray, dt: float, d_omega: float,
+                rng: np.random.Generator, *, n_modes: int = 1, n_pol: int = 1,
+                kind: str = "field") -> np.ndarray:
+    """One photon per mode, polarisation and active bin, with a random phase (the input
+    shot-noise model, ``noise.py:195-294``): amplitude ``sqrt(hbar omega / d_omega)
+    sqrt(2 pi) / dt``, halved on a field grid (its one-sided spectrum); the phase drawn
+    uniform on [0, 2 pi) over every bin, active or not, so that a seed means the same
+    realisation whatever the band."""
+    amplitude = np.zeros(len(omega))
+    scale = np.sqrt(2.0 * np.pi) / dt
+    if kind == "field":
+        scale = 0.5 * scale
+    amplitude[active] = scale * np.sqrt(HBAR * omega[active] / d_omega)
+    phase = rng.uniform(0.0, 2.0 * np.pi, size=(n_modes, n_pol, len(omega)))
+    return amplitude * np.exp(1j * phase)
+
+
 def collar(t: np.ndarray, half_window: float):
     """The temporal collar: one on the central 80 %, a cos^2 taper over each 10 % edge."""
     edge = 0.2 * half_window
@@ -220,9 +239,12 @@ def capillary_record(p: ScanPoint) -> tuple[ProblemRecord, dict]:
     a *= math.sqrt(p.energy / (np.sum(a * a) * dt))
     field0 = np.zeros((n_modes, 1, n_omega), dtype=np.complex128)
     field0[0, 0] = np.fft.rfft(a) * active
-    rng = np.random.default_rng(p.seed)
-    amp = np.sqrt(HBAR * omega * n_t / (2 * dt))
-    noise0 = (amp * np.exp(2j * np.pi * rng.random((n_modes, 1, n_omega)))) * active
+    # the state is the vacuum-normalised amplitude: true-power spectra divided by the root
+    # of the modes' power weight Re n_eff (fourier.py:300-340, driver/inputs.py:484-488)
+    root_weight = np.sqrt(np.where(active, beta * C0 / np.maximum(omega, 1e-300), 1.0))[:, None, :]
+    field0 /= root_weight
+    noise0 = input_noise(omega, active, dt, 2 * np.pi / (n_t * dt), np.random.default_rng(p.seed),
+                         n_modes=n_modes) / root_weight
     rt = rate_table(p.gas)
     rec = ProblemRecord(
         grid_kind="field", n_modes=n_modes, n_pol=1, n_omega=n_omega, n_t=n_t, n_to=n_to,

@@ -354,11 +354,17 @@ def gnlse_case(case, seed):
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
 
 
-def workload_case(case, *, seed, **common):
-    """A full-size configuration: the problem, the march policy and two reference
-    source evaluations (no run: at this size the reference takes seconds per step)."""
+def workload_case(case, *, seed, n_save=3, **common):
+    """A full-size configuration: the problem, the march policy, two reference source
+    evaluations, and the reference's whole adaptive run (exponential Adams at the route's
+    defaults) with its states at ``n_save`` planes, its step history and its counts."""
     sim = capillary(case, **common)
     problem, request = sim.translate(), sim.run_request()
+    _, zs, states, (hist, counts), wall = drive(capillary(case, **common, n_save=n_save))
+    adaptive = {"adaptive.z": zs, "adaptive.states": states, "adaptive.history": hist,
+                "adaptive.counts": counts, "adaptive.wall": np.array(wall),
+                "adaptive.policy": drive.policy}
+    print(f"{case}: adaptive run {counts} attempts/rejected in {wall:.1f} s", flush=True)
     backend = NumpyRefBackend(problem, request, grid=sim.grid, modes=sim.modes,
                               profiles=sim.profiles)
     session = backend.prepare(problem, request).start(Start.entrance(problem))
@@ -372,6 +378,71 @@ def workload_case(case, *, seed, **common):
         golden[f"src{i}.lab"] = lab
         golden[f"src{i}.z"] = np.array(z)
         golden[f"src{i}.source"] = ws.lab_source(lab, z)
+    golden.update(adaptive)
+    write(case, problem, golden)
+
+
+# Config-4 scan points built by the reference's own capillary translation (its defaults:
+# Gauss-Kronrod radial rule, band-rule running integrals, in-stage collar), with the
+# reference's input shot noise drawn from each point's seed.  The corner of the scan's
+# distribution is here: eight modes on a 32768-sample grid.
+SCAN_POINTS = [
+    # radius, length, gas, pressure (bar), energy, fwhm, modes, n_to, seed
+    (100e-6, 1.2, "He", 1.5, 150e-6, 12e-15, 8, 32768, 11),
+    (60e-6, 0.6, "Ar", 2.5, 300e-6, 8e-15, 1, 4096, 12),
+    (140e-6, 1.8, "Ne", 0.5, 60e-6, 25e-15, 4, 16384, 13),
+    (110e-6, 1.0, "Ar", 1.0, 40e-6, 20e-15, 3, 8192, 14),
+]
+SCAN_ATTEMPTS = 24
+
+
+def scan_point_sim(radius, length, gas, pressure, energy, fwhm, modes, n_to, seed, n_save=2):
+    """One scan point through ``Simulation.from_capillary``: constant pressure, 800 nm,
+    the 150 nm - 4 um band on a pow2 field grid of ``n_to`` fine samples."""
+    omega_max = 2 * np.pi * C0 / 150e-9
+    dt_fine = 2 * np.pi / (6.0 * omega_max)  # the grid's default ffac of 6
+    # a request 0.75 n_to dt_fine wide after the outside collars rounds up to n_to
+    trange = 0.8 * 0.75 * n_to * dt_fine
+    grid = FieldGrid.from_limits(length, 800e-9, (150e-9, 4e-6), trange, fft_size="pow2")
+    assert grid.n_to == n_to, (grid.n_to, n_to)
+    fill = Mixture.fill({gas_species(gas): 1.0}, pressure)
+    return Simulation.from_capillary(
+        radius, length, fill, None, wavelength=800e-9, grid=grid, fwhm=fwhm, energy=energy,
+        cladding=1.45 + 0j, modes=modes, plasma=adk_oracle(gas), noise="input", seed=seed,
+        rtol=1e-6, n_save=n_save, backend="numpy_ref", boundary_check=None)
+
+
+def scan_case(index, params):
+    """The lowered problem, the launch state, one source evaluation and the state after
+    ``SCAN_ATTEMPTS`` adaptive exponential-Adams attempts of one scan point."""
+    case = f"scan{index}"
+    sim = scan_point_sim(*params)
+    problem, request = sim.translate(), sim.run_request()
+    backend = NumpyRefBackend(problem, request, grid=sim.grid, modes=sim.modes,
+                              profiles=sim.profiles)
+    session = backend.prepare(problem, request).start(Start.entrance(problem))
+    golden = {"adaptive.policy": policy_record(session, request), "params": np.array(params[:2] + params[3:], float),
+              "gas": np.frombuffer(params[2].encode(), np.uint8)}
+    from solprop.translate.linop import power_weight_at
+
+    # the draw enters the problem divided by the root of this row (driver/inputs.py:484-488)
+    golden["power_weight"] = np.asarray(power_weight_at(problem, 0.0))
+    ws = backend._workspace
+    golden["launch"] = np.array(ws.committed())
+    golden["src0.lab"] = golden["launch"]
+    golden["src0.z"] = np.array(0.0)
+    golden["src0.source"] = ws.lab_source(golden["launch"], 0.0)
+    t0 = time.time()
+    done = 0
+    while done < SCAN_ATTEMPTS:
+        batch = session.advance(work_limit=SCAN_ATTEMPTS - done)
+        session.acknowledge(batch.receipt)
+        done = int(session.status().attempts)
+    status = session.status()
+    golden["attempts.state"] = np.array(ws.committed())
+    golden["attempts.counts"] = np.array([status.attempts, status.rejected])
+    print(f"{case}: {status.attempts} attempts ({status.rejected} rejected) in "
+          f"{time.time() - t0:.1f} s, {problem.transform.synthesis.shape[0]} nodes", flush=True)
     write(case, problem, golden)
 
 
@@ -399,3 +470,6 @@ if __name__ == "__main__":
         workload_case("config1", seed=5, gas="Ar", pressure=1.0, length=1.0,
                       n_t_limits=(150e-9, 4e-6), trange=400e-15, energy=100e-6, fwhm=10e-15,
                       modes=1)
+    for i, params in enumerate(SCAN_POINTS):
+        if not only or f"scan{i}" in only or "scan" in only:
+            scan_case(i, params)

@@ -74,8 +74,10 @@ def test_fixed_schedule_matches_reference(case):
     assert plane == len(zs)
 
 
-@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he", "gnlse_raman"])
+@pytest.mark.parametrize("case", ["cap1_ar", "cap4_he", "gnlse_raman", "config1", "config2"])
 def test_adaptive_run_matches_reference(case):
+    """Whole adaptive runs, configs 1 and 2 at full size among them (1870 and 1408
+    attempts of the reference's own march)."""
     rec, problem, ws = _workspace(case)
     g = golden(case)
     pol = policy(g, "adaptive")
