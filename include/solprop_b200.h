@@ -126,13 +126,63 @@ typedef struct sp_run_desc {
   int32_t lag, estimator_order;
 } sp_run_desc;
 
-/* What one advance() returns (the _core.SessionBatch / SessionEvent essentials). */
+/* Why an advance() returned (the native march's Reason,
+ * native/include/solprop_native/march/adams_march.hpp:325-347, same codes). */
+enum {
+  SP_REASON_REACHED = 0,   /* a save plane or the end was reached */
+  SP_REASON_BOUND = 3,     /* the call's attempts or its deadline are spent */
+  SP_REASON_FLOOR = 5,     /* a proposal fell below dz_min (a convergence failure) */
+  SP_REASON_ERROR = 6,     /* a device or argument failure; earlier steps stand */
+  SP_REASON_DIVERGED = 7,  /* a replayed step's norm is not finite */
+  SP_REASON_STOPPED = 11,  /* sp_session_request_stop was called */
+  SP_REASON_HALTED = 12    /* sp_session_request_snapshot: an accepted endpoint to save */
+};
+/* What class of solprop error a failure maps to (adams_march.hpp:349-358, same codes):
+ * convergence -> solprop's ConvergenceError, backend -> BackendError, value ->
+ * ValueError, refused -> BackendRefusal. */
+enum {
+  SP_CATEGORY_NONE = 0, SP_CATEGORY_CONVERGENCE = 1, SP_CATEGORY_BACKEND = 2,
+  SP_CATEGORY_VALUE = 3, SP_CATEGORY_REFUSED = 4
+};
+/* Events of a batch (_core.SessionEvent's kind and outcome, folded). */
+enum {
+  SP_EVENT_NONE = 0,     /* the work limit or the deadline ended the call */
+  SP_EVENT_PLANE = 1,    /* a save plane was reached */
+  SP_EVENT_FINISHED = 2, /* the run reached its end */
+  SP_EVENT_FAILED = 3,   /* the run failed; reason and category say how */
+  SP_EVENT_STOPPED = 4,  /* the run was stopped on request; it takes no more attempts */
+  SP_EVENT_HALTED = 5    /* an accepted endpoint after sp_session_request_snapshot */
+};
+
+/* What one advance() returns (the _core.SessionBatch / SessionEvent essentials,
+ * native/src/solprop_native/_core.pyi:499-557).  `rows`, when not NULL, is the caller's
+ * buffer of `rows_capacity` attempt rows of five doubles -- end, step, norm (infinity when
+ * not finite), accepted (1 or 0), wall seconds of the attempt -- filled with the call's
+ * attempts in order (`n_rows` of them; an attempt past the capacity is counted in the
+ * totals but not written). */
 typedef struct sp_batch {
-  int32_t event;       /* 0 none (work limit), 1 plane reached, 2 finished, 3 failed */
+  int32_t event;       /* SP_EVENT_* */
   int32_t plane_index; /* the save plane reached, or -1 */
   double z;            /* position after the batch */
   int64_t attempts, rejected, evaluations; /* cumulative counts of the run */
+  int32_t reason;      /* SP_REASON_* */
+  int32_t category;    /* SP_CATEGORY_*, on a failure */
+  double* rows;        /* caller's buffer of rows_capacity x 5 doubles, or NULL */
+  int32_t rows_capacity;
+  int32_t n_rows;      /* rows written by this call */
 } sp_batch;
+
+/* The march's state between calls (_core.Session.march_state / status,
+ * _core.pyi:470-476, 559-587). */
+typedef struct sp_march_state {
+  double z, proposal;
+  int64_t attempts, rejected, evaluations;
+  int32_t order;          /* Adams: the order the next attempt takes */
+  int32_t history_rows;   /* Adams: accepted rows held (0 right after a restart) */
+  int32_t rejections;     /* consecutive rejections */
+  int32_t plane_index;    /* the next save plane */
+  int32_t outcome;        /* 0 none, 1 completed, 2 stopped, 3 failed */
+} sp_march_state;
 
 /* ---- library ---- */
 /* Copies the message of the last failure on this thread into buf (NUL-terminated). */
@@ -172,10 +222,34 @@ void* sp_workspace_stream(sp_workspace* ws);
 
 /* ---- session (replaces _core.Session, _core.pyi:430-470) ---- */
 sp_status sp_session_start(sp_workspace* ws, const sp_run_desc* run, sp_session** out);
-/* Step until a save plane, the end, or work_limit attempts (the native call's bound). */
-sp_status sp_session_advance(sp_session* s, int32_t work_limit, sp_batch* out);
+/* Step until a save plane, the end, work_limit attempts or `deadline` host seconds (the
+ * native call's bounds, _core.pyi:469 Session.advance(work_limit, deadline); a deadline
+ * <= 0 or not finite means none), a requested stop or snapshot.  A failure returns its
+ * status with out->event SP_EVENT_FAILED and its reason and category filled; the
+ * attempts before it stand. */
+sp_status sp_session_advance(sp_session* s, int32_t work_limit, double deadline, sp_batch* out);
+/* Ask a running advance() -- from any thread -- to stop at the next attempt boundary
+ * (_core.Session.request_stop, _core.pyi:471): it returns SP_EVENT_STOPPED, and the run
+ * takes no more attempts. */
+sp_status sp_session_request_stop(sp_session* s);
+/* Ask advance() to return at the next accepted endpoint (SP_EVENT_HALTED), where a
+ * snapshot holds a consistent history (_core.Session.request_snapshot, _core.pyi:472). */
+sp_status sp_session_request_snapshot(sp_session* s);
+/* The march's state (_core.Session.march_state / status). */
+sp_status sp_session_march_state(const sp_session* s, sp_march_state* out);
 /* Copies the current state to out, host complex (n_modes, n_pol, n_omega). */
 sp_status sp_session_export(sp_session* s, double* out);
+/* The run's resumable state as one self-describing byte string (_core.Session.snapshot,
+ * _core.pyi:484-494; the Adams history rows of native trial_adams.inc:526-605): the
+ * march's scalars and history positions, the state, and the device history rows.  With
+ * buf NULL (or capacity too small) it writes the size needed to *size and copies nothing
+ * (SP_ERR_ARGUMENT when buf is not NULL). */
+sp_status sp_session_snapshot(sp_session* s, void* buf, size_t capacity, size_t* size);
+/* A session continuing a snapshot on a workspace of the same problem: the run's policy
+ * comes from `run` (its field0 may be NULL), everything else from the snapshot, and the
+ * continuation takes the bits the uninterrupted run would. */
+sp_status sp_session_restore(sp_workspace* ws, const sp_run_desc* run, const void* snapshot,
+                             size_t size, sp_session** out);
 sp_status sp_session_destroy(sp_session* s);
 
 /* Per-kernel device timing of a session (replaces the native timing probe and counters,

@@ -79,7 +79,24 @@ class SpRunDesc(C.Structure):
 
 class SpBatch(C.Structure):
     _fields_ = [("event", C.c_int32), ("plane_index", C.c_int32), ("z", C.c_double),
-                ("attempts", C.c_int64), ("rejected", C.c_int64), ("evaluations", C.c_int64)]
+                ("attempts", C.c_int64), ("rejected", C.c_int64), ("evaluations", C.c_int64),
+                ("reason", C.c_int32), ("category", C.c_int32),
+                ("rows", C.POINTER(C.c_double)), ("rows_capacity", C.c_int32),
+                ("n_rows", C.c_int32)]
+
+
+class SpMarchState(C.Structure):
+    _fields_ = [("z", C.c_double), ("proposal", C.c_double), ("attempts", C.c_int64),
+                ("rejected", C.c_int64), ("evaluations", C.c_int64), ("order", C.c_int32),
+                ("history_rows", C.c_int32), ("rejections", C.c_int32),
+                ("plane_index", C.c_int32), ("outcome", C.c_int32)]
+
+
+# sp_batch.event, .reason and .category (include/solprop_b200.h)
+EVENTS = {0: "none", 1: "plane", 2: "finished", 3: "failed", 4: "stopped", 5: "halted"}
+REASONS = {0: "reached", 3: "bound", 5: "floor", 6: "error", 7: "diverged", 11: "stopped",
+           12: "halted"}
+CATEGORIES = {0: "none", 1: "convergence", 2: "backend", 3: "value", 4: "refused"}
 
 
 class SpScanStatus(C.Structure):
@@ -119,7 +136,13 @@ SIGNATURES = {
     "sp_workspace_source_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_void_p]),
     "sp_workspace_launches_per_source": (C.c_int, [C.c_void_p]),
     "sp_session_start": (C.c_int, [C.c_void_p, C.POINTER(SpRunDesc), C.POINTER(C.c_void_p)]),
-    "sp_session_advance": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SpBatch)]),
+    "sp_session_advance": (C.c_int, [C.c_void_p, C.c_int32, C.c_double, C.POINTER(SpBatch)]),
+    "sp_session_request_stop": (C.c_int, [C.c_void_p]),
+    "sp_session_request_snapshot": (C.c_int, [C.c_void_p]),
+    "sp_session_march_state": (C.c_int, [C.c_void_p, C.POINTER(SpMarchState)]),
+    "sp_session_snapshot": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "sp_session_restore": (C.c_int, [C.c_void_p, C.POINTER(SpRunDesc), C.c_void_p, C.c_size_t,
+                                     C.POINTER(C.c_void_p)]),
     "sp_session_export": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "sp_session_destroy": (C.c_int, [C.c_void_p]),
     "sp_workspace_stream": (C.c_void_p, [C.c_void_p]),
@@ -160,6 +183,23 @@ class BackendRefusal(NativeError):
     """The library refuses this problem by name (``SP_ERR_REFUSED``)."""
 
 
+class ConvergenceError(NativeError):
+    """Step control fell below its floor or a replayed step diverged
+    (``SP_ERR_CONVERGENCE``; solprop's ``ConvergenceError`` category)."""
+
+
+class BackendError(NativeError):
+    """A device failure (``SP_ERR_CUDA``; solprop's ``BackendError`` category)."""
+
+
+class SessionLifecycleError(NativeError):
+    """A call out of the session's lifecycle (``SP_ERR_STATE``; native
+    ``_core.SessionLifecycleError``): after a failure, a stop or a close."""
+
+
+ERRORS = {2: BackendRefusal, 3: BackendError, 4: SessionLifecycleError, 5: ConvergenceError}
+
+
 def library() -> C.CDLL:
     """Load ``libsolprop_b200.so`` once; raise if it has not been built."""
     global _LIB
@@ -182,7 +222,7 @@ def check(status: int) -> None:
         buf = C.create_string_buffer(4096)
         library().sp_last_error(buf, 4096)
         message = buf.value.decode(errors="replace")
-        raise (BackendRefusal if status == 2 else NativeError)(status, message)
+        raise ERRORS.get(status, NativeError)(status, message)
 
 
 def _ptr(array: np.ndarray | None, ctype=C.c_double):
@@ -410,6 +450,10 @@ class Workspace:
     def start(self, policy: dict, *, field0=None, schedule=None) -> "Session":
         return Session(self, policy, field0=field0, schedule=schedule)
 
+    def restore(self, policy: dict, snapshot: bytes, *, schedule=None) -> "Session":
+        """A session continuing ``snapshot`` (``Session.snapshot``) under ``policy``."""
+        return Session(self, policy, schedule=schedule, snapshot=snapshot)
+
     def close(self):
         if getattr(self, "handle", None):
             self._lib.sp_workspace_destroy(self.handle)
@@ -421,19 +465,62 @@ class Workspace:
 class Session:
     """One run on a workspace (``sp_session``; native ``_core.Session``)."""
 
-    def __init__(self, ws: Workspace, policy: dict, *, field0=None, schedule=None):
+    def __init__(self, ws: Workspace, policy: dict, *, field0=None, schedule=None, snapshot=None):
         self.handle = None
         self._lib = library()
         self.ws = ws
         desc, keep = run_desc(ws.problem.record, policy, field0=field0, schedule=schedule)
         handle = C.c_void_p()
-        check(library().sp_session_start(ws.handle, C.byref(desc), C.byref(handle)))
+        if snapshot is None:
+            check(library().sp_session_start(ws.handle, C.byref(desc), C.byref(handle)))
+        else:
+            check(library().sp_session_restore(ws.handle, C.byref(desc), snapshot, len(snapshot),
+                                                C.byref(handle)))
         self.handle = handle
         self.batch = SpBatch()
 
-    def advance(self, work_limit: int = 256) -> SpBatch:
-        check(library().sp_session_advance(self.handle, int(work_limit), C.byref(self.batch)))
-        return self.batch
+    def advance(self, work_limit: int = 256, deadline: float = 0.0, *, rows: bool = False) -> SpBatch:
+        """Step until a save plane, the end, ``work_limit`` attempts or ``deadline`` host
+        seconds (0: none).  With ``rows`` the batch's ``attempt_rows`` holds one row per
+        attempt of this call: end, step, norm, accepted, wall seconds."""
+        b = self.batch
+        if rows:
+            buf = np.zeros((max(int(work_limit), 1), 5))
+            b.rows = buf.ctypes.data_as(C.POINTER(C.c_double))
+            b.rows_capacity = buf.shape[0]
+        else:
+            buf = None
+            b.rows = C.POINTER(C.c_double)()
+            b.rows_capacity = 0
+        try:
+            check(library().sp_session_advance(self.handle, int(work_limit), float(deadline),
+                                               C.byref(b)))
+        finally:
+            b.attempt_rows = None if buf is None else buf[: b.n_rows].copy()
+            b.rows = C.POINTER(C.c_double)()
+            b.rows_capacity = 0
+        return b
+
+    def request_stop(self) -> None:
+        """Stop at the next attempt boundary; safe from another thread."""
+        check(library().sp_session_request_stop(self.handle))
+
+    def request_snapshot(self) -> None:
+        """Return at the next accepted endpoint (event "halted") for a snapshot."""
+        check(library().sp_session_request_snapshot(self.handle))
+
+    def march_state(self) -> dict:
+        st = SpMarchState()
+        check(library().sp_session_march_state(self.handle, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in SpMarchState._fields_}
+
+    def snapshot(self) -> bytes:
+        """The run's resumable state (``Workspace.restore`` continues it)."""
+        size = C.c_size_t()
+        check(library().sp_session_snapshot(self.handle, None, 0, C.byref(size)))
+        buf = C.create_string_buffer(size.value)
+        check(library().sp_session_snapshot(self.handle, buf, size.value, C.byref(size)))
+        return buf.raw[: size.value]
 
     def set_timing(self, enable: bool) -> None:
         check(library().sp_session_set_timing(self.handle, int(enable)))

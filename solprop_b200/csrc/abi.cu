@@ -6,6 +6,7 @@
 // from the norms the device reduces, one device synchronisation per attempt, as the
 // reference's native march does (native/src/march/adams_march.cpp, rk_march.cpp).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -29,7 +30,9 @@ thread_local std::string g_error;
 
 struct Failure : std::runtime_error {
   sp_status code;
-  Failure(sp_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+  int reason;  // SP_REASON_* a session reports for it
+  Failure(sp_status c, const std::string& m, int r = SP_REASON_ERROR)
+      : std::runtime_error(m), code(c), reason(r) {}
 };
 
 #define CUDA_CHECK(call)                                                                    \
@@ -733,6 +736,14 @@ struct sp_session {
   bool last_rejected = false;
   // RK
   std::vector<double> norms_hist;
+  // the last attempt, for the batch's attempt rows: end, step, norm, accepted
+  struct Row {
+    double end = 0, step = 0, norm = 0;
+    bool accepted = false;
+  } row;
+  // requests from other threads, polled between attempts
+  std::atomic<bool> stop_requested{false}, snapshot_requested{false};
+  bool stopped = false;
 };
 
 static void adams_start(sp_session* S) {
@@ -770,7 +781,7 @@ static double limit_step(double dz, double factor, double dz_min, double dz_max)
     char buf[160];
     std::snprintf(buf, sizeof buf, "step control asked for %.3e m, below the floor dz_min = %.3e m",
                   proposed, dz_min);
-    throw Failure(SP_ERR_CONVERGENCE, buf);
+    throw Failure(SP_ERR_CONVERGENCE, buf, SP_REASON_FLOOR);
   }
   return proposed;
 }
@@ -897,6 +908,7 @@ static bool decide_attempt(sp_session* S, const Pending& pd, const double* sums)
   const double norm = norms[0];
   const int order = pd.order;
   const double dz = pd.dz;
+  S->row = {pd.end, dz, norm, false};
   auto factor = [&](double nm, int o, double growth) {
     if (nm <= 0.0) return growth;
     double raw = R.safety * std::pow(nm, -1.0 / (o + 1));
@@ -948,6 +960,7 @@ static bool decide_attempt(sp_session* S, const Pending& pd, const double* sums)
   }
   S->order = stored;
   S->last_rejected = false;
+  S->row.accepted = true;
   S->z = pd.end;
   if (pd.kink) S->history.clear();
   S->proposal = limit_step(dz, factor(cnorm, control, R.max_growth), R.dz_min, R.dz_max);
@@ -1161,6 +1174,7 @@ static void rk_adaptive_attempt(sp_session* S, double target) {
   const double equivalent = std::isfinite(norm) ? norm * std::pow(S->proposal / dz, q1) : norm;
   const bool accepted = std::isfinite(norm) && norm <= 1.0;
   const double end = stop.landed ? stop.target : S->z + dz;
+  S->row = {end, dz, norm, accepted};
   if (accepted) {
     rk_accept(S);
     S->z = end;
@@ -1366,21 +1380,50 @@ sp_status sp_session_start(sp_workspace* ws, const sp_run_desc* run, sp_session*
   });
 }
 
-sp_status sp_session_advance(sp_session* S, int32_t work_limit, sp_batch* out) {
+static int category_of(sp_status code) {
+  switch (code) {
+    case SP_ERR_CONVERGENCE: return SP_CATEGORY_CONVERGENCE;
+    case SP_ERR_CUDA: return SP_CATEGORY_BACKEND;
+    case SP_ERR_REFUSED: return SP_CATEGORY_REFUSED;
+    default: return SP_CATEGORY_VALUE;
+  }
+}
+
+sp_status sp_session_advance(sp_session* S, int32_t work_limit, double deadline, sp_batch* out) {
   return guarded([&] {
     if (!S || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    if (out->rows && out->rows_capacity < 0) throw Failure(SP_ERR_ARGUMENT, "negative rows_capacity");
     if (S->failed) throw Failure(SP_ERR_STATE, "the session failed; close it");
+    if (S->stopped) throw Failure(SP_ERR_STATE, "the session was stopped; close it");
     CUDA_CHECK(cudaSetDevice(S->ws->device));
-    out->event = 0;
+    out->event = SP_EVENT_NONE;
     out->plane_index = -1;
+    out->reason = SP_REASON_BOUND;
+    out->category = SP_CATEGORY_NONE;
+    out->n_rows = 0;
     const sp_run_desc& R = S->run;
+    const auto t_call = std::chrono::steady_clock::now();
+    const bool timed = std::isfinite(deadline) && deadline > 0.0;
+    auto counts = [&] {
+      out->z = S->z;
+      out->attempts = S->attempts;
+      out->rejected = S->rejected;
+      out->evaluations = S->evaluations;
+    };
     int done = 0;
     try {
       if (!S->finished && reached(S->z, R.z_end)) {
         S->finished = true;
-        out->event = 2;
+        out->event = SP_EVENT_FINISHED;
+        out->reason = SP_REASON_REACHED;
       }
       while (!S->finished && done < work_limit) {
+        if (S->stop_requested.load()) {
+          S->stopped = true;
+          out->event = SP_EVENT_STOPPED;
+          out->reason = SP_REASON_STOPPED;
+          break;
+        }
         // the next stop: a save plane or the end
         double target = R.z_end;
         int plane = -1;
@@ -1391,8 +1434,14 @@ sp_status sp_session_advance(sp_session* S, int32_t work_limit, sp_batch* out) {
           target = S->planes[S->plane_cursor];
           plane = S->plane_cursor;
         }
+        const auto t_attempt = std::chrono::steady_clock::now();
         if (!S->schedule.empty()) {
-          if (S->sched_cursor >= (int)S->schedule.size()) { S->finished = true; out->event = 2; break; }
+          if (S->sched_cursor >= (int)S->schedule.size()) {
+            S->finished = true;
+            out->event = SP_EVENT_FINISHED;
+            out->reason = SP_REASON_REACHED;
+            break;
+          }
           const double dz = S->schedule[S->sched_cursor];
           const double end = S->sched_edges[S->sched_cursor + 1];
           if (R.method == 0) {
@@ -1400,7 +1449,9 @@ sp_status sp_session_advance(sp_session* S, int32_t work_limit, sp_batch* out) {
             adams_attempt(S, dz, end, false, true);
           } else {
             double nm = rk_trial(S, dz);
-            if (!std::isfinite(nm)) throw Failure(SP_ERR_CONVERGENCE, "a replayed step diverged");
+            S->row = {end, dz, nm, true};
+            if (!std::isfinite(nm))
+              throw Failure(SP_ERR_CONVERGENCE, "a replayed step diverged", SP_REASON_DIVERGED);
             rk_accept(S);
             S->z = end;
           }
@@ -1411,6 +1462,15 @@ sp_status sp_session_advance(sp_session* S, int32_t work_limit, sp_batch* out) {
           rk_adaptive_attempt(S, target);
         }
         ++done;
+        const auto t_now = std::chrono::steady_clock::now();
+        if (out->rows && out->n_rows < out->rows_capacity) {
+          double* r = out->rows + (size_t)5 * out->n_rows++;
+          r[0] = S->row.end;
+          r[1] = S->row.step;
+          r[2] = std::isfinite(S->row.norm) ? S->row.norm : INFINITY;
+          r[3] = S->row.accepted ? 1.0 : 0.0;
+          r[4] = std::chrono::duration<double>(t_now - t_attempt).count();
+        }
         const bool on_plane =
             plane >= 0 && std::fabs(S->z - S->planes[plane]) <=
                               std::max(1e-9 * std::fabs(R.z_end), kLandingUlps * ulp(S->planes[plane]));
@@ -1420,23 +1480,210 @@ sp_status sp_session_advance(sp_session* S, int32_t work_limit, sp_batch* out) {
         }
         if (reached(S->z, R.z_end)) {
           S->finished = true;
-          out->event = 2;
+          out->event = SP_EVENT_FINISHED;
+          out->reason = SP_REASON_REACHED;
           break;
         }
         if (on_plane) {
-          out->event = 1;
+          out->event = SP_EVENT_PLANE;
+          out->reason = SP_REASON_REACHED;
           break;
         }
+        if (S->row.accepted && S->snapshot_requested.exchange(false)) {
+          out->event = SP_EVENT_HALTED;
+          out->reason = SP_REASON_HALTED;
+          break;
+        }
+        if (timed && std::chrono::duration<double>(t_now - t_call).count() >= deadline) break;
       }
-    } catch (const Failure&) {
+    } catch (const Failure& f) {
       S->failed = true;
-      out->event = 3;
+      out->event = SP_EVENT_FAILED;
+      out->reason = f.reason;
+      out->category = category_of(f.code);
+      counts();
       throw;
     }
+    counts();
+  });
+}
+
+sp_status sp_session_request_stop(sp_session* S) {
+  if (!S) return SP_ERR_ARGUMENT;
+  S->stop_requested.store(true);
+  return SP_OK;
+}
+
+sp_status sp_session_request_snapshot(sp_session* S) {
+  if (!S) return SP_ERR_ARGUMENT;
+  S->snapshot_requested.store(true);
+  return SP_OK;
+}
+
+sp_status sp_session_march_state(const sp_session* S, sp_march_state* out) {
+  return guarded([&] {
+    if (!S || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
     out->z = S->z;
+    out->proposal = S->proposal;
     out->attempts = S->attempts;
     out->rejected = S->rejected;
     out->evaluations = S->evaluations;
+    out->order = S->order;
+    out->history_rows = (int32_t)S->history.size();
+    out->rejections = S->rejections;
+    out->plane_index = S->plane_cursor;
+    out->outcome = S->failed ? 3 : S->stopped ? 2 : S->finished ? 1 : 0;
+  });
+}
+
+// ---- snapshots: the march's scalars, its history positions and the device rows a later
+// attempt reads (the state, the Adams history rows of sources, and with a varying
+// operator the rows of states and rates), as one byte string with a header that names
+// the problem's shape, so that a restore on another problem is refused.
+namespace {
+struct SnapshotHeader {
+  char magic[8];
+  int32_t version, method, compensated, n_slots;
+  int64_t n, n_modes, n_pol, n_omega;
+  double z, proposal;
+  int64_t attempts, rejected, evaluations;
+  int32_t plane_cursor, sched_cursor, finished, rejections, order, last_rejected;
+  int64_t n_history, n_norms;
+};
+constexpr char kSnapshotMagic[8] = {'s', 'p', 's', 'n', 'a', 'p', '\0', '\0'};
+
+struct SnapshotLayout {
+  size_t history, norms, state, rows, total;
+  int row_buffers;  // device row buffers after the state: 0 (RK), 1 (store) or 3
+};
+
+SnapshotLayout snapshot_layout(int method, bool compensated, size_t n, size_t n_history, size_t n_norms) {
+  SnapshotLayout L{};
+  L.history = sizeof(SnapshotHeader);
+  L.norms = L.history + n_history * 2 * sizeof(double);
+  L.state = L.norms + n_norms * sizeof(double);
+  L.rows = L.state + n * sizeof(double2);
+  L.row_buffers = method == 0 ? (compensated ? 3 : 1) : 0;
+  L.total = L.rows + (size_t)L.row_buffers * kMaxSlots * n * sizeof(double2);
+  return L;
+}
+}  // namespace
+
+sp_status sp_session_snapshot(sp_session* S, void* buf, size_t capacity, size_t* size) {
+  return guarded([&] {
+    if (!S || !size) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    if (S->failed) throw Failure(SP_ERR_STATE, "the session failed; there is nothing to resume");
+    sp_workspace* ws = S->ws;
+    const sp_problem& P = *ws->P;
+    const bool comp = S->run.method == 0 && P.d.phi_expansion;
+    const SnapshotLayout L =
+        snapshot_layout(S->run.method, comp, P.n, S->history.size(), S->norms_hist.size());
+    *size = L.total;
+    if (!buf) return;
+    if (capacity < L.total) throw Failure(SP_ERR_ARGUMENT, "the snapshot buffer is too small");
+    CUDA_CHECK(cudaSetDevice(ws->device));
+    unsigned char* b = static_cast<unsigned char*>(buf);
+    SnapshotHeader h{};
+    std::memcpy(h.magic, kSnapshotMagic, sizeof h.magic);
+    h.version = 1;
+    h.method = S->run.method;
+    h.compensated = comp;
+    h.n_slots = kMaxSlots;
+    h.n = (int64_t)P.n;
+    h.n_modes = P.d.n_modes;
+    h.n_pol = P.d.n_pol;
+    h.n_omega = P.d.n_omega;
+    h.z = S->z;
+    h.proposal = S->proposal;
+    h.attempts = S->attempts;
+    h.rejected = S->rejected;
+    h.evaluations = S->evaluations;
+    h.plane_cursor = S->plane_cursor;
+    h.sched_cursor = S->sched_cursor;
+    h.finished = S->finished;
+    h.rejections = S->rejections;
+    h.order = S->order;
+    h.last_rejected = S->last_rejected;
+    h.n_history = (int64_t)S->history.size();
+    h.n_norms = (int64_t)S->norms_hist.size();
+    std::memcpy(b, &h, sizeof h);
+    double* hist = reinterpret_cast<double*>(b + L.history);
+    for (size_t i = 0; i < S->history.size(); ++i) {
+      hist[2 * i] = S->history[i].first;
+      hist[2 * i + 1] = (double)S->history[i].second;
+    }
+    if (!S->norms_hist.empty())
+      std::memcpy(b + L.norms, S->norms_hist.data(), S->norms_hist.size() * sizeof(double));
+    const size_t row = P.n * sizeof(double2);
+    CUDA_CHECK(cudaMemcpyAsync(b + L.state, ws->state.p, row, cudaMemcpyDeviceToHost, ws->stream));
+    const double2* rows[3] = {ws->store.p, ws->states.p, ws->rates.p};
+    for (int k = 0; k < L.row_buffers; ++k)
+      CUDA_CHECK(cudaMemcpyAsync(b + L.rows + (size_t)k * kMaxSlots * row, rows[k], kMaxSlots * row,
+                                 cudaMemcpyDeviceToHost, ws->stream));
+    CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+  });
+}
+
+sp_status sp_session_restore(sp_workspace* ws, const sp_run_desc* run, const void* snapshot,
+                             size_t size, sp_session** out) {
+  return guarded([&] {
+    if (!ws || !run || !snapshot || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    if (size < sizeof(SnapshotHeader)) throw Failure(SP_ERR_ARGUMENT, "not a snapshot: too short");
+    SnapshotHeader h;
+    std::memcpy(&h, snapshot, sizeof h);
+    if (std::memcmp(h.magic, kSnapshotMagic, sizeof h.magic) != 0 || h.version != 1)
+      throw Failure(SP_ERR_ARGUMENT, "not a snapshot of this library");
+    const sp_problem& P = *ws->P;
+    if (h.method != run->method) throw Failure(SP_ERR_ARGUMENT, "the snapshot is of another method");
+    if (h.n != (int64_t)P.n || h.n_modes != P.d.n_modes || h.n_pol != P.d.n_pol ||
+        h.n_omega != P.d.n_omega || h.n_slots != kMaxSlots ||
+        h.compensated != (run->method == 0 && P.d.phi_expansion))
+      throw Failure(SP_ERR_ARGUMENT, "the snapshot is of another problem");
+    if (h.n_history < 0 || h.n_norms < 0 || h.n_history > kMaxSlots)
+      throw Failure(SP_ERR_ARGUMENT, "a corrupt snapshot");
+    const SnapshotLayout L = snapshot_layout(h.method, h.compensated, P.n, (size_t)h.n_history,
+                                             (size_t)h.n_norms);
+    if (size < L.total) throw Failure(SP_ERR_ARGUMENT, "a truncated snapshot");
+    // start the session as sp_session_start does, with the snapshot's state as the field
+    const unsigned char* b = static_cast<const unsigned char*>(snapshot);
+    sp_run_desc r = *run;
+    r.field0 = reinterpret_cast<const double*>(b + L.state);
+    sp_session* raw = nullptr;
+    const sp_status st = sp_session_start(ws, &r, &raw);
+    if (st != SP_OK) throw Failure(st, g_error);
+    std::unique_ptr<sp_session> S(raw);
+    S->run.field0 = nullptr;  // the caller's pointer is not kept
+    // the state exactly as saved (the start masked it: the saved one is already masked)
+    const size_t row = P.n * sizeof(double2);
+    CUDA_CHECK(cudaMemcpyAsync(ws->state.p, b + L.state, row, cudaMemcpyHostToDevice, ws->stream));
+    double2* rows[3] = {ws->store.p, ws->states.p, ws->rates.p};
+    for (int k = 0; k < L.row_buffers; ++k)
+      CUDA_CHECK(cudaMemcpyAsync(rows[k], b + L.rows + (size_t)k * kMaxSlots * row, kMaxSlots * row,
+                                 cudaMemcpyHostToDevice, ws->stream));
+    S->z = h.z;
+    S->proposal = h.proposal;
+    S->attempts = h.attempts;
+    S->rejected = h.rejected;
+    S->evaluations = h.evaluations;
+    S->plane_cursor = h.plane_cursor;
+    S->sched_cursor = h.sched_cursor;
+    S->finished = h.finished != 0;
+    S->rejections = h.rejections;
+    S->order = h.order;
+    S->last_rejected = h.last_rejected != 0;
+    const double* hist = reinterpret_cast<const double*>(b + L.history);
+    S->history.clear();
+    for (int64_t i = 0; i < h.n_history; ++i) {
+      const int slot = (int)hist[2 * i + 1];
+      if (slot < 0 || slot >= kMaxSlots) throw Failure(SP_ERR_ARGUMENT, "a corrupt snapshot");
+      S->history.push_back({hist[2 * i], slot});
+    }
+    S->norms_hist.assign(reinterpret_cast<const double*>(b + L.norms),
+                         reinterpret_cast<const double*>(b + L.norms) + h.n_norms);
+    if (S->sched_cursor < 0 || S->sched_cursor > (int)S->schedule.size() || S->plane_cursor < 0)
+      throw Failure(SP_ERR_ARGUMENT, "the snapshot's cursors do not fit the run");
+    CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+    *out = S.release();
   });
 }
 
@@ -2330,6 +2577,9 @@ sp_status sp_scan_run(sp_scan* S, int32_t run, double* state, sp_batch* info) {
       info->attempts = ss->attempts;
       info->rejected = ss->rejected;
       info->evaluations = ss->evaluations;
+      info->reason = ss->failed ? SP_REASON_ERROR : ss->finished ? SP_REASON_REACHED : SP_REASON_BOUND;
+      info->category = ss->failed ? SP_CATEGORY_BACKEND : SP_CATEGORY_NONE;
+      info->n_rows = 0;
     }
   });
 }

@@ -10,8 +10,9 @@ of the reference's ``numpy_ref`` backend.
 On the CPU: the restated shot-noise draw (``scan.input_noise``) gives the reference's
 realisation bit for bit, and the oracle reproduces the reference's launch state, source
 evaluation and attempts.  On the GPU: a batched scan of the four runs, in both column
-forms and both transform forms, lands every run on the reference's state after 24
-attempts at 1e-10 relative L2, with the reference's attempt and rejection counts.
+forms and with the transforms in one CTA per row or over clusters, lands every run on
+the reference's state after 24 attempts at 1e-10 relative L2, with the reference's
+attempt and rejection counts.
 """
 
 import numpy as np
@@ -67,20 +68,24 @@ def test_oracle_attempts_match_the_reference(case):
     assert rel(ws.state, g["attempts.state"]) < 1e-13
 
 
+# the transforms' forms per grid size, (inverse, forward): 0 is one CTA per row, k a
+# cluster of k CTAs; an FP64 row of 32768 samples needs 2 CTAs inverse and 4 forward
+NARROW = {4096: (0, 0), 8192: (0, 0), 16384: (0, 0), 32768: (2, 4)}
+WIDE = {8192: (2, 2), 16384: (4, 4), 32768: (4, 8)}
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("form", ["tiles", "sweep"])
-@pytest.mark.parametrize("cluster", [0, 2])
-def test_batched_scan_matches_the_reference_after_24_attempts(form, cluster):
+@pytest.mark.parametrize("transforms", ["narrow", "wide"])
+def test_batched_scan_matches_the_reference_after_24_attempts(form, transforms):
     from solprop_b200 import _lib
 
     recs = [record(c) for c in CASES]
     pols = [policy(golden(c), "adaptive") for c in CASES]
     sc = _lib.Scan(recs, pols)
     sc.set_column(form)
-    for n_to in sorted({r.n_to for r in recs}):
-        # one CTA per row, or 2-CTA clusters, where the row admits them
-        if cluster == 0 or n_to >= 8192:
-            sc.set_transforms(n_to, cluster, cluster)
+    for n_to, (inverse, forward) in (NARROW if transforms == "narrow" else WIDE).items():
+        sc.set_transforms(n_to, inverse, forward)
     steps = int(golden(CASES[0])["attempts.counts"][0])
     sc.advance(steps)
     for i, case in enumerate(CASES):
