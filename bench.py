@@ -272,8 +272,16 @@ def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024
         e_ev.record(stream)
         torch.cuda.synchronize()
         attempts, ms = across_ranks(status.attempts - before, s_ev.elapsed_time(e_ev))
+        # the families' device times over a few more batch steps, events around each
+        sc.set_timing(True)
+        sc.timing(reset=True)
+        timed_steps = 5
+        sc.advance(timed_steps)
+        families = sc.timing(reset=True)
+        sc.set_timing(False)
         batched[precision] = {"attempts_per_s": attempts / (ms / 1e3),
                               "ms_per_batch_step": ms / steps, "active_runs_at_end": status.active,
+                              "roofline": scan_roofline(records, families, timed_steps, precision),
                               "transform_plan": sc.describe().strip().splitlines()}
         sc.close()
     # the plain path: each run alone, three attempts after one warm-up
@@ -307,11 +315,68 @@ def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024
             "speedup_vs_plain": {k: v["attempts_per_s"] / plain for k, v in batched.items()}}
 
 
-def complete_scan_leg(device: int, n_runs: int, seed: int = 2024, rank: int = 0, world: int = 1) -> dict:
+def scan_roofline(records, families: dict, steps: int, precision: str) -> dict:
+    """Achieved bandwidth of each batched family over the timed batch steps: its
+    algorithmic bytes per batch step (every run in the batch, the byte counts below) over
+    its CUDA-event time, against the measured copy bandwidth.  Per run, with n the state's
+    complex elements, c its modal columns, T its fine samples, r the transforms' and the
+    column's real size (8 in FP64, 4 in the mixed form), P its prefactor terms:
+    predict 14 x 16 n (state, five history rows, lab, six moments, flow, exponent),
+    correct 15 x 16 n, accept 4 x 16 n; inverse 16 n + 2 x 8 c T (lab in, the modal field
+    and the collar's stream out, FP64 in both forms); column 8 c T + 3 r c T (modal field
+    in, three projected streams out); forward 4 r c T + 8 r n (four streams in, four
+    spectra out); output 8 r n + (P + 2) 16 n."""
+    r = 8 if precision == "fp64" else 4
+    bytes_ = dict.fromkeys(("adams_predict", "inverse_fft", "response_column", "forward_fft",
+                            "stage_output", "adams_correct", "adams_accept"), 0.0)
+    for rec in records:
+        n, c, T, P = rec.n_cols * rec.n_omega, rec.n_cols, rec.n_to, rec.prefactor_terms.shape[0]
+        bytes_["adams_predict"] += 14 * 16 * n
+        bytes_["adams_correct"] += 15 * 16 * n
+        bytes_["adams_accept"] += 4 * 16 * n
+        bytes_["inverse_fft"] += 16 * n + 2 * 8 * c * T
+        bytes_["response_column"] += 8 * c * T + 3 * r * c * T
+        bytes_["forward_fft"] += 4 * r * c * T + 8 * r * n
+        bytes_["stage_output"] += 8 * r * n + (P + 2) * 16 * n
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    out = {}
+    for name, b in bytes_.items():
+        ms, launches = families.get(name, (0.0, 0))
+        if not launches:
+            continue
+        per_step_ms = ms / steps
+        achieved = b / (per_step_ms * 1e-3) / 1e9
+        out[name] = {"algorithmic_bytes": b, "ms_per_batch_step": per_step_ms,
+                     "achieved_gbs": achieved, "frac": achieved / peak}
+    top = max(out, key=lambda k: out[k]["ms_per_batch_step"])
+    return {"bound": "hbm", "kernel": top, "achieved": out[top]["achieved_gbs"], "peak": peak,
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "unit": "GB/s",
+            "frac": out[top]["frac"], "families": out}
+
+
+def run_errors(mixed: list, reference: list, records) -> dict:
+    """Relative L2 of each mixed-precision run's final state against the plain FP64 run of
+    the same point: in the spectrum, and in time (the fields the states make)."""
+    spectral, temporal = [], []
+    for a, b, rec in zip(mixed, reference, records):
+        spectral.append(float(np.linalg.norm(a - b) / np.linalg.norm(b)))
+        ta = np.fft.irfft(a.reshape(-1, a.shape[-1]), n=rec.n_t, axis=-1)
+        tb = np.fft.irfft(b.reshape(-1, b.shape[-1]), n=rec.n_t, axis=-1)
+        temporal.append(float(np.linalg.norm(ta - tb) / np.linalg.norm(tb)))
+    spectral, temporal = np.array(spectral), np.array(temporal)
+    return {"spectral_max": float(spectral.max()), "spectral_median": float(np.median(spectral)),
+            "temporal_max": float(temporal.max()), "temporal_median": float(np.median(temporal)),
+            "runs_at_most_1e-6": int((spectral <= 1e-6).sum()), "runs": int(spectral.size)}
+
+
+def complete_scan_leg(device: int, n_runs: int, seed: int = 2024, rank: int = 0, world: int = 1,
+                      batched_fp64: bool = True) -> dict:
     """The scan's first n_runs points solved to the end, in runs per second: the batched
-    mixed solver (re-planning as runs finish, long runs going on alone) against the plain
-    FP64 path solving the same runs one after another.  Host wall time around the stepping
-    (creation excluded on both sides), slowest rank's for the batched side."""
+    mixed solver (re-planning as runs finish, long runs going on alone), and the batched
+    FP64 solver, against the plain FP64 path solving the same runs one after another.
+    Host wall time around the stepping (creation excluded on all sides), slowest rank's
+    for the batched sides; every mixed run's final state against its plain FP64 run's."""
     import time
 
     import torch
@@ -322,19 +387,26 @@ def complete_scan_leg(device: int, n_runs: int, seed: int = 2024, rank: int = 0,
     points = [points[i] for i in scan.shard(points, rank, world)]
     built = [scan.capillary_record(p) for p in points]
     records, policies = [b[0] for b in built], [b[1] for b in built]
-    sc = _lib.Scan(records, policies, device, "mixed")
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    while sc.advance(1000).active:
-        pass
-    torch.cuda.synchronize()
-    batched_s = time.perf_counter() - t0
-    infos = [sc.run(i, state=False)[1] for i in range(len(records))]
-    batched_attempts = sum(int(i.attempts) for i in infos)
-    finished = sum(int(i.event) == 2 for i in infos)
-    plan = [line for line in sc.describe().splitlines() if line.startswith("work lists")]
-    sc.close()
-    plain_s, plain_attempts = 0.0, 0
+    sides = {}
+    finals = {}
+    for precision in ("mixed", "fp64") if batched_fp64 else ("mixed",):
+        sc = _lib.Scan(records, policies, device, precision)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        while sc.advance(1000).active:
+            pass
+        torch.cuda.synchronize()
+        seconds = time.perf_counter() - t0
+        runs = [sc.run(i) for i in range(len(records))]
+        finals[precision] = [state for state, _ in runs]
+        sides[precision] = {
+            "seconds": seconds, "attempts": sum(int(i.attempts) for _, i in runs),
+            "finished": sum(int(i.event) == 2 for _, i in runs),
+            "plan": [line for line in sc.describe().splitlines() if line.startswith("work lists")]}
+        sc.close()
+    batched_s = sides["mixed"]["seconds"]
+    finished = sides["mixed"]["finished"]
+    plain_s, plain_attempts, plain_finals = 0.0, 0, []
     for rec, pol in zip(records, policies):
         problem = _lib.Problem(rec)
         ws = _lib.Workspace(problem, device)
@@ -346,21 +418,32 @@ def complete_scan_leg(device: int, n_runs: int, seed: int = 2024, rank: int = 0,
         torch.cuda.synchronize()
         plain_s += time.perf_counter() - t0
         plain_attempts += int(session.batch.attempts)
+        plain_finals.append(session.export())
         session.close()
         ws.close()
         problem.close()
+    errors = run_errors(finals["mixed"], plain_finals, records)
+    batched64_s = sides["fp64"]["seconds"] if "fp64" in sides else None
     if world > 1:
         import torch.distributed as dist
 
-        t = torch.tensor([batched_s, plain_s], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        batched_s, plain_s = float(t[0].item()), float(t[1].item())
-    return {"runs": n_runs, "finished": finished * world if world > 1 else finished,
-            "batched_mixed": {"seconds": batched_s, "runs_per_s": n_runs / batched_s,
-                              "attempts": batched_attempts, "plan": plan},
-            "plain_fp64": {"seconds": plain_s, "runs_per_s": n_runs / plain_s, "attempts": plain_attempts},
-            "runs_per_s_ratio": plain_s / batched_s}
+        t = torch.tensor([batched_s, batched64_s or 0.0, plain_s], dtype=torch.float64,
+                         device=f"cuda:{device}")
+        dist.all_reduce(t[:2], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[2:], op=dist.ReduceOp.SUM)
+        batched_s, plain_s = float(t[0].item()), float(t[2].item())
+        batched64_s = float(t[1].item()) if batched64_s is not None else None
+    out = {"runs": n_runs, "finished": finished * world if world > 1 else finished,
+           "batched_mixed": {"seconds": batched_s, "runs_per_s": n_runs / batched_s,
+                             "attempts": sides["mixed"]["attempts"], "plan": sides["mixed"]["plan"]},
+           "plain_fp64": {"seconds": plain_s, "runs_per_s": n_runs / plain_s, "attempts": plain_attempts},
+           "runs_per_s_ratio": plain_s / batched_s,
+           "mixed_vs_fp64": errors}
+    if batched64_s is not None:
+        out["batched_fp64"] = {"seconds": batched64_s, "runs_per_s": n_runs / batched64_s,
+                               "attempts": sides["fp64"]["attempts"], "plan": sides["fp64"]["plan"],
+                               "runs_per_s_ratio": plain_s / batched64_s}
+    return out
 
 
 def main() -> int:
@@ -372,15 +455,30 @@ def main() -> int:
     parser.add_argument("--cpu-budget", type=float, default=20.0)
     parser.add_argument("--scan-runs", type=int, default=256)
     parser.add_argument("--scan-steps", type=int, default=30)
-    parser.add_argument("--complete-runs", type=int, default=32,
+    parser.add_argument("--complete-runs", type=int, default=256,
                         help="scan runs solved to the end for the runs/s comparison (0: skip)")
     parser.add_argument("--config2-only", action="store_true",
                         help="measure config 2 alone (no runs, surrogate or scan legs), e.g. under ncu")
+    parser.add_argument("--scan-only", type=int, default=0, metavar="RUNS",
+                        help="only the full-batch scan leg over RUNS runs (--scan-steps batch "
+                             "steps after --warmup), e.g. under ncu; prints its JSON")
+    parser.add_argument("--surrogate-only", type=int, default=0, metavar="POINTS",
+                        help="only the surrogate's tcgen05 inference over POINTS points; prints its JSON")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.scan_only or args.surrogate_only:
+        import torch
+
+        torch.cuda.set_device(local)
+        if args.scan_only:
+            result = scan_leg(local, args.scan_only, args.scan_steps, warmup=args.warmup)
+        else:
+            result = surrogate_leg(local, points=args.surrogate_only)
+        print(json.dumps(result), flush=True)
+        return 0
     rec, pol = load_workload()
     config = {"workload": "config2: 4-mode He capillary 1.5 m 0.8->0 bar, n_to 16384, 64 nodes",
               "state": [rec.n_modes, rec.n_pol, rec.n_omega], "n_to": rec.n_to,

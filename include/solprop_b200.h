@@ -289,6 +289,13 @@ sp_status sp_scan_advance(sp_scan* scan, int32_t steps, sp_scan_status* out);
 /* One run's state (host complex, may be NULL) and counts (event 2: finished, 3: failed). */
 sp_status sp_scan_run(sp_scan* scan, int32_t run, double* state, sp_batch* info);
 void* sp_scan_stream(sp_scan* scan);
+/* Per-family device timing of a scan's batch steps (the session's SP_K_* families: the
+ * batched predictor, inverse transforms, response column, forward transforms, stage
+ * output, corrector and accept).  While enabled, CUDA events are recorded around every
+ * batched launch family and the attempt phase runs as plain launches instead of its
+ * captured graph.  No counterpart in the reference. */
+sp_status sp_scan_set_timing(sp_scan* scan, int enable);
+sp_status sp_scan_timing(sp_scan* scan, double* ms, int64_t* launches, int reset);
 /* The scan's plan, as text: whether the attempt phase runs as one captured CUDA graph,
  * the response column's form, the host's time per batch step so far, and per grid size
  * whether the inverse and forward transforms run in one CTA per row or over a cluster of

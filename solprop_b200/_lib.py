@@ -161,6 +161,8 @@ SIGNATURES = {
     "sp_scan_set_transforms": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
     "sp_scan_run": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(SpBatch)]),
     "sp_scan_stream": (C.c_void_p, [C.c_void_p]),
+    "sp_scan_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "sp_scan_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]),
     "sp_scan_destroy": (C.c_int, [C.c_void_p]),
 }
 
@@ -611,6 +613,18 @@ class Scan:
     @property
     def stream(self) -> int:
         return int(library().sp_scan_stream(self.handle) or 0)
+
+    def set_timing(self, enable: bool) -> None:
+        """Events around every batched launch family of the batch steps that follow."""
+        check(library().sp_scan_set_timing(self.handle, int(enable)))
+
+    def timing(self, reset: bool = False) -> dict:
+        """Accumulated device milliseconds and launch counts per kernel family."""
+        n = len(KERNEL_NAMES)
+        ms = (C.c_double * n)()
+        counts = (C.c_int64 * n)()
+        check(library().sp_scan_timing(self.handle, ms, counts, int(reset)))
+        return {name: (ms[i], counts[i]) for i, name in enumerate(KERNEL_NAMES)}
 
     def close(self):
         if getattr(self, "handle", None):

@@ -1832,8 +1832,17 @@ struct sp_scan {
   // CUDA graph, captured at the first attempt and replayed at every later one
   cudaGraphExec_t attempt_graph = nullptr;
   bool graph_failed = false;
+  // per-family device timing (sp_scan_set_timing): events around every batched launch
+  // family, the attempt phase launched plainly meanwhile
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+  size_t ev_next = 0;
+  double t_ms[SP_K_COUNT] = {};
+  int64_t t_count[SP_K_COUNT] = {};
   ~sp_scan() {
     if (stream) cudaStreamSynchronize(stream);
+    for (auto e : ev_pool) cudaEventDestroy(e);
     if (attempt_graph) cudaGraphExecDestroy(attempt_graph);
     for (void* p : {(void*)h_adams_start, (void*)h_adams_att, (void*)h_stages_start,
                     (void*)h_stages_att, (void*)h_norms, (void*)h_flag_start, (void*)h_flag_att,
@@ -1850,6 +1859,41 @@ namespace {
 template <class T>
 void upload_all(DevBuf<T>& dev, const T* host, size_t n, cudaStream_t s) {
   CUDA_CHECK(cudaMemcpyAsync(dev.p, host, n * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+// One batched launch family, with events around it while the scan's timing is on.
+template <class F>
+void timed_family(sp_scan* S, int kind, F&& launch) {
+  if (!S->timing) {
+    launch();
+    return;
+  }
+  auto event = [&] {
+    if (S->ev_next == S->ev_pool.size()) {
+      cudaEvent_t e;
+      CUDA_CHECK(cudaEventCreate(&e));
+      S->ev_pool.push_back(e);
+    }
+    return S->ev_pool[S->ev_next++];
+  };
+  cudaEvent_t a = event(), b = event();
+  CUDA_CHECK(cudaEventRecord(a, S->stream));
+  launch();
+  CUDA_CHECK(cudaEventRecord(b, S->stream));
+  S->ev_pending.push_back({kind, {a, b}});
+}
+
+void flush_scan_timing(sp_scan* S) {
+  if (S->ev_pending.empty()) return;
+  CUDA_CHECK(cudaStreamSynchronize(S->stream));
+  for (auto& p : S->ev_pending) {
+    float ms = 0.f;
+    CUDA_CHECK(cudaEventElapsedTime(&ms, p.second.first, p.second.second));
+    S->t_ms[p.first] += ms;
+    S->t_count[p.first] += 1;
+  }
+  S->ev_pending.clear();
+  S->ev_next = 0;
 }
 
 // Which forms a class's rows may take: one CTA when the row fits its shared memory, a
@@ -1936,14 +1980,20 @@ void plan_items(sp_scan* S, const std::vector<int>& live, bool first) {
 template <class R>
 void scan_transforms(sp_scan* S, const int* flags, const InverseArgs* inv, const ColumnArgsT<R>* col,
                      const ForwardArgsT<R>* fwd) {
-  for (auto& c : S->classes)
-    if (c->n_inv) CUDA_CHECK(launch_inverse_form(inv, *c, c->inv_form, flags, S->stream));
-  if (S->column_sweep)
-    CUDA_CHECK(launch_column_sweep_b(col, S->sweep_items.p, flags, S->n_sweep_items, S->stream));
-  else
-    CUDA_CHECK(launch_column_b(col, S->col_items.p, flags, S->n_col_items, S->stream));
-  for (auto& c : S->classes)
-    if (c->n_fwd) CUDA_CHECK(launch_forward_form(fwd, *c, c->fwd_form, flags, S->stream));
+  timed_family(S, SP_K_INVERSE, [&] {
+    for (auto& c : S->classes)
+      if (c->n_inv) CUDA_CHECK(launch_inverse_form(inv, *c, c->inv_form, flags, S->stream));
+  });
+  timed_family(S, SP_K_COLUMN, [&] {
+    if (S->column_sweep)
+      CUDA_CHECK(launch_column_sweep_b(col, S->sweep_items.p, flags, S->n_sweep_items, S->stream));
+    else
+      CUDA_CHECK(launch_column_b(col, S->col_items.p, flags, S->n_col_items, S->stream));
+  });
+  timed_family(S, SP_K_FORWARD, [&] {
+    for (auto& c : S->classes)
+      if (c->n_fwd) CUDA_CHECK(launch_forward_form(fwd, *c, c->fwd_form, flags, S->stream));
+  });
 }
 
 // The scan's transform autotuner: for every grid size, time every form each transform may
@@ -2057,7 +2107,9 @@ void scan_source(sp_scan* S, bool start) {
     scan_transforms(S, flags, start ? S->inv_start.p : S->inv_att.p,
                     start ? S->col_start.p : S->col_att.p, S->fwd.p);
   const DevBuf<OutputArgs>& out = start ? S->out_start : S->out_att;
-  CUDA_CHECK(launch_output_b(out.p, S->out_items.p, flags, S->n_out_items, S->stream));
+  timed_family(S, SP_K_OUTPUT, [&] {
+    CUDA_CHECK(launch_output_b(out.p, S->out_items.p, flags, S->n_out_items, S->stream));
+  });
 }
 
 void scan_attempt_launches(sp_scan* S) {
@@ -2065,9 +2117,13 @@ void scan_attempt_launches(sp_scan* S) {
   upload_all(S->flag_att, S->h_flag_att, R, S->stream);
   upload_all(S->stages_att, S->h_stages_att, 2 * (size_t)R, S->stream);
   upload_all(S->adams_att, S->h_adams_att, R, S->stream);
-  CUDA_CHECK(launch_step_b(0, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
+  timed_family(S, SP_K_PREDICT, [&] {
+    CUDA_CHECK(launch_step_b(0, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
+  });
   scan_source(S, false);
-  CUDA_CHECK(launch_step_b(1, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
+  timed_family(S, SP_K_CORRECT, [&] {
+    CUDA_CHECK(launch_step_b(1, S->step_att.p, S->step_items.p, S->flag_att.p, S->n_step_items, R, S->stream));
+  });
   CUDA_CHECK(cudaMemcpyAsync(S->h_norms, S->norms.p, sizeof(double) * 8 * R, cudaMemcpyDeviceToHost,
                              S->stream));
 }
@@ -2188,7 +2244,7 @@ void scan_step(sp_scan* S) {
   if (!n_att) return;
   // every operand of the attempt phase lives at a fixed address (pinned host tables, device
   // argument arrays), so its launches are captured once and replayed
-  if (!S->attempt_graph && !S->graph_failed) {
+  if (!S->attempt_graph && !S->graph_failed && !S->timing) {
     cudaGraph_t graph = nullptr;
     bool ok = cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
     if (ok) {
@@ -2208,7 +2264,7 @@ void scan_step(sp_scan* S) {
     }
   }
   const auto t_launch = clock::now();
-  if (S->attempt_graph) CUDA_CHECK(cudaGraphLaunch(S->attempt_graph, S->stream));
+  if (S->attempt_graph && !S->timing) CUDA_CHECK(cudaGraphLaunch(S->attempt_graph, S->stream));
   else scan_attempt_launches(S);
   CUDA_CHECK(cudaStreamSynchronize(S->stream));
   const auto t_decide = clock::now();
@@ -2226,7 +2282,9 @@ void scan_step(sp_scan* S) {
     }
   });
   upload_all(S->flag_accept, S->h_flag_accept, R, S->stream);
-  CUDA_CHECK(launch_step_b(2, S->step_att.p, S->step_items.p, S->flag_accept.p, S->n_step_items, R, S->stream));
+  timed_family(S, SP_K_ACCEPT, [&] {
+    CUDA_CHECK(launch_step_b(2, S->step_att.p, S->step_items.p, S->flag_accept.p, S->n_step_items, R, S->stream));
+  });
   const auto t_end = clock::now();
   auto ms = [](clock::time_point a, clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
@@ -2585,6 +2643,31 @@ sp_status sp_scan_run(sp_scan* S, int32_t run, double* state, sp_batch* info) {
 }
 
 void* sp_scan_stream(sp_scan* S) { return S ? (void*)S->stream : nullptr; }
+
+sp_status sp_scan_set_timing(sp_scan* S, int enable) {
+  return guarded([&] {
+    if (!S) throw Failure(SP_ERR_ARGUMENT, "NULL scan");
+    CUDA_CHECK(cudaSetDevice(S->device));
+    flush_scan_timing(S);
+    S->timing = enable != 0;
+  });
+}
+
+sp_status sp_scan_timing(sp_scan* S, double* ms, int64_t* launches, int reset) {
+  return guarded([&] {
+    if (!S || !ms || !launches) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    CUDA_CHECK(cudaSetDevice(S->device));
+    flush_scan_timing(S);
+    for (int k = 0; k < SP_K_COUNT; ++k) {
+      ms[k] = S->t_ms[k];
+      launches[k] = S->t_count[k];
+    }
+    if (reset) {
+      std::fill(S->t_ms, S->t_ms + SP_K_COUNT, 0.0);
+      std::fill(S->t_count, S->t_count + SP_K_COUNT, int64_t(0));
+    }
+  });
+}
 
 size_t sp_scan_describe(const sp_scan* S, char* buf, size_t len) {
   std::string text;
