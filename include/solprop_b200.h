@@ -239,6 +239,29 @@ sp_status sp_session_request_snapshot(sp_session* s);
 sp_status sp_session_march_state(const sp_session* s, sp_march_state* out);
 /* Copies the current state to out, host complex (n_modes, n_pol, n_omega). */
 sp_status sp_session_export(sp_session* s, double* out);
+/* A plane's statistics, formed on the device from the run's current state (the native
+ * workspace's statistics pass, native/src/general/statistics.cpp:106-450, with solprop's
+ * definitions, src/solprop/stats/definitions.py:148-500): only these small arrays come
+ * back.  Each pointer is the caller's host buffer, or NULL to skip that statistic.
+ *   energy           n_modes*n_pol  J per column: dt / n_t sum_k w_k |a_k|^2 p_k, w_k 1 at a
+ *                                   field grid's DC and Nyquist bins, 4 inside, 1 on an
+ *                                   envelope grid (fourier.energy_omega)
+ *   omega0           n_modes*n_pol  rad/s: the centroid sum omega |a|^2 p / sum |a|^2 p, NaN
+ *                                   for an empty column
+ *   peak_power       n_modes        W: max over time of sum_pol |E_a(t)|^2, E_a the analytic
+ *                                   signal of the column on the coarse grid
+ *   peak_power_total 1              W: max over time of the power summed over every column
+ *   spectrum         n_omega        J per bin: dt / n_t w_k sum_columns |a_k|^2 p_k
+ * p is the caller's power weight (n_modes, n_pol, n_omega) or 1 when power_weight is NULL;
+ * the peak powers are the unweighted ones (solprop's saved-field definitions). */
+typedef struct sp_statistics {
+  double* energy;
+  double* omega0;
+  double* peak_power;
+  double* peak_power_total;
+  double* spectrum;
+} sp_statistics;
+sp_status sp_session_statistics(sp_session* s, const double* power_weight, sp_statistics* out);
 /* The run's resumable state as one self-describing byte string (_core.Session.snapshot,
  * _core.pyi:484-494; the Adams history rows of native trial_adams.inc:526-605): the
  * march's scalars and history positions, the state, and the device history rows.  With
@@ -289,6 +312,11 @@ sp_status sp_scan_advance(sp_scan* scan, int32_t steps, sp_scan_status* out);
 /* One run's state (host complex, may be NULL) and counts (event 2: finished, 3: failed). */
 sp_status sp_scan_run(sp_scan* scan, int32_t run, double* state, sp_batch* info);
 void* sp_scan_stream(sp_scan* scan);
+/* One scan run's statistics at its current state, as sp_session_statistics: a scan
+ * reports per-run statistics without exporting the states.  No counterpart in the
+ * reference, which has no batch. */
+sp_status sp_scan_statistics(sp_scan* scan, int32_t run, const double* power_weight,
+                             sp_statistics* out);
 /* Per-family device timing of a scan's batch steps (the session's SP_K_* families: the
  * batched predictor, inverse transforms, response column, forward transforms, stage
  * output, corrector and accept).  While enabled, CUDA events are recorded around every

@@ -99,6 +99,30 @@ REASONS = {0: "reached", 3: "bound", 5: "floor", 6: "error", 7: "diverged", 11: 
 CATEGORIES = {0: "none", 1: "convergence", 2: "backend", 3: "value", 4: "refused"}
 
 
+class SpStatistics(C.Structure):
+    _fields_ = [("energy", C.POINTER(C.c_double)), ("omega0", C.POINTER(C.c_double)),
+                ("peak_power", C.POINTER(C.c_double)), ("peak_power_total", C.POINTER(C.c_double)),
+                ("spectrum", C.POINTER(C.c_double))]
+
+
+def statistics_call(fn, rec, power_weight=None) -> dict:
+    """Run an ``sp_*_statistics`` entry point ``fn(power_weight_ptr, out_ptr)`` into fresh
+    host arrays: energy and omega0 per (mode, polarisation), peak_power per mode,
+    peak_power_total, and the energy per bin."""
+    out = {"energy": np.empty((rec.n_modes, rec.n_pol)), "omega0": np.empty((rec.n_modes, rec.n_pol)),
+           "peak_power": np.empty(rec.n_modes), "peak_power_total": np.empty(1),
+           "spectrum": np.empty(rec.n_omega)}
+    st = SpStatistics(*(out[name].ctypes.data_as(C.POINTER(C.c_double)) for name in
+                        ("energy", "omega0", "peak_power", "peak_power_total", "spectrum")))
+    pw = None
+    if power_weight is not None:
+        pw = np.ascontiguousarray(np.broadcast_to(power_weight, (rec.n_modes, rec.n_pol, rec.n_omega)),
+                                  dtype=np.float64)
+    check(fn(_ptr(pw), C.byref(st)))
+    out["peak_power_total"] = float(out["peak_power_total"][0])
+    return out
+
+
 class SpScanStatus(C.Structure):
     _fields_ = [("active", C.c_int32), ("attempts", C.c_int64), ("rejected", C.c_int64),
                 ("evaluations", C.c_int64), ("batch_steps", C.c_int64)]
@@ -144,6 +168,9 @@ SIGNATURES = {
     "sp_session_restore": (C.c_int, [C.c_void_p, C.POINTER(SpRunDesc), C.c_void_p, C.c_size_t,
                                      C.POINTER(C.c_void_p)]),
     "sp_session_export": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "sp_session_statistics": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(SpStatistics)]),
+    "sp_scan_statistics": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double),
+                                     C.POINTER(SpStatistics)]),
     "sp_session_destroy": (C.c_int, [C.c_void_p]),
     "sp_workspace_stream": (C.c_void_p, [C.c_void_p]),
     "sp_session_set_timing": (C.c_int, [C.c_void_p, C.c_int]),
@@ -516,6 +543,13 @@ class Session:
         check(library().sp_session_march_state(self.handle, C.byref(st)))
         return {name: getattr(st, name) for name, _ in SpMarchState._fields_}
 
+    def statistics(self, power_weight=None) -> dict:
+        """The current state's plane statistics, formed on the device
+        (``sp_session_statistics``)."""
+        return statistics_call(
+            lambda pw, out: library().sp_session_statistics(self.handle, pw, out),
+            self.ws.problem.record, power_weight)
+
     def snapshot(self) -> bytes:
         """The run's resumable state (``Workspace.restore`` continues it)."""
         size = C.c_size_t()
@@ -613,6 +647,13 @@ class Scan:
     @property
     def stream(self) -> int:
         return int(library().sp_scan_stream(self.handle) or 0)
+
+    def statistics(self, index: int, power_weight=None) -> dict:
+        """Run ``index``'s plane statistics at its current state, formed on the device:
+        no state leaves it (``sp_scan_statistics``)."""
+        return statistics_call(
+            lambda pw, out: library().sp_scan_statistics(self.handle, int(index), pw, out),
+            self.records[index], power_weight)
 
     def set_timing(self, enable: bool) -> None:
         """Events around every batched launch family of the batch steps that follow."""

@@ -67,6 +67,7 @@ void ensure_configured(int device) {
   std::lock_guard<std::mutex> lock(g_configure_mutex);
   if (g_configured[device]) return;
   CUDA_CHECK(configure_source_kernels());
+  CUDA_CHECK(configure_statistics_kernels());
   g_configured[device] = true;
 }
 
@@ -248,6 +249,7 @@ struct sp_workspace {
   DevBuf<unsigned long long> ticket;  // the response column's tile counter
   DevBuf<double2> env_twiddles;       // envelope route: exp(-2 pi i m / (2 n_to)), m < n_to
   DevBuf<double> raman_undamped;
+  DevBuf<double> stat_power, stat_out, stat_weight;  // plane statistics, on first use
   // the mixed-precision form's FP32 copies of the source evaluation's buffers
   int precision = SP_PRECISION_FP64;
   struct {
@@ -1536,6 +1538,71 @@ sp_status sp_session_march_state(const sp_session* S, sp_march_state* out) {
   });
 }
 
+// ---- plane statistics of a workspace's state, formed on the device; the small results
+// alone come back (native statistics.cpp, solprop stats/definitions.py)
+static void plane_statistics(sp_workspace* ws, const double* power_weight, sp_statistics* out) {
+  const sp_problem& P = *ws->P;
+  const sp_problem_desc& d = P.d;
+  const bool envelope = d.grid_kind == 1;
+  if (envelope ? d.n_omega != d.n_t : d.n_omega != d.n_t / 2 + 1)
+    throw Failure(SP_ERR_REFUSED, "statistics need the coarse grid's full spectrum");
+  const bool peaks = out->peak_power || out->peak_power_total;
+  if (peaks && (d.n_t & (d.n_t - 1)))
+    throw Failure(SP_ERR_REFUSED, "peak powers need a power-of-two coarse grid");
+  if (d.n_modes > kStatMaxModes) throw Failure(SP_ERR_REFUSED, "statistics of more than 32 modes");
+  if (!ws->state.p) throw Failure(SP_ERR_STATE, "the workspace holds no state");
+  const size_t n = P.n;
+  const int peak_offset = 2 * P.n_cols, spectrum_offset = peak_offset + d.n_modes + 1;
+  if (!ws->stat_out.p) {
+    ws->stat_out.alloc((size_t)spectrum_offset + d.n_omega);
+    ws->stat_power.alloc((size_t)P.n_cols * d.n_t);
+  }
+  if (power_weight) {
+    for (size_t i = 0; i < n; ++i)
+      if (!(power_weight[i] > 0.0) || !std::isfinite(power_weight[i]))
+        throw Failure(SP_ERR_ARGUMENT, "power weights must be positive and finite");
+    if (!ws->stat_weight.p) ws->stat_weight.alloc(n);
+    CUDA_CHECK(cudaMemcpyAsync(ws->stat_weight.p, power_weight, n * sizeof(double),
+                               cudaMemcpyHostToDevice, ws->stream));
+  }
+  StatisticsArgs a{};
+  a.state = ws->state.p;
+  a.power_weight = power_weight ? ws->stat_weight.p : nullptr;
+  a.omega = ws->omega.p;
+  a.twiddles = ws->twiddles.p;
+  a.power = ws->stat_power.p;
+  a.out = ws->stat_out.p;
+  a.n_modes = d.n_modes;
+  a.n_pol = d.n_pol;
+  a.n_cols = P.n_cols;
+  a.n_omega = d.n_omega;
+  a.n_t = d.n_t;
+  a.log_m = std::min(ilog2(std::max(d.n_t, 1)), kStatLogRow);
+  a.log_table = ws->log_n_to;
+  a.envelope = envelope;
+  a.dt = d.dt;
+  a.peak_offset = peak_offset;
+  a.spectrum_offset = spectrum_offset;
+  CUDA_CHECK(launch_statistics(a, peaks, ws->stream));
+  std::vector<double> h((size_t)spectrum_offset + d.n_omega);
+  CUDA_CHECK(cudaMemcpyAsync(h.data(), ws->stat_out.p, h.size() * sizeof(double),
+                             cudaMemcpyDeviceToHost, ws->stream));
+  CUDA_CHECK(cudaStreamSynchronize(ws->stream));
+  if (out->energy) std::copy(h.begin(), h.begin() + P.n_cols, out->energy);
+  if (out->omega0) std::copy(h.begin() + P.n_cols, h.begin() + 2 * P.n_cols, out->omega0);
+  if (out->peak_power) std::copy(h.begin() + peak_offset, h.begin() + peak_offset + d.n_modes, out->peak_power);
+  if (out->peak_power_total) *out->peak_power_total = h[peak_offset + d.n_modes];
+  if (out->spectrum) std::copy(h.begin() + spectrum_offset, h.end(), out->spectrum);
+}
+
+sp_status sp_session_statistics(sp_session* S, const double* power_weight, sp_statistics* out) {
+  return guarded([&] {
+    if (!S || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
+    CUDA_CHECK(cudaSetDevice(S->ws->device));
+    plane_statistics(S->ws, power_weight, out);
+  });
+}
+
 // ---- snapshots: the march's scalars, its history positions and the device rows a later
 // attempt reads (the state, the Adams history rows of sources, and with a varying
 // operator the rows of states and rates), as one byte string with a header that names
@@ -2643,6 +2710,15 @@ sp_status sp_scan_run(sp_scan* S, int32_t run, double* state, sp_batch* info) {
 }
 
 void* sp_scan_stream(sp_scan* S) { return S ? (void*)S->stream : nullptr; }
+
+sp_status sp_scan_statistics(sp_scan* S, int32_t run, const double* power_weight, sp_statistics* out) {
+  return guarded([&] {
+    if (!S || run < 0 || run >= S->R || !out) throw Failure(SP_ERR_ARGUMENT, "bad scan statistics arguments");
+    CUDA_CHECK(cudaSetDevice(S->device));
+    CUDA_CHECK(cudaStreamSynchronize(S->stream));  // the run's last batched launches
+    plane_statistics(S->ws[run].get(), power_weight, out);
+  });
+}
 
 sp_status sp_scan_set_timing(sp_scan* S, int enable) {
   return guarded([&] {

@@ -154,6 +154,26 @@ cudaError_t launch_envelope(const EnvelopeArgs& a, cudaStream_t stream);
 cudaError_t configure_envelope_kernels();
 
 cudaError_t configure_source_kernels();
+
+// Plane statistics (statistics_kernels.cu).  out holds [energy: n_cols][omega0: n_cols],
+// then at peak_offset the peak power of each mode and of the whole field, then at
+// spectrum_offset the energy spectral density (n_omega).  power: (n_cols, n_t) scratch.
+constexpr int kStatEnergy = 0, kStatOmega0 = 1;
+constexpr int kStatMaxModes = 32;
+constexpr int kStatLogRow = 13;  // the longest row one CTA transforms: 8192 points
+struct StatisticsArgs {
+  const double2* state;         // (n_cols, n_omega)
+  const double* power_weight;   // (n_cols, n_omega) or null for one
+  const double* omega;          // (n_omega)
+  const double2* twiddles;      // exp(-2 pi i m / 2^log_table), m < 2^(log_table - 1)
+  double* power;                // (n_cols, n_t)
+  double* out;
+  int n_modes, n_pol, n_cols, n_omega, n_t, log_m, log_table, envelope;
+  double dt;
+  int peak_offset, spectrum_offset;
+};
+cudaError_t configure_statistics_kernels();
+cudaError_t launch_statistics(const StatisticsArgs& a, bool peaks, cudaStream_t s);
 int fft_cluster_size(int n_to);
 template <class R>
 cudaError_t launch_inverse_cluster(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream);

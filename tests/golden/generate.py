@@ -446,6 +446,42 @@ def scan_case(index, params):
     write(case, problem, golden)
 
 
+def stats_case(case):
+    """The reference's own plane statistics (``stats/definitions.py``: energy, omega0,
+    peak_power, peak_power_total; ``fourier.energy_weights`` times the columns' summed
+    |a|^2 for the energy per bin) of a fixture's last stored state -- the adaptive run's
+    last plane, or a scan point's state after its attempts -- added to its golden file as
+    ``stats.*``."""
+    from solprop import fourier
+    from solprop.stats import definitions as D
+
+    path = HERE / f"{case}.golden.npz"
+    golden = dict(np.load(path))
+    if case == "gnlse_raman":
+        grid = EnvelopeGrid.from_limits(0.05, 1030e-9, (700e-9, 1600e-9), 4e-12, fft_size="pow2")
+        state = golden["adaptive.states"][-1]
+    elif case.startswith("scan"):
+        grid = scan_point_sim(*SCAN_POINTS[int(case[4:])]).grid
+        state = golden["attempts.state"]
+    else:
+        params = {"cap4_he": dict(gas="He", pressure=(0.8, 0.0), length=0.05, n_t_limits=(150e-9, 4e-6),
+                                  trange=150e-15, energy=100e-6, fwhm=7.5e-15, modes=4, n_r=16,
+                                  radial_rule="gauss"),
+                  "config2": dict(gas="He", pressure=(0.8, 0.0), length=1.5, n_t_limits=(90e-9, 4e-6),
+                                  trange=400e-15, energy=275e-6, fwhm=7.5e-15, modes=4, n_r=64,
+                                  radial_rule="gauss", deep_uv=True)}[case]
+        grid = capillary(case, **params).grid
+        state = golden["adaptive.states"][-1]
+    golden["stats.energy"] = np.asarray(D.energy(grid, state))
+    golden["stats.omega0"] = np.asarray(D.omega0(grid, state))
+    golden["stats.peak_power"] = np.asarray(D.peak_power(grid, state))
+    golden["stats.peak_power_total"] = np.asarray(D.peak_power_total(grid, state))
+    weights = fourier.energy_weights(grid.n_omega, grid.dt, kind=grid.kind)
+    golden["stats.spectrum"] = weights * np.sum(np.abs(state) ** 2, axis=(0, 1))
+    np.savez_compressed(path, **golden)
+    print(f"{case}: statistics added", flush=True)
+
+
 if __name__ == "__main__":
     only = set(sys.argv[1:])
     if not only or "cap1_ar" in only:
@@ -473,3 +509,6 @@ if __name__ == "__main__":
     for i, params in enumerate(SCAN_POINTS):
         if not only or f"scan{i}" in only or "scan" in only:
             scan_case(i, params)
+    for case in ("cap4_he", "config2", "gnlse_raman", "scan0"):
+        if not only or f"stats_{case}" in only or "stats" in only:
+            stats_case(case)
