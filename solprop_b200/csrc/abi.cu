@@ -266,6 +266,10 @@ struct sp_workspace {
   AdamsDev* h_adams = nullptr;       // pinned
   DevBuf<double> partials, norms;
   double* h_norms = nullptr;         // pinned
+  // Recorded after every asynchronous copy out of h_stage and h_adams: the host waits on
+  // it before it writes them again, so that a copy still in flight never reads the next
+  // attempt's tables.
+  cudaEvent_t host_tables_free = nullptr;
   static constexpr int kStageSlots = 10;
   // per-kernel timing (sp_session_set_timing)
   bool timing = false;
@@ -300,6 +304,7 @@ struct sp_workspace {
   ~sp_workspace() {
     if (borrowed) return;
     for (auto e : ev_pool) cudaEventDestroy(e);
+    if (host_tables_free) cudaEventDestroy(host_tables_free);
     if (stream) cudaStreamSynchronize(stream);
     if (h_stage) cudaFreeHost(h_stage);
     if (h_adams) cudaFreeHost(h_adams);
@@ -325,9 +330,20 @@ struct KernelTimer {
   }
 };
 
+// The pinned stage and Adams tables are copied to the device asynchronously: before the
+// host writes them, it waits for the copies already issued from them; after issuing
+// copies, it marks them.
+static void claim_host_tables(sp_workspace* ws) {
+  if (ws->host_tables_free) CUDA_CHECK(cudaEventSynchronize(ws->host_tables_free));
+}
+static void release_host_tables(sp_workspace* ws) {
+  if (ws->host_tables_free) CUDA_CHECK(cudaEventRecord(ws->host_tables_free, ws->stream));
+}
+
 // host evaluation of one stage's scalars into slot `slot` of the pinned buffer
 static void fill_stage(sp_workspace* ws, int slot, double z0, double z1) {
   const sp_problem& P = *ws->P;
+  claim_host_tables(ws);
   StageScalarsDev& s = ws->h_stage[slot];
   std::memset(&s, 0, sizeof(s));
   s.z0 = z0;
@@ -358,6 +374,7 @@ static void fill_stage(sp_workspace* ws, int slot, double z0, double z1) {
 static void upload_stages(sp_workspace* ws, int count) {
   CUDA_CHECK(cudaMemcpyAsync(ws->stage.p, ws->h_stage, count * sizeof(StageScalarsDev),
                              cudaMemcpyHostToDevice, ws->stream));
+  release_host_tables(ws);
 }
 
 // The response column's tiles: windows of kWindow samples owning column_owned(K) each.
@@ -640,6 +657,7 @@ static void build_workspace(sp_workspace* ws) {
   ws->spectra.alloc((size_t)4 * n);
   ws->spectra.zero(s);
   ws->stage.alloc(sp_workspace::kStageSlots);
+  CUDA_CHECK(cudaEventCreateWithFlags(&ws->host_tables_free, cudaEventDisableTiming));
   CUDA_CHECK(cudaMallocHost(&ws->h_stage, sizeof(StageScalarsDev) * sp_workspace::kStageSlots));
   CUDA_CHECK(cudaMallocHost(&ws->h_adams, sizeof(AdamsDev)));
   CUDA_CHECK(cudaMallocHost(&ws->h_norms, sizeof(double) * 8));
@@ -756,8 +774,10 @@ static void adams_start(sp_session* S) {
   std::memset(&ad, 0, sizeof(ad));
   const bool comp = P.d.phi_expansion;
   if (comp) P.phi_rate.eval(S->z, ad.rate0_w);
-  upload_stages(ws, 2);
+  CUDA_CHECK(cudaMemcpyAsync(ws->stage.p, ws->h_stage, 2 * sizeof(StageScalarsDev),
+                             cudaMemcpyHostToDevice, ws->stream));
   CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, &ad, sizeof(AdamsDev), cudaMemcpyHostToDevice, ws->stream));
+  release_host_tables(ws);  // the attempt that follows refills both tables
   eval_source(ws, ws->state.p, 1, nullptr, ws->src.p, false);
   StepArgs a{};
   a.stage = ws->stage.p + 1;
@@ -838,6 +858,7 @@ static Pending prepare_attempt(sp_session* S, double dz, double end, bool kink, 
     pd.free_slot = free_slot;
   }
   int width = 1 + *std::max_element(pd.orders, pd.orders + pd.n_orders);
+  claim_host_tables(ws);
   AdamsDev& ad = *ws->h_adams;
   std::memset(&ad, 0, sizeof(ad));
   ad.dz = dz;
@@ -1011,6 +1032,7 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
   Pending pd = prepare_attempt(S, dz, end, kink, fixed);
   upload_stages(ws, 2);
   CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, ws->h_adams, sizeof(AdamsDev), cudaMemcpyHostToDevice, ws->stream));
+  release_host_tables(ws);
   StepArgs a = step_args_of(ws, ws->adams.p, ws->stage.p);
   { KernelTimer t(ws, SP_K_PREDICT); CUDA_CHECK(launch_adams_predict(a, ws->stream)); }
   eval_source(ws, ws->lab.p, 1, nullptr, ws->src.p, false);
