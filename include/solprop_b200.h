@@ -201,6 +201,19 @@ sp_status sp_workspace_create(const sp_problem* problem, int device, sp_workspac
 /* The same with a precision (SP_PRECISION_*). */
 sp_status sp_workspace_create_ex(const sp_problem* problem, int device, int precision,
                                  sp_workspace** out);
+/* How a workspace evaluates the modal transform (synthesis of the node field from the
+ * modes, projection of the node streams back; numpy_ref passes/transforms.py:87-187):
+ *   SP_MODAL_FUSED  inside the response column, on CUDA cores, from a modal window in
+ *                   shared memory -- up to 8 modal columns;
+ *   SP_MODAL_GEMM   as dense products: FP64 products in the plain form; in the mixed form
+ *                   tcgen05 products of three-part BF16 splits of each operand, accumulated
+ *                   in FP32 (the reference's synthesis and projection GEMMs,
+ *                   native/src/general/trial.cpp:181-315, transforms/gemm.hpp:55-275) --
+ *                   up to 64 modal columns, field grid, one field component;
+ *   SP_MODAL_AUTO   FUSED up to 8 columns, GEMM above. */
+enum { SP_MODAL_AUTO = 0, SP_MODAL_FUSED = 1, SP_MODAL_GEMM = 2 };
+sp_status sp_workspace_create_ex2(const sp_problem* problem, int device, int precision, int modal,
+                                  sp_workspace** out);
 sp_status sp_workspace_destroy(sp_workspace* ws);
 /* One source evaluation F at a lab-frame field, untransported (numpy_ref
  * workspace.py:819 lab_source): lab and out are host complex (n_modes,n_pol,n_omega).

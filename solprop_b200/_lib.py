@@ -137,6 +137,7 @@ SIGNATURES = {
     "sp_problem_destroy": (C.c_int, [C.c_void_p]),
     "sp_workspace_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "sp_workspace_create_ex": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "sp_workspace_create_ex2": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     # the scan surrogate's perceptron kernels (device pointers, stream may be NULL)
     "sp_mlp_gemm": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
                               C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
@@ -443,14 +444,21 @@ def precision_code(precision: str) -> int:
 class Workspace:
     """Device buffers of one problem (``sp_workspace``; native ``_core.Workspace``)."""
 
-    def __init__(self, problem: Problem, device: int = 0, precision: str = "fp64"):
+    MODAL = {"auto": 0, "fused": 1, "gemm": 2}
+
+    def __init__(self, problem: Problem, device: int = 0, precision: str = "fp64", modal: str = "auto"):
+        """``modal``: the modal transform inside the response column ("fused", up to 8
+        columns), as dense products ("gemm": FP64 products, or tcgen05 products of
+        three-part BF16 splits in the mixed form), or "auto" (fused up to 8 columns)."""
         self.handle = None
         self._lib = library()
         self.problem = problem
         self.precision = precision
+        if modal not in self.MODAL:
+            raise ValueError(f"modal transform {modal!r}: expected one of {sorted(self.MODAL)}")
         handle = C.c_void_p()
-        check(library().sp_workspace_create_ex(problem.handle, device, precision_code(precision),
-                                               C.byref(handle)))
+        check(library().sp_workspace_create_ex2(problem.handle, device, precision_code(precision),
+                                                self.MODAL[modal], C.byref(handle)))
         self.handle = handle
         self.shape = (problem.record.n_modes, problem.record.n_pol, problem.record.n_omega)
 

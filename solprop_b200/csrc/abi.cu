@@ -68,6 +68,7 @@ void ensure_configured(int device) {
   if (g_configured[device]) return;
   CUDA_CHECK(configure_source_kernels());
   CUDA_CHECK(configure_statistics_kernels());
+  CUDA_CHECK(configure_modal_gemm());
   g_configured[device] = true;
 }
 
@@ -198,8 +199,8 @@ static void validate(const sp_problem_desc* d) {
   const bool envelope = d->grid_kind == 1;
   if (d->n_pol * d->n_pol_transform != 1)
     throw Failure(SP_ERR_REFUSED, "two field components (vector Kerr) are not built yet");
-  if (d->n_modes * d->n_pol > kMaxModes)
-    throw Failure(SP_ERR_REFUSED, "more than 8 modal columns: the tensor-core transform is not built yet");
+  if (d->n_modes * d->n_pol > kMaxGemmModes)
+    throw Failure(SP_ERR_REFUSED, "more than 64 modal columns");
   if (envelope) {
     // the envelope route: one modal column on one node (the single-mode GNLSE)
     if (d->n_modes * d->n_pol != 1 || d->n_nodes != 1)
@@ -250,11 +251,18 @@ struct sp_workspace {
   DevBuf<double2> env_twiddles;       // envelope route: exp(-2 pi i m / (2 n_to)), m < n_to
   DevBuf<double> raman_undamped;
   DevBuf<double> stat_power, stat_out, stat_weight;  // plane statistics, on first use
+  // the modal transform as products (SP_MODAL_GEMM): the node field and streams in HBM;
+  // the mixed form's operands in three BF16 parts, rows padded to kpad
+  bool gemm = false;
+  int kpad_modes = 0, kpad_nodes = 0;
+  DevBuf<double> node_field, node_streams;
+  DevBuf<uint16_t> s_parts, w_parts, modal_parts, node_parts;
   // the mixed-precision form's FP32 copies of the source evaluation's buffers
   int precision = SP_PRECISION_FP64;
   struct {
     DevBuf<float2> twiddles, spectra;
     DevBuf<float> t_window, t_window_d, synthesis, projection, rate_coeff, taps, proj;
+    DevBuf<float> node_field, node_streams;
   } f32;
   DevBuf<unsigned char> active, norm;
   DevBuf<StageScalarsDev> stage;   // kStageSlots slots
@@ -495,6 +503,57 @@ static OutputArgs output_args(const sp_workspace* ws, const StageScalarsDev* sta
                     absorber};
 }
 
+// The field grid's source on the GEMM route: inverse transforms, the synthesis product
+// (node field), the response column over the node field (node streams), the projection
+// products (the projected streams, group 0's rows), forward transforms.  The taper tau
+// of the stage scales the synthesis and divides the projection, read on the device.
+static void eval_source_gemm(sp_workspace* ws, const double2* lab, int slot, bool absorber) {
+  const sp_problem& P = *ws->P;
+  const sp_problem_desc& d = P.d;
+  const double* taper = &(ws->stage.p + slot)->taper;
+  double* status = ws->norms.p + kColumnStatus;
+  const int n_streams = d.plasma_enabled ? 3 : 1;
+  const size_t stride = (size_t)P.n_cols * d.n_to;  // one projected stream's rows
+  const auto ia = inverse_args(ws, lab, absorber);
+  { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
+  if (ws->precision == SP_PRECISION_MIXED) {
+    {
+      KernelTimer t(ws, SP_K_PROJECT);
+      CUDA_CHECK(modal_synthesis_split3(ws->s_parts.p, ws->modal_t.p, ws->modal_parts.p, ws->f32.node_field.p,
+                                        d.n_nodes, d.n_modes, d.n_to, ws->kpad_modes, taper, status, ws->stream));
+    }
+    auto ca = column_args<float>(ws, ws->stage.p + slot);
+    ca.node_field = ws->f32.node_field.p;
+    ca.node_streams = ws->f32.node_streams.p;
+    { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column_nodes(ca, ws->stream)); }
+    {
+      KernelTimer t(ws, SP_K_PROJECT);
+      CUDA_CHECK(modal_projection_split3(ws->w_parts.p, ws->f32.node_streams.p, ws->node_parts.p,
+                                         ws->f32.proj.p, n_streams, d.n_modes, d.n_nodes, d.n_to,
+                                         ws->kpad_nodes, stride, taper, status, ws->stream));
+    }
+    const auto fa = forward_args<float>(ws);
+    { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
+  } else {
+    {
+      KernelTimer t(ws, SP_K_PROJECT);
+      CUDA_CHECK(modal_synthesis_f64(ws->synthesis.p, ws->modal_t.p, ws->node_field.p, d.n_nodes, d.n_modes,
+                                     d.n_to, taper, ws->stream));
+    }
+    auto ca = column_args<double>(ws, ws->stage.p + slot);
+    ca.node_field = ws->node_field.p;
+    ca.node_streams = ws->node_streams.p;
+    { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column_nodes(ca, ws->stream)); }
+    {
+      KernelTimer t(ws, SP_K_PROJECT);
+      CUDA_CHECK(modal_projection_f64(ws->projection.p, ws->node_streams.p, ws->proj.p, n_streams, d.n_modes,
+                                      d.n_nodes, d.n_to, stride, taper, ws->stream));
+    }
+    const auto fa = forward_args<double>(ws);
+    { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
+  }
+}
+
 // One source evaluation at lab (device), stage slot, optional inverse propagator.
 static void eval_source(sp_workspace* ws, const double2* lab, int slot, const double2* inv_prop,
                         double2* out, bool quiet) {
@@ -523,6 +582,8 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
     ea.n_to = d.n_to;
     ea.log_n_to = ws->log_n_to;
     { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_envelope(ea, ws->stream)); }
+  } else if (ws->gemm) {
+    eval_source_gemm(ws, lab, slot, absorber);
   } else if (ws->precision == SP_PRECISION_MIXED) {
     const auto ia = inverse_args(ws, lab, absorber);
     { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_inverse(ia, P.n_cols, ws->stream)); }
@@ -585,7 +646,7 @@ static void build_mixed(sp_workspace* ws, const std::vector<double2>& tw, const 
   }
   keep.push_back(std::move(r32));
   up(f.rate_coeff, keep.back());
-  const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
+  const size_t n_groups = ws->gemm ? 1 : (d.n_nodes + kGroup - 1) / kGroup;  // the products write group 0's rows
   f.proj.alloc(n_groups * 3 * P.n_cols * d.n_to);
   f.proj.zero(s);
   f.spectra.alloc((size_t)4 * P.n);
@@ -650,8 +711,31 @@ static void build_workspace(sp_workspace* ws) {
   ws->arrivals.zero(s);
   ws->ticket.alloc(1);
   ws->ticket.zero(s);
-  ws->proj.alloc(n_groups * 3 * P.n_cols * d.n_to);
+  ws->proj.alloc((ws->gemm ? 1 : n_groups) * 3 * P.n_cols * d.n_to);
   ws->proj.zero(s);
+  if (ws->gemm) {
+    const size_t field = (size_t)d.n_nodes * d.n_to;
+    ws->kpad_modes = modal_kpad(d.n_modes);
+    ws->kpad_nodes = modal_kpad(d.n_nodes);
+    if (ws->precision == SP_PRECISION_MIXED) {
+      ws->f32.node_field.alloc(field);
+      ws->f32.node_streams.alloc(3 * field);
+      ws->f32.node_streams.zero(s);
+      std::vector<uint16_t> parts;
+      split3_host(P.synthesis.data(), d.n_nodes, d.n_modes, ws->kpad_modes, parts);
+      ws->s_parts.upload(parts.data(), parts.size(), s);
+      CUDA_CHECK(cudaStreamSynchronize(s));  // the host copy goes with this scope
+      split3_host(P.projection.data(), d.n_modes, d.n_nodes, ws->kpad_nodes, parts);
+      ws->w_parts.upload(parts.data(), parts.size(), s);
+      CUDA_CHECK(cudaStreamSynchronize(s));
+      ws->modal_parts.alloc((size_t)3 * d.n_to * ws->kpad_modes);
+      ws->node_parts.alloc((size_t)3 * d.n_to * ws->kpad_nodes);
+    } else {
+      ws->node_field.alloc(field);
+      ws->node_streams.alloc(3 * field);
+      ws->node_streams.zero(s);
+    }
+  }
   ws->streams.alloc((size_t)4 * P.n_cols * d.n_to);
   ws->streams.zero(s);
   ws->spectra.alloc((size_t)4 * n);
@@ -666,6 +750,10 @@ static void build_workspace(sp_workspace* ws) {
   ws->norms.alloc(kMaxOrders + 2);
   ws->norms.zero(s);
   ws->launches = 5;
+  if (ws->gemm) {  // inverse, synthesis, column, one projection per stream, forward, output
+    const int per_product = ws->precision == SP_PRECISION_MIXED ? 2 : 1;  // (split,) product
+    ws->launches = 4 + per_product * (1 + (d.plasma_enabled ? 3 : 1));
+  }
   if (ws->precision == SP_PRECISION_MIXED) build_mixed(ws, tw, rc, taps);
   if (d.grid_kind == 1) {
     std::vector<double2> tw2(d.n_to);
@@ -1319,18 +1407,32 @@ sp_status sp_workspace_create(const sp_problem* problem, int device, sp_workspac
 
 sp_status sp_workspace_create_ex(const sp_problem* problem, int device, int precision,
                                  sp_workspace** out) {
+  return sp_workspace_create_ex2(problem, device, precision, SP_MODAL_AUTO, out);
+}
+
+sp_status sp_workspace_create_ex2(const sp_problem* problem, int device, int precision, int modal,
+                                  sp_workspace** out) {
   return guarded([&] {
     if (!problem || !out) throw Failure(SP_ERR_ARGUMENT, "NULL problem or out");
     if (precision != SP_PRECISION_FP64 && precision != SP_PRECISION_MIXED)
       throw Failure(SP_ERR_ARGUMENT, "unknown precision");
-    if (precision == SP_PRECISION_MIXED && problem->d.grid_kind == 1)
+    if (modal != SP_MODAL_AUTO && modal != SP_MODAL_FUSED && modal != SP_MODAL_GEMM)
+      throw Failure(SP_ERR_ARGUMENT, "unknown modal transform form");
+    const sp_problem_desc& d = problem->d;
+    if (precision == SP_PRECISION_MIXED && d.grid_kind == 1)
       throw Failure(SP_ERR_REFUSED, "the mixed precision of the envelope route is not built yet");
+    const bool gemm = modal == SP_MODAL_GEMM || (modal == SP_MODAL_AUTO && problem->n_cols > kMaxModes);
+    if (gemm && d.grid_kind != 0)
+      throw Failure(SP_ERR_REFUSED, "the modal transform's products take the field grid");
+    if (!gemm && problem->n_cols > kMaxModes)
+      throw Failure(SP_ERR_REFUSED, "more than 8 modal columns take the modal transform's products");
     CUDA_CHECK(cudaSetDevice(device));
     ensure_configured(device);
     auto ws = std::make_unique<sp_workspace>();
     ws->P = problem;
     ws->device = device;
     ws->precision = precision;
+    ws->gemm = gemm;
     CUDA_CHECK(cudaStreamCreateWithFlags(&ws->stream, cudaStreamNonBlocking));
     build_workspace(ws.get());
     *out = ws.release();
@@ -2543,6 +2645,9 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     if (n_runs < 1 || !problems || !runs || !out) throw Failure(SP_ERR_ARGUMENT, "bad scan arguments");
     if (precision != SP_PRECISION_FP64 && precision != SP_PRECISION_MIXED)
       throw Failure(SP_ERR_ARGUMENT, "unknown precision");
+    for (int r = 0; r < n_runs; ++r)
+      if (problems[r] && problems[r]->n_cols > kMaxModes)
+        throw Failure(SP_ERR_REFUSED, "a scan's runs take at most 8 modal columns (the fused transform)");
     CUDA_CHECK(cudaSetDevice(device));
     ensure_configured(device);
     auto S = std::make_unique<sp_scan>();
@@ -2933,6 +3038,8 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     if (!problem || !lab || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
     if (problem->d.grid_kind != 0)
       throw Failure(SP_ERR_REFUSED, "the no-allocation entry point takes field-grid problems");
+    if (problem->n_cols > kMaxModes)
+      throw Failure(SP_ERR_REFUSED, "the no-allocation entry point takes at most 8 modal columns");
     int device = 0;
     CUDA_CHECK(cudaGetDevice(&device));
     unsigned char* base = noalloc_base(device);

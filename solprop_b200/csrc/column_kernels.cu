@@ -319,9 +319,14 @@ __device__ __forceinline__ double predecessors(const double* sums, int node, int
 // carried per lane -- lane l holds the sum of tiles l, l + 32, ... added in tile order,
 // the association predecessors() uses, so both forms give the same bits -- and every
 // group keeps its own partial rows, which the forward transform adds in group order.
-template <class R, bool kSweep>
+//
+// kNodes = true is the GEMM route's form (tile-parallel only): the window's field is the
+// node field a synthesis product wrote, read in place of the synthesis, and the outputs
+// go to the node streams a projection product reads, in place of the projection.
+template <class R, bool kSweep, bool kNodes = false>
 __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, int group,
                                             unsigned long long epoch, double& carry0, double& carry1) {
+  static_assert(!(kSweep && kNodes), "the node-field form is tile-parallel");
   extern __shared__ __align__(16) unsigned char column_raw[];
   R* modal = reinterpret_cast<R*>(column_raw);    // [m][kPitch], then the streams
   R* streams = modal;                              // [s][warp][kPitch]
@@ -345,7 +350,9 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   double* next_modal = reinterpret_cast<double*>(column_raw + column_smem<R>());
   R* next_gate = reinterpret_cast<R*>(next_modal + (size_t)kMaxModes * kWindow);
   const bool copied = kSweep && tile > 0;
-  if (copied) {
+  if constexpr (kNodes) {
+    // nothing modal to stage: the field is read per node below
+  } else if (copied) {
     for (int i = threadIdx.x; i < n_modes * kWindow; i += blockDim.x)
       modal[(i / kWindow) * kPitch + pad(i % kWindow)] = R(next_modal[i]);
   } else {
@@ -355,7 +362,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       modal[m * kPitch + pad(u)] = (t >= 0 && t < n_to) ? R(modal_t[(size_t)m * n_to + t]) : R(0);
     }
   }
-  if (!kSweep || tile == 0) {  // the weights do not change along a sweep
+  if (!kNodes && (!kSweep || tile == 0)) {  // the weights do not change along a sweep
     const R* projection = a.projection;
     for (int k = threadIdx.x; k < n_modes * kGroup; k += blockDim.x) {
       const int m = k / kGroup, w = k % kGroup, nd = group * kGroup + w;
@@ -398,15 +405,20 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
     const R* synthesis = a.synthesis;
 #pragma unroll
     for (int m = 0; m < kMaxModes; ++m)
-      srow[m] = (live && m < n_modes) ? synthesis[node * n_modes + m] * tau : R(0);
+      srow[m] = (!kNodes && live && m < n_modes) ? synthesis[node * n_modes + m] * tau : R(0);
     const RateLookup<R> rates = rate_lookup(a);
+    const R* field_row = kNodes && live ? a.node_field + (size_t)node * n_to : nullptr;
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
       const int u = kPer * lane + j, t = tw + u;
       R e = R(0);
+      if constexpr (kNodes) {
+        if (field_row && t >= 0 && t < n_to) e = field_row[t];
+      } else {
 #pragma unroll
-      for (int m = 0; m < kMaxModes; ++m)
-        if (m < n_modes) e += srow[m] * modal[m * kPitch + pad(u)];
+        for (int m = 0; m < kMaxModes; ++m)
+          if (m < n_modes) e += srow[m] * modal[m * kPitch + pad(u)];
+      }
       E[j] = e;
       W[j] = (plasma && t >= 0 && t < n_to) ? rate_of(rates, fabs(e)) : R(0);
     }
@@ -543,11 +555,24 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
           z = gate_d[pad(u)] * current;
         }
       }
-      streams[(0 * kGroup + warp) * kPitch + pad(u)] = p;
-      streams[(1 * kGroup + warp) * kPitch + pad(u)] = x;
-      streams[(2 * kGroup + warp) * kPitch + pad(u)] = z;
+      if constexpr (kNodes) {
+        if (live && u >= A && u < own_hi) {
+          const size_t at = (size_t)node * n_to + (size_t)(tw + u);
+          const size_t plane = (size_t)n_nodes * n_to;
+          a.node_streams[at] = p;
+          if (plasma) {
+            a.node_streams[plane + at] = x;
+            a.node_streams[2 * plane + at] = z;
+          }
+        }
+      } else {
+        streams[(0 * kGroup + warp) * kPitch + pad(u)] = p;
+        streams[(1 * kGroup + warp) * kPitch + pad(u)] = x;
+        streams[(2 * kGroup + warp) * kPitch + pad(u)] = z;
+      }
     }
   }
+  if constexpr (kNodes) return;  // the projection product takes the node streams
   // Ahead of the pulse no node of the group carries a current: the two current streams
   // are zeros of either sign, whose projections are +0, written without the products.
   const bool currents = __syncthreads_or(!quiet) != 0;
@@ -612,7 +637,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   }
 }
 
-template <class R>
+template <class R, bool kNodes = false>
 __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   __shared__ unsigned long long ticket;
   if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1ull);
@@ -620,7 +645,7 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   const unsigned long long epoch = ticket / (unsigned long long)a.n_blocks;
   const int index = (int)(ticket % (unsigned long long)a.n_blocks);
   double unused0 = 0.0, unused1 = 0.0;
-  column_tile<R, false>(a, index / a.n_groups, index % a.n_groups, epoch, unused0, unused1);
+  column_tile<R, false, kNodes>(a, index / a.n_groups, index % a.n_groups, epoch, unused0, unused1);
 }
 
 // one node group through every tile of the row, in tile order
@@ -642,6 +667,11 @@ template <class R> constexpr int column_residency() { return sizeof(R) == 8 ? 2 
 template <class R>
 __global__ void __launch_bounds__(kThreads, column_residency<R>()) k_column(ColumnArgsT<R> a) {
   column_body(a);
+}
+
+template <class R>
+__global__ void __launch_bounds__(kThreads, column_residency<R>()) k_column_nodes(ColumnArgsT<R> a) {
+  column_body<R, true>(a);
 }
 
 // batched: items[blockIdx.x].x = the run; a run's CTAs take their tiles from its counter
@@ -683,6 +713,14 @@ cudaError_t launch_column(const ColumnArgsT<R>& a, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+template <class R>
+cudaError_t launch_column_nodes(const ColumnArgsT<R>& a, cudaStream_t stream) {
+  k_column_nodes<R><<<a.n_blocks, kThreads, column_smem<R>(), stream>>>(a);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_column_nodes<double>(const ColumnArgsT<double>&, cudaStream_t);
+template cudaError_t launch_column_nodes<float>(const ColumnArgsT<float>&, cudaStream_t);
 template cudaError_t launch_column<double>(const ColumnArgsT<double>&, cudaStream_t);
 template cudaError_t launch_column<float>(const ColumnArgsT<float>&, cudaStream_t);
 template cudaError_t launch_column_b<double>(const ColumnArgsT<double>*, const int4*, const int*, int,
@@ -695,12 +733,14 @@ template cudaError_t launch_column_sweep_b<float>(const ColumnArgsT<float>*, con
                                                   int, cudaStream_t);
 
 cudaError_t configure_column_kernels() {
-  const void* kernels[6] = {(const void*)k_column<double>, (const void*)k_column_b<double>,
+  const void* kernels[8] = {(const void*)k_column<double>, (const void*)k_column_b<double>,
                             (const void*)k_column_sweep_b<double>, (const void*)k_column<float>,
-                            (const void*)k_column_b<float>, (const void*)k_column_sweep_b<float>};
-  const size_t shm[6] = {column_smem<double>(), column_smem<double>(), column_sweep_smem<double>(),
-                         column_smem<float>(), column_smem<float>(), column_sweep_smem<float>()};
-  for (int i = 0; i < 6; ++i) {
+                            (const void*)k_column_b<float>, (const void*)k_column_sweep_b<float>,
+                            (const void*)k_column_nodes<double>, (const void*)k_column_nodes<float>};
+  const size_t shm[8] = {column_smem<double>(), column_smem<double>(), column_sweep_smem<double>(),
+                         column_smem<float>(), column_smem<float>(), column_sweep_smem<float>(),
+                         column_smem<double>(), column_smem<float>()};
+  for (int i = 0; i < 8; ++i) {
     cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shm[i]);
     if (e != cudaSuccess) return e;

@@ -3,6 +3,8 @@
 // host-to-device copy before the launches, so that a captured CUDA graph replays with
 // the values of the current attempt.
 #pragma once
+#include <vector>
+
 #include "sp_common.cuh"
 
 namespace sp {
@@ -102,11 +104,19 @@ struct ColumnArgsT {
   double log_field_min, d_log_field, field_min, field_max, rate_max;
   const R* rate_coefficients;
   const R* taps;
+  // the modal transform on the GEMM route: the node field the synthesis product wrote,
+  // (n_nodes, n_to), and the node streams P, X, Z the projection product reads,
+  // (3, n_nodes, n_to); null on the fused route
+  const R* node_field;
+  R* node_streams;
 };
 using ColumnTileArgs = ColumnArgsT<double>;
 
 template <class R>
 cudaError_t launch_column(const ColumnArgsT<R>& a, cudaStream_t stream);
+// the response column on the GEMM route: node field in, node streams out
+template <class R>
+cudaError_t launch_column_nodes(const ColumnArgsT<R>& a, cudaStream_t stream);
 cudaError_t configure_column_kernels();
 
 template <class R>
@@ -173,6 +183,24 @@ struct StatisticsArgs {
   int peak_offset, spectrum_offset;
 };
 cudaError_t configure_statistics_kernels();
+
+// The modal transform as products (modal_gemm.cu): the GEMM route.  The mixed form's
+// operands are three BF16 parts (hi, mid, lo) per value, panel after panel, rows of kpad.
+constexpr int kMaxGemmModes = 64;   // modal columns the route's projection tile holds
+int modal_kpad(int k);              // k rounded up to the products' 64-wide K slices
+cudaError_t configure_modal_gemm();
+void split3_host(const double* src, int rows, int cols, int ld_out, std::vector<uint16_t>& out);
+cudaError_t modal_synthesis_f64(const double* S, const double* modal, double* E, int n_nodes, int n_modes,
+                                int n_to, const double* taper, cudaStream_t s);
+cudaError_t modal_projection_f64(const double* W, const double* node_streams, double* out, int n_streams,
+                                 int n_modes, int n_nodes, int n_to, size_t out_stride, const double* taper,
+                                 cudaStream_t s);
+cudaError_t modal_synthesis_split3(const uint16_t* s_parts, const double* modal, uint16_t* modal_parts, float* E,
+                                   int n_nodes, int n_modes, int n_to, int kpad, const double* taper,
+                                   double* status, cudaStream_t s);
+cudaError_t modal_projection_split3(const uint16_t* w_parts, const float* node_streams, uint16_t* node_parts,
+                                    float* out, int n_streams, int n_modes, int n_nodes, int n_to, int kpad,
+                                    size_t out_stride, const double* taper, double* status, cudaStream_t s);
 cudaError_t launch_statistics(const StatisticsArgs& a, bool peaks, cudaStream_t s);
 int fft_cluster_size(int n_to);
 template <class R>

@@ -492,6 +492,11 @@ if __name__ == "__main__":
         cap_case("cap4_he", gas="He", pressure=(0.8, 0.0), length=0.05, limits=(150e-9, 4e-6),
                  trange=150e-15, energy=100e-6, fwhm=7.5e-15, modes=4, n_r=16,
                  radial_rule="gauss", fixed_dz=0.005, n_fixed_planes=11, seed=2)
+    if not only or "cap12_ne" in only:
+        # twelve modes: more modal columns than the fused column holds (the GEMM route)
+        cap_case("cap12_ne", gas="Ne", pressure=1.5, length=0.02, limits=(200e-9, 4e-6),
+                 trange=100e-15, energy=60e-6, fwhm=10e-15, modes=12, n_r=96,
+                 radial_rule="gauss", fixed_dz=0.001, n_fixed_planes=6, seed=6)
     if not only or "gnlse_raman" in only:
         gnlse_case("gnlse_raman", seed=3)
     if not only or "config2" in only:
