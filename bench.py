@@ -228,6 +228,75 @@ def surrogate_leg(device: int, points: int = 16384, members: int = 5, repeats: i
                          "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"}}
 
 
+def modal_products_record(n_modes: int = 30, n_nodes: int = 16384):
+    """A config-3-sized modal transform on config 2's field grid (n_to 16 384): n_modes
+    columns on n_nodes nodes.  Synthetic operands with config 2's magnitudes -- node i,
+    mode m takes config 2's synthesis and projection weights of node i mod 64 and mode
+    m mod 4, the projection divided by the node multiple, each times a seeded factor in
+    [0.9, 1.1] -- and config 2's operator and prefactor per mode m mod 4; the launch field
+    is config 2's in the first four modes."""
+    rec, pol = load_workload()
+    rng = np.random.default_rng(7)
+    base_s, base_w = rec.synthesis, rec.projection
+    modes = np.arange(n_modes) % rec.n_modes
+    nodes = np.arange(n_nodes) % rec.n_nodes
+    rec.synthesis = np.ascontiguousarray(base_s[nodes][:, modes] * rng.uniform(0.9, 1.1, (n_nodes, n_modes)))
+    rec.projection = np.ascontiguousarray(base_w[modes][:, nodes] * (rec.n_nodes / n_nodes)
+                                          * rng.uniform(0.9, 1.1, (n_modes, n_nodes)))
+    rec.projection_coarse = rec.projection.copy()
+    rec.phi_terms = np.ascontiguousarray(rec.phi_terms[:, modes])
+    rec.prefactor_terms = np.ascontiguousarray(rec.prefactor_terms[:, modes])
+    field0 = np.zeros((n_modes,) + rec.field0.shape[1:], dtype=np.complex128)
+    field0[: rec.n_modes] = rec.field0
+    rec.field0 = field0
+    rec.n_modes, rec.n_nodes = n_modes, n_nodes
+    return rec, pol
+
+
+def modal_products_leg(device: int, repeats: int = 3) -> dict:
+    """The modal transform as products at a config-3 size (30 modes, 16 384 nodes, 16 384
+    samples; config 3's own route -- envelope grid, vector modes, tensor Raman -- is not
+    built): per source evaluation, the products' device time (synthesis and the three
+    streams' projections, the mixed form's splits included) and their FLOP rate against
+    the measured BF16 peak, in the mixed form (tcgen05, three-part BF16 splits) and the
+    plain FP64 form.  FLOPs counted are the product's own, 2 N_q n_m n_to for the synthesis
+    and 2 x 3 n_m N_q n_to for the projections; the split form executes six BF16 products
+    for each."""
+    from solprop_b200 import _lib
+
+    rec, pol = modal_products_record()
+    flops = 2.0 * rec.n_nodes * rec.n_modes * rec.n_to * (1 + 3)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = peaks.get("bf16_tflops", 1590.0)
+    problem = _lib.Problem(rec)
+    out = {"workload": "modal transform: 30 modes x 16384 nodes x 16384 samples, config 2 grid and "
+                       "response (synthetic operands)", "flops_per_evaluation": flops}
+    lab = rec.field0
+    for precision in ("mixed", "fp64"):
+        ws = _lib.Workspace(problem, device, precision, modal="gemm")
+        session = ws.start(pol, field0=lab)  # the timing switch lives on a session
+        ws.source(lab, 0.0)  # warm-up
+        session.set_timing(True)
+        session.timing(reset=True)
+        for _ in range(repeats):
+            ws.source(lab, 0.0)
+        fams = session.timing(reset=True)
+        session.set_timing(False)
+        prod_ms = fams["project"][0] / repeats
+        total_ms = sum(v[0] for v in fams.values()) / repeats
+        achieved = flops / (prod_ms * 1e-3) / 1e12
+        out[precision] = {"products_ms": prod_ms, "column_ms": fams["response_column"][0] / repeats,
+                          "evaluation_ms": total_ms, "products_tflops": achieved,
+                          "frac_of_bf16_peak": achieved / peak}
+        session.close()
+        ws.close()
+    out["roofline"] = {"bound": "tensor", "kernel": "modal products (tcgen05, split BF16)",
+                       "achieved": out["mixed"]["products_tflops"], "peak": peak, "unit": "TFLOP/s",
+                       "frac": out["mixed"]["frac_of_bf16_peak"],
+                       "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"}
+    return out
+
+
 def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024,
              rank: int = 0, world: int = 1) -> dict:
     """The parameter-scan workload (config 4): n_runs seeded uneven capillary runs, stepped together.
@@ -464,17 +533,21 @@ def main() -> int:
                              "steps after --warmup), e.g. under ncu; prints its JSON")
     parser.add_argument("--surrogate-only", type=int, default=0, metavar="POINTS",
                         help="only the surrogate's tcgen05 inference over POINTS points; prints its JSON")
+    parser.add_argument("--modal-only", action="store_true",
+                        help="only the modal transform's products at a config-3 size; prints its JSON")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.scan_only or args.surrogate_only:
+    if args.scan_only or args.surrogate_only or args.modal_only:
         import torch
 
         torch.cuda.set_device(local)
         if args.scan_only:
             result = scan_leg(local, args.scan_only, args.scan_steps, warmup=args.warmup)
+        elif args.modal_only:
+            result = modal_products_leg(local)
         else:
             result = surrogate_leg(local, points=args.surrogate_only)
         print(json.dumps(result), flush=True)
@@ -603,6 +676,7 @@ def main() -> int:
 
     runs_result = None if args.config2_only else runs_leg(local)
     surrogate_result = None if args.config2_only else surrogate_leg(local)
+    modal_result = None if args.config2_only else modal_products_leg(local)
     scan_result = None
     if args.scan_runs > 0 and not args.config2_only:
         scan_result = scan_leg(local, args.scan_runs, args.scan_steps, warmup=3, rank=rank, world=world)
@@ -615,7 +689,7 @@ def main() -> int:
             "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "clocks": clocks.summary(), "runs": runs_result, "scan": scan_result,
-            "surrogate": surrogate_result}
+            "surrogate": surrogate_result, "modal_products": modal_result}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del session, s2

@@ -31,8 +31,12 @@ def policy(g, kind: str) -> dict:
 
 
 def fixed_schedule(g):
-    """The fixed run's steps: uniform between the first and last plane, one per row."""
+    """The fixed run's steps: uniform between the first and last plane, of the size the
+    history records (its rows may be one per step or one per plane)."""
     zs = g["fixed.z"]
-    n = len(g["fixed.history"]) if "fixed.history" in g.files else 100
+    if "fixed.history" in g.files:
+        n = int(round(zs[-1] / g["fixed.history"][0, 1]))
+    else:
+        n = 100
     edges = np.linspace(0.0, zs[-1], n + 1)
     return np.diff(edges), edges
