@@ -257,6 +257,7 @@ struct sp_workspace {
   int kpad_modes = 0, kpad_nodes = 0;
   DevBuf<double> node_field, node_streams;
   DevBuf<uint16_t> s_parts, w_parts, modal_parts, node_parts;
+  DevBuf<double> proj_scratch;  // the projections' split-K partial tiles (FP32 in the mixed form)
   // the mixed-precision form's FP32 copies of the source evaluation's buffers
   int precision = SP_PRECISION_FP64;
   struct {
@@ -530,7 +531,8 @@ static void eval_source_gemm(sp_workspace* ws, const double2* lab, int slot, boo
       KernelTimer t(ws, SP_K_PROJECT);
       CUDA_CHECK(modal_projection_split3(ws->w_parts.p, ws->f32.node_streams.p, ws->node_parts.p,
                                          ws->f32.proj.p, n_streams, d.n_modes, d.n_nodes, d.n_to,
-                                         ws->kpad_nodes, stride, taper, status, ws->stream));
+                                         ws->kpad_nodes, stride, taper, status,
+                                         reinterpret_cast<float*>(ws->proj_scratch.p), ws->stream));
     }
     const auto fa = forward_args<float>(ws);
     { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
@@ -547,7 +549,7 @@ static void eval_source_gemm(sp_workspace* ws, const double2* lab, int slot, boo
     {
       KernelTimer t(ws, SP_K_PROJECT);
       CUDA_CHECK(modal_projection_f64(ws->projection.p, ws->node_streams.p, ws->proj.p, n_streams, d.n_modes,
-                                      d.n_nodes, d.n_to, stride, taper, ws->stream));
+                                      d.n_nodes, d.n_to, stride, taper, ws->proj_scratch.p, ws->stream));
     }
     const auto fa = forward_args<double>(ws);
     { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
@@ -717,6 +719,7 @@ static void build_workspace(sp_workspace* ws) {
     const size_t field = (size_t)d.n_nodes * d.n_to;
     ws->kpad_modes = modal_kpad(d.n_modes);
     ws->kpad_nodes = modal_kpad(d.n_nodes);
+    ws->proj_scratch.alloc(modal_projection_scratch(d.n_modes, d.n_nodes, d.n_to));
     if (ws->precision == SP_PRECISION_MIXED) {
       ws->f32.node_field.alloc(field);
       ws->f32.node_streams.alloc(3 * field);
@@ -752,7 +755,8 @@ static void build_workspace(sp_workspace* ws) {
   ws->launches = 5;
   if (ws->gemm) {  // inverse, synthesis, column, one projection per stream, forward, output
     const int per_product = ws->precision == SP_PRECISION_MIXED ? 2 : 1;  // (split,) product
-    ws->launches = 4 + per_product * (1 + (d.plasma_enabled ? 3 : 1));
+    const int streams = d.plasma_enabled ? 3 : 1;  // each: (split,) product, reduction of the K splits
+    ws->launches = 4 + per_product + (per_product + 1) * streams;
   }
   if (ws->precision == SP_PRECISION_MIXED) build_mixed(ws, tw, rc, taps);
   if (d.grid_kind == 1) {

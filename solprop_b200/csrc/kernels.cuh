@@ -192,15 +192,18 @@ cudaError_t configure_modal_gemm();
 void split3_host(const double* src, int rows, int cols, int ld_out, std::vector<uint16_t>& out);
 cudaError_t modal_synthesis_f64(const double* S, const double* modal, double* E, int n_nodes, int n_modes,
                                 int n_to, const double* taper, cudaStream_t s);
+// scratch the projections' split-K partial tiles need (elements of either form's type)
+size_t modal_projection_scratch(int n_modes, int n_nodes, int n_to);
 cudaError_t modal_projection_f64(const double* W, const double* node_streams, double* out, int n_streams,
                                  int n_modes, int n_nodes, int n_to, size_t out_stride, const double* taper,
-                                 cudaStream_t s);
+                                 double* scratch, cudaStream_t s);
 cudaError_t modal_synthesis_split3(const uint16_t* s_parts, const double* modal, uint16_t* modal_parts, float* E,
                                    int n_nodes, int n_modes, int n_to, int kpad, const double* taper,
                                    double* status, cudaStream_t s);
 cudaError_t modal_projection_split3(const uint16_t* w_parts, const float* node_streams, uint16_t* node_parts,
                                     float* out, int n_streams, int n_modes, int n_nodes, int n_to, int kpad,
-                                    size_t out_stride, const double* taper, double* status, cudaStream_t s);
+                                    size_t out_stride, const double* taper, double* status, float* scratch,
+                                    cudaStream_t s);
 cudaError_t launch_statistics(const StatisticsArgs& a, bool peaks, cudaStream_t s);
 int fft_cluster_size(int n_to);
 template <class R>

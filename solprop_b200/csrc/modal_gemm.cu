@@ -52,7 +52,7 @@ struct SplitMaps {
 template <int BN>
 __global__ void __launch_bounds__(kGThreads, 1)
     k_gemm_split3(const __grid_constant__ SplitMaps maps, float* C, int ldc, int M, int n_valid, int K,
-                  int transposed, const double* scale, int divide, double* status) {
+                  int transposed, const double* scale, int divide, double* status, size_t split_stride) {
   constexpr uint32_t kStage = stage_bytes<BN>();
   constexpr uint32_t kIdescN = idesc_bf16(kGM, BN);
   extern __shared__ __align__(1024) unsigned char g_raw[];
@@ -64,8 +64,13 @@ __global__ void __launch_bounds__(kGThreads, 1)
   __shared__ int failed;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int m0 = blockIdx.y * kGM, n0 = blockIdx.x * BN;
-  const int n_k = K / kGK;
+  // split K: CTA z of gridDim.z takes K slices [ks0, ks1) of every term and writes its own
+  // partial tile, C + z split_stride (added in split order by k_reduce_splits)
+  const int n_all = K / kGK;
+  const int ks0 = (int)((long)blockIdx.z * n_all / gridDim.z), ks1 = (int)((long)(blockIdx.z + 1) * n_all / gridDim.z);
+  const int n_k = ks1 - ks0;
   const int total = 6 * n_k;
+  C += (size_t)blockIdx.z * split_stride;
   if (threadIdx.x == 0) {
     failed = 0;
     for (int s = 0; s < kGStages; ++s) {
@@ -95,7 +100,7 @@ __global__ void __launch_bounds__(kGThreads, 1)
         failed = 1;
         break;
       }
-      const int term = it / n_k, ks = it % n_k;
+      const int term = it / n_k, ks = ks0 + it % n_k;
       unsigned char* stage = ring + (size_t)s * kStage;
       mbar_expect_tx(&full[s], kStage);
       tma_load_2d(stage, &maps.a[c_terms[term][0]], &full[s], ks * kGK, m0);
@@ -147,8 +152,8 @@ __global__ void __launch_bounds__(kGThreads, 1)
     for (int j = 0; j < 16; ++j) tile[row * kPitch + c_lo + j] = __uint_as_float(r[j]);
   }
   __syncthreads();
-  if (ok && !failed) {
-    const float f = (float)(divide ? 1.0 / *scale : *scale);
+  if (ok && !failed && total > 0) {
+    const float f = scale ? (float)(divide ? 1.0 / *scale : *scale) : 1.0f;
     if (!transposed) {
       // C[m][n]: a warp per row, lanes along n
       for (int rr = warp; rr < kGM && m0 + rr < M; rr += kGThreads / 32)
@@ -166,6 +171,22 @@ __global__ void __launch_bounds__(kGThreads, 1)
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN) : "memory");
   if (threadIdx.x == 0 && (!ok || failed)) *status = 1.0;
+}
+
+// out[i] = f sum_z partials[z][i], the splits added in order; f = *scale or 1 / *scale
+template <class T>
+__global__ void k_reduce_splits(const T* __restrict__ partials, int splits, size_t count, size_t stride,
+                                T* __restrict__ out, size_t out_stride, int rows, const double* scale,
+                                int divide) {
+  // `rows` blocks of `count` values, block r at r * stride in each split and r * out_stride out
+  const T f = (T)(divide ? 1.0 / *scale : *scale);
+  const size_t total = (size_t)rows * count;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < total; g += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = g / count, i = g % count;
+    T acc = T(0);
+    for (int z = 0; z < splits; ++z) acc += partials[(size_t)z * rows * stride + r * stride + i];
+    out[r * out_stride + i] = f * acc;
+  }
 }
 
 // the three BF16 parts of x, in the order hi, mid, lo
@@ -209,13 +230,17 @@ __global__ void __launch_bounds__(256) k_split3_transpose(const T* __restrict__ 
 constexpr int kFM = 64, kFN = 64, kFK = 16;
 __global__ void __launch_bounds__(256) k_gemm_f64(const double* __restrict__ A, int lda, const double* __restrict__ B,
                                                   int ldb, double* __restrict__ C, int ldc, int M, int N, int K,
-                                                  const double* scale, int divide) {
+                                                  const double* scale, int divide, size_t split_stride) {
   __shared__ double As[kFK][kFM + 1];
   __shared__ double Bs[kFK][kFN + 1];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   const int m0 = blockIdx.y * kFM, n0 = blockIdx.x * kFN;
+  // split K over gridDim.z: this CTA's slices of kFK, its partial tile at C + z split_stride
+  const int n_all = (K + kFK - 1) / kFK;
+  const int kb0 = (int)((long)blockIdx.z * n_all / gridDim.z), kb1 = (int)((long)(blockIdx.z + 1) * n_all / gridDim.z);
+  C += (size_t)blockIdx.z * split_stride;
   double acc[4][4] = {};
-  for (int k0 = 0; k0 < K; k0 += kFK) {
+  for (int k0 = kb0 * kFK; k0 < kb1 * kFK; k0 += kFK) {
     for (int i = threadIdx.x; i < kFM * kFK; i += 256) {
       const int mm = i / kFK, kk = i % kFK;
       As[kk][mm] = (m0 + mm < M && k0 + kk < K) ? A[(size_t)(m0 + mm) * lda + k0 + kk] : 0.0;
@@ -239,7 +264,7 @@ __global__ void __launch_bounds__(256) k_gemm_f64(const double* __restrict__ A, 
     }
     __syncthreads();
   }
-  const double s = *scale;
+  const double s = scale ? *scale : 1.0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int m = m0 + ty + 16 * i;
@@ -247,9 +272,17 @@ __global__ void __launch_bounds__(256) k_gemm_f64(const double* __restrict__ A, 
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int n = n0 + tx + 16 * j;
-      if (n < N) C[(size_t)m * ldc + n] = divide ? acc[i][j] / s : s * acc[i][j];
+      if (n < N) C[(size_t)m * ldc + n] = !scale ? acc[i][j] : divide ? acc[i][j] / s : s * acc[i][j];
     }
   }
+}
+
+// split-K factor: enough CTAs for about four waves of the 148 SMs, each split at least
+// `min_slices` K slices long
+int splits_for(int tiles, int k_slices, int min_slices) {
+  int s = 1;
+  while (tiles * s < 4 * 148 && k_slices / (2 * s) >= min_slices) s *= 2;
+  return s;
 }
 
 bool split_maps(SplitMaps* maps, const uint16_t* a_parts, int a_rows, const uint16_t* b_parts, int b_rows,
@@ -301,17 +334,30 @@ void split3_host(const double* src, int rows, int cols, int ld_out, std::vector<
 cudaError_t modal_synthesis_f64(const double* S, const double* modal, double* E, int n_nodes, int n_modes,
                                 int n_to, const double* taper, cudaStream_t s) {
   const dim3 grid((n_to + kFN - 1) / kFN, (n_nodes + kFM - 1) / kFM);
-  k_gemm_f64<<<grid, 256, 0, s>>>(S, n_modes, modal, n_to, E, n_to, n_nodes, n_to, n_modes, taper, 0);
+  k_gemm_f64<<<grid, 256, 0, s>>>(S, n_modes, modal, n_to, E, n_to, n_nodes, n_to, n_modes, taper, 0, 0);
   return cudaGetLastError();
+}
+
+size_t modal_projection_scratch(int n_modes, int n_nodes, int n_to) {
+  const int tiles_f64 = ((n_to + kFN - 1) / kFN) * ((n_modes + kFM - 1) / kFM);
+  const int tiles_tc = (n_modes + 63) / 64 * ((n_to + kGM - 1) / kGM);
+  const int s = std::max(splits_for(tiles_f64, (n_nodes + kFK - 1) / kFK, 16),
+                         splits_for(tiles_tc, modal_kpad(n_nodes) / kGK, 4));
+  return (size_t)s * n_modes * n_to;
 }
 
 cudaError_t modal_projection_f64(const double* W, const double* node_streams, double* out, int n_streams,
                                  int n_modes, int n_nodes, int n_to, size_t out_stride, const double* taper,
-                                 cudaStream_t s) {
-  const dim3 grid((n_to + kFN - 1) / kFN, (n_modes + kFM - 1) / kFM);
+                                 double* scratch, cudaStream_t s) {
+  const int tiles = ((n_to + kFN - 1) / kFN) * ((n_modes + kFM - 1) / kFM);
+  const int splits = splits_for(tiles, (n_nodes + kFK - 1) / kFK, 16);
+  const size_t part = (size_t)n_modes * n_to;
+  const dim3 grid((n_to + kFN - 1) / kFN, (n_modes + kFM - 1) / kFM, splits);
   for (int st = 0; st < n_streams; ++st) {
-    k_gemm_f64<<<grid, 256, 0, s>>>(W, n_nodes, node_streams + (size_t)st * n_nodes * n_to, n_to,
-                                    out + st * out_stride, n_to, n_modes, n_to, n_nodes, taper, 1);
+    k_gemm_f64<<<grid, 256, 0, s>>>(W, n_nodes, node_streams + (size_t)st * n_nodes * n_to, n_to, scratch, n_to,
+                                    n_modes, n_to, n_nodes, nullptr, 1, part);
+    k_reduce_splits<double><<<592, 256, 0, s>>>(scratch, splits, part, part, out + st * out_stride, part, 1,
+                                                taper, 1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
@@ -328,13 +374,17 @@ cudaError_t modal_synthesis_split3(const uint16_t* s_parts, const double* modal,
   if (!split_maps(&maps, s_parts, n_nodes, modal_parts, n_to, kpad, 256)) return cudaErrorInvalidValue;
   const dim3 grid((n_to + 255) / 256, (n_nodes + kGM - 1) / kGM);
   k_gemm_split3<256><<<grid, kGThreads, gemm_smem<256>(), s>>>(maps, E, n_to, n_nodes, n_to, kpad, 0, taper, 0,
-                                                                status);
+                                                                status, 0);
   return cudaGetLastError();
 }
 
 cudaError_t modal_projection_split3(const uint16_t* w_parts, const float* node_streams, uint16_t* node_parts,
                                     float* out, int n_streams, int n_modes, int n_nodes, int n_to, int kpad,
-                                    size_t out_stride, const double* taper, double* status, cudaStream_t s) {
+                                    size_t out_stride, const double* taper, double* status, float* scratch,
+                                    cudaStream_t s) {
+  const int tiles = (n_modes + 63) / 64 * ((n_to + kGM - 1) / kGM);
+  const int splits = splits_for(tiles, kpad / kGK, 4);
+  const size_t part = (size_t)n_modes * n_to;
   for (int st = 0; st < n_streams; ++st) {
     // A = the stream transposed, (n_to, kpad) in three parts
     cudaError_t e = split_transpose<float>(node_streams + (size_t)st * n_nodes * n_to, n_nodes, n_to, n_to,
@@ -342,9 +392,11 @@ cudaError_t modal_projection_split3(const uint16_t* w_parts, const float* node_s
     if (e != cudaSuccess) return e;
     SplitMaps maps;
     if (!split_maps(&maps, node_parts, n_to, w_parts, n_modes, kpad, 64)) return cudaErrorInvalidValue;
-    const dim3 grid((n_modes + 63) / 64, (n_to + kGM - 1) / kGM);
-    k_gemm_split3<64><<<grid, kGThreads, gemm_smem<64>(), s>>>(maps, out + st * out_stride, n_to, n_to, n_modes,
-                                                               kpad, 1, taper, 1, status);
+    const dim3 grid((n_modes + 63) / 64, (n_to + kGM - 1) / kGM, splits);
+    k_gemm_split3<64><<<grid, kGThreads, gemm_smem<64>(), s>>>(maps, scratch, n_to, n_to, n_modes, kpad, 1,
+                                                               nullptr, 1, status, part);
+    k_reduce_splits<float><<<592, 256, 0, s>>>(scratch, splits, part, part, out + st * out_stride, part, 1, taper,
+                                               1);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
