@@ -253,7 +253,7 @@ def modal_products_record(n_modes: int = 30, n_nodes: int = 16384):
     return rec, pol
 
 
-def modal_products_leg(device: int, repeats: int = 3) -> dict:
+def modal_products_leg(device: int, repeats: int = 3, n_nodes: int = 16384) -> dict:
     """The modal transform as products at a config-3 size (30 modes, 16 384 nodes, 16 384
     samples; config 3's own route -- envelope grid, vector modes, tensor Raman -- is not
     built): per source evaluation, the products' device time (synthesis and the three
@@ -264,12 +264,12 @@ def modal_products_leg(device: int, repeats: int = 3) -> dict:
     for each."""
     from solprop_b200 import _lib
 
-    rec, pol = modal_products_record()
+    rec, pol = modal_products_record(n_nodes=n_nodes)
     flops = 2.0 * rec.n_nodes * rec.n_modes * rec.n_to * (1 + 3)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = peaks.get("bf16_tflops", 1590.0)
     problem = _lib.Problem(rec)
-    out = {"workload": "modal transform: 30 modes x 16384 nodes x 16384 samples, config 2 grid and "
+    out = {"workload": f"modal transform: 30 modes x {n_nodes} nodes x 16384 samples, config 2 grid and "
                        "response (synthetic operands)", "flops_per_evaluation": flops}
     lab = rec.field0
     for precision in ("mixed", "fp64"):
@@ -533,8 +533,9 @@ def main() -> int:
                              "steps after --warmup), e.g. under ncu; prints its JSON")
     parser.add_argument("--surrogate-only", type=int, default=0, metavar="POINTS",
                         help="only the surrogate's tcgen05 inference over POINTS points; prints its JSON")
-    parser.add_argument("--modal-only", action="store_true",
-                        help="only the modal transform's products at a config-3 size; prints its JSON")
+    parser.add_argument("--modal-only", type=int, nargs="?", const=16384, default=0, metavar="NODES",
+                        help="only the modal transform's products (30 modes, NODES nodes, default 16384: "
+                             "config 3's size); prints its JSON")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -547,7 +548,7 @@ def main() -> int:
         if args.scan_only:
             result = scan_leg(local, args.scan_only, args.scan_steps, warmup=args.warmup)
         elif args.modal_only:
-            result = modal_products_leg(local)
+            result = modal_products_leg(local, n_nodes=args.modal_only)
         else:
             result = surrogate_leg(local, points=args.surrogate_only)
         print(json.dumps(result), flush=True)

@@ -199,29 +199,36 @@ __device__ __forceinline__ void split3(T x, __nv_bfloat16 (&p)[3]) {
   p[2] = __float2bfloat16_rn(r1 - __bfloat162float(p[1]));
 }
 
-// out[p][r][c] = part p of src[c][r] (c < C; 0 for C <= c < ld_out), r < R; 32 x 32 tiles
-// through shared memory so that both sides are coalesced.  src rows have pitch ld_src.
+// out[p][r][c] = part p of src[c][r] (c < C; 0 for C <= c < ld_out), r < R; 64 (c) x 32 (r)
+// tiles through shared memory: the source is read in 128-byte rows, and each warp stores a
+// part's 64 columns of one row as 32 BF16 pairs, a 128-byte row.  src rows have pitch
+// ld_src; ld_out is even.
 template <class T>
 __global__ void __launch_bounds__(256) k_split3_transpose(const T* __restrict__ src, int C, int R, int ld_src,
                                                           __nv_bfloat16* __restrict__ out, int ld_out) {
-  __shared__ T tile[32][33];
-  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  __shared__ T tile[64][33];
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 64;
   const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 32 x 8
-  for (int j = ty; j < 32; j += 8) {
+  for (int j = ty; j < 64; j += 8) {
     const int c = c0 + j, r = r0 + tx;
     tile[j][tx] = (c < C && r < R) ? src[(size_t)c * ld_src + r] : T(0);
   }
   __syncthreads();
   const size_t panel = (size_t)R * ld_out;
   for (int j = ty; j < 32; j += 8) {
-    const int r = r0 + j, c = c0 + tx;
+    const int r = r0 + j, c = c0 + 2 * tx;
     if (r >= R || c >= ld_out) continue;
-    __nv_bfloat16 p[3];
-    split3(tile[tx][j], p);
+    __nv_bfloat16 a[3], b[3];
+    split3(tile[2 * tx][j], a);
+    split3(tile[2 * tx + 1][j], b);
     const size_t at = (size_t)r * ld_out + c;
-    out[at] = p[0];
-    out[panel + at] = p[1];
-    out[2 * panel + at] = p[2];
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      __nv_bfloat162 v;
+      v.x = a[p];
+      v.y = b[p];
+      *reinterpret_cast<__nv_bfloat162*>(out + p * panel + at) = v;
+    }
   }
 }
 
@@ -297,7 +304,7 @@ bool split_maps(SplitMaps* maps, const uint16_t* a_parts, int a_rows, const uint
 
 template <class T>
 cudaError_t split_transpose(const T* src, int C, int R, int ld_src, uint16_t* out, int ld_out, cudaStream_t s) {
-  const dim3 grid((R + 31) / 32, (ld_out + 31) / 32);
+  const dim3 grid((R + 31) / 32, (ld_out + 63) / 64);
   k_split3_transpose<T><<<grid, 256, 0, s>>>(src, C, R, ld_src, reinterpret_cast<__nv_bfloat16*>(out), ld_out);
   return cudaGetLastError();
 }
