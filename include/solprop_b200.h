@@ -209,7 +209,7 @@ sp_status sp_workspace_create_ex(const sp_problem* problem, int device, int prec
  *                   tcgen05 products of three-part BF16 splits of each operand, accumulated
  *                   in FP32 (the reference's synthesis and projection GEMMs,
  *                   native/src/general/trial.cpp:181-315, transforms/gemm.hpp:55-275) --
- *                   up to 64 modal columns, field grid, one field component;
+ *                   up to 1024 modal columns, field grid, one field component;
  *   SP_MODAL_AUTO   FUSED up to 8 columns, GEMM above. */
 enum { SP_MODAL_AUTO = 0, SP_MODAL_FUSED = 1, SP_MODAL_GEMM = 2 };
 sp_status sp_workspace_create_ex2(const sp_problem* problem, int device, int precision, int modal,

@@ -200,7 +200,7 @@ static void validate(const sp_problem_desc* d) {
   if (d->n_pol * d->n_pol_transform != 1)
     throw Failure(SP_ERR_REFUSED, "two field components (vector Kerr) are not built yet");
   if (d->n_modes * d->n_pol > kMaxGemmModes)
-    throw Failure(SP_ERR_REFUSED, "more than 64 modal columns");
+    throw Failure(SP_ERR_REFUSED, "more than 1024 modal columns");
   if (envelope) {
     // the envelope route: one modal column on one node (the single-mode GNLSE)
     if (d->n_modes * d->n_pol != 1 || d->n_nodes != 1)

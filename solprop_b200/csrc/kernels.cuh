@@ -186,7 +186,7 @@ cudaError_t configure_statistics_kernels();
 
 // The modal transform as products (modal_gemm.cu): the GEMM route.  The mixed form's
 // operands are three BF16 parts (hi, mid, lo) per value, panel after panel, rows of kpad.
-constexpr int kMaxGemmModes = 64;   // modal columns the route's projection tile holds
+constexpr int kMaxGemmModes = 1024;  // modal columns the products take (the projection tiles them by 64)
 int modal_kpad(int k);              // k rounded up to the products' 64-wide K slices
 cudaError_t configure_modal_gemm();
 void split3_host(const double* src, int rows, int cols, int ld_out, std::vector<uint16_t>& out);

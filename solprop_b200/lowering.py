@@ -42,8 +42,22 @@ def lower(problem) -> ProblemRecord:
     grids, linear, transform = problem.grids, problem.linear, problem.transform
     responses, initial = problem.responses, problem.initial
     n_modes, n_pol, n_omega = problem.shape
-    if transform.geometry is not None or transform.modal_tables is not None:
-        raise BackendRefusal(f"route {transform.kind!r}: only the modal route is lowered")
+    geometry = transform.geometry
+    if transform.modal_tables is not None:
+        raise BackendRefusal("the general modal route's tables are not lowered")
+    if geometry is not None:
+        # the radial free-space route is the modal route's arithmetic on a square Hankel
+        # pair (its plasma projected after the nodes' transforms: the same linear maps in
+        # another order, backends/numpy_ref/source.py:702-735); Cartesian, line and slab
+        # grids transform in space instead, and the radial collar adds a spatial matrix
+        if geometry.kind != "radial":
+            raise BackendRefusal(f"route {transform.kind!r}: the modal and radial routes are lowered")
+        if np.any(np.asarray(geometry.absorber_rate)):
+            raise BackendRefusal("the radial spatial absorber (a spectral-space matrix) is not executed")
+    if responses.temporal_absorber_fine is not None and responses.absorber_scheme != "nonlinear":
+        raise BackendRefusal(
+            f"the {responses.absorber_scheme!r} temporal absorber: the device march takes the "
+            "in-stage (nonlinear) scheme")
     if linear.coupled_flow is not None:
         raise BackendRefusal("a coupled flow is not executed by this backend")
     if linear.phi_representation not in ("constant", "expansion"):

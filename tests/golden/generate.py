@@ -354,6 +354,52 @@ def gnlse_case(case, seed):
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
 
 
+def radial_case(case, *, n_r, length, seed):
+    """The radial free-space route (``Simulation.from_free`` on a ``RadialGrid``): an
+    argon filament with Kerr (the real cubic form) and ADK plasma, the in-stage collar,
+    exponential Adams at the route's default rtol; the Hankel pair is square, n_r x n_r.
+    The fixed schedule steps with DOPRI5, whose stability interval admits its steps under
+    the in-stage collar."""
+    from solprop.driver.settings import SimulationSettings
+    from solprop.grid import RadialGrid
+    from solprop.nonlinear.responses import KerrResponse, PlasmaResponse
+    from solprop.pulses import GaussianPulse, SpatialPulse
+    from solprop.spatial import SpatialMedium
+    from solprop.stats import StatsSpec
+
+    species = gas_species("Ar")
+    medium = SpatialMedium(Mixture.fill({species: 1.0}, 1.0))
+    eps0 = 8.8541878188e-12
+
+    def build(schedule=None, n_save=3, integrator=None):
+        grid = FieldGrid.from_limits(length, 800e-9, (350e-9, 2e-6), 150e-15, fft_size="pow2")
+        responses = [KerrResponse(GAMMA3["Ar"] * eps0, thg=True), PlasmaResponse(species, adk_oracle("Ar"))]
+        pulse = SpatialPulse(GaussianPulse(wavelength=800e-9, fwhm=30e-15, energy=0.5e-3), 100e-6)
+        settings = SimulationSettings(backend="numpy_ref", absorber_scheme="nonlinear", boundary_check=None,
+                                      ionisation_field_range=(1e7, 1e11), stats=StatsSpec(names=()),
+                                      schedule=schedule, n_save=n_save, integrator=integrator)
+        return Simulation.from_free(grid, RadialGrid(1.5e-3, n_r), medium, responses, pulse, settings=settings)
+
+    sim = build()
+    problem = sim.translate()
+    golden = source_fixture(sim, problem, [0.0, 0.4 * length], seed)
+    _, zs, states, (hist, counts), wall = drive(build())
+    golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.history": hist,
+                   "adaptive.counts": counts, "adaptive.wall": np.array(wall),
+                   "adaptive.policy": drive.policy})
+    print(f"{case}: adaptive run {counts} attempts/rejected in {wall:.2f} s", flush=True)
+    # the fixed schedule: 50 DOPRI5 steps, inside the in-stage collar's stability limit for
+    # that method (the explicit Adams march's is about 7 um here)
+    planes = np.linspace(0.0, length, 6)
+    fixed_problem, zs, states, (hist, counts), wall = drive(
+        build(FixedSchedule.uniform(0.0, length, length / 50, save_planes=planes), n_save=6,
+              integrator=RungeKutta()))
+    golden.update({"fixed.z": zs, "fixed.states": states, "fixed.history": hist,
+                   "fixed.policy": drive.policy})
+    write(case, problem, golden)
+    save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
+
+
 def workload_case(case, *, seed, n_save=3, **common):
     """A full-size configuration: the problem, the march policy, two reference source
     evaluations, and the reference's whole adaptive run (exponential Adams at the route's
@@ -497,6 +543,9 @@ if __name__ == "__main__":
         cap_case("cap12_ne", gas="Ne", pressure=1.5, length=0.02, limits=(200e-9, 4e-6),
                  trange=100e-15, energy=60e-6, fwhm=10e-15, modes=12, n_r=96,
                  radial_rule="gauss", fixed_dz=0.001, n_fixed_planes=6, seed=6)
+    if not only or "radial_ar" in only:
+        # the radial free-space route on 48 radial nodes (a 48 x 48 Hankel pair)
+        radial_case("radial_ar", n_r=48, length=0.01, seed=7)
     if not only or "gnlse_raman" in only:
         gnlse_case("gnlse_raman", seed=3)
     if not only or "config2" in only:
