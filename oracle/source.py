@@ -255,8 +255,8 @@ def lab_source(rec, lab: np.ndarray, z: float, *, quiet: bool = False, out: dict
     if rec.kerr_enabled:
         total = total + kerr_polarisation(rec, field_t, sc.kerr_density, rec.carrier)
     if rec.raman_enabled:
-        density = 1.0 if len(rec.raman_rates) > 1 and False else sc.raman_density
-        total = total + raman_polarisation(rec, field_t, raman_spectrum(rec, sc.raman_rates), density)
+        spectrum = raman_spectrum(rec, sc.raman_rates)
+        total = total + raman_polarisation(rec, field_t, spectrum, sc.raman_density)
     polarisation = total * rec.t_window
     projected = project(rec, polarisation, sc.taper)
     spectrum = to_frequency(rec, projected)

@@ -69,6 +69,7 @@ void ensure_configured(int device) {
   CUDA_CHECK(configure_source_kernels());
   CUDA_CHECK(configure_statistics_kernels());
   CUDA_CHECK(configure_modal_gemm());
+  CUDA_CHECK(configure_raman_kernels());
   g_configured[device] = true;
 }
 
@@ -218,7 +219,13 @@ static void validate(const sp_problem_desc* d) {
       if (d->raman_thg) throw Failure(SP_ERR_REFUSED, "a third-harmonic Raman drive on the envelope grid");
     }
   } else {
-    if (d->raman_enabled) throw Failure(SP_ERR_REFUSED, "field-grid Raman is not built yet");
+    if (d->raman_enabled) {
+      need(d->raman_terms >= 1 && d->raman_terms <= 4 && d->raman_undamped, "Raman terms");
+      if (!d->raman_thg)
+        throw Failure(SP_ERR_REFUSED, "the field grid's Raman drive without the harmonic (an analytic signal)");
+      if (d->n_to > kMaxRamanSamples)
+        throw Failure(SP_ERR_REFUSED, "field-grid Raman above 4096 fine samples");
+    }
     if (d->kerr_enabled && d->kerr_analytic)
       throw Failure(SP_ERR_REFUSED, "the analytic Kerr cubic belongs to the envelope grid");
   }
@@ -251,6 +258,7 @@ struct sp_workspace {
   DevBuf<double2> env_twiddles;       // envelope route: exp(-2 pi i m / (2 n_to)), m < n_to
   DevBuf<double> raman_undamped;
   DevBuf<double> stat_power, stat_out, stat_weight;  // plane statistics, on first use
+  DevBuf<double2> raman_spectrum;  // field-grid Raman: the damped kernel's spectrum (n_to + 1)
   // the modal transform as products (SP_MODAL_GEMM): the node field and streams in HBM;
   // the mixed form's operands in three BF16 parts, rows padded to kpad
   bool gemm = false;
@@ -504,6 +512,23 @@ static OutputArgs output_args(const sp_workspace* ws, const StageScalarsDev* sta
                     absorber};
 }
 
+// The field-grid Raman pass's arguments (the doubled grid's table, the stage's rates)
+static RamanArgs raman_args(const sp_workspace* ws, int slot) {
+  const sp_problem_desc& d = ws->P->d;
+  RamanArgs ra{};
+  ra.stage = ws->stage.p + slot;
+  ra.undamped = ws->raman_undamped.p;
+  ra.spectrum = ws->raman_spectrum.p;
+  ra.twiddles = ws->env_twiddles.p;
+  ra.t_window = ws->t_window.p;
+  ra.n_to = d.n_to;
+  ra.log_n_to = ws->log_n_to;
+  ra.terms = d.raman_terms;
+  ra.fraction = d.raman_fraction;
+  ra.dt = d.dt_fine;
+  return ra;
+}
+
 // The field grid's source on the GEMM route: inverse transforms, the synthesis product
 // (node field), the response column over the node field (node streams), the projection
 // products (the projected streams, group 0's rows), forward transforms.  The taper tau
@@ -527,6 +552,11 @@ static void eval_source_gemm(sp_workspace* ws, const double2* lab, int slot, boo
     ca.node_field = ws->f32.node_field.p;
     ca.node_streams = ws->f32.node_streams.p;
     { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column_nodes(ca, ws->stream)); }
+    if (d.raman_enabled) {
+      KernelTimer t(ws, SP_K_COLUMN);
+      CUDA_CHECK(launch_raman(raman_args(ws, slot), ws->f32.node_field.p, ws->f32.node_streams.p, d.n_nodes,
+                              ws->stream));
+    }
     {
       KernelTimer t(ws, SP_K_PROJECT);
       CUDA_CHECK(modal_projection_split3(ws->w_parts.p, ws->f32.node_streams.p, ws->node_parts.p,
@@ -546,6 +576,10 @@ static void eval_source_gemm(sp_workspace* ws, const double2* lab, int slot, boo
     ca.node_field = ws->node_field.p;
     ca.node_streams = ws->node_streams.p;
     { KernelTimer t(ws, SP_K_COLUMN); CUDA_CHECK(launch_column_nodes(ca, ws->stream)); }
+    if (d.raman_enabled) {
+      KernelTimer t(ws, SP_K_COLUMN);
+      CUDA_CHECK(launch_raman(raman_args(ws, slot), ws->node_field.p, ws->node_streams.p, d.n_nodes, ws->stream));
+    }
     {
       KernelTimer t(ws, SP_K_PROJECT);
       CUDA_CHECK(modal_projection_f64(ws->projection.p, ws->node_streams.p, ws->proj.p, n_streams, d.n_modes,
@@ -756,10 +790,10 @@ static void build_workspace(sp_workspace* ws) {
   if (ws->gemm) {  // inverse, synthesis, column, one projection per stream, forward, output
     const int per_product = ws->precision == SP_PRECISION_MIXED ? 2 : 1;  // (split,) product
     const int streams = d.plasma_enabled ? 3 : 1;  // each: (split,) product, reduction of the K splits
-    ws->launches = 4 + per_product + (per_product + 1) * streams;
+    ws->launches = 4 + per_product + (per_product + 1) * streams + (d.raman_enabled ? 2 : 0);
   }
   if (ws->precision == SP_PRECISION_MIXED) build_mixed(ws, tw, rc, taps);
-  if (d.grid_kind == 1) {
+  if (d.grid_kind == 1 || d.raman_enabled) {  // the doubled grid's table: envelope route, Raman
     std::vector<double2> tw2(d.n_to);
     for (int m = 0; m < d.n_to; ++m) {
       long double ang = two_pi * (long double)m / (long double)(2 * d.n_to);
@@ -767,6 +801,7 @@ static void build_workspace(sp_workspace* ws) {
     }
     ws->env_twiddles.upload(tw2.data(), tw2.size(), s);
     if (d.raman_enabled) ws->raman_undamped.upload(P.raman_undamped.data(), P.raman_undamped.size(), s);
+    if (d.raman_enabled && d.grid_kind == 0) ws->raman_spectrum.alloc((size_t)d.n_to + 1);
     CUDA_CHECK(cudaStreamSynchronize(s));
   }
   CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1425,11 +1460,15 @@ sp_status sp_workspace_create_ex2(const sp_problem* problem, int device, int pre
     const sp_problem_desc& d = problem->d;
     if (precision == SP_PRECISION_MIXED && d.grid_kind == 1)
       throw Failure(SP_ERR_REFUSED, "the mixed precision of the envelope route is not built yet");
-    const bool gemm = modal == SP_MODAL_GEMM || (modal == SP_MODAL_AUTO && problem->n_cols > kMaxModes);
+    const bool field_raman = d.grid_kind == 0 && d.raman_enabled;
+    const bool gemm = modal == SP_MODAL_GEMM ||
+                      (modal == SP_MODAL_AUTO && (problem->n_cols > kMaxModes || field_raman));
     if (gemm && d.grid_kind != 0)
       throw Failure(SP_ERR_REFUSED, "the modal transform's products take the field grid");
     if (!gemm && problem->n_cols > kMaxModes)
       throw Failure(SP_ERR_REFUSED, "more than 8 modal columns take the modal transform's products");
+    if (!gemm && field_raman)
+      throw Failure(SP_ERR_REFUSED, "field-grid Raman takes the modal transform's products (its node field)");
     CUDA_CHECK(cudaSetDevice(device));
     ensure_configured(device);
     auto ws = std::make_unique<sp_workspace>();
@@ -2650,8 +2689,10 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     if (precision != SP_PRECISION_FP64 && precision != SP_PRECISION_MIXED)
       throw Failure(SP_ERR_ARGUMENT, "unknown precision");
     for (int r = 0; r < n_runs; ++r)
-      if (problems[r] && problems[r]->n_cols > kMaxModes)
-        throw Failure(SP_ERR_REFUSED, "a scan's runs take at most 8 modal columns (the fused transform)");
+      if (problems[r] && (problems[r]->n_cols > kMaxModes ||
+                          (problems[r]->d.raman_enabled && problems[r]->d.grid_kind == 0)))
+        throw Failure(SP_ERR_REFUSED,
+                      "a scan's runs take at most 8 modal columns and no field-grid Raman (the fused transform)");
     CUDA_CHECK(cudaSetDevice(device));
     ensure_configured(device);
     auto S = std::make_unique<sp_scan>();
@@ -3042,8 +3083,9 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     if (!problem || !lab || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
     if (problem->d.grid_kind != 0)
       throw Failure(SP_ERR_REFUSED, "the no-allocation entry point takes field-grid problems");
-    if (problem->n_cols > kMaxModes)
-      throw Failure(SP_ERR_REFUSED, "the no-allocation entry point takes at most 8 modal columns");
+    if (problem->n_cols > kMaxModes || (problem->d.raman_enabled && problem->d.grid_kind == 0))
+      throw Failure(SP_ERR_REFUSED,
+                    "the no-allocation entry point takes at most 8 modal columns and no field-grid Raman");
     int device = 0;
     CUDA_CHECK(cudaGetDevice(&device));
     unsigned char* base = noalloc_base(device);

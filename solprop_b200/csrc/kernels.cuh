@@ -184,6 +184,21 @@ struct StatisticsArgs {
 };
 cudaError_t configure_statistics_kernels();
 
+// The Raman response on the field grid (raman_kernels.cu), node by node on the GEMM route.
+constexpr int kMaxRamanSamples = 4096;  // n_to: the doubled grid's packed transform in one CTA
+struct RamanArgs {
+  const StageScalarsDev* stage;  // the damping rates and the Raman density at the stage
+  const double* undamped;        // (terms, 2 n_to)
+  double2* spectrum;             // (n_to + 1): dt rfft of the damped kernel
+  const double2* twiddles;       // exp(-2 pi i m / (2 n_to)), m < n_to
+  const double* t_window;        // (n_to) the window g
+  int n_to, log_n_to, terms;
+  double fraction, dt;
+};
+cudaError_t configure_raman_kernels();
+template <class R>
+cudaError_t launch_raman(const RamanArgs& a, const R* field, R* polarisation, int n_nodes, cudaStream_t s);
+
 // The modal transform as products (modal_gemm.cu): the GEMM route.  The mixed form's
 // operands are three BF16 parts (hi, mid, lo) per value, panel after panel, rows of kpad.
 constexpr int kMaxGemmModes = 1024;  // modal columns the products take (the projection tiles them by 64)

@@ -1,0 +1,138 @@
+// The Raman response on the field grid, node by node, on the modal transform's products
+// route (where the node field lives in HBM): backends/numpy_ref/passes/responses.py:218-290
+// (the damped kernel's spectrum) and 395-498 (the delayed polarisation):
+//
+//   H = dt rfft(f_R sum_r u_r(s) exp(-g_r s dt)),  s in [0, 2 n_to)     once per evaluation
+//   P_R(t) = eps0 rho_R E(t) irfft(H rfft(D))(t),  D = E^2 on [0, n_to), 0 above
+//
+// -- the drive of a field grid that keeps the harmonic, the convolution linear on the
+// doubled, zero-padded grid.  P_R, gated by the window g, is added to the node's
+// polarisation stream after the response column has written the Kerr part there.  Real
+// transforms of length 2 n_to run as complex transforms of length n_to (even samples real,
+// odd imaginary) with the usual unpacking, over the table exp(-2 pi i m / (2 n_to)),
+// m < n_to -- the envelope route's arithmetic (envelope_kernels.cu), in FP64 in both forms.
+#include "fft.cuh"
+#include "kernels.cuh"
+
+namespace sp {
+
+namespace {
+
+constexpr double kEps0 = 8.8541878188e-12;  // vacuum permittivity (F/m), CODATA 2022, as solprop.constants
+constexpr int kRamanThreads = 1024;
+
+// X[k] = E_k + w^k O_k of a packed real transform of length 2 n (k in [0, n]); Z in
+// bit-reversed order, w = exp(-2 pi i k / 2n) = tw[k] (k < n), -1 at k = n
+__device__ __forceinline__ double2 unpack(const double2* Z, const double2* tw, int k, int n, int log_n) {
+  const int kk = k == n ? 0 : k;
+  const int km = k == 0 ? 0 : (n - k == n ? 0 : n - k);
+  const double2 zk = Z[bitrev(kk, log_n)];
+  const double2 zm = cconj(Z[bitrev(km, log_n)]);
+  const double2 e = cscale(0.5, cadd(zk, zm));
+  const double2 o = cscale(0.5, mul_mi(csub(zk, zm)));
+  const double2 w = k < n ? tw[k] : make_double2(-1.0, 0.0);
+  return cadd(e, cmul(w, o));
+}
+
+__global__ void __launch_bounds__(kRamanThreads) k_raman_kernel(RamanArgs a) {
+  extern __shared__ __align__(16) double2 rk_raw[];
+  const int n = a.n_to;
+  double2* B = rk_raw;
+  const StageScalarsDev& st = *a.stage;
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    double v[2];
+    for (int q = 0; q < 2; ++q) {
+      const int s = 2 * m + q;
+      double k = 0.0;
+      for (int r = 0; r < a.terms; ++r)
+        k += a.undamped[(size_t)r * 2 * n + s] * exp(-st.raman_rates[r] * ((double)s * a.dt));
+      v[q] = a.fraction * k;
+    }
+    B[m] = make_double2(v[0], v[1]);
+  }
+  __syncthreads();
+  fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
+  for (int k = threadIdx.x; k <= n; k += blockDim.x) a.spectrum[k] = cscale(a.dt, unpack(B, a.twiddles, k, n, a.log_n_to));
+}
+
+template <class R>
+__global__ void __launch_bounds__(kRamanThreads) k_raman_nodes(RamanArgs a, const R* __restrict__ field,
+                                                                R* __restrict__ polarisation) {
+  extern __shared__ __align__(16) double2 rn_raw[];
+  const int n = a.n_to;
+  double2* B = rn_raw;  // the drive's transform, then the convolution's
+  double2* C = B + n;   // H D
+  __shared__ double2 top;  // bin n
+  const int node = blockIdx.x;
+  const R* e_row = field + (size_t)node * n;
+  // the drive E^2 on [0, n), zero on [n, 2n), packed
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    double v[2] = {0.0, 0.0};
+    if (2 * m < n) {
+      const double e0 = (double)e_row[2 * m], e1 = (double)e_row[2 * m + 1];
+      v[0] = e0 * e0;
+      v[1] = e1 * e1;
+    }
+    B[m] = make_double2(v[0], v[1]);
+  }
+  __syncthreads();
+  fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
+  for (int k = threadIdx.x; k <= n; k += blockDim.x) {
+    const double2 y = cmul(a.spectrum[k], unpack(B, a.twiddles, k, n, a.log_n_to));
+    if (k < n) C[k] = y;
+    else top = y;
+  }
+  __syncthreads();
+  // irfft of length 2n: Z_k = E_k + i O_k, E_k = (Y_k + Y*_{n-k}) / 2,
+  // O_k = (Y_k - Y*_{n-k}) conj(w^k) / 2; the imaginary parts of bins 0 and n dropped
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    double2 yk = C[k], ym = k == 0 ? top : C[n - k];
+    if (k == 0) {
+      yk.y = 0.0;
+      ym.y = 0.0;
+    }
+    ym = cconj(ym);
+    const double2 e = cscale(0.5, cadd(yk, ym));
+    const double2 o = cscale(0.5, cmul(csub(yk, ym), cconj(a.twiddles[k])));
+    B[k] = cadd(e, mul_pi(o));
+  }
+  __syncthreads();
+  fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/true);
+  const StageScalarsDev& st = *a.stage;
+  const double scale = kEps0 * st.raman_density;
+  const double inv_n = 1.0 / (double)n;
+  R* p_row = polarisation + (size_t)node * n;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const double2 z = B[bitrev(t >> 1, a.log_n_to)];
+    const double conv = ((t & 1) ? z.y : z.x) * inv_n;  // irfft's 1 / (2n), with the packing's 2
+    const double p = scale * (double)e_row[t] * conv;
+    p_row[t] = (R)((double)p_row[t] + a.t_window[t] * p);
+  }
+}
+
+}  // namespace
+
+size_t raman_smem(int n_to) { return (size_t)2 * n_to * sizeof(double2); }
+
+cudaError_t configure_raman_kernels() {
+  cudaError_t e = cudaFuncSetAttribute(k_raman_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)raman_smem(kMaxRamanSamples) / 2);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_raman_nodes<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)raman_smem(kMaxRamanSamples));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_raman_nodes<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)raman_smem(kMaxRamanSamples));
+}
+
+template <class R>
+cudaError_t launch_raman(const RamanArgs& a, const R* field, R* polarisation, int n_nodes, cudaStream_t s) {
+  k_raman_kernel<<<1, kRamanThreads, raman_smem(a.n_to) / 2, s>>>(a);
+  k_raman_nodes<R><<<n_nodes, kRamanThreads, raman_smem(a.n_to), s>>>(a, field, polarisation);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_raman<double>(const RamanArgs&, const double*, double*, int, cudaStream_t);
+template cudaError_t launch_raman<float>(const RamanArgs&, const float*, float*, int, cudaStream_t);
+
+}  // namespace sp

@@ -400,6 +400,49 @@ def radial_case(case, *, n_r, length, seed):
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
 
 
+def raman_case(case, *, seed):
+    """A nitrogen-filled capillary with the gas's rotational and vibrational Raman response
+    on the field grid (the drive E^2, the harmonic kept) and the real Kerr cubic, no plasma:
+    the reference's test-only molecular constants (``tests/former_raman.py``), Börzsönyi et
+    al.'s nitrogen index; two modes, n_to 4096."""
+    from former_raman import FORMER_N2
+
+    lam = np.geomspace(120e-9, 200e-6, 4000)[::-1]
+    om = 2 * np.pi * C0 / lam
+    l2 = (lam * 1e6) ** 2
+    b1, c1, b2, c2 = 39209.95e-8, 1146.24e-6, 18806.48e-8, 13.476e-3  # N2, 1 bar, 0 C
+    n2m1 = b1 * l2 / (l2 - c1) + b2 * l2 / (l2 - c2)
+    rho0 = 1e5 / (K_B * 273.15)
+    sus = TabulatedSusceptibility(om, (np.sqrt(1 + n2m1) - 1) / rho0, np.zeros_like(om),
+                                  (121e-9, 199e-6), "Borzsonyi 2008 N2")
+    nitrogen = Species("N2", sus, IdealGas(), gamma3=1.1e-52, raman=FORMER_N2)
+    length = 0.05
+
+    def build(**kw):
+        fill = Mixture.fill({nitrogen: 1.0}, 3.0)
+        grid = FieldGrid.from_limits(length, 800e-9, (300e-9, 3e-6), 300e-15, fft_size="pow2")
+        return Simulation.from_capillary(
+            125e-6, length, fill, None, wavelength=800e-9, grid=grid, fwhm=30e-15, energy=80e-6,
+            cladding=1.45 + 0j, modes=2, plasma=False, raman=True, thg=True, noise=None, rtol=1e-6,
+            backend="numpy_ref", boundary_check=None, **kw)
+
+    sim = build(n_save=3)
+    problem = sim.translate()
+    golden = source_fixture(sim, problem, [0.0, 0.37 * length], seed)
+    _, zs, states, (hist, counts), wall = drive(build(n_save=3))
+    golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.history": hist,
+                   "adaptive.counts": counts, "adaptive.wall": np.array(wall),
+                   "adaptive.policy": drive.policy})
+    print(f"{case}: adaptive run {counts} attempts/rejected in {wall:.2f} s", flush=True)
+    planes = np.linspace(0.0, length, 6)
+    schedule = FixedSchedule.uniform(0.0, length, length / 50, save_planes=planes)
+    fixed_problem, zs, states, (hist, counts), wall = drive(build(absorber=False, schedule=schedule, n_save=6))
+    golden.update({"fixed.z": zs, "fixed.states": states, "fixed.history": hist,
+                   "fixed.policy": drive.policy})
+    write(case, problem, golden)
+    save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
+
+
 def workload_case(case, *, seed, n_save=3, **common):
     """A full-size configuration: the problem, the march policy, two reference source
     evaluations, and the reference's whole adaptive run (exponential Adams at the route's
@@ -543,6 +586,8 @@ if __name__ == "__main__":
         cap_case("cap12_ne", gas="Ne", pressure=1.5, length=0.02, limits=(200e-9, 4e-6),
                  trange=100e-15, energy=60e-6, fwhm=10e-15, modes=12, n_r=96,
                  radial_rule="gauss", fixed_dz=0.001, n_fixed_planes=6, seed=6)
+    if not only or "raman_n2" in only:
+        raman_case("raman_n2", seed=8)
     if not only or "radial_ar" in only:
         # the radial free-space route on 48 radial nodes (a 48 x 48 Hankel pair)
         radial_case("radial_ar", n_r=48, length=0.01, seed=7)
