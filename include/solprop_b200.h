@@ -53,6 +53,27 @@ typedef struct sp_table {
   const double* coefficients; /* n_intervals * n_deg * n_values */
 } sp_table;
 
+/* A further field-plasma channel of a gas mixture (passes/plasma.py:326-485): its own rate
+ * table, exposure scan and population; channel 0 is the descriptor's own plasma fields. */
+typedef struct sp_plasma_channel {
+  double charge_mass_ratio, ionisation_potential; /* ratio x electrons per event */
+  int32_t rate_intervals;
+  const double* rate_coefficients; /* (4, rate_intervals) */
+  double log_field_min, d_log_field, field_min, field_max, rate_max;
+  sp_table plasma_density, preionisation;
+} sp_plasma_channel;
+
+/* A further Raman-active component of a gas mixture (passes/responses.py:293-334,
+ * mixture_raman_spectrum): its rows damped at their own rates, weighted by its fraction and
+ * density; component 0 is the descriptor's own Raman fields. */
+typedef struct sp_raman_component {
+  int32_t terms;
+  const double* undamped; /* (terms, 2*n_to) */
+  sp_table rates[4];
+  double fraction;
+  sp_table density;
+} sp_raman_component;
+
 /* The lowered problem (solprop_b200.record.ProblemRecord; kernel-contract.md 1-6). */
 typedef struct sp_problem_desc {
   int32_t grid_kind; /* 0 field (r2c/c2r), 1 envelope (c2c) */
@@ -100,6 +121,12 @@ typedef struct sp_problem_desc {
   /* the in-stage temporal absorber (stepping.py:286-369) */
   int32_t absorber_in_stage;
   const double* temporal_absorber_fine; /* n_to */
+  /* a gas mixture: plasma channels and Raman components after the first (up to 3 each;
+   * zero-initialised: none) */
+  int32_t n_extra_channels;
+  const sp_plasma_channel* extra_channels;
+  int32_t n_extra_raman;
+  const sp_raman_component* extra_raman;
 } sp_problem_desc;
 
 typedef struct sp_problem sp_problem;

@@ -35,6 +35,10 @@ class StageScalars:
     preionisation: float
     raman_rates: tuple
     raman_density: float
+    channel_densities: tuple = ()  # every plasma channel of a mixture, in order
+    channel_preionisation: tuple = ()
+    raman_rates_by_component: tuple = ()  # every Raman component's rates, in order
+    raman_densities: tuple = ()
 
 
 def stage_scalars(rec, z0: float, z1: float) -> StageScalars:
@@ -52,6 +56,11 @@ def stage_scalars(rec, z0: float, z1: float) -> StageScalars:
         preionisation=rec.scalar(rec.preionisation, z1, 0.0),
         raman_rates=tuple(float(t(z1)[0]) for t in rec.raman_rates),
         raman_density=density if rec.raman_density is None else rec.scalar(rec.raman_density, z1, 1.0),
+        channel_densities=tuple(rec.scalar(ch.plasma_density, z1, density) for ch in rec.extra_channels),
+        channel_preionisation=tuple(rec.scalar(ch.preionisation, z1, 0.0) for ch in rec.extra_channels),
+        raman_rates_by_component=tuple(tuple(float(t(z1)[0]) for t in comp.rates) for comp in rec.extra_raman),
+        raman_densities=tuple(density if comp.density is None else rec.scalar(comp.density, z1, 1.0)
+                              for comp in rec.extra_raman),
     )
 
 
@@ -113,7 +122,8 @@ def magnitude(field_t: np.ndarray) -> np.ndarray:
 def rate_lookup(rec, field_amplitude: np.ndarray) -> np.ndarray:
     """``translate/ionisation.py:242-323``: exp of a cubic in ``log|E|`` on uniform knots.
 
-    Exactly zero below ``field_min`` and ``rate_max`` above ``field_max``.
+    Exactly zero below ``field_min`` and ``rate_max`` above ``field_max``.  ``rec`` is the
+    record (its first channel's table) or a further channel's record.
     """
     flat = np.abs(field_amplitude).ravel()
     rate = np.zeros_like(flat)
@@ -186,6 +196,32 @@ def plasma_column(rec, field_t: np.ndarray, sc: StageScalars):
     return rate, fraction, current
 
 
+def channels_current(rec, field_t: np.ndarray, sc: StageScalars) -> np.ndarray:
+    """``passes/plasma.py:326-372`` and ``:426-485``: a mixture's channels, each with its own
+    rate and exposure scan, their weights summed before the one free-current integral.
+
+    Returns the ungated total current, the channel densities inside.
+    """
+    dt = rec.dt_fine
+    mag = magnitude(field_t)
+    channels = [rec, *rec.extra_channels]
+    densities = (sc.plasma_density, *sc.channel_densities)
+    initial = (sc.preionisation, *sc.channel_preionisation)
+    weight = np.zeros_like(mag)
+    work = np.zeros_like(mag)
+    for channel, density, f0 in zip(channels, densities, initial):
+        rate = rate_lookup(channel, mag)
+        exposure = floor(rec, running_integral(rec, rate, dt))
+        fraction = 1.0 - (1.0 - f0) * np.exp(-exposure)
+        weight += density * fraction * channel.charge_mass_ratio
+        work += density * channel.ionisation_potential * rate * (1.0 - fraction)
+    free = running_integral(rec, weight[..., None, :] * field_t, dt)
+    squared = mag ** 2
+    guard = np.zeros_like(work)
+    np.divide(work, squared, out=guard, where=squared > 0.0)
+    return free + guard[..., None, :] * field_t
+
+
 def kerr_polarisation(rec, field_t: np.ndarray, density: float, carrier=None) -> np.ndarray:
     """``passes/responses.py:65-139``: the real or analytic cubic."""
     factor = rec.kerr_coefficient * density
@@ -209,6 +245,23 @@ def raman_spectrum(rec, rates) -> np.ndarray:
     for row, rate in zip(rec.raman_undamped, rates):
         kernel = kernel + row * np.exp(-rate * t)
     return np.fft.rfft(rec.raman_fraction * kernel) * rec.dt_fine
+
+
+def mixture_raman_spectrum(rec, sc: StageScalars) -> np.ndarray:
+    """``passes/responses.py:293-334``: every component's rows damped at their own rates,
+    weighted by its density and fraction, summed, ``rfft * dt`` (the densities inside)."""
+    n2 = rec.raman_undamped.shape[1]
+    t = np.arange(n2) * rec.dt_fine
+    total = np.zeros(n2)
+    parts = [(rec.raman_undamped, sc.raman_rates, rec.raman_fraction, sc.raman_density)]
+    parts += [(c.undamped, r, c.fraction, d)
+              for c, r, d in zip(rec.extra_raman, sc.raman_rates_by_component, sc.raman_densities)]
+    for undamped, rates, fraction, density in parts:
+        amplitude = np.zeros(n2)
+        for row, rate in zip(undamped, rates):
+            amplitude += row * np.exp(-rate * t)
+        total += density * fraction * amplitude
+    return np.fft.rfft(total) * rec.dt_fine
 
 
 def raman_polarisation(rec, field_t: np.ndarray, spectrum: np.ndarray, density: float) -> np.ndarray:
@@ -249,14 +302,19 @@ def lab_source(rec, lab: np.ndarray, z: float, *, quiet: bool = False, out: dict
     modal_t = to_time(rec, field_in)
     field_t = synthesise(rec, modal_t, sc.taper)
     total = np.zeros_like(field_t)
-    current = None
-    if rec.plasma_enabled:
+    current = rate = fraction = None
+    if rec.plasma_enabled and rec.extra_channels:
+        current = channels_current(rec, field_t, sc)
+    elif rec.plasma_enabled:
         rate, fraction, current = plasma_column(rec, field_t, sc)
     if rec.kerr_enabled:
         total = total + kerr_polarisation(rec, field_t, sc.kerr_density, rec.carrier)
     if rec.raman_enabled:
-        spectrum = raman_spectrum(rec, sc.raman_rates)
-        total = total + raman_polarisation(rec, field_t, spectrum, sc.raman_density)
+        if rec.extra_raman:  # a mixture: one spectrum, the densities inside it
+            spectrum, density = mixture_raman_spectrum(rec, sc), 1.0
+        else:
+            spectrum, density = raman_spectrum(rec, sc.raman_rates), sc.raman_density
+        total = total + raman_polarisation(rec, field_t, spectrum, density)
     polarisation = total * rec.t_window
     projected = project(rec, polarisation, sc.taper)
     spectrum = to_frequency(rec, projected)

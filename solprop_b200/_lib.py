@@ -23,6 +23,19 @@ class SpTable(C.Structure):
                 ("breakpoints", C.POINTER(C.c_double)), ("coefficients", C.POINTER(C.c_double))]
 
 
+class SpPlasmaChannel(C.Structure):
+    _fields_ = [("charge_mass_ratio", C.c_double), ("ionisation_potential", C.c_double),
+                ("rate_intervals", C.c_int32), ("rate_coefficients", C.POINTER(C.c_double)),
+                ("log_field_min", C.c_double), ("d_log_field", C.c_double), ("field_min", C.c_double),
+                ("field_max", C.c_double), ("rate_max", C.c_double),
+                ("plasma_density", SpTable), ("preionisation", SpTable)]
+
+
+class SpRamanComponent(C.Structure):
+    _fields_ = [("terms", C.c_int32), ("undamped", C.POINTER(C.c_double)), ("rates", SpTable * 4),
+                ("fraction", C.c_double), ("density", SpTable)]
+
+
 class SpProblemDesc(C.Structure):
     _fields_ = [
         ("grid_kind", C.c_int32),
@@ -54,6 +67,8 @@ class SpProblemDesc(C.Structure):
         ("raman_undamped", C.POINTER(C.c_double)), ("raman_rates", SpTable * 4),
         ("raman_fraction", C.c_double), ("raman_density", SpTable),
         ("absorber_in_stage", C.c_int32), ("temporal_absorber_fine", C.POINTER(C.c_double)),
+        ("n_extra_channels", C.c_int32), ("extra_channels", C.POINTER(SpPlasmaChannel)),
+        ("n_extra_raman", C.c_int32), ("extra_raman", C.POINTER(SpRamanComponent)),
     ]
 
 
@@ -265,7 +280,7 @@ class Marshalled:
     """A record's arrays converted to the C layout, kept alive beside the descriptor."""
 
     def __init__(self):
-        self.keep: list[np.ndarray] = []
+        self.keep: list = []  # arrays and ctypes arrays
 
     def f64(self, a) -> C.POINTER(C.c_double):
         if a is None:
@@ -360,6 +375,33 @@ def problem_desc(rec) -> tuple[SpProblemDesc, Marshalled]:
         d.raman_density = m.table(rec.raman_density)
     d.absorber_in_stage = int(rec.absorber_scheme == "nonlinear")
     d.temporal_absorber_fine = m.f64(rec.temporal_absorber_fine)
+    if rec.extra_channels:
+        channels = (SpPlasmaChannel * len(rec.extra_channels))()
+        for i, ch in enumerate(rec.extra_channels):
+            c = channels[i]
+            c.charge_mass_ratio, c.ionisation_potential = ch.charge_mass_ratio, ch.ionisation_potential
+            c.rate_intervals = ch.rate_coefficients.shape[1]
+            c.rate_coefficients = m.f64(ch.rate_coefficients)
+            c.log_field_min, c.d_log_field = ch.log_field_min, ch.d_log_field
+            c.field_min, c.field_max, c.rate_max = ch.field_min, ch.field_max, ch.rate_max
+            c.plasma_density = m.table(ch.plasma_density)
+            c.preionisation = m.table(ch.preionisation)
+        m.keep.append(channels)
+        d.n_extra_channels = len(rec.extra_channels)
+        d.extra_channels = C.cast(channels, C.POINTER(SpPlasmaChannel))
+    if rec.extra_raman:
+        components = (SpRamanComponent * len(rec.extra_raman))()
+        for i, comp in enumerate(rec.extra_raman):
+            c = components[i]
+            c.terms = comp.undamped.shape[0]
+            c.undamped = m.f64(comp.undamped)
+            for j, t in enumerate(comp.rates[:4]):
+                c.rates[j] = m.table(t)
+            c.fraction = comp.fraction
+            c.density = m.table(comp.density)
+        m.keep.append(components)
+        d.n_extra_raman = len(rec.extra_raman)
+        d.extra_raman = C.cast(components, C.POINTER(SpRamanComponent))
     return d, m
 
 

@@ -177,8 +177,21 @@ struct sp_problem {
   std::vector<unsigned char> active, norm;
   std::vector<double> phi_terms, pre_terms, synthesis, projection, rate_coeff, taps;
   Table phi_weights, phi_rate, pre_weights, density, kerr_density, plasma_density, preion, taper;
-  Table raman_rates[4], raman_density;
-  std::vector<double> raman_undamped;  // (raman_terms, 2 n_to)
+  Table raman_rates[kMaxRamanRows], raman_density;
+  std::vector<double> raman_undamped;  // (rows, 2 n_to): every Raman component's rows, in order
+  // a gas mixture (n_extra_channels > 0): every plasma channel, channel 0 the descriptor's
+  struct Channel {
+    double charge_mass_ratio, ionisation_potential, log_field_min, d_log_field, field_min, field_max,
+        rate_max;
+    std::vector<double> coefficients;  // (4, n)
+    Table density, preion;
+  };
+  std::vector<Channel> channels;
+  // every Raman component (component 0 the descriptor's): rows, fraction, density
+  std::vector<int> raman_first_row{0};
+  std::vector<double> raman_fraction;
+  std::vector<Table> raman_densities;
+  int raman_rows() const { return raman_first_row.back(); }
 };
 
 static void validate(const sp_problem_desc* d) {
@@ -218,6 +231,7 @@ static void validate(const sp_problem_desc* d) {
       need(d->raman_terms >= 1 && d->raman_terms <= 4 && d->raman_undamped, "Raman terms");
       if (d->raman_thg) throw Failure(SP_ERR_REFUSED, "a third-harmonic Raman drive on the envelope grid");
     }
+    if (d->n_extra_raman) throw Failure(SP_ERR_REFUSED, "a Raman mixture on the envelope grid");
   } else {
     if (d->raman_enabled) {
       need(d->raman_terms >= 1 && d->raman_terms <= 4 && d->raman_undamped, "Raman terms");
@@ -228,6 +242,23 @@ static void validate(const sp_problem_desc* d) {
     }
     if (d->kerr_enabled && d->kerr_analytic)
       throw Failure(SP_ERR_REFUSED, "the analytic Kerr cubic belongs to the envelope grid");
+  }
+  need(d->n_extra_channels >= 0 && d->n_extra_channels < kMaxChannels, "at most four plasma channels");
+  need(d->n_extra_channels == 0 || (d->plasma_enabled && d->extra_channels), "mixture channels");
+  for (int c = 0; c < d->n_extra_channels; ++c)
+    need(d->extra_channels[c].rate_intervals >= 1 && d->extra_channels[c].rate_coefficients &&
+             d->extra_channels[c].d_log_field > 0.0,
+         "a mixture channel's rate table");
+  need(d->n_extra_raman >= 0 && d->n_extra_raman < kMaxRamanComponents, "at most four Raman components");
+  need(d->n_extra_raman == 0 || (d->raman_enabled && d->extra_raman), "mixture Raman components");
+  {
+    int rows = d->raman_enabled ? d->raman_terms : 0;
+    for (int c = 0; c < d->n_extra_raman; ++c) {
+      need(d->extra_raman[c].terms >= 1 && d->extra_raman[c].terms <= 4 && d->extra_raman[c].undamped,
+           "a mixture component's Raman terms");
+      rows += d->extra_raman[c].terms;
+    }
+    if (rows > kMaxRamanRows) throw Failure(SP_ERR_REFUSED, "more than eight damped Raman rows in a mixture");
   }
   if (d->plasma_enabled) {
     need(d->rate_intervals >= 1 && d->rate_coefficients, "rate table");
@@ -259,6 +290,7 @@ struct sp_workspace {
   DevBuf<double> raman_undamped;
   DevBuf<double> stat_power, stat_out, stat_weight;  // plane statistics, on first use
   DevBuf<double2> raman_spectrum;  // field-grid Raman: the damped kernel's spectrum (n_to + 1)
+  DevBuf<ChannelTableT<double>> channels;  // a mixture's plasma channels (rate_coeff holds their tables)
   // the modal transform as products (SP_MODAL_GEMM): the node field and streams in HBM;
   // the mixed form's operands in three BF16 parts, rows padded to kpad
   bool gemm = false;
@@ -272,6 +304,7 @@ struct sp_workspace {
     DevBuf<float2> twiddles, spectra;
     DevBuf<float> t_window, t_window_d, synthesis, projection, rate_coeff, taps, proj;
     DevBuf<float> node_field, node_streams;
+    DevBuf<ChannelTableT<float>> channels;
   } f32;
   DevBuf<unsigned char> active, norm;
   DevBuf<StageScalarsDev> stage;   // kStageSlots slots
@@ -371,8 +404,16 @@ static void fill_stage(sp_workspace* ws, int slot, double z0, double z1) {
   s.plasma_density = P.plasma_density.scalar(z1, s.density);
   s.preionisation = P.preion.scalar(z1, 0.0);
   if (P.d.raman_enabled) {  // translate/stage.py scalars: the damping rates and the density
-    for (int r = 0; r < P.d.raman_terms; ++r) s.raman_rates[r] = P.raman_rates[r].scalar(z1, 0.0);
+    for (int r = 0; r < P.raman_rows(); ++r) s.raman_rates[r] = P.raman_rates[r].scalar(z1, 0.0);
     s.raman_density = P.raman_density.scalar(z1, s.density);
+    for (size_t c = 0; c < P.raman_densities.size(); ++c)
+      s.raman_densities[c] = P.raman_densities[c].scalar(z1, s.density);
+  }
+  s.channel_density[0] = s.plasma_density;
+  s.channel_preionisation[0] = s.preionisation;
+  for (size_t c = 1; c < P.channels.size(); ++c) {  // a mixture's further channels
+    s.channel_density[c] = P.channels[c].density.scalar(z1, s.density);
+    s.channel_preionisation[c] = P.channels[c].preion.scalar(z1, 0.0);
   }
   s.n_phi = P.d.n_phi_terms;
   s.n_pre = P.d.n_prefactor_terms;
@@ -479,6 +520,11 @@ static ColumnArgsT<R> column_args(const sp_workspace* ws, const StageScalarsDev*
   ca.rate_max = d.rate_max;
   ca.rate_coefficients = v.rate_coeff;
   ca.taps = v.taps;
+  ca.n_channels = std::max<int>(1, (int)P.channels.size());
+  if constexpr (sizeof(R) == 8)
+    ca.channels = ws->channels.p;
+  else
+    ca.channels = ws->f32.channels.p;
   return ca;
 }
 
@@ -523,8 +569,9 @@ static RamanArgs raman_args(const sp_workspace* ws, int slot) {
   ra.t_window = ws->t_window.p;
   ra.n_to = d.n_to;
   ra.log_n_to = ws->log_n_to;
-  ra.terms = d.raman_terms;
-  ra.fraction = d.raman_fraction;
+  ra.n_components = (int)ws->P->raman_fraction.size();
+  for (int c = 0; c <= ra.n_components; ++c) ra.first_row[c] = ws->P->raman_first_row[c];
+  for (int c = 0; c < ra.n_components; ++c) ra.fraction[c] = ws->P->raman_fraction[c];
   ra.dt = d.dt_fine;
   return ra;
 }
@@ -669,19 +716,44 @@ static void build_mixed(sp_workspace* ws, const std::vector<double2>& tw, const 
   up(f.projection, keep.back());
   keep.push_back(to_float(taps));
   up(f.taps, keep.back());
-  const int n = std::max(d.rate_intervals, 1);
-  std::vector<float> r32((size_t)5 * n, 0.0f);
-  if (rc.size() >= (size_t)4 * n) {
+  // the rate tables in the FP32 form: (c0, c1, c2, exp c3, 1 / knot) per interval, every
+  // channel's in channel order
+  std::vector<float> r32;
+  auto convert = [&](const double* c, int n, double log_field_min, double d_log_field) {
+    const size_t at = r32.size();
+    r32.resize(at + (size_t)5 * n, 0.0f);
     for (int i = 0; i < n; ++i) {
-      r32[i] = (float)rc[i];
-      r32[n + i] = (float)rc[n + i];
-      r32[2 * n + i] = (float)rc[2 * n + i];
-      r32[3 * n + i] = (float)std::exp(rc[3 * n + i]);
-      r32[4 * n + i] = (float)std::exp(-(d.log_field_min + (double)i * d.d_log_field));
+      r32[at + i] = (float)c[i];
+      r32[at + n + i] = (float)c[n + i];
+      r32[at + 2 * n + i] = (float)c[2 * n + i];
+      r32[at + 3 * n + i] = (float)std::exp(c[3 * n + i]);
+      r32[at + 4 * n + i] = (float)std::exp(-(log_field_min + (double)i * d_log_field));
     }
+    return at;
+  };
+  std::vector<size_t> offsets;
+  if (!P.channels.empty()) {
+    for (const auto& ch : P.channels)
+      offsets.push_back(convert(ch.coefficients.data(), (int)(ch.coefficients.size() / 4), ch.log_field_min,
+                                ch.d_log_field));
+  } else if (rc.size() >= (size_t)4 * std::max(d.rate_intervals, 1) && d.rate_intervals >= 1) {
+    convert(rc.data(), d.rate_intervals, d.log_field_min, d.d_log_field);
+  } else {
+    r32.assign(5, 0.0f);
   }
   keep.push_back(std::move(r32));
   up(f.rate_coeff, keep.back());
+  if (!P.channels.empty()) {
+    std::vector<ChannelTableT<float>> tables;
+    for (size_t c = 0; c < P.channels.size(); ++c) {
+      const auto& ch = P.channels[c];
+      tables.push_back({f.rate_coeff.p + offsets[c], (int)(ch.coefficients.size() / 4), ch.log_field_min,
+                        ch.d_log_field, ch.field_min, ch.field_max, ch.rate_max, ch.charge_mass_ratio,
+                        ch.ionisation_potential});
+    }
+    f.channels.upload(tables.data(), tables.size(), s);
+    CUDA_CHECK(cudaStreamSynchronize(s));
+  }
   const size_t n_groups = ws->gemm ? 1 : (d.n_nodes + kGroup - 1) / kGroup;  // the products write group 0's rows
   f.proj.alloc(n_groups * 3 * P.n_cols * d.n_to);
   f.proj.zero(s);
@@ -717,7 +789,26 @@ static void build_workspace(sp_workspace* ws) {
   ws->synthesis.upload(P.synthesis.data(), P.synthesis.size(), s);
   ws->projection.upload(P.projection.data(), P.projection.size(), s);
   std::vector<double> rc = P.rate_coeff.empty() ? std::vector<double>(4, 0.0) : P.rate_coeff;
+  std::vector<size_t> channel_at;  // a mixture: every channel's table, channel 0's first
+  if (!P.channels.empty()) {
+    rc.clear();
+    for (const auto& ch : P.channels) {
+      channel_at.push_back(rc.size());
+      rc.insert(rc.end(), ch.coefficients.begin(), ch.coefficients.end());
+    }
+  }
   ws->rate_coeff.upload(rc.data(), rc.size(), s);
+  if (!P.channels.empty()) {
+    std::vector<ChannelTableT<double>> tables;
+    for (size_t c = 0; c < P.channels.size(); ++c) {
+      const auto& ch = P.channels[c];
+      tables.push_back({ws->rate_coeff.p + channel_at[c], (int)(ch.coefficients.size() / 4), ch.log_field_min,
+                        ch.d_log_field, ch.field_min, ch.field_max, ch.rate_max, ch.charge_mass_ratio,
+                        ch.ionisation_potential});
+    }
+    ws->channels.upload(tables.data(), tables.size(), s);
+    CUDA_CHECK(cudaStreamSynchronize(s));
+  }
   std::vector<double> taps = P.taps.empty() ? std::vector<double>(1, 1.0) : P.taps;
   ws->taps.upload(taps.data(), taps.size(), s);
   ws->crop.upload(P.crop.data(), d.n_omega, s);
@@ -739,7 +830,7 @@ static void build_workspace(sp_workspace* ws) {
   ws->modal_t.alloc((size_t)P.n_cols * d.n_to);
   const size_t n_tiles = column_tiles(d);
   const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
-  ws->sums0.alloc((size_t)d.n_nodes * n_tiles);
+  ws->sums0.alloc((size_t)std::max<size_t>(1, P.channels.size()) * d.n_nodes * n_tiles);  // a plane per channel
   ws->sums1.alloc((size_t)d.n_nodes * n_tiles);
   ws->chain_flags.alloc(n_groups * n_tiles);
   ws->chain_flags.zero(s);
@@ -1428,7 +1519,41 @@ sp_status sp_problem_create(const sp_problem_desc* d, sp_problem** out) {
       for (int r = 0; r < d->raman_terms; ++r) P->raman_rates[r].load(d->raman_rates[r]);
       P->raman_density.load(d->raman_density);
       P->raman_undamped.assign(d->raman_undamped, d->raman_undamped + (size_t)d->raman_terms * 2 * d->n_to);
+      P->raman_first_row.push_back(d->raman_terms);
+      P->raman_fraction.push_back(d->raman_fraction);
+      P->raman_densities.push_back(P->raman_density);
+      for (int c = 0; c < d->n_extra_raman; ++c) {  // a mixture's further components
+        const sp_raman_component& rc = d->extra_raman[c];
+        const int r0 = P->raman_rows();
+        for (int r = 0; r < rc.terms; ++r) P->raman_rates[r0 + r].load(rc.rates[r]);
+        P->raman_undamped.insert(P->raman_undamped.end(), rc.undamped,
+                                 rc.undamped + (size_t)rc.terms * 2 * d->n_to);
+        P->raman_first_row.push_back(r0 + rc.terms);
+        P->raman_fraction.push_back(rc.fraction);
+        P->raman_densities.emplace_back();
+        P->raman_densities.back().load(rc.density);
+      }
     }
+    if (d->n_extra_channels) {  // a mixture: every channel, the descriptor's first
+      auto add = [&](double qm, double ip, const double* coeff, int n, double lmin, double dl, double fmin,
+                     double fmax, double rmax, const sp_table& dens, const sp_table& pre) {
+        sp_problem::Channel ch{qm, ip, lmin, dl, fmin, fmax, rmax, {}, {}, {}};
+        ch.coefficients.assign(coeff, coeff + (size_t)4 * n);
+        ch.density.load(dens);
+        ch.preion.load(pre);
+        P->channels.push_back(std::move(ch));
+      };
+      add(d->charge_mass_ratio, d->ionisation_potential, d->rate_coefficients, d->rate_intervals,
+          d->log_field_min, d->d_log_field, d->field_min, d->field_max, d->rate_max, d->plasma_density,
+          d->preionisation);
+      for (int c = 0; c < d->n_extra_channels; ++c) {
+        const sp_plasma_channel& e = d->extra_channels[c];
+        add(e.charge_mass_ratio, e.ionisation_potential, e.rate_coefficients, e.rate_intervals, e.log_field_min,
+            e.d_log_field, e.field_min, e.field_max, e.rate_max, e.plasma_density, e.preionisation);
+      }
+    }
+    P->d.extra_channels = nullptr;  // copied above: nothing keeps the caller's arrays
+    P->d.extra_raman = nullptr;
     if (d->phi_expansion && (!P->phi_weights.present() || !P->phi_rate.present()))
       throw Failure(SP_ERR_ARGUMENT, "an expansion of Phi needs its weight and rate tables");
     *out = P.release();
@@ -2688,11 +2813,14 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
     if (n_runs < 1 || !problems || !runs || !out) throw Failure(SP_ERR_ARGUMENT, "bad scan arguments");
     if (precision != SP_PRECISION_FP64 && precision != SP_PRECISION_MIXED)
       throw Failure(SP_ERR_ARGUMENT, "unknown precision");
-    for (int r = 0; r < n_runs; ++r)
+    for (int r = 0; r < n_runs; ++r) {
       if (problems[r] && (problems[r]->n_cols > kMaxModes ||
                           (problems[r]->d.raman_enabled && problems[r]->d.grid_kind == 0)))
         throw Failure(SP_ERR_REFUSED,
                       "a scan's runs take at most 8 modal columns and no field-grid Raman (the fused transform)");
+      if (problems[r] && !problems[r]->channels.empty())
+        throw Failure(SP_ERR_REFUSED, "a scan's runs take one plasma channel (no gas mixture)");
+    }
     CUDA_CHECK(cudaSetDevice(device));
     ensure_configured(device);
     auto S = std::make_unique<sp_scan>();
@@ -3086,6 +3214,8 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     if (problem->n_cols > kMaxModes || (problem->d.raman_enabled && problem->d.grid_kind == 0))
       throw Failure(SP_ERR_REFUSED,
                     "the no-allocation entry point takes at most 8 modal columns and no field-grid Raman");
+    if (!problem->channels.empty())
+      throw Failure(SP_ERR_REFUSED, "the no-allocation entry point takes one plasma channel (no gas mixture)");
     int device = 0;
     CUDA_CHECK(cudaGetDevice(&device));
     unsigned char* base = noalloc_base(device);

@@ -78,6 +78,15 @@ __device__ __forceinline__ RateLookup<float> rate_lookup(const ColumnArgsT<float
           (float)(1.0 / a.d_log_field), a.rate_coefficients, a.rate_intervals};
 }
 
+__device__ __forceinline__ RateLookup<double> rate_lookup(const ChannelTableT<double>& c) {
+  return {c.field_min, c.field_max, c.rate_max, c.log_field_min, c.d_log_field, c.rate_coefficients,
+          c.rate_intervals};
+}
+__device__ __forceinline__ RateLookup<float> rate_lookup(const ChannelTableT<float>& c) {
+  return {(float)c.field_min, (float)c.field_max, (float)c.rate_max, (float)c.log_field_min,
+          (float)(1.0 / c.d_log_field), c.rate_coefficients, c.rate_intervals};
+}
+
 __device__ __forceinline__ double rate_of(const RateLookup<double>& a, double magnitude) {
   if (magnitude > a.field_max) return a.rate_max;
   if (!(magnitude >= a.field_min)) return 0.0;
@@ -311,6 +320,119 @@ __device__ __forceinline__ double predecessors(const double* sums, int node, int
 
 }  // namespace
 
+// The plasma of a gas mixture on one tile (passes/plasma.py:326-485): every channel's rate
+// and exposure scan in channel order, each handed over between tiles as the single
+// channel's is (channel c publishes its exposure sums as stage first + c, in its own plane
+// of sums0), the weights rho_c f_c q_c and the works rho_c I_c W_c (1 - f_c) summed over the
+// channels, then the one free-current integral of the summed weight times the field
+// (published as stage first + n_channels).  J receives the free current, L the summed work
+// (the loss current is L E / |E|^2); the densities are inside both.
+template <class R>
+__device__ __forceinline__ void mixture_plasma(const ColumnArgsT<R>& a, const StageScalarsDev& st,
+                                               const R (&E)[kPer], R (&J)[kPer], R (&L)[kPer], int tw,
+                                               int K, int owned, int own_hi, bool at_end, int node,
+                                               bool live, int group, int tile, int first, R* row,
+                                               int lane, bool& quiet) {
+  const int n_to = a.n_to, A = a.lead;
+  const R dt = R(a.dt);
+  const size_t plane = (size_t)a.n_nodes * a.n_tiles;
+  R weight[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) weight[j] = L[j] = R(0);
+  bool all_dark = true;
+  for (int c = 0; c < a.n_channels; ++c) {
+    const ChannelTableT<R> ch = a.channels[c];
+    const RateLookup<R> rates = rate_lookup(ch);
+    R W[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int t = tw + kPer * lane + j;
+      W[j] = (t >= 0 && t < n_to) ? rate_of(rates, fabs(E[j])) : R(0);
+    }
+    bool dark = true;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) dark = dark && W[j] == R(0);
+    dark = __all_sync(0xffffffffu, dark);
+    R inc[kPer];
+    double s0 = 0.0;
+    if (!dark) {
+      R Wf[kPer];
+      if (at_end) {
+        R Wg[kPer];
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) Wg[j] = W[j];
+        reflect_ends(Wg, row, tw, n_to, K, lane);
+        band_filter(Wg, Wf, a.taps, K);
+      } else {
+        band_filter(W, Wf, a.taps, K);
+      }
+      trapezoid(Wf, inc, dt, tw, A - K, A + owned + K, n_to, lane);
+      s0 = owned_sum(inc, A, own_hi, lane);
+    }
+    double* sums = a.sums0 + (size_t)c * plane;
+    if (lane == 0 && live) sums[(size_t)node * a.n_tiles + tile] = s0;
+    publish(a, group, tile, first + c);
+    await_predecessors(a, group, tile, first + c);
+    const double off0 = live ? predecessors(sums, node, a.n_tiles, tile, lane) : 0.0;
+    const R f0 = R(st.channel_preionisation[c]), rho = R(st.channel_density[c]);
+    const R qm = R(ch.charge_mass_ratio), ip = R(ch.ionisation_potential);
+    if (dark) {
+      const R x = R(off0);
+      const R f = fraction(f0, a.band ? fmax(x, R(0)) : x);
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) {
+        const int u = kPer * lane + j, t = tw + u;
+        if (u >= A - K && u <= A + owned + K && t >= 0 && t < n_to) weight[j] += rho * f * qm;
+      }
+    } else {
+      double P[kPer];
+      const double at_t0 = window_prefix(inc, P, A, lane);
+#pragma unroll
+      for (int j = 0; j < kPer; ++j) {
+        const int u = kPer * lane + j, t = tw + u;
+        if (u >= A - K && u <= A + owned + K && t >= 0 && t < n_to) {
+          const R x = R(off0 + (P[j] - at_t0));
+          const R f = fraction(f0, a.band ? fmax(x, R(0)) : x);
+          weight[j] += rho * f * qm;
+          L[j] += rho * ip * W[j] * (R(1) - f);
+        }
+      }
+    }
+    all_dark = all_dark && dark;
+  }
+  R g[kPer];
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) g[j] = weight[j] * E[j];
+  bool still = true;
+#pragma unroll
+  for (int j = 0; j < kPer; ++j) still = still && g[j] == R(0);
+  still = __all_sync(0xffffffffu, still);
+  R inc[kPer];
+  double s1 = 0.0;
+  if (!still) {
+    if (at_end) reflect_ends(g, row, tw, n_to, K, lane);
+    R gf[kPer];
+    band_filter(g, gf, a.taps, K);
+    trapezoid(gf, inc, dt, tw, A, A + owned, n_to, lane);
+    s1 = owned_sum(inc, A, own_hi, lane);
+  }
+  const int last = first + a.n_channels;
+  if (lane == 0 && live) a.sums1[(size_t)node * a.n_tiles + tile] = s1;
+  publish(a, group, tile, last);
+  await_predecessors(a, group, tile, last);
+  const double off1 = live ? predecessors(a.sums1, node, a.n_tiles, tile, lane) : 0.0;
+  quiet = all_dark && still && off1 == 0.0;
+  if (still) {
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) J[j] = R(off1);
+  } else {
+    double P[kPer];
+    const double at_t0 = window_prefix(inc, P, A, lane);
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) J[j] = R(off1 + (P[j] - at_t0));
+  }
+}
+
 // One tile of one node group: the window's synthesis, rate, running integrals, outputs and
 // projection.  kSweep = false: the tile is one CTA's whole work and learns its running
 // integrals' offsets from its predecessors' published sums (the hand-over above); the
@@ -323,10 +445,14 @@ __device__ __forceinline__ double predecessors(const double* sums, int node, int
 // kNodes = true is the GEMM route's form (tile-parallel only): the window's field is the
 // node field a synthesis product wrote, read in place of the synthesis, and the outputs
 // go to the node streams a projection product reads, in place of the projection.
-template <class R, bool kSweep, bool kNodes = false>
+//
+// kMulti = true is a gas mixture's form (tile-parallel only): the channels' plasma of
+// mixture_plasma in place of the single channel's.
+template <class R, bool kSweep, bool kNodes = false, bool kMulti = false>
 __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, int group,
                                             unsigned long long epoch, double& carry0, double& carry1) {
   static_assert(!(kSweep && kNodes), "the node-field form is tile-parallel");
+  static_assert(!(kSweep && kMulti), "a mixture's form is tile-parallel");
   extern __shared__ __align__(16) unsigned char column_raw[];
   R* modal = reinterpret_cast<R*>(column_raw);    // [m][kPitch], then the streams
   R* streams = modal;                              // [s][warp][kPitch]
@@ -420,7 +546,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
           if (m < n_modes) e += srow[m] * modal[m * kPitch + pad(u)];
       }
       E[j] = e;
-      W[j] = (plasma && t >= 0 && t < n_to) ? rate_of(rates, fabs(e)) : R(0);
+      W[j] = (!kMulti && plasma && t >= 0 && t < n_to) ? rate_of(rates, fabs(e)) : R(0);
     }
   }
   __syncthreads();  // the modal window's space becomes the streams'
@@ -429,7 +555,12 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
 #pragma unroll
   for (int j = 0; j < kPer; ++j) F[j] = J[j] = R(0);
   bool quiet = true;  // this node carries no current on the window (warp-uniform)
-  if (plasma) {
+  if (kMulti && plasma) {
+    // J: the free current, F: the summed work (both with the channel densities inside)
+    const int first = (int)((unsigned long long)(a.n_channels + 1) * epoch + 1);
+    mixture_plasma(a, st, E, J, F, tw, K, owned, own_hi, at_end, node, live, group, tile, first,
+                   scratch + (size_t)warp * kPitch, lane, quiet);
+  } else if (plasma) {
     const int first = (int)(2 * epoch + 1);
     const R dt = R(a.dt);
     R* row = scratch + (size_t)warp * kPitch;
@@ -545,7 +676,13 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
         const R e = E[j];
         const R win = gate[pad(u)];
         p = (a.kerr ? factor * (e * e) * e : R(0)) * win;
-        if (plasma) {
+        if (kMulti && plasma) {  // J + (L / |E|^2) E, the densities inside (plasma.py:471-485)
+          const R squared = fabs(e) * fabs(e);
+          const R guard = squared > R(0) ? divide(F[j], squared) : R(0);
+          const R current = J[j] + guard * e;
+          x = win * current;
+          z = gate_d[pad(u)] * current;
+        } else if (plasma) {
           const R w = W[j], f = F[j];
           const R squared = fabs(e) * fabs(e);
           R scale = R(0);
@@ -637,7 +774,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   }
 }
 
-template <class R, bool kNodes = false>
+template <class R, bool kNodes = false, bool kMulti = false>
 __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   __shared__ unsigned long long ticket;
   if (threadIdx.x == 0) ticket = atomicAdd(a.ticket, 1ull);
@@ -645,7 +782,7 @@ __device__ __forceinline__ void column_body(const ColumnArgsT<R>& a) {
   const unsigned long long epoch = ticket / (unsigned long long)a.n_blocks;
   const int index = (int)(ticket % (unsigned long long)a.n_blocks);
   double unused0 = 0.0, unused1 = 0.0;
-  column_tile<R, false, kNodes>(a, index / a.n_groups, index % a.n_groups, epoch, unused0, unused1);
+  column_tile<R, false, kNodes, kMulti>(a, index / a.n_groups, index % a.n_groups, epoch, unused0, unused1);
 }
 
 // one node group through every tile of the row, in tile order
@@ -672,6 +809,17 @@ __global__ void __launch_bounds__(kThreads, column_residency<R>()) k_column(Colu
 template <class R>
 __global__ void __launch_bounds__(kThreads, column_residency<R>()) k_column_nodes(ColumnArgsT<R> a) {
   column_body<R, true>(a);
+}
+
+// a gas mixture's plasma channels, on either route
+template <class R>
+__global__ void __launch_bounds__(kThreads, column_residency<R>()) k_column_mix(ColumnArgsT<R> a) {
+  column_body<R, false, true>(a);
+}
+
+template <class R>
+__global__ void __launch_bounds__(kThreads, column_residency<R>()) k_column_nodes_mix(ColumnArgsT<R> a) {
+  column_body<R, true, true>(a);
 }
 
 // batched: items[blockIdx.x].x = the run; a run's CTAs take their tiles from its counter
@@ -709,13 +857,19 @@ cudaError_t launch_column_b(const ColumnArgsT<R>* args, const int4* items, const
 
 template <class R>
 cudaError_t launch_column(const ColumnArgsT<R>& a, cudaStream_t stream) {
-  k_column<R><<<a.n_blocks, kThreads, column_smem<R>(), stream>>>(a);
+  if (a.plasma && a.n_channels > 1)
+    k_column_mix<R><<<a.n_blocks, kThreads, column_smem<R>(), stream>>>(a);
+  else
+    k_column<R><<<a.n_blocks, kThreads, column_smem<R>(), stream>>>(a);
   return cudaGetLastError();
 }
 
 template <class R>
 cudaError_t launch_column_nodes(const ColumnArgsT<R>& a, cudaStream_t stream) {
-  k_column_nodes<R><<<a.n_blocks, kThreads, column_smem<R>(), stream>>>(a);
+  if (a.plasma && a.n_channels > 1)
+    k_column_nodes_mix<R><<<a.n_blocks, kThreads, column_smem<R>(), stream>>>(a);
+  else
+    k_column_nodes<R><<<a.n_blocks, kThreads, column_smem<R>(), stream>>>(a);
   return cudaGetLastError();
 }
 
@@ -733,14 +887,17 @@ template cudaError_t launch_column_sweep_b<float>(const ColumnArgsT<float>*, con
                                                   int, cudaStream_t);
 
 cudaError_t configure_column_kernels() {
-  const void* kernels[8] = {(const void*)k_column<double>, (const void*)k_column_b<double>,
-                            (const void*)k_column_sweep_b<double>, (const void*)k_column<float>,
-                            (const void*)k_column_b<float>, (const void*)k_column_sweep_b<float>,
-                            (const void*)k_column_nodes<double>, (const void*)k_column_nodes<float>};
-  const size_t shm[8] = {column_smem<double>(), column_smem<double>(), column_sweep_smem<double>(),
-                         column_smem<float>(), column_smem<float>(), column_sweep_smem<float>(),
-                         column_smem<double>(), column_smem<float>()};
-  for (int i = 0; i < 8; ++i) {
+  const void* kernels[12] = {(const void*)k_column<double>, (const void*)k_column_b<double>,
+                             (const void*)k_column_sweep_b<double>, (const void*)k_column<float>,
+                             (const void*)k_column_b<float>, (const void*)k_column_sweep_b<float>,
+                             (const void*)k_column_nodes<double>, (const void*)k_column_nodes<float>,
+                             (const void*)k_column_mix<double>, (const void*)k_column_mix<float>,
+                             (const void*)k_column_nodes_mix<double>, (const void*)k_column_nodes_mix<float>};
+  const size_t shm[12] = {column_smem<double>(), column_smem<double>(), column_sweep_smem<double>(),
+                          column_smem<float>(), column_smem<float>(), column_sweep_smem<float>(),
+                          column_smem<double>(), column_smem<float>(), column_smem<double>(),
+                          column_smem<float>(), column_smem<double>(), column_smem<float>()};
+  for (int i = 0; i < 12; ++i) {
     cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)shm[i]);
     if (e != cudaSuccess) return e;

@@ -27,12 +27,30 @@ __device__ __forceinline__ const T& own_args(const T* args, int run) {
   return own;
 }
 
+constexpr int kMaxChannels = 4;    // field-plasma channels of a gas mixture
+constexpr int kMaxRamanRows = 8;   // damped Raman rows over a mixture's components
+constexpr int kMaxRamanComponents = 4;
+
 struct StageScalarsDev {
   double z0, z1, taper, density, kerr_density, plasma_density, preionisation, raman_density;
   int n_pre, n_phi;
   double pre_w[kMaxTerms];
   double phi_w[kMaxTerms];   // weights of Phi(z1) - Phi(z0)
-  double raman_rates[4];
+  double raman_rates[kMaxRamanRows];  // every component's rows, in order
+  // a gas mixture: every plasma channel's density and initial fraction (channel 0 as
+  // plasma_density and preionisation), every Raman component's density
+  double channel_density[kMaxChannels], channel_preionisation[kMaxChannels];
+  double raman_densities[kMaxRamanComponents];
+};
+
+// One plasma channel's rate table and constants (translate/ionisation.py:242-323): the
+// coefficients are (4, n) in FP64 and the FP32 form's (5, n) table (column_kernels.cu).
+template <class R>
+struct ChannelTableT {
+  const R* rate_coefficients;
+  int rate_intervals;
+  double log_field_min, d_log_field, field_min, field_max, rate_max;
+  double charge_mass_ratio, ionisation_potential;  // the ratio times the electrons per event
 };
 
 // One Adams trial's tables (backends/numpy_ref/adams_tables.py, multistep.py _trial).
@@ -109,6 +127,10 @@ struct ColumnArgsT {
   // (3, n_nodes, n_to); null on the fused route
   const R* node_field;
   R* node_streams;
+  // a gas mixture's plasma channels (n_channels > 1; sums0 then holds one plane of
+  // (n_nodes, n_tiles) per channel); single-channel problems read the fields above
+  int n_channels;
+  const ChannelTableT<R>* channels;
 };
 using ColumnTileArgs = ColumnArgsT<double>;
 
@@ -187,13 +209,16 @@ cudaError_t configure_statistics_kernels();
 // The Raman response on the field grid (raman_kernels.cu), node by node on the GEMM route.
 constexpr int kMaxRamanSamples = 4096;  // n_to: the doubled grid's packed transform in one CTA
 struct RamanArgs {
-  const StageScalarsDev* stage;  // the damping rates and the Raman density at the stage
-  const double* undamped;        // (terms, 2 n_to)
+  const StageScalarsDev* stage;  // the damping rates and the Raman densities at the stage
+  const double* undamped;        // (rows, 2 n_to): every component's rows, in order
   double2* spectrum;             // (n_to + 1): dt rfft of the damped kernel
   const double2* twiddles;       // exp(-2 pi i m / (2 n_to)), m < n_to
   const double* t_window;        // (n_to) the window g
-  int n_to, log_n_to, terms;
-  double fraction, dt;
+  int n_to, log_n_to;
+  int n_components;              // > 1: a mixture, its densities inside the kernel
+  int first_row[kMaxRamanComponents + 1];  // component c: rows [first_row[c], first_row[c + 1])
+  double fraction[kMaxRamanComponents];
+  double dt;
 };
 cudaError_t configure_raman_kernels();
 template <class R>

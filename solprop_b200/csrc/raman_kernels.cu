@@ -1,6 +1,7 @@
 // The Raman response on the field grid, node by node, on the modal transform's products
-// route (where the node field lives in HBM): backends/numpy_ref/passes/responses.py:218-290
-// (the damped kernel's spectrum) and 395-498 (the delayed polarisation):
+// route (where the node field lives in HBM): backends/numpy_ref/passes/responses.py:218-334
+// (the damped kernel's spectrum, one component or a mixture's) and 395-498 (the delayed
+// polarisation):
 //
 //   H = dt rfft(f_R sum_r u_r(s) exp(-g_r s dt)),  s in [0, 2 n_to)     once per evaluation
 //   P_R(t) = eps0 rho_R E(t) irfft(H rfft(D))(t),  D = E^2 on [0, n_to), 0 above
@@ -39,14 +40,22 @@ __global__ void __launch_bounds__(kRamanThreads) k_raman_kernel(RamanArgs a) {
   const int n = a.n_to;
   double2* B = rk_raw;
   const StageScalarsDev& st = *a.stage;
+  // one component: f_R sum_r u_r(s) e^(-g_r s dt); a mixture (passes/responses.py:293-334):
+  // sum_c rho_c f_c sum_r u_r(s) e^(-g_r s dt), rows in component order
+  const bool mixture = a.n_components > 1;
   for (int m = threadIdx.x; m < n; m += blockDim.x) {
     double v[2];
     for (int q = 0; q < 2; ++q) {
       const int s = 2 * m + q;
-      double k = 0.0;
-      for (int r = 0; r < a.terms; ++r)
-        k += a.undamped[(size_t)r * 2 * n + s] * exp(-st.raman_rates[r] * ((double)s * a.dt));
-      v[q] = a.fraction * k;
+      const double delay = (double)s * a.dt;
+      double total = 0.0;
+      for (int c = 0; c < a.n_components; ++c) {
+        double k = 0.0;
+        for (int r = a.first_row[c]; r < a.first_row[c + 1]; ++r)
+          k += a.undamped[(size_t)r * 2 * n + s] * exp(-st.raman_rates[r] * delay);
+        total += mixture ? st.raman_densities[c] * a.fraction[c] * k : a.fraction[c] * k;
+      }
+      v[q] = total;
     }
     B[m] = make_double2(v[0], v[1]);
   }
@@ -99,7 +108,7 @@ __global__ void __launch_bounds__(kRamanThreads) k_raman_nodes(RamanArgs a, cons
   __syncthreads();
   fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/true);
   const StageScalarsDev& st = *a.stage;
-  const double scale = kEps0 * st.raman_density;
+  const double scale = kEps0 * (a.n_components > 1 ? 1.0 : st.raman_density);  // a mixture's are inside
   const double inv_n = 1.0 / (double)n;
   R* p_row = polarisation + (size_t)node * n;
   for (int t = threadIdx.x; t < n; t += blockDim.x) {

@@ -2,7 +2,8 @@
 
 The counterpart of the native backend's lowering (``native/src/solprop_native/
 _lowering.py:334-926``), for the routes this backend executes: the modal route on a
-field or envelope grid, Kerr, one field-plasma channel and scalar Raman, under a
+field or envelope grid (and the radial free-space route), Kerr, the field-plasma
+channels and scalar Raman components of a gas mixture (up to four of each), under a
 constant or expansion representation of ``Phi`` and of the prefactor.  Anything else is
 refused by name, before anything is allocated, as the contract asks
 (``docs/dev/kernel-contract.md`` section 1).  solprop itself is imported by duck typing
@@ -13,7 +14,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from solprop_b200.record import PiecewiseTable, ProblemRecord
+from solprop_b200.record import PiecewiseTable, PlasmaChannelRecord, ProblemRecord, RamanComponentRecord
 
 __all__ = ["BackendRefusal", "lower"]
 
@@ -69,10 +70,10 @@ def lower(problem) -> ProblemRecord:
         raise BackendRefusal(f"prefactor as a {responses.prefactor_representation!r}")
     if responses.dispersive_kerr is not None or responses.envelope_plasma is not None:
         raise BackendRefusal("dispersive Kerr and envelope plasma are not executed")
-    if len(responses.plasma_channels) > 1:
-        raise BackendRefusal("more than one plasma channel")
-    if len(responses.raman_terms) > 1:
-        raise BackendRefusal("more than one Raman component")
+    if len(responses.plasma_channels) > 4:
+        raise BackendRefusal("more than four plasma channels")
+    if len(responses.raman_terms) > 4:
+        raise BackendRefusal("more than four Raman components")
     if getattr(problem.route, "tdse", None) is not None:
         raise BackendRefusal("a TDSE response is not executed by this backend")
 
@@ -190,4 +191,30 @@ def lower(problem) -> ProblemRecord:
         record.raman_density = _table(term.density) if term.density is not None else None
         if n_pol * transform._n_pol != 1:
             raise BackendRefusal("vector Raman (two components) is not executed yet")
+        for term in responses.raman_terms:
+            if len(term.decay_rates) > 4:
+                raise BackendRefusal("a Raman component with more than four damped rows")
+        for term in responses.raman_terms[1:]:
+            if bool(term.thg) != record.raman_thg:
+                raise BackendRefusal("Raman components with different drives")
+            record.extra_raman.append(RamanComponentRecord(
+                undamped=np.ascontiguousarray(term.undamped, dtype=np.float64),
+                rates=[_table(t) for t in term.decay_rates],
+                fraction=float(term.fraction),
+                density=_table(term.density) if term.density is not None else None,
+            ))
+    for channel in responses.plasma_channels[1:]:
+        table = channel.rate
+        record.extra_channels.append(PlasmaChannelRecord(
+            charge_mass_ratio=float(channel.charge_mass_ratio * channel.electrons_per_event),
+            ionisation_potential=float(channel.ionisation_potential),
+            rate_coefficients=np.ascontiguousarray(table.coefficients, dtype=np.float64),
+            log_field_min=float(table.log_field_min),
+            d_log_field=float(table.d_log_field),
+            field_min=float(table.field_min),
+            field_max=float(table.field_max),
+            rate_max=float(table.rate_max),
+            plasma_density=_table(channel.density),
+            preionisation=_table(channel.preionisation),
+        ))
     return record

@@ -26,7 +26,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-__all__ = ["PiecewiseTable", "ProblemRecord", "load_record", "save_record"]
+__all__ = ["PiecewiseTable", "PlasmaChannelRecord", "ProblemRecord", "RamanComponentRecord", "load_record",
+           "save_record"]
 
 # Fraction of a table's span a position may lie outside it (translate/chebyshev.py,
 # EDGE_SLACK_FRACTION): positions reached by summing steps arrive a few ulp off.
@@ -110,6 +111,34 @@ class PiecewiseTable:
 
 
 @dataclass
+class PlasmaChannelRecord:
+    """A further field-plasma channel of a gas mixture (``passes/plasma.py:326-485``): its
+    own rate table (``translate/ionisation.py:242-323``), population and path tables."""
+
+    charge_mass_ratio: float  # times the electrons per event
+    ionisation_potential: float
+    rate_coefficients: np.ndarray  # (4, n_intervals)
+    log_field_min: float
+    d_log_field: float
+    field_min: float
+    field_max: float
+    rate_max: float
+    plasma_density: PiecewiseTable | None = None
+    preionisation: PiecewiseTable | None = None
+
+
+@dataclass
+class RamanComponentRecord:
+    """A further Raman-active component of a gas mixture (``passes/responses.py:293-334``):
+    rows damped at their own rates, weighted by the fraction and the density."""
+
+    undamped: np.ndarray  # (n_terms, 2 n_to)
+    rates: list[PiecewiseTable]
+    fraction: float = 1.0
+    density: PiecewiseTable | None = None
+
+
+@dataclass
 class ProblemRecord:
     """One trajectory's lowered problem (see the module docstring).
 
@@ -187,6 +216,9 @@ class ProblemRecord:
     raman_fraction: float = 1.0
     raman_thg: bool = False
     raman_density: PiecewiseTable | None = None
+    # ---- a gas mixture: the plasma channels and Raman components after the first
+    extra_channels: list[PlasmaChannelRecord] = field(default_factory=list)
+    extra_raman: list[RamanComponentRecord] = field(default_factory=list)
     # ---- temporal absorber (stepping.py:286-369)
     absorber_scheme: str = "none"  # "nonlinear" | "split_step" | "none"
     temporal_absorber_fine: np.ndarray | None = None
@@ -260,6 +292,16 @@ def _table_arrays(prefix: str, table: PiecewiseTable | None, out: dict) -> None:
         out[f"{prefix}.c"] = table.coefficients
 
 
+_CHANNEL_SCALARS = ("charge_mass_ratio", "ionisation_potential", "log_field_min", "d_log_field",
+                    "field_min", "field_max", "rate_max")
+
+
+def _read_table(data, names, prefix: str) -> PiecewiseTable | None:
+    if f"{prefix}.bp" not in names:
+        return None
+    return PiecewiseTable(np.array(data[f"{prefix}.bp"]), np.array(data[f"{prefix}.c"]))
+
+
 def save_record(record: ProblemRecord, path) -> None:
     """Write a record to an ``.npz`` file: arrays by name, scalars as one JSON entry."""
     arrays: dict[str, np.ndarray] = {}
@@ -272,6 +314,23 @@ def save_record(record: ProblemRecord, path) -> None:
             for i, table in enumerate(value):
                 _table_arrays(f"raman_rates.{i}", table, arrays)
             meta["n_raman_rates"] = len(value)
+        elif f.name == "extra_channels":
+            scalars = []
+            for i, ch in enumerate(value):
+                arrays[f"extra_channels.{i}.rate_coefficients"] = ch.rate_coefficients
+                _table_arrays(f"extra_channels.{i}.plasma_density", ch.plasma_density, arrays)
+                _table_arrays(f"extra_channels.{i}.preionisation", ch.preionisation, arrays)
+                scalars.append({k: getattr(ch, k) for k in _CHANNEL_SCALARS})
+            meta["extra_channels"] = scalars
+        elif f.name == "extra_raman":
+            scalars = []
+            for i, comp in enumerate(value):
+                arrays[f"extra_raman.{i}.undamped"] = comp.undamped
+                for j, table in enumerate(comp.rates):
+                    _table_arrays(f"extra_raman.{i}.rates.{j}", table, arrays)
+                _table_arrays(f"extra_raman.{i}.density", comp.density, arrays)
+                scalars.append({"fraction": comp.fraction, "n_rates": len(comp.rates)})
+            meta["extra_raman"] = scalars
         elif isinstance(value, np.ndarray):
             arrays[f.name] = value
         elif value is None:
@@ -289,6 +348,8 @@ def load_record(path) -> ProblemRecord:
     kwargs: dict[str, object] = {}
     names = set(data.keys()) if isinstance(data, dict) else set(data.files)
     n_rates = int(meta.pop("n_raman_rates", 0))
+    channels = meta.pop("extra_channels", [])
+    components = meta.pop("extra_raman", [])
     for f in dataclasses.fields(ProblemRecord):
         if f.name in meta:
             kwargs[f.name] = meta[f.name]
@@ -301,6 +362,24 @@ def load_record(path) -> ProblemRecord:
     kwargs["raman_rates"] = [
         PiecewiseTable(np.array(data[f"raman_rates.{i}.bp"]), np.array(data[f"raman_rates.{i}.c"]))
         for i in range(n_rates)
+    ]
+    kwargs["extra_channels"] = [
+        PlasmaChannelRecord(
+            rate_coefficients=np.array(data[f"extra_channels.{i}.rate_coefficients"]),
+            plasma_density=_read_table(data, names, f"extra_channels.{i}.plasma_density"),
+            preionisation=_read_table(data, names, f"extra_channels.{i}.preionisation"),
+            **scalars,
+        )
+        for i, scalars in enumerate(channels)
+    ]
+    kwargs["extra_raman"] = [
+        RamanComponentRecord(
+            undamped=np.array(data[f"extra_raman.{i}.undamped"]),
+            rates=[_read_table(data, names, f"extra_raman.{i}.rates.{j}") for j in range(c["n_rates"])],
+            fraction=float(c["fraction"]),
+            density=_read_table(data, names, f"extra_raman.{i}.density"),
+        )
+        for i, c in enumerate(components)
     ]
     return ProblemRecord(**kwargs)
 

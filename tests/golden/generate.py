@@ -443,6 +443,91 @@ def raman_case(case, *, seed):
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
 
 
+def mixture_case(case, *, seed):
+    """A helium-argon mixture (0.7 : 0.3 at 1 bar) in a capillary: two field-plasma
+    channels, each with its own quasi-static ADK rate (the reference's test-only oracle),
+    exposure scan and population, their currents formed by the reference's multi-channel
+    pass; two modes, n_to 2048."""
+    he, ar = gas_species("He"), gas_species("Ar")
+    length = 0.02
+
+    def build(**kw):
+        fill = Mixture.fill({he: 0.7, ar: 0.3}, 1.0)
+        grid = FieldGrid.from_limits(length, 800e-9, (200e-9, 4e-6), 100e-15, fft_size="pow2")
+        return Simulation.from_capillary(
+            125e-6, length, fill, None, wavelength=800e-9, grid=grid, fwhm=10e-15, energy=60e-6,
+            cladding=1.45 + 0j, modes=2, plasma={"He": adk_oracle("He"), "Ar": adk_oracle("Ar")},
+            noise=None, rtol=1e-6, backend="numpy_ref", boundary_check=None, **kw)
+
+    sim = build(n_save=3)
+    problem = sim.translate()
+    assert len(problem.responses.plasma_channels) == 2
+    golden = source_fixture(sim, problem, [0.0, 0.37 * length], seed)
+    _, zs, states, (hist, counts), wall = drive(build(n_save=3))
+    golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.history": hist,
+                   "adaptive.counts": counts, "adaptive.wall": np.array(wall),
+                   "adaptive.policy": drive.policy})
+    print(f"{case}: adaptive run {counts} attempts/rejected in {wall:.2f} s", flush=True)
+    planes = np.linspace(0.0, length, 6)
+    schedule = FixedSchedule.uniform(0.0, length, length / 20, save_planes=planes)
+    fixed_problem, zs, states, (hist, counts), wall = drive(build(absorber=False, schedule=schedule, n_save=6))
+    golden.update({"fixed.z": zs, "fixed.states": states, "fixed.history": hist,
+                   "fixed.policy": drive.policy})
+    write(case, problem, golden)
+    save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
+
+
+def raman_mixture_case(case, *, seed):
+    """A nitrogen-hydrogen mixture (0.6 : 0.4 at 3 bar) with both gases' rotational and
+    vibrational Raman lines on the field grid -- two Raman components, one kernel spectrum
+    with the densities inside -- beside the real Kerr cubic, no plasma: the reference's
+    test-only molecular constants (``tests/former_raman.py``); Börzsönyi et al.'s
+    nitrogen index and Peck and Hung's hydrogen index (J. Opt. Soc. Am. 67, 1550 (1977));
+    two modes, n_to 4096."""
+    from former_raman import FORMER_H2, FORMER_N2
+
+    lam = np.geomspace(120e-9, 200e-6, 4000)[::-1]
+    om = 2 * np.pi * C0 / lam
+    l2 = (lam * 1e6) ** 2
+    rho0 = 1e5 / (K_B * 273.15)
+    b1, c1, b2, c2 = 39209.95e-8, 1146.24e-6, 18806.48e-8, 13.476e-3  # N2, 1 bar, 0 C
+    n2m1 = b1 * l2 / (l2 - c1) + b2 * l2 / (l2 - c2)
+    sus_n2 = TabulatedSusceptibility(om, (np.sqrt(1 + n2m1) - 1) / rho0, np.zeros_like(om),
+                                     (121e-9, 199e-6), "Borzsonyi 2008 N2")
+    inv = 1.0 / l2
+    h2m1 = 0.0148956 / (180.7 - inv) + 0.0049037 / (92.0 - inv)  # H2, 1 atm, 0 C
+    sus_h2 = TabulatedSusceptibility(om, h2m1 / (101325.0 / (K_B * 273.15)), np.zeros_like(om),
+                                     (121e-9, 199e-6), "Peck and Hung 1977 H2")
+    nitrogen = Species("N2", sus_n2, IdealGas(), gamma3=1.1e-52, raman=FORMER_N2)
+    hydrogen = Species("H2", sus_h2, IdealGas(), gamma3=6.4e-53, raman=FORMER_H2)
+    length = 0.05
+
+    def build(**kw):
+        fill = Mixture.fill({nitrogen: 0.6, hydrogen: 0.4}, 3.0)
+        grid = FieldGrid.from_limits(length, 800e-9, (300e-9, 3e-6), 300e-15, fft_size="pow2")
+        return Simulation.from_capillary(
+            125e-6, length, fill, None, wavelength=800e-9, grid=grid, fwhm=30e-15, energy=80e-6,
+            cladding=1.45 + 0j, modes=2, plasma=False, raman=True, thg=True, noise=None, rtol=1e-6,
+            backend="numpy_ref", boundary_check=None, **kw)
+
+    sim = build(n_save=3)
+    problem = sim.translate()
+    assert len(problem.responses.raman_terms) == 2
+    golden = source_fixture(sim, problem, [0.0, 0.37 * length], seed)
+    _, zs, states, (hist, counts), wall = drive(build(n_save=3))
+    golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.history": hist,
+                   "adaptive.counts": counts, "adaptive.wall": np.array(wall),
+                   "adaptive.policy": drive.policy})
+    print(f"{case}: adaptive run {counts} attempts/rejected in {wall:.2f} s", flush=True)
+    planes = np.linspace(0.0, length, 6)
+    schedule = FixedSchedule.uniform(0.0, length, length / 50, save_planes=planes)
+    fixed_problem, zs, states, (hist, counts), wall = drive(build(absorber=False, schedule=schedule, n_save=6))
+    golden.update({"fixed.z": zs, "fixed.states": states, "fixed.history": hist,
+                   "fixed.policy": drive.policy})
+    write(case, problem, golden)
+    save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
+
+
 def workload_case(case, *, seed, n_save=3, **common):
     """A full-size configuration: the problem, the march policy, two reference source
     evaluations, and the reference's whole adaptive run (exponential Adams at the route's
@@ -588,6 +673,10 @@ if __name__ == "__main__":
                  radial_rule="gauss", fixed_dz=0.001, n_fixed_planes=6, seed=6)
     if not only or "raman_n2" in only:
         raman_case("raman_n2", seed=8)
+    if not only or "mix_hear" in only:
+        mixture_case("mix_hear", seed=9)
+    if not only or "raman_mix" in only:
+        raman_mixture_case("raman_mix", seed=10)
     if not only or "radial_ar" in only:
         # the radial free-space route on 48 radial nodes (a 48 x 48 Hankel pair)
         radial_case("radial_ar", n_r=48, length=0.01, seed=7)

@@ -69,9 +69,10 @@ def test_reference_registry_refuses_by_name(reference):
     problem, request = sim.translate(), sim.run_request()
     import dataclasses
 
-    # two plasma channels: the device column carries one
+    # five plasma channels: the device column carries a mixture of four at most
     responses = problem.responses
-    doubled = dataclasses.replace(responses, plasma_channels=responses.plasma_channels * 2)
-    bad = dataclasses.replace(problem, responses=doubled)
+    five = dataclasses.replace(responses, plasma_channels=responses.plasma_channels * 5,
+                               ionisation_table=tuple(responses.ionisation_table) * 5)
+    bad = dataclasses.replace(problem, responses=five)
     with pytest.raises(BackendError, match="refused by the B200 backend"):
         registry.select("native", bad, request, grid=sim.grid, modes=sim.modes)
