@@ -151,6 +151,10 @@ typedef struct sp_run_desc {
   /* Runge-Kutta PI controller */
   double beta1, beta2, max_factor;
   int32_t lag, estimator_order;
+  /* Runge-Kutta start-up (rk_core.py:67-107): after the first accepted step, the deadbeat
+   * proposal its norm implies, at most start_growth times the first (0: off) */
+  int32_t auto_init;
+  double start_growth;
 } sp_run_desc;
 
 /* Why an advance() returned (the native march's Reason,

@@ -531,6 +531,23 @@ class RungeKuttaMarch:
         f = c["safety"] * (1.0 / current) ** c["beta1"] * (1.0 / previous) ** c["beta2"]
         return min(max(f, c["min_factor"]), c["max_factor"])
 
+    def _start_up(self, norm):
+        """``rk_core.py:67-107`` (``start_up``) with ``controller.py:528-561``
+        (``start_factor``): after the first accepted step the deadbeat proposal its norm
+        implies, at most ``start_growth`` times the first; the history records the norm
+        the first step would have scored at that length, or zero where the cap binds."""
+        c, p = self.c, self.p
+        growth = float(p.get("start_growth", 100.0))
+        q1 = c["estimator_order"] + 1
+        if not math.isfinite(norm) or norm <= 0.0:
+            factor = growth if norm == 0.0 else c["min_factor"]
+        else:
+            factor = min(max(c["safety"] * (1.0 / norm) ** (1.0 / q1), c["min_factor"]), growth)
+        following = limit_step(self.proposal, factor, p["dz_min"], p["dz_max"])
+        recorded = 0.0 if factor >= growth else norm * (following / self.proposal) ** q1
+        self.proposal = following
+        self.norms[-1] = recorded
+
     def march_to(self, target):
         p, c = self.p, self.c
         planes = tuple(float(v) for v in p["save_planes"])
@@ -549,6 +566,8 @@ class RungeKuttaMarch:
                 self.engine.accept()
                 self.z = end
                 self.norms.append(equivalent)
+                if p.get("auto_init") and len(self.norms) == 1:
+                    self._start_up(equivalent)
                 self.proposal = limit_step(self.proposal, self._propose_factor(), p["dz_min"], p["dz_max"])
             else:
                 self.rejected += 1

@@ -89,6 +89,7 @@ class SpRunDesc(C.Structure):
         ("real_intervals", C.c_double * 8),
         ("beta1", C.c_double), ("beta2", C.c_double), ("max_factor", C.c_double),
         ("lag", C.c_int32), ("estimator_order", C.c_int32),
+        ("auto_init", C.c_int32), ("start_growth", C.c_double),
     ]
 
 
@@ -448,6 +449,8 @@ def run_desc(rec, policy: dict, *, field0=None, schedule=None) -> tuple[SpRunDes
         r.beta1, r.beta2 = float(control["beta1"]), float(control["beta2"])
         r.lag = int(control["lag"])
         r.estimator_order = int(control["estimator_order"])
+        r.auto_init = int(bool(policy.get("auto_init", False)))
+        r.start_growth = float(policy.get("start_growth", 100.0))
     return r, m
 
 

@@ -70,6 +70,7 @@ void ensure_configured(int device) {
   CUDA_CHECK(configure_statistics_kernels());
   CUDA_CHECK(configure_modal_gemm());
   CUDA_CHECK(configure_raman_kernels());
+  CUDA_CHECK(configure_env_modal_kernels());
   g_configured[device] = true;
 }
 
@@ -216,14 +217,11 @@ static void validate(const sp_problem_desc* d) {
   if (d->n_modes * d->n_pol > kMaxGemmModes)
     throw Failure(SP_ERR_REFUSED, "more than 1024 modal columns");
   if (envelope) {
-    // the envelope route: one modal column on one node (the single-mode GNLSE)
-    if (d->n_modes * d->n_pol != 1 || d->n_nodes != 1)
-      throw Failure(SP_ERR_REFUSED, "the envelope grid with more than one mode or node is not built yet");
+    // the envelope route: one modal column on one node in one CTA (the single-mode GNLSE),
+    // or many modes and nodes on the products
     if (d->n_to > kMaxEnvelopeSamples)
       throw Failure(SP_ERR_REFUSED, "the envelope grid above 4096 samples is not built yet");
     if (d->plasma_enabled) throw Failure(SP_ERR_REFUSED, "envelope plasma is not built yet");
-    if (d->absorber_in_stage)
-      throw Failure(SP_ERR_REFUSED, "the in-stage absorber on the envelope grid is not built yet");
     if (d->kerr_enabled && (!d->kerr_analytic || d->kerr_take_real ||
                             (d->carrier && d->kerr_harmonic != 0.0)))
       throw Failure(SP_ERR_REFUSED, "the envelope route takes the analytic Kerr cubic without a harmonic");
@@ -637,12 +635,64 @@ static void eval_source_gemm(sp_workspace* ws, const double2* lab, int slot, boo
   }
 }
 
+// The envelope grid's source on the products: inverse transforms into the modal field (and
+// the absorber's spectrum), the synthesis product, the Raman kernel's spectrum, the nodes'
+// responses, the projection product, forward transforms.  Rows are complex, interleaved:
+// the products see N = 2 n_to.
+static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int slot, bool absorber) {
+  const sp_problem& P = *ws->P;
+  const sp_problem_desc& d = P.d;
+  const double* taper = &(ws->stage.p + slot)->taper;
+  const int n2 = 2 * d.n_to;
+  EnvModalArgs ea{};
+  ea.stage = ws->stage.p + slot;
+  ea.lab = lab;
+  ea.crop = ws->crop.p;
+  ea.twiddles = ws->env_twiddles.p;
+  ea.t_window = ws->t_window.p;
+  ea.alpha = absorber ? ws->alpha.p : nullptr;
+  ea.modal_t = ws->modal_t.p;
+  ea.node_field = ws->node_field.p;
+  ea.node_streams = ws->node_streams.p;
+  ea.projected = ws->proj.p;
+  ea.spectra = ws->spectra.p;
+  ea.raman_spectrum = d.raman_enabled ? ws->raman_spectrum.p : nullptr;
+  ea.n_cols = P.n_cols;
+  ea.n_omega = d.n_omega;
+  ea.n_to = d.n_to;
+  ea.log_n_to = ws->log_n_to;
+  ea.kerr = d.kerr_enabled;
+  ea.raman_mixture = P.raman_fraction.size() > 1;
+  ea.kerr_coefficient = d.kerr_coefficient;
+  ea.kerr_self = d.kerr_self;
+  ea.kerr_conjugate = d.kerr_conjugate;
+  { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_env_inverse(ea, ws->stream)); }
+  {
+    KernelTimer t(ws, SP_K_PROJECT);
+    CUDA_CHECK(modal_synthesis_f64(ws->synthesis.p, ws->modal_t.p, ws->node_field.p, d.n_nodes, d.n_modes, n2,
+                                   taper, ws->stream));
+  }
+  {
+    KernelTimer t(ws, SP_K_COLUMN);
+    if (d.raman_enabled) CUDA_CHECK(launch_raman_spectrum(raman_args(ws, slot), ws->stream));
+    CUDA_CHECK(launch_env_nodes(ea, d.n_nodes, ws->stream));
+  }
+  {
+    KernelTimer t(ws, SP_K_PROJECT);
+    CUDA_CHECK(modal_projection_f64(ws->projection.p, ws->node_streams.p, ws->proj.p, 1, d.n_modes, d.n_nodes,
+                                    n2, (size_t)P.n_cols * n2, taper, ws->proj_scratch.p, ws->stream));
+  }
+  { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_env_forward(ea, ws->stream)); }
+}
+
 // One source evaluation at lab (device), stage slot, optional inverse propagator.
 static void eval_source(sp_workspace* ws, const double2* lab, int slot, const double2* inv_prop,
                         double2* out, bool quiet) {
   const sp_problem& P = *ws->P;
   const bool absorber = P.d.absorber_in_stage && !quiet;
-  if (P.d.grid_kind == 1) {
+  if (P.d.grid_kind == 1 && ws->gemm) {
+    eval_source_envelope_gemm(ws, lab, slot, absorber);
+  } else if (P.d.grid_kind == 1) {
     const sp_problem_desc& d = P.d;
     EnvelopeArgs ea{};
     ea.stage = ws->stage.p + slot;
@@ -827,7 +877,8 @@ static void build_workspace(sp_workspace* ws) {
   ws->norm.upload(P.norm.data(), d.n_omega, s);
   ws->lab.alloc(n);
   ws->out.alloc(n);
-  ws->modal_t.alloc((size_t)P.n_cols * d.n_to);
+  const size_t cplx_rows = d.grid_kind == 1 ? 2 : 1;  // the envelope's rows are complex, interleaved
+  ws->modal_t.alloc(cplx_rows * P.n_cols * d.n_to);
   const size_t n_tiles = column_tiles(d);
   const size_t n_groups = (d.n_nodes + kGroup - 1) / kGroup;
   ws->sums0.alloc((size_t)std::max<size_t>(1, P.channels.size()) * d.n_nodes * n_tiles);  // a plane per channel
@@ -841,10 +892,10 @@ static void build_workspace(sp_workspace* ws) {
   ws->proj.alloc((ws->gemm ? 1 : n_groups) * 3 * P.n_cols * d.n_to);
   ws->proj.zero(s);
   if (ws->gemm) {
-    const size_t field = (size_t)d.n_nodes * d.n_to;
+    const size_t field = cplx_rows * d.n_nodes * d.n_to;
     ws->kpad_modes = modal_kpad(d.n_modes);
     ws->kpad_nodes = modal_kpad(d.n_nodes);
-    ws->proj_scratch.alloc(modal_projection_scratch(d.n_modes, d.n_nodes, d.n_to));
+    ws->proj_scratch.alloc(modal_projection_scratch(d.n_modes, d.n_nodes, (int)cplx_rows * d.n_to));
     if (ws->precision == SP_PRECISION_MIXED) {
       ws->f32.node_field.alloc(field);
       ws->f32.node_streams.alloc(3 * field);
@@ -878,7 +929,9 @@ static void build_workspace(sp_workspace* ws) {
   ws->norms.alloc(kMaxOrders + 2);
   ws->norms.zero(s);
   ws->launches = 5;
-  if (ws->gemm) {  // inverse, synthesis, column, one projection per stream, forward, output
+  if (ws->gemm && d.grid_kind == 1) {  // inverse, synthesis, (Raman spectrum,) nodes, projection, reduction,
+    ws->launches = 6 + (d.raman_enabled ? 1 : 0);  // forward, output
+  } else if (ws->gemm) {  // inverse, synthesis, column, one projection per stream, forward, output
     const int per_product = ws->precision == SP_PRECISION_MIXED ? 2 : 1;  // (split,) product
     const int streams = d.plasma_enabled ? 3 : 1;  // each: (split,) product, reduction of the K splits
     ws->launches = 4 + per_product + (per_product + 1) * streams + (d.raman_enabled ? 2 : 0);
@@ -892,7 +945,7 @@ static void build_workspace(sp_workspace* ws) {
     }
     ws->env_twiddles.upload(tw2.data(), tw2.size(), s);
     if (d.raman_enabled) ws->raman_undamped.upload(P.raman_undamped.data(), P.raman_undamped.size(), s);
-    if (d.raman_enabled && d.grid_kind == 0) ws->raman_spectrum.alloc((size_t)d.n_to + 1);
+    if (d.raman_enabled && (d.grid_kind == 0 || ws->gemm)) ws->raman_spectrum.alloc((size_t)d.n_to + 1);
     CUDA_CHECK(cudaStreamSynchronize(s));
   }
   CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1421,6 +1474,20 @@ static void rk_adaptive_attempt(sp_session* S, double target) {
     rk_accept(S);
     S->z = end;
     S->norms_hist.push_back(equivalent);
+    if (R.auto_init && S->norms_hist.size() == 1) {
+      // the start-up rule (rk_core.py:67-107, controller.py:528-561): the deadbeat step the
+      // first norm implies, capped at start_growth times the first; the history records the
+      // norm at that length, or zero where the cap binds
+      const double growth = R.start_growth > 0.0 ? R.start_growth : 100.0;
+      double factor;
+      if (!std::isfinite(equivalent) || equivalent <= 0.0)
+        factor = equivalent == 0.0 ? growth : R.min_factor;
+      else
+        factor = std::min(std::max(R.safety * std::pow(1.0 / equivalent, 1.0 / q1), R.min_factor), growth);
+      const double following = limit_step(S->proposal, factor, R.dz_min, R.dz_max);
+      S->norms_hist.back() = factor >= growth ? 0.0 : equivalent * std::pow(following / S->proposal, q1);
+      S->proposal = following;
+    }
     S->proposal = limit_step(S->proposal, rk_propose_factor(S), R.dz_min, R.dz_max);
   } else {
     S->rejected += 1;
@@ -1586,10 +1653,13 @@ sp_status sp_workspace_create_ex2(const sp_problem* problem, int device, int pre
     if (precision == SP_PRECISION_MIXED && d.grid_kind == 1)
       throw Failure(SP_ERR_REFUSED, "the mixed precision of the envelope route is not built yet");
     const bool field_raman = d.grid_kind == 0 && d.raman_enabled;
+    // the envelope grid's single CTA takes one column on one node without the absorber
+    const bool env_products = d.grid_kind == 1 && (problem->n_cols > 1 || d.n_nodes > 1 || d.absorber_in_stage);
     const bool gemm = modal == SP_MODAL_GEMM ||
-                      (modal == SP_MODAL_AUTO && (problem->n_cols > kMaxModes || field_raman));
-    if (gemm && d.grid_kind != 0)
-      throw Failure(SP_ERR_REFUSED, "the modal transform's products take the field grid");
+                      (modal == SP_MODAL_AUTO && (problem->n_cols > kMaxModes || field_raman || env_products));
+    if (!gemm && env_products)
+      throw Failure(SP_ERR_REFUSED,
+                    "the envelope grid's modes, nodes and in-stage absorber take the modal transform's products");
     if (!gemm && problem->n_cols > kMaxModes)
       throw Failure(SP_ERR_REFUSED, "more than 8 modal columns take the modal transform's products");
     if (!gemm && field_raman)

@@ -134,6 +134,11 @@ cudaError_t configure_raman_kernels() {
                               (int)raman_smem(kMaxRamanSamples));
 }
 
+cudaError_t launch_raman_spectrum(const RamanArgs& a, cudaStream_t s) {
+  k_raman_kernel<<<1, kRamanThreads, raman_smem(a.n_to) / 2, s>>>(a);
+  return cudaGetLastError();
+}
+
 template <class R>
 cudaError_t launch_raman(const RamanArgs& a, const R* field, R* polarisation, int n_nodes, cudaStream_t s) {
   k_raman_kernel<<<1, kRamanThreads, raman_smem(a.n_to) / 2, s>>>(a);

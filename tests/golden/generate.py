@@ -528,6 +528,53 @@ def raman_mixture_case(case, *, seed):
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
 
 
+def envelope_modal_case(case, *, seed, modes, integrator=None):
+    """A nitrogen-filled capillary on the envelope grid: several modes on the radial rule's
+    nodes, the analytic Kerr cubic, the gas's rotational and vibrational Raman response
+    (the drive |A|^2 / 2) and the in-stage collar -- the multimode generalised NLSE of the
+    reference's envelope modal route.  ``integrator`` None is the route's default march
+    (exponential Adams); the fixed schedule runs without the collar."""
+    from former_raman import FORMER_N2
+
+    lam = np.geomspace(120e-9, 200e-6, 4000)[::-1]
+    om = 2 * np.pi * C0 / lam
+    l2 = (lam * 1e6) ** 2
+    b1, c1, b2, c2 = 39209.95e-8, 1146.24e-6, 18806.48e-8, 13.476e-3  # N2, 1 bar, 0 C
+    n2m1 = b1 * l2 / (l2 - c1) + b2 * l2 / (l2 - c2)
+    rho0 = 1e5 / (K_B * 273.15)
+    sus = TabulatedSusceptibility(om, (np.sqrt(1 + n2m1) - 1) / rho0, np.zeros_like(om),
+                                  (121e-9, 199e-6), "Borzsonyi 2008 N2")
+    nitrogen = Species("N2", sus, IdealGas(), gamma3=1.1e-52, raman=FORMER_N2)
+    length = 0.1
+
+    def build(**kw):
+        fill = Mixture.fill({nitrogen: 1.0}, 2.0)
+        grid = EnvelopeGrid.from_limits(length, 800e-9, (550e-9, 1300e-9), 800e-15, fft_size="pow2")
+        extra = {} if integrator is None else {"integrator": integrator}
+        return Simulation.from_capillary(
+            100e-6, length, fill, None, wavelength=800e-9, grid=grid, fwhm=40e-15, energy=150e-6,
+            cladding=1.45 + 0j, modes=modes, raman=True, noise=None, rtol=1e-6, backend="numpy_ref",
+            boundary_check=None, envelope=True, **extra, **kw)
+
+    sim = build(n_save=3)
+    problem = sim.translate()
+    assert problem.grid_kind == "envelope" and problem.shape[0] == modes
+    print(f"{case}: n_to {problem.grids.n_to}, nodes {problem.transform.synthesis.shape[0]}", flush=True)
+    golden = source_fixture(sim, problem, [0.0, 0.37 * length], seed)
+    _, zs, states, (hist, counts), wall = drive(build(n_save=3))
+    golden.update({"adaptive.z": zs, "adaptive.states": states, "adaptive.history": hist,
+                   "adaptive.counts": counts, "adaptive.wall": np.array(wall),
+                   "adaptive.policy": drive.policy})
+    print(f"{case}: adaptive run {counts} attempts/rejected in {wall:.2f} s", flush=True)
+    planes = np.linspace(0.0, length, 6)
+    schedule = FixedSchedule.uniform(0.0, length, length / 50, save_planes=planes)
+    fixed_problem, zs, states, (hist, counts), wall = drive(build(absorber=False, schedule=schedule, n_save=6))
+    golden.update({"fixed.z": zs, "fixed.states": states, "fixed.history": hist,
+                   "fixed.policy": drive.policy})
+    write(case, problem, golden)
+    save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
+
+
 def workload_case(case, *, seed, n_save=3, **common):
     """A full-size configuration: the problem, the march policy, two reference source
     evaluations, and the reference's whole adaptive run (exponential Adams at the route's
@@ -677,6 +724,10 @@ if __name__ == "__main__":
         mixture_case("mix_hear", seed=9)
     if not only or "raman_mix" in only:
         raman_mixture_case("raman_mix", seed=10)
+    if not only or "env4_n2" in only:
+        envelope_modal_case("env4_n2", seed=11, modes=4)
+    if not only or "env3_rk" in only:
+        envelope_modal_case("env3_rk", seed=12, modes=3, integrator=RungeKutta())
     if not only or "radial_ar" in only:
         # the radial free-space route on 48 radial nodes (a 48 x 48 Hankel pair)
         radial_case("radial_ar", n_r=48, length=0.01, seed=7)

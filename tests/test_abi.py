@@ -40,7 +40,8 @@ def test_problem_descriptor_round_trip_and_refusals():
     # the problem object validates and copies on the host; no device needed
     problem = _lib.Problem(rec)
     problem.close()
-    # the single-mode envelope GNLSE with Raman is taken; a two-mode one is refused by name
+    # the envelope GNLSE with Raman is taken with one mode or two; above 4096 samples, or
+    # with plasma, it is refused by name
     env = load_record(ROOT / "tests" / "golden" / "gnlse_raman.problem.npz")
     _lib.Problem(env).close()
     env.n_modes = 2
@@ -49,7 +50,10 @@ def test_problem_descriptor_round_trip_and_refusals():
     env.phi_terms = np.repeat(env.phi_terms, 2, axis=1)
     env.prefactor_terms = np.repeat(env.prefactor_terms, 2, axis=1)
     env.field0 = np.repeat(env.field0, 2, axis=0)
-    with pytest.raises(_lib.BackendRefusal, match="envelope grid with more than one mode"):
+    _lib.Problem(env).close()
+    env.plasma_enabled = True
+    env.rate_coefficients = np.zeros((4, 1))
+    with pytest.raises(_lib.BackendRefusal, match="envelope plasma"):
         _lib.Problem(env)
 
 

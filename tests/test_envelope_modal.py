@@ -1,0 +1,89 @@
+"""The envelope grid's modal route with many modes and nodes, against the reference.
+
+``env4_n2`` and ``env3_rk`` are nitrogen-filled capillaries on the envelope grid: four and
+three modes on 33 radial nodes, n_to 1024, the analytic Kerr cubic, the gas's Raman
+response (drive |A|^2 / 2) and the in-stage collar -- the multimode generalised NLSE,
+stepped by exponential Adams and by DOPRI5.  A workspace takes the modal transform's
+products for them by itself (complex rows interleaved, N = 2 n_to); the single-CTA
+envelope kernel, which holds one column on one node, refuses them by name.
+"""
+
+import pytest
+
+from tests._cases import fixed_schedule, golden, policy, record, rel
+
+SOURCE_TOL = 1e-10  # the plain form, as every source test
+
+
+def test_many_modes_are_refused_by_the_single_cta_form():
+    from solprop_b200 import _lib
+
+    problem = _lib.Problem(record("env4_n2"))
+    with pytest.raises(_lib.BackendRefusal, match="envelope grid's modes, nodes and in-stage absorber"):
+        _lib.Workspace(problem, 0, "fp64", modal="fused")
+    with pytest.raises(_lib.BackendRefusal, match="mixed precision of the envelope route"):
+        _lib.Workspace(problem, 0, "mixed")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["env4_n2", "env3_rk"])
+@pytest.mark.parametrize("index", [0, 1])
+def test_source_matches_the_reference(case, index):
+    from solprop_b200 import _lib
+
+    rec, g = record(case), golden(case)
+    ws = _lib.Workspace(_lib.Problem(rec))
+    got = ws.source(g[f"src{index}.lab"], float(g[f"src{index}.z"]))
+    assert rel(got, g[f"src{index}.source"]) < SOURCE_TOL
+
+
+@pytest.mark.gpu
+def test_the_single_mode_envelope_gives_the_same_source_on_either_form():
+    """The GNLSE fixture (one column, one node) through the single CTA and the products."""
+    from solprop_b200 import _lib
+
+    rec, g = record("gnlse_raman"), golden("gnlse_raman")
+    problem = _lib.Problem(rec)
+    got = [_lib.Workspace(problem, 0, "fp64", modal=m).source(g["src1.lab"], float(g["src1.z"]))
+           for m in ("fused", "gemm")]
+    assert rel(got[1], g["src1.source"]) < SOURCE_TOL
+    assert rel(got[1], got[0]) < 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["env4_n2", "env3_rk"])
+def test_envelope_runs_step_with_the_reference(case):
+    """A fixed schedule plane by plane at 1e-10, and the adaptive run within its rtol with
+    the reference's attempt count (to +-3)."""
+    from solprop_b200 import _lib
+
+    rec, g = record(case, fixed=True), golden(case)
+    ws = _lib.Workspace(_lib.Problem(rec))
+    steps, _ = fixed_schedule(g)
+    session = ws.start(policy(g, "fixed"), schedule=steps)
+    zs, states = g["fixed.z"], g["fixed.states"]
+    plane = 1
+    while True:
+        batch = session.advance(1)
+        if plane < len(zs) and abs(batch.z - zs[plane]) < 1e-12:
+            assert rel(session.export(), states[plane]) < 1e-10, plane
+            plane += 1
+        if batch.event in (2, 3):
+            break
+    assert plane == len(zs)
+    rec = record(case)
+    ws = _lib.Workspace(_lib.Problem(rec))
+    pol = policy(g, "adaptive")
+    session = ws.start(pol)
+    zs, states = g["adaptive.z"], g["adaptive.states"]
+    seen = 1
+    while True:
+        batch = session.advance(256)
+        assert batch.event != 3
+        if batch.event in (1, 2):
+            assert rel(session.export(), states[seen]) < pol["rtol"]
+            seen += 1
+        if batch.event == 2:
+            break
+    assert seen == len(zs)
+    assert abs(batch.attempts - int(g["adaptive.counts"][0])) <= 3
