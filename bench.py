@@ -147,38 +147,6 @@ def cpu_arm(rec, pol, steps: int, warmup: int, budget_s: float, threads: int | N
     return done, elapsed
 
 
-def replayed_error(problem, pol: dict, device: int) -> dict:
-    """The precision error alone: the plain FP64 run's accepted steps, read off its attempt
-    rows, replayed as a fixed schedule in both precisions; the relative L2 difference of
-    the two final spectra.  An adaptive mixed run chooses its own steps, so its difference
-    from the FP64 run also holds the stepping error of two step sequences at the run's rtol."""
-    from solprop_b200 import _lib
-
-    ws = _lib.Workspace(problem, device, "fp64")
-    session = ws.start(pol)
-    ends = [0.0]
-    while True:
-        batch = session.advance(4096, rows=True)
-        ends += [float(r[0]) for r in batch.attempt_rows if r[3] > 0.5]
-        if batch.event in (2, 3):
-            break
-    session.close()
-    ws.close()
-    steps = np.diff(np.asarray(ends))
-    finals = {}
-    for precision in ("fp64", "mixed"):
-        ws = _lib.Workspace(problem, device, precision)
-        session = ws.start(pol, schedule=steps)
-        while session.advance(4096).event not in (2, 3):
-            pass
-        finals[precision] = session.export()
-        session.close()
-        ws.close()
-    a64, a32 = finals["fp64"], finals["mixed"]
-    return {"steps": int(steps.size),
-            "spectral_rel_l2": float(np.linalg.norm(a32 - a64) / np.linalg.norm(a64))}
-
-
 def runs_leg(device: int) -> dict:
     """Configs 1 and 2 run start to end, plain FP64 and mixed precision: runs per second,
     attempts per second, and the mixed run's relative L2 error against the FP64 run in
@@ -217,7 +185,6 @@ def runs_leg(device: int) -> dict:
         t32 = np.fft.irfft(a32.reshape(-1, a32.shape[-1]), axis=-1)
         out[case]["mixed_vs_fp64_spectral_rel_l2"] = float(np.linalg.norm(a32 - a64) / np.linalg.norm(a64))
         out[case]["mixed_vs_fp64_temporal_rel_l2"] = float(np.linalg.norm(t32 - t64) / np.linalg.norm(t64))
-        out[case]["mixed_vs_fp64_same_steps"] = replayed_error(problem, pol, device)
     return out
 
 
@@ -508,7 +475,7 @@ def complete_scan_leg(device: int, n_runs: int, seed: int = 2024, rank: int = 0,
         sc.close()
     batched_s = sides["mixed"]["seconds"]
     finished = sides["mixed"]["finished"]
-    plain_s, plain_attempts, plain_finals, plain_counts = 0.0, 0, [], []
+    plain_s, plain_attempts, plain_finals = 0.0, 0, []
     for rec, pol in zip(records, policies):
         problem = _lib.Problem(rec)
         ws = _lib.Workspace(problem, device)
@@ -520,18 +487,11 @@ def complete_scan_leg(device: int, n_runs: int, seed: int = 2024, rank: int = 0,
         torch.cuda.synchronize()
         plain_s += time.perf_counter() - t0
         plain_attempts += int(session.batch.attempts)
-        plain_counts.append(int(session.batch.attempts))
         plain_finals.append(session.export())
         session.close()
         ws.close()
         problem.close()
     errors = run_errors(finals["mixed"], plain_finals, records)
-    # the precision error alone on the runs whose adaptive difference is largest (among the
-    # runs of at most 8000 attempts): both precisions on the FP64 run's own steps
-    spectral = [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(finals["mixed"], plain_finals)]
-    worst = sorted((i for i in range(len(records)) if plain_counts[i] <= 8000), key=lambda i: -spectral[i])[:4]
-    errors["same_steps"] = [{"run": int(i), "adaptive": spectral[i],
-                             **replayed_error(_lib.Problem(records[i]), policies[i], device)} for i in worst]
     batched64_s = sides["fp64"]["seconds"] if "fp64" in sides else None
     if world > 1:
         import torch.distributed as dist
