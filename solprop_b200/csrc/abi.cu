@@ -303,6 +303,7 @@ struct sp_workspace {
     DevBuf<float> t_window, t_window_d, synthesis, projection, rate_coeff, taps, proj;
     DevBuf<float> node_field, node_streams;
     DevBuf<ChannelTableT<float>> channels;
+    DevBuf<float2> env_twiddles;
   } f32;
   DevBuf<unsigned char> active, norm;
   DevBuf<StageScalarsDev> stage;   // kStageSlots slots
@@ -638,13 +639,13 @@ static void eval_source_gemm(sp_workspace* ws, const double2* lab, int slot, boo
 // The envelope grid's source on the products: inverse transforms into the modal field (and
 // the absorber's spectrum), the synthesis product, the Raman kernel's spectrum, the nodes'
 // responses, the projection product, forward transforms.  Rows are complex, interleaved:
-// the products see N = 2 n_to.
-static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int slot, bool absorber) {
+// the products see N = 2 n_to.  The mixed form's products are the tcgen05 products of
+// three-part BF16 splits; its node field, streams and spectra are FP32.
+template <class R>
+static EnvModalArgsT<R> env_modal_args(const sp_workspace* ws, const double2* lab, int slot, bool absorber) {
   const sp_problem& P = *ws->P;
   const sp_problem_desc& d = P.d;
-  const double* taper = &(ws->stage.p + slot)->taper;
-  const int n2 = 2 * d.n_to;
-  EnvModalArgs ea{};
+  EnvModalArgsT<R> ea{};
   ea.stage = ws->stage.p + slot;
   ea.lab = lab;
   ea.crop = ws->crop.p;
@@ -652,10 +653,6 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
   ea.t_window = ws->t_window.p;
   ea.alpha = absorber ? ws->alpha.p : nullptr;
   ea.modal_t = ws->modal_t.p;
-  ea.node_field = ws->node_field.p;
-  ea.node_streams = ws->node_streams.p;
-  ea.projected = ws->proj.p;
-  ea.spectra = ws->spectra.p;
   ea.raman_spectrum = d.raman_enabled ? ws->raman_spectrum.p : nullptr;
   ea.n_cols = P.n_cols;
   ea.n_omega = d.n_omega;
@@ -666,6 +663,52 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
   ea.kerr_coefficient = d.kerr_coefficient;
   ea.kerr_self = d.kerr_self;
   ea.kerr_conjugate = d.kerr_conjugate;
+  if constexpr (sizeof(R) == 8) {
+    ea.twiddles_r = ws->env_twiddles.p;
+    ea.node_field = ws->node_field.p;
+    ea.node_streams = ws->node_streams.p;
+    ea.projected = ws->proj.p;
+    ea.spectra = ws->spectra.p;
+  } else {
+    ea.twiddles_r = ws->f32.env_twiddles.p;
+    ea.node_field = ws->f32.node_field.p;
+    ea.node_streams = ws->f32.node_streams.p;
+    ea.projected = ws->f32.proj.p;
+    ea.spectra = ws->f32.spectra.p;
+  }
+  return ea;
+}
+
+static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int slot, bool absorber) {
+  const sp_problem& P = *ws->P;
+  const sp_problem_desc& d = P.d;
+  const double* taper = &(ws->stage.p + slot)->taper;
+  double* status = ws->norms.p + kColumnStatus;
+  const int n2 = 2 * d.n_to;
+  const size_t stride = (size_t)P.n_cols * n2;
+  if (ws->precision == SP_PRECISION_MIXED) {
+    const auto ea = env_modal_args<float>(ws, lab, slot, absorber);
+    { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_env_inverse(ea, ws->stream)); }
+    {
+      KernelTimer t(ws, SP_K_PROJECT);
+      CUDA_CHECK(modal_synthesis_split3(ws->s_parts.p, ws->modal_t.p, ws->modal_parts.p, ws->f32.node_field.p,
+                                        d.n_nodes, d.n_modes, n2, ws->kpad_modes, taper, status, ws->stream));
+    }
+    {
+      KernelTimer t(ws, SP_K_COLUMN);
+      if (d.raman_enabled) CUDA_CHECK(launch_raman_spectrum(raman_args(ws, slot), ws->stream));
+      CUDA_CHECK(launch_env_nodes(ea, d.n_nodes, ws->stream));
+    }
+    {
+      KernelTimer t(ws, SP_K_PROJECT);
+      CUDA_CHECK(modal_projection_split3(ws->w_parts.p, ws->f32.node_streams.p, ws->node_parts.p, ws->f32.proj.p,
+                                         1, d.n_modes, d.n_nodes, n2, ws->kpad_nodes, stride, taper, status,
+                                         reinterpret_cast<float*>(ws->proj_scratch.p), ws->stream));
+    }
+    { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_env_forward(ea, ws->stream)); }
+    return;
+  }
+  const auto ea = env_modal_args<double>(ws, lab, slot, absorber);
   { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_env_inverse(ea, ws->stream)); }
   {
     KernelTimer t(ws, SP_K_PROJECT);
@@ -680,7 +723,7 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
   {
     KernelTimer t(ws, SP_K_PROJECT);
     CUDA_CHECK(modal_projection_f64(ws->projection.p, ws->node_streams.p, ws->proj.p, 1, d.n_modes, d.n_nodes,
-                                    n2, (size_t)P.n_cols * n2, taper, ws->proj_scratch.p, ws->stream));
+                                    n2, stride, taper, ws->proj_scratch.p, ws->stream));
   }
   { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_env_forward(ea, ws->stream)); }
 }
@@ -907,8 +950,8 @@ static void build_workspace(sp_workspace* ws) {
       split3_host(P.projection.data(), d.n_modes, d.n_nodes, ws->kpad_nodes, parts);
       ws->w_parts.upload(parts.data(), parts.size(), s);
       CUDA_CHECK(cudaStreamSynchronize(s));
-      ws->modal_parts.alloc((size_t)3 * d.n_to * ws->kpad_modes);
-      ws->node_parts.alloc((size_t)3 * d.n_to * ws->kpad_nodes);
+      ws->modal_parts.alloc((size_t)3 * cplx_rows * d.n_to * ws->kpad_modes);
+      ws->node_parts.alloc((size_t)3 * cplx_rows * d.n_to * ws->kpad_nodes);
     } else {
       ws->node_field.alloc(field);
       ws->node_streams.alloc(3 * field);
@@ -930,7 +973,8 @@ static void build_workspace(sp_workspace* ws) {
   ws->norms.zero(s);
   ws->launches = 5;
   if (ws->gemm && d.grid_kind == 1) {  // inverse, synthesis, (Raman spectrum,) nodes, projection, reduction,
-    ws->launches = 6 + (d.raman_enabled ? 1 : 0);  // forward, output
+    ws->launches = 6 + (d.raman_enabled ? 1 : 0) + (ws->precision == SP_PRECISION_MIXED ? 2 : 0);  // forward,
+                                                                  // output; the mixed form's two split passes
   } else if (ws->gemm) {  // inverse, synthesis, column, one projection per stream, forward, output
     const int per_product = ws->precision == SP_PRECISION_MIXED ? 2 : 1;  // (split,) product
     const int streams = d.plasma_enabled ? 3 : 1;  // each: (split,) product, reduction of the K splits
@@ -944,6 +988,12 @@ static void build_workspace(sp_workspace* ws) {
       tw2[m] = make_double2((double)cosl(ang), (double)(-sinl(ang)));
     }
     ws->env_twiddles.upload(tw2.data(), tw2.size(), s);
+    if (ws->precision == SP_PRECISION_MIXED) {
+      std::vector<float2> tw2f(tw2.size());
+      for (size_t m = 0; m < tw2.size(); ++m) tw2f[m] = make_float2((float)tw2[m].x, (float)tw2[m].y);
+      ws->f32.env_twiddles.upload(tw2f.data(), tw2f.size(), s);
+      CUDA_CHECK(cudaStreamSynchronize(s));  // the host copy goes with this scope
+    }
     if (d.raman_enabled) ws->raman_undamped.upload(P.raman_undamped.data(), P.raman_undamped.size(), s);
     if (d.raman_enabled && (d.grid_kind == 0 || ws->gemm)) ws->raman_spectrum.alloc((size_t)d.n_to + 1);
     CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1650,13 +1700,14 @@ sp_status sp_workspace_create_ex2(const sp_problem* problem, int device, int pre
     if (modal != SP_MODAL_AUTO && modal != SP_MODAL_FUSED && modal != SP_MODAL_GEMM)
       throw Failure(SP_ERR_ARGUMENT, "unknown modal transform form");
     const sp_problem_desc& d = problem->d;
-    if (precision == SP_PRECISION_MIXED && d.grid_kind == 1)
-      throw Failure(SP_ERR_REFUSED, "the mixed precision of the envelope route is not built yet");
     const bool field_raman = d.grid_kind == 0 && d.raman_enabled;
     // the envelope grid's single CTA takes one column on one node without the absorber
-    const bool env_products = d.grid_kind == 1 && (problem->n_cols > 1 || d.n_nodes > 1 || d.absorber_in_stage);
+    const bool env_products = d.grid_kind == 1 && (problem->n_cols > 1 || d.n_nodes > 1 || d.absorber_in_stage ||
+                                                   precision == SP_PRECISION_MIXED);
     const bool gemm = modal == SP_MODAL_GEMM ||
                       (modal == SP_MODAL_AUTO && (problem->n_cols > kMaxModes || field_raman || env_products));
+    if (!gemm && precision == SP_PRECISION_MIXED && d.grid_kind == 1)
+      throw Failure(SP_ERR_REFUSED, "the mixed precision of the envelope route takes the modal transform's products");
     if (!gemm && env_products)
       throw Failure(SP_ERR_REFUSED,
                     "the envelope grid's modes, nodes and in-stage absorber take the modal transform's products");

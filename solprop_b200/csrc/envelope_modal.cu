@@ -9,12 +9,15 @@
 //                  interleaved (re, im) rows of 2 n_to; the absorber's spectrum
 //                  FFT[-alpha a / 2], cropped, into its spectra block
 //   products       E = tau S a and P_m = sum W P / tau over the interleaved rows
-//                  (modal_gemm.cu), N = 2 n_to
+//                  (modal_gemm.cu), N = 2 n_to: FP64 products, or tcgen05 products of
+//                  three-part BF16 splits accumulated in FP32 in the mixed form
 //   k_env_nodes    one CTA per node: the Kerr cubic, the Raman convolution, the window g
 //   k_env_forward  one CTA per modal column: fft of the projected row, cropped
 //
 // Every transform is the shared-memory radix-4 FFT of fft.cuh over the table
-// exp(-2 pi i m / (2 n_to)), m < n_to, in FP64.
+// exp(-2 pi i m / (2 n_to)), m < n_to.  The inverse transform and the modal field are
+// FP64 in both forms; the nodes' responses and the forward transform run in the form's
+// type R (FP32 in the mixed form, the Raman kernel's spectrum rounded to it).
 #include "fft.cuh"
 #include "kernels.cuh"
 
@@ -27,18 +30,27 @@ constexpr int kEnvThreads = 1024;
 
 // X[k] = E_k + w^k O_k of a packed real transform of length 2 n (k in [0, n]); Z in
 // bit-reversed order, w = exp(-2 pi i k / 2n) = tw[k] (k < n), -1 at k = n
-__device__ __forceinline__ double2 unpack_real(const double2* Z, const double2* tw, int k, int n, int log_n) {
+template <class C>
+__device__ __forceinline__ C unpack_real(const C* Z, const C* tw, int k, int n, int log_n) {
+  using R = decltype(C{}.x);
   const int kk = k == n ? 0 : k;
   const int km = k == 0 ? 0 : (n - k == n ? 0 : n - k);
-  const double2 zk = Z[bitrev(kk, log_n)];
-  const double2 zm = cconj(Z[bitrev(km, log_n)]);
-  const double2 e = cscale(0.5, cadd(zk, zm));
-  const double2 o = cscale(0.5, mul_mi(csub(zk, zm)));
-  const double2 w = k < n ? tw[k] : make_double2(-1.0, 0.0);
+  const C zk = Z[bitrev(kk, log_n)];
+  const C zm = cconj(Z[bitrev(km, log_n)]);
+  const C e = cscale(R(0.5), cadd(zk, zm));
+  const C o = cscale(R(0.5), mul_mi(csub(zk, zm)));
+  C w;
+  if (k < n) {
+    w = tw[k];
+  } else {
+    w.x = R(-1);
+    w.y = R(0);
+  }
   return cadd(e, cmul(w, o));
 }
 
-__global__ void __launch_bounds__(kEnvThreads) k_env_inverse(EnvModalArgs a) {
+template <class R>
+__global__ void __launch_bounds__(kEnvThreads) k_env_inverse(EnvModalArgsT<R> a) {
   extern __shared__ __align__(16) double2 ei_raw[];
   const int n = a.n_to, col = blockIdx.x;
   double2* A = ei_raw;
@@ -54,90 +66,98 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_inverse(EnvModalArgs a) {
   if (!a.alpha) return;
   // the in-stage absorber -alpha a / 2, transformed and cropped (stage output masks it)
   double2* B = A + n;
-  __syncthreads();  // the rows above read A in bit-reversed order
   for (int t = threadIdx.x; t < n; t += blockDim.x)
     B[t] = cscale(-0.5 * a.alpha[t], cscale(inv_n, A[bitrev(t, a.log_n_to)]));
   __syncthreads();
   fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
-  double2* absorber = a.spectra + (size_t)3 * a.n_cols * a.n_omega + (size_t)col * a.n_omega;
-  for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) absorber[j] = B[bitrev((int)a.crop[j], a.log_n_to)];
+  cplx<R>* absorber = a.spectra + (size_t)3 * a.n_cols * a.n_omega + (size_t)col * a.n_omega;
+  for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x)
+    absorber[j] = to_c<cplx<R>>(B[bitrev((int)a.crop[j], a.log_n_to)]);
 }
 
-__global__ void __launch_bounds__(kEnvThreads) k_env_nodes(EnvModalArgs a) {
-  extern __shared__ __align__(16) double2 en_raw[];
+template <class R>
+__global__ void __launch_bounds__(kEnvThreads) k_env_nodes(EnvModalArgsT<R> a) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char en_raw[];
   const int n = a.n_to, node = blockIdx.x;
-  double2* B = en_raw;  // the drive's transform, then the convolution's
-  double2* C = B + n;   // H D
-  __shared__ double2 top;  // bin n
+  C* B = reinterpret_cast<C*>(en_raw);  // the drive's transform, then the convolution's
+  C* H = B + n;                          // H D
+  __shared__ C top;                      // bin n
   const StageScalarsDev& st = *a.stage;
-  const double2* E = reinterpret_cast<const double2*>(a.node_field) + (size_t)node * n;
+  const C* E = reinterpret_cast<const C*>(a.node_field) + (size_t)node * n;
   const bool raman = a.raman_spectrum != nullptr;
   if (raman) {
     // the drive |E|^2 / 2 on [0, n), zero on [n, 2n), packed
     for (int m = threadIdx.x; m < n; m += blockDim.x) {
-      double v[2] = {0.0, 0.0};
+      R v[2] = {R(0), R(0)};
       if (2 * m < n) {
         for (int q = 0; q < 2; ++q) {
-          const double2 e = E[2 * m + q];
-          v[q] = 0.5 * (e.x * e.x + e.y * e.y);
+          const C e = E[2 * m + q];
+          v[q] = R(0.5) * (e.x * e.x + e.y * e.y);
         }
       }
-      B[m] = make_double2(v[0], v[1]);
+      B[m].x = v[0];
+      B[m].y = v[1];
     }
     __syncthreads();
-    fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
+    fft_dif_inplace(B, a.log_n_to, a.twiddles_r, a.log_n_to + 1, /*inverse=*/false);
     for (int k = threadIdx.x; k <= n; k += blockDim.x) {
-      const double2 y = cmul(a.raman_spectrum[k], unpack_real(B, a.twiddles, k, n, a.log_n_to));
-      if (k < n) C[k] = y;
+      const C y = cmul(to_c<C>(a.raman_spectrum[k]), unpack_real(B, a.twiddles_r, k, n, a.log_n_to));
+      if (k < n) H[k] = y;
       else top = y;
     }
     __syncthreads();
     // irfft of length 2n: Z_k = E_k + i O_k, E_k = (Y_k + Y*_{n-k}) / 2,
     // O_k = (Y_k - Y*_{n-k}) conj(w^k) / 2; the imaginary parts of bins 0 and n dropped
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      double2 yk = C[k], ym = k == 0 ? top : C[n - k];
+      C yk = H[k], ym = k == 0 ? top : H[n - k];
       if (k == 0) {
-        yk.y = 0.0;
-        ym.y = 0.0;
+        yk.y = R(0);
+        ym.y = R(0);
       }
       ym = cconj(ym);
-      const double2 e = cscale(0.5, cadd(yk, ym));
-      const double2 o = cscale(0.5, cmul(csub(yk, ym), cconj(a.twiddles[k])));
+      const C e = cscale(R(0.5), cadd(yk, ym));
+      const C o = cscale(R(0.5), cmul(csub(yk, ym), cconj(a.twiddles_r[k])));
       B[k] = cadd(e, mul_pi(o));
     }
     __syncthreads();
-    fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/true);
+    fft_dif_inplace(B, a.log_n_to, a.twiddles_r, a.log_n_to + 1, /*inverse=*/true);
   }
-  const double factor = a.kerr ? a.kerr_coefficient * st.kerr_density : 0.0;
-  const double raman_scale = kEps0 * (a.raman_mixture ? 1.0 : st.raman_density);  // a mixture's are inside
-  const double inv_n = 1.0 / (double)n;
-  double2* P = reinterpret_cast<double2*>(a.node_streams) + (size_t)node * n;
+  const R factor = R(a.kerr ? a.kerr_coefficient * st.kerr_density : 0.0);
+  const R self = R(a.kerr_self), conj = R(a.kerr_conjugate);
+  const R raman_scale = R(kEps0 * (a.raman_mixture ? 1.0 : st.raman_density));  // a mixture's are inside
+  const R inv_n = R(1.0 / (double)n);
+  C* P = reinterpret_cast<C*>(a.node_streams) + (size_t)node * n;
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
-    const double2 e = E[t];
-    double2 p = make_double2(0.0, 0.0);
+    const C e = E[t];
+    C p;
+    p.x = R(0);
+    p.y = R(0);
     if (a.kerr) {
-      const double mod = e.x * e.x + e.y * e.y;
-      const double2 sq = cmul(e, e);
-      p = cscale(factor, cadd(cscale(a.kerr_self * mod, e), cscale(a.kerr_conjugate, cmul(sq, cconj(e)))));
+      const R mod = e.x * e.x + e.y * e.y;
+      const C sq = cmul(e, e);
+      p = cscale(factor, cadd(cscale(self * mod, e), cscale(conj, cmul(sq, cconj(e)))));
     }
     if (raman) {
-      const double2 z = B[bitrev(t >> 1, a.log_n_to)];
-      const double conv = ((t & 1) ? z.y : z.x) * inv_n;  // irfft's 1 / (2n), with the packing's 2
+      const C z = B[bitrev(t >> 1, a.log_n_to)];
+      const R conv = ((t & 1) ? z.y : z.x) * inv_n;  // irfft's 1 / (2n), with the packing's 2
       p = cadd(p, cscale(raman_scale * conv, e));
     }
-    P[t] = cscale(a.t_window[t], p);
+    P[t] = cscale(R(a.t_window[t]), p);
   }
 }
 
-__global__ void __launch_bounds__(kEnvThreads) k_env_forward(EnvModalArgs a) {
-  extern __shared__ __align__(16) double2 ef_raw[];
+template <class R>
+__global__ void __launch_bounds__(kEnvThreads) k_env_forward(EnvModalArgsT<R> a) {
+  using C = cplx<R>;
+  extern __shared__ __align__(16) unsigned char ef_raw[];
   const int n = a.n_to, col = blockIdx.x;
-  double2* A = ef_raw;
-  const double2* row = reinterpret_cast<const double2*>(a.projected) + (size_t)col * n;
+  C* A = reinterpret_cast<C*>(ef_raw);
+  const C* row = reinterpret_cast<const C*>(a.projected) + (size_t)col * n;
   for (int t = threadIdx.x; t < n; t += blockDim.x) A[t] = row[t];
   __syncthreads();
-  fft_dif_inplace(A, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
-  double2* spectra = a.spectra + (size_t)col * a.n_omega;
+  fft_dif_inplace(A, a.log_n_to, a.twiddles_r, a.log_n_to + 1, /*inverse=*/false);
+  C* spectra = a.spectra + (size_t)col * a.n_omega;
   for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) spectra[j] = A[bitrev((int)a.crop[j], a.log_n_to)];
 }
 
@@ -145,27 +165,41 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_forward(EnvModalArgs a) {
 
 cudaError_t configure_env_modal_kernels() {
   const int two = (int)(2 * kMaxEnvelopeSamples * sizeof(double2)), one = two / 2;
-  cudaError_t e = cudaFuncSetAttribute(k_env_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, two);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_env_nodes, cudaFuncAttributeMaxDynamicSharedMemorySize, two);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_env_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, one);
+  const void* kernels[6] = {(const void*)k_env_inverse<double>, (const void*)k_env_inverse<float>,
+                            (const void*)k_env_nodes<double>,   (const void*)k_env_nodes<float>,
+                            (const void*)k_env_forward<double>, (const void*)k_env_forward<float>};
+  const int shm[6] = {two, two, two, one, one, one / 2};
+  for (int i = 0; i < 6; ++i) {
+    cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shm[i]);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
-cudaError_t launch_env_inverse(const EnvModalArgs& a, cudaStream_t s) {
+template <class R>
+cudaError_t launch_env_inverse(const EnvModalArgsT<R>& a, cudaStream_t s) {
   const size_t row = (size_t)a.n_to * sizeof(double2);
-  k_env_inverse<<<a.n_cols, kEnvThreads, a.alpha ? 2 * row : row, s>>>(a);
+  k_env_inverse<R><<<a.n_cols, kEnvThreads, a.alpha ? 2 * row : row, s>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_env_nodes(const EnvModalArgs& a, int n_nodes, cudaStream_t s) {
-  k_env_nodes<<<n_nodes, kEnvThreads, (size_t)2 * a.n_to * sizeof(double2), s>>>(a);
+template <class R>
+cudaError_t launch_env_nodes(const EnvModalArgsT<R>& a, int n_nodes, cudaStream_t s) {
+  k_env_nodes<R><<<n_nodes, kEnvThreads, (size_t)2 * a.n_to * sizeof(cplx<R>), s>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_env_forward(const EnvModalArgs& a, cudaStream_t s) {
-  k_env_forward<<<a.n_cols, kEnvThreads, (size_t)a.n_to * sizeof(double2), s>>>(a);
+template <class R>
+cudaError_t launch_env_forward(const EnvModalArgsT<R>& a, cudaStream_t s) {
+  k_env_forward<R><<<a.n_cols, kEnvThreads, (size_t)a.n_to * sizeof(cplx<R>), s>>>(a);
   return cudaGetLastError();
 }
+
+template cudaError_t launch_env_inverse<double>(const EnvModalArgsT<double>&, cudaStream_t);
+template cudaError_t launch_env_inverse<float>(const EnvModalArgsT<float>&, cudaStream_t);
+template cudaError_t launch_env_nodes<double>(const EnvModalArgsT<double>&, int, cudaStream_t);
+template cudaError_t launch_env_nodes<float>(const EnvModalArgsT<float>&, int, cudaStream_t);
+template cudaError_t launch_env_forward<double>(const EnvModalArgsT<double>&, cudaStream_t);
+template cudaError_t launch_env_forward<float>(const EnvModalArgsT<float>&, cudaStream_t);
 
 }  // namespace sp

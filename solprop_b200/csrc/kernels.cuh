@@ -224,27 +224,35 @@ cudaError_t configure_raman_kernels();
 cudaError_t launch_raman_spectrum(const RamanArgs& a, cudaStream_t s);  // the kernel's spectrum alone
 
 // The envelope grid's modal route with many modes and nodes on the products
-// (envelope_modal.cu): complex rows interleaved (re, im), n_to <= kMaxEnvelopeSamples.
-struct EnvModalArgs {
+// (envelope_modal.cu): complex rows interleaved (re, im), n_to <= kMaxEnvelopeSamples.  R
+// is the form's real type: the inverse transform and the modal field are FP64 in both
+// forms; the node field and streams, the nodes' responses, the forward transform and the
+// spectra are R.
+template <class R>
+struct EnvModalArgsT {
   const StageScalarsDev* stage;
   const double2* lab;             // (n_cols, n_omega)
   const long long* crop;          // (n_omega): coarse bin -> fine bin
   const double2* twiddles;        // exp(-2 pi i m / (2 n_to)), m < n_to
+  const cplx<R>* twiddles_r;      // the same table in the form's type
   const double* t_window;         // (n_to)
   const double* alpha;            // the in-stage absorber's rate (n_to), or null
   double* modal_t;                // (n_cols, 2 n_to): a(t)
-  const double* node_field;       // (n_nodes, 2 n_to): E = tau S a
-  double* node_streams;           // (n_nodes, 2 n_to): the gated polarisation
-  const double* projected;        // (n_cols, 2 n_to): sum W P / tau
-  double2* spectra;               // (4, n_cols, n_omega): P, -, -, absorber
+  const R* node_field;            // (n_nodes, 2 n_to): E = tau S a
+  R* node_streams;                // (n_nodes, 2 n_to): the gated polarisation
+  const R* projected;             // (n_cols, 2 n_to): sum W P / tau
+  cplx<R>* spectra;               // (4, n_cols, n_omega): P, -, -, absorber
   const double2* raman_spectrum;  // (n_to + 1), or null without Raman
   int n_cols, n_omega, n_to, log_n_to, kerr, raman_mixture;
   double kerr_coefficient, kerr_self, kerr_conjugate;
 };
 cudaError_t configure_env_modal_kernels();
-cudaError_t launch_env_inverse(const EnvModalArgs& a, cudaStream_t s);
-cudaError_t launch_env_nodes(const EnvModalArgs& a, int n_nodes, cudaStream_t s);
-cudaError_t launch_env_forward(const EnvModalArgs& a, cudaStream_t s);
+template <class R>
+cudaError_t launch_env_inverse(const EnvModalArgsT<R>& a, cudaStream_t s);
+template <class R>
+cudaError_t launch_env_nodes(const EnvModalArgsT<R>& a, int n_nodes, cudaStream_t s);
+template <class R>
+cudaError_t launch_env_forward(const EnvModalArgsT<R>& a, cudaStream_t s);
 template <class R>
 cudaError_t launch_raman(const RamanArgs& a, const R* field, R* polarisation, int n_nodes, cudaStream_t s);
 

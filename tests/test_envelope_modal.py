@@ -13,6 +13,7 @@ import pytest
 from tests._cases import fixed_schedule, golden, policy, record, rel
 
 SOURCE_TOL = 1e-10  # the plain form, as every source test
+MIXED_TOL = 2e-6  # the mixed form's source tolerance (tests/test_mixed.py)
 
 
 def test_many_modes_are_refused_by_the_single_cta_form():
@@ -21,8 +22,9 @@ def test_many_modes_are_refused_by_the_single_cta_form():
     problem = _lib.Problem(record("env4_n2"))
     with pytest.raises(_lib.BackendRefusal, match="envelope grid's modes, nodes and in-stage absorber"):
         _lib.Workspace(problem, 0, "fp64", modal="fused")
-    with pytest.raises(_lib.BackendRefusal, match="mixed precision of the envelope route"):
-        _lib.Workspace(problem, 0, "mixed")
+    single = _lib.Problem(record("gnlse_raman"))
+    with pytest.raises(_lib.BackendRefusal, match="mixed precision of the envelope route takes"):
+        _lib.Workspace(single, 0, "mixed", modal="fused")
 
 
 @pytest.mark.gpu
@@ -35,6 +37,39 @@ def test_source_matches_the_reference(case, index):
     ws = _lib.Workspace(_lib.Problem(rec))
     got = ws.source(g[f"src{index}.lab"], float(g[f"src{index}.z"]))
     assert rel(got, g[f"src{index}.source"]) < SOURCE_TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "gnlse_raman"])
+def test_split_bf16_products_match_the_reference_to_fp32(case):
+    """The mixed form: tcgen05 products of three-part BF16 splits, FP32 responses."""
+    from solprop_b200 import _lib
+
+    rec, g = record(case), golden(case)
+    ws = _lib.Workspace(_lib.Problem(rec), 0, "mixed")
+    for index in (0, 1):
+        got = ws.source(g[f"src{index}.lab"], float(g[f"src{index}.z"]))
+        assert rel(got, g[f"src{index}.source"]) < MIXED_TOL, index
+
+
+@pytest.mark.gpu
+def test_mixed_envelope_run_stays_near_the_reference():
+    """The adaptive Adams run in the mixed form: every plane within 1e-5 of the reference."""
+    from solprop_b200 import _lib
+
+    rec, g = record("env4_n2"), golden("env4_n2")
+    session = _lib.Workspace(_lib.Problem(rec), 0, "mixed").start(policy(g, "adaptive"))
+    zs, states = g["adaptive.z"], g["adaptive.states"]
+    seen = 1
+    while True:
+        batch = session.advance(256)
+        assert batch.event != 3
+        if batch.event in (1, 2):
+            assert rel(session.export(), states[seen]) < 1e-5
+            seen += 1
+        if batch.event == 2:
+            break
+    assert seen == len(zs)
 
 
 @pytest.mark.gpu
