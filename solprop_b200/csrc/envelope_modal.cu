@@ -15,9 +15,9 @@
 //   k_env_forward  one CTA per modal column: fft of the projected row, cropped
 //
 // Every transform is the shared-memory radix-4 FFT of fft.cuh over the table
-// exp(-2 pi i m / (2 n_to)), m < n_to.  The inverse transform and the modal field are
-// FP64 in both forms; the nodes' responses and the forward transform run in the form's
-// type R (FP32 in the mixed form, the Raman kernel's spectrum rounded to it).
+// exp(-2 pi i m / (2 n_to)), m < n_to.  The inverse transform, the modal field and the
+// Raman convolution are FP64 in both forms; the Kerr cubic and the forward transform run
+// in the form's type R (FP32 in the mixed form).
 #include "fft.cuh"
 #include "kernels.cuh"
 
@@ -75,34 +75,35 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_inverse(EnvModalArgsT<R> a)
     absorber[j] = to_c<cplx<R>>(B[bitrev((int)a.crop[j], a.log_n_to)]);
 }
 
+// The Raman convolution runs in FP64 in both forms: a molecular gas's kernel spectrum in SI
+// units (about 1e-55 at a femtosecond spacing) lies below FP32's range.
 template <class R>
 __global__ void __launch_bounds__(kEnvThreads) k_env_nodes(EnvModalArgsT<R> a) {
   using C = cplx<R>;
-  extern __shared__ __align__(16) unsigned char en_raw[];
+  extern __shared__ __align__(16) double2 en_raw[];
   const int n = a.n_to, node = blockIdx.x;
-  C* B = reinterpret_cast<C*>(en_raw);  // the drive's transform, then the convolution's
-  C* H = B + n;                          // H D
-  __shared__ C top;                      // bin n
+  double2* B = en_raw;  // the drive's transform, then the convolution's
+  double2* H = B + n;   // H D
+  __shared__ double2 top;  // bin n
   const StageScalarsDev& st = *a.stage;
   const C* E = reinterpret_cast<const C*>(a.node_field) + (size_t)node * n;
   const bool raman = a.raman_spectrum != nullptr;
   if (raman) {
     // the drive |E|^2 / 2 on [0, n), zero on [n, 2n), packed
     for (int m = threadIdx.x; m < n; m += blockDim.x) {
-      R v[2] = {R(0), R(0)};
+      double v[2] = {0.0, 0.0};
       if (2 * m < n) {
         for (int q = 0; q < 2; ++q) {
-          const C e = E[2 * m + q];
-          v[q] = R(0.5) * (e.x * e.x + e.y * e.y);
+          const double2 e = to_d2(E[2 * m + q]);
+          v[q] = 0.5 * (e.x * e.x + e.y * e.y);
         }
       }
-      B[m].x = v[0];
-      B[m].y = v[1];
+      B[m] = make_double2(v[0], v[1]);
     }
     __syncthreads();
-    fft_dif_inplace(B, a.log_n_to, a.twiddles_r, a.log_n_to + 1, /*inverse=*/false);
+    fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
     for (int k = threadIdx.x; k <= n; k += blockDim.x) {
-      const C y = cmul(to_c<C>(a.raman_spectrum[k]), unpack_real(B, a.twiddles_r, k, n, a.log_n_to));
+      const double2 y = cmul(a.raman_spectrum[k], unpack_real(B, a.twiddles, k, n, a.log_n_to));
       if (k < n) H[k] = y;
       else top = y;
     }
@@ -110,23 +111,25 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_nodes(EnvModalArgsT<R> a) {
     // irfft of length 2n: Z_k = E_k + i O_k, E_k = (Y_k + Y*_{n-k}) / 2,
     // O_k = (Y_k - Y*_{n-k}) conj(w^k) / 2; the imaginary parts of bins 0 and n dropped
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      C yk = H[k], ym = k == 0 ? top : H[n - k];
+      double2 yk = H[k], ym = k == 0 ? top : H[n - k];
       if (k == 0) {
-        yk.y = R(0);
-        ym.y = R(0);
+        yk.y = 0.0;
+        ym.y = 0.0;
       }
       ym = cconj(ym);
-      const C e = cscale(R(0.5), cadd(yk, ym));
-      const C o = cscale(R(0.5), cmul(csub(yk, ym), cconj(a.twiddles_r[k])));
+      const double2 e = cscale(0.5, cadd(yk, ym));
+      const double2 o = cscale(0.5, cmul(csub(yk, ym), cconj(a.twiddles[k])));
       B[k] = cadd(e, mul_pi(o));
     }
     __syncthreads();
-    fft_dif_inplace(B, a.log_n_to, a.twiddles_r, a.log_n_to + 1, /*inverse=*/true);
+    fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/true);
   }
-  const R factor = R(a.kerr ? a.kerr_coefficient * st.kerr_density : 0.0);
+  // the Kerr coefficient times the density (about 1e-37 in SI units for a gas) is applied in
+  // FP64 to the cubic formed in R, so that it never rounds to an FP32 subnormal
+  const double factor = a.kerr ? a.kerr_coefficient * st.kerr_density : 0.0;
   const R self = R(a.kerr_self), conj = R(a.kerr_conjugate);
-  const R raman_scale = R(kEps0 * (a.raman_mixture ? 1.0 : st.raman_density));  // a mixture's are inside
-  const R inv_n = R(1.0 / (double)n);
+  const double raman_scale = kEps0 * (a.raman_mixture ? 1.0 : st.raman_density);  // a mixture's are inside
+  const double inv_n = 1.0 / (double)n;
   C* P = reinterpret_cast<C*>(a.node_streams) + (size_t)node * n;
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
     const C e = E[t];
@@ -136,12 +139,14 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_nodes(EnvModalArgsT<R> a) {
     if (a.kerr) {
       const R mod = e.x * e.x + e.y * e.y;
       const C sq = cmul(e, e);
-      p = cscale(factor, cadd(cscale(self * mod, e), cscale(conj, cmul(sq, cconj(e)))));
+      const C cubic = cadd(cscale(self * mod, e), cscale(conj, cmul(sq, cconj(e))));
+      p.x = R(factor * (double)cubic.x);
+      p.y = R(factor * (double)cubic.y);
     }
     if (raman) {
-      const C z = B[bitrev(t >> 1, a.log_n_to)];
-      const R conv = ((t & 1) ? z.y : z.x) * inv_n;  // irfft's 1 / (2n), with the packing's 2
-      p = cadd(p, cscale(raman_scale * conv, e));
+      const double2 z = B[bitrev(t >> 1, a.log_n_to)];
+      const double conv = ((t & 1) ? z.y : z.x) * inv_n;  // irfft's 1 / (2n), with the packing's 2
+      p = cadd(p, cscale(R(raman_scale * conv), e));
     }
     P[t] = cscale(R(a.t_window[t]), p);
   }
@@ -168,7 +173,7 @@ cudaError_t configure_env_modal_kernels() {
   const void* kernels[6] = {(const void*)k_env_inverse<double>, (const void*)k_env_inverse<float>,
                             (const void*)k_env_nodes<double>,   (const void*)k_env_nodes<float>,
                             (const void*)k_env_forward<double>, (const void*)k_env_forward<float>};
-  const int shm[6] = {two, two, two, one, one, one / 2};
+  const int shm[6] = {two, two, two, two, one, one / 2};
   for (int i = 0; i < 6; ++i) {
     cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shm[i]);
     if (e != cudaSuccess) return e;
@@ -185,7 +190,7 @@ cudaError_t launch_env_inverse(const EnvModalArgsT<R>& a, cudaStream_t s) {
 
 template <class R>
 cudaError_t launch_env_nodes(const EnvModalArgsT<R>& a, int n_nodes, cudaStream_t s) {
-  k_env_nodes<R><<<n_nodes, kEnvThreads, (size_t)2 * a.n_to * sizeof(cplx<R>), s>>>(a);
+  k_env_nodes<R><<<n_nodes, kEnvThreads, (size_t)2 * a.n_to * sizeof(double2), s>>>(a);
   return cudaGetLastError();
 }
 
