@@ -72,6 +72,7 @@ typedef struct sp_raman_component {
   sp_table rates[4];
   double fraction;
   sp_table density;
+  const double* tensor_weights; /* (terms, 2): trace, traceless; two field components only */
 } sp_raman_component;
 
 /* The lowered problem (solprop_b200.record.ProblemRecord; kernel-contract.md 1-6). */
@@ -127,6 +128,9 @@ typedef struct sp_problem_desc {
   const sp_plasma_channel* extra_channels;
   int32_t n_extra_raman;
   const sp_raman_component* extra_raman;
+  /* two Cartesian field components (n_pol_transform 2, envelope grid): the Raman rows'
+   * trace and traceless weights, (raman_terms, 2) (passes/responses.py:337-392) */
+  const double* raman_tensor_weights;
 } sp_problem_desc;
 
 typedef struct sp_problem sp_problem;

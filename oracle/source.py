@@ -264,6 +264,57 @@ def mixture_raman_spectrum(rec, sc: StageScalars) -> np.ndarray:
     return np.fft.rfft(total) * rec.dt_fine
 
 
+def tensor_raman_spectrum(rec, sc: StageScalars) -> np.ndarray:
+    """``passes/responses.py:337-392``: the trace and (when any row has one) the traceless
+    kernels of two Cartesian components, every component's rows weighted, the densities
+    inside for a mixture and 1 for one component (its density multiplies outside)."""
+    n2 = rec.raman_undamped.shape[1]
+    t = np.arange(n2) * rec.dt_fine
+    parts = [(rec.raman_undamped, rec.raman_tensor_weights, sc.raman_rates, rec.raman_fraction,
+              sc.raman_density)]
+    parts += [(c.undamped, c.tensor_weights, r, c.fraction, d)
+              for c, r, d in zip(rec.extra_raman, sc.raman_rates_by_component, sc.raman_densities)]
+    n_kernels = 2 if any(np.any(w[:, 1]) for _, w, _, _, _ in parts) else 1
+    mixture = len(parts) > 1
+    total = np.zeros((n_kernels, n2))
+    for undamped, weights, rates, fraction, density in parts:
+        amplitude = np.zeros_like(total)
+        for row, w, rate in zip(undamped, weights, rates):
+            damped = row * np.exp(-rate * t)
+            for k in range(n_kernels):
+                amplitude[k] += w[k] * damped
+        total += (density if mixture else 1.0) * fraction * amplitude
+    return np.fft.rfft(total, axis=-1) * rec.dt_fine
+
+
+def vector_raman_polarisation(rec, field_t: np.ndarray, spectrum: np.ndarray, density: float) -> np.ndarray:
+    """``passes/responses.py:501-550``: the trace, difference and coherence drives of two
+    Cartesian components convolved with the trace and traceless kernels, the symmetric
+    matrix they make applied to the field (on the envelope grid, drives of ``|a|^2 / 2``)."""
+    n_to = field_t.shape[-1]
+    if rec.grid_kind != "envelope":
+        raise NotImplementedError("vector Raman on a field grid")
+    x, y = field_t[:, 0], field_t[:, 1]
+    half = 0.5
+    xx = half * (np.real(x) ** 2 + np.imag(x) ** 2)
+    yy = half * (np.real(y) ** 2 + np.imag(y) ** 2)
+    n_drives = 1 if spectrum.shape[0] == 1 else 3
+    drive = np.zeros((field_t.shape[0], n_drives, 2 * n_to))
+    drive[:, 0, :n_to] = xx + yy
+    if n_drives == 3:
+        drive[:, 1, :n_to] = xx - yy
+        drive[:, 2, :n_to] = 2 * half * (np.real(x) * np.real(y) + np.imag(x) * np.imag(y))
+    kernels = spectrum if n_drives == 1 else spectrum[[0, 1, 1]]
+    conv = np.fft.irfft(kernels * np.fft.rfft(drive, axis=-1), n=2 * n_to, axis=-1)[..., :n_to]
+    if n_drives == 1:
+        return (EPS0 * density) * field_t * conv
+    u, v, w = conv[:, 0], conv[:, 1], conv[:, 2]
+    out = np.empty_like(field_t)
+    out[:, 0] = (u + v) * field_t[:, 0] + w * field_t[:, 1]
+    out[:, 1] = w * field_t[:, 0] + (u - v) * field_t[:, 1]
+    return (EPS0 * density) * out
+
+
 def raman_polarisation(rec, field_t: np.ndarray, spectrum: np.ndarray, density: float) -> np.ndarray:
     """``passes/responses.py:395-498`` (scalar): ``eps0 rho E irfft(H rfft(D))`` doubled."""
     n_to = field_t.shape[-1]
@@ -309,7 +360,10 @@ def lab_source(rec, lab: np.ndarray, z: float, *, quiet: bool = False, out: dict
         rate, fraction, current = plasma_column(rec, field_t, sc)
     if rec.kerr_enabled:
         total = total + kerr_polarisation(rec, field_t, sc.kerr_density, rec.carrier)
-    if rec.raman_enabled:
+    if rec.raman_enabled and field_t.shape[-2] == 2:  # two Cartesian components: the tensor
+        density = 1.0 if rec.extra_raman else sc.raman_density
+        total = total + vector_raman_polarisation(rec, field_t, tensor_raman_spectrum(rec, sc), density)
+    elif rec.raman_enabled:
         if rec.extra_raman:  # a mixture: one spectrum, the densities inside it
             spectrum, density = mixture_raman_spectrum(rec, sc), 1.0
         else:

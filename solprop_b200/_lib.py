@@ -33,7 +33,7 @@ class SpPlasmaChannel(C.Structure):
 
 class SpRamanComponent(C.Structure):
     _fields_ = [("terms", C.c_int32), ("undamped", C.POINTER(C.c_double)), ("rates", SpTable * 4),
-                ("fraction", C.c_double), ("density", SpTable)]
+                ("fraction", C.c_double), ("density", SpTable), ("tensor_weights", C.POINTER(C.c_double))]
 
 
 class SpProblemDesc(C.Structure):
@@ -69,6 +69,7 @@ class SpProblemDesc(C.Structure):
         ("absorber_in_stage", C.c_int32), ("temporal_absorber_fine", C.POINTER(C.c_double)),
         ("n_extra_channels", C.c_int32), ("extra_channels", C.POINTER(SpPlasmaChannel)),
         ("n_extra_raman", C.c_int32), ("extra_raman", C.POINTER(SpRamanComponent)),
+        ("raman_tensor_weights", C.POINTER(C.c_double)),
     ]
 
 
@@ -374,6 +375,7 @@ def problem_desc(rec) -> tuple[SpProblemDesc, Marshalled]:
             d.raman_rates[i] = m.table(t)
         d.raman_fraction = rec.raman_fraction
         d.raman_density = m.table(rec.raman_density)
+        d.raman_tensor_weights = m.f64(rec.raman_tensor_weights)
     d.absorber_in_stage = int(rec.absorber_scheme == "nonlinear")
     d.temporal_absorber_fine = m.f64(rec.temporal_absorber_fine)
     if rec.extra_channels:
@@ -400,6 +402,7 @@ def problem_desc(rec) -> tuple[SpProblemDesc, Marshalled]:
                 c.rates[j] = m.table(t)
             c.fraction = comp.fraction
             c.density = m.table(comp.density)
+            c.tensor_weights = m.f64(comp.tensor_weights)
         m.keep.append(components)
         d.n_extra_raman = len(rec.extra_raman)
         d.extra_raman = C.cast(components, C.POINTER(SpRamanComponent))

@@ -192,6 +192,8 @@ struct sp_problem {
   std::vector<int> raman_first_row{0};
   std::vector<double> raman_fraction;
   std::vector<Table> raman_densities;
+  std::vector<double> raman_weights;  // two components: (rows, 2) trace and traceless weights
+  int raman_kernels = 1;              // 2 when any row has a traceless weight
   int raman_rows() const { return raman_first_row.back(); }
 };
 
@@ -212,8 +214,15 @@ static void validate(const sp_problem_desc* d) {
        "prefactor terms");
   if (d->grid_kind != 0 && d->grid_kind != 1) throw Failure(SP_ERR_ARGUMENT, "unknown grid kind");
   const bool envelope = d->grid_kind == 1;
-  if (d->n_pol * d->n_pol_transform != 1)
-    throw Failure(SP_ERR_REFUSED, "two field components (vector Kerr) are not built yet");
+  if (d->n_pol != 1 || (d->n_pol_transform != 1 && d->n_pol_transform != 2))
+    throw Failure(SP_ERR_REFUSED, "a state with two polarisation columns is not built");
+  if (d->n_pol_transform == 2 && !envelope)
+    throw Failure(SP_ERR_REFUSED, "two field components on the field grid (vector Kerr, tensor Raman) are not built");
+  if (d->n_pol_transform == 2 && d->raman_enabled) {
+    need(d->raman_tensor_weights != nullptr, "two components' Raman needs its tensor weights");
+    for (int c = 0; c < d->n_extra_raman; ++c)
+      need(d->extra_raman[c].tensor_weights != nullptr, "two components' Raman needs its tensor weights");
+  }
   if (d->n_modes * d->n_pol > kMaxGemmModes)
     throw Failure(SP_ERR_REFUSED, "more than 1024 modal columns");
   if (envelope) {
@@ -285,7 +294,7 @@ struct sp_workspace {
   DevBuf<unsigned> arrivals;
   DevBuf<unsigned long long> ticket;  // the response column's tile counter
   DevBuf<double2> env_twiddles;       // envelope route: exp(-2 pi i m / (2 n_to)), m < n_to
-  DevBuf<double> raman_undamped;
+  DevBuf<double> raman_undamped, raman_weights;
   DevBuf<double> stat_power, stat_out, stat_weight;  // plane statistics, on first use
   DevBuf<double2> raman_spectrum;  // field-grid Raman: the damped kernel's spectrum (n_to + 1)
   DevBuf<ChannelTableT<double>> channels;  // a mixture's plasma channels (rate_coeff holds their tables)
@@ -572,6 +581,8 @@ static RamanArgs raman_args(const sp_workspace* ws, int slot) {
   for (int c = 0; c <= ra.n_components; ++c) ra.first_row[c] = ws->P->raman_first_row[c];
   for (int c = 0; c < ra.n_components; ++c) ra.fraction[c] = ws->P->raman_fraction[c];
   ra.dt = d.dt_fine;
+  ra.tensor_weights = ws->P->raman_weights.empty() ? nullptr : ws->raman_weights.p;
+  ra.n_kernels = ws->P->raman_kernels;
   return ra;
 }
 
@@ -663,6 +674,8 @@ static EnvModalArgsT<R> env_modal_args(const sp_workspace* ws, const double2* la
   ea.kerr_coefficient = d.kerr_coefficient;
   ea.kerr_self = d.kerr_self;
   ea.kerr_conjugate = d.kerr_conjugate;
+  ea.n_components = d.n_pol_transform;
+  ea.raman_kernels = P.raman_kernels;
   if constexpr (sizeof(R) == 8) {
     ea.twiddles_r = ws->env_twiddles.p;
     ea.node_field = ws->node_field.p;
@@ -685,6 +698,7 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
   const double* taper = &(ws->stage.p + slot)->taper;
   double* status = ws->norms.p + kColumnStatus;
   const int n2 = 2 * d.n_to;
+  const int rows = d.n_nodes * d.n_pol_transform;  // two components: rows x, y per node
   const size_t stride = (size_t)P.n_cols * n2;
   if (ws->precision == SP_PRECISION_MIXED) {
     const auto ea = env_modal_args<float>(ws, lab, slot, absorber);
@@ -692,7 +706,7 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
     {
       KernelTimer t(ws, SP_K_PROJECT);
       CUDA_CHECK(modal_synthesis_split3(ws->s_parts.p, ws->modal_t.p, ws->modal_parts.p, ws->f32.node_field.p,
-                                        d.n_nodes, d.n_modes, n2, ws->kpad_modes, taper, status, ws->stream));
+                                        rows, d.n_modes, n2, ws->kpad_modes, taper, status, ws->stream));
     }
     {
       KernelTimer t(ws, SP_K_COLUMN);
@@ -702,7 +716,7 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
     {
       KernelTimer t(ws, SP_K_PROJECT);
       CUDA_CHECK(modal_projection_split3(ws->w_parts.p, ws->f32.node_streams.p, ws->node_parts.p, ws->f32.proj.p,
-                                         1, d.n_modes, d.n_nodes, n2, ws->kpad_nodes, stride, taper, status,
+                                         1, d.n_modes, rows, n2, ws->kpad_nodes, stride, taper, status,
                                          reinterpret_cast<float*>(ws->proj_scratch.p), ws->stream));
     }
     { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_env_forward(ea, ws->stream)); }
@@ -712,7 +726,7 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
   { KernelTimer t(ws, SP_K_INVERSE); CUDA_CHECK(launch_env_inverse(ea, ws->stream)); }
   {
     KernelTimer t(ws, SP_K_PROJECT);
-    CUDA_CHECK(modal_synthesis_f64(ws->synthesis.p, ws->modal_t.p, ws->node_field.p, d.n_nodes, d.n_modes, n2,
+    CUDA_CHECK(modal_synthesis_f64(ws->synthesis.p, ws->modal_t.p, ws->node_field.p, rows, d.n_modes, n2,
                                    taper, ws->stream));
   }
   {
@@ -722,7 +736,7 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
   }
   {
     KernelTimer t(ws, SP_K_PROJECT);
-    CUDA_CHECK(modal_projection_f64(ws->projection.p, ws->node_streams.p, ws->proj.p, 1, d.n_modes, d.n_nodes,
+    CUDA_CHECK(modal_projection_f64(ws->projection.p, ws->node_streams.p, ws->proj.p, 1, d.n_modes, rows,
                                     n2, stride, taper, ws->proj_scratch.p, ws->stream));
   }
   { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_env_forward(ea, ws->stream)); }
@@ -935,19 +949,20 @@ static void build_workspace(sp_workspace* ws) {
   ws->proj.alloc((ws->gemm ? 1 : n_groups) * 3 * P.n_cols * d.n_to);
   ws->proj.zero(s);
   if (ws->gemm) {
-    const size_t field = cplx_rows * d.n_nodes * d.n_to;
+    const int node_rows = d.n_nodes * d.n_pol_transform;  // two components: rows x, y per node
+    const size_t field = cplx_rows * node_rows * d.n_to;
     ws->kpad_modes = modal_kpad(d.n_modes);
-    ws->kpad_nodes = modal_kpad(d.n_nodes);
-    ws->proj_scratch.alloc(modal_projection_scratch(d.n_modes, d.n_nodes, (int)cplx_rows * d.n_to));
+    ws->kpad_nodes = modal_kpad(node_rows);
+    ws->proj_scratch.alloc(modal_projection_scratch(d.n_modes, node_rows, (int)cplx_rows * d.n_to));
     if (ws->precision == SP_PRECISION_MIXED) {
       ws->f32.node_field.alloc(field);
       ws->f32.node_streams.alloc(3 * field);
       ws->f32.node_streams.zero(s);
       std::vector<uint16_t> parts;
-      split3_host(P.synthesis.data(), d.n_nodes, d.n_modes, ws->kpad_modes, parts);
+      split3_host(P.synthesis.data(), node_rows, d.n_modes, ws->kpad_modes, parts);
       ws->s_parts.upload(parts.data(), parts.size(), s);
       CUDA_CHECK(cudaStreamSynchronize(s));  // the host copy goes with this scope
-      split3_host(P.projection.data(), d.n_modes, d.n_nodes, ws->kpad_nodes, parts);
+      split3_host(P.projection.data(), d.n_modes, node_rows, ws->kpad_nodes, parts);
       ws->w_parts.upload(parts.data(), parts.size(), s);
       CUDA_CHECK(cudaStreamSynchronize(s));
       ws->modal_parts.alloc((size_t)3 * cplx_rows * d.n_to * ws->kpad_modes);
@@ -995,7 +1010,9 @@ static void build_workspace(sp_workspace* ws) {
       CUDA_CHECK(cudaStreamSynchronize(s));  // the host copy goes with this scope
     }
     if (d.raman_enabled) ws->raman_undamped.upload(P.raman_undamped.data(), P.raman_undamped.size(), s);
-    if (d.raman_enabled && (d.grid_kind == 0 || ws->gemm)) ws->raman_spectrum.alloc((size_t)d.n_to + 1);
+    if (!P.raman_weights.empty()) ws->raman_weights.upload(P.raman_weights.data(), P.raman_weights.size(), s);
+    if (d.raman_enabled && (d.grid_kind == 0 || ws->gemm))
+      ws->raman_spectrum.alloc((size_t)P.raman_kernels * (d.n_to + 1));
     CUDA_CHECK(cudaStreamSynchronize(s));
   }
   CUDA_CHECK(cudaStreamSynchronize(s));
@@ -1639,6 +1656,8 @@ sp_status sp_problem_create(const sp_problem_desc* d, sp_problem** out) {
       P->raman_first_row.push_back(d->raman_terms);
       P->raman_fraction.push_back(d->raman_fraction);
       P->raman_densities.push_back(P->raman_density);
+      if (d->n_pol_transform == 2)
+        P->raman_weights.assign(d->raman_tensor_weights, d->raman_tensor_weights + (size_t)2 * d->raman_terms);
       for (int c = 0; c < d->n_extra_raman; ++c) {  // a mixture's further components
         const sp_raman_component& rc = d->extra_raman[c];
         const int r0 = P->raman_rows();
@@ -1649,7 +1668,11 @@ sp_status sp_problem_create(const sp_problem_desc* d, sp_problem** out) {
         P->raman_fraction.push_back(rc.fraction);
         P->raman_densities.emplace_back();
         P->raman_densities.back().load(rc.density);
+        if (d->n_pol_transform == 2)
+          P->raman_weights.insert(P->raman_weights.end(), rc.tensor_weights, rc.tensor_weights + (size_t)2 * rc.terms);
       }
+      for (size_t r = 1; r < P->raman_weights.size(); r += 2)
+        if (P->raman_weights[r] != 0.0) P->raman_kernels = 2;
     }
     if (d->n_extra_channels) {  // a mixture: every channel, the descriptor's first
       auto add = [&](double qm, double ip, const double* coeff, int n, double lmin, double dl, double fmin,
@@ -1671,6 +1694,7 @@ sp_status sp_problem_create(const sp_problem_desc* d, sp_problem** out) {
     }
     P->d.extra_channels = nullptr;  // copied above: nothing keeps the caller's arrays
     P->d.extra_raman = nullptr;
+    P->d.raman_tensor_weights = nullptr;
     if (d->phi_expansion && (!P->phi_weights.present() || !P->phi_rate.present()))
       throw Failure(SP_ERR_ARGUMENT, "an expansion of Phi needs its weight and rate tables");
     *out = P.release();
@@ -1702,8 +1726,8 @@ sp_status sp_workspace_create_ex2(const sp_problem* problem, int device, int pre
     const sp_problem_desc& d = problem->d;
     const bool field_raman = d.grid_kind == 0 && d.raman_enabled;
     // the envelope grid's single CTA takes one column on one node without the absorber
-    const bool env_products = d.grid_kind == 1 && (problem->n_cols > 1 || d.n_nodes > 1 || d.absorber_in_stage ||
-                                                   precision == SP_PRECISION_MIXED);
+    const bool env_products = d.grid_kind == 1 && (problem->n_cols > 1 || d.n_nodes > 1 || d.n_pol_transform > 1 ||
+                                                   d.absorber_in_stage || precision == SP_PRECISION_MIXED);
     const bool gemm = modal == SP_MODAL_GEMM ||
                       (modal == SP_MODAL_AUTO && (problem->n_cols > kMaxModes || field_raman || env_products));
     if (!gemm && precision == SP_PRECISION_MIXED && d.grid_kind == 1)

@@ -76,34 +76,50 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_inverse(EnvModalArgsT<R> a)
 }
 
 // The Raman convolution runs in FP64 in both forms: a molecular gas's kernel spectrum in SI
-// units (about 1e-55 at a femtosecond spacing) lies below FP32's range.
+// units (about 1e-55 at a femtosecond spacing) lies below FP32's range.  With two field
+// components (rows x, y of the node) the Kerr cubic sums over them and the Raman response
+// is the tensor one (passes/responses.py:501-550): the trace drive |a_x|^2/2 + |a_y|^2/2 and,
+// with a traceless kernel, the difference and coherence drives, three convolutions u, v, w
+// whose symmetric matrix [[u + v, w], [w, u - v]] multiplies the field.
 template <class R>
 __global__ void __launch_bounds__(kEnvThreads) k_env_nodes(EnvModalArgsT<R> a) {
   using C = cplx<R>;
   extern __shared__ __align__(16) double2 en_raw[];
-  const int n = a.n_to, node = blockIdx.x;
-  double2* B = en_raw;  // the drive's transform, then the convolution's
+  const int n = a.n_to, node = blockIdx.x, nc = a.n_components;
+  double2* B = en_raw;  // a drive's transform, then its convolution's
   double2* H = B + n;   // H D
+  double* U = reinterpret_cast<double*>(H + n);  // three drives: the trace and difference convolutions
+  double* V = U + n;
   __shared__ double2 top;  // bin n
   const StageScalarsDev& st = *a.stage;
-  const C* E = reinterpret_cast<const C*>(a.node_field) + (size_t)node * n;
+  const C* Ex = reinterpret_cast<const C*>(a.node_field) + (size_t)node * nc * n;
+  const C* Ey = Ex + (nc == 2 ? n : 0);
   const bool raman = a.raman_spectrum != nullptr;
-  if (raman) {
-    // the drive |E|^2 / 2 on [0, n), zero on [n, 2n), packed
+  const int drives = !raman ? 0 : (nc == 2 && a.raman_kernels == 2 ? 3 : 1);
+  for (int dr = 0; dr < drives; ++dr) {
+    // the drive on [0, n), zero on [n, 2n), packed
     for (int m = threadIdx.x; m < n; m += blockDim.x) {
       double v[2] = {0.0, 0.0};
       if (2 * m < n) {
         for (int q = 0; q < 2; ++q) {
-          const double2 e = to_d2(E[2 * m + q]);
-          v[q] = 0.5 * (e.x * e.x + e.y * e.y);
+          const double2 x = to_d2(Ex[2 * m + q]);
+          const double xx = 0.5 * (x.x * x.x + x.y * x.y);
+          if (nc == 1) {
+            v[q] = xx;
+          } else {
+            const double2 y = to_d2(Ey[2 * m + q]);
+            const double yy = 0.5 * (y.x * y.x + y.y * y.y);
+            v[q] = dr == 0 ? xx + yy : dr == 1 ? xx - yy : 2.0 * 0.5 * (x.x * y.x + x.y * y.y);
+          }
         }
       }
       B[m] = make_double2(v[0], v[1]);
     }
     __syncthreads();
     fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
+    const double2* kernel = a.raman_spectrum + (dr == 0 ? 0 : (size_t)(n + 1));  // trace, then traceless
     for (int k = threadIdx.x; k <= n; k += blockDim.x) {
-      const double2 y = cmul(a.raman_spectrum[k], unpack_real(B, a.twiddles, k, n, a.log_n_to));
+      const double2 y = cmul(kernel[k], unpack_real(B, a.twiddles, k, n, a.log_n_to));
       if (k < n) H[k] = y;
       else top = y;
     }
@@ -123,6 +139,15 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_nodes(EnvModalArgsT<R> a) {
     }
     __syncthreads();
     fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/true);
+    if (dr + 1 < drives) {  // keep u and v in natural order; the last one stays in B
+      double* keep = dr == 0 ? U : V;
+      const double inv = 1.0 / (double)n;
+      for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        const double2 z = B[bitrev(t >> 1, a.log_n_to)];
+        keep[t] = ((t & 1) ? z.y : z.x) * inv;
+      }
+      __syncthreads();
+    }
   }
   // the Kerr coefficient times the density (about 1e-37 in SI units for a gas) is applied in
   // FP64 to the cubic formed in R, so that it never rounds to an FP32 subnormal
@@ -130,25 +155,41 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_nodes(EnvModalArgsT<R> a) {
   const R self = R(a.kerr_self), conj = R(a.kerr_conjugate);
   const double raman_scale = kEps0 * (a.raman_mixture ? 1.0 : st.raman_density);  // a mixture's are inside
   const double inv_n = 1.0 / (double)n;
-  C* P = reinterpret_cast<C*>(a.node_streams) + (size_t)node * n;
+  C* Px = reinterpret_cast<C*>(a.node_streams) + (size_t)node * nc * n;
+  C* Py = Px + (nc == 2 ? n : 0);
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
-    const C e = E[t];
-    C p;
-    p.x = R(0);
-    p.y = R(0);
-    if (a.kerr) {
-      const R mod = e.x * e.x + e.y * e.y;
-      const C sq = cmul(e, e);
-      const C cubic = cadd(cscale(self * mod, e), cscale(conj, cmul(sq, cconj(e))));
-      p.x = R(factor * (double)cubic.x);
-      p.y = R(factor * (double)cubic.y);
+    const C x = Ex[t], y = Ey[t];
+    double2 px = make_double2(0.0, 0.0), py = px;
+    if (a.kerr) {  // c rho (s (sum |a|^2) a_p + q (sum a^2) a_p*), summed over the components
+      R mod = x.x * x.x + x.y * x.y;
+      C sq = cmul(x, x);
+      if (nc == 2) {
+        mod += y.x * y.x + y.y * y.y;
+        sq = cadd(sq, cmul(y, y));
+      }
+      const C cx = cadd(cscale(self * mod, x), cscale(conj, cmul(sq, cconj(x))));
+      px = make_double2(factor * (double)cx.x, factor * (double)cx.y);
+      if (nc == 2) {
+        const C cy = cadd(cscale(self * mod, y), cscale(conj, cmul(sq, cconj(y))));
+        py = make_double2(factor * (double)cy.x, factor * (double)cy.y);
+      }
     }
-    if (raman) {
+    if (drives > 0) {
       const double2 z = B[bitrev(t >> 1, a.log_n_to)];
-      const double conv = ((t & 1) ? z.y : z.x) * inv_n;  // irfft's 1 / (2n), with the packing's 2
-      p = cadd(p, cscale(R(raman_scale * conv), e));
+      const double last = ((t & 1) ? z.y : z.x) * inv_n;  // irfft's 1 / (2n), with the packing's 2
+      const double2 dx = to_d2(x), dy = to_d2(y);
+      if (drives == 1) {
+        px = cadd(px, cscale(raman_scale * last, dx));
+        if (nc == 2) py = cadd(py, cscale(raman_scale * last, dy));
+      } else {
+        const double u = U[t], v = V[t], w = last;
+        px = cadd(px, cscale(raman_scale, cadd(cscale(u + v, dx), cscale(w, dy))));
+        py = cadd(py, cscale(raman_scale, cadd(cscale(w, dx), cscale(u - v, dy))));
+      }
     }
-    P[t] = cscale(R(a.t_window[t]), p);
+    const double g = a.t_window[t];
+    Px[t] = to_c<C>(cscale(g, px));
+    if (nc == 2) Py[t] = to_c<C>(cscale(g, py));
   }
 }
 
@@ -173,7 +214,8 @@ cudaError_t configure_env_modal_kernels() {
   const void* kernels[6] = {(const void*)k_env_inverse<double>, (const void*)k_env_inverse<float>,
                             (const void*)k_env_nodes<double>,   (const void*)k_env_nodes<float>,
                             (const void*)k_env_forward<double>, (const void*)k_env_forward<float>};
-  const int shm[6] = {two, two, two, two, one, one / 2};
+  const int nodes = (int)(kMaxEnvelopeSamples * (2 * sizeof(double2) + 2 * sizeof(double)));
+  const int shm[6] = {two, two, nodes, nodes, one, one / 2};
   for (int i = 0; i < 6; ++i) {
     cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shm[i]);
     if (e != cudaSuccess) return e;
@@ -190,7 +232,9 @@ cudaError_t launch_env_inverse(const EnvModalArgsT<R>& a, cudaStream_t s) {
 
 template <class R>
 cudaError_t launch_env_nodes(const EnvModalArgsT<R>& a, int n_nodes, cudaStream_t s) {
-  k_env_nodes<R><<<n_nodes, kEnvThreads, (size_t)2 * a.n_to * sizeof(double2), s>>>(a);
+  const bool three = a.n_components == 2 && a.raman_kernels == 2 && a.raman_spectrum;  // u, v kept
+  const size_t bytes = (size_t)a.n_to * (2 * sizeof(double2) + (three ? 2 * sizeof(double) : 0));
+  k_env_nodes<R><<<n_nodes, kEnvThreads, bytes, s>>>(a);
   return cudaGetLastError();
 }
 

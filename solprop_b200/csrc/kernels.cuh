@@ -219,6 +219,10 @@ struct RamanArgs {
   int first_row[kMaxRamanComponents + 1];  // component c: rows [first_row[c], first_row[c + 1])
   double fraction[kMaxRamanComponents];
   double dt;
+  // two field components: each row's trace and traceless weights (rows, 2), and the
+  // kernels formed (1: the trace; 2: trace and traceless, spectra (2, n_to + 1)); null: scalar
+  const double* tensor_weights;
+  int n_kernels;
 };
 cudaError_t configure_raman_kernels();
 cudaError_t launch_raman_spectrum(const RamanArgs& a, cudaStream_t s);  // the kernel's spectrum alone
@@ -242,8 +246,10 @@ struct EnvModalArgsT {
   R* node_streams;                // (n_nodes, 2 n_to): the gated polarisation
   const R* projected;             // (n_cols, 2 n_to): sum W P / tau
   cplx<R>* spectra;               // (4, n_cols, n_omega): P, -, -, absorber
-  const double2* raman_spectrum;  // (n_to + 1), or null without Raman
+  const double2* raman_spectrum;  // (raman_kernels, n_to + 1), or null without Raman
   int n_cols, n_omega, n_to, log_n_to, kerr, raman_mixture;
+  int n_components;               // field components per node (1, or 2: rows x, y)
+  int raman_kernels;              // two components: 1 (trace) or 2 (trace, traceless)
   double kerr_coefficient, kerr_self, kerr_conjugate;
 };
 cudaError_t configure_env_modal_kernels();

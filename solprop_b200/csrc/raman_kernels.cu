@@ -35,11 +35,13 @@ __device__ __forceinline__ double2 unpack(const double2* Z, const double2* tw, i
   return cadd(e, cmul(w, o));
 }
 
+// one CTA per kernel: blockIdx.x 0 the trace (or the scalar kernel), 1 the traceless
 __global__ void __launch_bounds__(kRamanThreads) k_raman_kernel(RamanArgs a) {
   extern __shared__ __align__(16) double2 rk_raw[];
-  const int n = a.n_to;
+  const int n = a.n_to, kernel = blockIdx.x;
   double2* B = rk_raw;
   const StageScalarsDev& st = *a.stage;
+  const double* weights = a.tensor_weights;  // (rows, 2), or null for one component
   // one component: f_R sum_r u_r(s) e^(-g_r s dt); a mixture (passes/responses.py:293-334):
   // sum_c rho_c f_c sum_r u_r(s) e^(-g_r s dt), rows in component order
   const bool mixture = a.n_components > 1;
@@ -51,8 +53,10 @@ __global__ void __launch_bounds__(kRamanThreads) k_raman_kernel(RamanArgs a) {
       double total = 0.0;
       for (int c = 0; c < a.n_components; ++c) {
         double k = 0.0;
-        for (int r = a.first_row[c]; r < a.first_row[c + 1]; ++r)
-          k += a.undamped[(size_t)r * 2 * n + s] * exp(-st.raman_rates[r] * delay);
+        for (int r = a.first_row[c]; r < a.first_row[c + 1]; ++r) {
+          const double damped = a.undamped[(size_t)r * 2 * n + s] * exp(-st.raman_rates[r] * delay);
+          k += weights ? weights[2 * r + kernel] * damped : damped;
+        }
         total += mixture ? st.raman_densities[c] * a.fraction[c] * k : a.fraction[c] * k;
       }
       v[q] = total;
@@ -61,7 +65,8 @@ __global__ void __launch_bounds__(kRamanThreads) k_raman_kernel(RamanArgs a) {
   }
   __syncthreads();
   fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
-  for (int k = threadIdx.x; k <= n; k += blockDim.x) a.spectrum[k] = cscale(a.dt, unpack(B, a.twiddles, k, n, a.log_n_to));
+  double2* spectrum = a.spectrum + (size_t)kernel * (n + 1);
+  for (int k = threadIdx.x; k <= n; k += blockDim.x) spectrum[k] = cscale(a.dt, unpack(B, a.twiddles, k, n, a.log_n_to));
 }
 
 template <class R>
@@ -135,7 +140,7 @@ cudaError_t configure_raman_kernels() {
 }
 
 cudaError_t launch_raman_spectrum(const RamanArgs& a, cudaStream_t s) {
-  k_raman_kernel<<<1, kRamanThreads, raman_smem(a.n_to) / 2, s>>>(a);
+  k_raman_kernel<<<a.tensor_weights ? a.n_kernels : 1, kRamanThreads, raman_smem(a.n_to) / 2, s>>>(a);
   return cudaGetLastError();
 }
 

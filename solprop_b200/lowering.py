@@ -189,8 +189,12 @@ def lower(problem) -> ProblemRecord:
         record.raman_fraction = float(term.fraction)
         record.raman_thg = bool(term.thg)
         record.raman_density = _table(term.density) if term.density is not None else None
-        if n_pol * transform._n_pol != 1:
-            raise BackendRefusal("vector Raman (two components) is not executed yet")
+        if n_pol != 1:
+            raise BackendRefusal("a state with two polarisation columns is not executed")
+        if transform._n_pol == 2:  # two Cartesian components: the tensor response
+            if not all(t.tensor_capable for t in responses.raman_terms):
+                raise BackendRefusal("vector Raman needs tensor-capable Raman components")
+            record.raman_tensor_weights = np.ascontiguousarray(term.tensor_weights, dtype=np.float64)
         for term in responses.raman_terms:
             if len(term.decay_rates) > 4:
                 raise BackendRefusal("a Raman component with more than four damped rows")
@@ -202,6 +206,8 @@ def lower(problem) -> ProblemRecord:
                 rates=[_table(t) for t in term.decay_rates],
                 fraction=float(term.fraction),
                 density=_table(term.density) if term.density is not None else None,
+                tensor_weights=(np.ascontiguousarray(term.tensor_weights, dtype=np.float64)
+                                if transform._n_pol == 2 else None),
             ))
     for channel in responses.plasma_channels[1:]:
         table = channel.rate

@@ -136,6 +136,7 @@ class RamanComponentRecord:
     rates: list[PiecewiseTable]
     fraction: float = 1.0
     density: PiecewiseTable | None = None
+    tensor_weights: np.ndarray | None = None  # (n_terms, 2), two components only
 
 
 @dataclass
@@ -216,6 +217,7 @@ class ProblemRecord:
     raman_fraction: float = 1.0
     raman_thg: bool = False
     raman_density: PiecewiseTable | None = None
+    raman_tensor_weights: np.ndarray | None = None  # (n_terms, 2): trace, traceless (two components)
     # ---- a gas mixture: the plasma channels and Raman components after the first
     extra_channels: list[PlasmaChannelRecord] = field(default_factory=list)
     extra_raman: list[RamanComponentRecord] = field(default_factory=list)
@@ -326,6 +328,8 @@ def save_record(record: ProblemRecord, path) -> None:
             scalars = []
             for i, comp in enumerate(value):
                 arrays[f"extra_raman.{i}.undamped"] = comp.undamped
+                if comp.tensor_weights is not None:
+                    arrays[f"extra_raman.{i}.tensor_weights"] = comp.tensor_weights
                 for j, table in enumerate(comp.rates):
                     _table_arrays(f"extra_raman.{i}.rates.{j}", table, arrays)
                 _table_arrays(f"extra_raman.{i}.density", comp.density, arrays)
@@ -378,6 +382,8 @@ def load_record(path) -> ProblemRecord:
             rates=[_read_table(data, names, f"extra_raman.{i}.rates.{j}") for j in range(c["n_rates"])],
             fraction=float(c["fraction"]),
             density=_read_table(data, names, f"extra_raman.{i}.density"),
+            tensor_weights=(np.array(data[f"extra_raman.{i}.tensor_weights"])
+                            if f"extra_raman.{i}.tensor_weights" in names else None),
         )
         for i, c in enumerate(components)
     ]

@@ -10,7 +10,7 @@ import numpy as np
 from solprop_b200.record import load_record
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-CASES = ("cap1_ar", "cap4_he", "gnlse_raman", "raman_n2", "mix_hear", "raman_mix", "env4_n2", "env3_rk")
+CASES = ("cap1_ar", "cap4_he", "gnlse_raman", "raman_n2", "mix_hear", "raman_mix", "env4_n2", "env3_rk", "envv_n2")
 
 
 def rel(a, b) -> float:

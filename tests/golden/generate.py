@@ -528,6 +528,18 @@ def raman_mixture_case(case, *, seed):
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
 
 
+def vector_envelope_case(case, *, seed):
+    """A nitrogen-filled capillary on the envelope grid with two Cartesian field components:
+    HE11 polarised along x and along y, and HE12 -- the reference's vector route, with the
+    analytic Kerr cubic summed over the components and nitrogen's tensor Raman response
+    (the trace and traceless kernels, three drives per node)."""
+    from solprop.modes import MarcatiliMode
+
+    he11 = MarcatiliMode(100e-6, kind="HE", n=1, m=1, cladding=1.45 + 0j)
+    modes = [he11, he11.orthogonal_polarisation, MarcatiliMode(100e-6, kind="HE", n=1, m=2, cladding=1.45 + 0j)]
+    envelope_modal_case(case, seed=seed, modes=modes)
+
+
 def envelope_modal_case(case, *, seed, modes, integrator=None):
     """A nitrogen-filled capillary on the envelope grid: several modes on the radial rule's
     nodes, the analytic Kerr cubic, the gas's rotational and vibrational Raman response
@@ -558,7 +570,7 @@ def envelope_modal_case(case, *, seed, modes, integrator=None):
 
     sim = build(n_save=3)
     problem = sim.translate()
-    assert problem.grid_kind == "envelope" and problem.shape[0] == modes
+    assert problem.grid_kind == "envelope" and problem.shape[0] == (modes if np.isscalar(modes) else len(modes))
     print(f"{case}: n_to {problem.grids.n_to}, nodes {problem.transform.synthesis.shape[0]}", flush=True)
     golden = source_fixture(sim, problem, [0.0, 0.37 * length], seed)
     _, zs, states, (hist, counts), wall = drive(build(n_save=3))
@@ -726,6 +738,8 @@ if __name__ == "__main__":
         raman_mixture_case("raman_mix", seed=10)
     if not only or "env4_n2" in only:
         envelope_modal_case("env4_n2", seed=11, modes=4)
+    if not only or "envv_n2" in only:
+        vector_envelope_case("envv_n2", seed=13)
     if not only or "env3_rk" in only:
         envelope_modal_case("env3_rk", seed=12, modes=3, integrator=RungeKutta())
     if not only or "radial_ar" in only:

@@ -3,7 +3,9 @@
 ``env4_n2`` and ``env3_rk`` are nitrogen-filled capillaries on the envelope grid: four and
 three modes on 33 radial nodes, n_to 1024, the analytic Kerr cubic, the gas's Raman
 response (drive |A|^2 / 2) and the in-stage collar -- the multimode generalised NLSE,
-stepped by exponential Adams and by DOPRI5.  A workspace takes the modal transform's
+stepped by exponential Adams and by DOPRI5.  ``envv_n2`` has two Cartesian field
+components (HE11 along x and along y, HE12): the Kerr cubic summed over the components and
+nitrogen's tensor Raman response (trace and traceless kernels, three drives per node).  A workspace takes the modal transform's
 products for them by itself (complex rows interleaved, N = 2 n_to); the single-CTA
 envelope kernel, which holds one column on one node, refuses them by name.
 """
@@ -14,6 +16,17 @@ from tests._cases import fixed_schedule, golden, policy, record, rel
 
 SOURCE_TOL = 1e-10  # the plain form, as every source test
 MIXED_TOL = 2e-6  # the mixed form's source tolerance (tests/test_mixed.py)
+
+
+def test_two_components_are_taken_on_the_envelope_grid_only():
+    from solprop_b200 import _lib
+
+    rec = record("envv_n2")
+    assert rec.n_pol_transform == 2 and rec.raman_tensor_weights.shape == (2, 2)
+    _lib.Problem(rec).close()
+    rec.grid_kind = "field"
+    with pytest.raises(_lib.BackendRefusal, match="two field components on the field grid"):
+        _lib.Problem(rec)
 
 
 def test_many_modes_are_refused_by_the_single_cta_form():
@@ -28,7 +41,7 @@ def test_many_modes_are_refused_by_the_single_cta_form():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["env4_n2", "env3_rk"])
+@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "envv_n2"])
 @pytest.mark.parametrize("index", [0, 1])
 def test_source_matches_the_reference(case, index):
     from solprop_b200 import _lib
@@ -40,7 +53,7 @@ def test_source_matches_the_reference(case, index):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "gnlse_raman"])
+@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "envv_n2", "gnlse_raman"])
 def test_split_bf16_products_match_the_reference_to_fp32(case):
     """The mixed form: tcgen05 products of three-part BF16 splits, FP32 responses."""
     from solprop_b200 import _lib
@@ -86,7 +99,7 @@ def test_the_single_mode_envelope_gives_the_same_source_on_either_form():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["env4_n2", "env3_rk"])
+@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "envv_n2"])
 def test_envelope_runs_step_with_the_reference(case):
     """A fixed schedule plane by plane at 1e-10, and the adaptive run within its rtol with
     the reference's attempt count (to +-3)."""
