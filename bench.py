@@ -297,6 +297,57 @@ def modal_products_leg(device: int, repeats: int = 3, n_nodes: int = 16384) -> d
     return out
 
 
+def config3_leg(device: int, attempts: int = 3, grid: int = 128) -> dict:
+    """Config 3's route at its mode and node counts: 30 vector graded-index modes on
+    ``grid x grid`` Cartesian nodes (two field components per node), the envelope grid
+    (4 096 samples: the route's row limit; config 3 asks for 2^14), the analytic Kerr cubic
+    and the tensor Raman response, DOPRI5 -- ``solprop_b200.grin``'s seeded synthetic
+    workload.  Per precision: DOPRI5 attempts per second and, per source evaluation, the
+    device time of its kernel families (session timing, CUDA events); the products' roofline
+    in HBM bytes -- the node field written and the node stream read, N_rows x 2 n_to
+    elements each -- since with K = 30 modes the products are bound by those bytes, not by
+    the tensor pipe."""
+    from solprop_b200 import _lib, grin
+
+    rec, pol = grin.grin_record(n_to=4096, grid=grid)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    rows = rec.n_nodes * rec.n_pol_transform
+    problem = _lib.Problem(rec)
+    out = {"workload": f"config 3 (synthetic graded-index fibre): {rec.n_modes} vector modes on {grid}x{grid} "
+                       f"nodes x 2 components, envelope n_to {rec.n_to}, Kerr + tensor Raman, DOPRI5",
+           "modes": rec.n_modes, "nodes": rec.n_nodes, "n_to": rec.n_to}
+    for precision in ("mixed", "fp64"):
+        ws = _lib.Workspace(problem, device, precision)
+        session = ws.start(pol)
+        session.advance(1)  # warm-up: the first attempt
+        session.set_timing(True)
+        session.timing(reset=True)
+        t0 = time.perf_counter()
+        batch = session.advance(attempts)
+        wall = time.perf_counter() - t0
+        fams = session.timing(reset=True)
+        session.set_timing(False)
+        done = int(batch.attempts) - 1
+        evaluations = max(fams.get("response_column", (0.0, 1))[1], 1)
+        elem = 4 if precision == "mixed" else 8
+        algorithmic = 2.0 * rows * 2 * rec.n_to * elem
+        prod_ms = fams["project"][0] / evaluations
+        out[precision] = {
+            "attempts": done, "attempts_per_s": done / wall,
+            "evaluation_ms": sum(v[0] for v in fams.values()) / evaluations,
+            "families_ms_per_evaluation": {k: v[0] / evaluations for k, v in fams.items()},
+            "products_ms": prod_ms, "products_gbs": algorithmic / (prod_ms * 1e-3) / 1e9,
+            "products_frac_of_hbm": algorithmic / (prod_ms * 1e-3) / 1e9 / hbm}
+        session.close()
+        ws.close()
+    out["roofline"] = {"bound": "hbm", "kernel": "modal products (tcgen05, split BF16)",
+                       "achieved": out["mixed"]["products_gbs"], "peak": hbm, "unit": "GB/s",
+                       "frac": out["mixed"]["products_frac_of_hbm"],
+                       "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    return out
+
+
 def scan_leg(device: int, n_runs: int, steps: int, warmup: int, seed: int = 2024,
              rank: int = 0, world: int = 1) -> dict:
     """The parameter-scan workload (config 4): n_runs seeded uneven capillary runs, stepped together.
@@ -533,6 +584,9 @@ def main() -> int:
                              "steps after --warmup), e.g. under ncu; prints its JSON")
     parser.add_argument("--surrogate-only", type=int, default=0, metavar="POINTS",
                         help="only the surrogate's tcgen05 inference over POINTS points; prints its JSON")
+    parser.add_argument("--config3-only", type=int, nargs="?", const=128, default=0, metavar="GRID",
+                        help="only config 3's route (30 vector modes on GRID x GRID nodes, default 128); "
+                             "prints its JSON")
     parser.add_argument("--modal-only", type=int, nargs="?", const=16384, default=0, metavar="NODES",
                         help="only the modal transform's products (30 modes, NODES nodes, default 16384: "
                              "config 3's size); prints its JSON")
@@ -541,12 +595,14 @@ def main() -> int:
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.scan_only or args.surrogate_only or args.modal_only:
+    if args.scan_only or args.surrogate_only or args.modal_only or args.config3_only:
         import torch
 
         torch.cuda.set_device(local)
         if args.scan_only:
             result = scan_leg(local, args.scan_only, args.scan_steps, warmup=args.warmup)
+        elif args.config3_only:
+            result = config3_leg(local, grid=args.config3_only)
         elif args.modal_only:
             result = modal_products_leg(local, n_nodes=args.modal_only)
         else:
@@ -678,6 +734,7 @@ def main() -> int:
     runs_result = None if args.config2_only else runs_leg(local)
     surrogate_result = None if args.config2_only else surrogate_leg(local)
     modal_result = None if args.config2_only else modal_products_leg(local)
+    config3_result = None if args.config2_only else config3_leg(local)
     scan_result = None
     if args.scan_runs > 0 and not args.config2_only:
         scan_result = scan_leg(local, args.scan_runs, args.scan_steps, warmup=3, rank=rank, world=world)
@@ -690,7 +747,7 @@ def main() -> int:
             "config": config, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "clocks": clocks.summary(), "runs": runs_result, "scan": scan_result,
-            "surrogate": surrogate_result, "modal_products": modal_result}
+            "surrogate": surrogate_result, "modal_products": modal_result, "config3": config3_result}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del session, s2
