@@ -75,121 +75,150 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_inverse(EnvModalArgsT<R> a)
     absorber[j] = to_c<cplx<R>>(B[bitrev((int)a.crop[j], a.log_n_to)]);
 }
 
-// The Raman convolution runs in FP64 in both forms: a molecular gas's kernel spectrum in SI
-// units (about 1e-55 at a femtosecond spacing) lies below FP32's range.  With two field
-// components (rows x, y of the node) the Kerr cubic sums over them and the Raman response
-// is the tensor one (passes/responses.py:501-550): the trace drive |a_x|^2/2 + |a_y|^2/2 and,
-// with a traceless kernel, the difference and coherence drives, three convolutions u, v, w
-// whose symmetric matrix [[u + v, w], [w, u - v]] multiplies the field.
+constexpr int kNodeThreads = 512;  // one radix-8 butterfly per thread at 4 096 samples
+constexpr int kMaxPairs = kMaxEnvelopeSamples / 2 / kNodeThreads + 1;
+
+// Y = H X on the packed spectrum of a real drive of length 2n, and the packing of the
+// inverse real transform, in place over the swizzled row: Z[j] (j < n, bit-reversed slots)
+// holds the forward transform of d(2m) + i d(2m + 1).  Pair (k, n - k) needs Z[k] and
+// Z[n - k] alone and gives Z'[k] and Z'[n - k] (k = 0 also makes bin n), so every thread
+// reads its pairs, the block meets, and the thread writes them back in natural order:
+//   X[k] = E_k + w^k O_k,  E_k = (Z[k] + Z*[n-k]) / 2,  O_k = -i (Z[k] - Z*[n-k]) / 2
+//   Z'[k] = E'_k + i O'_k, E'_k = (Y[k] + Y*[n-k]) / 2, O'_k = (Y[k] - Y*[n-k]) conj(w^k) / 2
+// with w = exp(-2 pi i / 2n) and the imaginary parts of Y[0] and Y[n] dropped.
+__device__ __forceinline__ void spectrum_product(double2* B, const double2* __restrict__ H,
+                                                 const double2* __restrict__ tw, int n, int log_n) {
+  double2 za[kMaxPairs], zb[kMaxPairs];
+  int count = 0;
+  for (int k = threadIdx.x; k <= n / 2; k += blockDim.x, ++count) {
+    const int km = k == 0 ? 0 : n - k;
+    const double2 a = B[row_slot<double2>(bitrev(k, log_n))];
+    const double2 b = B[row_slot<double2>(bitrev(km, log_n))];
+    if (k == 0) {
+      // X[0] = Re Z0 + Im Z0, X[n] = Re Z0 - Im Z0 (both real)
+      double2 y0 = cmul(H[0], make_double2(a.x + a.y, 0.0));
+      double2 yn = cmul(H[n], make_double2(a.x - a.y, 0.0));
+      y0.y = 0.0;
+      yn.y = 0.0;
+      // Z'[0] = (Y0 + Yn) / 2 + i (Y0 - Yn) / 2, conj(w^0) = 1
+      za[count] = make_double2(0.5 * (y0.x + yn.x), 0.5 * (y0.x - yn.x));
+      zb[count] = za[count];
+      continue;
+    }
+    const double2 e = cscale(0.5, cadd(a, cconj(b)));
+    const double2 o = cscale(0.5, mul_mi(csub(a, cconj(b))));
+    const double2 wk = tw[k], wm = tw[km];
+    const double2 xk = cadd(e, cmul(wk, o));
+    // X[n - k]: E_{n-k} = conj(E_k), O_{n-k} = -i (Z[n-k] - Z*[k]) / 2
+    const double2 om = cscale(0.5, mul_mi(csub(b, cconj(a))));
+    const double2 xm = cadd(cconj(e), cmul(wm, om));
+    const double2 yk = cmul(H[k], xk), ym = cmul(H[km], xm);
+    za[count] = cadd(cscale(0.5, cadd(yk, cconj(ym))), mul_pi(cscale(0.5, cmul(csub(yk, cconj(ym)), cconj(wk)))));
+    zb[count] = cadd(cscale(0.5, cadd(ym, cconj(yk))), mul_pi(cscale(0.5, cmul(csub(ym, cconj(yk)), cconj(wm)))));
+  }
+  __syncthreads();
+  count = 0;
+  for (int k = threadIdx.x; k <= n / 2; k += blockDim.x, ++count) {
+    B[row_slot<double2>(k)] = za[count];
+    if (k != 0 && k != n / 2) B[row_slot<double2>(n - k)] = zb[count];
+  }
+  __syncthreads();
+}
+
+// The nodes' responses, one CTA per node.  The Raman convolutions run in FP64 in both
+// forms: a molecular gas's kernel spectrum in SI units (about 1e-55 at a femtosecond
+// spacing) lies below FP32's range.  With two field components (rows x, y of the node) the
+// Kerr cubic sums over them and the Raman response is the tensor one
+// (passes/responses.py:501-550): the trace drive |a_x|^2/2 + |a_y|^2/2 and, with a
+// traceless kernel, the difference and coherence drives, three convolutions u, v, w whose
+// symmetric matrix [[u + v, w], [w, u - v]] multiplies the field.  Each convolution is
+// added to the node's stream as it is formed (the first with the Kerr cubic), so the row
+// of shared memory is the transform's alone.
 template <class R>
-__global__ void __launch_bounds__(kEnvThreads) k_env_nodes(EnvModalArgsT<R> a) {
+__global__ void __launch_bounds__(kNodeThreads, 2) k_env_nodes(EnvModalArgsT<R> a) {
   using C = cplx<R>;
   extern __shared__ __align__(16) double2 en_raw[];
   const int n = a.n_to, node = blockIdx.x, nc = a.n_components;
-  double2* B = en_raw;  // a drive's transform, then its convolution's
-  double2* H = B + n;   // H D
-  double* U = reinterpret_cast<double*>(H + n);  // three drives: the trace and difference convolutions
-  double* V = U + n;
-  __shared__ double2 top;  // bin n
+  double2* B = en_raw;  // a drive's transform, then its convolution's (swizzled slots)
   const StageScalarsDev& st = *a.stage;
   const C* Ex = reinterpret_cast<const C*>(a.node_field) + (size_t)node * nc * n;
   const C* Ey = Ex + (nc == 2 ? n : 0);
+  C* Px = reinterpret_cast<C*>(a.node_streams) + (size_t)node * nc * n;
+  C* Py = Px + (nc == 2 ? n : 0);
   const bool raman = a.raman_spectrum != nullptr;
   const int drives = !raman ? 0 : (nc == 2 && a.raman_kernels == 2 ? 3 : 1);
-  for (int dr = 0; dr < drives; ++dr) {
-    // the drive on [0, n), zero on [n, 2n), packed
-    for (int m = threadIdx.x; m < n; m += blockDim.x) {
-      double v[2] = {0.0, 0.0};
-      if (2 * m < n) {
-        for (int q = 0; q < 2; ++q) {
-          const double2 x = to_d2(Ex[2 * m + q]);
-          const double xx = 0.5 * (x.x * x.x + x.y * x.y);
-          if (nc == 1) {
-            v[q] = xx;
-          } else {
-            const double2 y = to_d2(Ey[2 * m + q]);
-            const double yy = 0.5 * (y.x * y.x + y.y * y.y);
-            v[q] = dr == 0 ? xx + yy : dr == 1 ? xx - yy : 2.0 * 0.5 * (x.x * y.x + x.y * y.y);
-          }
-        }
-      }
-      B[m] = make_double2(v[0], v[1]);
-    }
-    __syncthreads();
-    fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
-    const double2* kernel = a.raman_spectrum + (dr == 0 ? 0 : (size_t)(n + 1));  // trace, then traceless
-    for (int k = threadIdx.x; k <= n; k += blockDim.x) {
-      const double2 y = cmul(kernel[k], unpack_real(B, a.twiddles, k, n, a.log_n_to));
-      if (k < n) H[k] = y;
-      else top = y;
-    }
-    __syncthreads();
-    // irfft of length 2n: Z_k = E_k + i O_k, E_k = (Y_k + Y*_{n-k}) / 2,
-    // O_k = (Y_k - Y*_{n-k}) conj(w^k) / 2; the imaginary parts of bins 0 and n dropped
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      double2 yk = H[k], ym = k == 0 ? top : H[n - k];
-      if (k == 0) {
-        yk.y = 0.0;
-        ym.y = 0.0;
-      }
-      ym = cconj(ym);
-      const double2 e = cscale(0.5, cadd(yk, ym));
-      const double2 o = cscale(0.5, cmul(csub(yk, ym), cconj(a.twiddles[k])));
-      B[k] = cadd(e, mul_pi(o));
-    }
-    __syncthreads();
-    fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/true);
-    if (dr + 1 < drives) {  // keep u and v in natural order; the last one stays in B
-      double* keep = dr == 0 ? U : V;
-      const double inv = 1.0 / (double)n;
-      for (int t = threadIdx.x; t < n; t += blockDim.x) {
-        const double2 z = B[bitrev(t >> 1, a.log_n_to)];
-        keep[t] = ((t & 1) ? z.y : z.x) * inv;
-      }
-      __syncthreads();
-    }
-  }
   // the Kerr coefficient times the density (about 1e-37 in SI units for a gas) is applied in
   // FP64 to the cubic formed in R, so that it never rounds to an FP32 subnormal
   const double factor = a.kerr ? a.kerr_coefficient * st.kerr_density : 0.0;
   const R self = R(a.kerr_self), conj = R(a.kerr_conjugate);
   const double raman_scale = kEps0 * (a.raman_mixture ? 1.0 : st.raman_density);  // a mixture's are inside
   const double inv_n = 1.0 / (double)n;
-  C* Px = reinterpret_cast<C*>(a.node_streams) + (size_t)node * nc * n;
-  C* Py = Px + (nc == 2 ? n : 0);
-  for (int t = threadIdx.x; t < n; t += blockDim.x) {
-    const C x = Ex[t], y = Ey[t];
-    double2 px = make_double2(0.0, 0.0), py = px;
-    if (a.kerr) {  // c rho (s (sum |a|^2) a_p + q (sum a^2) a_p*), summed over the components
-      R mod = x.x * x.x + x.y * x.y;
-      C sq = cmul(x, x);
-      if (nc == 2) {
-        mod += y.x * y.x + y.y * y.y;
-        sq = cadd(sq, cmul(y, y));
-      }
-      const C cx = cadd(cscale(self * mod, x), cscale(conj, cmul(sq, cconj(x))));
-      px = make_double2(factor * (double)cx.x, factor * (double)cx.y);
-      if (nc == 2) {
-        const C cy = cadd(cscale(self * mod, y), cscale(conj, cmul(sq, cconj(y))));
-        py = make_double2(factor * (double)cy.x, factor * (double)cy.y);
-      }
-    }
+  for (int dr = 0; dr < (drives > 0 ? drives : 1); ++dr) {
     if (drives > 0) {
-      const double2 z = B[bitrev(t >> 1, a.log_n_to)];
-      const double last = ((t & 1) ? z.y : z.x) * inv_n;  // irfft's 1 / (2n), with the packing's 2
+      // the drive on [0, n), zero on [n, 2n), packed: B[m] = d(2m) + i d(2m + 1)
+      for (int m = threadIdx.x; m < n; m += blockDim.x) {
+        double v[2] = {0.0, 0.0};
+        if (2 * m < n) {
+          for (int q = 0; q < 2; ++q) {
+            const double2 x = to_d2(Ex[2 * m + q]);
+            const double xx = 0.5 * (x.x * x.x + x.y * x.y);
+            if (nc == 1) {
+              v[q] = xx;
+            } else {
+              const double2 y = to_d2(Ey[2 * m + q]);
+              const double yy = 0.5 * (y.x * y.x + y.y * y.y);
+              v[q] = dr == 0 ? xx + yy : dr == 1 ? xx - yy : 2.0 * 0.5 * (x.x * y.x + x.y * y.y);
+            }
+          }
+        }
+        B[row_slot<double2>(m)] = make_double2(v[0], v[1]);
+      }
+      __syncthreads();
+      fft_dif_swizzled<false>(B, a.log_n_to, a.twiddles, a.log_n_to + 1);
+      const double2* H = a.raman_spectrum + (dr == 0 ? 0 : (size_t)(n + 1));  // trace, then traceless
+      spectrum_product(B, H, a.twiddles, n, a.log_n_to);
+      fft_dif_swizzled<true>(B, a.log_n_to, a.twiddles, a.log_n_to + 1);
+    }
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      const C x = Ex[t], y = Ey[t];
+      const double g = a.t_window[t];
+      double conv = 0.0;
+      if (drives > 0) {
+        const double2 z = B[row_slot<double2>(bitrev(t >> 1, a.log_n_to))];
+        conv = raman_scale * (((t & 1) ? z.y : z.x) * inv_n);  // irfft's 1 / (2n), with the packing's 2
+      }
       const double2 dx = to_d2(x), dy = to_d2(y);
-      if (drives == 1) {
-        px = cadd(px, cscale(raman_scale * last, dx));
-        if (nc == 2) py = cadd(py, cscale(raman_scale * last, dy));
-      } else {
-        const double u = U[t], v = V[t], w = last;
-        px = cadd(px, cscale(raman_scale, cadd(cscale(u + v, dx), cscale(w, dy))));
-        py = cadd(py, cscale(raman_scale, cadd(cscale(w, dx), cscale(u - v, dy))));
+      if (dr == 0) {  // the Kerr cubic and the first convolution
+        double2 px = make_double2(0.0, 0.0), py = px;
+        if (a.kerr) {  // c rho (s (sum |a|^2) a_p + q (sum a^2) a_p*), summed over the components
+          R mod = x.x * x.x + x.y * x.y;
+          C sq = cmul(x, x);
+          if (nc == 2) {
+            mod += y.x * y.x + y.y * y.y;
+            sq = cadd(sq, cmul(y, y));
+          }
+          const C cx = cadd(cscale(self * mod, x), cscale(conj, cmul(sq, cconj(x))));
+          px = make_double2(factor * (double)cx.x, factor * (double)cx.y);
+          if (nc == 2) {
+            const C cy = cadd(cscale(self * mod, y), cscale(conj, cmul(sq, cconj(y))));
+            py = make_double2(factor * (double)cy.x, factor * (double)cy.y);
+          }
+        }
+        px = cadd(px, cscale(conv, dx));
+        Px[t] = to_c<C>(cscale(g, px));
+        if (nc == 2) {
+          py = cadd(py, cscale(conv, dy));
+          Py[t] = to_c<C>(cscale(g, py));
+        }
+      } else if (dr == 1) {  // + v [[1, 0], [0, -1]]
+        Px[t] = to_c<C>(cadd(to_d2(Px[t]), cscale(g * conv, dx)));
+        Py[t] = to_c<C>(csub(to_d2(Py[t]), cscale(g * conv, dy)));
+      } else {  // + w [[0, 1], [1, 0]]
+        Px[t] = to_c<C>(cadd(to_d2(Px[t]), cscale(g * conv, dy)));
+        Py[t] = to_c<C>(cadd(to_d2(Py[t]), cscale(g * conv, dx)));
       }
     }
-    const double g = a.t_window[t];
-    Px[t] = to_c<C>(cscale(g, px));
-    if (nc == 2) Py[t] = to_c<C>(cscale(g, py));
+    __syncthreads();  // the next drive's packing overwrites the row
   }
 }
 
@@ -214,8 +243,7 @@ cudaError_t configure_env_modal_kernels() {
   const void* kernels[6] = {(const void*)k_env_inverse<double>, (const void*)k_env_inverse<float>,
                             (const void*)k_env_nodes<double>,   (const void*)k_env_nodes<float>,
                             (const void*)k_env_forward<double>, (const void*)k_env_forward<float>};
-  const int nodes = (int)(kMaxEnvelopeSamples * (2 * sizeof(double2) + 2 * sizeof(double)));
-  const int shm[6] = {two, two, nodes, nodes, one, one / 2};
+  const int shm[6] = {two, two, one, one, one, one / 2};
   for (int i = 0; i < 6; ++i) {
     cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shm[i]);
     if (e != cudaSuccess) return e;
@@ -232,9 +260,7 @@ cudaError_t launch_env_inverse(const EnvModalArgsT<R>& a, cudaStream_t s) {
 
 template <class R>
 cudaError_t launch_env_nodes(const EnvModalArgsT<R>& a, int n_nodes, cudaStream_t s) {
-  const bool three = a.n_components == 2 && a.raman_kernels == 2 && a.raman_spectrum;  // u, v kept
-  const size_t bytes = (size_t)a.n_to * (2 * sizeof(double2) + (three ? 2 * sizeof(double) : 0));
-  k_env_nodes<R><<<n_nodes, kEnvThreads, bytes, s>>>(a);
+  k_env_nodes<R><<<n_nodes, kNodeThreads, (size_t)a.n_to * sizeof(double2), s>>>(a);
   return cudaGetLastError();
 }
 
