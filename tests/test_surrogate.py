@@ -209,3 +209,29 @@ def test_training_fits_and_screening_routes_disagreement():
     far = rng.uniform(4, 6, (64, 6)).astype(np.float32)
     _, far_spread = ens.predict(far)
     assert np.median(far_spread) > 3 * np.median(spread)
+
+
+@pytest.mark.gpu
+def test_trained_network_gains_over_the_method_without_it():
+    """On the solver's own data (config 5's distribution: 1-4 modes, n_to 8192, exit
+    spectra from the batched mixed solver): without the network, the best guess of a
+    point's exit spectrum is the training runs' mean spectrum; the trained ensemble beats
+    that guess on held-out points."""
+    from solprop_b200 import scan
+    from solprop_b200 import surrogate as S
+
+    points = scan.draw_points(160, 11, modes=(1, 4), grids=(13,))
+    spectra, done, _ = S.solve_points(points, precision="mixed", max_batch_steps=4096)
+    keep = np.flatnonzero(done)
+    assert keep.size >= 100
+    x, y = S.features([points[i] for i in keep]), spectra[keep]
+    n_train = keep.size - 24
+    ens = S.Ensemble(members=3, seed=2)
+    ens.fit(x[:n_train], y[:n_train], epochs=150, batch=32, lr=2e-3)
+    mean, _ = ens.predict(x[n_train:])
+    trained = S.energy_weighted_error(mean, y[n_train:])
+    without = S.energy_weighted_error(np.broadcast_to(S.floored(y[:n_train]).mean(axis=0), mean.shape),
+                                      y[n_train:])
+    print(f"held-out energy-weighted error: trained median {np.median(trained):.3f}, "
+          f"without the network {np.median(without):.3f}")
+    assert np.median(trained) < 0.8 * np.median(without)
