@@ -666,7 +666,12 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
   }
   // outputs on the owned samples: P = (c rho E^2 E) g, X = g rho J, Z = g' rho J
   {
-    const R factor = R(a.kerr ? a.kerr_coefficient * st.kerr_density : 0.0);
+    // The Kerr factor (coefficient times density: about 1e-39 for helium at a fifth of a bar)
+    // lies among FP32's subnormals; the FP32 form carries it scaled by 2^64 and takes the
+    // scale out of the cubic, both exact powers of two.  FP64 takes it as it is.
+    constexpr double kKerrScale = sizeof(R) == 4 ? 18446744073709551616.0 : 1.0;  // 2^64
+    const R factor = R(a.kerr ? a.kerr_coefficient * st.kerr_density * kKerrScale : 0.0);
+    const R unscale = R(1.0 / kKerrScale);
     const R rho = R(st.plasma_density), ip = R(a.ionisation_potential);
 #pragma unroll
     for (int j = 0; j < kPer; ++j) {
@@ -675,7 +680,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       if (live && u >= A && u < own_hi) {
         const R e = E[j];
         const R win = gate[pad(u)];
-        p = (a.kerr ? factor * (e * e) * e : R(0)) * win;
+        p = (a.kerr ? factor * (e * e) * e * unscale : R(0)) * win;
         if (kMulti && plasma) {  // J + (L / |E|^2) E, the densities inside (plasma.py:471-485)
           const R squared = fabs(e) * fabs(e);
           const R guard = squared > R(0) ? divide(F[j], squared) : R(0);
