@@ -228,8 +228,8 @@ static void validate(const sp_problem_desc* d) {
   if (envelope) {
     // the envelope route: one modal column on one node in one CTA (the single-mode GNLSE),
     // or many modes and nodes on the products
-    if (d->n_to > kMaxEnvelopeSamples)
-      throw Failure(SP_ERR_REFUSED, "the envelope grid above 4096 samples is not built yet");
+    if (d->n_to > kMaxEnvelopeProducts)
+      throw Failure(SP_ERR_REFUSED, "the envelope grid above 8192 samples is not built yet");
     if (d->plasma_enabled) throw Failure(SP_ERR_REFUSED, "envelope plasma is not built yet");
     if (d->kerr_enabled && (!d->kerr_analytic || d->kerr_take_real ||
                             (d->carrier && d->kerr_harmonic != 0.0)))
@@ -1727,14 +1727,15 @@ sp_status sp_workspace_create_ex2(const sp_problem* problem, int device, int pre
     const bool field_raman = d.grid_kind == 0 && d.raman_enabled;
     // the envelope grid's single CTA takes one column on one node without the absorber
     const bool env_products = d.grid_kind == 1 && (problem->n_cols > 1 || d.n_nodes > 1 || d.n_pol_transform > 1 ||
-                                                   d.absorber_in_stage || precision == SP_PRECISION_MIXED);
+                                                   d.absorber_in_stage || precision == SP_PRECISION_MIXED ||
+                                                   d.n_to > kMaxEnvelopeSamples);
     const bool gemm = modal == SP_MODAL_GEMM ||
                       (modal == SP_MODAL_AUTO && (problem->n_cols > kMaxModes || field_raman || env_products));
     if (!gemm && precision == SP_PRECISION_MIXED && d.grid_kind == 1)
       throw Failure(SP_ERR_REFUSED, "the mixed precision of the envelope route takes the modal transform's products");
     if (!gemm && env_products)
       throw Failure(SP_ERR_REFUSED,
-                    "the envelope grid's modes, nodes and in-stage absorber take the modal transform's products");
+                    "the envelope grid's modes, nodes, in-stage absorber and rows above 4096 samples take the modal transform's products");
     if (!gemm && problem->n_cols > kMaxModes)
       throw Failure(SP_ERR_REFUSED, "more than 8 modal columns take the modal transform's products");
     if (!gemm && field_raman)

@@ -64,10 +64,11 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_inverse(EnvModalArgsT<R> a)
   double2* row = reinterpret_cast<double2*>(a.modal_t + (size_t)col * 2 * n);
   for (int t = threadIdx.x; t < n; t += blockDim.x) row[t] = cscale(inv_n, A[bitrev(t, a.log_n_to)]);
   if (!a.alpha) return;
-  // the in-stage absorber -alpha a / 2, transformed and cropped (stage output masks it)
-  double2* B = A + n;
-  for (int t = threadIdx.x; t < n; t += blockDim.x)
-    B[t] = cscale(-0.5 * a.alpha[t], cscale(inv_n, A[bitrev(t, a.log_n_to)]));
+  // the in-stage absorber -alpha a / 2, transformed and cropped (stage output masks it); the
+  // row of shared memory is reused, a(t) read back from the modal field just written
+  __syncthreads();
+  double2* B = A;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) B[t] = cscale(-0.5 * a.alpha[t], row[t]);
   __syncthreads();
   fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
   cplx<R>* absorber = a.spectra + (size_t)3 * a.n_cols * a.n_omega + (size_t)col * a.n_omega;
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_inverse(EnvModalArgsT<R> a)
 }
 
 constexpr int kNodeThreads = 512;  // one radix-8 butterfly per thread at 4 096 samples
-constexpr int kMaxPairs = kMaxEnvelopeSamples / 2 / kNodeThreads + 1;
+constexpr int kMaxPairs = kMaxEnvelopeProducts / 2 / kNodeThreads + 1;
 
 // Y = H X on the packed spectrum of a real drive of length 2n, and the packing of the
 // inverse real transform, in place over the swizzled row: Z[j] (j < n, bit-reversed slots)
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_forward(EnvModalArgsT<R> a)
 }  // namespace
 
 cudaError_t configure_env_modal_kernels() {
-  const int two = (int)(2 * kMaxEnvelopeSamples * sizeof(double2)), one = two / 2;
+  const int one = (int)(kMaxEnvelopeProducts * sizeof(double2)), two = one;  // one FP64 row
   const void* kernels[6] = {(const void*)k_env_inverse<double>, (const void*)k_env_inverse<float>,
                             (const void*)k_env_nodes<double>,   (const void*)k_env_nodes<float>,
                             (const void*)k_env_forward<double>, (const void*)k_env_forward<float>};
@@ -253,8 +254,7 @@ cudaError_t configure_env_modal_kernels() {
 
 template <class R>
 cudaError_t launch_env_inverse(const EnvModalArgsT<R>& a, cudaStream_t s) {
-  const size_t row = (size_t)a.n_to * sizeof(double2);
-  k_env_inverse<R><<<a.n_cols, kEnvThreads, a.alpha ? 2 * row : row, s>>>(a);
+  k_env_inverse<R><<<a.n_cols, kEnvThreads, (size_t)a.n_to * sizeof(double2), s>>>(a);
   return cudaGetLastError();
 }
 

@@ -169,7 +169,8 @@ struct OutputArgs {
 };
 
 // The envelope route (envelope_kernels.cu): one modal column on one node, one CTA.
-constexpr int kMaxEnvelopeSamples = 4096;
+constexpr int kMaxEnvelopeSamples = 4096;   // the single CTA's three rows
+constexpr int kMaxEnvelopeProducts = 8192;  // the products route: one FP64 row per CTA
 struct EnvelopeArgs {
   const StageScalarsDev* stage;
   const double2* lab;            // (n_omega)
@@ -228,7 +229,7 @@ cudaError_t configure_raman_kernels();
 cudaError_t launch_raman_spectrum(const RamanArgs& a, cudaStream_t s);  // the kernel's spectrum alone
 
 // The envelope grid's modal route with many modes and nodes on the products
-// (envelope_modal.cu): complex rows interleaved (re, im), n_to <= kMaxEnvelopeSamples.  R
+// (envelope_modal.cu): complex rows interleaved (re, im), n_to <= kMaxEnvelopeProducts.  R
 // is the form's real type: the inverse transform and the modal field are FP64 in both
 // forms; the node field and streams, the nodes' responses, the forward transform and the
 // spectra are R.

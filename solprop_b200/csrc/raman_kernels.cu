@@ -130,7 +130,7 @@ size_t raman_smem(int n_to) { return (size_t)2 * n_to * sizeof(double2); }
 
 cudaError_t configure_raman_kernels() {
   cudaError_t e = cudaFuncSetAttribute(k_raman_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)raman_smem(kMaxRamanSamples) / 2);
+                                       (int)raman_smem(kMaxEnvelopeProducts) / 2);  // one row
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_raman_nodes<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)raman_smem(kMaxRamanSamples));

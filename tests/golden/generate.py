@@ -540,7 +540,8 @@ def vector_envelope_case(case, *, seed):
     envelope_modal_case(case, seed=seed, modes=modes)
 
 
-def envelope_modal_case(case, *, seed, modes, integrator=None):
+def envelope_modal_case(case, *, seed, modes, integrator=None, limits=(550e-9, 1300e-9), trange=800e-15,
+                        length=0.1):
     """A nitrogen-filled capillary on the envelope grid: several modes on the radial rule's
     nodes, the analytic Kerr cubic, the gas's rotational and vibrational Raman response
     (the drive |A|^2 / 2) and the in-stage collar -- the multimode generalised NLSE of the
@@ -557,11 +558,9 @@ def envelope_modal_case(case, *, seed, modes, integrator=None):
     sus = TabulatedSusceptibility(om, (np.sqrt(1 + n2m1) - 1) / rho0, np.zeros_like(om),
                                   (121e-9, 199e-6), "Borzsonyi 2008 N2")
     nitrogen = Species("N2", sus, IdealGas(), gamma3=1.1e-52, raman=FORMER_N2)
-    length = 0.1
-
     def build(**kw):
         fill = Mixture.fill({nitrogen: 1.0}, 2.0)
-        grid = EnvelopeGrid.from_limits(length, 800e-9, (550e-9, 1300e-9), 800e-15, fft_size="pow2")
+        grid = EnvelopeGrid.from_limits(length, 800e-9, limits, trange, fft_size="pow2")
         extra = {} if integrator is None else {"integrator": integrator}
         return Simulation.from_capillary(
             100e-6, length, fill, None, wavelength=800e-9, grid=grid, fwhm=40e-15, energy=150e-6,
@@ -740,6 +739,9 @@ if __name__ == "__main__":
         envelope_modal_case("env4_n2", seed=11, modes=4)
     if not only or "envv_n2" in only:
         vector_envelope_case("envv_n2", seed=13)
+    if not only or "env2_8k" in only:
+        # rows of 8192 envelope samples: the products route's longest
+        envelope_modal_case("env2_8k", seed=14, modes=2, limits=(400e-9, 2000e-9), trange=6.4e-12, length=0.05)
     if not only or "env3_rk" in only:
         envelope_modal_case("env3_rk", seed=12, modes=3, integrator=RungeKutta())
     if not only or "radial_ar" in only:
