@@ -25,7 +25,7 @@ physics, for throughput measurement at config 3's size:
   the fraction f_R of the nonlinear index, trace weight 1 and a traceless weight 0.5;
 * an in-stage temporal collar and a DOPRI5 march at rtol 1e-6.
 
-Config 3 asks for 2^14 samples; the envelope route holds rows of 4 096 samples
+Config 3 asks for 2^14 samples; the envelope route holds rows of up to 8 192 samples
 (``n_to`` is the record's argument), so the window's sampling is the one thing reduced.
 """
 
