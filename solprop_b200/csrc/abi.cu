@@ -328,6 +328,11 @@ struct sp_workspace {
   // it before it writes them again, so that a copy still in flight never reads the next
   // attempt's tables.
   cudaEvent_t host_tables_free = nullptr;
+  // A single run's Adams attempt phase (table uploads, predict, source, correct, the norms'
+  // read-back), captured once and replayed: its launches and arguments are the same for
+  // every attempt, the tables' contents change in the pinned buffers the copies read
+  cudaGraph_t attempt_graph = nullptr;
+  cudaGraphExec_t attempt_exec = nullptr;
   static constexpr int kStageSlots = 10;
   // per-kernel timing (sp_session_set_timing)
   bool timing = false;
@@ -361,6 +366,8 @@ struct sp_workspace {
   bool borrowed = false;
   ~sp_workspace() {
     if (borrowed) return;
+    if (attempt_exec) cudaGraphExecDestroy(attempt_exec);
+    if (attempt_graph) cudaGraphDestroy(attempt_graph);
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (host_tables_free) cudaEventDestroy(host_tables_free);
     if (stream) cudaStreamSynchronize(stream);
@@ -1364,19 +1371,46 @@ static void check_column(const double* h_norms, double* d_norms, cudaStream_t s)
   throw Failure(SP_ERR_CUDA, "response column: a tile gave up waiting for its predecessors");
 }
 
-// One Adams attempt of a single run; returns accepted.
-static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool fixed) {
-  sp_workspace* ws = S->ws;
-  Pending pd = prepare_attempt(S, dz, end, kink, fixed);
-  upload_stages(ws, 2);
+// The attempt phase of a single run's Adams attempt, issued on the workspace's stream: the
+// step's two stage slots and tables from the pinned buffers, the predictor, the source at the
+// predicted field, the corrector with its reduction, the norms to the pinned host buffer.
+static void issue_attempt(sp_workspace* ws, const StepArgs& a) {
+  CUDA_CHECK(cudaMemcpyAsync(ws->stage.p, ws->h_stage, 2 * sizeof(StageScalarsDev), cudaMemcpyHostToDevice,
+                             ws->stream));
   CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, ws->h_adams, sizeof(AdamsDev), cudaMemcpyHostToDevice, ws->stream));
-  release_host_tables(ws);
-  StepArgs a = step_args_of(ws, ws->adams.p, ws->stage.p);
   { KernelTimer t(ws, SP_K_PREDICT); CUDA_CHECK(launch_adams_predict(a, ws->stream)); }
   eval_source(ws, ws->lab.p, 1, nullptr, ws->src.p, false);
   { KernelTimer t(ws, SP_K_CORRECT); CUDA_CHECK(launch_adams_correct(a, ws->stream)); }
   CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, sizeof(double) * (kColumnStatus + 1),
                              cudaMemcpyDeviceToHost, ws->stream));
+}
+
+// One Adams attempt of a single run; returns accepted.  Without per-kernel timing the attempt
+// phase is a CUDA graph, captured on the first attempt and replayed (one launch instead of
+// nine); the copies out of the pinned tables are released by an event recorded after it.
+static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool fixed) {
+  sp_workspace* ws = S->ws;
+  Pending pd = prepare_attempt(S, dz, end, kink, fixed);
+  StepArgs a = step_args_of(ws, ws->adams.p, ws->stage.p);
+  if (ws->timing) {
+    issue_attempt(ws, a);
+  } else {
+    if (!ws->attempt_exec) {
+      CUDA_CHECK(cudaStreamBeginCapture(ws->stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        issue_attempt(ws, a);
+      } catch (...) {
+        cudaGraph_t partial = nullptr;
+        cudaStreamEndCapture(ws->stream, &partial);
+        if (partial) cudaGraphDestroy(partial);
+        throw;
+      }
+      CUDA_CHECK(cudaStreamEndCapture(ws->stream, &ws->attempt_graph));
+      CUDA_CHECK(cudaGraphInstantiate(&ws->attempt_exec, ws->attempt_graph, 0));
+    }
+    CUDA_CHECK(cudaGraphLaunch(ws->attempt_exec, ws->stream));
+  }
+  release_host_tables(ws);
   CUDA_CHECK(cudaStreamSynchronize(ws->stream));
   ws->flush_timing();
   check_column(ws->h_norms, ws->norms.p, ws->stream);
