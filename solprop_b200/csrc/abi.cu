@@ -297,6 +297,8 @@ struct sp_workspace {
   DevBuf<double> raman_undamped, raman_weights;
   DevBuf<double> stat_power, stat_out, stat_weight;  // plane statistics, on first use
   DevBuf<double2> raman_spectrum;  // field-grid Raman: the damped kernel's spectrum (n_to + 1)
+  DevBuf<float2> raman_spectrum32;  // the envelope products' mixed form: the spectra scaled, complex64
+  DevBuf<int> raman_scale;          // ... and their powers of two
   DevBuf<ChannelTableT<double>> channels;  // a mixture's plasma channels (rate_coeff holds their tables)
   // the modal transform as products (SP_MODAL_GEMM): the node field and streams in HBM;
   // the mixed form's operands in three BF16 parts, rows padded to kpad
@@ -691,6 +693,8 @@ static EnvModalArgsT<R> env_modal_args(const sp_workspace* ws, const double2* la
     ea.spectra = ws->spectra.p;
   } else {
     ea.twiddles_r = ws->f32.env_twiddles.p;
+    ea.raman_spectrum32 = ws->raman_spectrum32.p;
+    ea.raman_scale = ws->raman_scale.p;
     ea.node_field = ws->f32.node_field.p;
     ea.node_streams = ws->f32.node_streams.p;
     ea.projected = ws->f32.proj.p;
@@ -717,7 +721,12 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
     }
     {
       KernelTimer t(ws, SP_K_COLUMN);
-      if (d.raman_enabled) CUDA_CHECK(launch_raman_spectrum(raman_args(ws, slot), ws->stream));
+      if (d.raman_enabled) {
+        RamanArgs ra = raman_args(ws, slot);
+        ra.spectrum32 = ws->raman_spectrum32.p;
+        ra.scale = ws->raman_scale.p;
+        CUDA_CHECK(launch_raman_spectrum(ra, ws->stream));
+      }
       CUDA_CHECK(launch_env_nodes(ea, d.n_nodes, ws->stream));
     }
     {
@@ -1020,6 +1029,10 @@ static void build_workspace(sp_workspace* ws) {
     if (!P.raman_weights.empty()) ws->raman_weights.upload(P.raman_weights.data(), P.raman_weights.size(), s);
     if (d.raman_enabled && (d.grid_kind == 0 || ws->gemm))
       ws->raman_spectrum.alloc((size_t)P.raman_kernels * (d.n_to + 1));
+    if (d.raman_enabled && d.grid_kind == 1 && ws->gemm && ws->precision == SP_PRECISION_MIXED) {
+      ws->raman_spectrum32.alloc((size_t)P.raman_kernels * (d.n_to + 1));
+      ws->raman_scale.alloc(2);
+    }
     CUDA_CHECK(cudaStreamSynchronize(s));
   }
   CUDA_CHECK(cudaStreamSynchronize(s));

@@ -15,9 +15,9 @@
 //   k_env_forward  one CTA per modal column: fft of the projected row, cropped
 //
 // Every transform is the shared-memory radix-4 FFT of fft.cuh over the table
-// exp(-2 pi i m / (2 n_to)), m < n_to.  The inverse transform, the modal field and the
-// Raman convolution are FP64 in both forms; the Kerr cubic and the forward transform run
-// in the form's type R (FP32 in the mixed form).
+// exp(-2 pi i m / (2 n_to)), m < n_to.  The inverse transform and the modal field are FP64
+// in both forms; the Kerr cubic, the Raman convolutions and the forward transform run in the
+// form's type R (FP32 in the mixed form).
 #include "fft.cuh"
 #include "kernels.cuh"
 
@@ -87,48 +87,72 @@ constexpr int kMaxPairs = kMaxEnvelopeProducts / 2 / kNodeThreads + 1;
 //   X[k] = E_k + w^k O_k,  E_k = (Z[k] + Z*[n-k]) / 2,  O_k = -i (Z[k] - Z*[n-k]) / 2
 //   Z'[k] = E'_k + i O'_k, E'_k = (Y[k] + Y*[n-k]) / 2, O'_k = (Y[k] - Y*[n-k]) conj(w^k) / 2
 // with w = exp(-2 pi i / 2n) and the imaginary parts of Y[0] and Y[n] dropped.
-__device__ __forceinline__ void spectrum_product(double2* B, const double2* __restrict__ H,
-                                                 const double2* __restrict__ tw, int n, int log_n) {
-  double2 za[kMaxPairs], zb[kMaxPairs];
+// The Raman convolution's arithmetic: FP64 in the FP64 form; FP32 in the mixed form, on the
+// kernel spectrum scaled by 2^scale (a molecular gas's SI spectrum, about 1e-55, lies below
+// FP32's range; the scale is taken back out in FP64)
+template <class R>
+__device__ __forceinline__ const cplx<R>* spectrum_table(const EnvModalArgsT<R>& a) {
+  if constexpr (sizeof(R) == 8) return a.twiddles;
+  else return a.twiddles_r;
+}
+template <class R>
+__device__ __forceinline__ const cplx<R>* kernel_spectrum(const EnvModalArgsT<R>& a, int kernel) {
+  if constexpr (sizeof(R) == 8) return a.raman_spectrum + (size_t)kernel * (a.n_to + 1);
+  else return a.raman_spectrum32 + (size_t)kernel * (a.n_to + 1);
+}
+template <class R>
+__device__ __forceinline__ double spectrum_unscale(const EnvModalArgsT<R>& a, int kernel, double v) {
+  if constexpr (sizeof(R) == 8) return v;
+  else return scalbn(v, -a.raman_scale[kernel]);
+}
+
+template <class C>
+__device__ __forceinline__ void spectrum_product(C* B, const C* __restrict__ H, const C* __restrict__ tw, int n,
+                                                 int log_n) {
+  using T = decltype(C{}.x);
+  C za[kMaxPairs], zb[kMaxPairs];
   int count = 0;
+  const T half = T(0.5);
   for (int k = threadIdx.x; k <= n / 2; k += blockDim.x, ++count) {
     const int km = k == 0 ? 0 : n - k;
-    const double2 a = B[row_slot<double2>(bitrev(k, log_n))];
-    const double2 b = B[row_slot<double2>(bitrev(km, log_n))];
+    const C a = B[row_slot<C>(bitrev(k, log_n))];
+    const C b = B[row_slot<C>(bitrev(km, log_n))];
     if (k == 0) {
-      // X[0] = Re Z0 + Im Z0, X[n] = Re Z0 - Im Z0 (both real)
-      double2 y0 = cmul(H[0], make_double2(a.x + a.y, 0.0));
-      double2 yn = cmul(H[n], make_double2(a.x - a.y, 0.0));
-      y0.y = 0.0;
-      yn.y = 0.0;
-      // Z'[0] = (Y0 + Yn) / 2 + i (Y0 - Yn) / 2, conj(w^0) = 1
-      za[count] = make_double2(0.5 * (y0.x + yn.x), 0.5 * (y0.x - yn.x));
+      // X[0] = Re Z0 + Im Z0, X[n] = Re Z0 - Im Z0 (both real); Y's imaginary parts dropped;
+      // Z'[0] = (Y0 + Yn) / 2 + i (Y0 - Yn) / 2
+      C x0, xn;
+      x0.x = a.x + a.y;
+      x0.y = T(0);
+      xn.x = a.x - a.y;
+      xn.y = T(0);
+      const T y0 = cmul(H[0], x0).x, yn = cmul(H[n], xn).x;
+      za[count].x = half * (y0 + yn);
+      za[count].y = half * (y0 - yn);
       zb[count] = za[count];
       continue;
     }
-    const double2 e = cscale(0.5, cadd(a, cconj(b)));
-    const double2 o = cscale(0.5, mul_mi(csub(a, cconj(b))));
-    const double2 wk = tw[k], wm = tw[km];
-    const double2 xk = cadd(e, cmul(wk, o));
+    const C e = cscale(half, cadd(a, cconj(b)));
+    const C o = cscale(half, mul_mi(csub(a, cconj(b))));
+    const C wk = tw[k], wm = tw[km];
+    const C xk = cadd(e, cmul(wk, o));
     // X[n - k]: E_{n-k} = conj(E_k), O_{n-k} = -i (Z[n-k] - Z*[k]) / 2
-    const double2 om = cscale(0.5, mul_mi(csub(b, cconj(a))));
-    const double2 xm = cadd(cconj(e), cmul(wm, om));
-    const double2 yk = cmul(H[k], xk), ym = cmul(H[km], xm);
-    za[count] = cadd(cscale(0.5, cadd(yk, cconj(ym))), mul_pi(cscale(0.5, cmul(csub(yk, cconj(ym)), cconj(wk)))));
-    zb[count] = cadd(cscale(0.5, cadd(ym, cconj(yk))), mul_pi(cscale(0.5, cmul(csub(ym, cconj(yk)), cconj(wm)))));
+    const C om = cscale(half, mul_mi(csub(b, cconj(a))));
+    const C xm = cadd(cconj(e), cmul(wm, om));
+    const C yk = cmul(H[k], xk), ym = cmul(H[km], xm);
+    za[count] = cadd(cscale(half, cadd(yk, cconj(ym))), mul_pi(cscale(half, cmul(csub(yk, cconj(ym)), cconj(wk)))));
+    zb[count] = cadd(cscale(half, cadd(ym, cconj(yk))), mul_pi(cscale(half, cmul(csub(ym, cconj(yk)), cconj(wm)))));
   }
   __syncthreads();
   count = 0;
   for (int k = threadIdx.x; k <= n / 2; k += blockDim.x, ++count) {
-    B[row_slot<double2>(k)] = za[count];
-    if (k != 0 && k != n / 2) B[row_slot<double2>(n - k)] = zb[count];
+    B[row_slot<C>(k)] = za[count];
+    if (k != 0 && k != n / 2) B[row_slot<C>(n - k)] = zb[count];
   }
   __syncthreads();
 }
 
-// The nodes' responses, one CTA per node.  The Raman convolutions run in FP64 in both
-// forms: a molecular gas's kernel spectrum in SI units (about 1e-55 at a femtosecond
-// spacing) lies below FP32's range.  With two field components (rows x, y of the node) the
+// The nodes' responses, one CTA per node.  The Raman convolutions run in the form's type
+// (the mixed form's on a scaled spectrum, above).  With two field components (rows x, y of the node) the
 // Kerr cubic sums over them and the Raman response is the tensor one
 // (passes/responses.py:501-550): the trace drive |a_x|^2/2 + |a_y|^2/2 and, with a
 // traceless kernel, the difference and coherence drives, three convolutions u, v, w whose
@@ -138,9 +162,9 @@ __device__ __forceinline__ void spectrum_product(double2* B, const double2* __re
 template <class R>
 __global__ void __launch_bounds__(kNodeThreads, 2) k_env_nodes(EnvModalArgsT<R> a) {
   using C = cplx<R>;
-  extern __shared__ __align__(16) double2 en_raw[];
+  extern __shared__ __align__(16) unsigned char en_raw[];
   const int n = a.n_to, node = blockIdx.x, nc = a.n_components;
-  double2* B = en_raw;  // a drive's transform, then its convolution's (swizzled slots)
+  C* B = reinterpret_cast<C*>(en_raw);  // a drive's transform, then its convolution's (swizzled slots)
   const StageScalarsDev& st = *a.stage;
   const C* Ex = reinterpret_cast<const C*>(a.node_field) + (size_t)node * nc * n;
   const C* Ey = Ex + (nc == 2 ? n : 0);
@@ -158,35 +182,39 @@ __global__ void __launch_bounds__(kNodeThreads, 2) k_env_nodes(EnvModalArgsT<R> 
     if (drives > 0) {
       // the drive on [0, n), zero on [n, 2n), packed: B[m] = d(2m) + i d(2m + 1)
       for (int m = threadIdx.x; m < n; m += blockDim.x) {
-        double v[2] = {0.0, 0.0};
+        R v[2] = {R(0), R(0)};
         if (2 * m < n) {
           for (int q = 0; q < 2; ++q) {
-            const double2 x = to_d2(Ex[2 * m + q]);
-            const double xx = 0.5 * (x.x * x.x + x.y * x.y);
+            const C x = Ex[2 * m + q];
+            const R xx = R(0.5) * (x.x * x.x + x.y * x.y);
             if (nc == 1) {
               v[q] = xx;
             } else {
-              const double2 y = to_d2(Ey[2 * m + q]);
-              const double yy = 0.5 * (y.x * y.x + y.y * y.y);
-              v[q] = dr == 0 ? xx + yy : dr == 1 ? xx - yy : 2.0 * 0.5 * (x.x * y.x + x.y * y.y);
+              const C y = Ey[2 * m + q];
+              const R yy = R(0.5) * (y.x * y.x + y.y * y.y);
+              v[q] = dr == 0 ? xx + yy : dr == 1 ? xx - yy : R(2) * R(0.5) * (x.x * y.x + x.y * y.y);
             }
           }
         }
-        B[row_slot<double2>(m)] = make_double2(v[0], v[1]);
+        C packed;
+        packed.x = v[0];
+        packed.y = v[1];
+        B[row_slot<C>(m)] = packed;
       }
       __syncthreads();
-      fft_dif_swizzled<false>(B, a.log_n_to, a.twiddles, a.log_n_to + 1);
-      const double2* H = a.raman_spectrum + (dr == 0 ? 0 : (size_t)(n + 1));  // trace, then traceless
-      spectrum_product(B, H, a.twiddles, n, a.log_n_to);
-      fft_dif_swizzled<true>(B, a.log_n_to, a.twiddles, a.log_n_to + 1);
+      const C* table = spectrum_table<R>(a);
+      fft_dif_swizzled<false>(B, a.log_n_to, table, a.log_n_to + 1);
+      spectrum_product(B, kernel_spectrum<R>(a, dr == 0 ? 0 : 1), table, n, a.log_n_to);  // trace, then traceless
+      fft_dif_swizzled<true>(B, a.log_n_to, table, a.log_n_to + 1);
     }
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
       const C x = Ex[t], y = Ey[t];
       const double g = a.t_window[t];
       double conv = 0.0;
       if (drives > 0) {
-        const double2 z = B[row_slot<double2>(bitrev(t >> 1, a.log_n_to))];
-        conv = raman_scale * (((t & 1) ? z.y : z.x) * inv_n);  // irfft's 1 / (2n), with the packing's 2
+        const C z = B[row_slot<C>(bitrev(t >> 1, a.log_n_to))];
+        // irfft's 1 / (2n), with the packing's 2; the mixed form's spectrum scale taken out
+        conv = raman_scale * spectrum_unscale<R>(a, dr == 0 ? 0 : 1, (double)((t & 1) ? z.y : z.x) * inv_n);
       }
       const double2 dx = to_d2(x), dy = to_d2(y);
       if (dr == 0) {  // the Kerr cubic and the first convolution
@@ -260,7 +288,7 @@ cudaError_t launch_env_inverse(const EnvModalArgsT<R>& a, cudaStream_t s) {
 
 template <class R>
 cudaError_t launch_env_nodes(const EnvModalArgsT<R>& a, int n_nodes, cudaStream_t s) {
-  k_env_nodes<R><<<n_nodes, kNodeThreads, (size_t)a.n_to * sizeof(double2), s>>>(a);
+  k_env_nodes<R><<<n_nodes, kNodeThreads, (size_t)a.n_to * sizeof(cplx<R>), s>>>(a);
   return cudaGetLastError();
 }
 

@@ -224,6 +224,10 @@ struct RamanArgs {
   // kernels formed (1: the trace; 2: trace and traceless, spectra (2, n_to + 1)); null: scalar
   const double* tensor_weights;
   int n_kernels;
+  // the mixed form's envelope products: the spectra also in complex64, each scaled by the
+  // power of two 2^scale[kernel] that brings its largest bin near one (else null)
+  float2* spectrum32;
+  int* scale;
 };
 cudaError_t configure_raman_kernels();
 cudaError_t launch_raman_spectrum(const RamanArgs& a, cudaStream_t s);  // the kernel's spectrum alone
@@ -248,6 +252,8 @@ struct EnvModalArgsT {
   const R* projected;             // (n_cols, 2 n_to): sum W P / tau
   cplx<R>* spectra;               // (4, n_cols, n_omega): P, -, -, absorber
   const double2* raman_spectrum;  // (raman_kernels, n_to + 1), or null without Raman
+  const float2* raman_spectrum32; // the mixed form: the spectra scaled by 2^raman_scale[k], complex64
+  const int* raman_scale;
   int n_cols, n_omega, n_to, log_n_to, kerr, raman_mixture;
   int n_components;               // field components per node (1, or 2: rows x, y)
   int raman_kernels;              // two components: 1 (trace) or 2 (trace, traceless)

@@ -66,7 +66,30 @@ __global__ void __launch_bounds__(kRamanThreads) k_raman_kernel(RamanArgs a) {
   __syncthreads();
   fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
   double2* spectrum = a.spectrum + (size_t)kernel * (n + 1);
-  for (int k = threadIdx.x; k <= n; k += blockDim.x) spectrum[k] = cscale(a.dt, unpack(B, a.twiddles, k, n, a.log_n_to));
+  double largest = 0.0;
+  for (int k = threadIdx.x; k <= n; k += blockDim.x) {
+    const double2 h = cscale(a.dt, unpack(B, a.twiddles, k, n, a.log_n_to));
+    spectrum[k] = h;
+    largest = fmax(largest, fmax(fabs(h.x), fabs(h.y)));
+  }
+  if (!a.spectrum32) return;
+  // the mixed form's complex64 copy: a molecular gas's spectrum in SI units (about 1e-55)
+  // lies below FP32's range, so it is scaled by the power of two that brings its largest
+  // bin into [1, 2); the convolution takes the scale back out in FP64
+  __shared__ double block_max[kRamanThreads / 32];
+  for (int d = 16; d > 0; d >>= 1) largest = fmax(largest, __shfl_xor_sync(0xffffffffu, largest, d));
+  if (threadIdx.x % 32 == 0) block_max[threadIdx.x / 32] = largest;
+  __syncthreads();
+  double all = 0.0;
+  for (int w = 0; w < (int)(blockDim.x / 32); ++w) all = fmax(all, block_max[w]);
+  const int shift = all > 0.0 ? -ilogb(all) : 0;
+  if (threadIdx.x == 0) a.scale[kernel] = shift;
+  float2* out = a.spectrum32 + (size_t)kernel * (n + 1);
+  __syncthreads();  // every thread's spectrum bins are written
+  for (int k = threadIdx.x; k <= n; k += blockDim.x) {
+    const double2 h = spectrum[k];
+    out[k] = make_float2((float)scalbn(h.x, shift), (float)scalbn(h.y, shift));
+  }
 }
 
 template <class R>
