@@ -416,10 +416,17 @@ sp_status sp_mlp_gemm(const float* A, int lda, int transA, const float* B, int l
  * TMA): C[M,N] = A[M,K] W[N,K]^T (+ bias) (GELU), A and W BF16 with K contiguous (row
  * pitches lda, ldw elements, multiples of 8; 16-byte aligned), K a multiple of 64, N a
  * multiple of 256; writes FP32 C (pitch ldc) and/or BF16 C16 (pitch ldc16) when not NULL.
- * *status (device int) is set to 1 if a wait inside the kernel gave up. */
+ * epilogue 0: none, 1: + bias[n], 2: GELU(. + bias[n]), 3 (training): C the pre-activation
+ * . + bias[n], C16 its GELU.  *status (device int) is set to 1 if a wait inside the kernel
+ * gave up. */
 sp_status sp_mlp_gemm_tc(const void* A, int lda, const void* W, int ldw, float* C, int ldc,
                          void* C16, int ldc16, int M, int N, int K, const float* bias,
                          int epilogue, int* status, void* stream);
+/* The transpose of a (rows, cols) FP32 (src_bf16 0) or BF16 (1) matrix as BF16,
+ * dst[c * ld_dst + r], zero-padded from rows to rows_pad: the operands of the training's
+ * weight and input gradients as products C = A W^T on the tensor cores. */
+sp_status sp_mlp_transpose_bf16(const void* src, int src_bf16, int ld_src, int rows, int cols,
+                                void* dst, int ld_dst, int rows_pad, void* stream);
 /* FP32 rows to BF16 rows, zero-padded from cols to cols_out columns. */
 sp_status sp_mlp_to_bf16(const float* src, int ld_src, int rows, int cols, void* dst,
                          int ld_dst, int cols_out, void* stream);

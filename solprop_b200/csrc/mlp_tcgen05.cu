@@ -140,6 +140,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int n = n0 + cc;
         float v = tile[rr * kPitch + cc];
         if (epilogue >= 1 && bias) v += bias[n];
+        if (epilogue == 3) {  // training: the pre-activation in FP32, the activation in BF16
+          if (C) C[m * ldc + n] = v;
+          if (C16) C16[m * ldc16 + n] = __float2bfloat16_rn(gelu(v));
+          continue;
+        }
         if (epilogue == 2) v = gelu(v);
         if (C) C[m * ldc + n] = v;
         if (C16) C16[m * ldc16 + n] = __float2bfloat16_rn(v);
@@ -163,6 +168,29 @@ __global__ void k_to_bf16(const float* src, int ld_src, int rows, int cols, __nv
   }
 }
 
+// dst[c][r] = BF16(src[r][c]) for r < rows, zero for rows <= r < rows_pad (32 x 32 tiles
+// through shared memory, both sides coalesced)
+template <class T>
+__global__ void k_transpose_bf16(const T* src, int ld_src, int rows, int cols, __nv_bfloat16* dst, int ld_dst,
+                                 int rows_pad) {
+  __shared__ float tile[32][33];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int r = r0 + i, c = c0 + threadIdx.x;
+    float v = 0.0f;
+    if (r < rows && c < cols) {
+      if constexpr (sizeof(T) == 4) v = src[(size_t)r * ld_src + c];
+      else v = __bfloat162float(src[(size_t)r * ld_src + c]);
+    }
+    tile[i][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int c = c0 + i, r = r0 + threadIdx.x;
+    if (c < cols && r < rows_pad) dst[(size_t)c * ld_dst + r] = __float2bfloat16_rn(tile[threadIdx.x][i]);
+  }
+}
+
 // a rows x cols BF16 matrix (row pitch ld elements) as 2-D tiles of box_rows x 64
 bool make_map(CUtensorMap* map, const void* base, int rows, int cols, int ld, int box_rows) {
   return tc::make_bf16_map(map, base, rows, cols, ld, box_rows, kTK);
@@ -177,7 +205,7 @@ sp_status sp_mlp_gemm_tc(const void* A, int lda, const void* W, int ldw, float* 
                          int ldc16, int M, int N, int K, const float* bias, int epilogue, int* status,
                          void* stream) {
   using namespace sp;
-  if (!A || !W || (!C && !C16) || !status || M < 1 || N < 1 || K < 1 || epilogue < 0 || epilogue > 2)
+  if (!A || !W || (!C && !C16) || !status || M < 1 || N < 1 || K < 1 || epilogue < 0 || epilogue > 3)
     return SP_ERR_ARGUMENT;
   // the tiling's and the tensor maps' rules: whole 256-column tiles and 64-wide K slices,
   // 16-byte aligned rows
@@ -192,6 +220,21 @@ sp_status sp_mlp_gemm_tc(const void* A, int lda, const void* W, int ldw, float* 
   const dim3 grid(N / kTN, (M + kTM - 1) / kTM);
   k_mlp_gemm_tc<<<grid, kThreads, kSmemBytes, (cudaStream_t)stream>>>(
       map_a, map_w, C, static_cast<__nv_bfloat16*>(C16), bias, M, N, K, ldc, ldc16, epilogue, status);
+  return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ERR_CUDA;
+}
+
+sp_status sp_mlp_transpose_bf16(const void* src, int src_bf16, int ld_src, int rows, int cols, void* dst,
+                                int ld_dst, int rows_pad, void* stream) {
+  if (!src || !dst || rows < 0 || cols < 0 || rows_pad < rows || ld_dst < rows_pad) return SP_ERR_ARGUMENT;
+  if (!rows_pad || !cols) return SP_OK;
+  const dim3 grid((cols + 31) / 32, (rows_pad + 31) / 32), block(32, 8);
+  if (src_bf16)
+    sp::k_transpose_bf16<__nv_bfloat16><<<grid, block, 0, (cudaStream_t)stream>>>(
+        static_cast<const __nv_bfloat16*>(src), ld_src, rows, cols, static_cast<__nv_bfloat16*>(dst), ld_dst,
+        rows_pad);
+  else
+    sp::k_transpose_bf16<float><<<grid, block, 0, (cudaStream_t)stream>>>(
+        static_cast<const float*>(src), ld_src, rows, cols, static_cast<__nv_bfloat16*>(dst), ld_dst, rows_pad);
   return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ERR_CUDA;
 }
 

@@ -94,6 +94,20 @@ def to_bf16(x, cols_out: int):
     return out
 
 
+def transpose_bf16(x, rows_pad: int):
+    """The (cols, rows_pad) BF16 transpose of an FP32 or BF16 (rows, cols) tensor, zero-padded."""
+    import torch
+
+    out = torch.empty((x.shape[1], rows_pad), dtype=torch.bfloat16, device=x.device)
+    _check(_bind().sp_mlp_transpose_bf16(_ptr(x), int(x.dtype == torch.bfloat16), x.stride(0), x.shape[0],
+                                         x.shape[1], _ptr(out), out.stride(0), rows_pad, None))
+    return out
+
+
+def _pad64(n: int) -> int:
+    return -(-n // 64) * 64
+
+
 # ------------------------------------------------------------------ features and targets
 def features(points) -> np.ndarray:
     """The six inputs of each point, each mapped onto [-1, 1] over the scan's ranges."""
@@ -197,6 +211,60 @@ class Perceptron:
             a = out
         return a, cache
 
+    def forward_tc(self, x, keep: bool = False, status=None):
+        """The training's forward pass on the tcgen05 products (``gemm_tc``): BF16 operands,
+        FP32 accumulation; the hidden layers write their pre-activations in FP32 and their
+        activations in BF16 (epilogue 3).  Returns the output, the cache and the status."""
+        import torch
+
+        a = to_bf16(x, _pad64(x.shape[1]))
+        cache = []
+        last = len(self.weights) - 1
+        for i, (w, b) in enumerate(zip(self.weights, self.biases)):
+            w16 = to_bf16(w, _pad64(w.shape[1]))
+            if i == last:
+                out = torch.empty((a.shape[0], w.shape[0]), dtype=torch.float32, device=self.device)
+                status = gemm_tc(a, w16, out=out, bias=b, epilogue=1, status=status)
+                cache.append((x if i == 0 else a, None))
+                return out, cache, status
+            pre = torch.empty((a.shape[0], w.shape[0]), dtype=torch.float32, device=self.device)
+            nxt = torch.empty((a.shape[0], w.shape[0]), dtype=torch.bfloat16, device=self.device)
+            status = gemm_tc(a, w16, out=pre, out16=nxt, bias=b, epilogue=3, status=status)
+            cache.append((x if i == 0 else a, pre if keep else None))
+            a = nxt
+
+    def gradients_tc(self, cache, dy, status=None):
+        """dW, db of every layer from dL/dy on the tcgen05 products: the weight gradient
+        dz^T a and the input gradient dz W as products C = A W^T of BF16 transposes (the
+        batch zero-padded to a multiple of 64); the first layer's 6-input weight gradient,
+        below the products' 256-column tiles, on the FP32 path.  Returns (grads, status)."""
+        import torch
+
+        lib = _bind()
+        grads = [None] * len(self.params)
+        g = dy
+        rows = _pad64(dy.shape[0])
+        for i in range(len(self.weights) - 1, -1, -1):
+            a, pre = cache[i]
+            w = self.weights[i]
+            if pre is not None:
+                dz = torch.empty_like(g)
+                _check(lib.sp_mlp_gelu_backward(_ptr(g), _ptr(pre), _ptr(dz), g.numel(), None))
+                g = dz
+            dw = torch.empty_like(w)
+            if w.shape[1] % 256 == 0:
+                status = gemm_tc(transpose_bf16(g, rows), transpose_bf16(a, rows), out=dw, status=status)
+            else:
+                gemm(g, a, dw, trans_a=True)
+            db = torch.empty_like(self.biases[i])
+            _check(lib.sp_mlp_bias_grad(_ptr(g), g.shape[0], g.shape[1], _ptr(db), None))
+            grads[2 * i], grads[2 * i + 1] = dw, db
+            if i:
+                da = torch.empty((g.shape[0], w.shape[1]), dtype=torch.float32, device=self.device)
+                status = gemm_tc(to_bf16(g, g.shape[1]), transpose_bf16(w, w.shape[0]), out=da, status=status)
+                g = da
+        return grads, status
+
     def gradients(self, cache, dy):
         """dW, db of every layer from dL/dy (the backward pass)."""
         import torch
@@ -277,14 +345,18 @@ class Ensemble:
                 order = torch.tensor(rng.permutation(n), device=dev)
                 total, count = torch.zeros((), device=dev), 0
                 rate = lr * 0.5 * (1.0 + math.cos(math.pi * epoch / epochs))  # cosine decay
+                status = torch.zeros(1, dtype=torch.int32, device=dev)
                 for s in range(0, n - batch + 1, batch):
                     idx = order[s:s + batch]
                     xb, yb = xt[idx].contiguous(), yt[idx].contiguous()
-                    out, cache = member.forward(xb, keep=True)
+                    out, cache, status = member.forward_tc(xb, keep=True, status=status)
                     loss, dy = mse(out, yb)
-                    member.adam(member.gradients(cache, dy), rate)
+                    grads, status = member.gradients_tc(cache, dy, status=status)
+                    member.adam(grads, rate)
                     total += loss[0]
                     count += 1
+                if int(status.item()):
+                    raise RuntimeError("a tensor-core product's wait gave up during training")
                 if log and (epoch % 50 == 0 or epoch == epochs - 1):
                     log(f"member {k} epoch {epoch} loss {float(total) / max(count, 1):.4e}")
             last = float(total) / max(count, 1)

@@ -153,6 +153,36 @@ def test_backward_matches_oracle_gradients():
 
 
 @gpu
+def test_tcgen05_training_pass_matches_oracle_gradients():
+    """The training's forward and backward on the tcgen05 products (``forward_tc``,
+    ``gradients_tc``: BF16 transposes, the batch zero-padded) for a full-size member on a
+    batch of 40: output within 1e-3 and every gradient within 2e-2 (relative L2) of the
+    oracle's with BF16 operands."""
+    from solprop_b200 import surrogate as S
+
+    torch = _torch()
+    net = S.Perceptron(seed=7)
+    rng = np.random.default_rng(6)
+    x = rng.uniform(-1, 1, (40, 6)).astype(np.float32)
+    t = rng.normal(size=(40, 2048)).astype(np.float32)
+    xt, tt = torch.tensor(x, device="cuda"), torch.tensor(t, device="cuda")
+    y, cache, status = net.forward_tc(xt, keep=True)
+    loss, dy = S.mse(y, tt)
+    grads, status = net.gradients_tc(cache, dy, status=status)
+    assert int(status.item()) == 0
+    ws = [w.cpu().numpy().astype(np.float64) for w in net.weights]
+    bs = [b.cpu().numpy().astype(np.float64) for b in net.biases]
+    yo, co = O.forward(ws, bs, x)
+    lo, dyo = O.mse(yo, t)
+    go = O.backward(ws, co, dyo)
+    assert np.linalg.norm(y.cpu().numpy() - yo) <= 1e-3 * np.linalg.norm(yo)
+    for i, (dw, db) in enumerate(go):
+        gw, gb = grads[2 * i].cpu().numpy(), grads[2 * i + 1].cpu().numpy()
+        assert np.linalg.norm(gw - dw) <= 2e-2 * np.linalg.norm(dw), i
+        assert np.linalg.norm(gb - db) <= 2e-2 * np.linalg.norm(db), i
+
+
+@gpu
 def test_adam_step_matches_its_formula():
     from solprop_b200 import _lib
     from solprop_b200.surrogate import _ptr
