@@ -229,7 +229,7 @@ static void validate(const sp_problem_desc* d) {
     // the envelope route: one modal column on one node in one CTA (the single-mode GNLSE),
     // or many modes and nodes on the products
     if (d->n_to > kMaxEnvelopeProducts)
-      throw Failure(SP_ERR_REFUSED, "the envelope grid above 8192 samples is not built yet");
+      throw Failure(SP_ERR_REFUSED, "the envelope grid above 16384 samples is not built yet");
     if (d->plasma_enabled) throw Failure(SP_ERR_REFUSED, "envelope plasma is not built yet");
     if (d->kerr_enabled && (!d->kerr_analytic || d->kerr_take_real ||
                             (d->carrier && d->kerr_harmonic != 0.0)))
@@ -299,6 +299,8 @@ struct sp_workspace {
   DevBuf<double2> raman_spectrum;  // field-grid Raman: the damped kernel's spectrum (n_to + 1)
   DevBuf<float2> raman_spectrum32;  // the envelope products' mixed form: the spectra scaled, complex64
   DevBuf<int> raman_scale;          // ... and their powers of two
+  DevBuf<double2> env_scratch;      // the envelope products' FP64 rows above 8192 samples: 1.5 n_to per row
+  DevBuf<double2> raman_scratch;    // ... and the Raman kernel's spectra
   DevBuf<ChannelTableT<double>> channels;  // a mixture's plasma channels (rate_coeff holds their tables)
   // the modal transform as products (SP_MODAL_GEMM): the node field and streams in HBM;
   // the mixed form's operands in three BF16 parts, rows padded to kpad
@@ -592,6 +594,7 @@ static RamanArgs raman_args(const sp_workspace* ws, int slot) {
   ra.dt = d.dt_fine;
   ra.tensor_weights = ws->P->raman_weights.empty() ? nullptr : ws->raman_weights.p;
   ra.n_kernels = ws->P->raman_kernels;
+  ra.scratch = ws->raman_scratch.p;
   return ra;
 }
 
@@ -673,6 +676,7 @@ static EnvModalArgsT<R> env_modal_args(const sp_workspace* ws, const double2* la
   ea.t_window = ws->t_window.p;
   ea.alpha = absorber ? ws->alpha.p : nullptr;
   ea.modal_t = ws->modal_t.p;
+  ea.scratch = ws->env_scratch.p;
   ea.raman_spectrum = d.raman_enabled ? ws->raman_spectrum.p : nullptr;
   ea.n_cols = P.n_cols;
   ea.n_omega = d.n_omega;
@@ -1032,6 +1036,14 @@ static void build_workspace(sp_workspace* ws) {
     if (d.raman_enabled && d.grid_kind == 1 && ws->gemm && ws->precision == SP_PRECISION_MIXED) {
       ws->raman_spectrum32.alloc((size_t)P.raman_kernels * (d.n_to + 1));
       ws->raman_scale.alloc(2);
+    }
+    if (d.grid_kind == 1 && ws->gemm && d.n_to > kMaxEnvelopeRowF64) {
+      // rows of FP64 too long for one CTA: the inverse transforms' (every column), and in the
+      // FP64 form the nodes' and the forward transforms'
+      const size_t rows = ws->precision == SP_PRECISION_MIXED ? (size_t)P.n_cols
+                                                              : std::max<size_t>(P.n_cols, d.n_nodes);
+      ws->env_scratch.alloc(rows * ((size_t)d.n_to + d.n_to / 2));
+      if (d.raman_enabled) ws->raman_scratch.alloc((size_t)P.raman_kernels * ((size_t)d.n_to + d.n_to / 2));
     }
     CUDA_CHECK(cudaStreamSynchronize(s));
   }

@@ -19,6 +19,7 @@
 // in both forms; the Kerr cubic, the Raman convolutions and the forward transform run in the
 // form's type R (FP32 in the mixed form).
 #include "fft.cuh"
+#include "fft_long.cuh"
 #include "kernels.cuh"
 
 namespace sp {
@@ -151,6 +152,48 @@ __device__ __forceinline__ void spectrum_product(C* B, const C* __restrict__ H, 
   __syncthreads();
 }
 
+// One sample t of a node's gated polarisation: with drive 0 the Kerr cubic and the first
+// convolution conv (already times eps0 rho) times the field; the later drives add
+// conv [[1, 0], [0, -1]] (the difference) or conv [[0, 1], [1, 0]] (the coherence) times it.
+template <class R>
+__device__ __forceinline__ void node_sample(const EnvModalArgsT<R>& a, const cplx<R>* Ex, const cplx<R>* Ey,
+                                            cplx<R>* Px, cplx<R>* Py, int t, double conv, int dr, int nc,
+                                            double factor, R self, R conj) {
+  using C = cplx<R>;
+  const C x = Ex[t], y = Ey[t];
+  const double g = a.t_window[t];
+  const double2 dx = to_d2(x), dy = to_d2(y);
+  if (dr == 0) {  // the Kerr cubic and the first convolution
+    double2 px = make_double2(0.0, 0.0), py = px;
+    if (a.kerr) {  // c rho (s (sum |a|^2) a_p + q (sum a^2) a_p*), summed over the components
+      R mod = x.x * x.x + x.y * x.y;
+      C sq = cmul(x, x);
+      if (nc == 2) {
+        mod += y.x * y.x + y.y * y.y;
+        sq = cadd(sq, cmul(y, y));
+      }
+      const C cx = cadd(cscale(self * mod, x), cscale(conj, cmul(sq, cconj(x))));
+      px = make_double2(factor * (double)cx.x, factor * (double)cx.y);
+      if (nc == 2) {
+        const C cy = cadd(cscale(self * mod, y), cscale(conj, cmul(sq, cconj(y))));
+        py = make_double2(factor * (double)cy.x, factor * (double)cy.y);
+      }
+    }
+    px = cadd(px, cscale(conv, dx));
+    Px[t] = to_c<C>(cscale(g, px));
+    if (nc == 2) {
+      py = cadd(py, cscale(conv, dy));
+      Py[t] = to_c<C>(cscale(g, py));
+    }
+  } else if (dr == 1) {  // + v [[1, 0], [0, -1]]
+    Px[t] = to_c<C>(cadd(to_d2(Px[t]), cscale(g * conv, dx)));
+    Py[t] = to_c<C>(csub(to_d2(Py[t]), cscale(g * conv, dy)));
+  } else {  // + w [[0, 1], [1, 0]]
+    Px[t] = to_c<C>(cadd(to_d2(Px[t]), cscale(g * conv, dy)));
+    Py[t] = to_c<C>(cadd(to_d2(Py[t]), cscale(g * conv, dx)));
+  }
+}
+
 // The nodes' responses, one CTA per node.  The Raman convolutions run in the form's type
 // (the mixed form's on a scaled spectrum, above).  With two field components (rows x, y of the node) the
 // Kerr cubic sums over them and the Raman response is the tensor one
@@ -208,44 +251,13 @@ __global__ void __launch_bounds__(kNodeThreads, 2) k_env_nodes(EnvModalArgsT<R> 
       fft_dif_swizzled<true>(B, a.log_n_to, table, a.log_n_to + 1);
     }
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
-      const C x = Ex[t], y = Ey[t];
-      const double g = a.t_window[t];
       double conv = 0.0;
       if (drives > 0) {
         const C z = B[row_slot<C>(bitrev(t >> 1, a.log_n_to))];
         // irfft's 1 / (2n), with the packing's 2; the mixed form's spectrum scale taken out
         conv = raman_scale * spectrum_unscale<R>(a, dr == 0 ? 0 : 1, (double)((t & 1) ? z.y : z.x) * inv_n);
       }
-      const double2 dx = to_d2(x), dy = to_d2(y);
-      if (dr == 0) {  // the Kerr cubic and the first convolution
-        double2 px = make_double2(0.0, 0.0), py = px;
-        if (a.kerr) {  // c rho (s (sum |a|^2) a_p + q (sum a^2) a_p*), summed over the components
-          R mod = x.x * x.x + x.y * x.y;
-          C sq = cmul(x, x);
-          if (nc == 2) {
-            mod += y.x * y.x + y.y * y.y;
-            sq = cadd(sq, cmul(y, y));
-          }
-          const C cx = cadd(cscale(self * mod, x), cscale(conj, cmul(sq, cconj(x))));
-          px = make_double2(factor * (double)cx.x, factor * (double)cx.y);
-          if (nc == 2) {
-            const C cy = cadd(cscale(self * mod, y), cscale(conj, cmul(sq, cconj(y))));
-            py = make_double2(factor * (double)cy.x, factor * (double)cy.y);
-          }
-        }
-        px = cadd(px, cscale(conv, dx));
-        Px[t] = to_c<C>(cscale(g, px));
-        if (nc == 2) {
-          py = cadd(py, cscale(conv, dy));
-          Py[t] = to_c<C>(cscale(g, py));
-        }
-      } else if (dr == 1) {  // + v [[1, 0], [0, -1]]
-        Px[t] = to_c<C>(cadd(to_d2(Px[t]), cscale(g * conv, dx)));
-        Py[t] = to_c<C>(csub(to_d2(Py[t]), cscale(g * conv, dy)));
-      } else {  // + w [[0, 1], [1, 0]]
-        Px[t] = to_c<C>(cadd(to_d2(Px[t]), cscale(g * conv, dy)));
-        Py[t] = to_c<C>(cadd(to_d2(Py[t]), cscale(g * conv, dx)));
-      }
+      node_sample<R>(a, Ex, Ey, Px, Py, t, conv, dr, nc, factor, self, conj);
     }
     __syncthreads();  // the next drive's packing overwrites the row
   }
@@ -265,16 +277,167 @@ __global__ void __launch_bounds__(kEnvThreads) k_env_forward(EnvModalArgsT<R> a)
   for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) spectra[j] = A[bitrev((int)a.crop[j], a.log_n_to)];
 }
 
+// ---- FP64 rows of 16 384 samples: the halves of fft_long.cuh over each row's scratch
+// (1.5 n_to complex: the n_to-point spectrum, then the even half's transform)
+
+__global__ void __launch_bounds__(kEnvThreads) k_env_inverse_long(EnvModalArgsT<double> a) {
+  extern __shared__ __align__(16) double2 el_raw[];
+  const int n = a.n_to, h = n / 2, log_h = a.log_n_to - 1, col = blockIdx.x;
+  double2* S = el_raw;
+  double2* gz = a.scratch + (size_t)col * (n + h);
+  double2* ge = gz + n;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) gz[k] = make_double2(0.0, 0.0);
+  __syncthreads();
+  const double2* lab = a.lab + (size_t)col * a.n_omega;
+  for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) gz[a.crop[j]] = lab[j];
+  __syncthreads();
+  const double inv_n = 1.0 / (double)n;  // scipy's ifft carries 1 / n_to
+  double2* row = reinterpret_cast<double2*>(a.modal_t + (size_t)col * 2 * n);
+  for (int half = 0; half < 2; ++half) {
+    long_inverse_half(gz, S, a.twiddles, log_h, half);
+    for (int i = threadIdx.x; i < h; i += blockDim.x)
+      row[2 * i + half] = cscale(inv_n, S[row_slot<double2>(bitrev(i, log_h))]);
+    __syncthreads();
+  }
+  if (!a.alpha) return;
+  long_forward([&](int m) { return cscale(-0.5 * a.alpha[m], row[m]); }, S, gz, ge, a.twiddles, log_h);
+  double2* absorber = a.spectra + (size_t)3 * a.n_cols * a.n_omega + (size_t)col * a.n_omega;
+  for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) absorber[j] = gz[a.crop[j]];
+}
+
+// the mixed form's inverse: the same FP64 transform, the absorber's spectrum in complex64
+__global__ void __launch_bounds__(kEnvThreads) k_env_inverse_long32(EnvModalArgsT<float> a) {
+  extern __shared__ __align__(16) double2 em_raw[];
+  const int n = a.n_to, h = n / 2, log_h = a.log_n_to - 1, col = blockIdx.x;
+  double2* S = em_raw;
+  double2* gz = a.scratch + (size_t)col * (n + h);
+  double2* ge = gz + n;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) gz[k] = make_double2(0.0, 0.0);
+  __syncthreads();
+  const double2* lab = a.lab + (size_t)col * a.n_omega;
+  for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) gz[a.crop[j]] = lab[j];
+  __syncthreads();
+  const double inv_n = 1.0 / (double)n;
+  double2* row = reinterpret_cast<double2*>(a.modal_t + (size_t)col * 2 * n);
+  for (int half = 0; half < 2; ++half) {
+    long_inverse_half(gz, S, a.twiddles, log_h, half);
+    for (int i = threadIdx.x; i < h; i += blockDim.x)
+      row[2 * i + half] = cscale(inv_n, S[row_slot<double2>(bitrev(i, log_h))]);
+    __syncthreads();
+  }
+  if (!a.alpha) return;
+  long_forward([&](int m) { return cscale(-0.5 * a.alpha[m], row[m]); }, S, gz, ge, a.twiddles, log_h);
+  float2* absorber = a.spectra + (size_t)3 * a.n_cols * a.n_omega + (size_t)col * a.n_omega;
+  for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) absorber[j] = to_c<float2>(gz[a.crop[j]]);
+}
+
+__global__ void __launch_bounds__(kEnvThreads) k_env_forward_long(EnvModalArgsT<double> a) {
+  extern __shared__ __align__(16) double2 ef_long_raw[];
+  const int n = a.n_to, h = n / 2, log_h = a.log_n_to - 1, col = blockIdx.x;
+  double2* gz = a.scratch + (size_t)col * (n + h);
+  const double2* row = reinterpret_cast<const double2*>(a.projected) + (size_t)col * n;
+  long_forward([&](int m) { return row[m]; }, ef_long_raw, gz, gz + n, a.twiddles, log_h);
+  double2* spectra = a.spectra + (size_t)col * a.n_omega;
+  for (int j = threadIdx.x; j < a.n_omega; j += blockDim.x) spectra[j] = gz[a.crop[j]];
+}
+
+// The spectrum product of spectrum_product over a natural-order row in global memory: the
+// thread of pair (k, n - k) reads and writes those two bins alone.
+__device__ __forceinline__ void spectrum_product_global(double2* Z, const double2* __restrict__ H,
+                                                        const double2* __restrict__ tw, int n) {
+  for (int k = threadIdx.x; k <= n / 2; k += blockDim.x) {
+    const int km = k == 0 ? 0 : n - k;
+    const double2 a = Z[k], b = Z[km];
+    if (k == 0) {
+      const double y0 = cmul(H[0], make_double2(a.x + a.y, 0.0)).x, yn = cmul(H[n], make_double2(a.x - a.y, 0.0)).x;
+      Z[0] = make_double2(0.5 * (y0 + yn), 0.5 * (y0 - yn));
+      continue;
+    }
+    const double2 e = cscale(0.5, cadd(a, cconj(b)));
+    const double2 o = cscale(0.5, mul_mi(csub(a, cconj(b))));
+    const double2 wk = tw[k], wm = tw[km];
+    const double2 xk = cadd(e, cmul(wk, o));
+    const double2 om = cscale(0.5, mul_mi(csub(b, cconj(a))));
+    const double2 xm = cadd(cconj(e), cmul(wm, om));
+    const double2 yk = cmul(H[k], xk), ym = cmul(H[km], xm);
+    Z[k] = cadd(cscale(0.5, cadd(yk, cconj(ym))), mul_pi(cscale(0.5, cmul(csub(yk, cconj(ym)), cconj(wk)))));
+    if (k != n / 2)
+      Z[km] = cadd(cscale(0.5, cadd(ym, cconj(yk))), mul_pi(cscale(0.5, cmul(csub(ym, cconj(yk)), cconj(wm)))));
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kNodeThreads, 1) k_env_nodes_long(EnvModalArgsT<double> a) {
+  extern __shared__ __align__(16) double2 en_long_raw[];
+  const int n = a.n_to, h = n / 2, log_h = a.log_n_to - 1, node = blockIdx.x, nc = a.n_components;
+  double2* S = en_long_raw;
+  double2* gz = a.scratch + (size_t)node * (n + h);
+  double2* ge = gz + n;
+  const StageScalarsDev& st = *a.stage;
+  const double2* Ex = reinterpret_cast<const double2*>(a.node_field) + (size_t)node * nc * n;
+  const double2* Ey = Ex + (nc == 2 ? n : 0);
+  double2* Px = reinterpret_cast<double2*>(a.node_streams) + (size_t)node * nc * n;
+  double2* Py = Px + (nc == 2 ? n : 0);
+  const bool raman = a.raman_spectrum != nullptr;
+  const int drives = !raman ? 0 : (nc == 2 && a.raman_kernels == 2 ? 3 : 1);
+  const double factor = a.kerr ? a.kerr_coefficient * st.kerr_density : 0.0;
+  const double self = a.kerr_self, conj = a.kerr_conjugate;
+  const double raman_scale = kEps0 * (a.raman_mixture ? 1.0 : st.raman_density);
+  const double inv_n = 1.0 / (double)n;
+  if (drives == 0) {
+    for (int t = threadIdx.x; t < n; t += blockDim.x) node_sample<double>(a, Ex, Ey, Px, Py, t, 0.0, 0, nc, factor, self, conj);
+    return;
+  }
+  for (int dr = 0; dr < drives; ++dr) {
+    // the drive on [0, n), zero on [n, 2n), packed b[m] = d(2m) + i d(2m + 1), transformed
+    long_forward(
+        [&](int m) {
+          double v[2] = {0.0, 0.0};
+          if (2 * m < n) {
+            for (int q = 0; q < 2; ++q) {
+              const double2 x = Ex[2 * m + q];
+              const double xx = 0.5 * (x.x * x.x + x.y * x.y);
+              if (nc == 1) {
+                v[q] = xx;
+              } else {
+                const double2 y = Ey[2 * m + q];
+                const double yy = 0.5 * (y.x * y.x + y.y * y.y);
+                v[q] = dr == 0 ? xx + yy : dr == 1 ? xx - yy : 2.0 * 0.5 * (x.x * y.x + x.y * y.y);
+              }
+            }
+          }
+          return make_double2(v[0], v[1]);
+        },
+        S, gz, ge, a.twiddles, log_h);
+    spectrum_product_global(gz, a.raman_spectrum + (dr == 0 ? 0 : (size_t)(n + 1)), a.twiddles, n);
+    // the convolution at samples t < n: packed bins j = t >> 1 < h, j = 2 i + half
+    for (int half = 0; half < 2; ++half) {
+      long_inverse_half(gz, S, a.twiddles, log_h, half);
+      for (int i = threadIdx.x; i < h / 2; i += blockDim.x) {
+        const double2 z = S[row_slot<double2>(bitrev(i, log_h))];
+        for (int q = 0; q < 2; ++q) {
+          const int t = 4 * i + 2 * half + q;
+          node_sample<double>(a, Ex, Ey, Px, Py, t, raman_scale * ((q ? z.y : z.x) * inv_n), dr, nc, factor,
+                              self, conj);
+        }
+      }
+      __syncthreads();  // the next half's inputs overwrite the row
+    }
+  }
+}
+
 }  // namespace
 
 cudaError_t configure_env_modal_kernels() {
-  const int one = (int)(kMaxEnvelopeProducts * sizeof(double2)), two = one;  // one FP64 row
-  const void* kernels[6] = {(const void*)k_env_inverse<double>, (const void*)k_env_inverse<float>,
-                            (const void*)k_env_nodes<double>,   (const void*)k_env_nodes<float>,
-                            (const void*)k_env_forward<double>, (const void*)k_env_forward<float>};
-  const int shm[6] = {two, two, one, one, one, one / 2};
-  for (int i = 0; i < 6; ++i) {
-    cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shm[i]);
+  const int row = (int)(kMaxEnvelopeRowF64 * sizeof(double2));  // one FP64 row (or half a long one)
+  const void* kernels[10] = {(const void*)k_env_inverse<double>, (const void*)k_env_inverse<float>,
+                             (const void*)k_env_nodes<double>,   (const void*)k_env_nodes<float>,
+                             (const void*)k_env_forward<double>, (const void*)k_env_forward<float>,
+                             (const void*)k_env_inverse_long,    (const void*)k_env_inverse_long32,
+                             (const void*)k_env_forward_long,    (const void*)k_env_nodes_long};
+  for (int i = 0; i < 10; ++i) {
+    const int shm = row;  // an FP32 row of 16 384 samples is as long as an FP64 row of 8 192
+    cudaError_t e = cudaFuncSetAttribute(kernels[i], cudaFuncAttributeMaxDynamicSharedMemorySize, shm);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -282,18 +445,34 @@ cudaError_t configure_env_modal_kernels() {
 
 template <class R>
 cudaError_t launch_env_inverse(const EnvModalArgsT<R>& a, cudaStream_t s) {
+  if (a.n_to > kMaxEnvelopeRowF64) {
+    const size_t half = (size_t)a.n_to / 2 * sizeof(double2);
+    if constexpr (sizeof(R) == 8) k_env_inverse_long<<<a.n_cols, kEnvThreads, half, s>>>(a);
+    else k_env_inverse_long32<<<a.n_cols, kEnvThreads, half, s>>>(a);
+    return cudaGetLastError();
+  }
   k_env_inverse<R><<<a.n_cols, kEnvThreads, (size_t)a.n_to * sizeof(double2), s>>>(a);
   return cudaGetLastError();
 }
 
 template <class R>
 cudaError_t launch_env_nodes(const EnvModalArgsT<R>& a, int n_nodes, cudaStream_t s) {
+  if (sizeof(R) == 8 && a.n_to > kMaxEnvelopeRowF64) {
+    if constexpr (sizeof(R) == 8)
+      k_env_nodes_long<<<n_nodes, kNodeThreads, (size_t)a.n_to / 2 * sizeof(double2), s>>>(a);
+    return cudaGetLastError();
+  }
   k_env_nodes<R><<<n_nodes, kNodeThreads, (size_t)a.n_to * sizeof(cplx<R>), s>>>(a);
   return cudaGetLastError();
 }
 
 template <class R>
 cudaError_t launch_env_forward(const EnvModalArgsT<R>& a, cudaStream_t s) {
+  if (sizeof(R) == 8 && a.n_to > kMaxEnvelopeRowF64) {
+    if constexpr (sizeof(R) == 8)
+      k_env_forward_long<<<a.n_cols, kEnvThreads, (size_t)a.n_to / 2 * sizeof(double2), s>>>(a);
+    return cudaGetLastError();
+  }
   k_env_forward<R><<<a.n_cols, kEnvThreads, (size_t)a.n_to * sizeof(cplx<R>), s>>>(a);
   return cudaGetLastError();
 }

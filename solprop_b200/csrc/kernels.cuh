@@ -170,7 +170,9 @@ struct OutputArgs {
 
 // The envelope route (envelope_kernels.cu): one modal column on one node, one CTA.
 constexpr int kMaxEnvelopeSamples = 4096;   // the single CTA's three rows
-constexpr int kMaxEnvelopeProducts = 8192;  // the products route: one FP64 row per CTA
+constexpr int kMaxEnvelopeProducts = 16384;  // the products route's rows
+constexpr int kMaxEnvelopeRowF64 = 8192;     // an FP64 row in one CTA's shared memory; longer
+                                             // FP64 rows take two halves and a global scratch
 struct EnvelopeArgs {
   const StageScalarsDev* stage;
   const double2* lab;            // (n_omega)
@@ -228,6 +230,7 @@ struct RamanArgs {
   // power of two 2^scale[kernel] that brings its largest bin near one (else null)
   float2* spectrum32;
   int* scale;
+  double2* scratch;  // rows above kMaxEnvelopeRowF64: 1.5 n_to complex per kernel
 };
 cudaError_t configure_raman_kernels();
 cudaError_t launch_raman_spectrum(const RamanArgs& a, cudaStream_t s);  // the kernel's spectrum alone
@@ -251,6 +254,7 @@ struct EnvModalArgsT {
   R* node_streams;                // (n_nodes, 2 n_to): the gated polarisation
   const R* projected;             // (n_cols, 2 n_to): sum W P / tau
   cplx<R>* spectra;               // (4, n_cols, n_omega): P, -, -, absorber
+  double2* scratch;               // FP64 rows above kMaxEnvelopeRowF64: 1.5 n_to per row
   const double2* raman_spectrum;  // (raman_kernels, n_to + 1), or null without Raman
   const float2* raman_spectrum32; // the mixed form: the spectra scaled by 2^raman_scale[k], complex64
   const int* raman_scale;

@@ -12,7 +12,10 @@
 // transforms of length 2 n_to run as complex transforms of length n_to (even samples real,
 // odd imaginary) with the usual unpacking, over the table exp(-2 pi i m / (2 n_to)),
 // m < n_to -- the envelope route's arithmetic (envelope_kernels.cu), in FP64 in both forms.
+#include <algorithm>
+
 #include "fft.cuh"
+#include "fft_long.cuh"
 #include "kernels.cuh"
 
 namespace sp {
@@ -45,7 +48,7 @@ __global__ void __launch_bounds__(kRamanThreads) k_raman_kernel(RamanArgs a) {
   // one component: f_R sum_r u_r(s) e^(-g_r s dt); a mixture (passes/responses.py:293-334):
   // sum_c rho_c f_c sum_r u_r(s) e^(-g_r s dt), rows in component order
   const bool mixture = a.n_components > 1;
-  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+  auto packed = [&](int m) {
     double v[2];
     for (int q = 0; q < 2; ++q) {
       const int s = 2 * m + q;
@@ -61,16 +64,33 @@ __global__ void __launch_bounds__(kRamanThreads) k_raman_kernel(RamanArgs a) {
       }
       v[q] = total;
     }
-    B[m] = make_double2(v[0], v[1]);
-  }
-  __syncthreads();
-  fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
+    return make_double2(v[0], v[1]);
+  };
   double2* spectrum = a.spectrum + (size_t)kernel * (n + 1);
   double largest = 0.0;
-  for (int k = threadIdx.x; k <= n; k += blockDim.x) {
-    const double2 h = cscale(a.dt, unpack(B, a.twiddles, k, n, a.log_n_to));
-    spectrum[k] = h;
-    largest = fmax(largest, fmax(fabs(h.x), fabs(h.y)));
+  if (n > kMaxEnvelopeRowF64) {
+    // a row of 16 384 (the envelope grid's longest): two halves through the scratch, the
+    // transform left in natural order there
+    double2* gz = a.scratch + (size_t)kernel * (n + n / 2);
+    long_forward(packed, B, gz, gz + n, a.twiddles, a.log_n_to - 1);
+    for (int k = threadIdx.x; k <= n; k += blockDim.x) {
+      const int kk = k == n ? 0 : k, km = k == 0 ? 0 : (n - k == n ? 0 : n - k);
+      const double2 zk = gz[kk], zm = cconj(gz[km]);
+      const double2 e = cscale(0.5, cadd(zk, zm)), o = cscale(0.5, mul_mi(csub(zk, zm)));
+      const double2 w = k < n ? a.twiddles[k] : make_double2(-1.0, 0.0);
+      const double2 h = cscale(a.dt, cadd(e, cmul(w, o)));
+      spectrum[k] = h;
+      largest = fmax(largest, fmax(fabs(h.x), fabs(h.y)));
+    }
+  } else {
+    for (int m = threadIdx.x; m < n; m += blockDim.x) B[m] = packed(m);
+    __syncthreads();
+    fft_dif_inplace(B, a.log_n_to, a.twiddles, a.log_n_to + 1, /*inverse=*/false);
+    for (int k = threadIdx.x; k <= n; k += blockDim.x) {
+      const double2 h = cscale(a.dt, unpack(B, a.twiddles, k, n, a.log_n_to));
+      spectrum[k] = h;
+      largest = fmax(largest, fmax(fabs(h.x), fabs(h.y)));
+    }
   }
   if (!a.spectrum32) return;
   // the mixed form's complex64 copy: a molecular gas's spectrum in SI units (about 1e-55)
@@ -153,7 +173,7 @@ size_t raman_smem(int n_to) { return (size_t)2 * n_to * sizeof(double2); }
 
 cudaError_t configure_raman_kernels() {
   cudaError_t e = cudaFuncSetAttribute(k_raman_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)raman_smem(kMaxEnvelopeProducts) / 2);  // one row
+                                       (int)(kMaxEnvelopeRowF64 * sizeof(double2)));  // one row
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_raman_nodes<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)raman_smem(kMaxRamanSamples));
@@ -163,7 +183,8 @@ cudaError_t configure_raman_kernels() {
 }
 
 cudaError_t launch_raman_spectrum(const RamanArgs& a, cudaStream_t s) {
-  k_raman_kernel<<<a.tensor_weights ? a.n_kernels : 1, kRamanThreads, raman_smem(a.n_to) / 2, s>>>(a);
+  const size_t row = (size_t)std::min(a.n_to, kMaxEnvelopeRowF64) * sizeof(double2);  // a row, or half a long one
+  k_raman_kernel<<<a.tensor_weights ? a.n_kernels : 1, kRamanThreads, row, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -541,7 +541,7 @@ def vector_envelope_case(case, *, seed):
 
 
 def envelope_modal_case(case, *, seed, modes, integrator=None, limits=(550e-9, 1300e-9), trange=800e-15,
-                        length=0.1):
+                        length=0.1, trim=False):
     """A nitrogen-filled capillary on the envelope grid: several modes on the radial rule's
     nodes, the analytic Kerr cubic, the gas's rotational and vibrational Raman response
     (the drive |A|^2 / 2) and the in-stage collar -- the multimode generalised NLSE of the
@@ -582,6 +582,9 @@ def envelope_modal_case(case, *, seed, modes, integrator=None, limits=(550e-9, 1
     fixed_problem, zs, states, (hist, counts), wall = drive(build(absorber=False, schedule=schedule, n_save=6))
     golden.update({"fixed.z": zs, "fixed.states": states, "fixed.history": hist,
                    "fixed.policy": drive.policy})
+    if trim:  # long rows: the sources and the runs, without the first source's passes
+        golden = {k: v for k, v in golden.items()
+                  if not k.startswith("src0.") or k in ("src0.lab", "src0.z", "src0.source")}
     write(case, problem, golden)
     save_record(lower(fixed_problem), HERE / f"{case}_fixed.problem.npz")
 
@@ -742,6 +745,10 @@ if __name__ == "__main__":
     if not only or "env2_8k" in only:
         # rows of 8192 envelope samples: the products route's longest
         envelope_modal_case("env2_8k", seed=14, modes=2, limits=(400e-9, 2000e-9), trange=6.4e-12, length=0.05)
+    if not only or "env2_16k" in only:
+        # rows of 16384 envelope samples: FP64 rows split into halves through a scratch
+        envelope_modal_case("env2_16k", seed=15, modes=2, limits=(400e-9, 2000e-9), trange=12.8e-12, length=0.02,
+                            trim=True)
     if not only or "env3_rk" in only:
         envelope_modal_case("env3_rk", seed=12, modes=3, integrator=RungeKutta())
     if not only or "radial_ar" in only:

@@ -6,7 +6,8 @@ response (drive |A|^2 / 2) and the in-stage collar -- the multimode generalised 
 stepped by exponential Adams and by DOPRI5.  ``envv_n2`` has two Cartesian field
 components (HE11 along x and along y, HE12): the Kerr cubic summed over the components and
 nitrogen's tensor Raman response (trace and traceless kernels, three drives per node).
-``env2_8k`` has rows of 8 192 samples, the products route's longest.  A workspace takes the modal transform's
+``env2_8k`` and ``env2_16k`` have rows of 8 192 and 16 384 samples (config 3's count): the
+FP64 rows of 16 384 take two halves of shared memory and a global scratch.  A workspace takes the modal transform's
 products for them by itself (complex rows interleaved, N = 2 n_to); the single-CTA
 envelope kernel, which holds one column on one node, refuses them by name.
 """
@@ -40,6 +41,15 @@ def test_oracle_matches_the_reference_on_rows_of_8192():
     assert [march.attempts, march.rejected] == list(g["adaptive.counts"])
 
 
+def test_oracle_matches_the_reference_on_rows_of_16384():
+    from oracle import source as S
+
+    rec, g = record("env2_16k"), golden("env2_16k")
+    assert rec.n_to == 16384
+    for i in (0, 1):
+        assert rel(S.lab_source(rec, g[f"src{i}.lab"], float(g[f"src{i}.z"])), g[f"src{i}.source"]) < 1e-13
+
+
 def test_two_components_are_taken_on_the_envelope_grid_only():
     from solprop_b200 import _lib
 
@@ -63,7 +73,7 @@ def test_many_modes_are_refused_by_the_single_cta_form():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "envv_n2", "env2_8k"])
+@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "envv_n2", "env2_8k", "env2_16k"])
 @pytest.mark.parametrize("index", [0, 1])
 def test_source_matches_the_reference(case, index):
     from solprop_b200 import _lib
@@ -75,7 +85,7 @@ def test_source_matches_the_reference(case, index):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "envv_n2", "env2_8k", "gnlse_raman"])
+@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "envv_n2", "env2_8k", "env2_16k", "gnlse_raman"])
 def test_split_bf16_products_match_the_reference_to_fp32(case):
     """The mixed form: tcgen05 products of three-part BF16 splits, FP32 responses."""
     from solprop_b200 import _lib
@@ -121,7 +131,7 @@ def test_the_single_mode_envelope_gives_the_same_source_on_either_form():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "envv_n2", "env2_8k"])
+@pytest.mark.parametrize("case", ["env4_n2", "env3_rk", "envv_n2", "env2_8k", "env2_16k"])
 def test_envelope_runs_step_with_the_reference(case):
     """A fixed schedule plane by plane at 1e-10, and the adaptive run within its rtol with
     the reference's attempt count (to +-3)."""
