@@ -300,7 +300,7 @@ def modal_products_leg(device: int, repeats: int = 3, n_nodes: int = 16384) -> d
 def config3_leg(device: int, attempts: int = 3, grid: int = 128) -> dict:
     """Config 3's route at its mode and node counts: 30 vector graded-index modes on
     ``grid x grid`` Cartesian nodes (two field components per node), the envelope grid
-    (8 192 samples: the route's row limit; config 3 asks for 2^14), the analytic Kerr cubic
+    with config 3's 2^14 samples, the analytic Kerr cubic
     and the tensor Raman response, DOPRI5 -- ``solprop_b200.grin``'s seeded synthetic
     workload.  Per precision: DOPRI5 attempts per second and, per source evaluation, the
     device time of its kernel families (session timing, CUDA events); the products' roofline
@@ -309,7 +309,7 @@ def config3_leg(device: int, attempts: int = 3, grid: int = 128) -> dict:
     the tensor pipe."""
     from solprop_b200 import _lib, grin
 
-    rec, pol = grin.grin_record(n_to=8192, grid=grid)
+    rec, pol = grin.grin_record(n_to=16384, grid=grid)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
     rows = rec.n_nodes * rec.n_pol_transform

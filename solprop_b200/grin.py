@@ -3,7 +3,7 @@
 A multimode graded-index fibre: parabolic index, core diameter 62.5 um, NA 0.275, the
 lowest mode groups of its Hermite-Gauss modes in both polarisations (30 vector modes)
 sampled on a Cartesian quadrature of the core (128 x 128 nodes), a 10 ps envelope window
-at 1030 nm, Kerr (n2 = 2.7e-20 m^2/W) and a silica-like tensor Raman response (f_R 0.18,
+at 1030 nm (2^14 samples), Kerr (n2 = 2.7e-20 m^2/W) and a silica-like tensor Raman response (f_R 0.18,
 tau_1 12.2 fs, tau_2 32 fs), 500 nJ of a 200 fs Gaussian split equally over the first ten
 modes with seeded phases.  The reference builds graded-index fibres on its field-grid
 general modal route only, so this record is the envelope route restated from published
@@ -24,9 +24,6 @@ physics, for throughput measurement at config 3's size:
   ``K (tau1^2 + tau2^2) / (tau1 tau2^2) e^(-t / tau2) sin(t / tau1)`` with ``K`` giving it
   the fraction f_R of the nonlinear index, trace weight 1 and a traceless weight 0.5;
 * an in-stage temporal collar and a DOPRI5 march at rtol 1e-6.
-
-Config 3 asks for 2^14 samples; the envelope route holds rows of up to 8 192 samples
-(``n_to`` is the record's argument), so the window's sampling is the one thing reduced.
 """
 
 from __future__ import annotations
@@ -65,7 +62,7 @@ def mode_orders(n_groups: int = 5) -> list[tuple[int, int]]:
     return [(m, g - m) for g in range(n_groups) for m in range(g, -1, -1)]
 
 
-def grin_record(n_to: int = 4096, grid: int = 128, seed: int = 3) -> tuple[ProblemRecord, dict]:
+def grin_record(n_to: int = 16384, grid: int = 128, seed: int = 3) -> tuple[ProblemRecord, dict]:
     """The record and DOPRI5 policy of the graded-index workload: 2 x 15 modes on
     ``grid x grid`` Cartesian nodes, ``n_to`` envelope samples over the 10 ps window."""
     dt = WINDOW / n_to
