@@ -332,6 +332,7 @@ struct sp_workspace {
   // it before it writes them again, so that a copy still in flight never reads the next
   // attempt's tables.
   cudaEvent_t host_tables_free = nullptr;
+  bool tables_in_flight = false;  // a copy out of h_stage / h_adams issued since the last wait
   // A single run's Adams attempt phase (table uploads, predict, source, correct, the norms'
   // read-back), captured once and replayed: its launches and arguments are the same for
   // every attempt, the tables' contents change in the pinned buffers the copies read
@@ -402,11 +403,19 @@ struct KernelTimer {
 // The pinned stage and Adams tables are copied to the device asynchronously: before the
 // host writes them, it waits for the copies already issued from them; after issuing
 // copies, it marks them.
+// A wait only follows a release: the batched scan reads the per-run tables on the host and
+// issues no copy from them, so its prepares make no driver call here.
 static void claim_host_tables(sp_workspace* ws) {
-  if (ws->host_tables_free) CUDA_CHECK(cudaEventSynchronize(ws->host_tables_free));
+  if (ws->host_tables_free && ws->tables_in_flight) {
+    CUDA_CHECK(cudaEventSynchronize(ws->host_tables_free));
+    ws->tables_in_flight = false;
+  }
 }
 static void release_host_tables(sp_workspace* ws) {
-  if (ws->host_tables_free) CUDA_CHECK(cudaEventRecord(ws->host_tables_free, ws->stream));
+  if (ws->host_tables_free) {
+    CUDA_CHECK(cudaEventRecord(ws->host_tables_free, ws->stream));
+    ws->tables_in_flight = true;
+  }
 }
 
 // host evaluation of one stage's scalars into slot `slot` of the pinned buffer
