@@ -689,7 +689,6 @@ def main() -> int:
     kernels = session.timing(reset=True)
     session.set_timing(False)
     launches_per_step = sum(c for c in (v[1] for v in kernels.values())) / kernel_steps
-    launches_per_step += kernels["adams_correct"][1] / kernel_steps  # correct + its reduction
     top = max(kernels, key=lambda k: kernels[k][0])
     top_ms = kernels[top][0] / max(kernels[top][1], 1)
     algo = algorithmic_bytes(rec)

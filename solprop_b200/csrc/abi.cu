@@ -327,6 +327,7 @@ struct sp_workspace {
   DevBuf<AdamsDev> adams;
   AdamsDev* h_adams = nullptr;       // pinned
   DevBuf<double> partials, norms;
+  DevBuf<unsigned> norm_arrivals;    // the single-run corrector's block count (zero between launches)
   double* h_norms = nullptr;         // pinned
   // Recorded after every asynchronous copy out of h_stage and h_adams: the host waits on
   // it before it writes them again, so that a copy still in flight never reads the next
@@ -1015,6 +1016,8 @@ static void build_workspace(sp_workspace* ws) {
   ws->partials.alloc((kMaxOrders + 2) * kNormBlocks);
   ws->norms.alloc(kMaxOrders + 2);
   ws->norms.zero(s);
+  ws->norm_arrivals.alloc(1);
+  ws->norm_arrivals.zero(s);
   ws->launches = 5;
   if (ws->gemm && d.grid_kind == 1) {  // inverse, synthesis, (Raman spectrum,) nodes, projection, reduction,
     ws->launches = 6 + (d.raman_enabled ? 1 : 0) + (ws->precision == SP_PRECISION_MIXED ? 2 : 0);  // forward,
@@ -1394,6 +1397,7 @@ static StepArgs step_args_of(sp_workspace* ws, const AdamsDev* adams_dev, const 
   a.partials = ws->partials.p;
   a.norms = ws->norms.p;
   a.n_blocks = kNormBlocks;
+  a.norm_arrivals = ws->norm_arrivals.p;
   return a;
 }
 

@@ -357,6 +357,8 @@ struct StepArgs {
   double* partials;           // (kMaxOrders + 2, kNormBlocks)
   double* norms;              // (kMaxOrders + 2)
   int n_blocks;               // blocks of the grid-stride loops (<= kNormBlocks)
+  unsigned* norm_arrivals;    // single run: the corrector's block count (its last block
+                              // reduces the partials); null: a separate reduction launch
 };
 
 cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t stream);

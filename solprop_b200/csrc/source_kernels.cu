@@ -200,7 +200,9 @@ __device__ __forceinline__ void stage_output_body(const OutputArgs& a, const CS*
     if (st.pre_w[0] != 1.0) pre = cscale(st.pre_w[0], pre);
   } else {
     pre = make_double2(0.0, 0.0);
-    for (int p = 0; p < st.n_pre; ++p)
+    const int n_pre = st.n_pre;
+#pragma unroll 8  // eight terms' loads in flight at a time
+    for (int p = 0; p < n_pre; ++p)
       pre = cadd(pre, cscale(st.pre_w[p], a.prefactor_terms[(size_t)p * total + idx]));
   }
   double2 spec = to_d2(spectra[idx]);  // stream 0: P

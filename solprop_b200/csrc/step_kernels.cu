@@ -85,6 +85,15 @@ __device__ __forceinline__ void phi_functions(double2 x, int order, double2 (&ou
   }
 }
 
+// sum_p w[p] terms[p][i] from +0 in term order, the loads of eight terms in flight at a time
+__device__ __forceinline__ double2 contract_terms(const double* w, int n_terms, const double2* terms,
+                                                  size_t n, size_t i) {
+  double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 8
+  for (int p = 0; p < n_terms; ++p) acc = cadd(acc, cscale(w[p], terms[(size_t)p * n + i]));
+  return acc;
+}
+
 __device__ __forceinline__ double2 combine_terms(const double* w, int n_terms,
                                                  const double2* terms, int n, int i) {
   // translate/stage.py:292-342: one term multiplied (or itself for a unit weight),
@@ -93,10 +102,27 @@ __device__ __forceinline__ double2 combine_terms(const double* w, int n_terms,
     double2 t = terms[i];
     return w[0] == 1.0 ? t : cscale(w[0], t);
   }
-  double2 acc = make_double2(0.0, 0.0);
+  return contract_terms(w, n_terms, terms, n, i);
+}
+
+// x = combine_terms(wx, ...) and r = contract_terms(wr, ...) in one pass over the rows
+__device__ __forceinline__ void combine_two(const double* wx, const double* wr, int n_terms,
+                                            const double2* terms, size_t n, size_t i, double2& x, double2& r) {
+  if (n_terms == 1) {
+    const double2 t = terms[i];
+    x = wx[0] == 1.0 ? t : cscale(wx[0], t);
+    r = cadd(make_double2(0.0, 0.0), cscale(wr[0], t));
+    return;
+  }
+  double2 ax = make_double2(0.0, 0.0), ar = make_double2(0.0, 0.0);
 #pragma unroll 8
-  for (int p = 0; p < n_terms; ++p) acc = cadd(acc, cscale(w[p], terms[(size_t)p * n + i]));
-  return acc;
+  for (int p = 0; p < n_terms; ++p) {
+    const double2 t = terms[(size_t)p * n + i];
+    ax = cadd(ax, cscale(wx[p], t));
+    ar = cadd(ar, cscale(wr[p], t));
+  }
+  x = ax;
+  r = ar;
 }
 
 // sum of n_q values per thread into partials[q][blockIdx.x]; deterministic order
@@ -143,9 +169,44 @@ __global__ void k_reduce_b(const StepArgs* args, const int* flags, int nq) {
   reduce_body(a.partials, a.norms, blockIdx.x, a.n_blocks);
 }
 
+// A single run's corrector reduces its own partials: every block counts itself in on the
+// arrival counter once its partials are written (and fenced), and the last block to arrive
+// adds every block's partials, one warp per quantity in the order reduce_body uses, then
+// resets the counter for the next launch.  The partials are read from L2 (written by other SMs).
+__device__ __forceinline__ void reduce_if_last(const StepArgs& a, int nq) {
+  __shared__ int last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(a.norm_arrivals, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int lane = threadIdx.x & 31;
+  for (int q = threadIdx.x >> 5; q < nq; q += blockDim.x >> 5) {
+    double x = 0.0;
+    for (int b = lane; b < a.n_blocks; b += 32) x += __ldcg(a.partials + q * kNormBlocks + b);
+    for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+    if (lane == 0) a.norms[q] = x;
+  }
+  if (threadIdx.x == 0) *a.norm_arrivals = 0u;
+}
+
+// The trial's coefficient table, copied into shared memory once per block.  Every thread
+// reads each coefficient right before its use; from global memory each such read is a
+// stall of the one warp per scheduler that a single run's passes have.
+static_assert(sizeof(AdamsDev) % 8 == 0, "the table is copied in 8-byte words");
+__device__ __forceinline__ const AdamsDev& staged_adams(const AdamsDev* src) {
+  __shared__ AdamsDev table;
+  const unsigned long long* from = reinterpret_cast<const unsigned long long*>(src);
+  unsigned long long* to = reinterpret_cast<unsigned long long*>(&table);
+  for (int w = threadIdx.x; w < (int)(sizeof(AdamsDev) / 8); w += blockDim.x) to[w] = from[w];
+  __syncthreads();
+  return table;
+}
+
 // ------------------------------------------------------------------ Adams predict
 __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block) {
-  const AdamsDev& ad = *a.adams;
+  const AdamsDev& ad = staged_adams(a.adams);
   const StageScalarsDev& st = *a.stage;
   const int width = ad.width, order = ad.order;
   double v[1] = {0.0};
@@ -163,7 +224,9 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
         state_rows[j] = a.states[(size_t)ad.slots[j] * a.n + i];
       }
     }
-    const double2 x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
+    double2 x, rate_end = make_double2(0.0, 0.0);
+    if (ad.compensated) combine_two(st.phi_w, ad.rate_w, st.n_phi, a.phi_terms, a.n, i, x, rate_end);
+    else x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
     double2 phi[kMaxWidth + 1];
     phi_functions(x, width, phi);
     // beyond |x| = 3 the recurrence started from exp(x) itself
@@ -194,6 +257,10 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
     }
     double2 lab = cadd(cmul(fl, y), cscale(ad.dz, total));
     if (ad.compensated) {
+      // D(z + dz) = sum_p r_p terms_p, contracted always (translate/linop.py:2332-2334), for
+      // the corrector's endpoint; it and the predicted state go to the free slot's rows
+      // (adams_kernels.py accept), which no row of this trial's stencil reads
+      a.rates[(size_t)ad.free_slot * a.n + i] = rate_end;
       // carried rows exp((1 - theta_j) x) ((D(z_j) - x/dz) u_j)   (adams_kernels.py carry)
       const double2 ref = make_double2(x.x / ad.dz, x.y / ad.dz);
       double2 comp = make_double2(0.0, 0.0);
@@ -209,6 +276,7 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
       lab = cadd(lab, cscale(ad.dz, comp));
     }
     a.lab[i] = lab;
+    if (ad.compensated) a.states[(size_t)ad.free_slot * a.n + i] = lab;
     const int bin = i % a.n_omega;
     if (a.norm_mask[bin]) v[0] += y.x * y.x + y.y * y.y;
   }
@@ -219,7 +287,7 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
 // Every loop runs to the compile-time bound (kMaxWidth, kMaxOrders) and stops at the
 // trial's width and order count, so the operand rows stay in registers.
 __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block) {
-  const AdamsDev& ad = *a.adams;
+  const AdamsDev& ad = staged_adams(a.adams);
   const int width = ad.width, n_orders = ad.n_orders;
   double v[kMaxOrders] = {0.0, 0.0, 0.0};
   for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
@@ -255,10 +323,8 @@ __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block)
     if (ad.compensated) {
       const double2 x = a.exponent[i];
       const double2 ref = make_double2(x.x / ad.dz, x.y / ad.dz);
-      // D(z + dz) = sum_p r_p terms_p, contracted always (translate/linop.py:2332-2334)
-      double2 rate_end = make_double2(0.0, 0.0);
-      for (int p = 0; p < a.stage->n_phi; ++p)
-        rate_end = cadd(rate_end, cscale(ad.rate_w[p], a.phi_terms[(size_t)p * a.n + i]));
+      // D(z + dz), contracted by the predictor into the free slot's rate row
+      const double2 rate_end = a.rates[(size_t)ad.free_slot * a.n + i];
       endpoint = cmul(csub(rate_end, ref), a.lab[i]);
 #pragma unroll
       for (int j = 0; j < kMaxWidth - 1; ++j) {
@@ -312,21 +378,14 @@ __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block)
   block_partials<kMaxOrders>(v, a.partials, block);
 }
 
-__device__ __forceinline__ void adams_accept_body(const StepArgs& a, int free_slot, int write_rate,
-                                                  int block) {
-  const AdamsDev& ad = *a.adams;
+// The compensated rows of the free slot (the predicted state and the rate at the step's
+// end) were written by the predictor; accepting adds the source row and the new state.
+__device__ __forceinline__ void adams_accept_body(const StepArgs& a, int free_slot, int block) {
   for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
     const int bin = i % a.n_omega;
     const double2 adv = a.advanced[i];
     a.state[i] = a.active_mask[bin] ? adv : make_double2(adv.x * 0.0, adv.y * 0.0);
     a.store[(size_t)free_slot * a.n + i] = a.source[i];
-    if (write_rate) {
-      a.states[(size_t)free_slot * a.n + i] = a.lab[i];
-      double2 r = make_double2(0.0, 0.0);
-      for (int p = 0; p < a.stage->n_phi; ++p)
-        r = cadd(r, cscale(ad.rate_w[p], a.phi_terms[(size_t)p * a.n + i]));
-      a.rates[(size_t)free_slot * a.n + i] = r;
-    }
   }
 }
 
@@ -336,10 +395,7 @@ __device__ __forceinline__ void adams_start_body(const StepArgs& a, int write_ra
     a.store[i] = a.source[i];
     if (write_rate) {
       a.states[i] = a.state[i];
-      double2 r = make_double2(0.0, 0.0);
-      for (int p = 0; p < a.stage->n_phi; ++p)
-        r = cadd(r, cscale(ad.rate0_w[p], a.phi_terms[(size_t)p * a.n + i]));
-      a.rates[i] = r;
+      a.rates[i] = contract_terms(ad.rate0_w, a.stage->n_phi, a.phi_terms, a.n, i);
     }
   }
 }
@@ -350,10 +406,11 @@ __device__ __forceinline__ void adams_start_body(const StepArgs& a, int write_ra
 // bound by HBM: the register budget is capped so that more warps keep loads in flight.
 constexpr int kStepThreads = 128;
 __global__ void __launch_bounds__(kStepThreads) k_adams_predict(StepArgs a) { adams_predict_body(a, blockIdx.x); }
-__global__ void __launch_bounds__(kStepThreads) k_adams_correct(StepArgs a) { adams_correct_body(a, blockIdx.x); }
-__global__ void k_adams_accept(StepArgs a, int free_slot, int write_rate) {
-  adams_accept_body(a, free_slot, write_rate, blockIdx.x);
+__global__ void __launch_bounds__(kStepThreads) k_adams_correct(StepArgs a) {
+  adams_correct_body(a, blockIdx.x);
+  if (a.norm_arrivals) reduce_if_last(a, kMaxOrders + 1);
 }
+__global__ void k_adams_accept(StepArgs a, int free_slot) { adams_accept_body(a, free_slot, blockIdx.x); }
 __global__ void k_adams_start(StepArgs a, int write_rate) { adams_start_body(a, write_rate, blockIdx.x); }
 
 // batched: items[blockIdx.x] = (run, block of that run)
@@ -373,7 +430,7 @@ __global__ void k_adams_accept_b(const StepArgs* args, const int2* items, const 
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
   const StepArgs& a = own_args(args, it.x);
-  adams_accept_body(a, a.adams->free_slot, a.states != nullptr, it.y);
+  adams_accept_body(a, a.adams->free_slot, it.y);
 }
 __global__ void k_adams_start_b(const StepArgs* args, const int2* items, const int* flags) {
   const int2 it = items[blockIdx.x];
@@ -388,11 +445,11 @@ cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t s) {
 }
 cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t s) {
   k_adams_correct<<<a.n_blocks, kStepThreads, 0, s>>>(a);
-  k_reduce<<<kMaxOrders + 1, 32, 0, s>>>(a.partials, a.norms, kMaxOrders + 1, a.n_blocks);
+  if (!a.norm_arrivals) k_reduce<<<kMaxOrders + 1, 32, 0, s>>>(a.partials, a.norms, kMaxOrders + 1, a.n_blocks);
   return cudaGetLastError();
 }
 cudaError_t launch_adams_accept(const StepArgs& a, int free_slot, double2*, cudaStream_t s) {
-  k_adams_accept<<<a.n_blocks, 256, 0, s>>>(a, free_slot, a.states != nullptr);
+  k_adams_accept<<<a.n_blocks, 256, 0, s>>>(a, free_slot);
   return cudaGetLastError();
 }
 cudaError_t launch_adams_start(const StepArgs& a, cudaStream_t s) {
