@@ -334,6 +334,10 @@ struct sp_workspace {
   // attempt's tables.
   cudaEvent_t host_tables_free = nullptr;
   bool tables_in_flight = false;  // a copy out of h_stage / h_adams issued since the last wait
+  // The free slot of a single run's accepted trial whose accept (the new state, the source
+  // row) the next predictor applies, or -1: settle_accept() writes it at once for anything
+  // else that reads the state or the history rows.
+  int pending_accept = -1;
   // A single run's Adams attempt phase (table uploads, predict, source, correct, the norms'
   // read-back), captured once and replayed: its launches and arguments are the same for
   // every attempt, the tables' contents change in the pinned buffers the copies read
@@ -1136,6 +1140,9 @@ struct sp_session {
   std::vector<std::pair<double, int>> history;  // (z, row), oldest first
   int rejections = 0, order = 1;
   bool last_rejected = false;
+  // the public single-run API leaves an accepted trial's accept to the next predictor
+  // (sp_workspace::pending_accept); a scan's runs accept at once
+  bool defer_accept = false;
   // RK
   std::vector<double> norms_hist;
   // the last attempt, for the batch's attempt rows: end, step, norm, accepted
@@ -1148,9 +1155,12 @@ struct sp_session {
   bool stopped = false;
 };
 
+static void settle_accept(sp_workspace* ws);
+
 static void adams_start(sp_session* S) {
   sp_workspace* ws = S->ws;
   const sp_problem& P = *ws->P;
+  settle_accept(ws);  // the start reads the state
   fill_stage(ws, 1, S->z, S->z);  // source at (z, z)
   AdamsDev& ad = *ws->h_adams;
   std::memset(&ad, 0, sizeof(ad));
@@ -1243,6 +1253,10 @@ static Pending prepare_attempt(sp_session* S, double dz, double end, bool kink, 
   claim_host_tables(ws);
   AdamsDev& ad = *ws->h_adams;
   std::memset(&ad, 0, sizeof(ad));
+  if (ws->pending_accept >= 0) {  // this trial's predictor applies the accept before it
+    ad.settle = ws->pending_accept + 1;
+    ws->pending_accept = -1;
+  }
   ad.dz = dz;
   ad.rtol = R.rtol;
   ad.atol = R.atol;
@@ -1401,6 +1415,17 @@ static StepArgs step_args_of(sp_workspace* ws, const AdamsDev* adams_dev, const 
   return a;
 }
 
+// A pending accept written now (launched on the workspace's stream), for a reader of the
+// state or of the history rows other than the next trial's predictor.
+static void settle_accept(sp_workspace* ws) {
+  if (ws->pending_accept < 0) return;
+  const int slot = ws->pending_accept;
+  ws->pending_accept = -1;
+  const StepArgs a = step_args_of(ws, ws->adams.p, ws->stage.p);
+  KernelTimer t(ws, SP_K_ACCEPT);
+  CUDA_CHECK(launch_adams_accept(a, slot, nullptr, ws->stream));
+}
+
 // A response column whose tiles gave up waiting on one another marks the norms' status
 // slot; the host turns that into an error (and clears the mark).
 static void check_column(const double* h_norms, double* d_norms, cudaStream_t s) {
@@ -1454,8 +1479,12 @@ static bool adams_attempt(sp_session* S, double dz, double end, bool kink, bool 
   check_column(ws->h_norms, ws->norms.p, ws->stream);
   const bool accepted = decide_attempt(S, pd, ws->h_norms);
   if (accepted) {
-    KernelTimer t(ws, SP_K_ACCEPT);
-    CUDA_CHECK(launch_adams_accept(a, pd.free_slot, nullptr, ws->stream));
+    if (S->defer_accept) {
+      ws->pending_accept = pd.free_slot;
+    } else {
+      KernelTimer t(ws, SP_K_ACCEPT);
+      CUDA_CHECK(launch_adams_accept(a, pd.free_slot, nullptr, ws->stream));
+    }
   }
   return accepted;
 }
@@ -1837,6 +1866,7 @@ sp_status sp_workspace_source_device(sp_workspace* ws, const void* lab, double z
   return guarded([&] {
     if (!ws || !lab || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
     CUDA_CHECK(cudaSetDevice(ws->device));
+    settle_accept(ws);
     fill_stage(ws, 0, z, z);
     upload_stages(ws, 1);
     eval_source(ws, (const double2*)lab, 0, nullptr, (double2*)out, quiet != 0);
@@ -1847,6 +1877,7 @@ sp_status sp_workspace_source(sp_workspace* ws, const double* lab, double z, int
   return guarded([&] {
     if (!ws || !lab || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
     CUDA_CHECK(cudaSetDevice(ws->device));
+    settle_accept(ws);
     const size_t bytes = (size_t)ws->P->n * sizeof(double2);
     CUDA_CHECK(cudaMemcpyAsync(ws->lab.p, lab, bytes, cudaMemcpyHostToDevice, ws->stream));
     fill_stage(ws, 0, z, z);
@@ -1867,9 +1898,11 @@ sp_status sp_session_start(sp_workspace* ws, const sp_run_desc* run, sp_session*
     if (run->method == 0 && (run->order < 1 || run->order > 5))
       throw Failure(SP_ERR_ARGUMENT, "Adams order must lie in [1, 5]");
     CUDA_CHECK(cudaSetDevice(ws->device));
+    settle_accept(ws);  // a session before this one on the workspace
     auto S = std::make_unique<sp_session>();
     S->ws = ws;
     S->run = *run;
+    S->defer_accept = true;
     S->planes.assign(run->save_planes, run->save_planes + run->n_save_planes);
     S->kinks.assign(run->hard_kinks, run->hard_kinks + run->n_hard_kinks);
     S->edges.assign(run->breakpoints, run->breakpoints + run->n_breakpoints);
@@ -2109,6 +2142,7 @@ sp_status sp_session_statistics(sp_session* S, const double* power_weight, sp_st
   return guarded([&] {
     if (!S || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
     CUDA_CHECK(cudaSetDevice(S->ws->device));
+    settle_accept(S->ws);
     plane_statistics(S->ws, power_weight, out);
   });
 }
@@ -2159,6 +2193,7 @@ sp_status sp_session_snapshot(sp_session* S, void* buf, size_t capacity, size_t*
     if (!buf) return;
     if (capacity < L.total) throw Failure(SP_ERR_ARGUMENT, "the snapshot buffer is too small");
     CUDA_CHECK(cudaSetDevice(ws->device));
+    settle_accept(ws);  // the state and the history rows as accepted
     unsigned char* b = static_cast<unsigned char*>(buf);
     SnapshotHeader h{};
     std::memcpy(h.magic, kSnapshotMagic, sizeof h.magic);
@@ -2268,6 +2303,7 @@ sp_status sp_session_export(sp_session* S, double* out) {
   return guarded([&] {
     if (!S || !out) throw Failure(SP_ERR_ARGUMENT, "NULL argument");
     CUDA_CHECK(cudaSetDevice(S->ws->device));
+    settle_accept(S->ws);
     const size_t bytes = (size_t)S->ws->P->n * sizeof(double2);
     CUDA_CHECK(cudaMemcpyAsync(out, S->ws->state.p, bytes, cudaMemcpyDeviceToHost, S->ws->stream));
     CUDA_CHECK(cudaStreamSynchronize(S->ws->stream));
@@ -3063,6 +3099,7 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
       sp_session* raw = nullptr;
       sp_status st = sp_session_start(w.get(), &runs[r], &raw);
       if (st != SP_OK) throw Failure(st, g_error);
+      raw->defer_accept = false;  // the scan reads its runs' states between attempts
       S->ss.emplace_back(raw);
       S->ws.push_back(std::move(w));
     }

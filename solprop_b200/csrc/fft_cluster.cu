@@ -135,9 +135,9 @@ __device__ __forceinline__ void inverse_cluster_body(const InverseArgsT<R>& a, i
   cluster.sync();  // no CTA leaves while another reads its shared memory
 }
 
-template <class R>
+template <class R, int C>
 __global__ void __launch_bounds__(512) k_inverse_cluster(InverseArgsT<R> a) {
-  inverse_cluster_body<kFftCluster>(a, blockIdx.y);
+  inverse_cluster_body<C>(a, blockIdx.y);
 }
 
 // batched: items[blockIdx.y] = (run, column)
@@ -220,9 +220,9 @@ __device__ __forceinline__ void forward_cluster_body(const ForwardArgsT<R>& a, i
   cluster.sync();
 }
 
-template <class R>
+template <class R, int C>
 __global__ void __launch_bounds__(512) k_forward_cluster(ForwardArgsT<R> a) {
-  forward_cluster_body<kFftCluster>(a, blockIdx.y);
+  forward_cluster_body<C>(a, blockIdx.y);
 }
 
 // batched: items[blockIdx.y] = (run, row index)
@@ -257,24 +257,57 @@ int fft_cluster_size(int n_to) {
   return kFftCluster;  // portable cluster; M / 8 points per CTA
 }
 
-template <class R>
-cudaError_t launch_inverse_cluster(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream) {
-  const int C = fft_cluster_size(a.n_to);
-  const int Mp = (a.n_to / 2) / C;
-  InverseArgsT<R> copy = a;
-  void* args[] = {&copy};
-  return launch_cluster((const void*)k_inverse_cluster<R>, dim3(C, n_cols), Mp >= 512 ? 512 : Mp,
-                        (size_t)Mp * sizeof(cplx<R>), C, stream, args);
+// A single run's rows are few, so its transforms are latency-bound: wider clusters cut each
+// CTA's passes but add cluster barriers and DSMEM gathers.  Measured on config 2's rows (n_to
+// 16 384, FP64, CUDA events per attempt): inverse over 1/2/4/8 CTAs 41.2/28.4/20.7/18.4 us,
+// forward (which also adds the node groups' partial rows) 31.2/27.1/19.0/26.0 us.
+int single_transform_width(int n_to, size_t complex_bytes, bool forward) {
+  (void)complex_bytes;
+  const int M = n_to / 2;
+  if (M <= 2048) return 1;
+  if (forward && M <= 8192) return 4;
+  return kFftCluster;
 }
 
 template <class R>
-cudaError_t launch_forward_cluster(const ForwardArgsT<R>& a, int n_rows, cudaStream_t stream) {
-  const int C = fft_cluster_size(a.n_to);
+static const void* single_inverse_kernel(int C) {
+  switch (C) {
+    case 2: return (const void*)k_inverse_cluster<R, 2>;
+    case 4: return (const void*)k_inverse_cluster<R, 4>;
+    case 8: return (const void*)k_inverse_cluster<R, 8>;
+    default: return nullptr;
+  }
+}
+template <class R>
+static const void* single_forward_kernel(int C) {
+  switch (C) {
+    case 2: return (const void*)k_forward_cluster<R, 2>;
+    case 4: return (const void*)k_forward_cluster<R, 4>;
+    case 8: return (const void*)k_forward_cluster<R, 8>;
+    default: return nullptr;
+  }
+}
+
+template <class R>
+cudaError_t launch_inverse_cluster(const InverseArgsT<R>& a, int n_cols, int C, cudaStream_t stream) {
+  const void* kernel = single_inverse_kernel<R>(C);
+  if (!kernel) return cudaErrorInvalidValue;
+  const int Mp = (a.n_to / 2) / C;
+  InverseArgsT<R> copy = a;
+  void* args[] = {&copy};
+  return launch_cluster(kernel, dim3(C, n_cols), Mp >= 512 ? 512 : Mp, (size_t)Mp * sizeof(cplx<R>), C,
+                        stream, args);
+}
+
+template <class R>
+cudaError_t launch_forward_cluster(const ForwardArgsT<R>& a, int n_rows, int C, cudaStream_t stream) {
+  const void* kernel = single_forward_kernel<R>(C);
+  if (!kernel) return cudaErrorInvalidValue;
   const int Mp = (a.n_to / 2) / C;
   ForwardArgsT<R> copy = a;
   void* args[] = {&copy};
-  return launch_cluster((const void*)k_forward_cluster<R>, dim3(C, n_rows), Mp >= 512 ? 512 : Mp,
-                        (size_t)2 * Mp * sizeof(cplx<R>), C, stream, args);
+  return launch_cluster(kernel, dim3(C, n_rows), Mp >= 512 ? 512 : Mp, (size_t)2 * Mp * sizeof(cplx<R>), C,
+                        stream, args);
 }
 
 template <class R>
@@ -323,8 +356,8 @@ cudaError_t launch_forward_cluster_b(const ForwardArgsT<R>* args, const int2* it
 }
 
 #define SP_CLUSTER_INSTANCES(R)                                                                      \
-  template cudaError_t launch_inverse_cluster<R>(const InverseArgsT<R>&, int, cudaStream_t);         \
-  template cudaError_t launch_forward_cluster<R>(const ForwardArgsT<R>&, int, cudaStream_t);         \
+  template cudaError_t launch_inverse_cluster<R>(const InverseArgsT<R>&, int, int, cudaStream_t);    \
+  template cudaError_t launch_forward_cluster<R>(const ForwardArgsT<R>&, int, int, cudaStream_t);    \
   template cudaError_t launch_inverse_cluster_b<R>(const InverseArgsT<R>*, const int2*, const int*, \
                                                    int, int, int, cudaStream_t);                     \
   template cudaError_t launch_forward_cluster_b<R>(const ForwardArgsT<R>*, const int2*, const int*, \
@@ -334,17 +367,11 @@ SP_CLUSTER_INSTANCES(float)
 #undef SP_CLUSTER_INSTANCES
 
 cudaError_t configure_cluster_fft() {
-  // the single-run kernels (eight CTAs): rows of up to 2^15 real samples, 2048 complex points
-  // per CTA, two buffers forward; the batched ones of every width: up to kClusterSmem
-  const int single = 2 * 2048 * (int)sizeof(double2);
-  const void* singles[4] = {(const void*)k_inverse_cluster<double>, (const void*)k_forward_cluster<double>,
-                            (const void*)k_inverse_cluster<float>, (const void*)k_forward_cluster<float>};
-  for (const void* k : singles) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, single);
-    if (e != cudaSuccess) return e;
-  }
+  // single-run and batched kernels of every width: rows of up to kClusterSmem per CTA
   for (int C : {2, 4, 8}) {
-    for (const void* k : {inverse_cluster_kernel<double>(C), forward_cluster_kernel<double>(C),
+    for (const void* k : {single_inverse_kernel<double>(C), single_forward_kernel<double>(C),
+                          single_inverse_kernel<float>(C), single_forward_kernel<float>(C),
+                          inverse_cluster_kernel<double>(C), forward_cluster_kernel<double>(C),
                           inverse_cluster_kernel<float>(C), forward_cluster_kernel<float>(C)}) {
       cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClusterSmem);
       if (e != cudaSuccess) return e;

@@ -68,6 +68,8 @@ struct AdamsDev {
   double comp_pred_main[kMaxWidth];
   double comp_corr_main[kMaxWidth + 1];
   int free_slot;               // the history row an accepted step writes
+  int settle;                  // 1 + the free slot of the accepted trial before this one whose
+                               // accept the predictor applies first (0: none pending)
   double rate_w[kMaxTerms];   // D(z + dz) weights (the endpoint rate, "before")
   double rate0_w[kMaxTerms];  // D(z) weights (startup)
 };
@@ -295,10 +297,12 @@ cudaError_t modal_projection_split3(const uint16_t* w_parts, const float* node_s
                                     cudaStream_t s);
 cudaError_t launch_statistics(const StatisticsArgs& a, bool peaks, cudaStream_t s);
 int fft_cluster_size(int n_to);
+// a single run's transforms: one CTA per row (1) or a cluster of 2, 4 or 8 CTAs per row
+int single_transform_width(int n_to, size_t complex_bytes, bool forward);
 template <class R>
-cudaError_t launch_inverse_cluster(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream);
+cudaError_t launch_inverse_cluster(const InverseArgsT<R>& a, int n_cols, int C, cudaStream_t stream);
 template <class R>
-cudaError_t launch_forward_cluster(const ForwardArgsT<R>& a, int n_rows, cudaStream_t stream);
+cudaError_t launch_forward_cluster(const ForwardArgsT<R>& a, int n_rows, int C, cudaStream_t stream);
 template <class R>
 cudaError_t launch_inverse(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream);
 template <class R>

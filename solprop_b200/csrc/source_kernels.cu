@@ -249,7 +249,8 @@ static size_t row_smem(int m) { return row_length<cplx<R>>(m) * sizeof(cplx<R>);
 
 template <class R>
 cudaError_t launch_inverse(const InverseArgsT<R>& a, int n_cols, cudaStream_t stream) {
-  if (fft_cluster_size(a.n_to) > 1) return launch_inverse_cluster(a, n_cols, stream);
+  const int C = single_transform_width(a.n_to, sizeof(cplx<R>), false);
+  if (C > 1) return launch_inverse_cluster(a, n_cols, C, stream);
   const int M = a.n_to >> 1;
   k_inverse_field<R><<<n_cols, threads_for<R>(M), row_smem<R>(M), stream>>>(a);
   return cudaGetLastError();
@@ -257,7 +258,8 @@ cudaError_t launch_inverse(const InverseArgsT<R>& a, int n_cols, cudaStream_t st
 
 template <class R>
 cudaError_t launch_forward(const ForwardArgsT<R>& a, int n_rows, cudaStream_t stream) {
-  if (fft_cluster_size(a.n_to) > 1) return launch_forward_cluster(a, n_rows, stream);
+  const int C = single_transform_width(a.n_to, sizeof(cplx<R>), true);
+  if (C > 1) return launch_forward_cluster(a, n_rows, C, stream);
   const int M = a.n_to >> 1;
   k_forward_field<R><<<n_rows, threads_for<R>(M), row_smem<R>(M), stream>>>(a);
   return cudaGetLastError();

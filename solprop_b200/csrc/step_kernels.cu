@@ -211,9 +211,19 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
   const int width = ad.width, order = ad.order;
   double v[1] = {0.0};
   for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
+    // the accept of the trial before, when the host left it to this pass: the new state and
+    // the source row of its free slot (which this trial's stencil reads as its newest row)
+    double2 y;
+    if (ad.settle) {
+      const double2 adv = a.advanced[i];
+      y = a.active_mask[i % a.n_omega] ? adv : make_double2(adv.x * 0.0, adv.y * 0.0);
+      a.state[i] = y;
+      a.store[(size_t)(ad.settle - 1) * a.n + i] = a.source[i];
+    } else {
+      y = a.state[i];
+    }
     // every operand row of this element is loaded up front, so that the loads overlap
     // one another and the phi functions instead of waiting in the loops below
-    const double2 y = a.state[i];
     constexpr int kRows = 5;  // the Adams order is at most 5: order and width - 1 rows
     double2 rows[kRows], rate_rows[kRows], state_rows[kRows];
 #pragma unroll
