@@ -193,6 +193,15 @@ __device__ __forceinline__ void stage_output_body(const OutputArgs& a, const CS*
   if (idx >= total) return;
   const int j = idx % a.n_omega;
   const StageScalarsDev& st = *a.stage;
+  // every operand is loaded before any is used (the streams of bins off the band too, which
+  // the selections below drop), so that the loads overlap
+  const double2 spec0 = to_d2(spectra[idx]);  // stream 0: P
+  const double2 xs = a.plasma ? to_d2(spectra[(size_t)1 * total + idx]) : make_double2(0.0, 0.0);
+  const double2 zs = a.plasma ? to_d2(spectra[(size_t)2 * total + idx]) : make_double2(0.0, 0.0);
+  const double2 ab_row = a.absorber ? to_d2(spectra[(size_t)3 * total + idx]) : make_double2(0.0, 0.0);
+  const double2 propagator = a.inverse_propagator ? a.inverse_propagator[idx] : make_double2(0.0, 0.0);
+  const bool active = a.active_mask[j];
+  const double omega = a.omega[j], window = a.omega_window[j];
   // prefactor = combine(weights, terms)    (translate/stage.py:292-342)
   double2 pre;
   if (st.n_pre == 1) {
@@ -205,21 +214,18 @@ __device__ __forceinline__ void stage_output_body(const OutputArgs& a, const CS*
     for (int p = 0; p < n_pre; ++p)
       pre = cadd(pre, cscale(st.pre_w[p], a.prefactor_terms[(size_t)p * total + idx]));
   }
-  double2 spec = to_d2(spectra[idx]);  // stream 0: P
-  const bool active = a.active_mask[j];
+  double2 spec = spec0;
   if (a.plasma && active) {
-    const double2 xs = to_d2(spectra[(size_t)1 * total + idx]);
-    const double2 zs = to_d2(spectra[(size_t)2 * total + idx]);
-    const double2 qv = make_double2(0.0, a.omega[j]);
+    const double2 qv = make_double2(0.0, omega);
     const double2 q2 = cmul(qv, qv);
     spec = cadd(spec, csub(cdiv(xs, qv), cdiv(zs, q2)));
   }
-  double2 normalised = cmul(cscale(a.omega_window[j], pre), spec);
+  double2 normalised = cmul(cscale(window, pre), spec);
   if (a.absorber) {
-    double2 ab = active ? to_d2(spectra[(size_t)3 * total + idx]) : make_double2(0.0, 0.0);
+    const double2 ab = active ? ab_row : make_double2(0.0, 0.0);
     normalised = cadd(normalised, ab);
   }
-  if (a.inverse_propagator) normalised = cmul(a.inverse_propagator[idx], normalised);
+  if (a.inverse_propagator) normalised = cmul(propagator, normalised);
   a.out[idx] = normalised;
 }
 

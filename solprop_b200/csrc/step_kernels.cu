@@ -205,75 +205,102 @@ __device__ __forceinline__ const AdamsDev& staged_adams(const AdamsDev* src) {
 }
 
 // ------------------------------------------------------------------ Adams predict
+// kPair: two warps per 32 elements (a single run, whose few elements leave most of the GPU
+// idle): the even warp of a pair takes the phi functions, the moments and the predicted
+// state, the odd warp the compensation (the carried rows, each with its own exponential,
+// and the step end's rate) and hands its sums to the even warp through shared memory, the
+// pair meeting at a named barrier once per trip (double-buffered, so one meeting per trip
+// suffices).  Otherwise every thread takes both parts of its element.
+template <bool kPair>
 __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block) {
   const AdamsDev& ad = staged_adams(a.adams);
   const StageScalarsDev& st = *a.stage;
   const int width = ad.width, order = ad.order;
+  const int lane = threadIdx.x & 31, warp_in_block = threadIdx.x >> 5;
+  const bool main_part = !kPair || !(warp_in_block & 1);
+  const bool comp_part = ad.compensated && (!kPair || (warp_in_block & 1));
+  // element groups of 32: one per warp, or one per warp pair
+  const int groups_per_block = kPair ? (int)(blockDim.x >> 6) : (int)(blockDim.x >> 5);
+  const int group = block * groups_per_block + (kPair ? warp_in_block >> 1 : warp_in_block);
+  const int n_groups = a.n_blocks * groups_per_block;
+  __shared__ double2 handed[2][kPair ? 16 : 1][32];  // the odd warps' sums, by trip parity
   double v[1] = {0.0};
-  for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
-    // the accept of the trial before, when the host left it to this pass: the new state and
-    // the source row of its free slot (which this trial's stencil reads as its newest row)
-    double2 y;
-    if (ad.settle) {
-      const double2 adv = a.advanced[i];
-      y = a.active_mask[i % a.n_omega] ? adv : make_double2(adv.x * 0.0, adv.y * 0.0);
-      a.state[i] = y;
-      a.store[(size_t)(ad.settle - 1) * a.n + i] = a.source[i];
-    } else {
-      y = a.state[i];
-    }
-    // every operand row of this element is loaded up front, so that the loads overlap
-    // one another and the phi functions instead of waiting in the loops below
-    constexpr int kRows = 5;  // the Adams order is at most 5: order and width - 1 rows
-    double2 rows[kRows], rate_rows[kRows], state_rows[kRows];
-#pragma unroll
-    for (int j = 0; j < kRows; ++j) {
-      if (j < order) rows[j] = a.store[(size_t)ad.slots[j] * a.n + i];
-      if (ad.compensated && j < width - 1) {
-        rate_rows[j] = a.rates[(size_t)ad.slots[j] * a.n + i];
-        state_rows[j] = a.states[(size_t)ad.slots[j] * a.n + i];
-      }
-    }
-    double2 x, rate_end = make_double2(0.0, 0.0);
-    if (ad.compensated) combine_two(st.phi_w, ad.rate_w, st.n_phi, a.phi_terms, a.n, i, x, rate_end);
-    else x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
-    double2 phi[kMaxWidth + 1];
-    phi_functions(x, width, phi);
-    // beyond |x| = 3 the recurrence started from exp(x) itself
-    const double2 fl = x.x * x.x + x.y * x.y > 9.0 ? phi[0] : cexp(x);
-    double fact = 1.0;
-    double2 mom[kMaxWidth];
-#pragma unroll
-    for (int k = 0; k < kMaxWidth; ++k) {
-      if (k >= width) break;
-      if (k > 0) fact *= (double)k;
-      mom[k] = cscale(fact, phi[k + 1]);
-      a.moments[(size_t)k * a.n + i] = mom[k];
-    }
-    a.flow[i] = fl;
-    a.exponent[i] = x;
-    double2 total = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int k = 0; k < kRows; ++k) {
-      if (k >= order) break;
-      double2 comb = make_double2(0.0, 0.0);
+  int trip = 0;
+  for (int base = group * 32; base < a.n; base += n_groups * 32, ++trip) {
+    const int i = base + lane;
+    const bool valid = i < a.n;
+    double2 x = make_double2(0.0, 0.0), rate_end = make_double2(0.0, 0.0);
+    double2 comp = make_double2(0.0, 0.0), lab = make_double2(0.0, 0.0), y = make_double2(0.0, 0.0);
+    constexpr int kRows = 5;  // the Adams order is at most 5
+    double2 rate_rows[kRows], state_rows[kRows];
+    if (valid && comp_part) {  // loaded first, to overlap with the loads and work below
 #pragma unroll
       for (int j = 0; j < kRows; ++j) {
-        if (j >= order) break;
-        const double c = ad.pred[j][k];
-        if (c != 0.0) comb = cadd(comb, cscale(c, rows[j]));
+        if (j < width - 1) {
+          rate_rows[j] = a.rates[(size_t)ad.slots[j] * a.n + i];
+          state_rows[j] = a.states[(size_t)ad.slots[j] * a.n + i];
+        }
       }
-      total = cadd(total, cmul(mom[k], comb));
     }
-    double2 lab = cadd(cmul(fl, y), cscale(ad.dz, total));
-    if (ad.compensated) {
+    if (valid && main_part) {
+      // the accept of the trial before, when the host left it to this pass: the new state
+      // and the source row of its free slot (which this trial's stencil reads as its newest
+      // row)
+      if (ad.settle) {
+        const double2 adv = a.advanced[i];
+        y = a.active_mask[i % a.n_omega] ? adv : make_double2(adv.x * 0.0, adv.y * 0.0);
+        a.state[i] = y;
+        a.store[(size_t)(ad.settle - 1) * a.n + i] = a.source[i];
+      } else {
+        y = a.state[i];
+      }
+      // every operand row is loaded up front, so that the loads overlap one another and the
+      // phi functions instead of waiting in the loops below
+      double2 rows[kRows];
+#pragma unroll
+      for (int j = 0; j < kRows; ++j)
+        if (j < order) rows[j] = a.store[(size_t)ad.slots[j] * a.n + i];
+      if (comp_part) combine_two(st.phi_w, ad.rate_w, st.n_phi, a.phi_terms, a.n, i, x, rate_end);
+      else x = combine_terms(st.phi_w, st.n_phi, a.phi_terms, a.n, i);
+      double2 phi[kMaxWidth + 1];
+      phi_functions(x, width, phi);
+      // beyond |x| = 3 the recurrence started from exp(x) itself
+      const double2 fl = x.x * x.x + x.y * x.y > 9.0 ? phi[0] : cexp(x);
+      double fact = 1.0;
+      double2 mom[kMaxWidth];
+#pragma unroll
+      for (int k = 0; k < kMaxWidth; ++k) {
+        if (k >= width) break;
+        if (k > 0) fact *= (double)k;
+        mom[k] = cscale(fact, phi[k + 1]);
+        a.moments[(size_t)k * a.n + i] = mom[k];
+      }
+      a.flow[i] = fl;
+      a.exponent[i] = x;
+      double2 total = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < kRows; ++k) {
+        if (k >= order) break;
+        double2 comb = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < kRows; ++j) {
+          if (j >= order) break;
+          const double c = ad.pred[j][k];
+          if (c != 0.0) comb = cadd(comb, cscale(c, rows[j]));
+        }
+        total = cadd(total, cmul(mom[k], comb));
+      }
+      lab = cadd(cmul(fl, y), cscale(ad.dz, total));
+    } else if (valid && comp_part) {
+      combine_two(st.phi_w, ad.rate_w, st.n_phi, a.phi_terms, a.n, i, x, rate_end);
+    }
+    if (valid && comp_part) {
       // D(z + dz) = sum_p r_p terms_p, contracted always (translate/linop.py:2332-2334), for
       // the corrector's endpoint; it and the predicted state go to the free slot's rows
       // (adams_kernels.py accept), which no row of this trial's stencil reads
       a.rates[(size_t)ad.free_slot * a.n + i] = rate_end;
       // carried rows exp((1 - theta_j) x) ((D(z_j) - x/dz) u_j)   (adams_kernels.py carry)
       const double2 ref = make_double2(x.x / ad.dz, x.y / ad.dz);
-      double2 comp = make_double2(0.0, 0.0);
 #pragma unroll
       for (int j = 0; j < kRows; ++j) {
         if (j >= width - 1) break;
@@ -283,12 +310,21 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
         a.carried[(size_t)j * a.n + i] = c;
         if (j < order) comp = cadd(comp, cscale(ad.comp_pred_main[j], c));
       }
-      lab = cadd(lab, cscale(ad.dz, comp));
     }
-    a.lab[i] = lab;
-    if (ad.compensated) a.states[(size_t)ad.free_slot * a.n + i] = lab;
-    const int bin = i % a.n_omega;
-    if (a.norm_mask[bin]) v[0] += y.x * y.x + y.y * y.y;
+    if (kPair) {
+      double2* slot = &handed[trip & 1][warp_in_block >> 1][lane];
+      if (!main_part) *slot = comp;
+      // the pair's two warps: barrier 1 + pair index, 64 threads
+      asm volatile("bar.sync %0, 64;" ::"r"(1 + (warp_in_block >> 1)) : "memory");
+      if (main_part) comp = *slot;
+    }
+    if (valid && main_part) {
+      if (ad.compensated) lab = cadd(lab, cscale(ad.dz, comp));
+      a.lab[i] = lab;
+      if (ad.compensated) a.states[(size_t)ad.free_slot * a.n + i] = lab;
+      const int bin = i % a.n_omega;
+      if (a.norm_mask[bin]) v[0] += y.x * y.x + y.y * y.y;
+    }
   }
   block_partials<1>(v, a.partials + (size_t)kMaxOrders * kNormBlocks, block);
 }
@@ -415,7 +451,9 @@ __device__ __forceinline__ void adams_start_body(const StepArgs& a, int write_ra
 // operand rows in registers.  Batched, the passes stream far more than L2 holds and are
 // bound by HBM: the register budget is capped so that more warps keep loads in flight.
 constexpr int kStepThreads = 128;
-__global__ void __launch_bounds__(kStepThreads) k_adams_predict(StepArgs a) { adams_predict_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(2 * kStepThreads) k_adams_predict(StepArgs a) {
+  adams_predict_body<true>(a, blockIdx.x);
+}
 __global__ void __launch_bounds__(kStepThreads) k_adams_correct(StepArgs a) {
   adams_correct_body(a, blockIdx.x);
   if (a.norm_arrivals) reduce_if_last(a, kMaxOrders + 1);
@@ -428,7 +466,7 @@ __global__ void __launch_bounds__(256, 2) k_adams_predict_b(const StepArgs* args
                                                            const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  adams_predict_body(own_args(args, it.x), it.y);
+  adams_predict_body<false>(own_args(args, it.x), it.y);
 }
 __global__ void __launch_bounds__(256, 4) k_adams_correct_b(const StepArgs* args, const int2* items,
                                                            const int* flags) {
@@ -450,7 +488,7 @@ __global__ void k_adams_start_b(const StepArgs* args, const int2* items, const i
 }
 
 cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t s) {
-  k_adams_predict<<<a.n_blocks, kStepThreads, 0, s>>>(a);
+  k_adams_predict<<<a.n_blocks, 2 * kStepThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
 cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t s) {
