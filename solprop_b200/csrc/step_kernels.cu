@@ -332,11 +332,20 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
 // ------------------------------------------------------------------ Adams correct
 // Every loop runs to the compile-time bound (kMaxWidth, kMaxOrders) and stops at the
 // trial's width and order count, so the operand rows stay in registers.
+// kPair: two warps per 32 elements (a single run): the even warp forms the advanced state,
+// the odd warp the defect norms; they share only their loads.
+template <bool kPair>
 __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block) {
   const AdamsDev& ad = staged_adams(a.adams);
   const int width = ad.width, n_orders = ad.n_orders;
+  const int lane = threadIdx.x & 31, warp_in_block = threadIdx.x >> 5;
+  const bool adv_part = !kPair || !(warp_in_block & 1);
+  const bool norm_part = !kPair || (warp_in_block & 1);
+  const int groups_per_block = kPair ? (int)(blockDim.x >> 6) : (int)(blockDim.x >> 5);
+  const int group = block * groups_per_block + (kPair ? warp_in_block >> 1 : warp_in_block);
+  const int n_groups = a.n_blocks * groups_per_block;
   double v[kMaxOrders] = {0.0, 0.0, 0.0};
-  for (int i = block * blockDim.x + threadIdx.x; i < a.n; i += a.n_blocks * blockDim.x) {
+  for (int i = group * 32 + lane; i < a.n; i += n_groups * 32) {
     double2 xs[kMaxWidth], mom[kMaxWidth];
     xs[0] = a.source[i];
 #pragma unroll
@@ -349,21 +358,6 @@ __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block)
       if (k >= width) break;
       mom[k] = a.moments[(size_t)k * a.n + i];
     }
-    // advanced = flow u + dz sum_k M_k sum_j corr_jk X_j
-    double2 total = make_double2(0.0, 0.0);
-#pragma unroll
-    for (int k = 0; k < kMaxWidth; ++k) {
-      if (k >= width) break;
-      double2 comb = make_double2(0.0, 0.0);
-#pragma unroll
-      for (int j = 0; j < kMaxWidth; ++j) {
-        if (j >= width) break;
-        const double c = ad.corr[j][k];
-        if (c != 0.0) comb = cadd(comb, cscale(c, xs[j]));
-      }
-      total = cadd(total, cmul(mom[k], comb));
-    }
-    double2 adv = cadd(cmul(a.flow[i], a.state[i]), cscale(ad.dz, total));
     double2 endpoint = make_double2(0.0, 0.0);
     double2 carried[kMaxWidth];
     if (ad.compensated) {
@@ -377,16 +371,36 @@ __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block)
         if (j >= width - 1) break;
         carried[j] = a.carried[(size_t)j * a.n + i];
       }
-      double2 c = cscale(ad.comp_corr_main[0], endpoint);
-      double2 t = make_double2(0.0, 0.0);
-#pragma unroll
-      for (int j = 0; j < kMaxWidth - 1; ++j) {
-        if (j >= ad.order) break;
-        t = cadd(t, cscale(ad.comp_corr_main[j + 1], carried[j]));
-      }
-      adv = cadd(adv, cscale(ad.dz, cadd(t, c)));
     }
-    a.advanced[i] = adv;
+    if (adv_part) {
+      // advanced = flow u + dz sum_k M_k sum_j corr_jk X_j
+      double2 total = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < kMaxWidth; ++k) {
+        if (k >= width) break;
+        double2 comb = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < kMaxWidth; ++j) {
+          if (j >= width) break;
+          const double c = ad.corr[j][k];
+          if (c != 0.0) comb = cadd(comb, cscale(c, xs[j]));
+        }
+        total = cadd(total, cmul(mom[k], comb));
+      }
+      double2 adv = cadd(cmul(a.flow[i], a.state[i]), cscale(ad.dz, total));
+      if (ad.compensated) {
+        double2 c = cscale(ad.comp_corr_main[0], endpoint);
+        double2 t = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int j = 0; j < kMaxWidth - 1; ++j) {
+          if (j >= ad.order) break;
+          t = cadd(t, cscale(ad.comp_corr_main[j + 1], carried[j]));
+        }
+        adv = cadd(adv, cscale(ad.dz, cadd(t, c)));
+      }
+      a.advanced[i] = adv;
+    }
+    if (!norm_part) continue;
     const int bin = i % a.n_omega;
     const bool scored = a.norm_mask[bin];
 #pragma unroll
@@ -454,8 +468,8 @@ constexpr int kStepThreads = 128;
 __global__ void __launch_bounds__(2 * kStepThreads) k_adams_predict(StepArgs a) {
   adams_predict_body<true>(a, blockIdx.x);
 }
-__global__ void __launch_bounds__(kStepThreads) k_adams_correct(StepArgs a) {
-  adams_correct_body(a, blockIdx.x);
+__global__ void __launch_bounds__(2 * kStepThreads) k_adams_correct(StepArgs a) {
+  adams_correct_body<true>(a, blockIdx.x);
   if (a.norm_arrivals) reduce_if_last(a, kMaxOrders + 1);
 }
 __global__ void k_adams_accept(StepArgs a, int free_slot) { adams_accept_body(a, free_slot, blockIdx.x); }
@@ -472,7 +486,7 @@ __global__ void __launch_bounds__(256, 4) k_adams_correct_b(const StepArgs* args
                                                            const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  adams_correct_body(own_args(args, it.x), it.y);
+  adams_correct_body<false>(own_args(args, it.x), it.y);
 }
 __global__ void k_adams_accept_b(const StepArgs* args, const int2* items, const int* flags) {
   const int2 it = items[blockIdx.x];
@@ -492,7 +506,7 @@ cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t s) {
-  k_adams_correct<<<a.n_blocks, kStepThreads, 0, s>>>(a);
+  k_adams_correct<<<a.n_blocks, 2 * kStepThreads, 0, s>>>(a);
   if (!a.norm_arrivals) k_reduce<<<kMaxOrders + 1, 32, 0, s>>>(a.partials, a.norms, kMaxOrders + 1, a.n_blocks);
   return cudaGetLastError();
 }
