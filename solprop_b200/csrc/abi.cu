@@ -538,6 +538,7 @@ static ColumnArgsT<R> column_args(const sp_workspace* ws, const StageScalarsDev*
   ca.n_tiles = column_tiles(d);
   ca.n_groups = (d.n_nodes + kGroup - 1) / kGroup;
   ca.n_blocks = ca.n_tiles * ca.n_groups;
+  ca.group_sum = 0;  // a single run's forward transform adds the node groups' rows
   ca.kerr = d.kerr_enabled;
   ca.plasma = d.plasma_enabled;
   ca.band = d.band;
@@ -574,8 +575,10 @@ static ForwardArgsT<R> forward_args(const sp_workspace* ws) {
   const sp_problem_desc& d = P.d;
   const int nc = P.n_cols;
   const SourceView<R> v = source_view<R>(ws);
-  // the response column leaves the node groups' sum in group 0's rows
-  return ForwardArgsT<R>{ws->streams.p, v.proj, 1, 3 * nc,
+  // the response column leaves a partial row per node group (the products: group 0's rows
+  // alone), which the transform adds in group order
+  const int n_groups = ws->gemm ? 1 : (d.n_nodes + kGroup - 1) / kGroup;
+  return ForwardArgsT<R>{ws->streams.p, v.proj, n_groups, 3 * nc,
                          d.plasma_enabled ? ws->rows.p : ws->rows.p + 4 * nc,
                          ws->crop.p, v.twiddles, v.spectra, d.n_to, d.n_omega, ws->log_m,
                          ws->log_n_to, P.crop_identity};
@@ -3148,11 +3151,13 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
       cs[r] = column_args(w, S->stages_start.p + r);
       ca[r] = column_args(w, S->stages_att.p + 2 * r + 1);
       cs[r].status = ca[r].status = S->norms.p + 8 * r + kColumnStatus;
+      cs[r].group_sum = ca[r].group_sum = 1;  // the batched forward reads group 0's rows after it
       fa[r] = forward_args(w);
       if (precision == SP_PRECISION_MIXED) {
         cs32[r] = column_args<float>(w, S->stages_start.p + r);
         ca32[r] = column_args<float>(w, S->stages_att.p + 2 * r + 1);
         cs32[r].status = ca32[r].status = S->norms.p + 8 * r + kColumnStatus;
+        cs32[r].group_sum = ca32[r].group_sum = 1;
         fa32[r] = forward_args<float>(w);
       }
       os[r] = output_args(w, S->stages_start.p + r, nullptr, w->src.p, absorber);

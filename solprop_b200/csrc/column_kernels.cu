@@ -754,10 +754,11 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       }
     }
   }
-  // The tile's node groups: the last of its n_groups CTAs to arrive adds the groups'
-  // partial rows in group order into group 0's (the forward transform reads those).
-  // Arrivals count up by n_groups per evaluation, so the counter needs no reset.
-  if (!kSweep && a.n_groups > 1) {
+  // The tile's node groups (group_sum): the last of its n_groups CTAs to arrive adds the
+  // groups' partial rows in group order into group 0's (the forward transform reads those).
+  // Arrivals count up by n_groups per evaluation, so the counter needs no reset.  Without
+  // group_sum the forward transform adds them, in the same order.
+  if (!kSweep && a.group_sum && a.n_groups > 1) {
     __shared__ int last;
     __threadfence();
     __syncthreads();

@@ -165,15 +165,28 @@ __device__ __forceinline__ void forward_cluster_body(const ForwardArgsT<R>& a, i
   const int slice = Mp / C;
   // z[C n2 + r] = x[2(C n2 + r)] + i x[2(C n2 + r) + 1]
   if (row < a.n_partial_rows) {
-#pragma unroll 4
+    // a projected stream: the node groups' partial rows summed in group order, eight
+    // groups' loads issued before their sums
+    constexpr int kBatch = 8;
+    const Cx* rows = reinterpret_cast<const Cx*>(a.partials + (size_t)row * a.n_to);
+    const size_t group_stride = (size_t)a.n_partial_rows * a.n_to / 2;  // in complex samples
+#pragma unroll 2
     for (int n2 = threadIdx.x; n2 < Mp; n2 += blockDim.x) {
       const int m = C * n2 + r;
       Cx acc;
       acc.x = R(0);
       acc.y = R(0);
-      for (int g = 0; g < a.n_groups; ++g)
-        acc = cadd(acc, reinterpret_cast<const Cx*>(
-                            a.partials + ((size_t)g * a.n_partial_rows + row) * a.n_to)[m]);
+      for (int g0 = 0; g0 < a.n_groups; g0 += kBatch) {
+        Cx x[kBatch];
+#pragma unroll
+        for (int g = 0; g < kBatch; ++g)
+          if (g0 + g < a.n_groups) x[g] = __ldg(rows + (size_t)(g0 + g) * group_stride + m);
+#pragma unroll
+        for (int g = 0; g < kBatch; ++g) {
+          if (g0 + g >= a.n_groups) break;
+          acc = cadd(acc, x[g]);
+        }
+      }
       sc[row_slot<Cx>(n2)] = acc;
     }
   } else {
