@@ -59,8 +59,11 @@ def algorithmic_bytes(rec) -> dict:
 
     The response column reads the modal field and the two temporal windows once and writes
     the projected streams (and its tiles' running-integral sums); nothing node-sized is
-    stored, and the node groups' partial rows (summed by the tile's last CTA) are not counted.
-    The forward transform reads the projected streams and writes the spectra.
+    stored, and the node groups' partial rows beyond one (added by the forward transform)
+    are not counted.  The forward transform reads the projected streams and writes the
+    spectra.  The corrector forms the stage output itself (its streams, prefactor terms and
+    source row are counted with it), and the predictor applies the accept of the trial
+    before (its rows are counted with it).
     """
     n = rec.n_cols * rec.n_omega
     c128, f64 = 16, 8
@@ -72,13 +75,12 @@ def algorithmic_bytes(rec) -> dict:
     absorber = 1 if rec.absorber_scheme == "nonlinear" else 0
     projected = streams * nc * nt * f64
     return {
-        "adams_predict": 14 * n * c128,
+        "adams_predict": 14 * n * c128 + 4 * n * c128,
         "inverse_fft": n * c128 + (1 + absorber) * nc * nt * f64 + absorber * nt * f64,
         "response_column": nc * nt * f64 + 2 * nt * f64 + 2 * nn * tiles * f64 + projected,
         "forward_fft": projected + absorber * nc * nt * f64 + (streams + absorber) * n * c128,
-        "stage_output": (streams + absorber) * n * c128 + rec.n_prefactor_terms * n * c128 + n * c128,
-        "adams_correct": 15 * n * c128,
-        "adams_accept": 4 * n * c128,
+        "adams_correct": 15 * n * c128 + (streams + absorber) * n * c128
+        + rec.n_prefactor_terms * n * c128 + n * c128,
     }
 
 

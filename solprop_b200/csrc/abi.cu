@@ -780,8 +780,17 @@ static void eval_source_envelope_gemm(sp_workspace* ws, const double2* lab, int 
 }
 
 // One source evaluation at lab (device), stage slot, optional inverse propagator.
+// The stage output's record of a source evaluation (its last pass)
+static OutputArgs source_output_args(const sp_workspace* ws, int slot, const double2* inv_prop, double2* out,
+                                     bool quiet) {
+  const bool absorber = ws->P->d.absorber_in_stage && !quiet;
+  return output_args(ws, ws->stage.p + slot, inv_prop, out, absorber);
+}
+
+// output: false leaves the stage output (the last pass) to the caller's next kernel, which
+// forms it from source_output_args (the single-run corrector)
 static void eval_source(sp_workspace* ws, const double2* lab, int slot, const double2* inv_prop,
-                        double2* out, bool quiet) {
+                        double2* out, bool quiet, bool output = true) {
   const sp_problem& P = *ws->P;
   const bool absorber = P.d.absorber_in_stage && !quiet;
   if (P.d.grid_kind == 1 && ws->gemm) {
@@ -826,7 +835,8 @@ static void eval_source(sp_workspace* ws, const double2* lab, int slot, const do
     const auto fa = forward_args<double>(ws);
     { KernelTimer t(ws, SP_K_FORWARD); CUDA_CHECK(launch_forward(fa, forward_rows(ws, absorber), ws->stream)); }
   }
-  const OutputArgs oa = output_args(ws, ws->stage.p + slot, inv_prop, out, absorber);
+  if (!output) return;
+  const OutputArgs oa = source_output_args(ws, slot, inv_prop, out, quiet);
   { KernelTimer t(ws, SP_K_OUTPUT); CUDA_CHECK(launch_output(oa, ws->stream)); }
 }
 
@@ -1445,8 +1455,9 @@ static void issue_attempt(sp_workspace* ws, const StepArgs& a) {
                              ws->stream));
   CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, ws->h_adams, sizeof(AdamsDev), cudaMemcpyHostToDevice, ws->stream));
   { KernelTimer t(ws, SP_K_PREDICT); CUDA_CHECK(launch_adams_predict(a, ws->stream)); }
-  eval_source(ws, ws->lab.p, 1, nullptr, ws->src.p, false);
-  { KernelTimer t(ws, SP_K_CORRECT); CUDA_CHECK(launch_adams_correct(a, ws->stream)); }
+  eval_source(ws, ws->lab.p, 1, nullptr, ws->src.p, false, /*output=*/false);
+  const OutputArgs oa = source_output_args(ws, 1, nullptr, ws->src.p, false);
+  { KernelTimer t(ws, SP_K_CORRECT); CUDA_CHECK(launch_adams_correct(a, &oa, ws->stream)); }
   CUDA_CHECK(cudaMemcpyAsync(ws->h_norms, ws->norms.p, sizeof(double) * (kColumnStatus + 1),
                              cudaMemcpyDeviceToHost, ws->stream));
 }

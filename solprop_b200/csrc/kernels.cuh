@@ -368,7 +368,9 @@ struct StepArgs {
 };
 
 cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t stream);
-cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t stream);
+// with an output record (non-null), the corrector forms the source row itself: the stage
+// output pass of the source evaluation before it, fused
+cudaError_t launch_adams_correct(const StepArgs& a, const OutputArgs* output, cudaStream_t stream);
 cudaError_t launch_adams_accept(const StepArgs& a, int free_slot, double2* rate_out, cudaStream_t s);
 cudaError_t launch_adams_start(const StepArgs& a, cudaStream_t stream);
 // batched step kernels: which = 0 predict, 1 correct (+ reduction), 2 accept, 3 start

@@ -5,6 +5,7 @@
 // single pass over the state; the norms are two-level deterministic reductions: a fixed
 // grid of kNormBlocks blocks writes one partial per block, one block adds them.
 #include "kernels.cuh"
+#include "stage_output.cuh"
 
 namespace sp {
 
@@ -333,9 +334,11 @@ __device__ __forceinline__ void adams_predict_body(const StepArgs& a, int block)
 // Every loop runs to the compile-time bound (kMaxWidth, kMaxOrders) and stops at the
 // trial's width and order count, so the operand rows stay in registers.
 // kPair: two warps per 32 elements (a single run): the even warp forms the advanced state,
-// the odd warp the defect norms; they share only their loads.
+// the odd warp the defect norms; they share only their loads.  With an output record the
+// source row is formed here from the transformed streams (the stage-output pass, fused) and
+// written by the even warp.
 template <bool kPair>
-__device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block) {
+__device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block, const OutputArgs* output) {
   const AdamsDev& ad = staged_adams(a.adams);
   const int width = ad.width, n_orders = ad.n_orders;
   const int lane = threadIdx.x & 31, warp_in_block = threadIdx.x >> 5;
@@ -347,7 +350,12 @@ __device__ __forceinline__ void adams_correct_body(const StepArgs& a, int block)
   double v[kMaxOrders] = {0.0, 0.0, 0.0};
   for (int i = group * 32 + lane; i < a.n; i += n_groups * 32) {
     double2 xs[kMaxWidth], mom[kMaxWidth];
-    xs[0] = a.source[i];
+    if (output) {
+      xs[0] = stage_output_value(*output, i);
+      if (adv_part) output->out[i] = xs[0];
+    } else {
+      xs[0] = a.source[i];
+    }
 #pragma unroll
     for (int j = 1; j < kMaxWidth; ++j) {
       if (j >= width) break;
@@ -468,8 +476,8 @@ constexpr int kStepThreads = 128;
 __global__ void __launch_bounds__(2 * kStepThreads) k_adams_predict(StepArgs a) {
   adams_predict_body<true>(a, blockIdx.x);
 }
-__global__ void __launch_bounds__(2 * kStepThreads) k_adams_correct(StepArgs a) {
-  adams_correct_body<true>(a, blockIdx.x);
+__global__ void __launch_bounds__(2 * kStepThreads) k_adams_correct(StepArgs a, const __grid_constant__ OutputArgs o) {
+  adams_correct_body<true>(a, blockIdx.x, o.out ? &o : nullptr);
   if (a.norm_arrivals) reduce_if_last(a, kMaxOrders + 1);
 }
 __global__ void k_adams_accept(StepArgs a, int free_slot) { adams_accept_body(a, free_slot, blockIdx.x); }
@@ -486,7 +494,7 @@ __global__ void __launch_bounds__(256, 4) k_adams_correct_b(const StepArgs* args
                                                            const int* flags) {
   const int2 it = items[blockIdx.x];
   if (!flags[it.x]) return;
-  adams_correct_body<false>(own_args(args, it.x), it.y);
+  adams_correct_body<false>(own_args(args, it.x), it.y, nullptr);
 }
 __global__ void k_adams_accept_b(const StepArgs* args, const int2* items, const int* flags) {
   const int2 it = items[blockIdx.x];
@@ -505,8 +513,8 @@ cudaError_t launch_adams_predict(const StepArgs& a, cudaStream_t s) {
   k_adams_predict<<<a.n_blocks, 2 * kStepThreads, 0, s>>>(a);
   return cudaGetLastError();
 }
-cudaError_t launch_adams_correct(const StepArgs& a, cudaStream_t s) {
-  k_adams_correct<<<a.n_blocks, 2 * kStepThreads, 0, s>>>(a);
+cudaError_t launch_adams_correct(const StepArgs& a, const OutputArgs* output, cudaStream_t s) {
+  k_adams_correct<<<a.n_blocks, 2 * kStepThreads, 0, s>>>(a, output ? *output : OutputArgs{});
   if (!a.norm_arrivals) k_reduce<<<kMaxOrders + 1, 32, 0, s>>>(a.partials, a.norms, kMaxOrders + 1, a.n_blocks);
   return cudaGetLastError();
 }
