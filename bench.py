@@ -40,8 +40,8 @@ sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "config2"
 # DRAM bytes read + written per k_column launch on this workload, from one ncu capture
-# (profiles/k_column_config2.md: 953 600 B read, 1 280 B written; the rest stays in L2)
-COLUMN_TRAFFIC = 954_880
+# (profiles/k_column_config2.md: 945 920 B read, 2 048 B written; the rest stays in L2)
+COLUMN_TRAFFIC = 947_968
 METRIC = "steps/s (exponential-Adams attempts, plain FP64, config 2 four-mode He capillary)"
 UNIT = "steps/s"
 

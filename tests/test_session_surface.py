@@ -140,3 +140,40 @@ def test_a_snapshot_of_another_problem_is_refused():
         ws.restore(policy(golden("cap4_he"), "adaptive"), snap)
     with pytest.raises(_lib.NativeError, match="not a snapshot"):
         ws.restore(policy(golden("cap4_he"), "adaptive"), b"x" * len(snap))
+
+
+@pytest.mark.parametrize("case", ["config1", "cap4_he"])
+def test_reads_between_attempts_leave_the_run_unchanged(case):
+    """A single run's accepted trial leaves its accept (the new state and the history's
+    source row) to the next trial's predictor; every other reader of the state or the rows
+    writes it first.  Exports, plane statistics, snapshots and workspace source calls after
+    every attempt must see the accepted state and leave the run on the bits of an
+    undisturbed run."""
+    from solprop_b200 import _lib
+
+    rec, ws, session = _session(case)
+    end_a = _to_end(session)
+    final_a = session.export()
+
+    ws2 = _lib.Workspace(_lib.Problem(rec))
+    session2 = ws2.start(policy(golden(case), "adaptive"))
+    lab = np.asarray(rec.field0, dtype=np.complex128)
+    states = []
+    while True:
+        b = session2.advance(1)
+        state = session2.export()  # the accepted state, whatever the next trial does
+        assert np.array_equal(session2.export(), state)
+        states.append(state)
+        k = len(states)
+        if k % 3 == 0:
+            session2.statistics()
+        if k % 5 == 0:
+            ws2.source(lab, b.z)
+        if k % 7 == 0:
+            session2.snapshot()
+        if b.event in (2, 3):
+            break
+    assert b.event == 2 and (b.attempts, b.rejected) == (end_a.attempts, end_a.rejected)
+    assert np.array_equal(session2.export(), final_a)
+    # a rejected trial leaves the state as it was; an accepted one moves it
+    assert any(not np.array_equal(states[i], states[i + 1]) for i in range(len(states) - 1))
