@@ -291,7 +291,6 @@ struct sp_workspace {
       rate_coeff, taps, modal_t, streams, sums0, sums1, proj;
   DevBuf<long long> crop;
   DevBuf<int> fine_to_coarse, rows, chain_flags;
-  DevBuf<unsigned> arrivals;
   DevBuf<unsigned long long> ticket;  // the response column's tile counter
   DevBuf<double2> env_twiddles;       // envelope route: exp(-2 pi i m / (2 n_to)), m < n_to
   DevBuf<double> raman_undamped, raman_weights;
@@ -525,7 +524,6 @@ static ColumnArgsT<R> column_args(const sp_workspace* ws, const StageScalarsDev*
   ca.sums1 = ws->sums1.p;
   ca.ticket = ws->ticket.p;
   ca.flags = ws->chain_flags.p;
-  ca.arrivals = ws->arrivals.p;
   ca.status = ws->norms.p + kColumnStatus;
   ca.partials = v.proj;
   ca.n_modes = d.n_modes;
@@ -538,7 +536,6 @@ static ColumnArgsT<R> column_args(const sp_workspace* ws, const StageScalarsDev*
   ca.n_tiles = column_tiles(d);
   ca.n_groups = (d.n_nodes + kGroup - 1) / kGroup;
   ca.n_blocks = ca.n_tiles * ca.n_groups;
-  ca.group_sum = 0;  // a single run's forward transform adds the node groups' rows
   ca.kerr = d.kerr_enabled;
   ca.plasma = d.plasma_enabled;
   ca.band = d.band;
@@ -989,8 +986,6 @@ static void build_workspace(sp_workspace* ws) {
   ws->sums1.alloc((size_t)d.n_nodes * n_tiles);
   ws->chain_flags.alloc(n_groups * n_tiles);
   ws->chain_flags.zero(s);
-  ws->arrivals.alloc(n_tiles);
-  ws->arrivals.zero(s);
   ws->ticket.alloc(1);
   ws->ticket.zero(s);
   ws->proj.alloc((ws->gemm ? 1 : n_groups) * 3 * P.n_cols * d.n_to);
@@ -2707,14 +2702,13 @@ void tune_column(sp_scan* S, const ColumnArgsT<R>* col, const std::vector<int>& 
   CUDA_CHECK(cudaStreamSynchronize(S->stream));
 }
 
-// The forward records for the column's form: the sweep leaves every node group's partial
-// rows for the forward transform to add, the tile-parallel column leaves their sum in
-// group 0's rows.  A captured attempt graph holds the old launches and is dropped.
+// The column's form: both leave every node group's partial rows for the forward transform
+// to add (in group order).  A captured attempt graph holds the old launches and is dropped.
 void set_column_form(sp_scan* S, bool sweep) {
   S->column_sweep = sweep;
   for (int r = 0; r < S->R; ++r) {
-    S->h_fwd[r].n_groups = sweep ? S->groups[r] : 1;
-    S->h_fwd32[r].n_groups = sweep ? S->groups[r] : 1;
+    S->h_fwd[r].n_groups = S->groups[r];
+    S->h_fwd32[r].n_groups = S->groups[r];
   }
   upload_all(S->fwd, S->h_fwd.data(), S->R, S->stream);
   if (S->precision == SP_PRECISION_MIXED) upload_all(S->fwd32, S->h_fwd32.data(), S->R, S->stream);
@@ -3162,13 +3156,11 @@ sp_status sp_scan_create_ex(int32_t n_runs, const sp_problem* const* problems, c
       cs[r] = column_args(w, S->stages_start.p + r);
       ca[r] = column_args(w, S->stages_att.p + 2 * r + 1);
       cs[r].status = ca[r].status = S->norms.p + 8 * r + kColumnStatus;
-      cs[r].group_sum = ca[r].group_sum = 1;  // the batched forward reads group 0's rows after it
       fa[r] = forward_args(w);
       if (precision == SP_PRECISION_MIXED) {
         cs32[r] = column_args<float>(w, S->stages_start.p + r);
         ca32[r] = column_args<float>(w, S->stages_att.p + 2 * r + 1);
         cs32[r].status = ca32[r].status = S->norms.p + 8 * r + kColumnStatus;
-        cs32[r].group_sum = ca32[r].group_sum = 1;
         fa32[r] = forward_args<float>(w);
       }
       os[r] = output_args(w, S->stages_start.p + r, nullptr, w->src.p, absorber);
@@ -3538,7 +3530,6 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     carve.take(ws.sums0, (size_t)d.n_nodes * n_tiles);
     carve.take(ws.sums1, (size_t)d.n_nodes * n_tiles);
     carve.take(ws.chain_flags, n_groups * n_tiles);
-    carve.take(ws.arrivals, n_tiles);
     carve.take(ws.ticket, 1);
     carve.take(ws.norms, kMaxOrders + 2);
     carve.take(ws.proj, n_groups * 3 * P.n_cols * d.n_to);
@@ -3585,7 +3576,6 @@ extern "C" sp_status sp_source_noalloc(const sp_problem* problem, const void* la
     ws.spectra.zero(s);
     ws.proj.zero(s);
     ws.chain_flags.zero(s);
-    ws.arrivals.zero(s);
     ws.ticket.zero(s);
     ws.norms.zero(s);
     ensure_configured(device);

@@ -16,8 +16,9 @@
 // order once they are published, and rescans its window from that offset.  The sums are
 // FP64 in both precisions (the mixed form's compensated integral).  The tile then forms
 // the total current, the Kerr cubic and the temporal collar, and projects the owned
-// samples onto the modes (partial sums per node group, added in group order by the tile's
-// last CTA).  Every sum has a fixed order, so the results are reproducible bit for bit.
+// samples onto the modes (a partial row per node group, added in group order by the
+// forward transform).  Every sum has a fixed order, so the results are reproducible bit for
+// bit.
 #include "kernels.cuh"
 
 namespace sp {
@@ -435,8 +436,8 @@ __device__ __forceinline__ void mixture_plasma(const ColumnArgsT<R>& a, const St
 
 // One tile of one node group: the window's synthesis, rate, running integrals, outputs and
 // projection.  kSweep = false: the tile is one CTA's whole work and learns its running
-// integrals' offsets from its predecessors' published sums (the hand-over above); the
-// node groups' projections are added by the tile's last CTA.  kSweep = true: one CTA walks
+// integrals' offsets from its predecessors' published sums (the hand-over above).
+// kSweep = true: one CTA walks
 // a node group through all tiles in order, so the offsets are its own running sums,
 // carried per lane -- lane l holds the sum of tiles l, l + 32, ... added in tile order,
 // the association predecessors() uses, so both forms give the same bits -- and every
@@ -754,30 +755,7 @@ __device__ __forceinline__ void column_tile(const ColumnArgsT<R>& a, int tile, i
       }
     }
   }
-  // The tile's node groups (group_sum): the last of its n_groups CTAs to arrive adds the
-  // groups' partial rows in group order into group 0's (the forward transform reads those).
-  // Arrivals count up by n_groups per evaluation, so the counter needs no reset.  Without
-  // group_sum the forward transform adds them, in the same order.
-  if (!kSweep && a.group_sum && a.n_groups > 1) {
-    __shared__ int last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const unsigned arrived = atomicAdd(a.arrivals + tile, 1u);
-      last = (arrived % (unsigned)a.n_groups) == (unsigned)(a.n_groups - 1);
-    }
-    __syncthreads();
-    if (last && mine) {
-      __threadfence();
-      for (int s = 0; s < n_streams; ++s)
-        for (int m = 0; m < n_modes; ++m) {
-          R* out = base + ((size_t)s * n_cols + m) * n_to;
-          R acc = R(0);
-          for (int g = 0; g < a.n_groups; ++g) acc = acc + __ldcg(out + g * row_of_group);
-          *out = acc;
-        }
-    }
-  }
+  // the node groups' partial rows stay apart: the forward transform adds them in group order
 }
 
 template <class R, bool kNodes = false, bool kMulti = false>

@@ -114,12 +114,9 @@ struct ColumnArgsT {
   double* sums1;           // current tile sums
   unsigned long long* ticket;  // tiles handed out so far (n_blocks per evaluation)
   int* flags;              // (n_groups, n_tiles) publication stage of each tile
-  unsigned* arrivals;      // (n_tiles) node-group CTAs of each tile done so far
   double* status;          // set to 1 when a tile gave up waiting
   R* partials;             // (n_groups, 3, n_cols, n_to) projected streams per node group
   int n_modes, n_nodes, n_cols, n_to, n_tiles, n_groups, n_blocks;
-  int group_sum;           // tile-parallel: 1, the tile's last CTA adds the node groups' partial
-                           // rows into group 0's; 0, the forward transform adds them
   int lead, owned;         // a window's halo and owned samples (column_lead, column_owned)
   int kerr, plasma, band, half_width, rate_intervals;
   double kerr_coefficient, charge_mass_ratio, ionisation_potential, dt;
