@@ -218,7 +218,7 @@ def surrogate_leg(device: int, points: int = 16384, members: int = 5, repeats: i
         torch.cuda.synchronize()
         return s_ev.elapsed_time(e_ev) / repeats
 
-    ms_tc = timed(lambda: [m.infer(x, status) for m in ens.members])
+    ms_tc = timed(lambda: ens.infer(x, status))  # each layer: every member in one launch
     ms_mma = timed(lambda: [m.forward(x) for m in ens.members])
     if int(status.item()):
         raise RuntimeError("a tensor-core product's wait gave up")

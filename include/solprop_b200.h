@@ -422,6 +422,12 @@ sp_status sp_mlp_gemm(const float* A, int lda, int transA, const float* B, int l
 sp_status sp_mlp_gemm_tc(const void* A, int lda, const void* W, int ldw, float* C, int ldc,
                          void* C16, int ldc16, int M, int N, int K, const float* bias,
                          int epilogue, int* status, void* stream);
+/* The same product for `count` (1..8) operand and output sets of one shape in one launch
+ * (an ensemble's members through one layer): A[q], W[q], C[q] / C16[q] (NULL arrays or
+ * entries where unused), bias[q] (or bias NULL). */
+sp_status sp_mlp_gemm_tc_batch(int count, const void* const* A, int lda, const void* const* W, int ldw,
+                               float* const* C, int ldc, void* const* C16, int ldc16, int M, int N, int K,
+                               const float* const* bias, int epilogue, int* status, void* stream);
 /* The transpose of a (rows, cols) FP32 (src_bf16 0) or BF16 (1) matrix as BF16,
  * dst[c * ld_dst + r], zero-padded from rows to rows_pad: the operands of the training's
  * weight and input gradients as products C = A W^T on the tensor cores. */

@@ -2,15 +2,16 @@
 //
 //   C[M, N] = A[M, K] W[N, K]^T (+ bias[n]) (GELU)     A, W: BF16, K contiguous, in HBM
 //
-// One CTA of sixteen warps computes a 128 x 256 tile.  The tensor memory accelerator brings
-// 64-wide K slices of A (128 rows) and W (256 rows) into shared memory, swizzled by 128
-// bytes, through a four-stage ring guarded by mbarriers; one thread issues tcgen05.mma
-// (kind::f16: BF16 operands, FP32 accumulation) for each 16-wide K step into a 128 x 256
-// FP32 accumulator held in tensor memory, and commits each stage back to its producer.
-// When the ring drains, each warp reads its 32 rows of the accumulator with tcgen05.ld and
-// applies the epilogue (bias, GELU, FP32 and/or BF16 stores).  Every mbarrier wait is
-// bounded: a wait that gives up sets *status, and the CTA still releases its tensor memory
-// before it returns.  No load is multicast.
+// A persistent CTA per SM (ten warps) computes 128 x 256 tiles in turn.  The tensor memory
+// accelerator brings 64-wide K slices of A (128 rows) and W (256 rows) into shared memory,
+// swizzled by 128 bytes, through a four-stage ring guarded by mbarriers; one thread issues
+// tcgen05.mma (kind::f16: BF16 operands, FP32 accumulation) for each 16-wide K step into a
+// 128 x 256 FP32 accumulator in tensor memory -- two of them, alternating by tile -- and
+// commits each stage back to its producer.  Eight warps drain the other accumulator with
+// tcgen05.ld meanwhile and apply the epilogue (bias, GELU, FP32 and/or BF16 stores, staged
+// through shared memory so that rows leave coalesced).  Every mbarrier wait is bounded: a
+// wait that gives up sets *status, and the CTA still waits for its products and loads and
+// releases its tensor memory before it returns.  No load is multicast.
 //
 // The shared-memory and instruction descriptors follow the sm_100 UMMA formats (K-major,
 // 128-byte swizzle: stride between 8-row groups 1024 bytes; a 16-element K step advances
@@ -28,47 +29,88 @@
 namespace sp {
 namespace {
 
-constexpr int kTM = 128, kTN = 256, kTK = 64, kStages = 4;
-// sixteen warps: one thread of warp 0 feeds the ring, one of warp 1 issues the products, and
-// all sixteen drain the accumulator (warp w reads lanes 32 (w % 4) .. + 31, columns
-// 64 (w / 4) .. + 63), so that the epilogue's arithmetic has warps to hide its latency
-constexpr int kThreads = 512;
-constexpr int kEpilogueColumns = kTN / (kThreads / 128);
+constexpr int kTM = 128, kTN = 256, kTK = 64, kStages = 3;
+// eighteen warps: one thread of warp 0 feeds the ring, one of warp 1 issues the products,
+// and warps 2..17 drain the accumulators (warp w may read tensor-memory lanes 32 (w % 4) ..
+// + 31; warps 2..5 take columns 0..63 of a tile, warps 6..9 columns 64..127, and so on):
+// the epilogue's arithmetic (bias, GELU, conversion) per output is what bounds a tile
+constexpr int kEpilogueWarps = 16;
+constexpr int kThreads = 32 * (2 + kEpilogueWarps);
+constexpr int kEpilogueColumns = kTN / (kEpilogueWarps / 4);
 constexpr uint32_t kABytes = kTM * kTK * 2;  // 16 KB
 constexpr uint32_t kBBytes = kTN * kTK * 2;  // 32 KB
 constexpr uint32_t kStageBytes = kABytes + kBBytes;
-constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + 1024 + 256;
-constexpr uint32_t kTmemColumns = 256;     // the FP32 accumulator: 256 columns x 128 lanes
+constexpr int kStagePitch = 33;  // an epilogue warp's 32 x 32 staging block, rows padded by a word
+constexpr size_t kStagingBytes = (size_t)kEpilogueWarps * 32 * kStagePitch * 4;
+constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + kStagingBytes + 1024 + 256;
+static_assert(kSmemBytes + 64 <= 232448, "the ring, the staging and the barriers fit one CTA");
+constexpr uint32_t kAccColumns = 256;      // one FP32 accumulator: 256 columns x 128 lanes
+constexpr uint32_t kTmemColumns = 2 * kAccColumns;
 constexpr uint32_t kIdesc = tc::idesc_bf16(kTM, kTN);
+constexpr int kMaxProducts = 8;  // products of one launch (the ensemble's members)
 using namespace tc;
+
+// The products of one launch: the same shapes, operands and outputs of their own (the
+// ensemble's members through one layer).  The tensor maps live in the kernel's parameters.
+struct GemmBatch {
+  CUtensorMap a[kMaxProducts], w[kMaxProducts];
+  float* C[kMaxProducts];
+  __nv_bfloat16* C16[kMaxProducts];
+  const float* bias[kMaxProducts];
+  int count;
+};
 
 __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// A persistent CTA per SM walks the output tiles t = blockIdx.x, + gridDim.x, ... of every
+// product of the batch in turn (the column tile fastest, so that the CTAs running together
+// share A's rows in L2).  The ring
+// of K slices runs on across tiles; the products of tile i go to accumulator i % 2, so that
+// the epilogue warps drain one while the next tile's products fill the other:
+//   full[s] / empty[s]   the ring's stages (TMA bytes in / products done reading)
+//   acc_full[b]          the products of accumulator b's tile are complete (commit)
+//   acc_empty[b]         the epilogue warps have read accumulator b (one arrival per warp)
+// Every wait is bounded; a wait that gives up sets `failed`, which the other roles poll, and
+// the CTA waits (bounded) for its own products and loads in flight before it frees its
+// tensor memory.
 __global__ void __launch_bounds__(kThreads, 1)
-    k_mlp_gemm_tc(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_w,
-                  float* C, __nv_bfloat16* C16, const float* bias, int M, int N, int K, int ldc, int ldc16,
-                  int epilogue, int* status) {
-  extern __shared__ __align__(1024) unsigned char tc_raw[];
+    k_mlp_gemm_tc(const __grid_constant__ GemmBatch p, int M, int N, int K, int ldc, int ldc16, int epilogue,
+                  int* status) {
+  extern __shared__ __align__(16) unsigned char tc_raw[];  // aligned to 1024 by hand (the slack)
   unsigned char* ring = reinterpret_cast<unsigned char*>(((uintptr_t)tc_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)kStages * kStageBytes);
+  float* staging = reinterpret_cast<float*>(ring + (size_t)kStages * kStageBytes);
+  uint64_t* full = reinterpret_cast<uint64_t*>(ring + (size_t)kStages * kStageBytes + kStagingBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* done = empty + kStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
-  __shared__ int failed;
+  uint64_t* acc_full = empty + kStages;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* drain = acc_empty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  __shared__ volatile int failed;
+  __shared__ int consumed;  // ring slices the products have taken (for the drain on failure)
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int m0 = blockIdx.y * kTM, n0 = blockIdx.x * kTN;
   const int n_k = K / kTK;
+  const int tiles_n = N / kTN, per_product = tiles_n * ((M + kTM - 1) / kTM);
+  const int tiles = per_product * p.count;
   if (threadIdx.x == 0) {
     failed = 0;
+    consumed = 0;
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(done, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], kEpilogueWarps);
+    }
+    mbar_init(drain, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncwarp();
-  if (warp == 0) {  // the whole warp allocates the accumulator's columns
+  if (warp == 0) {  // the whole warp allocates both accumulators' columns
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(kTmemColumns)
                  : "memory");
@@ -80,82 +122,126 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (threadIdx.x == 0) {
-    // producer: the K slices of A and W, stage by stage
-    for (int k = 0; k < n_k; ++k) {
-      const int s = k % kStages;
-      const uint32_t round = k / kStages;
-      if (k >= kStages && !mbar_wait(&empty[s], (round - 1) & 1)) {
-        failed = 1;
-        break;
+    // producer: the K slices of every tile of this CTA, through the ring
+    long g = 0;
+    for (int t = blockIdx.x; t < tiles && !failed; t += gridDim.x) {
+      const int q = t / per_product, u = t % per_product;
+      const int m0 = (u / tiles_n) * kTM, n0 = (u % tiles_n) * kTN;
+      for (int k = 0; k < n_k; ++k, ++g) {
+        const int s = (int)(g % kStages);
+        const uint32_t round = (uint32_t)(g / kStages);
+        if (g >= kStages && !mbar_wait(&empty[s], (round - 1) & 1)) {
+          failed = 1;
+          break;
+        }
+        if (failed) break;
+        unsigned char* stage = ring + (size_t)s * kStageBytes;
+        mbar_expect_tx(&full[s], kStageBytes);
+        tma_load_2d(stage, &p.a[q], &full[s], k * kTK, m0);
+        tma_load_2d(stage + kABytes, &p.w[q], &full[s], k * kTK, n0);
       }
-      unsigned char* stage = ring + (size_t)s * kStageBytes;
-      mbar_expect_tx(&full[s], kStageBytes);
-      tma_load_2d(stage, &map_a, &full[s], k * kTK, m0);
-      tma_load_2d(stage + kABytes, &map_w, &full[s], k * kTK, n0);
     }
+    // on failure: the loads still in flight land before the CTA leaves
+    if (failed)
+      for (long h = consumed; h < g; ++h) mbar_wait(&full[h % kStages], (uint32_t)(h / kStages) & 1);
   } else if (threadIdx.x == 32) {
-    // the MMA issuer: four 16-wide K steps per stage, the stage handed back on completion
-    for (int k = 0; k < n_k; ++k) {
-      const int s = k % kStages;
-      const uint32_t round = k / kStages;
-      if (!mbar_wait(&full[s], round & 1)) {
+    // the MMA issuer: tile i into accumulator i % 2 once the epilogue has read it
+    long g = 0;
+    int it = 0;
+    for (int t = blockIdx.x; t < tiles && !failed; t += gridDim.x, ++it) {
+      const int b = it & 1, use = it >> 1;
+      if (use >= 1 && !mbar_wait(&acc_empty[b], (use - 1) & 1)) {
         failed = 1;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const unsigned char* stage = ring + (size_t)s * kStageBytes;
-      const uint64_t da = sw128_desc(stage), db = sw128_desc(stage + kABytes);
-#pragma unroll
-      for (int kk = 0; kk < kTK / 16; ++kk)
-        umma_bf16(tmem, da + 2ull * kk, db + 2ull * kk, kIdesc, (k | kk) != 0 ? 1u : 0u);
-      umma_commit(&empty[s]);
-    }
-    umma_commit(done);  // every MMA issued above has completed when this arrives
-  }
-  __syncwarp();
-  // epilogue: warp w holds accumulator lanes (rows) 32 w .. 32 w + 31; the tile goes
-  // through shared memory (the drained ring, rows padded by one word against bank
-  // conflicts) so that it leaves in coalesced rows
-  const bool ok = mbar_wait(done, 0);
-  __syncwarp();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  constexpr int kPitch = kTN + 1;
-  static_assert((size_t)kTM * kPitch * 4 <= (size_t)kStages * kStageBytes, "the tile fits in the ring");
-  float* tile = reinterpret_cast<float*>(ring);
-  const int quarter = warp % 4;  // the accumulator lanes this warp may read
-  const int row = quarter * 32 + lane;
-  const int c_lo = (warp / 4) * kEpilogueColumns;
-  for (int c = c_lo; c < c_lo + kEpilogueColumns; c += 32) {
-    uint32_t r[32];
-    __syncwarp();  // the load is warp-wide (.sync.aligned)
-    tmem_load_32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c, r);
-#pragma unroll
-    for (int j = 0; j < 32; ++j) tile[row * kPitch + c + j] = __uint_as_float(r[j]);
-  }
-  __syncthreads();
-  if (ok && !failed) {
-    for (int rr = warp; rr < kTM && m0 + rr < M; rr += kThreads / 32) {
-      const size_t m = (size_t)(m0 + rr);
-      for (int cc = lane; cc < kTN; cc += 32) {
-        const int n = n0 + cc;
-        float v = tile[rr * kPitch + cc];
-        if (epilogue >= 1 && bias) v += bias[n];
-        if (epilogue == 3) {  // training: the pre-activation in FP32, the activation in BF16
-          if (C) C[m * ldc + n] = v;
-          if (C16) C16[m * ldc16 + n] = __float2bfloat16_rn(gelu(v));
-          continue;
+      const uint32_t acc = tmem + (uint32_t)b * kAccColumns;
+      for (int k = 0; k < n_k; ++k, ++g) {
+        const int s = (int)(g % kStages);
+        const uint32_t round = (uint32_t)(g / kStages);
+        if (!mbar_wait(&full[s], round & 1)) {
+          failed = 1;
+          break;
         }
-        if (epilogue == 2) v = gelu(v);
-        if (C) C[m * ldc + n] = v;
-        if (C16) C16[m * ldc16 + n] = __float2bfloat16_rn(v);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned char* stage = ring + (size_t)s * kStageBytes;
+        const uint64_t da = sw128_desc(stage), db = sw128_desc(stage + kABytes);
+#pragma unroll
+        for (int kk = 0; kk < kTK / 16; ++kk)
+          umma_bf16(acc, da + 2ull * kk, db + 2ull * kk, kIdesc, (k | kk) != 0 ? 1u : 0u);
+        umma_commit(&empty[s]);
+        consumed = (int)(g + 1);
+      }
+      if (failed) break;
+      umma_commit(&acc_full[b]);
+    }
+    umma_commit(drain);  // every product issued above has completed when this arrives
+  } else if (warp >= 2) {
+    // epilogue: warp w reads accumulator lanes (rows) 32 (w % 4) .. + 31, columns
+    // kEpilogueColumns ((w - 2) / 4) onwards, 32 at a time through its staging block, so
+    // that the rows leave coalesced
+    const int quarter = warp % 4, slice = (warp - 2) / 4;
+    float* stg = staging + (size_t)(warp - 2) * 32 * kStagePitch;
+    int it = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+      const int q = t / per_product, u = t % per_product;
+      const int m0 = (u / tiles_n) * kTM, n0 = (u % tiles_n) * kTN;
+      float* const C = p.C[q];
+      __nv_bfloat16* const C16 = p.C16[q];
+      const float* const bias = p.bias[q];
+      const int b = it & 1;
+      const bool ok = mbar_wait(&acc_full[b], (it >> 1) & 1);
+      if (!ok || failed) {
+        failed = 1;
+        break;
+      }
+      __syncwarp();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t acc = tmem + (uint32_t)b * kAccColumns + ((uint32_t)(quarter * 32) << 16);
+      for (int c = slice * kEpilogueColumns; c < (slice + 1) * kEpilogueColumns; c += 32) {
+        uint32_t r[32];
+        __syncwarp();  // the load is warp-wide (.sync.aligned)
+        tmem_load_32(acc + (uint32_t)c, r);
+        if (c + 32 == (slice + 1) * kEpilogueColumns) {
+          // the accumulator is read: the next tile's products may overwrite it
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[b]);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) stg[lane * kStagePitch + j] = __uint_as_float(r[j]);
+        __syncwarp();
+        const int n = n0 + c + lane;
+        const bool biased = epilogue >= 1 && bias;
+        const float bn = biased ? bias[n] : 0.0f;
+        for (int rr = 0; rr < 32; ++rr) {
+          const int row = m0 + quarter * 32 + rr;
+          if (row >= M) break;
+          const size_t m = (size_t)row;
+          float v = stg[rr * kStagePitch + lane];
+          if (biased) v += bn;
+          if (epilogue == 3) {  // training: the pre-activation in FP32, the activation in BF16
+            if (C) C[m * ldc + n] = v;
+            if (C16) C16[m * ldc16 + n] = __float2bfloat16_rn(gelu(v));
+            continue;
+          }
+          if (epilogue == 2) v = gelu(v);
+          if (C) C[m * ldc + n] = v;
+          if (C16) C16[m * ldc16 + n] = __float2bfloat16_rn(v);
+        }
+        __syncwarp();
       }
     }
   }
+  __syncwarp();  // warps 0 and 1 wait for their producing / issuing lane before the barrier
+  __syncthreads();
+  // the products issued (all of them, or those before a failure) are complete
+  if (threadIdx.x == 0 && !mbar_wait(drain, 0)) failed = 1;
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns) : "memory");
-  if (threadIdx.x == 0 && (!ok || failed)) atomicExch(status, 1);
+  if (threadIdx.x == 0 && failed) atomicExch(status, 1);
 }
 
 // FP32 rows -> BF16 rows (zero-padded to `cols_out` columns)
@@ -201,26 +287,52 @@ bool make_map(CUtensorMap* map, const void* base, int rows, int cols, int ld, in
 
 extern "C" {
 
-sp_status sp_mlp_gemm_tc(const void* A, int lda, const void* W, int ldw, float* C, int ldc, void* C16,
-                         int ldc16, int M, int N, int K, const float* bias, int epilogue, int* status,
-                         void* stream) {
+sp_status sp_mlp_gemm_tc_batch(int count, const void* const* A, int lda, const void* const* W, int ldw,
+                               float* const* C, int ldc, void* const* C16, int ldc16, int M, int N, int K,
+                               const float* const* bias, int epilogue, int* status, void* stream) {
   using namespace sp;
-  if (!A || !W || (!C && !C16) || !status || M < 1 || N < 1 || K < 1 || epilogue < 0 || epilogue > 3)
+  if (count < 1 || count > kMaxProducts || !A || !W || !status || M < 1 || N < 1 || K < 1 || epilogue < 0 ||
+      epilogue > 3)
     return SP_ERR_ARGUMENT;
   // the tiling's and the tensor maps' rules: whole 256-column tiles and 64-wide K slices,
   // 16-byte aligned rows
   if (N % kTN || K % kTK || lda % 8 || ldw % 8 || lda < K || ldw < K) return SP_ERR_ARGUMENT;
-  if (((uintptr_t)A | (uintptr_t)W) & 15) return SP_ERR_ARGUMENT;
-  CUtensorMap map_a, map_w;
-  if (!make_map(&map_a, A, M, K, lda, kTM) || !make_map(&map_w, W, N, K, ldw, kTN)) return SP_ERR_CUDA;
+  GemmBatch batch{};
+  batch.count = count;
+  for (int q = 0; q < count; ++q) {
+    float* c = C ? C[q] : nullptr;
+    void* c16 = C16 ? C16[q] : nullptr;
+    if (!A[q] || !W[q] || (!c && !c16)) return SP_ERR_ARGUMENT;
+    if (((uintptr_t)A[q] | (uintptr_t)W[q]) & 15) return SP_ERR_ARGUMENT;
+    if (!make_map(&batch.a[q], A[q], M, K, lda, kTM) || !make_map(&batch.w[q], W[q], N, K, ldw, kTN))
+      return SP_ERR_CUDA;
+    batch.C[q] = c;
+    batch.C16[q] = static_cast<__nv_bfloat16*>(c16);
+    batch.bias[q] = bias ? bias[q] : nullptr;
+  }
   static std::once_flag configured;
   std::call_once(configured, [] {
     cudaFuncSetAttribute(k_mlp_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
   });
-  const dim3 grid(N / kTN, (M + kTM - 1) / kTM);
-  k_mlp_gemm_tc<<<grid, kThreads, kSmemBytes, (cudaStream_t)stream>>>(
-      map_a, map_w, C, static_cast<__nv_bfloat16*>(C16), bias, M, N, K, ldc, ldc16, epilogue, status);
+  static int n_sms = 0;
+  if (!n_sms) {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || n_sms < 1)
+      return SP_ERR_CUDA;
+  }
+  const int tiles = count * (N / kTN) * ((M + kTM - 1) / kTM);
+  k_mlp_gemm_tc<<<tiles < n_sms ? tiles : n_sms, kThreads, kSmemBytes, (cudaStream_t)stream>>>(
+      batch, M, N, K, ldc, ldc16, epilogue, status);
   return cudaGetLastError() == cudaSuccess ? SP_OK : SP_ERR_CUDA;
+}
+
+sp_status sp_mlp_gemm_tc(const void* A, int lda, const void* W, int ldw, float* C, int ldc, void* C16,
+                         int ldc16, int M, int N, int K, const float* bias, int epilogue, int* status,
+                         void* stream) {
+  if (!C && !C16) return SP_ERR_ARGUMENT;
+  return sp_mlp_gemm_tc_batch(1, &A, lda, &W, ldw, &C, ldc, &C16, ldc16, M, N, K, &bias, epilogue, status,
+                              stream);
 }
 
 sp_status sp_mlp_transpose_bf16(const void* src, int src_bf16, int ld_src, int rows, int cols, void* dst,

@@ -84,6 +84,34 @@ def gemm_tc(a16, w16, *, out=None, out16=None, bias=None, epilogue=0, status=Non
     return status
 
 
+def gemm_tc_batch(a16s, w16s, *, outs=None, outs16=None, biases=None, epilogue=0, status=None, stream=None):
+    """gemm_tc for several operand sets of one shape (an ensemble's members through one
+    layer) in one launch: out[q] / out16[q] = a16s[q] w16s[q]^T (+ biases[q]) (GELU)."""
+    import ctypes as C
+
+    import torch
+
+    lib = _bind()
+    count = len(a16s)
+    m, k = a16s[0].shape
+    n, kw = w16s[0].shape
+    if kw != k or len(w16s) != count or any(a.shape != (m, k) or a.stride(0) != a16s[0].stride(0) for a in a16s) \
+            or any(w.shape != (n, k) or w.stride(0) != w16s[0].stride(0) for w in w16s):
+        raise ValueError("gemm_tc_batch: every product takes the same shapes and pitches")
+    if status is None:
+        status = torch.zeros(1, dtype=torch.int32, device=a16s[0].device)
+
+    def pointers(ts):
+        return (C.c_void_p * count)(*[_ptr(t) if t is not None else None for t in ts]) if ts is not None else None
+
+    ld = outs[0].stride(0) if outs is not None else 0
+    ld16 = outs16[0].stride(0) if outs16 is not None else 0
+    _check(lib.sp_mlp_gemm_tc_batch(count, pointers(a16s), a16s[0].stride(0), pointers(w16s), w16s[0].stride(0),
+                                    pointers(outs), ld, pointers(outs16), ld16, m, n, k, pointers(biases),
+                                    epilogue, _ptr(status), stream))
+    return status
+
+
 def to_bf16(x, cols_out: int):
     """BF16 copy of an FP32 (rows, cols) tensor, zero-padded to cols_out columns."""
     import torch
@@ -363,6 +391,32 @@ class Ensemble:
             member.refresh_bf16()
         return last
 
+    def infer(self, x, status=None):
+        """Every member's outputs for x (rows), (members, rows, N_OUT) in FP32: the tcgen05
+        products with all members through a layer in one launch (BF16 activations between
+        the layers, FP32 accumulation), the same arithmetic as Perceptron.infer."""
+        import torch
+
+        for member in self.members:
+            if member.w16 is None:
+                member.refresh_bf16()
+        first = self.members[0]
+        a = to_bf16(x, first.w16[0].shape[1])
+        acts = [a] * len(self.members)
+        last = len(first.weights) - 1
+        for i in range(last + 1):
+            ws = [member.w16[i] for member in self.members]
+            bs = [member.biases[i] for member in self.members]
+            if i == last:
+                out = torch.empty((len(self.members), a.shape[0], ws[0].shape[0]), dtype=torch.float32,
+                                  device=first.device)
+                status = gemm_tc_batch(acts, ws, outs=list(out), biases=bs, epilogue=1, status=status)
+                return out, status
+            nxt = torch.empty((len(self.members), a.shape[0], ws[0].shape[0]), dtype=torch.bfloat16,
+                              device=first.device)
+            status = gemm_tc_batch(acts, ws, outs16=list(nxt), biases=bs, epilogue=2, status=status)
+            acts = list(nxt)
+
     def predict(self, x: np.ndarray, chunk: int = 16384):
         """Ensemble mean (log10 spectra) and disagreement of every row of x."""
         import torch
@@ -377,14 +431,12 @@ class Ensemble:
         for s in range(0, n, chunk):
             xb = torch.tensor(x[s:s + chunk], device=dev)
             m = xb.shape[0]
-            ys = torch.empty((e, m, N_OUT), dtype=torch.float32, device=dev)
             status = torch.zeros(1, dtype=torch.int32, device=dev)
-            for k, member in enumerate(self.members):
-                if m >= 128:
-                    out, status = member.infer(xb, status)
-                else:
-                    out, _ = member.forward(xb)
-                ys[k] = out * scale + offset
+            if m >= 128:
+                ys, status = self.infer(xb, status)
+                ys = ys * scale + offset
+            else:
+                ys = torch.stack([member.forward(xb)[0] for member in self.members]) * scale + offset
             if int(status.item()):
                 raise RuntimeError("a tensor-core product's wait gave up")
             mu = torch.empty((m, N_OUT), dtype=torch.float32, device=dev)

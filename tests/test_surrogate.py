@@ -108,6 +108,24 @@ def test_inference_on_tcgen05_matches_the_training_path():
 
 
 @gpu
+def test_ensemble_products_in_one_launch_match_each_member():
+    """Every member through a layer in one launch (the persistent kernel walks all their
+    tiles) gives each member's own products bit for bit, on a row count that leaves a
+    partial last row tile."""
+    from solprop_b200 import surrogate as S
+
+    torch = _torch()
+    ens = S.Ensemble(members=3, seed=4)
+    x = torch.tensor(np.random.default_rng(2).uniform(-1, 1, (700, 6)).astype(np.float32), device="cuda")
+    ys, status = ens.infer(x)
+    assert int(status.item()) == 0 and tuple(ys.shape) == (3, 700, S.N_OUT)
+    for k, member in enumerate(ens.members):
+        y, st = member.infer(x)
+        assert int(st.item()) == 0
+        assert torch.equal(ys[k], y)
+
+
+@gpu
 def test_gelu_epilogue_and_preactivation():
     from solprop_b200 import surrogate as S
 
