@@ -40,8 +40,8 @@ constexpr int kEpilogueColumns = kTN / (kEpilogueWarps / 4);
 constexpr uint32_t kABytes = kTM * kTK * 2;  // 16 KB
 constexpr uint32_t kBBytes = kTN * kTK * 2;  // 32 KB
 constexpr uint32_t kStageBytes = kABytes + kBBytes;
-constexpr int kStagePitch = 33;  // an epilogue warp's 32 x 32 staging block, rows padded by a word
-constexpr size_t kStagingBytes = (size_t)kEpilogueWarps * 32 * kStagePitch * 4;
+// an epilogue warp's 32 x 32 FP32 staging block (rows of 128 bytes, 16-byte units swizzled)
+constexpr size_t kStagingBytes = (size_t)kEpilogueWarps * 32 * 32 * 4;
 constexpr size_t kSmemBytes = (size_t)kStages * kStageBytes + kStagingBytes + 1024 + 256;
 static_assert(kSmemBytes + 64 <= 232448, "the ring, the staging and the barriers fit one CTA");
 constexpr uint32_t kAccColumns = 256;      // one FP32 accumulator: 256 columns x 128 lanes
@@ -178,17 +178,18 @@ __global__ void __launch_bounds__(kThreads, 1)
     umma_commit(drain);  // every product issued above has completed when this arrives
   } else if (warp >= 2) {
     // epilogue: warp w reads accumulator lanes (rows) 32 (w % 4) .. + 31, columns
-    // kEpilogueColumns ((w - 2) / 4) onwards, 32 at a time through its staging block, so
-    // that the rows leave coalesced
+    // kEpilogueColumns ((w - 2) / 4) onwards, 32 at a time: each lane applies the bias and
+    // the GELU to its row's 32 values in registers, and the rows leave through the warp's
+    // staging block as 16-byte stores
     const int quarter = warp % 4, slice = (warp - 2) / 4;
-    float* stg = staging + (size_t)(warp - 2) * 32 * kStagePitch;
+    float4* stg = reinterpret_cast<float4*>(staging + (size_t)(warp - 2) * 32 * 32);
     int it = 0;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
       const int q = t / per_product, u = t % per_product;
       const int m0 = (u / tiles_n) * kTM, n0 = (u % tiles_n) * kTN;
       float* const C = p.C[q];
       __nv_bfloat16* const C16 = p.C16[q];
-      const float* const bias = p.bias[q];
+      const float* const bias = epilogue >= 1 ? p.bias[q] : nullptr;
       const int b = it & 1;
       const bool ok = mbar_wait(&acc_full[b], (it >> 1) & 1);
       if (!ok || failed) {
@@ -198,6 +199,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       __syncwarp();
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t acc = tmem + (uint32_t)b * kAccColumns + ((uint32_t)(quarter * 32) << 16);
+      const int m_first = m0 + quarter * 32;
+      const int rows = min(32, M - m_first);  // the rows inside the matrix
       for (int c = slice * kEpilogueColumns; c < (slice + 1) * kEpilogueColumns; c += 32) {
         uint32_t r[32];
         __syncwarp();  // the load is warp-wide (.sync.aligned)
@@ -208,28 +211,67 @@ __global__ void __launch_bounds__(kThreads, 1)
           __syncwarp();
           if (lane == 0) mbar_arrive(&acc_empty[b]);
         }
+        const int nb = n0 + c;  // the chunk's first column
+        float v[32];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) stg[lane * kStagePitch + j] = __uint_as_float(r[j]);
-        __syncwarp();
-        const int n = n0 + c + lane;
-        const bool biased = epilogue >= 1 && bias;
-        const float bn = biased ? bias[n] : 0.0f;
-        for (int rr = 0; rr < 32; ++rr) {
-          const int row = m0 + quarter * 32 + rr;
-          if (row >= M) break;
-          const size_t m = (size_t)row;
-          float v = stg[rr * kStagePitch + lane];
-          if (biased) v += bn;
-          if (epilogue == 3) {  // training: the pre-activation in FP32, the activation in BF16
-            if (C) C[m * ldc + n] = v;
-            if (C16) C16[m * ldc16 + n] = __float2bfloat16_rn(gelu(v));
-            continue;
+        for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+        if (bias) {
+#pragma unroll
+          for (int j4 = 0; j4 < 8; ++j4) {
+            const float4 b4 = __ldg(reinterpret_cast<const float4*>(bias + nb) + j4);
+            v[4 * j4] += b4.x;
+            v[4 * j4 + 1] += b4.y;
+            v[4 * j4 + 2] += b4.z;
+            v[4 * j4 + 3] += b4.w;
           }
-          if (epilogue == 2) v = gelu(v);
-          if (C) C[m * ldc + n] = v;
-          if (C16) C16[m * ldc16 + n] = __float2bfloat16_rn(v);
         }
-        __syncwarp();
+        if (epilogue == 2) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
+        }
+        if (C) {
+          // FP32 rows: lane `lane` (row) writes its eight 16-byte units, unit s of row rr at
+          // slot s ^ (rr & 7) (eight lanes of a wavefront, eight banks groups); then lanes
+          // 8 i .. 8 i + 7 take row 4 k + i's units in turn, 16-byte stores along the row
+#pragma unroll
+          for (int s4 = 0; s4 < 8; ++s4)
+            stg[lane * 8 + (s4 ^ (lane & 7))] = make_float4(v[4 * s4], v[4 * s4 + 1], v[4 * s4 + 2], v[4 * s4 + 3]);
+          __syncwarp();
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const int rr = 4 * k + (lane >> 3), s4 = lane & 7;
+            const float4 x = stg[rr * 8 + (s4 ^ (rr & 7))];
+            if (rr < rows) *reinterpret_cast<float4*>(C + (size_t)(m_first + rr) * ldc + nb + 4 * s4) = x;
+          }
+          __syncwarp();
+        }
+        if (C16) {
+          if (epilogue == 3) {  // training: the pre-activation above, its GELU here
+#pragma unroll
+            for (int j = 0; j < 32; ++j) v[j] = gelu(v[j]);
+          }
+          // BF16 rows of 64 bytes: unit s (eight values) of row rr at slot s ^ ((rr >> 1) & 3)
+          // of that row's four; lanes 4 i .. 4 i + 3 then take row 8 k + i's units
+          uint4* stg16 = reinterpret_cast<uint4*>(stg);
+#pragma unroll
+          for (int s8 = 0; s8 < 4; ++s8) {
+            uint32_t w[4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+              const __nv_bfloat162 pair = __floats2bfloat162_rn(v[8 * s8 + 2 * h], v[8 * s8 + 2 * h + 1]);
+              w[h] = *reinterpret_cast<const uint32_t*>(&pair);
+            }
+            stg16[lane * 4 + (s8 ^ ((lane >> 1) & 3))] = make_uint4(w[0], w[1], w[2], w[3]);
+          }
+          __syncwarp();
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int rr = 8 * k + (lane >> 2), s8 = lane & 3;
+            const uint4 x = stg16[rr * 4 + (s8 ^ ((rr >> 1) & 3))];
+            if (rr < rows) *reinterpret_cast<uint4*>(C16 + (size_t)(m_first + rr) * ldc16 + nb + 8 * s8) = x;
+          }
+          __syncwarp();
+        }
       }
     }
   }
@@ -297,13 +339,16 @@ sp_status sp_mlp_gemm_tc_batch(int count, const void* const* A, int lda, const v
   // the tiling's and the tensor maps' rules: whole 256-column tiles and 64-wide K slices,
   // 16-byte aligned rows
   if (N % kTN || K % kTK || lda % 8 || ldw % 8 || lda < K || ldw < K) return SP_ERR_ARGUMENT;
+  // the epilogue's 16-byte row stores and bias loads
+  if ((C && ldc % 4) || (C16 && ldc16 % 8)) return SP_ERR_ARGUMENT;
   GemmBatch batch{};
   batch.count = count;
   for (int q = 0; q < count; ++q) {
     float* c = C ? C[q] : nullptr;
     void* c16 = C16 ? C16[q] : nullptr;
     if (!A[q] || !W[q] || (!c && !c16)) return SP_ERR_ARGUMENT;
-    if (((uintptr_t)A[q] | (uintptr_t)W[q]) & 15) return SP_ERR_ARGUMENT;
+    if (((uintptr_t)A[q] | (uintptr_t)W[q] | (uintptr_t)c | (uintptr_t)c16) & 15) return SP_ERR_ARGUMENT;
+    if (bias && bias[q] && ((uintptr_t)bias[q] & 15)) return SP_ERR_ARGUMENT;
     if (!make_map(&batch.a[q], A[q], M, K, lda, kTM) || !make_map(&batch.w[q], W[q], N, K, ldw, kTN))
       return SP_ERR_CUDA;
     batch.C[q] = c;
