@@ -325,6 +325,11 @@ struct sp_workspace {
       stages, back;
   DevBuf<AdamsDev> adams;
   AdamsDev* h_adams = nullptr;       // pinned
+  // The trial's table then the stage slots, in one pinned and one device allocation
+  // (h_adams / h_stage and adams / stage are views into them), so that a single copy
+  // carries an attempt's tables
+  unsigned char* h_tables = nullptr;
+  DevBuf<unsigned char> tables;
   DevBuf<double> partials, norms;
   DevBuf<unsigned> norm_arrivals;    // the single-run corrector's block count (zero between launches)
   double* h_norms = nullptr;         // pinned
@@ -380,8 +385,7 @@ struct sp_workspace {
     for (auto e : ev_pool) cudaEventDestroy(e);
     if (host_tables_free) cudaEventDestroy(host_tables_free);
     if (stream) cudaStreamSynchronize(stream);
-    if (h_stage) cudaFreeHost(h_stage);
-    if (h_adams) cudaFreeHost(h_adams);
+    if (h_tables) cudaFreeHost(h_tables);
     if (h_norms) cudaFreeHost(h_norms);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -1019,12 +1023,20 @@ static void build_workspace(sp_workspace* ws) {
   ws->streams.zero(s);
   ws->spectra.alloc((size_t)4 * n);
   ws->spectra.zero(s);
-  ws->stage.alloc(sp_workspace::kStageSlots);
+  static_assert(sizeof(AdamsDev) % alignof(StageScalarsDev) == 0, "the stage slots follow the trial's table");
+  const size_t table_bytes = sizeof(AdamsDev) + sizeof(StageScalarsDev) * sp_workspace::kStageSlots;
+  ws->tables.alloc(table_bytes);
+  ws->adams.p = reinterpret_cast<AdamsDev*>(ws->tables.p);
+  ws->adams.n = 1;
+  ws->adams.owned = false;
+  ws->stage.p = reinterpret_cast<StageScalarsDev*>(ws->tables.p + sizeof(AdamsDev));
+  ws->stage.n = sp_workspace::kStageSlots;
+  ws->stage.owned = false;
   CUDA_CHECK(cudaEventCreateWithFlags(&ws->host_tables_free, cudaEventDisableTiming));
-  CUDA_CHECK(cudaMallocHost(&ws->h_stage, sizeof(StageScalarsDev) * sp_workspace::kStageSlots));
-  CUDA_CHECK(cudaMallocHost(&ws->h_adams, sizeof(AdamsDev)));
+  CUDA_CHECK(cudaMallocHost(&ws->h_tables, table_bytes));
+  ws->h_adams = reinterpret_cast<AdamsDev*>(ws->h_tables);
+  ws->h_stage = reinterpret_cast<StageScalarsDev*>(ws->h_tables + sizeof(AdamsDev));
   CUDA_CHECK(cudaMallocHost(&ws->h_norms, sizeof(double) * 8));
-  ws->adams.alloc(1);
   ws->partials.alloc((kMaxOrders + 2) * kNormBlocks);
   ws->norms.alloc(kMaxOrders + 2);
   ws->norms.zero(s);
@@ -1446,9 +1458,9 @@ static void check_column(const double* h_norms, double* d_norms, cudaStream_t s)
 // step's two stage slots and tables from the pinned buffers, the predictor, the source at the
 // predicted field, the corrector with its reduction, the norms to the pinned host buffer.
 static void issue_attempt(sp_workspace* ws, const StepArgs& a) {
-  CUDA_CHECK(cudaMemcpyAsync(ws->stage.p, ws->h_stage, 2 * sizeof(StageScalarsDev), cudaMemcpyHostToDevice,
-                             ws->stream));
-  CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, ws->h_adams, sizeof(AdamsDev), cudaMemcpyHostToDevice, ws->stream));
+  // the trial's table and the step's two stage slots, contiguous on both sides: one copy
+  CUDA_CHECK(cudaMemcpyAsync(ws->adams.p, ws->h_adams, sizeof(AdamsDev) + 2 * sizeof(StageScalarsDev),
+                             cudaMemcpyHostToDevice, ws->stream));
   { KernelTimer t(ws, SP_K_PREDICT); CUDA_CHECK(launch_adams_predict(a, ws->stream)); }
   eval_source(ws, ws->lab.p, 1, nullptr, ws->src.p, false, /*output=*/false);
   const OutputArgs oa = source_output_args(ws, 1, nullptr, ws->src.p, false);
