@@ -62,3 +62,26 @@ def test_invalid_descriptor_is_an_argument_error():
     rec.n_to = 1000  # not a power of two
     with pytest.raises(_lib.NativeError, match="power of two"):
         _lib.Problem(rec)
+
+
+def test_batched_tensor_core_product_refuses_what_it_cannot_take():
+    """sp_mlp_gemm_tc_batch's argument checks run before any device work: a product count
+    outside 1..8, tiles the shapes do not fill, output pitches or operand addresses that its
+    16-byte loads and stores cannot take."""
+    import ctypes as C
+
+    lib = _lib.library()
+    fake = C.c_void_p(0x10000)  # never dereferenced: every call below is refused first
+    one = (C.c_void_p * 1)(fake)
+
+    def call(count=1, A=one, W=one, Cout=one, ldc=512, C16=None, ldc16=0, M=128, N=512, K=64,
+             lda=64, ldw=64):
+        return lib.sp_mlp_gemm_tc_batch(count, A, lda, W, ldw, Cout, ldc, C16, ldc16, M, N, K, None, 1,
+                                        fake, None)
+
+    assert call(count=0) == 1 and call(count=9) == 1
+    assert call(N=500) == 1 and call(K=96) == 1 and call(lda=60) == 1
+    assert call(ldc=510) == 1  # FP32 rows leave as 16-byte stores
+    assert call(Cout=None, C16=one, ldc16=500) == 1  # BF16 rows likewise
+    odd = (C.c_void_p * 1)(C.c_void_p(0x10008))
+    assert call(A=odd) == 1 and call(Cout=odd) == 1
